@@ -1,0 +1,309 @@
+"""ctypes wrappers for the test oracles.
+
+* ``Oracle``: the project's C restatement of the reference hot path
+  (oracle/c3d_oracle.c -> oracle/_build/liboracle_c3d.so).
+* ``RefProcess``-side helpers: the reference CPU path compiled from its own
+  sources (oracle/_ref/libc3dref.so). The reference keeps its state in process
+  globals, so each reference problem runs in its own spawned subprocess.
+
+Test infrastructure only; the product never imports this module.
+"""
+from __future__ import annotations
+
+import ctypes
+import multiprocessing as mp
+import os
+import tempfile
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_SO = os.path.join(REPO, "oracle", "_build", "liboracle_c3d.so")
+REF_SO = os.path.join(REPO, "oracle", "_ref", "libc3dref.so")
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+
+DEFAULT_LADDER = [0.0, 1e-3, 1e-2, 1e-1, 5e-1]
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(_dp)
+
+
+def _pi(a):
+    return None if a is None else a.ctypes.data_as(_ip)
+
+
+class ClosureOpts(ctypes.Structure):
+    _fields_ = [("nm", ctypes.c_int), ("nm2", ctypes.c_int), ("nq", ctypes.c_int),
+                ("batched", ctypes.c_int), ("maxIter", ctypes.c_int), ("tol", ctypes.c_double),
+                ("tolGamma", ctypes.c_double), ("condHMax", ctypes.c_double),
+                ("hessMode", ctypes.c_int), ("nreg", ctypes.c_int),
+                ("reg", ctypes.c_double * 16)]
+
+
+class CellOut(ctypes.Structure):
+    _fields_ = [("totalIter", ctypes.c_int), ("iterGamma", ctypes.c_int),
+                ("regIndex", ctypes.c_int), ("status", ctypes.c_int), ("r", ctypes.c_double),
+                ("gamma", ctypes.c_double), ("err", ctypes.c_double),
+                ("armijoUlps", ctypes.c_double), ("tolRel", ctypes.c_double)]
+
+
+CELL_OUT_DTYPE = np.dtype([("totalIter", "i4"), ("iterGamma", "i4"), ("regIndex", "i4"),
+                           ("status", "i4"), ("r", "f8"), ("gamma", "f8"), ("err", "f8"),
+                           ("armijoUlps", "f8"), ("tolRel", "f8")])
+
+# A decision is a rounding tie when it was taken by a margin below what two
+# correct FP64 evaluations of the same quantity may differ by: f is formed
+# from H_00 in one place and by a separate quadrature sum in the other
+# (src/opt/fobj.cpp:126 vs :141-154), each with ~nq roundings of |f|.
+TIE_ARMIJO_ULPS = 256.0
+TIE_TOL_REL = 1e-6
+
+
+def tie_cells(records):
+    """Boolean mask of cells whose solve met a rounding-tie decision."""
+    return (records["armijoUlps"] < TIE_ARMIJO_ULPS) | (records["tolRel"] < TIE_TOL_REL)
+
+
+class Tables(ctypes.Structure):
+    _fields_ = [("M", _dp), ("M2", _dp), ("w", _dp), ("xi", _dp), ("eta", _dp), ("mu", _dp),
+                ("beta", _dp), ("betaVal", _dp), ("betaCol", _ip), ("betaRow", _ip),
+                ("pnops", _dp)]
+
+
+class Grid(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+                ("nm", ctypes.c_int), ("nq", ctypes.c_int), ("dx", ctypes.c_double),
+                ("dy", ctypes.c_double), ("dz", ctypes.c_double), ("theta", ctypes.c_double)]
+
+
+def make_opts(nm, nq, *, nm2=0, batched=True, max_iter=100, tol=1e-8, tol_gamma=1.1,
+              cond_h_max=1e10, hess_mode=0, ladder=None):
+    o = ClosureOpts()
+    o.nm, o.nm2, o.nq = nm, nm2, nq
+    o.batched = 1 if batched else 0
+    o.maxIter = max_iter
+    o.tol = tol
+    o.tolGamma = tol_gamma if batched else 1.1
+    o.condHMax = cond_h_max
+    o.hessMode = hess_mode
+    lad = DEFAULT_LADDER if ladder is None else list(ladder)
+    o.nreg = len(lad)
+    for i, r in enumerate(lad):
+        o.reg[i] = r
+    return o
+
+
+class Oracle:
+    """The C restatement. Holds table arrays alive for the Tables struct."""
+
+    def __init__(self):
+        if not os.path.exists(ORACLE_SO):
+            raise FileNotFoundError(ORACLE_SO + " (run `make -C oracle oracle`)")
+        L = ctypes.CDLL(ORACLE_SO)
+        self.L = L
+        L.orc_closure_many.restype = ctypes.c_long
+        L.orc_closure_many.argtypes = [ctypes.POINTER(ClosureOpts), ctypes.POINTER(Tables),
+                                       ctypes.c_long, _dp, _dp, ctypes.c_void_p]
+        L.orc_step.restype = ctypes.c_long
+        L.orc_step.argtypes = [ctypes.POINTER(Grid), ctypes.POINTER(ClosureOpts),
+                               ctypes.POINTER(Tables), ctypes.c_int, ctypes.c_int, _dp, _dp, _dp,
+                               _dp, ctypes.c_double, ctypes.c_void_p, _dp]
+        L.orc_flux_kinetic.argtypes = [ctypes.POINTER(Grid), ctypes.POINTER(Tables), _dp,
+                                       ctypes.c_int, _dp, _dp]
+        L.orc_flux_moment.argtypes = [ctypes.POINTER(Grid), ctypes.POINTER(Tables), _dp, _dp]
+        L.orc_ghost_fill.argtypes = [ctypes.POINTER(Grid), _dp]
+        L.orc_euler.argtypes = [ctypes.POINTER(Grid), _dp, _dp, _dp, _dp, ctypes.c_double]
+        L.orc_pn_operators.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(Tables), _dp]
+        L.orc_hessian.argtypes = [ctypes.POINTER(ClosureOpts), ctypes.POINTER(Tables), _dp, _dp]
+        L.orc_potrf_lower.argtypes = [ctypes.c_int, _dp]
+        L.orc_pocon_lower.restype = ctypes.c_double
+        L.orc_pocon_lower.argtypes = [ctypes.c_int, _dp, ctypes.c_double]
+        L.orc_potrs_lower.argtypes = [ctypes.c_int, _dp, _dp]
+        L.orc_nrm2.restype = ctypes.c_double
+        L.orc_nrm2.argtypes = [ctypes.c_int, _dp]
+        L.orc_norm1.restype = ctypes.c_double
+        L.orc_norm1.argtypes = [ctypes.c_int, _dp]
+        L.c3d_build_quadrature.argtypes = [ctypes.c_int, ctypes.c_int] + [_dp] * 6
+        L.c3d_gaunt_dense.restype = ctypes.c_int
+        L.c3d_gaunt_dense.argtypes = [ctypes.c_int] * 3 + [_dp, _dp]
+        L.c3d_gaunt_csr.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _dp, _ip, _ip]
+
+    # ------------------------------------------------------------------ tables
+    def tables(self, N, Q, *, with_m2=True, gaunt=False, pn=False):
+        nq, nm, nm2 = 2 * Q * Q, (N + 1) ** 2, (2 * N + 1) ** 2
+        d = dict(w=np.zeros(nq), xi=np.zeros(nq), eta=np.zeros(nq), mu=np.zeros(nq),
+                 M=np.zeros(nq * nm), M2=np.zeros(nq * nm2) if with_m2 or gaunt else None)
+        self.L.c3d_build_quadrature(N, Q, _p(d["w"]), _p(d["xi"]), _p(d["eta"]), _p(d["mu"]),
+                                    _p(d["M"]), _p(d["M2"]))
+        d.update(N=N, Q=Q, nq=nq, nm=nm, nm2=nm2)
+        if gaunt:
+            beta = np.zeros(nm * nm * nm2)
+            nnz = self.L.c3d_gaunt_dense(nm, nm2, nq, _p(d["M2"]), _p(beta))
+            val, col, row = np.zeros(max(nnz, 1)), np.zeros(max(nnz, 1), np.int32), \
+                np.zeros(nm * nm + 1, np.int32)
+            self.L.c3d_gaunt_csr(nm, nm2, _p(beta), _p(val), _pi(col), _pi(row))
+            d.update(beta=beta, betaVal=val, betaCol=col, betaRow=row)
+        d["struct"] = self._tables_struct(d)
+        if pn:
+            ops = np.zeros(6 * nm * nm)
+            self.L.orc_pn_operators(nm, nq, ctypes.byref(d["struct"]), _p(ops))
+            d["pnops"] = ops
+            d["struct"] = self._tables_struct(d)
+        return d
+
+    @staticmethod
+    def _tables_struct(d):
+        t = Tables()
+        t.M, t.M2, t.w = _p(d["M"]), _p(d.get("M2")), _p(d["w"])
+        t.xi, t.eta, t.mu = _p(d["xi"]), _p(d["eta"]), _p(d["mu"])
+        t.beta, t.betaVal = _p(d.get("beta")), _p(d.get("betaVal"))
+        t.betaCol, t.betaRow = _pi(d.get("betaCol")), _pi(d.get("betaRow"))
+        t.pnops = _p(d.get("pnops"))
+        return t
+
+    # ------------------------------------------------------------------ closure
+    def closure(self, opts, tables, u, alpha):
+        """Solves every row of u/alpha (shape [n, nm]) in place; returns records."""
+        n = u.shape[0]
+        out = np.zeros(n, CELL_OUT_DTYPE)
+        self.L.orc_closure_many(ctypes.byref(opts), ctypes.byref(tables["struct"]), n, _p(u),
+                                _p(alpha), out.ctypes.data_as(ctypes.c_void_p))
+        return out
+
+    def hessian(self, opts, tables, alpha):
+        h = np.zeros(opts.nm * opts.nm)
+        self.L.orc_hessian(ctypes.byref(opts), ctypes.byref(tables["struct"]), _p(alpha), _p(h))
+        return h.reshape(opts.nm, opts.nm)
+
+    # ------------------------------------------------------------------ grid
+    @staticmethod
+    def grid(nx, ny, nz, nm, nq, dx, dy, dz, theta=2.0):
+        g = Grid()
+        g.nx, g.ny, g.nz, g.nm, g.nq = nx, ny, nz, nm, nq
+        g.dx, g.dy, g.dz, g.theta = dx, dy, dz, theta
+        return g
+
+    def step(self, g, opts, tables, u, alpha, sig_t, sig_s, dt, *, solver=1, pn_kinetic=0,
+             records=True):
+        nall = (g.nx + 4) * (g.ny + 4) * (g.nz + 4)
+        scratch = np.zeros(2 * nall * g.nm + nall)
+        rec = np.zeros(2 * nall, CELL_OUT_DTYPE) if records else None
+        bad = self.L.orc_step(ctypes.byref(g), ctypes.byref(opts), ctypes.byref(tables["struct"]),
+                              solver, pn_kinetic, _p(u), _p(alpha), _p(sig_t), _p(sig_s), dt,
+                              None if rec is None else rec.ctypes.data_as(ctypes.c_void_p),
+                              _p(scratch))
+        return bad, rec
+
+    def flux_kinetic(self, g, tables, alpha, is_pn=0):
+        nall = (g.nx + 4) * (g.ny + 4) * (g.nz + 4)
+        flux = np.zeros(nall * g.nm)
+        scratch = np.zeros(nall)
+        self.L.orc_flux_kinetic(ctypes.byref(g), ctypes.byref(tables["struct"]), _p(alpha), is_pn,
+                                _p(flux), _p(scratch))
+        return flux
+
+    def flux_moment(self, g, tables, u):
+        nall = (g.nx + 4) * (g.ny + 4) * (g.nz + 4)
+        flux = np.zeros(nall * g.nm)
+        self.L.orc_flux_moment(ctypes.byref(g), ctypes.byref(tables["struct"]), _p(u), _p(flux))
+        return flux
+
+    def ghost_fill(self, g, u):
+        self.L.orc_ghost_fill(ctypes.byref(g), _p(u))
+
+    def euler(self, g, u, flux, sig_t, sig_s, dt):
+        self.L.orc_euler(ctypes.byref(g), _p(u), _p(flux), _p(sig_t), _p(sig_s), dt)
+
+
+# ---------------------------------------------------------------------- reference
+DECK_KEYS_DEFAULT = dict(
+    SOLVER="mn", TFINAL="0.1", OUTDT="1000", OUTPUT_DATA="false", OUTPUT_OPT_STATS="false",
+    OUTPUT_TIMINGS="false", NX="8", NY="8", NZ="8", MPIX="1", MPIY="1", MPIZ="1", AX="-1",
+    AY="-1", AZ="-1", BX="1", BY="1", BZ="1", MOMENT_ORDER="2", QUAD_ORDER="12",
+    CFL_FACTOR="0.5", CROSS_SECTION="1.0", INIT_FLOOR="1e-4", GAUSS_SIGMA="0.2",
+    INIT_COND="gaussian", THETA="2.0", OMP_THREADS="4", PN_USE_KINETIC_FLUX="0", MN_TOL="1e-8",
+    MN_TOL_GAMMA="1.1", MN_COND_H_MAX="1e10", MN_MAX_ITER="100", MN_BATCHED="true",
+    MN_USE_GAUNT_COEF="false", MN_USE_GAUNT_SPARSE="false", CUDA_KINETIC="false",
+    CUDA_BATCHED="false", CUDA_BATCH_SIZE="50")
+
+
+def deck_text(**kw):
+    d = dict(DECK_KEYS_DEFAULT)
+    d.update({k: str(v) for k, v in kw.items()})
+    return "".join(f"{k} {v}\n" for k, v in d.items())
+
+
+def _ref_worker(conn, deck, ladder, nsteps, overrides, record, want):
+    """Runs inside a spawned process: one reference problem."""
+    L = ctypes.CDLL(REF_SO)
+    L.c3dref_init.argtypes = [ctypes.c_char_p]
+    L.c3dref_ptr.restype = _dp
+    L.c3dref_update.argtypes = [ctypes.c_double]
+    L.c3dref_step_traced.argtypes = [ctypes.c_double, _ip, _ip, _ip, _dp]
+    if ladder is not None:
+        lad = np.asarray(ladder, float)
+        L.c3dref_set_ladder(len(lad), _p(lad))
+    with tempfile.TemporaryDirectory() as tmp:
+        with open(os.path.join(tmp, "input.deck"), "w") as f:
+            f.write(deck)
+        rc = L.c3dref_init(tmp.encode())
+    assert rc == 0, rc
+    iv = (ctypes.c_int * 16)()
+    dv = (ctypes.c_double * 16)()
+    L.c3dref_info(iv, dv)
+    nx, ny, nz, nm, nm2, nq = iv[0], iv[1], iv[2], iv[3], iv[4], iv[5]
+    nall = (nx + 4) * (ny + 4) * (nz + 4)
+
+    def arr(which, n):
+        return np.ctypeslib.as_array(L.c3dref_ptr(which), shape=(n,))
+
+    u = arr(0, nall * nm)
+    alpha = arr(1, nall * nm) if iv[6] == 1 else None
+    sig_t, sig_s = arr(2, nall), arr(3, nall)
+    for name, val in (overrides or {}).items():
+        {"u": u, "alpha": alpha, "sigT": sig_t, "sigS": sig_s}[name][:] = val
+    res = dict(iv=list(iv)[:13], dv=list(dv)[:9],
+               u0=u.copy(), alpha0=None if alpha is None else alpha.copy(),
+               sigT=sig_t.copy(), sigS=sig_s.copy())
+    if "tables" in want:
+        res["M"] = arr(4, nq * nm).copy()
+        res["w"] = arr(6, nq).copy()
+        res["xi"], res["eta"], res["mu"] = arr(7, nq).copy(), arr(8, nq).copy(), arr(9, nq).copy()
+    dt = dv[3]
+    iters = []
+    for s in range(nsteps):
+        if record:
+            it = np.zeros(2 * nall, np.int32)
+            ig = np.zeros(2 * nall, np.int32)
+            rg = np.zeros(2 * nall, np.int32)
+            L.c3dref_step_traced(dt, _pi(it), _pi(ig), _pi(rg), None)
+            iters.append((it, ig, rg))
+        else:
+            L.c3dref_update(dt)
+    res["u"] = u.copy()
+    res["alpha"] = None if alpha is None else alpha.copy()
+    st = (ctypes.c_double * 32)()
+    L.c3dref_stats(st)
+    res["stats"] = list(st)[:5 + 16]
+    res["iters"] = iters
+    conn.send(res)
+    conn.close()
+
+
+def run_reference(deck, *, ladder=None, nsteps=1, overrides=None, record=True, want=()):
+    """Runs the reference on a deck in a fresh spawned process and returns its state."""
+    if not os.path.exists(REF_SO):
+        raise FileNotFoundError(REF_SO + " (run `make -C oracle ref`)")
+    ctx = mp.get_context("spawn")
+    a, b = ctx.Pipe(duplex=False)
+    p = ctx.Process(target=_ref_worker, args=(b, deck, ladder, nsteps, overrides, record,
+                                              tuple(want)))
+    p.start()
+    b.close()
+    res = a.recv()
+    p.join()
+    assert p.exitcode == 0, p.exitcode
+    return res
