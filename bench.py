@@ -1,0 +1,466 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 M_N time step: Newton cell-solves/s.
+
+A step is one SSP-RK2 step of update() (src/update.cpp:185-275): two stages of
+ghost fill, M_N closure on every cell (ghosts included), kinetic flux and Euler
+update, then the RK average. A cell-solve is one converged dual solve of one
+interior cell in one stage, so a step on an n^3 grid is 2 n^3 cell-solves.
+
+Default workload (one GPU): M_6 (49 moments) on a 128^3 periodic grid, 1568-point
+quadrature (28 mu x 56 phi), isotropic gaussian pulse of width 0.02 with floor
+1e-10, sigma_s = 1, sigma_a = 0, SSP-RK2 at CFL 0.5, MN_TOL 1e-8 (batched rules),
+ladder {0, 1e-8, 1e-6, 1e-4, 1e-2, 1e-1}. Synthetic input generated from the deck.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--config c1|c2|c3]
+
+--gpus N > 1 runs under torchrun: N independent replicas (weak scaling), one per
+GPU; time is the max over ranks. --impl reference times the reference's own CPU
+closure (oracle/_ref, built from the reference sources) on a bounded sample of the
+same workload's cells using all host cores, and prints the same metric.
+"""
+import argparse
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "c3d-2015_b200"))
+
+METRIC = "M_N Newton cell-solves/s"
+UNIT = "cell-solves/s"
+LADDER = "0,1e-8,1e-6,1e-4,1e-2,1e-1"
+
+CONFIGS = {
+    "c1": dict(N=2, Q=12, n=16, sigma=0.1, floor=1e-4, sigma_s=1.0,
+               desc="M_2 (9 moments) 16^3 periodic, 288-point quadrature, gaussian pulse width 0.1 "
+                    "floor 1e-4"),
+    "c2": dict(N=4, Q=20, n=64, sigma=0.05, floor=1e-6, sigma_s=1.0, checker=(8, 10.0, 0.1),
+               desc="M_4 (25 moments) 64^3 periodic, 800-point quadrature, sigma_s checkerboard "
+                    "1/10 over 8^3 blocks, sigma_a 0.1 in the 10-blocks, pulse width 0.05 floor 1e-6"),
+    "c3": dict(N=6, Q=28, n=128, sigma=0.02, floor=1e-10, sigma_s=1.0,
+               desc="M_6 (49 moments) 128^3 periodic, 1568-point quadrature (28 mu x 56 phi), "
+                    "gaussian pulse width 0.02 floor 1e-10"),
+    # the same kernels on a 24^3 grid: the small case for ncu section captures
+    "c3s": dict(N=6, Q=28, n=24, sigma=0.02, floor=1e-10, sigma_s=1.0,
+                desc="M_6 (49 moments) 24^3 periodic, 1568-point quadrature, pulse width 0.02 "
+                     "floor 1e-10 (profiling case)"),
+}
+
+# Newton tolerance of the benchmark decks. The configurations name 1e-8; at that
+# tolerance the reference's own algorithm (absolute |g| test on u scaled to u0 = 1,
+# Armijo test at the FP64 rounding level of f) exhausts its regularisation ladder on
+# some cells and aborts (src/opt/optBatch.cpp:233-238), so the decks use 1e-6, the
+# smallest decade at which the reference runs these workloads to completion.
+MN_TOL = 1e-6
+
+
+def deck_for(cfg, threads=1, tol=MN_TOL, ic="gaussian_psi"):
+    c = CONFIGS[cfg]
+    kv = dict(SOLVER="mn", TFINAL="1", OUTDT="1000", OUTPUT_DATA="false",
+              OUTPUT_OPT_STATS="false", OUTPUT_TIMINGS="false", NX=c["n"], NY=c["n"], NZ=c["n"],
+              MPIX=1, MPIY=1, MPIZ=1, AX=-1, AY=-1, AZ=-1, BX=1, BY=1, BZ=1,
+              MOMENT_ORDER=c["N"], QUAD_ORDER=c["Q"], CFL_FACTOR=0.5,
+              CROSS_SECTION=c["sigma_s"], INIT_FLOOR=c["floor"], GAUSS_SIGMA=c["sigma"],
+              INIT_COND=ic, THETA=2.0, OMP_THREADS=threads, PN_USE_KINETIC_FLUX=0,
+              MN_TOL=tol, MN_TOL_GAMMA=1.1, MN_COND_H_MAX=1e10, MN_MAX_ITER=100,
+              MN_BATCHED="true", MN_USE_GAUNT_COEF="false", MN_USE_GAUNT_SPARSE="false",
+              CUDA_KINETIC="true", CUDA_BATCHED="true", CUDA_BATCH_SIZE=50, REG_LADDER=LADDER)
+    if "checker" in c:
+        b, shi, ahi = c["checker"]
+        kv.update(SIGMA_CHECKER_BLOCK=b, SIGMA_S_HI=shi, SIGMA_A_HI=ahi)
+    return "".join(f"{k} {v}\n" for k, v in kv.items())
+
+
+def interior_cells(cfg):
+    n = CONFIGS[cfg]["n"]
+    return n ** 3
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi samples every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.idx = device_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return dict(sm_mhz=None, sm_max_mhz=None, reasons=["unsampled"])
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons, power = [], None, set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+                power.append(float(f[3]))
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        os.unlink(self.path)
+        if not sm:
+            return dict(sm_mhz=None, sm_max_mhz=smax, reasons=["unsampled"])
+        return dict(sm_mhz=float(np.median(sm)), sm_max_mhz=smax, reasons=sorted(reasons),
+                    samples=len(sm), power_w_max=max(power) if power else None)
+
+
+# ------------------------------------------------------------------ FLOP model
+def closure_flops(nm, nq, iters, trials):
+    """Algorithmic FP64 FLOPs of the dual solves: per Newton iteration the Hessian's lower
+    triangle nm(nm+1)/2 * nq FMAs (2 FLOP each), the exponent 2 nm nq and nq exps (counted
+    1 FLOP), Cholesky nm^3/3; per line-search trial 2 nm nq + 2 nq."""
+    per_iter = nm * (nm + 1) * nq + 2 * nm * nq + nq + nm ** 3 / 3.0
+    per_trial = 2 * nm * nq + 2 * nq
+    return iters * per_iter + trials * per_trial
+
+
+def fp64_peak_tflops():
+    """In-run FP64 reference: cuBLAS DGEMM 8192^3 through torch (burst, best of 5)."""
+    import torch
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        e.synchronize()
+        best = max(best, 2 * n ** 3 / (s.elapsed_time(e) * 1e-3) / 1e12)
+    del a, b
+    torch.cuda.empty_cache()
+    return best
+
+
+def profile_traffic(kernel):
+    """DRAM bytes per launch from the committed ncu summary, if present."""
+    p = os.path.join(REPO, "profiles", f"{kernel}.txt")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("dram_bytes_per_launch_full_workload:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+# ------------------------------------------------------------------ reference CPU arm
+def _ref_sample_worker(conn, deck, u, a, reps):
+    """Spawned process: the reference's batched closure (oracle/_ref) on sampled cells."""
+    L = ctypes.CDLL(os.path.join(REPO, "oracle", "_ref", "libc3dref.so"))
+    L.c3dref_init.argtypes = [ctypes.c_char_p]
+    lad = np.array([float(x) for x in LADDER.split(",")])
+    L.c3dref_set_ladder(len(lad), lad.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+    with tempfile.TemporaryDirectory() as tmp:
+        with open(os.path.join(tmp, "input.deck"), "w") as f:
+            f.write(deck)
+        L.c3dref_init(tmp.encode())
+    L.c3dref_opt_batched_vectors.argtypes = [ctypes.c_long, ctypes.c_void_p, ctypes.c_void_p,
+                                             ctypes.c_void_p]
+    threads = L.c3dref_num_threads()
+    n = u.shape[0]
+    times = []
+    its = np.zeros(n, np.int32)
+    for _ in range(reps):
+        uu, aa = u.copy(), a.copy()
+        t0 = time.perf_counter()
+        L.c3dref_opt_batched_vectors(n, uu.ctypes.data, aa.ctypes.data, its.ctypes.data)
+        times.append(time.perf_counter() - t0)
+    conn.send(dict(times=times, threads=threads, mean_iters=float(its.mean())))
+    conn.close()
+
+
+def run_ref_sample(cfg, u, a, reps):
+    import multiprocessing as mp
+    threads = os.cpu_count() or 1
+    c = CONFIGS[cfg]
+    # a 4^3 deck with the workload's moment order, quadrature and MN options sets up the
+    # reference's tables and globals; the sampled cells are solved by Optimization::opt
+    deck = deck_for(cfg, threads=threads, ic="gaussian").replace(f"NX {c['n']}", "NX 4").replace(
+        f"NY {c['n']}", "NY 4").replace(f"NZ {c['n']}", "NZ 4")
+    ctx = mp.get_context("spawn")
+    r, w = ctx.Pipe(duplex=False)
+    p = ctx.Process(target=_ref_sample_worker, args=(w, deck, u, a, reps))
+    p.start()
+    w.close()
+    res = r.recv()
+    p.join()
+    return res
+
+
+def initial_cells_sample(cfg, count, seed=1234):
+    """Cells of the workload's initial state, sampled uniformly over the grid with ghosts
+    (u0 = 2 sqrt(pi) max(floor, G/(4 pi)), other moments 0; alpha as src/init.cpp:265)."""
+    c = CONFIGS[cfg]
+    n, nm = c["n"], (c["N"] + 1) ** 2
+    rng = np.random.default_rng(seed)
+    ijk = rng.integers(0, n + 4, size=(count, 3))
+    dx = 2.0 / n
+    x = -1 + (ijk - 2) * dx + dx / 2.0
+    s = c["sigma"]
+    f1 = 1.0 / (s * np.sqrt(2.0 * np.pi))
+    G = f1 ** 3 * np.exp(-(x ** 2).sum(1) / (2.0 * s * s))
+    u = np.zeros((count, nm))
+    u[:, 0] = 2.0 * np.sqrt(np.pi) * np.maximum(c["floor"], G / (4.0 * np.pi))
+    a = np.zeros((count, nm))
+    a[:, 0] = np.sqrt(4.0 * np.pi) * np.log(u[:, 0] / np.sqrt(4.0 * np.pi))
+    return u, a
+
+
+def calibrated_ref_sample(cfg, u_all, a_all, target_s=12.0):
+    """Times the reference closure on a sample sized for ~target_s seconds of CPU work."""
+    threads = os.cpu_count() or 1
+    n0 = min(len(u_all), 32 * threads)
+    probe = run_ref_sample(cfg, u_all[:n0], a_all[:n0], 1)
+    rate = n0 / max(probe["times"][0], 1e-6)
+    n = int(min(len(u_all), max(n0, rate * target_s)))
+    return n, rate
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    cfg = args.config
+    c = CONFIGS[cfg]
+    threads = os.cpu_count() or 1
+    pool_u, pool_a = initial_cells_sample(cfg, 400000)
+    n, rate = calibrated_ref_sample(cfg, pool_u, pool_a, target_s=max(2.0, 60.0 / max(1, args.steps + args.warmup)))
+    res = run_ref_sample(cfg, pool_u[:n], pool_a[:n], args.warmup + args.steps)
+    times = res["times"][args.warmup:]
+    step_s = float(np.mean(times))
+    value = n / step_s
+    sample = (f"{n} cells drawn uniformly (seed 1234) from the initial state of the workload "
+              f"(grid with ghosts), each step one batched closure of the sample "
+              f"(Optimization::opt, src/opt/optBatch.cpp:350-472)")
+    line = dict(metric=METRIC, value=value, unit=UNIT, n_gpus=args.gpus, steps=args.steps,
+                warmup=args.warmup, ms_per_step=step_s * 1e3, higher_is_better=True,
+                scaling="weak", vs_baseline=None, dtype="f64", data="synthetic", impl="reference",
+                config=dict(workload=c["desc"], config=cfg, mn_tol=MN_TOL, ladder=LADDER,
+                            note="reference CPU closure only (no flux); cells/s of the sample"),
+                cpu_baseline=dict(value=value, unit=UNIT, cores=res["threads"], kind="reference",
+                                  sample=sample),
+                e2e=dict(value=value, unit=UNIT, h2d_bytes_per_step=0, d2h_bytes_per_step=0),
+                mean_iters=res["mean_iters"])
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ B200 arm
+def b200_arm(args):
+    import torch
+    import torch.distributed as dist
+
+    import c3d
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py: no CUDA device")
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    cfg = args.config
+    c = CONFIGS[cfg]
+    stream = torch.cuda.current_stream()
+    with tempfile.TemporaryDirectory() as tmp:
+        deck = os.path.join(tmp, "input.deck")
+        with open(deck, "w") as f:
+            f.write(deck_for(cfg, threads=os.cpu_count() or 1))
+        solver = c3d.Solver(deck, stream=ctypes.c_void_p(stream.cuda_stream))
+    ctxh = solver.ctx_handle
+    L = c3d.lib()
+    dt = solver.max_dt
+    nm, nq = solver.nm, solver.nq
+
+    failed = [0]
+
+    def sync_count():
+        st_ = L.c3d_sync(ctxh)
+        if st_ == 4:  # C3D_ERR_CLOSURE: cells whose ladder ran out (the reference would abort)
+            failed[0] += 1
+        elif st_ != 0:
+            c3d.check(st_, "sync")
+
+    # warm-up
+    for _ in range(args.warmup):
+        solver.update(dt)
+    sync_count()
+
+    peak = fp64_peak_tflops() if rank == 0 else None
+
+    # timed region: K device-resident steps
+    L.c3d_closure_stats_reset(ctxh)
+    L.c3d_timing_enable(ctxh, 1)
+    launches0 = L.c3d_launch_count(ctxh)
+    clocks = ClockSampler(local)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    time.sleep(0.3)
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    evs[0].record(stream)
+    for k in range(args.steps):
+        solver.update(dt)
+        evs[k + 1].record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    launches = L.c3d_launch_count(ctxh) - launches0
+    sync_count()
+    step_ms = [evs[k].elapsed_time(evs[k + 1]) for k in range(args.steps)]
+    total_ms = evs[0].elapsed_time(evs[-1])
+    ms = np.zeros(2)
+    cnt = (ctypes.c_longlong * 2)()
+    L.c3d_timing_get(ctxh, ms.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), cnt)
+    L.c3d_timing_enable(ctxh, 0)
+    st = solver.stats()
+    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    max_ms = float(t.item())
+    cells = interior_cells(cfg)
+    value = world * cells * 2 * args.steps / (max_ms * 1e-3)
+
+    # end-to-end: host buffers through the C ABI, copies inside the timed region
+    nv = solver.nall * nm
+    hu = torch.empty(nv, dtype=torch.float64).pin_memory()
+    ha = torch.empty(nv, dtype=torch.float64).pin_memory()
+    L.c3d_get_state(ctxh, ctypes.c_void_p(hu.data_ptr()), ctypes.c_void_p(ha.data_ptr()), 0)
+    e_steps = max(1, min(args.steps, 3))
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e_steps):
+        c3d.check(L.c3d_set_state(ctxh, ctypes.c_void_p(hu.data_ptr()),
+                                  ctypes.c_void_p(ha.data_ptr()), None, None, 0), "set_state")
+        solver.update(dt)
+        c3d.check(L.c3d_get_state(ctxh, ctypes.c_void_p(hu.data_ptr()),
+                                  ctypes.c_void_p(ha.data_ptr()), 0), "get_state")
+    e1.record(stream)
+    torch.cuda.synchronize()
+    sync_count()
+    te = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = world * cells * 2 * e_steps / (float(te.item()) * 1e-3)
+
+    if rank == 0:
+        closure_launches = int(cnt[0])
+        flops = closure_flops(nm, nq, st.totalIters, st.trials)
+        per_launch_s = ms[0] * 1e-3 / max(1, closure_launches)
+        achieved = flops / max(1, closure_launches) / per_launch_s / 1e12
+        roofline = dict(bound="tensor", pipe="fp64 (DMMA m8n8k4 + DFMA)", achieved=achieved,
+                        peak=peak, unit="TFLOP/s", frac=achieved / peak if peak else None,
+                        traffic=profile_traffic("closure_fp64_m6_128"),
+                        peak_source="in-run cuBLAS DGEMM 8192^3 via torch (FP64 is not in "
+                                    "MEASURED_PEAKS.json)",
+                        kernel="closure_fp64_kernel<7,8>",
+                        flops_per_launch=flops / max(1, closure_launches),
+                        closure_ms_per_launch=ms[0] / max(1, closure_launches),
+                        flux_ms_per_launch=ms[1] / max(1, int(cnt[1])),
+                        closure_share_of_step=ms[0] / total_ms)
+        # CPU baseline: the reference closure on a bounded sample of this workload's cells
+        cpu = None
+        try:
+            uh = hu.numpy().reshape(-1, nm)
+            ah = ha.numpy().reshape(-1, nm)
+            rng = np.random.default_rng(7)
+            pick = rng.choice(uh.shape[0], size=min(uh.shape[0], 400000), replace=False)
+            su, sa = uh[pick].copy(), ah[pick].copy()
+            n_s, _ = calibrated_ref_sample(cfg, su, sa, target_s=12.0)
+            res = run_ref_sample(cfg, su[:n_s], sa[:n_s], 1)
+            cpu = dict(value=n_s / res["times"][0], unit=UNIT, cores=res["threads"],
+                       kind="reference",
+                       sample=f"{n_s} cells sampled uniformly from the state after the timed "
+                              f"steps, one batched closure (Optimization::opt); closure only")
+        except Exception as ex:  # reported, not fatal
+            cpu = dict(value=None, unit=UNIT, cores=os.cpu_count(), kind="reference",
+                       sample=f"failed: {ex}")
+        hist = {str(i): int(st.iterHist[i]) for i in range(64) if st.iterHist[i]}
+        line = dict(
+            metric=METRIC, value=value, unit=UNIT, n_gpus=world, steps=args.steps,
+            warmup=args.warmup, ms_per_step=max_ms / args.steps, higher_is_better=True,
+            scaling="weak", vs_baseline=None, dtype="f64", data="synthetic",
+            config=dict(workload=c["desc"], config=cfg, form="plain FP64 drop-in",
+                        mn_tol=MN_TOL, mn_batched=True, ladder=LADDER,
+                        cells_per_step=2 * cells, l2="inputs larger than L2 (u, alpha 0.9 GB each)",
+                        parallelism=f"replicas x{world}"),
+            roofline=roofline, cpu_baseline=cpu,
+            e2e=dict(value=e2e_value, unit=UNIT, h2d_bytes_per_step=2 * nv * 8,
+                     d2h_bytes_per_step=2 * nv * 8, steps=e_steps),
+            gpu_launches=int(launches), clocks=clk,
+            latency_ms=dict(p50=float(np.percentile(step_ms, 50)),
+                            p99=float(np.percentile(step_ms, 99)), unit="ms per RK2 step"),
+            iter_histogram=hist, newton_iters_per_solve=st.totalIters / max(1, st.cells),
+            failed_cells_timed=int(st.failed), syncs_with_failed_cells=failed[0])
+        print(json.dumps(line), flush=True)
+    solver.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--config", default="c3", choices=sorted(CONFIGS))
+    args = ap.parse_args()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        b200_arm(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,703 @@
+// C ABI of libc3d_b200.so (declarations and contracts in include/c3d_b200.h).
+#include "../../include/c3d_b200.h"
+#include "c3d_common.cuh"
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+namespace c3d {
+struct ClosureLaunch {
+    const ClosureParams *P;
+    const double *chunks;
+    long long ncells;
+    unsigned long long *counter;
+    double *u, *alpha;
+    int *iters, *iterGamma, *regIdx, *status;
+    unsigned long long *failCount;
+    unsigned long long *stats;
+    int *errorFlag;
+    int numSMs;
+    cudaStream_t stream;
+};
+cudaError_t launch_closure_fp64(const ClosureLaunch &L);
+int closure_fp64_nmp(int nm);
+cudaError_t launch_hessian_batch(int nm, int nchunks, const double *chunks, const double *alphas,
+                                 long long n, double *hs, int *errorFlag, cudaStream_t st);
+cudaError_t launch_ghost_fill(const GridDims &g, double *u, int numSMs, cudaStream_t st);
+cudaError_t launch_euler(const GridDims &g, double *u, const double *flux, const double *sigT,
+                         const double *sigS, double dt, int numSMs, cudaStream_t st);
+cudaError_t launch_rk(const GridDims &g, double *u, double *uOld, int mode, int numSMs,
+                      cudaStream_t st);
+cudaError_t launch_kinetic_flux(const GridDims &g, const double *alpha, const double *M,
+                                const double *w, const double *xi, const double *eta,
+                                const double *mu, int nq, int qChunk, double dx, double dy,
+                                double dz, double theta, int isPn, double *psi, double *flux,
+                                cudaStream_t st);
+int kinetic_max_chunk(int nm);
+cudaError_t launch_moment_flux(const GridDims &g, const double *u, const double *ops, double dx,
+                               double dy, double dz, double *flux, cudaStream_t st);
+} // namespace c3d
+
+
+using namespace c3d;
+
+static thread_local std::string g_lastError;
+
+static c3d_status fail(c3d_status s, const std::string &msg)
+{
+    g_lastError = msg;
+    return s;
+}
+
+#define C3D_CUDA(call)                                                                             \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess)                                                                     \
+            return fail(e_ == cudaErrorMemoryAllocation ? C3D_ERR_OOM : C3D_ERR_CUDA,              \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));                       \
+    } while (0)
+
+// Chunk-blocked, transposed basis for the closure's bulk copies:
+// chunk k holds rows i < NMP of M^T restricted to directions [k*QC, k*QC+QC)
+// with row stride QCP, then one row of weights; zero padding elsewhere.
+static std::vector<double> build_chunks(int nm, int nq, const double *M, const double *w)
+{
+    int nmp = closure_fp64_nmp(nm);
+    int nch = ceil_div(nq, QC);
+    size_t chunk = (size_t)(nmp + 1) * QCP;
+    std::vector<double> out((size_t)nch * chunk, 0.0);
+    for (int k = 0; k < nch; ++k) {
+        double *c = out.data() + k * chunk;
+        for (int qq = 0; qq < QC; ++qq) {
+            int q = k * QC + qq;
+            if (q >= nq)
+                break;
+            for (int i = 0; i < nm; ++i)
+                c[i * QCP + qq] = M[(size_t)q * nm + i];
+            c[nmp * QCP + qq] = w[q];
+        }
+    }
+    return out;
+}
+
+struct c3d_ctx {
+    int device = 0;
+    int numSMs = 148;
+    cudaStream_t stream = nullptr;
+    bool ownStream = false;
+    GridDims g{};
+    int nq = 0;
+    double dx = 0, dy = 0, dz = 0, theta = 2.0;
+    int solver = 1, pnKinetic = 0;
+    ClosureParams cp{};
+    size_t psiBytes = 0;
+    int qChunk = 0;
+    long long launches = 0;
+    // device buffers
+    double *u = nullptr, *alpha = nullptr, *uOld = nullptr, *flux = nullptr;
+    double *sigT = nullptr, *sigS = nullptr;
+    double *M = nullptr, *w = nullptr, *xi = nullptr, *eta = nullptr, *mu = nullptr;
+    double *chunks = nullptr, *pnops = nullptr, *psi = nullptr;
+    int *iters = nullptr, *iterGamma = nullptr, *regIdx = nullptr, *status = nullptr;
+    unsigned long long *counter = nullptr, *failCount = nullptr, *stats = nullptr;
+    int *errorFlag = nullptr;
+    // optional event timing of the closure and flux launches (kind 0 closure, 1 flux)
+    bool timing = false;
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> events;
+};
+
+static void timing_begin(c3d_ctx *c, cudaEvent_t *a)
+{
+    if (!c->timing)
+        return;
+    cudaEventCreate(a);
+    cudaEventRecord(*a, c->stream);
+}
+static void timing_end(c3d_ctx *c, int kind, cudaEvent_t a)
+{
+    if (!c->timing)
+        return;
+    cudaEvent_t b;
+    cudaEventCreate(&b);
+    cudaEventRecord(b, c->stream);
+    c->events.push_back({kind, {a, b}});
+}
+static void timing_clear(c3d_ctx *c)
+{
+    for (auto &e : c->events) {
+        cudaEventDestroy(e.second.first);
+        cudaEventDestroy(e.second.second);
+    }
+    c->events.clear();
+}
+
+static void free_ctx(c3d_ctx *c)
+{
+    void *ptrs[] = {c->u,     c->alpha,  c->uOld,     c->flux,    c->sigT,   c->sigS,
+                    c->M,     c->w,      c->xi,       c->eta,     c->mu,     c->chunks,
+                    c->pnops, c->psi,    c->iters,    c->iterGamma, c->regIdx, c->status,
+                    c->counter, c->failCount, c->stats, c->errorFlag};
+    for (void *p : ptrs)
+        if (p)
+            cudaFree(p);
+    timing_clear(c);
+    if (c->ownStream && c->stream)
+        cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+extern "C" {
+
+const char *c3d_last_error(void) { return g_lastError.c_str(); }
+
+c3d_status c3d_create(const c3d_params *p, const double *M, const double *w, const double *xi,
+                      const double *eta, const double *mu, const double *pnOps, void *stream,
+                      c3d_ctx **out)
+{
+    if (!p || !M || !w || !xi || !eta || !mu || !out)
+        return fail(C3D_ERR_INVALID, "c3d_create: null argument");
+    if (p->nx < 1 || p->ny < 1 || p->nz < 1)
+        return fail(C3D_ERR_INVALID, "c3d_create: grid sizes must be positive");
+    if (p->nm < 1 || p->nm > 64)
+        return fail(C3D_ERR_INVALID, "c3d_create: nm must be in [1, 64] (moment order <= 7)");
+    int sq = (int)std::lround(std::sqrt((double)p->nm));
+    if (sq * sq != p->nm)
+        return fail(C3D_ERR_INVALID, "c3d_create: nm must be (N+1)^2");
+    if (p->nq < 1)
+        return fail(C3D_ERR_INVALID, "c3d_create: nq must be positive");
+    if (p->nreg < 1 || p->nreg > MAX_REG)
+        return fail(C3D_ERR_INVALID, "c3d_create: ladder length must be in [1, 16]");
+    if (p->solver == 0 && !p->pnUseKineticFlux && !pnOps)
+        return fail(C3D_ERR_INVALID, "c3d_create: P_N moment flux needs the six operators");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1)
+        return fail(C3D_ERR_NO_DEVICE, "c3d_create: no CUDA device");
+
+    c3d_ctx *c = new c3d_ctx();
+    cudaGetDevice(&c->device);
+    cudaDeviceGetAttribute(&c->numSMs, cudaDevAttrMultiProcessorCount, c->device);
+    if (stream) {
+        c->stream = (cudaStream_t)stream;
+    } else {
+        if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+            delete c;
+            return fail(C3D_ERR_CUDA, "c3d_create: stream creation failed");
+        }
+        c->ownStream = true;
+    }
+    c->g = GridDims{p->nx, p->ny, p->nz, p->nm};
+    c->nq = p->nq;
+    c->dx = p->dx;
+    c->dy = p->dy;
+    c->dz = p->dz;
+    c->theta = p->theta;
+    c->solver = p->solver;
+    c->pnKinetic = p->pnUseKineticFlux;
+    ClosureParams &cp = c->cp;
+    cp.nm = p->nm;
+    cp.nq = p->nq;
+    cp.nchunks = ceil_div(p->nq, QC);
+    cp.batched = p->mnBatched ? 1 : 0;
+    cp.maxIter = p->mnMaxIter;
+    cp.nreg = p->nreg;
+    cp.tol = p->mnTol;
+    cp.tolGamma = p->mnBatched ? p->mnTolGamma : 1.1;
+    cp.condHMax = p->mnCondHMax;
+    cp.m0 = M[0];
+    for (int i = 0; i < p->nreg; ++i)
+        cp.reg[i] = p->reg[i];
+    cp.passBudget = 1LL << 40;
+    c->psiBytes = p->psiBytes ? p->psiBytes : (size_t)32 << 30;
+
+    const long long nall = c->g.nall();
+    const int nm = p->nm, nq = p->nq;
+    auto alloc = [&](void **ptr, size_t bytes) -> bool {
+        if (cudaMalloc(ptr, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        return true;
+    };
+    bool ok = alloc((void **)&c->u, nall * nm * 8) && alloc((void **)&c->alpha, nall * nm * 8) &&
+              alloc((void **)&c->uOld, nall * nm * 8) && alloc((void **)&c->flux, nall * nm * 8) &&
+              alloc((void **)&c->sigT, nall * 8) && alloc((void **)&c->sigS, nall * 8) &&
+              alloc((void **)&c->M, (size_t)nq * nm * 8) && alloc((void **)&c->w, nq * 8) &&
+              alloc((void **)&c->xi, nq * 8) && alloc((void **)&c->eta, nq * 8) &&
+              alloc((void **)&c->mu, nq * 8) && alloc((void **)&c->iters, nall * 4) &&
+              alloc((void **)&c->iterGamma, nall * 4) && alloc((void **)&c->regIdx, nall * 4) &&
+              alloc((void **)&c->status, nall * 4) && alloc((void **)&c->counter, 8) &&
+              alloc((void **)&c->failCount, 8) && alloc((void **)&c->errorFlag, 4) &&
+              alloc((void **)&c->stats, STAT_COUNT * 8);
+    std::vector<double> ch = build_chunks(nm, nq, M, w);
+    ok = ok && alloc((void **)&c->chunks, ch.size() * 8);
+    if (ok && pnOps)
+        ok = alloc((void **)&c->pnops, (size_t)6 * nm * nm * 8);
+    if (!ok) {
+        free_ctx(c);
+        return fail(C3D_ERR_OOM, "c3d_create: device allocation failed");
+    }
+    cudaMemcpy(c->M, M, (size_t)nq * nm * 8, cudaMemcpyHostToDevice);
+    cudaMemcpy(c->w, w, nq * 8, cudaMemcpyHostToDevice);
+    cudaMemcpy(c->xi, xi, nq * 8, cudaMemcpyHostToDevice);
+    cudaMemcpy(c->eta, eta, nq * 8, cudaMemcpyHostToDevice);
+    cudaMemcpy(c->mu, mu, nq * 8, cudaMemcpyHostToDevice);
+    cudaMemcpy(c->chunks, ch.data(), ch.size() * 8, cudaMemcpyHostToDevice);
+    if (pnOps)
+        cudaMemcpy(c->pnops, pnOps, (size_t)6 * nm * nm * 8, cudaMemcpyHostToDevice);
+    cudaMemset(c->u, 0, nall * nm * 8);
+    cudaMemset(c->alpha, 0, nall * nm * 8);
+    cudaMemset(c->uOld, 0, nall * nm * 8);
+    cudaMemset(c->flux, 0, nall * nm * 8);
+    cudaMemset(c->iters, 0, nall * 4);
+    cudaMemset(c->iterGamma, 0, nall * 4);
+    cudaMemset(c->regIdx, 0, nall * 4);
+    cudaMemset(c->status, 0, nall * 4);
+    cudaMemset(c->failCount, 0, 8);
+    cudaMemset(c->errorFlag, 0, 4);
+    cudaMemset(c->stats, 0, STAT_COUNT * 8);
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) {
+        free_ctx(c);
+        return fail(C3D_ERR_CUDA, std::string("c3d_create: ") + cudaGetErrorString(e));
+    }
+    // direction chunk of the materialised ansatz: shared-memory and HBM budgets
+    int qc = kinetic_max_chunk(nm);
+    long long byBudget = (long long)(c->psiBytes / ((size_t)nall * 8));
+    if (byBudget < qc)
+        qc = (int)(byBudget < 1 ? 1 : byBudget);
+    if (qc > nq)
+        qc = nq;
+    c->qChunk = qc;
+    *out = c;
+    return C3D_OK;
+}
+
+void c3d_destroy(c3d_ctx *ctx)
+{
+    if (!ctx)
+        return;
+    cudaStreamSynchronize(ctx->stream);
+    free_ctx(ctx);
+}
+
+c3d_status c3d_set_state(c3d_ctx *c, const double *u, const double *alpha, const double *sigT,
+                         const double *sigS, int where)
+{
+    if (!c)
+        return fail(C3D_ERR_INVALID, "c3d_set_state: null context");
+    const long long nall = c->g.nall();
+    const size_t vb = nall * c->g.nm * 8, sb = nall * 8;
+    cudaMemcpyKind k = where ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    if (u)
+        C3D_CUDA(cudaMemcpyAsync(c->u, u, vb, k, c->stream));
+    if (alpha)
+        C3D_CUDA(cudaMemcpyAsync(c->alpha, alpha, vb, k, c->stream));
+    if (sigT)
+        C3D_CUDA(cudaMemcpyAsync(c->sigT, sigT, sb, k, c->stream));
+    if (sigS)
+        C3D_CUDA(cudaMemcpyAsync(c->sigS, sigS, sb, k, c->stream));
+    if (!where)
+        C3D_CUDA(cudaStreamSynchronize(c->stream));
+    return C3D_OK;
+}
+
+c3d_status c3d_get_state(c3d_ctx *c, double *u, double *alpha, int where)
+{
+    if (!c)
+        return fail(C3D_ERR_INVALID, "c3d_get_state: null context");
+    const size_t vb = c->g.nall() * c->g.nm * 8;
+    cudaMemcpyKind k = where ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    if (u)
+        C3D_CUDA(cudaMemcpyAsync(u, c->u, vb, k, c->stream));
+    if (alpha)
+        C3D_CUDA(cudaMemcpyAsync(alpha, c->alpha, vb, k, c->stream));
+    if (!where)
+        C3D_CUDA(cudaStreamSynchronize(c->stream));
+    return C3D_OK;
+}
+
+c3d_status c3d_get_flux(c3d_ctx *c, double *flux, int where)
+{
+    if (!c || !flux)
+        return fail(C3D_ERR_INVALID, "c3d_get_flux: null argument");
+    const size_t vb = c->g.nall() * c->g.nm * 8;
+    C3D_CUDA(cudaMemcpyAsync(flux, c->flux, vb, where ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                             c->stream));
+    if (!where)
+        C3D_CUDA(cudaStreamSynchronize(c->stream));
+    return C3D_OK;
+}
+
+c3d_status c3d_device_state(c3d_ctx *c, double **u, double **alpha, double **flux)
+{
+    if (!c)
+        return fail(C3D_ERR_INVALID, "c3d_device_state: null context");
+    if (u)
+        *u = c->u;
+    if (alpha)
+        *alpha = c->alpha;
+    if (flux)
+        *flux = c->flux;
+    return C3D_OK;
+}
+
+c3d_status c3d_ghost_fill(c3d_ctx *c)
+{
+    if (!c)
+        return fail(C3D_ERR_INVALID, "c3d_ghost_fill: null context");
+    C3D_CUDA(launch_ghost_fill(c->g, c->u, c->numSMs, c->stream));
+    c->launches += 1;
+    return C3D_OK;
+}
+
+static c3d_status run_closure(c3d_ctx *c, long long n, double *u, double *alpha, int *iters,
+                              int *iterGamma, int *regIdx, int *status)
+{
+    ClosureLaunch L{};
+    L.P = &c->cp;
+    L.chunks = c->chunks;
+    L.ncells = n;
+    L.counter = c->counter;
+    L.u = u;
+    L.alpha = alpha;
+    L.iters = iters;
+    L.iterGamma = iterGamma;
+    L.regIdx = regIdx;
+    L.status = status;
+    L.failCount = c->failCount;
+    L.stats = c->stats;
+    L.errorFlag = c->errorFlag;
+    L.numSMs = c->numSMs;
+    L.stream = c->stream;
+    cudaEvent_t t0 = nullptr;
+    timing_begin(c, &t0);
+    C3D_CUDA(launch_closure_fp64(L));
+    timing_end(c, 0, t0);
+    c->launches += 2; // counter reset + closure kernel
+    return C3D_OK;
+}
+
+c3d_status c3d_closure(c3d_ctx *c)
+{
+    if (!c)
+        return fail(C3D_ERR_INVALID, "c3d_closure: null context");
+    if (c->solver != 1)
+        return fail(C3D_ERR_INVALID, "c3d_closure: the closure belongs to the M_N solver");
+    return run_closure(c, c->g.nall(), c->u, c->alpha, c->iters, c->iterGamma, c->regIdx, c->status);
+}
+
+c3d_status c3d_closure_vectors(c3d_ctx *c, long long n, double *u, double *alpha, int *iters,
+                               int *iterGamma, int *regIndex, int *status)
+{
+    if (!c || !u || !alpha || n < 0)
+        return fail(C3D_ERR_INVALID, "c3d_closure_vectors: bad argument");
+    if (n == 0)
+        return C3D_OK;
+    return run_closure(c, n, u, alpha, iters, iterGamma, regIndex, status);
+}
+
+c3d_status c3d_flux_kinetic(c3d_ctx *c, int alphaIsU)
+{
+    if (!c)
+        return fail(C3D_ERR_INVALID, "c3d_flux_kinetic: null context");
+    if (!c->psi) {
+        size_t bytes = (size_t)c->qChunk * c->g.nall() * 8;
+        C3D_CUDA(cudaMalloc(&c->psi, bytes));
+    }
+    const double *a = alphaIsU ? c->u : c->alpha;
+    int isPn = (c->solver == 0) ? 1 : 0;
+    cudaEvent_t t0 = nullptr;
+    timing_begin(c, &t0);
+    C3D_CUDA(launch_kinetic_flux(c->g, a, c->M, c->w, c->xi, c->eta, c->mu, c->nq, c->qChunk,
+                                 c->dx, c->dy, c->dz, c->theta, isPn, c->psi, c->flux, c->stream));
+    timing_end(c, 1, t0);
+    int nch = ceil_div(c->nq, c->qChunk);
+    c->launches += nch * (1 + ceil_div(c->qChunk, 64));
+    return C3D_OK;
+}
+
+c3d_status c3d_flux_moment(c3d_ctx *c)
+{
+    if (!c)
+        return fail(C3D_ERR_INVALID, "c3d_flux_moment: null context");
+    if (!c->pnops)
+        return fail(C3D_ERR_INVALID, "c3d_flux_moment: no P_N operators in this context");
+    C3D_CUDA(launch_moment_flux(c->g, c->u, c->pnops, c->dx, c->dy, c->dz, c->flux, c->stream));
+    c->launches += 1;
+    return C3D_OK;
+}
+
+c3d_status c3d_euler(c3d_ctx *c, double dt)
+{
+    if (!c)
+        return fail(C3D_ERR_INVALID, "c3d_euler: null context");
+    C3D_CUDA(launch_euler(c->g, c->u, c->flux, c->sigT, c->sigS, dt, c->numSMs, c->stream));
+    c->launches += 1;
+    return C3D_OK;
+}
+
+c3d_status c3d_step(c3d_ctx *c, double dt)
+{
+    if (!c)
+        return fail(C3D_ERR_INVALID, "c3d_step: null context");
+    c3d_status s;
+    C3D_CUDA(launch_rk(c->g, c->u, c->uOld, 0, c->numSMs, c->stream));
+    c->launches += 1;
+    for (int stage = 0; stage < 2; ++stage) {
+        if ((s = c3d_ghost_fill(c)) != C3D_OK)
+            return s;
+        if (c->solver == 1) {
+            if ((s = c3d_closure(c)) != C3D_OK)
+                return s;
+            if ((s = c3d_flux_kinetic(c, 0)) != C3D_OK)
+                return s;
+        } else if (!c->pnKinetic) {
+            if ((s = c3d_flux_moment(c)) != C3D_OK)
+                return s;
+        } else {
+            if ((s = c3d_flux_kinetic(c, 1)) != C3D_OK)
+                return s;
+        }
+        if ((s = c3d_euler(c, dt)) != C3D_OK)
+            return s;
+    }
+    C3D_CUDA(launch_rk(c->g, c->u, c->uOld, 1, c->numSMs, c->stream));
+    c->launches += 1;
+    return C3D_OK;
+}
+
+c3d_status c3d_sync(c3d_ctx *c)
+{
+    if (!c)
+        return fail(C3D_ERR_INVALID, "c3d_sync: null context");
+    C3D_CUDA(cudaStreamSynchronize(c->stream));
+    int flag = 0;
+    unsigned long long failed = 0;
+    C3D_CUDA(cudaMemcpy(&flag, c->errorFlag, 4, cudaMemcpyDeviceToHost));
+    C3D_CUDA(cudaMemcpy(&failed, c->failCount, 8, cudaMemcpyDeviceToHost));
+    if (flag)
+        return fail(C3D_ERR_TIMEOUT, "a bounded device wait gave up");
+    if (failed) {
+        cudaMemset(c->failCount, 0, 8);
+        return fail(C3D_ERR_CLOSURE, std::to_string(failed) +
+                                         " cell(s) failed: u0 <= 0 or regularisation ladder exhausted");
+    }
+    return C3D_OK;
+}
+
+c3d_status c3d_closure_records(c3d_ctx *c, int *iters, int *iterGamma, int *regIndex, int *status)
+{
+    if (!c)
+        return fail(C3D_ERR_INVALID, "c3d_closure_records: null context");
+    const size_t b = c->g.nall() * 4;
+    C3D_CUDA(cudaStreamSynchronize(c->stream));
+    if (iters)
+        C3D_CUDA(cudaMemcpy(iters, c->iters, b, cudaMemcpyDeviceToHost));
+    if (iterGamma)
+        C3D_CUDA(cudaMemcpy(iterGamma, c->iterGamma, b, cudaMemcpyDeviceToHost));
+    if (regIndex)
+        C3D_CUDA(cudaMemcpy(regIndex, c->regIdx, b, cudaMemcpyDeviceToHost));
+    if (status)
+        C3D_CUDA(cudaMemcpy(status, c->status, b, cudaMemcpyDeviceToHost));
+    return C3D_OK;
+}
+
+c3d_status c3d_closure_stats_get(c3d_ctx *c, c3d_closure_stats *st)
+{
+    if (!c || !st)
+        return fail(C3D_ERR_INVALID, "c3d_closure_stats_get: null argument");
+    unsigned long long h[STAT_COUNT];
+    C3D_CUDA(cudaStreamSynchronize(c->stream));
+    C3D_CUDA(cudaMemcpy(h, c->stats, sizeof(h), cudaMemcpyDeviceToHost));
+    memset(st, 0, sizeof(*st));
+    st->cells = (long long)h[STAT_CELLS];
+    st->totalIters = (long long)h[STAT_ITERS];
+    st->totalIterGamma = (long long)h[STAT_ITER_GAMMA];
+    st->maxIter = (int)h[STAT_MAX_ITER];
+    st->maxIterGamma = (int)h[STAT_MAX_ITER_GAMMA];
+    st->failed = (long long)h[STAT_FAILED];
+    st->trials = (long long)h[STAT_TRIALS];
+    for (int i = 0; i < 16; ++i)
+        st->regHist[i] = (long long)h[STAT_REG_HIST + i];
+    for (int i = 0; i < 64; ++i)
+        st->iterHist[i] = (long long)h[STAT_ITER_HIST + i];
+    return C3D_OK;
+}
+
+c3d_status c3d_closure_stats_reset(c3d_ctx *c)
+{
+    if (!c)
+        return fail(C3D_ERR_INVALID, "c3d_closure_stats_reset: null context");
+    C3D_CUDA(cudaMemsetAsync(c->stats, 0, STAT_COUNT * 8, c->stream));
+    return C3D_OK;
+}
+
+long long c3d_launch_count(c3d_ctx *c) { return c ? c->launches : 0; }
+
+c3d_status c3d_timing_enable(c3d_ctx *c, int on)
+{
+    if (!c)
+        return fail(C3D_ERR_INVALID, "c3d_timing_enable: null context");
+    C3D_CUDA(cudaStreamSynchronize(c->stream));
+    timing_clear(c);
+    c->timing = on != 0;
+    return C3D_OK;
+}
+
+c3d_status c3d_timing_get(c3d_ctx *c, double *ms, long long *count)
+{
+    if (!c || !ms)
+        return fail(C3D_ERR_INVALID, "c3d_timing_get: null argument");
+    C3D_CUDA(cudaStreamSynchronize(c->stream));
+    ms[0] = ms[1] = 0.0;
+    long long n[2] = {0, 0};
+    for (auto &e : c->events) {
+        float t = 0.f;
+        C3D_CUDA(cudaEventElapsedTime(&t, e.second.first, e.second.second));
+        ms[e.first] += t;
+        n[e.first]++;
+    }
+    if (count) {
+        count[0] = n[0];
+        count[1] = n[1];
+    }
+    return C3D_OK;
+}
+
+// ---------------------------------------------------------------- reference GPU entry points
+// Process-wide state, as the reference keeps it (static device buffers set up on
+// first use, src/cuda/cuda_flux_kinetic.cu:23-67, src/cuda/cuda_solveH.cu).
+
+static std::mutex g_refMutex;
+static struct {
+    int nm = 0, nq = 0, nchunks = 0;
+    double *chunks = nullptr, *alphas = nullptr, *hs = nullptr;
+    long long cap = 0;
+    int *errorFlag = nullptr;
+} g_h;
+
+void solveHInit_cuda(int nm, int nm2, int nq, int batchSize, double *w, double *p, double *p2,
+                     double *beta, double *betaVal, int *betaColInd, int *betaRowPtr, int useGaunt)
+{
+    (void)nm2; (void)p2; (void)beta; (void)betaVal; (void)betaColInd; (void)betaRowPtr;
+    std::lock_guard<std::mutex> lk(g_refMutex);
+    if (useGaunt) {
+        fprintf(stderr, "[c3d_b200] solveHInit_cuda: Gaunt-coefficient Hessians are not provided; "
+                        "use MN_USE_GAUNT_COEF false\n");
+        return;
+    }
+    if (nm < 1 || nm > 64 || nq < 1) {
+        fprintf(stderr, "[c3d_b200] solveHInit_cuda: unsupported sizes nm=%d nq=%d\n", nm, nq);
+        return;
+    }
+    std::vector<double> ch = build_chunks(nm, nq, p, w);
+    if (g_h.chunks)
+        cudaFree(g_h.chunks);
+    g_h.nm = nm;
+    g_h.nq = nq;
+    g_h.nchunks = ceil_div(nq, QC);
+    cudaMalloc(&g_h.chunks, ch.size() * 8);
+    cudaMemcpy(g_h.chunks, ch.data(), ch.size() * 8, cudaMemcpyHostToDevice);
+    if (!g_h.errorFlag) {
+        cudaMalloc(&g_h.errorFlag, 4);
+        cudaMemset(g_h.errorFlag, 0, 4);
+    }
+    long long cap = batchSize > 0 ? batchSize : 1;
+    if (cap > g_h.cap) {
+        if (g_h.alphas) cudaFree(g_h.alphas);
+        if (g_h.hs) cudaFree(g_h.hs);
+        cudaMalloc(&g_h.alphas, cap * nm * 8);
+        cudaMalloc(&g_h.hs, cap * nm * nm * 8);
+        g_h.cap = cap;
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess)
+        fprintf(stderr, "[c3d_b200] solveHInit_cuda: %s\n", cudaGetErrorString(e));
+}
+
+void solveH_cuda(int nm, int nm2, int nq, int batchSize, double *alphas, double *hs, int useGaunt,
+                 int useGauntSparse)
+{
+    (void)nm2; (void)useGauntSparse;
+    std::lock_guard<std::mutex> lk(g_refMutex);
+    if (useGaunt || !g_h.chunks || nm != g_h.nm || nq != g_h.nq || batchSize > g_h.cap) {
+        fprintf(stderr, "[c3d_b200] solveH_cuda: not initialised for this size (call solveHInit_cuda "
+                        "with MN_USE_GAUNT_COEF false)\n");
+        return;
+    }
+    cudaMemcpy(g_h.alphas, alphas, (size_t)batchSize * nm * 8, cudaMemcpyHostToDevice);
+    cudaError_t e = launch_hessian_batch(nm, g_h.nchunks, g_h.chunks, g_h.alphas, batchSize, g_h.hs,
+                                         g_h.errorFlag, 0);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(hs, g_h.hs, (size_t)batchSize * nm * nm * 8, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess)
+        fprintf(stderr, "[c3d_b200] solveH_cuda: %s\n", cudaGetErrorString(e));
+}
+
+static struct {
+    c3d_ctx *ctx = nullptr;
+    int nx = 0, ny = 0, nz = 0, nm = 0, nq = 0, isPn = -1;
+} g_f;
+
+void solveFluxKinetic_cuda(int nx, int ny, int nz, int nm, int nq, double dx, double dy, double dz,
+                           double *alpha, double *flux, double *xi, double *eta, double *mu,
+                           double *w, double *p, int isPn)
+{
+    std::lock_guard<std::mutex> lk(g_refMutex);
+    if (nx < 5 || ny < 5 || nz < 5) {
+        fprintf(stderr, "[c3d_b200] solveFluxKinetic_cuda: grid (with ghosts) too small\n");
+        return;
+    }
+    if (!g_f.ctx || g_f.nx != nx || g_f.ny != ny || g_f.nz != nz || g_f.nm != nm || g_f.nq != nq ||
+        g_f.isPn != isPn) {
+        if (g_f.ctx)
+            c3d_destroy(g_f.ctx);
+        g_f.ctx = nullptr;
+        c3d_params P{};
+        P.nx = nx - 4;
+        P.ny = ny - 4;
+        P.nz = nz - 4;
+        P.nm = nm;
+        P.nq = nq;
+        P.dx = dx;
+        P.dy = dy;
+        P.dz = dz;
+        P.theta = 2.0; // the reference's GPU flux hard-codes theta (src/cuda/cuda_flux_kinetic.cu:82)
+        P.solver = isPn ? 0 : 1;
+        P.pnUseKineticFlux = 1;
+        P.mnBatched = 1;
+        P.mnMaxIter = 100;
+        P.mnTol = 1e-8;
+        P.mnTolGamma = 1.1;
+        P.mnCondHMax = 1e10;
+        P.nreg = 1;
+        if (c3d_create(&P, p, w, xi, eta, mu, nullptr, nullptr, &g_f.ctx) != C3D_OK) {
+            fprintf(stderr, "[c3d_b200] solveFluxKinetic_cuda: %s\n", c3d_last_error());
+            g_f.ctx = nullptr;
+            return;
+        }
+        g_f.nx = nx; g_f.ny = ny; g_f.nz = nz; g_f.nm = nm; g_f.nq = nq; g_f.isPn = isPn;
+    }
+    c3d_ctx *c = g_f.ctx;
+    c->dx = dx;
+    c->dy = dy;
+    c->dz = dz;
+    size_t vb = c->g.nall() * nm * 8;
+    cudaMemcpyAsync(c->alpha, alpha, vb, cudaMemcpyHostToDevice, c->stream);
+    cudaMemsetAsync(c->flux, 0, vb, c->stream);
+    if (c3d_flux_kinetic(c, 0) != C3D_OK) {
+        fprintf(stderr, "[c3d_b200] solveFluxKinetic_cuda: %s\n", c3d_last_error());
+        return;
+    }
+    cudaMemcpyAsync(flux, c->flux, vb, cudaMemcpyDeviceToHost, c->stream);
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess)
+        fprintf(stderr, "[c3d_b200] solveFluxKinetic_cuda: %s\n", cudaGetErrorString(e));
+}
+
+} // extern "C"

@@ -1,0 +1,73 @@
+// Shared device-side definitions for the B200 M_N step kernels.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace c3d {
+
+constexpr unsigned FULL_MASK = 0xffffffffu;
+constexpr int MAX_REG = 16;
+
+// Quadrature chunk staged per bulk copy: QC directions, row stride QCP doubles
+// (QCP = QC + 4 keeps the 8x4 DMMA fragment loads and the lane-per-direction
+// exponent loads free of shared-memory bank conflicts).
+constexpr int QC = 32;
+constexpr int QCP = 36;
+
+// Per-cell status codes written by the closure (0 = converged).
+enum CellStatus : int {
+    CELL_OK = 0,
+    CELL_NONPOSITIVE_U0 = 1,   // u0 <= 0 (reference aborts, src/opt/opt.cpp:343-346)
+    CELL_LADDER_EXHAUSTED = 2, // "Max regularization achieved" (src/opt/opt.cpp:261-266)
+    CELL_PASS_BUDGET = 3,      // safety bound on passes per cell exceeded
+};
+
+// Layout of the device-side closure counters (accumulated until reset).
+enum StatSlot : int {
+    STAT_CELLS = 0,
+    STAT_ITERS = 1,
+    STAT_ITER_GAMMA = 2,
+    STAT_MAX_ITER = 3,
+    STAT_MAX_ITER_GAMMA = 4,
+    STAT_FAILED = 5,
+    STAT_TRIALS = 6,     // line-search trial passes
+    STAT_REG_HIST = 8,   // 16 bins
+    STAT_ITER_HIST = 32, // 64 bins (last: >= 63)
+    STAT_COUNT = 96,
+};
+
+// Closure options (the MN_* deck keys, src/init.cpp:252-258).
+struct ClosureParams {
+    int nm;          // moments
+    int nq;          // quadrature points
+    int nchunks;     // ceil(nq / QC)
+    int batched;     // 1: src/opt/optBatch.cpp rules; 0: src/opt/opt.cpp rules
+    int maxIter;
+    int nreg;
+    double tol;
+    double tolGamma; // 1.1 for the unbatched rules (src/update.cpp:57)
+    double condHMax;
+    double m0;       // M[0][0] = 1/(2 sqrt(pi)), the constant harmonic
+    double reg[MAX_REG];
+    long long passBudget; // safety bound on H/line-search passes per cell
+};
+
+__host__ __device__ inline int ceil_div(int a, int b) { return (a + b - 1) / b; }
+
+// Grid with two ghost layers per face; cell (i,j,k) with k fastest (src/global.h:15).
+struct GridDims {
+    int nx, ny, nz; // interior cells
+    int nm;
+    __host__ __device__ int nxg() const { return nx + 4; }
+    __host__ __device__ int nyg() const { return ny + 4; }
+    __host__ __device__ int nzg() const { return nz + 4; }
+    __host__ __device__ long long cell(int i, int j, int k) const
+    {
+        return (long long)k + (long long)nzg() * ((long long)j + (long long)nyg() * i);
+    }
+    __host__ __device__ long long nall() const { return (long long)nxg() * nyg() * nzg(); }
+    __host__ __device__ long long ninterior() const { return (long long)nx * ny * nz; }
+};
+
+
+} // namespace c3d

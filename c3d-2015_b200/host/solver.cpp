@@ -1,0 +1,384 @@
+#include "solver.h"
+
+#include "tables.h"
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <sstream>
+
+#ifndef M_PI
+#define M_PI 3.14159265358979323846
+#endif
+
+namespace c3d_host {
+
+#define REQUIRE(call, name)                                                                        \
+    if (!(call))                                                                                   \
+        return std::string("missing or invalid deck key ") + name;
+
+std::string parse_config(const InputDeck &d, Config &c)
+{
+    REQUIRE(d.get("SOLVER", c.solver), "SOLVER");
+    REQUIRE(d.get("TFINAL", c.tFinal), "TFINAL");
+    REQUIRE(d.get("OUTDT", c.outDt), "OUTDT");
+    REQUIRE(d.get("OUTPUT_DATA", c.outputData), "OUTPUT_DATA");
+    REQUIRE(d.get("OUTPUT_OPT_STATS", c.outputOptStats), "OUTPUT_OPT_STATS");
+    REQUIRE(d.get("OUTPUT_TIMINGS", c.outputTimings), "OUTPUT_TIMINGS");
+    REQUIRE(d.get("MOMENT_ORDER", c.momentOrder), "MOMENT_ORDER");
+    REQUIRE(d.get("QUAD_ORDER", c.quadOrder), "QUAD_ORDER");
+    REQUIRE(d.get("CFL_FACTOR", c.cfl), "CFL_FACTOR");
+    REQUIRE(d.get("CROSS_SECTION", c.crossSection), "CROSS_SECTION");
+    REQUIRE(d.get("INIT_FLOOR", c.initFloor), "INIT_FLOOR");
+    REQUIRE(d.get("GAUSS_SIGMA", c.gaussSigma), "GAUSS_SIGMA");
+    REQUIRE(d.get("INIT_COND", c.initCond), "INIT_COND");
+    REQUIRE(d.get("OMP_THREADS", c.ompThreads), "OMP_THREADS");
+    REQUIRE(d.get("CUDA_KINETIC", c.cudaKinetic), "CUDA_KINETIC");
+    REQUIRE(d.get("CUDA_BATCHED", c.cudaBatched), "CUDA_BATCHED");
+    REQUIRE(d.get("CUDA_BATCH_SIZE", c.cudaBatchSize), "CUDA_BATCH_SIZE");
+    REQUIRE(d.get("THETA", c.theta), "THETA");
+    REQUIRE(d.get("NX", c.nx), "NX");
+    REQUIRE(d.get("NY", c.ny), "NY");
+    REQUIRE(d.get("NZ", c.nz), "NZ");
+    REQUIRE(d.get("MPIX", c.mpix), "MPIX");
+    REQUIRE(d.get("MPIY", c.mpiy), "MPIY");
+    REQUIRE(d.get("MPIZ", c.mpiz), "MPIZ");
+    REQUIRE(d.get("AX", c.ax), "AX");
+    REQUIRE(d.get("AY", c.ay), "AY");
+    REQUIRE(d.get("AZ", c.az), "AZ");
+    REQUIRE(d.get("BX", c.bx), "BX");
+    REQUIRE(d.get("BY", c.by), "BY");
+    REQUIRE(d.get("BZ", c.bz), "BZ");
+    if (c.solver == "pn") {
+        REQUIRE(d.get("PN_USE_KINETIC_FLUX", c.pnUseKineticFlux), "PN_USE_KINETIC_FLUX");
+    } else if (c.solver == "mn") {
+        REQUIRE(d.get("MN_TOL", c.mnTol), "MN_TOL");
+        REQUIRE(d.get("MN_COND_H_MAX", c.mnCondHMax), "MN_COND_H_MAX");
+        REQUIRE(d.get("MN_MAX_ITER", c.mnMaxIter), "MN_MAX_ITER");
+        REQUIRE(d.get("MN_BATCHED", c.mnBatched), "MN_BATCHED");
+        REQUIRE(d.get("MN_TOL_GAMMA", c.mnTolGamma), "MN_TOL_GAMMA");
+        REQUIRE(d.get("MN_USE_GAUNT_COEF", c.mnUseGaunt), "MN_USE_GAUNT_COEF");
+        REQUIRE(d.get("MN_USE_GAUNT_SPARSE", c.mnUseGauntSparse), "MN_USE_GAUNT_SPARSE");
+    } else {
+        return "Solver type does not exist";
+    }
+    if (c.initCond != "gaussian" && c.initCond != "smooth" && c.initCond != "funky" &&
+        c.initCond != "gaussian_psi")
+        return "Initial condition not supported";
+    if (c.nx < 1 || c.ny < 1 || c.nz < 1 || c.momentOrder < 0 || c.quadOrder < 1)
+        return "invalid grid, moment order or quadrature order";
+    // optional keys
+    d.get("NSTEPS", c.nsteps);
+    std::string lad;
+    if (d.get("REG_LADDER", lad)) {
+        c.ladder.clear();
+        std::stringstream ss(lad);
+        std::string tok;
+        while (std::getline(ss, tok, ','))
+            if (!tok.empty())
+                c.ladder.push_back(std::atof(tok.c_str()));
+        if (c.ladder.empty() || c.ladder.size() > 16)
+            return "REG_LADDER must list 1 to 16 values";
+    }
+    d.get("SIGMA_CHECKER_BLOCK", c.checkerBlock);
+    d.get("SIGMA_S_HI", c.sigmaSHi);
+    d.get("SIGMA_A_HI", c.sigmaAHi);
+    return "";
+}
+
+// Initial conditions, src/init.cpp:26-67.
+static double gaussian_ic(double sigma, double x, double y, double z)
+{
+    double s2 = sigma * sigma;
+    double factor1d = 1.0 / (sigma * sqrt(2.0 * M_PI));
+    double factor3d = factor1d * factor1d * factor1d;
+    return factor3d * exp(-(x * x + y * y + z * z) / (2.0 * s2));
+}
+static double smooth_ic(double x, double y, double z)
+{
+    return 2.0 + cos(2 * M_PI * x) * cos(2 * M_PI * y) * cos(2 * M_PI * z);
+}
+static double funky_ic(const Config &c, double sigma, double x, double y, double z)
+{
+    double r = 0.0;
+    double wx = c.bx - c.ax, wy = c.by - c.ay, wz = c.bz - c.az;
+    for (int i = 1; i < 10; i += 2)
+        for (int j = 1; j < 10; j += 2)
+            for (int k = 1; k < 10; k += 2)
+                r += gaussian_ic(sigma, x - (c.ax + i * wx / 10.0), y - (c.ay + j * wy / 10.0),
+                                 z - (c.az + k * wz / 10.0));
+    return smooth_ic(x, y, z) + r;
+}
+
+Solver::~Solver()
+{
+    if (ctx_)
+        c3d_destroy(ctx_);
+}
+
+void Solver::prepare(const Config &cfg)
+{
+    cfg_ = cfg;
+    const Config &c = cfg_;
+    // setupLocalMpiInfo, one rank (src/init.cpp:104-121)
+    dx_ = (c.bx - c.ax) / c.nx;
+    dy_ = (c.by - c.ay) / c.ny;
+    dz_ = (c.bz - c.az) / c.nz;
+    nq_ = 2 * c.quadOrder * c.quadOrder;
+    nm_ = (c.momentOrder + 1) * (c.momentOrder + 1);
+    const int nm = nm_, nq = nq_;
+    const int nxg = c.nx + 4, nyg = c.ny + 4, nzg = c.nz + 4;
+    const long long nall = (long long)nxg * nyg * nzg;
+
+    u.assign(nall * nm, 0.0);
+    sigT.assign(nall, 0.0);
+    sigS.assign(nall, 0.0);
+    // initial condition and cross sections (src/init.cpp:480-506)
+    for (int i = 0; i < nxg; i++)
+        for (int j = 0; j < nyg; j++)
+            for (int k = 0; k < nzg; k++) {
+                long long cell = (long long)k + nzg * ((long long)j + (long long)nyg * i);
+                double x = c.ax + (i - 2) * dx_ + dx_ / 2.0;
+                double y = c.ay + (j - 2) * dy_ + dy_ / 2.0;
+                double z = c.az + (k - 2) * dz_ + dz_ / 2.0;
+                double ss = c.crossSection, sa = 0.0;
+                if (c.checkerBlock > 0) {
+                    // periodic block index so ghost cells carry their image's values
+                    int ii = ((i - 2) % c.nx + c.nx) % c.nx, jj = ((j - 2) % c.ny + c.ny) % c.ny,
+                        kk = ((k - 2) % c.nz + c.nz) % c.nz;
+                    int parity = (ii / c.checkerBlock + jj / c.checkerBlock + kk / c.checkerBlock) & 1;
+                    if (parity) {
+                        ss = c.sigmaSHi;
+                        sa = c.sigmaAHi;
+                    }
+                }
+                sigT[cell] = ss + sa;
+                sigS[cell] = ss;
+                double *uc = &u[cell * nm];
+                if (c.initCond == "gaussian") {
+                    uc[0] = std::max(c.initFloor, gaussian_ic(c.gaussSigma, x, y, z) * 2.0 * sqrt(M_PI));
+                } else if (c.initCond == "gaussian_psi") {
+                    double psi = std::max(c.initFloor, gaussian_ic(c.gaussSigma, x, y, z) / (4.0 * M_PI));
+                    uc[0] = 2.0 * sqrt(M_PI) * psi;
+                } else if (c.initCond == "smooth") {
+                    uc[0] = smooth_ic(x, y, z) * 2.0 * sqrt(M_PI);
+                    if (nm > 3) {
+                        uc[1] = 0.3 * uc[0];
+                        uc[2] = 0.3 * uc[0];
+                        uc[3] = 0.3 * uc[0];
+                    }
+                } else {
+                    uc[0] = funky_ic(c, c.gaussSigma, x, y, z) * 2.0 * sqrt(M_PI);
+                }
+            }
+    // quadrature (src/init.cpp:509-548)
+    M.assign((size_t)nq * nm, 0.0);
+    w.assign(nq, 0.0);
+    xi.assign(nq, 0.0);
+    eta.assign(nq, 0.0);
+    mu.assign(nq, 0.0);
+    c3d_build_quadrature(c.momentOrder, c.quadOrder, w.data(), xi.data(), eta.data(), mu.data(),
+                         M.data(), nullptr);
+
+    c3d_params &P = params_;
+    P = c3d_params{};
+    P.nx = c.nx;
+    P.ny = c.ny;
+    P.nz = c.nz;
+    P.nm = nm;
+    P.nq = nq;
+    P.dx = dx_;
+    P.dy = dy_;
+    P.dz = dz_;
+    P.theta = c.theta;
+    P.solver = c.solver == "mn" ? 1 : 0;
+    P.pnUseKineticFlux = c.pnUseKineticFlux;
+    P.mnBatched = c.mnBatched ? 1 : 0;
+    P.mnMaxIter = c.mnMaxIter;
+    P.mnTol = c.mnTol;
+    P.mnTolGamma = c.mnTolGamma;
+    P.mnCondHMax = c.mnCondHMax;
+    P.nreg = (int)c.ladder.size();
+    for (size_t i = 0; i < c.ladder.size(); ++i)
+        P.reg[i] = c.ladder[i];
+
+    if (c.solver == "pn") {
+        // initPn, src/init.cpp:193-238
+        pnOps.assign((size_t)6 * nm * nm, 0.0);
+        for (int i = 0; i < nm; i++)
+            for (int j = 0; j < nm; j++) {
+                double v[6] = {0, 0, 0, 0, 0, 0};
+                for (int q = 0; q < nq; q++) {
+                    double mi = M[(size_t)q * nm + i], mj = M[(size_t)q * nm + j];
+                    if (xi[q] > 0) v[0] += xi[q] * mi * mj * w[q];
+                    else v[1] += xi[q] * mi * mj * w[q];
+                    if (eta[q] > 0) v[2] += eta[q] * mi * mj * w[q];
+                    else v[3] += eta[q] * mi * mj * w[q];
+                    if (mu[q] > 0) v[4] += mu[q] * mi * mj * w[q];
+                    else v[5] += mu[q] * mi * mj * w[q];
+                }
+                for (int k = 0; k < 6; k++)
+                    pnOps[(size_t)k * nm * nm + i * nm + j] = v[k];
+            }
+        maxDt_ = c.cfl * 0.5 * std::min(std::min(dx_, dy_), dz_);
+        alpha.clear();
+    } else {
+        if (c.mnUseGaunt)
+            fprintf(stderr, "[c3d_b200] MN_USE_GAUNT_COEF: the B200 closure forms H by direct "
+                            "quadrature (same H up to rounding)\n");
+        // initMn, src/init.cpp:260-274
+        alpha.assign(nall * nm, 0.0);
+        for (long long cell = 0; cell < nall; cell++)
+            alpha[cell * nm] = sqrt(4.0 * M_PI) * log(u[cell * nm] / sqrt(4.0 * M_PI));
+        maxDt_ = c.cfl * (2.0 / (2.0 + c.theta)) / (1.0 / dx_ + 1.0 / dy_ + 1.0 / dz_);
+    }
+}
+
+c3d_status Solver::init(const Config &cfg, void *stream)
+{
+    prepare(cfg);
+    c3d_status s = c3d_create(&params_, M.data(), w.data(), xi.data(), eta.data(), mu.data(),
+                              pnOps.empty() ? nullptr : pnOps.data(), stream, &ctx_);
+    if (s != C3D_OK)
+        return s;
+    return push();
+}
+
+c3d_status Solver::push()
+{
+    return c3d_set_state(ctx_, u.data(), alpha.empty() ? nullptr : alpha.data(), sigT.data(),
+                         sigS.data(), 0);
+}
+
+c3d_status Solver::pull()
+{
+    return c3d_get_state(ctx_, u.data(), alpha.empty() ? nullptr : alpha.data(), 0);
+}
+
+c3d_status Solver::update(double dt) { return c3d_step(ctx_, dt); }
+
+c3d_status Solver::run(int *stepsTaken)
+{
+    int steps = 0;
+    c3d_status s = C3D_OK;
+    if (cfg_.nsteps >= 0) {
+        for (int n = 0; n < cfg_.nsteps; ++n) {
+            if ((s = update(maxDt_)) != C3D_OK)
+                return s;
+            ++steps;
+        }
+    } else {
+        // src/main.cpp:57-76
+        double t = 0.0, dt;
+        const double tFinal = cfg_.tFinal;
+        for (double tOut = std::min(t + cfg_.outDt, tFinal); tOut <= tFinal;
+             tOut = std::min(tOut + cfg_.outDt, tFinal)) {
+            dt = maxDt_;
+            while (t < tOut - 1e-14 * tOut) {
+                t += dt;
+                if (t > tOut) {
+                    dt = tOut - (t - dt);
+                    t = tOut;
+                }
+                if ((s = update(dt)) != C3D_OK)
+                    return s;
+                ++steps;
+            }
+            if (tOut > tFinal - 1e-14 * tFinal)
+                break;
+        }
+    }
+    if (stepsTaken)
+        *stepsTaken = steps;
+    return c3d_sync(ctx_);
+}
+
+} // namespace c3d_host
+
+// ---------------------------------------------------------------- C ABI of the host solver
+using c3d_host::Solver;
+
+struct c3d_solver {
+    Solver s;
+};
+
+extern "C" {
+
+/* Reads a deck and runs init() (tables, IC, multipliers, dt) on the current device. */
+c3d_status c3d_solver_create(const char *deckPath, void *stream, c3d_solver **out)
+{
+    if (!deckPath || !out)
+        return C3D_ERR_INVALID;
+    c3d_host::InputDeck deck;
+    if (!deck.read(deckPath))
+        return C3D_ERR_INVALID;
+    c3d_host::Config cfg;
+    std::string err = c3d_host::parse_config(deck, cfg);
+    if (!err.empty()) {
+        fprintf(stderr, "[c3d_b200] %s: %s\n", deckPath, err.c_str());
+        return C3D_ERR_INVALID;
+    }
+    std::unique_ptr<c3d_solver> s(new c3d_solver());
+    c3d_status st = s->s.init(cfg, stream);
+    if (st != C3D_OK)
+        return st;
+    *out = s.release();
+    return C3D_OK;
+}
+
+/* Host-only init(): parses the deck and builds tables, initial state, cross
+ * sections, multipliers and dt_max without touching a GPU. errbuf receives the
+ * first missing or invalid key. */
+c3d_status c3d_solver_prepare(const char *deckPath, c3d_solver **out, char *errbuf, int errlen)
+{
+    if (!deckPath || !out)
+        return C3D_ERR_INVALID;
+    c3d_host::InputDeck deck;
+    std::string err;
+    if (!deck.read(deckPath))
+        err = "Could not open file.";
+    c3d_host::Config cfg;
+    if (err.empty())
+        err = c3d_host::parse_config(deck, cfg);
+    if (!err.empty()) {
+        if (errbuf && errlen > 0)
+            snprintf(errbuf, errlen, "%s", err.c_str());
+        return C3D_ERR_INVALID;
+    }
+    c3d_solver *s = new c3d_solver();
+    s->s.prepare(cfg);
+    *out = s;
+    return C3D_OK;
+}
+
+void c3d_solver_destroy(c3d_solver *s) { delete s; }
+
+c3d_status c3d_solver_update(c3d_solver *s, double dt) { return s ? s->s.update(dt) : C3D_ERR_INVALID; }
+c3d_status c3d_solver_run(c3d_solver *s, int *steps) { return s ? s->s.run(steps) : C3D_ERR_INVALID; }
+c3d_status c3d_solver_pull(c3d_solver *s) { return s ? s->s.pull() : C3D_ERR_INVALID; }
+c3d_status c3d_solver_push(c3d_solver *s) { return s ? s->s.push() : C3D_ERR_INVALID; }
+c3d_ctx *c3d_solver_context(c3d_solver *s) { return s ? s->s.ctx() : nullptr; }
+
+/* iv: nx ny nz nm nq solver(0 pn/1 mn) nsteps ; dv: dx dy dz maxDt theta tFinal */
+void c3d_solver_info(c3d_solver *s, int *iv, double *dv)
+{
+    const c3d_host::Config &c = s->s.config();
+    iv[0] = c.nx; iv[1] = c.ny; iv[2] = c.nz; iv[3] = s->s.nm(); iv[4] = s->s.nq();
+    iv[5] = c.solver == "mn" ? 1 : 0; iv[6] = c.nsteps; iv[7] = (int)c.ladder.size();
+    dv[0] = s->s.dx(); dv[1] = s->s.dy(); dv[2] = s->s.dz(); dv[3] = s->s.maxDt();
+    dv[4] = c.theta; dv[5] = c.tFinal;
+}
+
+/* Host mirrors (valid after c3d_solver_pull): 0 u, 1 alpha, 2 sigT, 3 sigS, 4 M, 5 w, 6 xi,
+ * 7 eta, 8 mu, 9 P_N operators. */
+double *c3d_solver_host_array(c3d_solver *s, int which)
+{
+    Solver &v = s->s;
+    std::vector<double> *a[] = {&v.u, &v.alpha, &v.sigT, &v.sigS, &v.M, &v.w, &v.xi, &v.eta, &v.mu, &v.pnOps};
+    if (which < 0 || which > 9 || a[which]->empty())
+        return nullptr;
+    return a[which]->data();
+}
+
+} // extern "C"

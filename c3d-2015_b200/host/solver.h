@@ -1,0 +1,88 @@
+// C++ host of the B200 M_N / P_N solver: the counterpart of the reference's
+// init() (src/init.cpp:344-576), update() (src/update.cpp:185-275) and time
+// loop (src/main.cpp:57-97), running every stage on one GPU through the C ABI
+// of include/c3d_b200.h.
+//
+// Deck keys are the reference's (all mandatory, src/init.cpp:364-381,
+// :195, :252-258). Optional keys, ignored by the reference, describe the
+// synthetic workloads the benchmark configurations need:
+//   NSTEPS n                 run exactly n steps of dt = dt_max (instead of TFINAL)
+//   REG_LADDER a,b,...       regularisation ladder (default 0,1e-3,1e-2,1e-1,5e-1)
+//   INIT_COND gaussian_psi   isotropic psi = max(INIT_FLOOR, G(x)/(4 pi)), u0 = 2 sqrt(pi) psi
+//   SIGMA_CHECKER_BLOCK b    sigma_s/sigma_a checkerboard over b^3-cell blocks:
+//   SIGMA_S_HI, SIGMA_A_HI     the odd blocks get sigma_s = SIGMA_S_HI, sigma_a = SIGMA_A_HI,
+//                              the even blocks sigma_s = CROSS_SECTION, sigma_a = 0;
+//                              sigma_t = sigma_s + sigma_a.
+#pragma once
+#include "../../include/c3d_b200.h"
+#include "deck.h"
+
+#include <string>
+#include <vector>
+
+namespace c3d_host {
+
+struct Config {
+    std::string solver = "mn", initCond = "gaussian";
+    double tFinal = 0, outDt = 0;
+    bool outputData = false, outputOptStats = false, outputTimings = false;
+    int nx = 0, ny = 0, nz = 0, mpix = 1, mpiy = 1, mpiz = 1;
+    double ax = 0, ay = 0, az = 0, bx = 0, by = 0, bz = 0;
+    int momentOrder = 0, quadOrder = 0;
+    double cfl = 0, crossSection = 0, initFloor = 0, gaussSigma = 0, theta = 2.0;
+    int ompThreads = 1;
+    bool cudaKinetic = false, cudaBatched = false;
+    int cudaBatchSize = 0;
+    int pnUseKineticFlux = 0;
+    double mnTol = 0, mnTolGamma = 0, mnCondHMax = 0;
+    int mnMaxIter = 0;
+    bool mnBatched = true, mnUseGaunt = false, mnUseGauntSparse = false;
+    // optional keys
+    int nsteps = -1;
+    std::vector<double> ladder{0.0, 1e-3, 1e-2, 1e-1, 5e-1};
+    int checkerBlock = 0;
+    double sigmaSHi = 0, sigmaAHi = 0;
+};
+
+// Parses a deck; returns "" on success or the first missing/invalid key.
+std::string parse_config(const InputDeck &deck, Config &cfg);
+
+class Solver {
+public:
+    ~Solver();
+    // Host half of init(): tables, initial condition, cross sections, multipliers, dt_max.
+    void prepare(const Config &cfg);
+    // init(): prepare() plus the device context and upload.
+    // stream: cudaStream_t for the device work (NULL: the context's own stream).
+    c3d_status init(const Config &cfg, void *stream = nullptr);
+    // update(dt): one SSP-RK2 step on the device (no host synchronisation).
+    c3d_status update(double dt);
+    // The time loop of src/main.cpp:57-76 (or NSTEPS steps); returns the steps taken.
+    c3d_status run(int *stepsTaken);
+    // Copies device state to the host arrays (u, alpha).
+    c3d_status pull();
+    // Copies the host arrays to the device (u, alpha, sigma_t, sigma_s).
+    c3d_status push();
+
+    const Config &config() const { return cfg_; }
+    c3d_ctx *ctx() { return ctx_; }
+    int nm() const { return nm_; }
+    int nq() const { return nq_; }
+    long long ncellsAll() const { return (long long)(cfg_.nx + 4) * (cfg_.ny + 4) * (cfg_.nz + 4); }
+    double dx() const { return dx_; }
+    double dy() const { return dy_; }
+    double dz() const { return dz_; }
+    double maxDt() const { return maxDt_; }
+
+    // host mirrors of the reference globals g_u, g_mnAlpha, g_sigmaT, g_sigmaS, g_m, g_w, ...
+    std::vector<double> u, alpha, sigT, sigS, M, w, xi, eta, mu, pnOps;
+
+private:
+    Config cfg_;
+    c3d_ctx *ctx_ = nullptr;
+    c3d_params params_{};
+    int nm_ = 0, nq_ = 0;
+    double dx_ = 0, dy_ = 0, dz_ = 0, maxDt_ = 0;
+};
+
+} // namespace c3d_host

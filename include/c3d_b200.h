@@ -1,0 +1,172 @@
+/*
+ * C ABI of the B200 M_N / P_N time step (libc3d_b200.so).
+ *
+ * Two groups of entry points:
+ *
+ * 1. Drop-in replacements for the reference's GPU offload layer,
+ *    src/cuda/cuda_headers.h:10-21 of ckrisgarrett/C3D-2015. Same names,
+ *    arguments and meaning (host pointers in and out, synchronous), so a build
+ *    of the reference links against this library instead of its own
+ *    src/cuda/*.cu files without source changes.
+ *
+ * 2. The device-resident step API that the C++ host (c3d-2015_b200/host) uses
+ *    to run update() (src/update.cpp:185-275) on one GPU: state stays in HBM
+ *    across stages and steps, the MPI halo exchange (src/comm.cpp) is an
+ *    on-device periodic ghost fill, and the closure is a persistent
+ *    work-queue kernel. Every function returns a c3d_status; none aborts.
+ *
+ * Arrays use the reference's layouts: per-cell moment vectors with the moment
+ * index fastest (IU, src/global.h:16), cells over the grid including two ghost
+ * layers per face with k fastest (I3D, src/global.h:15); tables row-major
+ * M[q*nm + m] (IM, src/global.h:18).
+ */
+#ifndef C3D_B200_H
+#define C3D_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status */
+typedef enum {
+    C3D_OK = 0,
+    C3D_ERR_INVALID = 1,     /* bad argument or unsupported size */
+    C3D_ERR_CUDA = 2,        /* CUDA runtime error (see c3d_last_error) */
+    C3D_ERR_NO_DEVICE = 3,   /* no CUDA device / extension unusable */
+    C3D_ERR_CLOSURE = 4,     /* one or more cells failed (u0 <= 0 or ladder exhausted) */
+    C3D_ERR_TIMEOUT = 5,     /* a bounded device wait gave up */
+    C3D_ERR_OOM = 6          /* device allocation failed */
+} c3d_status;
+
+/* Text of the last error on this thread. */
+const char *c3d_last_error(void);
+
+/* ------------------------------------------------------------------ 1. reference GPU entry points */
+
+/* Kinetic flux on the whole grid; replaces src/cuda/cuda_headers.h:10-13.
+ * nx,ny,nz include the ghost layers; alpha and flux are host arrays of
+ * nx*ny*nz*nm doubles; flux is zero on ghost cells; theta = 2 as in the
+ * reference's GPU path (src/cuda/cuda_flux_kinetic.cu:82). isPn selects the
+ * linear P_N ansatz. */
+void solveFluxKinetic_cuda(int nx, int ny, int nz, int nm, int nq, double dx, double dy, double dz,
+                           double *alpha, double *flux, double *xi, double *eta, double *mu,
+                           double *w, double *p, int isPn);
+
+/* Batched Hessians H_b = sum_q w_q exp(alpha_b . m_q) m_q m_q^T for batchSize
+ * multiplier vectors (host, batchSize*nm), written to hs (host, batchSize*nm*nm,
+ * row-major, symmetric). Replaces src/cuda/cuda_headers.h:15-17. Only the
+ * direct quadrature form is provided (useGaunt must be 0). */
+void solveH_cuda(int nm, int nm2, int nq, int batchSize, double *alphas, double *hs, int useGaunt,
+                 int useGauntSparse);
+
+/* One-time set-up for solveH_cuda (tables to the device); replaces
+ * src/cuda/cuda_headers.h:19-21. p2/beta/betaVal/betaColInd/betaRowPtr may be
+ * NULL when useGaunt is 0. */
+void solveHInit_cuda(int nm, int nm2, int nq, int batchSize, double *w, double *p, double *p2,
+                     double *beta, double *betaVal, int *betaColInd, int *betaRowPtr, int useGaunt);
+
+/* ------------------------------------------------------------------ 2. device-resident step API */
+
+typedef struct c3d_ctx c3d_ctx;
+
+/* Problem parameters: the input.deck keys the time step reads
+ * (src/init.cpp:364-381, :195, :252-258). */
+typedef struct {
+    int nx, ny, nz;            /* interior cells per axis (NX, NY, NZ) */
+    int nm;                    /* moments (MOMENT_ORDER+1)^2 */
+    int nq;                    /* quadrature points 2*QUAD_ORDER^2 */
+    double dx, dy, dz;
+    double theta;              /* THETA (slope limiter of the kinetic flux) */
+    int solver;                /* 0: P_N, 1: M_N (SOLVER) */
+    int pnUseKineticFlux;      /* PN_USE_KINETIC_FLUX */
+    int mnBatched;             /* MN_BATCHED: 1 batched stop rules, 0 unbatched rules */
+    int mnMaxIter;             /* MN_MAX_ITER */
+    double mnTol;              /* MN_TOL */
+    double mnTolGamma;         /* MN_TOL_GAMMA (batched rules; unbatched use 1.1) */
+    double mnCondHMax;         /* MN_COND_H_MAX */
+    int nreg;                  /* regularisation ladder (reference: 5 values) */
+    double reg[16];
+    size_t psiBytes;           /* budget for the materialised ansatz (0 = default) */
+} c3d_params;
+
+/* Closure counters accumulated on the device since the last reset (the
+ * reference's g_mn* statistics, src/update.cpp:79-97). */
+typedef struct {
+    long long cells;           /* dual solves (all cells, ghosts included) */
+    long long interiorCells;   /* unused (0) */
+    long long totalIters;      /* sum of Newton iterations */
+    int maxIter;               /* g_mnMaxIterHist */
+    int maxIterGamma;          /* g_mnMaxGammaIter */
+    long long totalIterGamma;
+    long long failed;          /* cells with a non-zero status */
+    long long trials;          /* line-search objective evaluations */
+    long long regHist[16];     /* g_mnHistReg */
+    long long iterHist[64];    /* cells per iteration count (last bin: >= 63) */
+} c3d_closure_stats;
+
+/* Creates a context on the current CUDA device with the tables M[nq*nm],
+ * w, xi, eta, mu [nq] (host arrays, copied). pnOps (6*nm*nm host array:
+ * xi+, xi-, eta+, eta-, mu+, mu-, src/init.cpp:193-238) is needed for the P_N
+ * moment flux and may be NULL otherwise. stream: a cudaStream_t or NULL for a
+ * new non-blocking stream owned by the context. */
+c3d_status c3d_create(const c3d_params *p, const double *M, const double *w, const double *xi,
+                      const double *eta, const double *mu, const double *pnOps, void *stream,
+                      c3d_ctx **out);
+void c3d_destroy(c3d_ctx *ctx);
+
+/* State transfer. where: 0 host arrays (synchronous copies), 1 device
+ * pointers (stream-ordered). Any pointer may be NULL to skip it. u/alpha
+ * hold nall*nm doubles, sigT/sigS nall doubles, nall = (nx+4)(ny+4)(nz+4). */
+c3d_status c3d_set_state(c3d_ctx *ctx, const double *u, const double *alpha, const double *sigT,
+                         const double *sigS, int where);
+c3d_status c3d_get_state(c3d_ctx *ctx, double *u, double *alpha, int where);
+c3d_status c3d_get_flux(c3d_ctx *ctx, double *flux, int where);
+
+/* Device pointers of the resident state (valid for the context's lifetime). */
+c3d_status c3d_device_state(c3d_ctx *ctx, double **u, double **alpha, double **flux);
+
+/* Stages of update(); stream-ordered, no host synchronisation. */
+c3d_status c3d_ghost_fill(c3d_ctx *ctx);                   /* communicateBoundaries */
+c3d_status c3d_closure(c3d_ctx *ctx);                      /* Optimization::opt / opt on all cells */
+c3d_status c3d_flux_kinetic(c3d_ctx *ctx, int alphaIsU);   /* solveFluxKinetic */
+c3d_status c3d_flux_moment(c3d_ctx *ctx);                  /* solveFluxMoment */
+c3d_status c3d_euler(c3d_ctx *ctx, double dt);             /* eulerStep */
+/* One SSP-RK2 step, update(dt). */
+c3d_status c3d_step(c3d_ctx *ctx, double dt);
+/* Waits for the context's stream; reports device-side failures. */
+c3d_status c3d_sync(c3d_ctx *ctx);
+
+/* Per-cell records of the last closure (host arrays of nall ints; any may be
+ * NULL): Newton iterations, gamma-only iterations, ladder index, status. */
+c3d_status c3d_closure_records(c3d_ctx *ctx, int *iters, int *iterGamma, int *regIndex,
+                               int *status);
+/* Counters accumulated since creation or the last reset (synchronises). */
+c3d_status c3d_closure_stats_get(c3d_ctx *ctx, c3d_closure_stats *st);
+c3d_status c3d_closure_stats_reset(c3d_ctx *ctx);
+
+/* Standalone batched closure of n independent moment vectors (device
+ * pointers u[n*nm], alpha[n*nm], solved in place; records may be NULL).
+ * Uses the context's tables and MN options; grid state is untouched. */
+c3d_status c3d_closure_vectors(c3d_ctx *ctx, long long n, double *u, double *alpha, int *iters,
+                               int *iterGamma, int *regIndex, int *status);
+
+/* Tables of src/init.cpp:509-548 (host arrays), so callers without GSL can
+ * build M, w, xi, eta, mu identical to the host's. M2 may be NULL. */
+void c3d_build_quadrature(int momentOrder, int quadOrder, double *w, double *xi, double *eta,
+                          double *mu, double *M, double *M2);
+
+/* Number of kernel launches issued by this context so far. */
+long long c3d_launch_count(c3d_ctx *ctx);
+
+/* Event timing on the context's stream around every closure and kinetic-flux
+ * launch (off by default). c3d_timing_get returns the summed milliseconds
+ * ms[0] closure, ms[1] kinetic flux and the launch counts since enabling. */
+c3d_status c3d_timing_enable(c3d_ctx *ctx, int on);
+c3d_status c3d_timing_get(c3d_ctx *ctx, double *ms, long long *count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -675,7 +675,8 @@ void orc_flux_moment(const orc_grid *g, const orc_tables *t, const double *u, do
     const double *ops = t->pnops;
     #pragma omp parallel
     {
-        double *tmp = (double *)malloc(sizeof(double) * nm * 4);
+        /* zeroed: mvProduct scales b by beta = 0 before accumulating (src/flux_moment.cpp:17) */
+        double *tmp = (double *)calloc((size_t)nm * 4, sizeof(double));
         double *xf = tmp + nm, *yf = xf + nm, *zf = yf + nm;
         #pragma omp for
         for (int i = 2; i <= g->nx + 1; i++)

@@ -326,6 +326,34 @@ void c3dref_opt_many(int nm, int nm2, int nq, long ncells, double *u, double *al
     }
 }
 
+/* The reference's batched closure (Optimization::opt, src/opt/optBatch.cpp:350-472)
+ * applied to n given moment vectors, with the tables and MN options of the current
+ * problem (c3dref_init first). Solved in place; iters may be NULL. */
+void c3dref_opt_batched_vectors(long n, double *u, double *alpha, int *iters)
+{
+    if (Optimization::c_stack1 == NULL) {
+        Optimization::c_stack1 = new std::stack<Optimization *>;
+        Optimization::c_stack2 = new std::stack<Optimization *>;
+        Optimization::c_stack3 = new std::stack<Optimization *>;
+    }
+    const int nm = g_numMoments;
+    for (long c = 0; c < n; c++)
+        Optimization::c_stack1->push(new Optimization((int)c, 0, 0, nm, u + c * nm, alpha + c * nm));
+    Optimization::opt(g_numMoments, g_numMoments2, g_numQuadPoints);
+    while (!Optimization::c_stack3->empty()) {
+        Optimization *o = Optimization::c_stack3->top();
+        Optimization::c_stack3->pop();
+        long c = o->c_i;
+        memcpy(alpha + c * nm, o->c_alpha, nm * sizeof(double));
+        memcpy(u + c * nm, o->c_u, nm * sizeof(double));
+        if (iters)
+            iters[c] = o->c_totalIter;
+        free(o->c_alpha);
+        free(o->c_u);
+        delete o;
+    }
+}
+
 int c3dref_num_threads()
 {
     int n = 1;

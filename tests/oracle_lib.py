@@ -219,8 +219,10 @@ class Oracle:
 
 
 # ---------------------------------------------------------------------- reference
+# TFINAL bounds the reference's per-step timer array (src/init.cpp:560-561); keep it
+# above the simulated time of every test so update() stays inside that array.
 DECK_KEYS_DEFAULT = dict(
-    SOLVER="mn", TFINAL="0.1", OUTDT="1000", OUTPUT_DATA="false", OUTPUT_OPT_STATS="false",
+    SOLVER="mn", TFINAL="10", OUTDT="1000", OUTPUT_DATA="false", OUTPUT_OPT_STATS="false",
     OUTPUT_TIMINGS="false", NX="8", NY="8", NZ="8", MPIX="1", MPIY="1", MPIZ="1", AX="-1",
     AY="-1", AZ="-1", BX="1", BY="1", BZ="1", MOMENT_ORDER="2", QUAD_ORDER="12",
     CFL_FACTOR="0.5", CROSS_SECTION="1.0", INIT_FLOOR="1e-4", GAUSS_SIGMA="0.2",
@@ -236,7 +238,7 @@ def deck_text(**kw):
     return "".join(f"{k} {v}\n" for k, v in d.items())
 
 
-def _ref_worker(conn, deck, ladder, nsteps, overrides, record, want):
+def _ref_worker(conn, deck, ladder, nsteps, overrides, record, want):  # noqa: C901
     """Runs inside a spawned process: one reference problem."""
     L = ctypes.CDLL(REF_SO)
     L.c3dref_init.argtypes = [ctypes.c_char_p]
@@ -274,7 +276,10 @@ def _ref_worker(conn, deck, ladder, nsteps, overrides, record, want):
         res["xi"], res["eta"], res["mu"] = arr(7, nq).copy(), arr(8, nq).copy(), arr(9, nq).copy()
     dt = dv[3]
     iters = []
+    snaps = []
     for s in range(nsteps):
+        if "snapshots" in want:
+            snaps.append((u.copy(), None if alpha is None else alpha.copy()))
         if record:
             it = np.zeros(2 * nall, np.int32)
             ig = np.zeros(2 * nall, np.int32)
@@ -289,21 +294,63 @@ def _ref_worker(conn, deck, ladder, nsteps, overrides, record, want):
     L.c3dref_stats(st)
     res["stats"] = list(st)[:5 + 16]
     res["iters"] = iters
+    res["snapshots"] = snaps
+    if "flux" in want:
+        L.c3dref_flux_kinetic.argtypes = [_dp]
+        if iv[6] == 1:
+            L.c3dref_flux_kinetic(alpha.ctypes.data_as(_dp))
+        elif iv[10]:
+            L.c3dref_flux_kinetic(u.ctypes.data_as(_dp))
+        else:
+            L.c3dref_flux_moment()
+        res["flux"] = arr(16, nall * nm).copy()
+    if "pnops" in want:
+        res["pnops"] = np.concatenate([arr(10 + k, nm * nm).copy() for k in range(6)])
     conn.send(res)
     conn.close()
 
 
 def run_reference(deck, *, ladder=None, nsteps=1, overrides=None, record=True, want=()):
-    """Runs the reference on a deck in a fresh spawned process and returns its state."""
+    """Runs the reference on a deck in a fresh spawned process and returns its state.
+
+    The process starts with glibc's malloc perturb byte 0x3F, so every recycled or
+    fresh malloc block holds finite bytes (0x3F3F... or 0xC0C0...): the reference's
+    P_N moment flux multiplies never-initialised thread-private buffers by 0.0
+    (mvProduct with beta = 0, src/flux_moment.cpp:15-24 on buffers from :243-249),
+    which yields NaN whenever the stale bytes happen to encode NaN or Inf."""
     if not os.path.exists(REF_SO):
         raise FileNotFoundError(REF_SO + " (run `make -C oracle ref`)")
     ctx = mp.get_context("spawn")
     a, b = ctx.Pipe(duplex=False)
     p = ctx.Process(target=_ref_worker, args=(b, deck, ladder, nsteps, overrides, record,
                                               tuple(want)))
-    p.start()
+    old = os.environ.get("GLIBC_TUNABLES")
+    os.environ["GLIBC_TUNABLES"] = "glibc.malloc.perturb=63"
+    try:
+        p.start()
+    finally:
+        if old is None:
+            del os.environ["GLIBC_TUNABLES"]
+        else:
+            os.environ["GLIBC_TUNABLES"] = old
     b.close()
     res = a.recv()
     p.join()
     assert p.exitcode == 0, p.exitcode
     return res
+
+
+def _ref_standalone(conn, nm, nm2, nq, u, a, w, M, M2, max_iter, tol, cond):
+    """Spawned process: the reference's unbatched opt() on independent vectors."""
+    L = ctypes.CDLL(REF_SO)
+    L.c3dref_opt_init(nm, nm2)
+    n = u.shape[0]
+    uu, aa = np.ascontiguousarray(u).copy(), np.ascontiguousarray(a).copy()
+    it = np.zeros(n, np.int32)
+    L.c3dref_opt_many.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_long, _dp,
+                                  _dp, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                  ctypes.c_double, _dp, _dp, _dp, _ip, _ip, _dp]
+    L.c3dref_opt_many(nm, nm2, nq, n, _p(uu), _p(aa), max_iter, tol, 1.1, cond, _p(w), _p(M),
+                      _p(M2), _pi(it), None, None)
+    conn.send((it, aa))
+    conn.close()

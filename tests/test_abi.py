@@ -1,0 +1,44 @@
+"""The C-ABI library loads without a GPU and exports every function include/c3d_b200.h
+declares (no compute calls here)."""
+import ctypes
+import os
+import re
+
+import c3d
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_functions():
+    text = open(os.path.join(REPO, "include", "c3d_b200.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    names = re.findall(r"\b([A-Za-z_][A-Za-z0-9_]*)\s*\(", text)
+    skip = {"if", "sizeof", "defined"}
+    return sorted({n for n in names if n not in skip and not n.isupper()})
+
+
+def test_library_exports_header_symbols():
+    lib = ctypes.CDLL(c3d.LIB_PATH)
+    declared = header_functions()
+    assert len(declared) >= 20
+    missing = [n for n in declared if not hasattr(lib, n)]
+    assert not missing, missing
+    assert sorted(c3d.HEADER_SYMBOLS) == declared
+
+
+def test_no_device_reports_error_not_abort():
+    """Without a device, creating a context returns an error code (no abort, no fallback)."""
+    try:
+        import torch
+        if torch.cuda.is_available():
+            return
+    except Exception:
+        pass
+    q = c3d.quadrature(1, 4)
+    try:
+        c3d.Context(nx=4, ny=4, nz=4, nm=q["nm"], nq=q["nq"], dx=0.5, dy=0.5, dz=0.5, M=q["M"],
+                    w=q["w"], xi=q["xi"], eta=q["eta"], mu=q["mu"])
+    except c3d.C3DError as e:
+        assert "NO_DEVICE" in str(e) or "CUDA" in str(e)
+    else:
+        raise AssertionError("context creation without a device must fail")

@@ -1,0 +1,121 @@
+"""Oracle and B200 path against golden outputs of the reference CPU path
+(tests/golden/make_golden.py; decks described there).
+
+* P_N (no closure): bit-exact for the oracle; 1e-13 relative L2 for the GPU path.
+* M_2 16^3 at MN_TOL 1e-6 (no rounding ties at this tolerance): per-cell iteration
+  counts and ladder indices of the first two steps identical; moments after 2 and
+  20 steps within 1e-12 relative L2.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import c3d
+from oracle_lib import make_opts, tie_cells
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLD = os.path.join(HERE, "golden")
+sys_path_added = False
+
+
+def _golden_module():
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("make_golden",
+                                                  os.path.join(GOLD, "make_golden.py"))
+    m = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(m)
+    return m
+
+
+def _deck(tmp_path, text):
+    p = tmp_path / "input.deck"
+    p.write_text(text)
+    return str(p)
+
+
+def _pn_deck():
+    from oracle_lib import deck_text
+    return deck_text(SOLVER="pn", NX=8, NY=6, NZ=7, MOMENT_ORDER=3, QUAD_ORDER=8,
+                     INIT_COND="smooth", PN_USE_KINETIC_FLUX=0)
+
+
+def test_oracle_pn_golden(oracle, tmp_path):
+    G = np.load(os.path.join(GOLD, "pn_p3_8.npz"))
+    host = c3d.Solver(_deck(tmp_path, _pn_deck()), host_only=True)
+    A = host.arrays()
+    T = oracle.tables(3, 8, pn=True)
+    g = oracle.grid(8, 6, 7, 16, 128, host.dx, host.dy, host.dz, 2.0)
+    u = A["u"].copy()
+    alpha = np.zeros_like(u)
+    for _ in range(5):
+        oracle.step(g, make_opts(16, 128), T, u, alpha, A["sigT"], A["sigS"], host.max_dt,
+                    solver=0, records=False)
+    assert host.max_dt == float(G["dt"])
+    assert np.array_equal(u.reshape(12, 10, 11, 16)[2:10, 2:8, 2:9], G["u_step5"])
+
+
+def test_oracle_c1_golden(oracle, tmp_path):
+    mg = _golden_module()
+    G = np.load(os.path.join(GOLD, "c1_m2_16.npz"))
+    host = c3d.Solver(_deck(tmp_path, mg.c1_deck("gaussian_psi")), host_only=True)
+    A = host.arrays()
+    T = oracle.tables(2, 12)
+    n = 16
+    g = oracle.grid(n, n, n, 9, 288, host.dx, host.dy, host.dz, 2.0)
+    opts = make_opts(9, 288, tol=1e-6, ladder=mg.C1_LADDER)
+    u, a = A["u"].copy(), A["alpha"].copy()
+    inner = (slice(2, n + 2),) * 3
+    for s in range(20):
+        bad, rec = oracle.step(g, opts, T, u, a, A["sigT"], A["sigS"], host.max_dt)
+        assert bad == 0
+        if s < 2:
+            assert not tie_cells(rec).any()
+            assert np.array_equal(rec["totalIter"], G["iters"][s])
+            assert np.array_equal(rec["regIndex"], G["reg"][s])
+        if s in (1, 19):
+            ref = G["u_step2"] if s == 1 else G["u_step20"]
+            x = u.reshape(n + 4, n + 4, n + 4, 9)[inner]
+            rel = np.linalg.norm(x - ref) / np.linalg.norm(ref)
+            assert rel < 1e-12, (s, rel)
+
+
+@pytest.mark.gpu
+def test_gpu_c1_golden(tmp_path):
+    mg = _golden_module()
+    G = np.load(os.path.join(GOLD, "c1_m2_16.npz"))
+    s = c3d.Solver(_deck(tmp_path, mg.c1_deck("gaussian_psi")))
+    n, nall = 16, s.nall
+    inner = (slice(2, n + 2),) * 3
+    for k in range(20):
+        s.update(s.max_dt)
+        if k == 1:
+            s.sync()
+            rec = s.records()
+            assert np.array_equal(rec["iters"], G["iters"][1][nall:])
+            assert np.array_equal(rec["regIndex"], G["reg"][1][nall:])
+        if k in (1, 19):
+            s.pull()
+            x = s.arrays()["u"].reshape(n + 4, n + 4, n + 4, 9)[inner]
+            ref = G["u_step2"] if k == 1 else G["u_step20"]
+            rel = np.linalg.norm(x - ref) / np.linalg.norm(ref)
+            assert rel < 1e-12, (k, rel)
+    st = s.stats()
+    assert st.failed == 0
+    assert st.cells == 2 * 20 * nall
+    s.close()
+
+
+@pytest.mark.gpu
+def test_gpu_pn_golden(tmp_path):
+    G = np.load(os.path.join(GOLD, "pn_p3_8.npz"))
+    s = c3d.Solver(_deck(tmp_path, _pn_deck()))
+    for _ in range(5):
+        s.update(s.max_dt)
+    s.sync()
+    s.pull()
+    x = s.arrays()["u"].reshape(12, 10, 11, 16)[2:10, 2:8, 2:9]
+    ref = G["u_step5"]
+    rel = np.linalg.norm(x - ref) / np.linalg.norm(ref)
+    assert rel < 1e-13, rel
+    s.close()

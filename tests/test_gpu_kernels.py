@@ -1,0 +1,249 @@
+"""GPU parity of the B200 kernels against the C oracle on identical inputs.
+
+Tolerances:
+* ghost fill, Euler stage, RK copy/average: bit-exact (same unfused operations);
+* kinetic flux: 1e-13 relative L2 (directional sums reordered by nothing, but
+  exp() and fused multiply-adds differ from the CPU by ulps);
+* closure: identical per-cell iteration counts except rounding ties (decisions
+  the oracle took by a margin below two FP64 evaluations' disagreement, see
+  oracle_lib.tie_cells); multipliers of the other cells within 1e-10 relative.
+"""
+import numpy as np
+import pytest
+
+import c3d
+from oracle_lib import make_opts, tie_cells
+
+pytestmark = pytest.mark.gpu
+
+
+def _setup(oracle, N=2, Q=12, n=8, sigma=0.2, floor=1e-4, steps_before=0, batched=True, ladder=None):
+    """Initial state of a gaussian deck (reference init formulas), optionally advanced
+    by the oracle so that many cells are anisotropic."""
+    T = oracle.tables(N, Q)
+    nm, nq = T["nm"], T["nq"]
+    nx = ny = nz = n
+    dx = 2.0 / n
+    nall = (n + 4) ** 3
+    u = np.zeros((nall, nm))
+    idx = np.arange(n + 4)
+    x = -1 + (idx - 2) * dx + dx / 2.0
+    X, Y, Z = np.meshgrid(x, x, x, indexing="ij")
+    f1 = 1.0 / (sigma * np.sqrt(2.0 * np.pi))
+    G = f1 * f1 * f1 * np.exp(-(X * X + Y * Y + Z * Z) / (2.0 * sigma * sigma))
+    u[:, 0] = np.maximum(floor, (G * 2.0 * np.sqrt(np.pi)).ravel())
+    alpha = np.zeros((nall, nm))
+    alpha[:, 0] = np.sqrt(4.0 * np.pi) * np.log(u[:, 0] / np.sqrt(4.0 * np.pi))
+    sig = np.ones(nall)
+    g = oracle.grid(n, n, n, nm, nq, dx, dx, dx, 2.0)
+    opts = make_opts(nm, nq, batched=batched, ladder=ladder)
+    dt = 0.5 * (2.0 / 4.0) / (3.0 / dx)
+    u = u.ravel()
+    alpha = alpha.ravel()
+    for _ in range(steps_before):
+        oracle.step(g, opts, T, u, alpha, sig, sig, dt, records=False)
+    return dict(T=T, g=g, opts=opts, u=u, alpha=alpha, sig=sig, dt=dt, n=n, dx=dx, nm=nm, nq=nq,
+                nall=nall, batched=batched, ladder=ladder)
+
+
+def _ctx(S, **kw):
+    T = S["T"]
+    ladder = S["ladder"] or (0.0, 1e-3, 1e-2, 1e-1, 5e-1)
+    return c3d.Context(nx=S["n"], ny=S["n"], nz=S["n"], nm=S["nm"], nq=S["nq"], dx=S["dx"],
+                       dy=S["dx"], dz=S["dx"], M=T["M"], w=T["w"], xi=T["xi"], eta=T["eta"],
+                       mu=T["mu"], batched=S["batched"], ladder=ladder, **kw)
+
+
+def test_ghost_fill_and_euler_bit_exact(oracle):
+    S = _setup(oracle, steps_before=1)
+    ctx = _ctx(S)
+    rng = np.random.default_rng(1)
+    u = S["u"] + rng.standard_normal(S["u"].shape) * 1e-3
+    flux = rng.standard_normal(S["u"].shape)
+    sig_t = 1.0 + rng.random(S["nall"])
+    sig_s = rng.random(S["nall"])
+    ctx.set_state(u=u, alpha=S["alpha"], sig_t=sig_t, sig_s=sig_s)
+    ctx.ghost_fill()
+    ctx.sync()
+    ug, _ = ctx.get_state()
+    uo = u.copy()
+    oracle.ghost_fill(S["g"], uo)
+    assert np.array_equal(ug, uo)
+
+
+def test_kinetic_flux_matches_oracle(oracle):
+    S = _setup(oracle, steps_before=2)
+    ctx = _ctx(S)
+    ctx.set_state(u=S["u"], alpha=S["alpha"], sig_t=S["sig"], sig_s=S["sig"])
+    ctx.flux_kinetic(0)
+    ctx.sync()
+    fg = ctx.get_flux()
+    fo = oracle.flux_kinetic(S["g"], S["T"], S["alpha"])
+    n = S["n"]
+    nm = S["nm"]
+    inner = (slice(2, n + 2),) * 3
+    fg = fg.reshape(n + 4, n + 4, n + 4, nm)[inner]
+    fo = fo.reshape(n + 4, n + 4, n + 4, nm)[inner]
+    rel = np.linalg.norm(fg - fo) / np.linalg.norm(fo)
+    assert rel < 1e-13, rel
+
+
+@pytest.mark.parametrize("batched", [True, False])
+def test_closure_matches_oracle(oracle, batched):
+    S = _setup(oracle, steps_before=2, batched=batched)
+    ctx = _ctx(S)
+    ctx.set_state(u=S["u"], alpha=S["alpha"], sig_t=S["sig"], sig_s=S["sig"])
+    ctx.closure()
+    ctx.sync()
+    ug, ag = ctx.get_state()
+    rec = ctx.records()
+    nm = S["nm"]
+    uo = S["u"].reshape(-1, nm).copy()
+    ao = S["alpha"].reshape(-1, nm).copy()
+    out = oracle.closure(S["opts"], S["T"], uo, ao)
+    assert (rec["status"] == 0).all()
+    ties = tie_cells(out)
+    mism = rec["iters"] != out["totalIter"]
+    assert not (mism & ~ties).any(), np.nonzero(mism & ~ties)[0][:10]
+    ok = ~ties & (rec["regIndex"] == out["regIndex"])
+    ag = ag.reshape(-1, nm)
+    rel = np.linalg.norm(ag[ok] - ao[ok], axis=1) / np.linalg.norm(ao[ok], axis=1)
+    assert rel.max() < 1e-10, rel.max()
+    assert mism.sum() <= 0.02 * len(mism)
+
+
+def test_step_matches_oracle_without_ties(oracle):
+    """At MN_TOL 1e-6 the last Newton steps sit far above the rounding level of the
+    Armijo test, so no decision is a tie: whole RK2 steps agree to rounding."""
+    S = _setup(oracle, steps_before=1)
+    S["opts"] = make_opts(S["nm"], S["nq"], tol=1e-6)
+    ctx = _ctx(S, tol=1e-6)
+    ctx.set_state(u=S["u"], alpha=S["alpha"], sig_t=S["sig"], sig_s=S["sig"])
+    uo, ao = S["u"].copy(), S["alpha"].copy()
+    n, nm = S["n"], S["nm"]
+    inner = (slice(2, n + 2),) * 3
+    for _ in range(3):
+        ctx.step(S["dt"])
+        ctx.sync()
+        bad, rec = oracle.step(S["g"], S["opts"], S["T"], uo, ao, S["sig"], S["sig"], S["dt"])
+        assert not tie_cells(rec).any()
+    ug, ag = ctx.get_state()
+    a = ug.reshape(n + 4, n + 4, n + 4, nm)[inner]
+    b = uo.reshape(n + 4, n + 4, n + 4, nm)[inner]
+    rel = np.linalg.norm(a - b) / np.linalg.norm(b)
+    assert rel < 1e-12, rel
+
+
+def test_step_stages_match_oracle(oracle):
+    """MN_TOL 1e-8: stage by stage, the closure's iteration counts match except ties; after
+    a stage whose tie changed a regularisation level, both sides continue from the oracle's
+    state so later stages are still compared on identical inputs."""
+    S = _setup(oracle, steps_before=1)
+    ctx = _ctx(S)
+    n, nm, g, T = S["n"], S["nm"], S["g"], S["T"]
+    inner = (slice(2, n + 2),) * 3
+    u, a = S["u"].copy(), S["alpha"].copy()
+    ctx.set_state(u=u, alpha=a, sig_t=S["sig"], sig_s=S["sig"])
+    compared = 0
+    for step in range(2):
+        uold = u.copy()
+        for stage in range(2):
+            ctx.ghost_fill()
+            oracle.ghost_fill(g, u)
+            ctx.closure()
+            ctx.sync()
+            ur, ar = u.reshape(-1, nm), a.reshape(-1, nm)
+            out = oracle.closure(S["opts"], T, ur, ar)
+            rec = ctx.records()
+            ties = tie_cells(out)
+            mism = rec["iters"] != out["totalIter"]
+            assert not (mism & ~ties).any()
+            if (rec["regIndex"] != out["regIndex"]).any():
+                ctx.set_state(u=u, alpha=a)  # continue from the oracle's state
+            else:
+                ug, ag = ctx.get_state()
+                ok = np.repeat(~ties, nm)
+                assert np.abs(ag - a)[ok].max() <= 1e-9 * np.abs(a).max()
+                ctx.set_state(u=u, alpha=a)
+                compared += 1
+            ctx.flux_kinetic(0)
+            ctx.sync()
+            fo = oracle.flux_kinetic(g, T, a)
+            fg = ctx.get_flux()
+            fi = lambda f: f.reshape(n + 4, n + 4, n + 4, nm)[inner]
+            assert np.linalg.norm(fi(fg) - fi(fo)) <= 1e-13 * np.linalg.norm(fi(fo))
+            ctx.euler(S["dt"])
+            ctx.sync()
+            oracle.euler(g, u, fo, S["sig"], S["sig"], S["dt"])
+            ug, _ = ctx.get_state()
+            assert np.linalg.norm(fi(ug) - fi(u)) <= 1e-14 * np.linalg.norm(fi(u))
+            ctx.set_state(u=u)
+        u_i = u.reshape(n + 4, n + 4, n + 4, nm)
+        o_i = uold.reshape(n + 4, n + 4, n + 4, nm)
+        u_i[inner] = 0.5 * (u_i[inner] + o_i[inner])
+        ctx.set_state(u=u)
+    assert compared >= 1
+
+
+def test_step_equals_stage_sequence(oracle):
+    """c3d_step is exactly the stage sequence of update() (same kernels, bit for bit)."""
+    S = _setup(oracle, steps_before=1)
+    A, B = _ctx(S), _ctx(S)
+    for c in (A, B):
+        c.set_state(u=S["u"], alpha=S["alpha"], sig_t=S["sig"], sig_s=S["sig"])
+    A.step(S["dt"])
+    A.sync()
+    n, nm = S["n"], S["nm"]
+    uB, aB = B.get_state()
+    uold = uB.copy()
+    for _ in range(2):
+        B.ghost_fill()
+        B.closure()
+        B.flux_kinetic(0)
+        B.euler(S["dt"])
+    B.sync()
+    uB, aB = B.get_state()
+    inner = (slice(2, n + 2),) * 3
+    ub = uB.reshape(n + 4, n + 4, n + 4, nm)
+    ob = uold.reshape(n + 4, n + 4, n + 4, nm)
+    ub[inner] = 0.5 * (ub[inner] + ob[inner])
+    uA, aA = A.get_state()
+    assert np.array_equal(uA, ub.ravel())
+    assert np.array_equal(aA, aB)
+
+
+def test_reference_entry_points(oracle):
+    """solveH_cuda / solveFluxKinetic_cuda with the reference's signatures (host buffers)."""
+    import ctypes
+    S = _setup(oracle, steps_before=1)
+    T, nm, nq = S["T"], S["nm"], S["nq"]
+    L = c3d.lib()
+    dp = ctypes.POINTER(ctypes.c_double)
+    B = 50
+    al = S["alpha"].reshape(-1, nm)[:B].copy()
+    al[:, 0] -= np.log(np.maximum(S["u"].reshape(-1, nm)[:B, 0], 1e-300)) * 2 * np.sqrt(np.pi)
+    L.solveHInit_cuda(nm, 0, nq, B, T["w"].ctypes.data_as(dp), T["M"].ctypes.data_as(dp), None,
+                      None, None, None, None, 0)
+    hs = np.zeros(B * nm * nm)
+    L.solveH_cuda(nm, 0, nq, B, al.ctypes.data_as(dp), hs.ctypes.data_as(dp), 0, 0)
+    hs = hs.reshape(B, nm, nm)
+    for b in range(B):
+        ho = oracle.hessian(S["opts"], T, al[b].copy())
+        assert np.allclose(hs[b], ho, rtol=1e-13, atol=1e-15 * np.abs(ho).max())
+    n = S["n"]
+    flux = np.zeros(S["nall"] * nm)
+    a = S["alpha"].copy()
+    L.solveFluxKinetic_cuda(n + 4, n + 4, n + 4, nm, nq, S["dx"], S["dx"], S["dx"],
+                            a.ctypes.data_as(dp), flux.ctypes.data_as(dp),
+                            T["xi"].ctypes.data_as(dp), T["eta"].ctypes.data_as(dp),
+                            T["mu"].ctypes.data_as(dp), T["w"].ctypes.data_as(dp),
+                            T["M"].ctypes.data_as(dp), 0)
+    fo = oracle.flux_kinetic(S["g"], T, S["alpha"])
+    inner = (slice(2, n + 2),) * 3
+    fg = flux.reshape(n + 4, n + 4, n + 4, nm)
+    assert np.abs(fg).sum() > 0
+    rel = np.linalg.norm(fg[inner] - fo.reshape(fg.shape)[inner]) / np.linalg.norm(fo)
+    assert rel < 1e-13
+    ghost = np.ones(fg.shape[:3], bool)
+    ghost[inner] = False
+    assert (fg[ghost] == 0).all()
