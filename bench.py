@@ -48,9 +48,10 @@ CONFIGS = {
     "c3": dict(N=6, Q=28, n=128, sigma=0.02, floor=1e-10, sigma_s=1.0,
                desc="M_6 (49 moments) 128^3 periodic, 1568-point quadrature (28 mu x 56 phi), "
                     "gaussian pulse width 0.02 floor 1e-10"),
-    # the same kernels on a 24^3 grid: the small case for ncu section captures
-    "c3s": dict(N=6, Q=28, n=24, sigma=0.02, floor=1e-10, sigma_s=1.0,
-                desc="M_6 (49 moments) 24^3 periodic, 1568-point quadrature, pulse width 0.02 "
+    # the same kernels on a 64^3 grid (u and alpha 0.12 GB each, above L2; about 2 GB on
+    # the device): the small case for ncu section captures
+    "c3m": dict(N=6, Q=28, n=64, sigma=0.02, floor=1e-10, sigma_s=1.0,
+                desc="M_6 (49 moments) 64^3 periodic, 1568-point quadrature, pulse width 0.02 "
                      "floor 1e-10 (profiling case)"),
 }
 
@@ -304,7 +305,10 @@ def b200_arm(args):
                                 device_id=torch.device("cuda", local))
     cfg = args.config
     c = CONFIGS[cfg]
-    stream = torch.cuda.current_stream()
+    # a dedicated (non-default) stream: the library launches on it and the CUDA events
+    # below are recorded on it
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     with tempfile.TemporaryDirectory() as tmp:
         deck = os.path.join(tmp, "input.deck")
         with open(deck, "w") as f:

@@ -212,7 +212,7 @@ c3d_status c3d_create(const c3d_params *p, const double *M, const double *w, con
     for (int i = 0; i < p->nreg; ++i)
         cp.reg[i] = p->reg[i];
     cp.passBudget = 1LL << 40;
-    c->psiBytes = p->psiBytes ? p->psiBytes : (size_t)32 << 30;
+    c->psiBytes = p->psiBytes ? p->psiBytes : (size_t)16 << 30;
 
     const long long nall = c->g.nall();
     const int nm = p->nm, nq = p->nq;
