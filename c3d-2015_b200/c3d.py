@@ -27,7 +27,7 @@ HEADER_SYMBOLS = [
     "c3d_ghost_fill", "c3d_closure", "c3d_flux_kinetic", "c3d_flux_moment", "c3d_euler",
     "c3d_step", "c3d_sync", "c3d_closure_records", "c3d_closure_stats_get",
     "c3d_closure_stats_reset", "c3d_closure_vectors", "c3d_build_quadrature",
-    "c3d_launch_count", "c3d_timing_enable", "c3d_timing_get",
+    "c3d_launch_count", "c3d_timing_enable", "c3d_timing_get", "c3d_closure_vectors_noalloc",
 ]
 
 

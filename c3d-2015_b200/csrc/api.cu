@@ -48,6 +48,10 @@ using namespace c3d;
 
 static thread_local std::string g_lastError;
 
+namespace c3d {
+void set_last_error(const std::string &msg) { g_lastError = msg; }
+} // namespace c3d
+
 static c3d_status fail(c3d_status s, const std::string &msg)
 {
     g_lastError = msg;
@@ -208,7 +212,6 @@ c3d_status c3d_create(const c3d_params *p, const double *M, const double *w, con
     cp.tol = p->mnTol;
     cp.tolGamma = p->mnBatched ? p->mnTolGamma : 1.1;
     cp.condHMax = p->mnCondHMax;
-    cp.m0 = M[0];
     for (int i = 0; i < p->nreg; ++i)
         cp.reg[i] = p->reg[i];
     cp.passBudget = 1LL << 40;

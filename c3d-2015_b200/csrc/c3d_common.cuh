@@ -47,7 +47,6 @@ struct ClosureParams {
     double tol;
     double tolGamma; // 1.1 for the unbatched rules (src/update.cpp:57)
     double condHMax;
-    double m0;       // M[0][0] = 1/(2 sqrt(pi)), the constant harmonic
     double reg[MAX_REG];
     long long passBudget; // safety bound on H/line-search passes per cell
 };

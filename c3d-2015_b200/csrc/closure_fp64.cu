@@ -525,10 +525,10 @@ __device__ void next_trial(Slot<NT> &sl, const ClosureParams &P, const Outputs &
 }
 
 template <int NT>
-__device__ void after_hessian(Slot<NT> &sl, const ClosureParams &P, const Outputs &O, int lane)
+__device__ void after_hessian(Slot<NT> &sl, const ClosureParams &P, const Outputs &O, int lane,
+                              double m0)
 {
     const int nm = P.nm;
-    const double m0 = P.m0;
     // g_i = H_i0 / m_0 - u_i ; f = H_00 / m_0^2 - alpha.u  (src/opt/fobj.cpp:121-129)
     for (int i = lane; i < nm; i += 32)
         sl.g[i] = sl.L[pidx(i, 0)] / m0 - sl.u[i];
@@ -686,6 +686,7 @@ __global__ void __launch_bounds__(W * 32, 1)
     const int nm = P.nm, nchunks = P.nchunks;
     const uint32_t chunkBytes = CH * sizeof(double);
     Slot<NT> &sl = slots[warp];
+    const double m0 = chunks[0]; // M[0][0], the constant harmonic 1/(2 sqrt(pi))
 
     if (tid == 0) {
         for (int s = 0; s < STAGES; ++s)
@@ -802,7 +803,7 @@ __global__ void __launch_bounds__(W * 32, 1)
                     }
                 }
             __syncwarp();
-            after_hessian(sl, P, O, lane);
+            after_hessian(sl, P, O, lane, m0);
         } else if (need == NEED_TRIAL) {
             double fq = warp_sum(fpart);
             after_trial(sl, P, O, lane, fq);

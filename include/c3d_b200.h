@@ -160,6 +160,41 @@ void c3d_build_quadrature(int momentOrder, int quadOrder, double *w, double *xi,
 /* Number of kernel launches issued by this context so far. */
 long long c3d_launch_count(c3d_ctx *ctx);
 
+/* ------------------------------------------------------------------ allocation-free closure */
+
+/* Closure options for the allocation-free entry point (the MN_* deck keys). */
+typedef struct {
+    int batched;        /* 1: batched stop rules (absolute tol, tolGamma); 0: unbatched */
+    int maxIter;
+    double tol;
+    double tolGamma;
+    double condHMax;
+    int nreg;
+    double reg[16];
+} c3d_closure_opts;
+
+/* Bytes of the per-GPU static scratch array used by c3d_closure_vectors_noalloc. */
+#define C3D_NOALLOC_SCRATCH_BYTES 1202176
+
+/* Standalone closure of n moment vectors that allocates no device memory. It has no
+ * counterpart in the reference: it exists for callers that may not call cudaMalloc,
+ * such as an application that serves this library device memory from its own
+ * pre-reserved pool (where an extra cudaMalloc fails or breaks its accounting) or
+ * a latency-critical caller that must avoid the implicit device synchronisation of
+ * cudaMalloc/cudaFree. All arguments are the caller's device pointers (M[nq*nm],
+ * w[nq], u and alpha [n*nm] solved in place; iters and status [n] may be NULL;
+ * unsolved cells report status -1) except opts (host). The kernel's scratch (work
+ * counter, failure and statistics counters, the chunked basis) lives in one static
+ * __device__ array of C3D_NOALLOC_SCRATCH_BYTES held by every GPU that loads the
+ * library until exit; sizes above nm = 64 or nq = 2048 are rejected with
+ * C3D_ERR_INVALID. The first call on a device looks up that array's device address
+ * (cudaGetSymbolAddress), so make that first call before any stream capture. All
+ * calls share the array: calls that overlap on the GPU race, so order them (one
+ * stream). Stream-ordered; returns without synchronising. */
+c3d_status c3d_closure_vectors_noalloc(int nm, int nq, const double *M, const double *w,
+                                       long long n, double *u, double *alpha, int *iters,
+                                       int *status, const c3d_closure_opts *opts, void *stream);
+
 /* Event timing on the context's stream around every closure and kinetic-flux
  * launch (off by default). c3d_timing_get returns the summed milliseconds
  * ms[0] closure, ms[1] kinetic flux and the launch counts since enabling. */
