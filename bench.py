@@ -63,7 +63,7 @@ CONFIGS = {
 MN_TOL = 1e-6
 
 
-def deck_for(cfg, threads=1, tol=MN_TOL, ic="gaussian_psi"):
+def deck_for(cfg, threads=1, tol=MN_TOL, ic="gaussian_psi", hessian="gaunt"):
     c = CONFIGS[cfg]
     kv = dict(SOLVER="mn", TFINAL="1", OUTDT="1000", OUTPUT_DATA="false",
               OUTPUT_OPT_STATS="false", OUTPUT_TIMINGS="false", NX=c["n"], NY=c["n"], NZ=c["n"],
@@ -72,7 +72,8 @@ def deck_for(cfg, threads=1, tol=MN_TOL, ic="gaussian_psi"):
               CROSS_SECTION=c["sigma_s"], INIT_FLOOR=c["floor"], GAUSS_SIGMA=c["sigma"],
               INIT_COND=ic, THETA=2.0, OMP_THREADS=threads, PN_USE_KINETIC_FLUX=0,
               MN_TOL=tol, MN_TOL_GAMMA=1.1, MN_COND_H_MAX=1e10, MN_MAX_ITER=100,
-              MN_BATCHED="true", MN_USE_GAUNT_COEF="false", MN_USE_GAUNT_SPARSE="false",
+              MN_BATCHED="true", MN_USE_GAUNT_COEF="true" if hessian == "gaunt" else "false",
+              MN_USE_GAUNT_SPARSE="true" if hessian == "gaunt" else "false",
               CUDA_KINETIC="true", CUDA_BATCHED="true", CUDA_BATCH_SIZE=50, REG_LADDER=LADDER)
     if "checker" in c:
         b, shi, ahi = c["checker"]
@@ -140,11 +141,16 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------ FLOP model
-def closure_flops(nm, nq, iters, trials):
-    """Algorithmic FP64 FLOPs of the dual solves: per Newton iteration the Hessian's lower
-    triangle nm(nm+1)/2 * nq FMAs (2 FLOP each), the exponent 2 nm nq and nq exps (counted
-    1 FLOP), Cholesky nm^3/3; per line-search trial 2 nm nq + 2 nq."""
-    per_iter = nm * (nm + 1) * nq + 2 * nm * nq + nq + nm ** 3 / 3.0
+def closure_flops(nm, nq, iters, trials, hessian="gaunt"):
+    """Algorithmic FP64 FLOPs of the dual solves. Per Newton iteration: the exponent
+    2 nm nq and nq exps (counted 1 FLOP each), the Hessian -- direct form: lower triangle
+    nm(nm+1)/2 nq FMAs; Gaunt form: the nm2 = (2N+1)^2 extended moments 2 nm2 nq (the
+    sparse beta contraction, ~1% of that, is not counted) -- and Cholesky nm^3/3. Per
+    line-search trial 2 nm nq + 2 nq."""
+    N = int(round(nm ** 0.5)) - 1
+    nm2 = (2 * N + 1) ** 2
+    hess = nm * (nm + 1) * nq if hessian == "direct" else 2 * nm2 * nq
+    per_iter = hess + 2 * nm * nq + nq + nm ** 3 / 3.0
     per_trial = 2 * nm * nq + 2 * nq
     return iters * per_iter + trials * per_trial
 
@@ -211,13 +217,13 @@ def _ref_sample_worker(conn, deck, u, a, reps):
     conn.close()
 
 
-def run_ref_sample(cfg, u, a, reps):
+def run_ref_sample(cfg, u, a, reps, hessian="gaunt"):
     import multiprocessing as mp
     threads = os.cpu_count() or 1
     c = CONFIGS[cfg]
     # a 4^3 deck with the workload's moment order, quadrature and MN options sets up the
     # reference's tables and globals; the sampled cells are solved by Optimization::opt
-    deck = deck_for(cfg, threads=threads, ic="gaussian").replace(f"NX {c['n']}", "NX 4").replace(
+    deck = deck_for(cfg, threads=threads, ic="gaussian", hessian=hessian).replace(f"NX {c['n']}", "NX 4").replace(
         f"NY {c['n']}", "NY 4").replace(f"NZ {c['n']}", "NZ 4")
     ctx = mp.get_context("spawn")
     r, w = ctx.Pipe(duplex=False)
@@ -248,11 +254,11 @@ def initial_cells_sample(cfg, count, seed=1234):
     return u, a
 
 
-def calibrated_ref_sample(cfg, u_all, a_all, target_s=12.0):
+def calibrated_ref_sample(cfg, u_all, a_all, target_s=12.0, hessian="gaunt"):
     """Times the reference closure on a sample sized for ~target_s seconds of CPU work."""
     threads = os.cpu_count() or 1
     n0 = min(len(u_all), 32 * threads)
-    probe = run_ref_sample(cfg, u_all[:n0], a_all[:n0], 1)
+    probe = run_ref_sample(cfg, u_all[:n0], a_all[:n0], 1, hessian)
     rate = n0 / max(probe["times"][0], 1e-6)
     n = int(min(len(u_all), max(n0, rate * target_s)))
     return n, rate
@@ -266,8 +272,10 @@ def reference_arm(args):
     c = CONFIGS[cfg]
     threads = os.cpu_count() or 1
     pool_u, pool_a = initial_cells_sample(cfg, 400000)
-    n, rate = calibrated_ref_sample(cfg, pool_u, pool_a, target_s=max(2.0, 60.0 / max(1, args.steps + args.warmup)))
-    res = run_ref_sample(cfg, pool_u[:n], pool_a[:n], args.warmup + args.steps)
+    n, rate = calibrated_ref_sample(cfg, pool_u, pool_a,
+                                    target_s=max(2.0, 60.0 / max(1, args.steps + args.warmup)),
+                                    hessian=args.hessian)
+    res = run_ref_sample(cfg, pool_u[:n], pool_a[:n], args.warmup + args.steps, args.hessian)
     times = res["times"][args.warmup:]
     step_s = float(np.mean(times))
     value = n / step_s
@@ -278,6 +286,7 @@ def reference_arm(args):
                 warmup=args.warmup, ms_per_step=step_s * 1e3, higher_is_better=True,
                 scaling="weak", vs_baseline=None, dtype="f64", data="synthetic", impl="reference",
                 config=dict(workload=c["desc"], config=cfg, mn_tol=MN_TOL, ladder=LADDER,
+                            hessian=args.hessian,
                             note="reference CPU closure only (no flux); cells/s of the sample"),
                 cpu_baseline=dict(value=value, unit=UNIT, cores=res["threads"], kind="reference",
                                   sample=sample),
@@ -312,7 +321,7 @@ def b200_arm(args):
     with tempfile.TemporaryDirectory() as tmp:
         deck = os.path.join(tmp, "input.deck")
         with open(deck, "w") as f:
-            f.write(deck_for(cfg, threads=os.cpu_count() or 1))
+            f.write(deck_for(cfg, threads=os.cpu_count() or 1, hessian=args.hessian))
         solver = c3d.Solver(deck, stream=ctypes.c_void_p(stream.cuda_stream))
     ctxh = solver.ctx_handle
     L = c3d.lib()
@@ -398,7 +407,7 @@ def b200_arm(args):
 
     if rank == 0:
         closure_launches = int(cnt[0])
-        flops = closure_flops(nm, nq, st.totalIters, st.trials)
+        flops = closure_flops(nm, nq, st.totalIters, st.trials, args.hessian)
         per_launch_s = ms[0] * 1e-3 / max(1, closure_launches)
         achieved = flops / max(1, closure_launches) / per_launch_s / 1e12
         roofline = dict(bound="tensor", pipe="fp64 (DMMA m8n8k4 + DFMA)", achieved=achieved,
@@ -406,7 +415,8 @@ def b200_arm(args):
                         traffic=profile_traffic("closure_fp64_m6_128"),
                         peak_source="in-run cuBLAS DGEMM 8192^3 via torch (FP64 is not in "
                                     "MEASURED_PEAKS.json)",
-                        kernel="closure_fp64_kernel<7,8>",
+                        kernel=("closure_gaunt_kernel<7,22,8>" if args.hessian == "gaunt"
+                                else "closure_fp64_kernel<7,8>"),
                         flops_per_launch=flops / max(1, closure_launches),
                         closure_ms_per_launch=ms[0] / max(1, closure_launches),
                         flux_ms_per_launch=ms[1] / max(1, int(cnt[1])),
@@ -419,8 +429,8 @@ def b200_arm(args):
             rng = np.random.default_rng(7)
             pick = rng.choice(uh.shape[0], size=min(uh.shape[0], 400000), replace=False)
             su, sa = uh[pick].copy(), ah[pick].copy()
-            n_s, _ = calibrated_ref_sample(cfg, su, sa, target_s=12.0)
-            res = run_ref_sample(cfg, su[:n_s], sa[:n_s], 1)
+            n_s, _ = calibrated_ref_sample(cfg, su, sa, target_s=12.0, hessian=args.hessian)
+            res = run_ref_sample(cfg, su[:n_s], sa[:n_s], 1, args.hessian)
             cpu = dict(value=n_s / res["times"][0], unit=UNIT, cores=res["threads"],
                        kind="reference",
                        sample=f"{n_s} cells sampled uniformly from the state after the timed "
@@ -434,6 +444,8 @@ def b200_arm(args):
             warmup=args.warmup, ms_per_step=max_ms / args.steps, higher_is_better=True,
             scaling="weak", vs_baseline=None, dtype="f64", data="synthetic",
             config=dict(workload=c["desc"], config=cfg, form="plain FP64 drop-in",
+                        hessian=("Gaunt sparse (MN_USE_GAUNT_COEF/SPARSE true, the reference "
+                                 "deck's default)" if args.hessian == "gaunt" else "direct"),
                         mn_tol=MN_TOL, mn_batched=True, ladder=LADDER,
                         cells_per_step=2 * cells, l2="inputs larger than L2 (u, alpha 0.9 GB each)",
                         parallelism=f"replicas x{world}"),
@@ -459,6 +471,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--config", default="c3", choices=sorted(CONFIGS))
+    ap.add_argument("--hessian", default="gaunt", choices=["gaunt", "direct"])
     args = ap.parse_args()
     if args.impl == "reference":
         reference_arm(args)

@@ -28,6 +28,7 @@ HEADER_SYMBOLS = [
     "c3d_step", "c3d_sync", "c3d_closure_records", "c3d_closure_stats_get",
     "c3d_closure_stats_reset", "c3d_closure_vectors", "c3d_build_quadrature",
     "c3d_launch_count", "c3d_timing_enable", "c3d_timing_get", "c3d_closure_vectors_noalloc",
+    "c3d_set_gaunt",
 ]
 
 
@@ -87,6 +88,7 @@ def lib():
         L.c3d_device_state.argtypes = [vp, ctypes.POINTER(vp), ctypes.POINTER(vp),
                                        ctypes.POINTER(vp)]
         L.c3d_build_quadrature.argtypes = [ctypes.c_int, ctypes.c_int] + [_dp] * 6
+        L.c3d_set_gaunt.argtypes = [vp, ctypes.c_int, _dp, _ip, _ip, _dp]
         L.c3d_timing_enable.argtypes = [vp, ctypes.c_int]
         L.c3d_timing_get.argtypes = [vp, _dp, ctypes.POINTER(ctypes.c_longlong)]
         L.c3d_launch_count.argtypes = [vp]
@@ -233,6 +235,18 @@ class Context:
 
     def launch_count(self):
         return lib().c3d_launch_count(self.h)
+
+    def set_gaunt(self, nm2, M2, row, col, val):
+        """Gaunt form of the Hessian (CSR of beta); None switches back to the direct form."""
+        if M2 is None:
+            check(lib().c3d_set_gaunt(self.h, nm2, None, None, None, None), "c3d_set_gaunt")
+            return
+        self._gaunt = [np.ascontiguousarray(M2, np.float64), np.ascontiguousarray(row, np.int32),
+                       np.ascontiguousarray(col, np.int32), np.ascontiguousarray(val, np.float64)]
+        g = self._gaunt
+        check(lib().c3d_set_gaunt(self.h, nm2, g[0].ctypes.data_as(_dp), g[1].ctypes.data_as(_ip),
+                                  g[2].ctypes.data_as(_ip), g[3].ctypes.data_as(_dp)),
+              "c3d_set_gaunt")
 
     def timing_enable(self, on=True):
         check(lib().c3d_timing_enable(self.h, int(on)), "timing")

@@ -26,6 +26,14 @@ struct ClosureLaunch {
 };
 cudaError_t launch_closure_fp64(const ClosureLaunch &L);
 int closure_fp64_nmp(int nm);
+struct GauntTables {
+    const double *chunks;
+    const int *row, *col;
+    const double *val;
+};
+cudaError_t launch_closure_gaunt(const ClosureLaunch &L, const GauntTables &G);
+bool closure_gaunt_supported(int nm);
+int closure_gaunt_nm2p(int nm2);
 cudaError_t launch_hessian_batch(int nm, int nchunks, const double *chunks, const double *alphas,
                                  long long n, double *hs, int *errorFlag, cudaStream_t st);
 cudaError_t launch_ghost_fill(const GridDims &g, double *u, int numSMs, cudaStream_t st);
@@ -110,6 +118,10 @@ struct c3d_ctx {
     int *iters = nullptr, *iterGamma = nullptr, *regIdx = nullptr, *status = nullptr;
     unsigned long long *counter = nullptr, *failCount = nullptr, *stats = nullptr;
     int *errorFlag = nullptr;
+    // Gaunt form of the Hessian (c3d_set_gaunt)
+    bool gaunt = false;
+    double *gChunks = nullptr, *gVal = nullptr;
+    int *gRow = nullptr, *gCol = nullptr;
     // optional event timing of the closure and flux launches (kind 0 closure, 1 flux)
     bool timing = false;
     std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> events;
@@ -145,7 +157,8 @@ static void free_ctx(c3d_ctx *c)
     void *ptrs[] = {c->u,     c->alpha,  c->uOld,     c->flux,    c->sigT,   c->sigS,
                     c->M,     c->w,      c->xi,       c->eta,     c->mu,     c->chunks,
                     c->pnops, c->psi,    c->iters,    c->iterGamma, c->regIdx, c->status,
-                    c->counter, c->failCount, c->stats, c->errorFlag};
+                    c->counter, c->failCount, c->stats, c->errorFlag, c->gChunks, c->gVal,
+                    c->gRow, c->gCol};
     for (void *p : ptrs)
         if (p)
             cudaFree(p);
@@ -379,7 +392,12 @@ static c3d_status run_closure(c3d_ctx *c, long long n, double *u, double *alpha,
     L.stream = c->stream;
     cudaEvent_t t0 = nullptr;
     timing_begin(c, &t0);
-    C3D_CUDA(launch_closure_fp64(L));
+    if (c->gaunt) {
+        GauntTables G{c->gChunks, c->gRow, c->gCol, c->gVal};
+        C3D_CUDA(launch_closure_gaunt(L, G));
+    } else {
+        C3D_CUDA(launch_closure_fp64(L));
+    }
     timing_end(c, 0, t0);
     c->launches += 2; // counter reset + closure kernel
     return C3D_OK;
@@ -392,6 +410,67 @@ c3d_status c3d_closure(c3d_ctx *c)
     if (c->solver != 1)
         return fail(C3D_ERR_INVALID, "c3d_closure: the closure belongs to the M_N solver");
     return run_closure(c, c->g.nall(), c->u, c->alpha, c->iters, c->iterGamma, c->regIdx, c->status);
+}
+
+c3d_status c3d_set_gaunt(c3d_ctx *c, int nm2, const double *M2, const int *rowPtr,
+                         const int *colInd, const double *val)
+{
+    if (!c)
+        return fail(C3D_ERR_INVALID, "c3d_set_gaunt: null context");
+    if (!M2 || !rowPtr || !colInd || !val) {
+        // back to the direct form
+        c->gaunt = false;
+        return C3D_OK;
+    }
+    const int nm = c->g.nm, nq = c->nq;
+    int n2 = (int)std::lround(std::sqrt((double)nm));
+    if (nm2 != (2 * n2 - 1) * (2 * n2 - 1))
+        return fail(C3D_ERR_INVALID, "c3d_set_gaunt: nm2 must be (2N+1)^2");
+    if (!closure_gaunt_supported(nm))
+        return fail(C3D_ERR_INVALID, "c3d_set_gaunt: the Gaunt form is provided for N <= 6");
+    const int nm2p = closure_gaunt_nm2p(nm2);
+    const int nch = ceil_div(nq, QC);
+    const size_t per = (size_t)(nm2p + 1) * QCP;
+    std::vector<double> ch((size_t)nch * per, 0.0), wh(nq);
+    C3D_CUDA(cudaMemcpy(wh.data(), c->w, nq * 8, cudaMemcpyDeviceToHost));
+    for (int k = 0; k < nch; ++k)
+        for (int qq = 0; qq < QC; ++qq) {
+            int q = k * QC + qq;
+            if (q >= nq)
+                break;
+            for (int r = 0; r < nm2; ++r)
+                ch[k * per + (size_t)r * QCP + qq] = M2[(size_t)q * nm2 + r];
+            ch[k * per + (size_t)nm2p * QCP + qq] = wh[q];
+        }
+    const int nnz = rowPtr[nm * nm];
+    double *dch = nullptr, *dval = nullptr;
+    int *drow = nullptr, *dcol = nullptr;
+    if (cudaMalloc(&dch, ch.size() * 8) != cudaSuccess ||
+        cudaMalloc(&drow, (size_t)(nm * nm + 1) * 4) != cudaSuccess ||
+        cudaMalloc(&dcol, (size_t)(nnz > 0 ? nnz : 1) * 4) != cudaSuccess ||
+        cudaMalloc(&dval, (size_t)(nnz > 0 ? nnz : 1) * 8) != cudaSuccess) {
+        cudaGetLastError();
+        if (dch) cudaFree(dch);
+        if (drow) cudaFree(drow);
+        if (dcol) cudaFree(dcol);
+        if (dval) cudaFree(dval);
+        return fail(C3D_ERR_OOM, "c3d_set_gaunt: device allocation failed");
+    }
+    cudaMemcpy(dch, ch.data(), ch.size() * 8, cudaMemcpyHostToDevice);
+    cudaMemcpy(drow, rowPtr, (size_t)(nm * nm + 1) * 4, cudaMemcpyHostToDevice);
+    cudaMemcpy(dcol, colInd, (size_t)nnz * 4, cudaMemcpyHostToDevice);
+    cudaMemcpy(dval, val, (size_t)nnz * 8, cudaMemcpyHostToDevice);
+    C3D_CUDA(cudaDeviceSynchronize());
+    if (c->gChunks) cudaFree(c->gChunks);
+    if (c->gRow) cudaFree(c->gRow);
+    if (c->gCol) cudaFree(c->gCol);
+    if (c->gVal) cudaFree(c->gVal);
+    c->gChunks = dch;
+    c->gRow = drow;
+    c->gCol = dcol;
+    c->gVal = dval;
+    c->gaunt = true;
+    return C3D_OK;
 }
 
 c3d_status c3d_closure_vectors(c3d_ctx *c, long long n, double *u, double *alpha, int *iters,

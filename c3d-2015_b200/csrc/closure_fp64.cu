@@ -50,9 +50,16 @@ struct SlotScalars {
     int need, iter, totalIter, iterGamma, regIndex, maxIter, status, exhausted;
 };
 
+// Largest moment count (N+1)^2 whose padding to 8 gives NT tiles.
+__host__ __device__ constexpr int max_nm_for(int nt)
+{
+    return nt == 1 ? 4 : nt == 2 ? 16 : nt == 4 ? 25 : nt == 5 ? 36 : nt == 7 ? 49 : 8 * nt;
+}
+
 template <int NT> struct Cfg {
     static constexpr int NMP = 8 * NT;
-    static constexpr int NPK = NMP * (NMP + 1) / 2;
+    static constexpr int NML = max_nm_for(NT);
+    static constexpr int NPK = NML * (NML + 1) / 2;
     static constexpr int ROWS = NMP + 1; // basis rows + weight row
     static constexpr int CHUNK = ROWS * QCP;
     static constexpr int NTILE = NT * (NT + 1) / 2;
@@ -541,14 +548,21 @@ __device__ void after_hessian(Slot<NT> &sl, const ClosureParams &P, const Output
     }
     f = __shfl_sync(FULL_MASK, f, 0);
     // 1-norm: max row sum of |H| (src/utils.cpp:35-49)
-    double rs = 0.0;
+    double rs = 0.0, gmin = 1.0 / 0.0;
     for (int i = lane; i < nm; i += 32) {
         double s = 0.0;
         for (int j = 0; j < nm; ++j)
             s += fabs(j <= i ? sl.L[pidx(i, j)] : sl.L[pidx(j, i)]);
         rs = fmax(rs, s);
+        gmin = fmin(gmin, 2.0 * sl.L[pidx(i, i)] - s); // Gershgorin: H_ii - sum_{j!=i} |H_ij|
     }
     double norm1 = warp_max(rs);
+    gmin = -warp_max(-gmin);
+    // All eigenvalues of H are >= gmin, so when gmin > 0, ||H^-1||_1 <= sqrt(n)/gmin and the
+    // 1-norm condition number is at most norm1 sqrt(n)/gmin. The Hager estimate can only be
+    // smaller, so if this bound is below condHMax/2 the reference's test `condest > condHMax`
+    // is false whatever the estimate; the estimate is then skipped.
+    bool condSure = gmin > 0.0 && norm1 * sqrt((double)nm) / gmin <= 0.5 * P.condHMax;
     __syncwarp();
     int info = warp_cholesky(sl, nm, lane);
     double cond = 0.0;
@@ -556,7 +570,8 @@ __device__ void after_hessian(Slot<NT> &sl, const ClosureParams &P, const Output
         for (int i = lane; i < nm; i += 32)
             sl.rinv[i] = 1.0 / sl.L[pidx(i, i)];
         __syncwarp();
-        cond = warp_condest(sl, nm, lane, norm1);
+        if (!condSure)
+            cond = warp_condest(sl, nm, lane, norm1);
     }
     __syncwarp();
 
@@ -812,6 +827,182 @@ __global__ void __launch_bounds__(W * 32, 1)
     }
 }
 
+// ---------------------------------------------------------------- Gaunt-form closure
+
+// The same per-cell Newton logic with H formed as in the reference's Gaunt modes
+// (src/opt/fobj.cpp:58-61, :75-95): extended moments mom_k = sum_q w_q e^{alpha.m_q} m2_qk
+// for the nm2 = (2N+1)^2 harmonics of degree <= 2N, then H_ij = sum_k beta_ijk mom_k over
+// the CSR table (|beta| > 1e-13 for the sparse mode, all nonzeros for the dense mode),
+// summed in the reference's order. Per chunk, each warp computes its cell's exponents
+// and writes the coefficients c_q = w_q e_q into a shared [q][cell] tile; then all warps
+// accumulate the moments of the CTA's W = 8 cells as one DMMA GEMM
+// (moments[k][cell] += M2^T[k][q] C[q][cell]) with the staged M2^T chunk as the shared
+// operand: ~7x fewer FLOPs than the direct lower triangle for M_6.
+constexpr int GSTAGES = 2;
+constexpr int CST = 12; // row stride of the coefficient tile (bank-conflict-free B fragments)
+
+template <int NT, int NT2, int W>
+__global__ void __launch_bounds__(W * 32, 1)
+    closure_gaunt_kernel(ClosureParams P, const double *__restrict__ chunks, long long ncells,
+                         unsigned long long *counter, Outputs O, int *errorFlag,
+                         const int *__restrict__ bRow, const int *__restrict__ bCol,
+                         const double *__restrict__ bVal)
+{
+    static_assert(W == 8, "the moment GEMM uses one 8-wide DMMA column tile of cells");
+    constexpr int NM2P = 8 * NT2;
+    constexpr int CH = (NM2P + 1) * QCP;
+    constexpr int RT = (NT2 + W - 1) / W;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    double *stage = reinterpret_cast<double *>(smem_raw);
+    Slot<NT> *slots = reinterpret_cast<Slot<NT> *>(stage + GSTAGES * CH);
+    double *mom = reinterpret_cast<double *>(slots + W); // W x NM2P
+    double *cbuf = mom + W * NM2P;                        // QC x CST
+    uint64_t *full = reinterpret_cast<uint64_t *>(cbuf + QC * CST);
+    __shared__ int s_abort;
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int nm = P.nm, nchunks = P.nchunks;
+    const uint32_t chunkBytes = CH * sizeof(double);
+    Slot<NT> &sl = slots[warp];
+    const double m0 = chunks[0];
+    const int npk = nm * (nm + 1) / 2;
+
+    if (tid == 0) {
+        for (int s = 0; s < GSTAGES; ++s)
+            mbar_init(&full[s], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        s_abort = 0;
+    }
+    if (lane == 0) {
+        sl.s.need = NEED_NONE;
+        sl.s.cell = -1;
+        sl.s.exhausted = 0;
+    }
+    __syncthreads();
+
+    uint32_t seq = 0;
+    for (;;) {
+        if (sl.s.need == NEED_NONE && !sl.s.exhausted) {
+            for (;;) {
+                unsigned long long c = 0;
+                if (lane == 0)
+                    c = atomicAdd(counter, 1ull);
+                c = __shfl_sync(FULL_MASK, c, 0);
+                if ((long long)c >= ncells) {
+                    if (lane == 0)
+                        sl.s.exhausted = 1;
+                    __syncwarp();
+                    break;
+                }
+                load_cell(sl, P, O, (long long)c, lane);
+                if (sl.s.need != NEED_NONE)
+                    break;
+            }
+        }
+        __syncwarp();
+        const int need = sl.s.need;
+        if (!__syncthreads_or(need != NEED_NONE))
+            break;
+        const bool anyH = __syncthreads_or(need == NEED_H);
+
+        double acc[RT][2];
+#pragma unroll
+        for (int r = 0; r < RT; ++r)
+            acc[r][0] = acc[r][1] = 0.0;
+        double fpart = 0.0;
+        if (tid == 0) {
+            for (int k = 0; k < GSTAGES && k < nchunks; ++k) {
+                uint32_t s = (seq + k) % GSTAGES;
+                mbar_expect_tx(&full[s], chunkBytes);
+                bulk_g2s(stage + s * CH, chunks + (size_t)k * CH, chunkBytes, &full[s]);
+            }
+        }
+        for (int k = 0; k < nchunks; ++k) {
+            uint32_t s = (seq + k) % GSTAGES;
+            uint32_t parity = ((seq + k) / GSTAGES) & 1u;
+            if (!mbar_wait(&full[s], parity))
+                s_abort = 1;
+            if (__syncthreads_or(s_abort)) {
+                if (tid == 0)
+                    atomicExch(errorFlag, 1);
+                return;
+            }
+            const double *ch = stage + s * CH;
+            double c = 0.0;
+            if (need != NEED_NONE) {
+                double z = 0.0;
+                for (int i = 0; i < nm; ++i)
+                    z = __dadd_rn(z, __dmul_rn(sl.alpha[i], ch[i * QCP + lane]));
+                c = ch[NM2P * QCP + lane] * exp(z);
+                if (need == NEED_TRIAL)
+                    fpart += c;
+            }
+            cbuf[lane * CST + warp] = (need == NEED_H) ? c : 0.0;
+            __syncthreads();
+            if (anyH) {
+#pragma unroll
+                for (int g = 0; g < QC / 4; ++g) {
+                    double b = cbuf[(4 * g + (lane & 3)) * CST + (lane >> 2)];
+#pragma unroll
+                    for (int r = 0; r < RT; ++r) {
+                        int rt = warp + r * W;
+                        if (rt < NT2) {
+                            double a = ch[(8 * rt + (lane >> 2)) * QCP + 4 * g + (lane & 3)];
+                            dmma(acc[r][0], acc[r][1], a, b);
+                        }
+                    }
+                }
+            }
+            __syncthreads();
+            if (tid == 0 && k + GSTAGES < nchunks) {
+                mbar_expect_tx(&full[s], chunkBytes);
+                bulk_g2s(stage + s * CH, chunks + (size_t)(k + GSTAGES) * CH, chunkBytes, &full[s]);
+            }
+        }
+        seq += nchunks;
+
+        if (anyH) {
+#pragma unroll
+            for (int r = 0; r < RT; ++r) {
+                int rt = warp + r * W;
+                if (rt < NT2) {
+                    int kk = 8 * rt + (lane >> 2), c0 = 2 * (lane & 3);
+                    mom[c0 * NM2P + kk] = acc[r][0];
+                    mom[(c0 + 1) * NM2P + kk] = acc[r][1];
+                }
+            }
+        }
+        __syncthreads();
+        if (need == NEED_H) {
+            // H_ij (i >= j) = sum over the CSR row of (j, i) of mom[col] * val, in CSR order
+            const double *mw = mom + warp * NM2P;
+            int ii = 0, jj = lane;
+            while (jj > ii) {
+                jj -= ii + 1;
+                ++ii;
+            }
+            for (int e = lane; e < npk; e += 32) {
+                int idx = jj * nm + ii;
+                double h = 0.0;
+                for (int t = bRow[idx]; t < bRow[idx + 1]; ++t)
+                    h = __dadd_rn(h, __dmul_rn(mw[bCol[t]], bVal[t]));
+                sl.L[e] = h;
+                jj += 32;
+                while (jj > ii) {
+                    jj -= ii + 1;
+                    ++ii;
+                }
+            }
+            __syncwarp();
+            after_hessian(sl, P, O, lane, m0);
+        } else if (need == NEED_TRIAL) {
+            double fq = warp_sum(fpart);
+            after_trial(sl, P, O, lane, fq);
+        }
+        __syncthreads();
+    }
+}
+
 // ---------------------------------------------------------------- batched Hessians
 
 // H_b = sum_q w_q exp(alpha_b . m_q) m_q m_q^T for a batch of multiplier vectors
@@ -955,6 +1146,59 @@ int closure_fp64_nmp(int nm)
     int nt = (nm + 7) / 8;
     return 8 * nt;
 }
+
+struct GauntTables {
+    const double *chunks; // (NM2P + 1) x QCP per chunk
+    const int *row, *col;
+    const double *val;
+};
+
+template <int NT, int NT2>
+static cudaError_t launch_gaunt_t(const ClosureLaunch &L, const GauntTables &G)
+{
+    constexpr int W = 8;
+    constexpr int NM2P = 8 * NT2;
+    size_t smem = GSTAGES * (size_t)(NM2P + 1) * QCP * sizeof(double) + W * sizeof(Slot<NT>) +
+                  (size_t)W * NM2P * sizeof(double) + (size_t)QC * CST * sizeof(double) +
+                  GSTAGES * sizeof(uint64_t);
+    auto kern = closure_gaunt_kernel<NT, NT2, W>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess)
+        return e;
+    Outputs O{L.u, L.alpha, L.iters, L.iterGamma, L.regIdx, L.status, L.failCount, L.stats};
+    long long maxCtas = (L.ncells + W - 1) / W;
+    int grid = L.numSMs;
+    if (maxCtas < grid)
+        grid = (int)maxCtas;
+    if (grid < 1)
+        grid = 1;
+    e = cudaMemsetAsync(L.counter, 0, sizeof(unsigned long long), L.stream);
+    if (e != cudaSuccess)
+        return e;
+    kern<<<grid, W * 32, smem, L.stream>>>(*L.P, G.chunks, L.ncells, L.counter, O, L.errorFlag,
+                                            G.row, G.col, G.val);
+    return cudaGetLastError();
+}
+
+// Moment counts with a Gaunt-form kernel (N <= 6).
+bool closure_gaunt_supported(int nm) { return nm == 1 || nm == 4 || nm == 9 || nm == 16 || nm == 25 || nm == 36 || nm == 49; }
+
+cudaError_t launch_closure_gaunt(const ClosureLaunch &L, const GauntTables &G)
+{
+    switch (L.P->nm) {
+    case 1: return launch_gaunt_t<1, 1>(L, G);
+    case 4: return launch_gaunt_t<1, 2>(L, G);
+    case 9: return launch_gaunt_t<2, 4>(L, G);
+    case 16: return launch_gaunt_t<2, 7>(L, G);
+    case 25: return launch_gaunt_t<4, 11>(L, G);
+    case 36: return launch_gaunt_t<5, 16>(L, G);
+    case 49: return launch_gaunt_t<7, 22>(L, G);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+// Rows of the Gaunt chunk (8 * ceil(nm2/8) harmonics + weights).
+int closure_gaunt_nm2p(int nm2) { return 8 * ((nm2 + 7) / 8); }
 
 template <int NT, int W>
 static cudaError_t launch_hessian_t(int nm, int nchunks, const double *chunks, const double *alphas,

@@ -224,15 +224,33 @@ void Solver::prepare(const Config &cfg)
         maxDt_ = c.cfl * 0.5 * std::min(std::min(dx_, dy_), dz_);
         alpha.clear();
     } else {
-        if (c.mnUseGaunt)
-            fprintf(stderr, "[c3d_b200] MN_USE_GAUNT_COEF: the B200 closure forms H by direct "
-                            "quadrature (same H up to rounding)\n");
         // initMn, src/init.cpp:260-274
         alpha.assign(nall * nm, 0.0);
         for (long long cell = 0; cell < nall; cell++)
             alpha[cell * nm] = sqrt(4.0 * M_PI) * log(u[cell * nm] / sqrt(4.0 * M_PI));
         maxDt_ = c.cfl * (2.0 / (2.0 + c.theta)) / (1.0 / dx_ + 1.0 / dy_ + 1.0 / dz_);
     }
+}
+
+void Solver::prepare_gaunt()
+{
+    // Gaunt coefficients by least squares over the quadrature (src/init.cpp:287-336)
+    const int N = cfg_.momentOrder, nm = nm_, nq = nq_;
+    const int nm2 = (2 * N + 1) * (2 * N + 1);
+    std::vector<double> w2(nq), xi2(nq), eta2(nq), mu2(nq), M1((size_t)nq * nm);
+    M2.assign((size_t)nq * nm2, 0.0);
+    c3d_build_quadrature(N, cfg_.quadOrder, w2.data(), xi2.data(), eta2.data(), mu2.data(),
+                         M1.data(), M2.data());
+    std::vector<double> beta((size_t)nm * nm * nm2);
+    c3d_gaunt_dense(nm, nm2, nq, M2.data(), beta.data());
+    double thr = cfg_.mnUseGauntSparse ? 1e-13 : 0.0;
+    int nnz = c3d_gaunt_csr_threshold(nm, nm2, beta.data(), thr, nullptr, nullptr, nullptr);
+    betaRow.assign((size_t)nm * nm + 1, 0);
+    betaCol.assign(nnz > 0 ? nnz : 1, 0);
+    betaVal.assign(nnz > 0 ? nnz : 1, 0.0);
+    c3d_gaunt_csr_threshold(nm, nm2, beta.data(), thr, betaVal.data(), betaCol.data(),
+                            betaRow.data());
+    nm2_ = nm2;
 }
 
 c3d_status Solver::init(const Config &cfg, void *stream)
@@ -242,6 +260,18 @@ c3d_status Solver::init(const Config &cfg, void *stream)
                               pnOps.empty() ? nullptr : pnOps.data(), stream, &ctx_);
     if (s != C3D_OK)
         return s;
+    if (cfg_.solver == "mn" && cfg_.mnUseGaunt) {
+        if (nm_ > 49) {
+            fprintf(stderr, "[c3d_b200] MN_USE_GAUNT_COEF: Gaunt form provided for N <= 6; the "
+                            "closure forms H by direct quadrature (same H up to rounding)\n");
+        } else {
+            prepare_gaunt();
+            s = c3d_set_gaunt(ctx_, nm2_, M2.data(), betaRow.data(), betaCol.data(),
+                              betaVal.data());
+            if (s != C3D_OK)
+                return s;
+        }
+    }
     return push();
 }
 

@@ -76,12 +76,16 @@ public:
 
     // host mirrors of the reference globals g_u, g_mnAlpha, g_sigmaT, g_sigmaS, g_m, g_w, ...
     std::vector<double> u, alpha, sigT, sigS, M, w, xi, eta, mu, pnOps;
+    // Gaunt form (MN_USE_GAUNT_COEF): g_m2 and the CSR of g_beta
+    std::vector<double> M2, betaVal;
+    std::vector<int> betaRow, betaCol;
 
 private:
     Config cfg_;
     c3d_ctx *ctx_ = nullptr;
     c3d_params params_{};
-    int nm_ = 0, nq_ = 0;
+    int nm_ = 0, nq_ = 0, nm2_ = 0;
+    void prepare_gaunt();
     double dx_ = 0, dy_ = 0, dz_ = 0, maxDt_ = 0;
 };
 

@@ -299,3 +299,26 @@ void c3d_gaunt_csr(int nm, int nm2, const double *beta, double *val, int *colInd
     }
     rowPtr[nm * nm] = ptr;
 }
+
+int c3d_gaunt_csr_threshold(int nm, int nm2, const double *beta, double threshold, double *val,
+                            int *colInd, int *rowPtr)
+{
+    int ptr = 0;
+    for (int idx = 0; idx < nm * nm; idx++) {
+        if (rowPtr)
+            rowPtr[idx] = ptr;
+        for (int k = 0; k < nm2; k++) {
+            double v = beta[idx * nm2 + k];
+            if (fabs(v) > threshold) {
+                if (val)
+                    val[ptr] = v;
+                if (colInd)
+                    colInd[ptr] = k;
+                ptr++;
+            }
+        }
+    }
+    if (rowPtr)
+        rowPtr[nm * nm] = ptr;
+    return ptr;
+}

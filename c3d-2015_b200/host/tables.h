@@ -54,6 +54,11 @@ int c3d_gaunt_dense(int nm, int nm2, int nq, const double *M2, double *beta);
  * rowPtr[nm*nm+1]; val/colInd sized by c3d_gaunt_dense's return value. */
 void c3d_gaunt_csr(int nm, int nm2, const double *beta, double *val, int *colInd, int *rowPtr);
 
+/* CSR of the entries with |beta| > threshold (threshold 0: every nonzero, the dense
+ * mode's terms). Returns nnz; val/colInd may be NULL to count only. */
+int c3d_gaunt_csr_threshold(int nm, int nm2, const double *beta, double threshold, double *val,
+                            int *colInd, int *rowPtr);
+
 #ifdef __cplusplus
 }
 #endif

@@ -146,6 +146,15 @@ c3d_status c3d_closure_records(c3d_ctx *ctx, int *iters, int *iterGamma, int *re
 c3d_status c3d_closure_stats_get(c3d_ctx *ctx, c3d_closure_stats *st);
 c3d_status c3d_closure_stats_reset(c3d_ctx *ctx);
 
+/* Switches the closure to the Gaunt form of the Hessian (MN_USE_GAUNT_COEF true,
+ * src/opt/fobj.cpp:58-95): extended moments over the harmonics of degree <= 2N, then
+ * H_ij = sum_k beta_ijk mom_k in CSR order. M2[nq*nm2] and the CSR table
+ * rowPtr[nm*nm+1], colInd[nnz], val[nnz] indexed by i*nm+j are host arrays (copied);
+ * keep |beta| > 1e-13 for MN_USE_GAUNT_SPARSE true (src/init.cpp:318-336), all nonzeros
+ * for the dense mode. NULL tables switch back to the direct form. N <= 6. */
+c3d_status c3d_set_gaunt(c3d_ctx *ctx, int nm2, const double *M2, const int *rowPtr,
+                         const int *colInd, const double *val);
+
 /* Standalone batched closure of n independent moment vectors (device
  * pointers u[n*nm], alpha[n*nm], solved in place; records may be NULL).
  * Uses the context's tables and MN options; grid state is untouched. */

@@ -247,3 +247,46 @@ def test_reference_entry_points(oracle):
     ghost = np.ones(fg.shape[:3], bool)
     ghost[inner] = False
     assert (fg[ghost] == 0).all()
+
+
+def _gaunt_csr(T, threshold):
+    nm, nm2 = T["nm"], T["nm2"]
+    beta = T["beta"].reshape(nm * nm, nm2)
+    row = [0]
+    col, val = [], []
+    for idx in range(nm * nm):
+        nz = np.nonzero(np.abs(beta[idx]) > threshold)[0]
+        col.extend(nz.tolist())
+        val.extend(beta[idx, nz].tolist())
+        row.append(len(col))
+    return np.array(row, np.int32), np.array(col, np.int32), np.array(val)
+
+
+@pytest.mark.parametrize("mode", [2, 1])
+@pytest.mark.parametrize("N,Q", [(2, 12), (4, 12)])
+def test_gaunt_closure_matches_oracle(oracle, mode, N, Q):
+    """Gaunt-form Hessian (MN_USE_GAUNT_COEF true): sparse (|beta| > 1e-13) and dense."""
+    S = _setup(oracle, N=N, Q=Q, steps_before=2)
+    T = oracle.tables(N, Q, gaunt=True)
+    S["T"] = T
+    ctx = _ctx(S)
+    row, col, val = _gaunt_csr(T, 1e-13 if mode == 2 else 0.0)
+    ctx.set_gaunt(T["nm2"], T["M2"], row, col, val)
+    ctx.set_state(u=S["u"], alpha=S["alpha"], sig_t=S["sig"], sig_s=S["sig"])
+    ctx.closure()
+    ctx.sync()
+    ug, ag = ctx.get_state()
+    rec = ctx.records()
+    nm = S["nm"]
+    uo = S["u"].reshape(-1, nm).copy()
+    ao = S["alpha"].reshape(-1, nm).copy()
+    out = oracle.closure(make_opts(nm, S["nq"], nm2=T["nm2"], hess_mode=mode), T, uo, ao)
+    assert (rec["status"] == 0).all()
+    ties = tie_cells(out)
+    mism = rec["iters"] != out["totalIter"]
+    assert not (mism & ~ties).any(), np.nonzero(mism & ~ties)[0][:10]
+    ok = ~ties & (rec["regIndex"] == out["regIndex"])
+    ag = ag.reshape(-1, nm)
+    rel = np.linalg.norm(ag[ok] - ao[ok], axis=1) / np.linalg.norm(ao[ok], axis=1)
+    assert rel.max() < 1e-10, rel.max()
+    assert (out["totalIter"] > 1).sum() > 100

@@ -117,17 +117,24 @@ def test_pn_steps_bit_exact(oracle, kinetic):
     assert np.array_equal(u, ref["u"])
 
 
-@pytest.mark.parametrize("batched,ladder", [(True, None), (False, None), (True, BASELINE_LADDER)])
-def test_closure_steps_vs_reference(oracle, batched, ladder):
+@pytest.mark.parametrize("batched,ladder,gaunt", [(True, None, 0), (False, None, 0),
+                                                   (True, BASELINE_LADDER, 0), (True, None, 2),
+                                                   (True, None, 1)])
+def test_closure_steps_vs_reference(oracle, batched, ladder, gaunt):
+    """gaunt: 0 direct H, 1 dense Gaunt, 2 sparse Gaunt (MN_USE_GAUNT_COEF/_SPARSE)."""
     deck = deck_text(NX=8, NY=8, NZ=8, MOMENT_ORDER=2, QUAD_ORDER=12,
-                     MN_BATCHED="true" if batched else "false")
+                     MN_BATCHED="true" if batched else "false",
+                     MN_USE_GAUNT_COEF="true" if gaunt else "false",
+                     MN_USE_GAUNT_SPARSE="true" if gaunt == 2 else "false",
+                     # the reference exhausts its ladder in the Gaunt modes at 1e-8 here
+                     MN_TOL="1e-6" if gaunt else "1e-8")
     nsteps = 3
     ref = run_reference(deck, nsteps=nsteps, ladder=ladder, want=("snapshots",))
-    T = oracle.tables(2, 12)
+    T = oracle.tables(2, 12, gaunt=bool(gaunt))
     g = _grid(oracle, ref)
     iv, dv = ref["iv"], ref["dv"]
-    opts = make_opts(g.nm, g.nq, batched=batched, max_iter=iv[11], tol=dv[5], tol_gamma=dv[6],
-                     cond_h_max=dv[7], ladder=ladder)
+    opts = make_opts(g.nm, g.nq, nm2=25, batched=batched, max_iter=iv[11], tol=dv[5],
+                     tol_gamma=dv[6], cond_h_max=dv[7], ladder=ladder, hess_mode=gaunt)
     nall = (g.nx + 4) * (g.ny + 4) * (g.nz + 4)
     exact_steps = 0
     total_mism = 0
