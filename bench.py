@@ -325,6 +325,7 @@ def b200_arm(args):
         solver = c3d.Solver(deck, stream=ctypes.c_void_p(stream.cuda_stream))
     ctxh = solver.ctx_handle
     L = c3d.lib()
+    c3d.check(L.c3d_set_engine(ctxh, 0 if args.engine == "rounds" else 1), "engine")
     dt = solver.max_dt
     nm, nq = solver.nm, solver.nq
 
@@ -415,8 +416,13 @@ def b200_arm(args):
                         traffic=profile_traffic("closure_fp64_m6_128"),
                         peak_source="in-run cuBLAS DGEMM 8192^3 via torch (FP64 is not in "
                                     "MEASURED_PEAKS.json)",
-                        kernel=("closure_gaunt_kernel<7,22,8>" if args.hessian == "gaunt"
-                                else "closure_fp64_kernel<7,8>"),
+                        kernel=(("closure work-list rounds: rounds_pass_gaunt_kernel<7,22> + "
+                                 "rounds_newton_kernel" if args.hessian == "gaunt" else
+                                 "closure work-list rounds: rounds_pass_direct_kernel<7> + "
+                                 "rounds_newton_kernel") if args.engine == "rounds" else
+                                ("closure_gaunt_kernel<7,22,8>" if args.hessian == "gaunt"
+                                 else "closure_fp64_kernel<7,8>")),
+                        unit_of_launch="one c3d_closure call (all its kernels)",
                         flops_per_launch=flops / max(1, closure_launches),
                         closure_ms_per_launch=ms[0] / max(1, closure_launches),
                         flux_ms_per_launch=ms[1] / max(1, int(cnt[1])),
@@ -446,6 +452,7 @@ def b200_arm(args):
             config=dict(workload=c["desc"], config=cfg, form="plain FP64 drop-in",
                         hessian=("Gaunt sparse (MN_USE_GAUNT_COEF/SPARSE true, the reference "
                                  "deck's default)" if args.hessian == "gaunt" else "direct"),
+                        engine=args.engine,
                         mn_tol=MN_TOL, mn_batched=True, ladder=LADDER,
                         cells_per_step=2 * cells, l2="inputs larger than L2 (u, alpha 0.9 GB each)",
                         parallelism=f"replicas x{world}"),
@@ -456,7 +463,9 @@ def b200_arm(args):
             latency_ms=dict(p50=float(np.percentile(step_ms, 50)),
                             p99=float(np.percentile(step_ms, 99)), unit="ms per RK2 step"),
             iter_histogram=hist, newton_iters_per_solve=st.totalIters / max(1, st.cells),
-            failed_cells_timed=int(st.failed), syncs_with_failed_cells=failed[0])
+            failed_cells_timed=int(st.failed), syncs_with_failed_cells=failed[0],
+            closure_phase_clocks=dict(refill=st.clkRefill, passes=st.clkPass,
+                                      newton_logic=st.clkSerial, n_passes=st.passes))
         print(json.dumps(line), flush=True)
     solver.close()
     if world > 1:
@@ -472,6 +481,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--config", default="c3", choices=sorted(CONFIGS))
     ap.add_argument("--hessian", default="gaunt", choices=["gaunt", "direct"])
+    ap.add_argument("--engine", default="rounds", choices=["rounds", "persistent"])
     args = ap.parse_args()
     if args.impl == "reference":
         reference_arm(args)

@@ -28,7 +28,7 @@ HEADER_SYMBOLS = [
     "c3d_step", "c3d_sync", "c3d_closure_records", "c3d_closure_stats_get",
     "c3d_closure_stats_reset", "c3d_closure_vectors", "c3d_build_quadrature",
     "c3d_launch_count", "c3d_timing_enable", "c3d_timing_get", "c3d_closure_vectors_noalloc",
-    "c3d_set_gaunt",
+    "c3d_set_gaunt", "c3d_set_engine",
 ]
 
 
@@ -52,6 +52,8 @@ class ClosureStats(ctypes.Structure):
                 ("totalIters", ctypes.c_longlong), ("maxIter", ctypes.c_int),
                 ("maxIterGamma", ctypes.c_int), ("totalIterGamma", ctypes.c_longlong),
                 ("failed", ctypes.c_longlong), ("trials", ctypes.c_longlong),
+                ("clkRefill", ctypes.c_longlong), ("clkPass", ctypes.c_longlong),
+                ("clkSerial", ctypes.c_longlong), ("passes", ctypes.c_longlong),
                 ("regHist", ctypes.c_longlong * 16),
                 ("iterHist", ctypes.c_longlong * 64)]
 
@@ -89,6 +91,7 @@ def lib():
                                        ctypes.POINTER(vp)]
         L.c3d_build_quadrature.argtypes = [ctypes.c_int, ctypes.c_int] + [_dp] * 6
         L.c3d_set_gaunt.argtypes = [vp, ctypes.c_int, _dp, _ip, _ip, _dp]
+        L.c3d_set_engine.argtypes = [vp, ctypes.c_int]
         L.c3d_timing_enable.argtypes = [vp, ctypes.c_int]
         L.c3d_timing_get.argtypes = [vp, _dp, ctypes.POINTER(ctypes.c_longlong)]
         L.c3d_launch_count.argtypes = [vp]
@@ -235,6 +238,10 @@ class Context:
 
     def launch_count(self):
         return lib().c3d_launch_count(self.h)
+
+    def set_engine(self, engine):
+        """0: work-list rounds (default), 1: persistent kernel."""
+        check(lib().c3d_set_engine(self.h, engine), "c3d_set_engine")
 
     def set_gaunt(self, nm2, M2, row, col, val):
         """Gaunt form of the Hessian (CSR of beta); None switches back to the direct form."""

@@ -32,6 +32,30 @@ struct GauntTables {
     const double *val;
 };
 cudaError_t launch_closure_gaunt(const ClosureLaunch &L, const GauntTables &G);
+struct RoundsLaunch {
+    const ClosureParams *P;
+    const double *chunks;
+    const int *bRow, *bCol;
+    const double *bVal;
+    double m0;
+    long long ncells;
+    double *u, *alpha;
+    int *iters, *iterGamma, *regIdx, *status;
+    unsigned long long *failCount, *stats;
+    void *state;
+    int *listA, *listB;
+    unsigned int *counts;
+    unsigned int *hostCount;
+    double *buf;
+    long long batch;
+    int *errorFlag;
+    cudaStream_t stream;
+    long long *launches;
+    long long maxRounds;
+};
+cudaError_t launch_closure_rounds(const RoundsLaunch &R, bool gaunt);
+size_t rounds_state_bytes(int nm);
+size_t rounds_buf_doubles(int nm, int nm2, bool gaunt);
 bool closure_gaunt_supported(int nm);
 int closure_gaunt_nm2p(int nm2);
 cudaError_t launch_hessian_batch(int nm, int nchunks, const double *chunks, const double *alphas,
@@ -118,6 +142,16 @@ struct c3d_ctx {
     int *iters = nullptr, *iterGamma = nullptr, *regIdx = nullptr, *status = nullptr;
     unsigned long long *counter = nullptr, *failCount = nullptr, *stats = nullptr;
     int *errorFlag = nullptr;
+    double m0 = 0.0; // M[0][0]
+    int engine = 0;  // 0: work-list rounds, 1: persistent kernels
+    // work-list buffers (sized on first use)
+    void *rState = nullptr;
+    int *rListA = nullptr, *rListB = nullptr;
+    unsigned int *rCounts = nullptr, *rHostCount = nullptr;
+    double *rBuf = nullptr;
+    long long rCells = 0, rBatch = 0;
+    size_t rBufPer = 0;
+    int nm2 = 0;
     // Gaunt form of the Hessian (c3d_set_gaunt)
     bool gaunt = false;
     double *gChunks = nullptr, *gVal = nullptr;
@@ -158,11 +192,13 @@ static void free_ctx(c3d_ctx *c)
                     c->M,     c->w,      c->xi,       c->eta,     c->mu,     c->chunks,
                     c->pnops, c->psi,    c->iters,    c->iterGamma, c->regIdx, c->status,
                     c->counter, c->failCount, c->stats, c->errorFlag, c->gChunks, c->gVal,
-                    c->gRow, c->gCol};
+                    c->gRow, c->gCol, c->rState, c->rListA, c->rListB, c->rCounts, c->rBuf};
     for (void *p : ptrs)
         if (p)
             cudaFree(p);
     timing_clear(c);
+    if (c->rHostCount)
+        cudaFreeHost(c->rHostCount);
     if (c->ownStream && c->stream)
         cudaStreamDestroy(c->stream);
     delete c;
@@ -225,6 +261,7 @@ c3d_status c3d_create(const c3d_params *p, const double *M, const double *w, con
     cp.tol = p->mnTol;
     cp.tolGamma = p->mnBatched ? p->mnTolGamma : 1.1;
     cp.condHMax = p->mnCondHMax;
+    c->m0 = M[0];
     for (int i = 0; i < p->nreg; ++i)
         cp.reg[i] = p->reg[i];
     cp.passBudget = 1LL << 40;
@@ -371,9 +408,78 @@ c3d_status c3d_ghost_fill(c3d_ctx *c)
     return C3D_OK;
 }
 
+// Work-list buffers for n cells (grown on demand).
+static c3d_status ensure_rounds(c3d_ctx *c, long long n)
+{
+    size_t per = rounds_buf_doubles(c->g.nm, c->nm2, c->gaunt);
+    long long batch = n < (1LL << 20) ? n : (1LL << 20);
+    if (n <= c->rCells && per <= c->rBufPer && batch <= c->rBatch)
+        return C3D_OK;
+    void *ptrs[] = {c->rState, c->rListA, c->rListB, c->rCounts, c->rBuf};
+    for (void *p : ptrs)
+        if (p)
+            cudaFree(p);
+    c->rState = nullptr;
+    c->rListA = c->rListB = nullptr;
+    c->rCounts = nullptr;
+    c->rBuf = nullptr;
+    c->rCells = c->rBatch = 0;
+    C3D_CUDA(cudaMalloc(&c->rState, (size_t)n * rounds_state_bytes(c->g.nm)));
+    C3D_CUDA(cudaMalloc(&c->rListA, (size_t)n * sizeof(int)));
+    C3D_CUDA(cudaMalloc(&c->rListB, (size_t)n * sizeof(int)));
+    C3D_CUDA(cudaMalloc(&c->rCounts, 4 * sizeof(unsigned int)));
+    C3D_CUDA(cudaMalloc(&c->rBuf, (size_t)batch * per * sizeof(double)));
+    if (!c->rHostCount)
+        C3D_CUDA(cudaMallocHost(&c->rHostCount, sizeof(unsigned int)));
+    c->rCells = n;
+    c->rBatch = batch;
+    c->rBufPer = per;
+    return C3D_OK;
+}
+
 static c3d_status run_closure(c3d_ctx *c, long long n, double *u, double *alpha, int *iters,
                               int *iterGamma, int *regIdx, int *status)
 {
+    if (c->engine == 0) {
+        c3d_status s = ensure_rounds(c, n);
+        if (s != C3D_OK)
+            return s;
+        RoundsLaunch R{};
+        R.P = &c->cp;
+        R.chunks = c->gaunt ? c->gChunks : c->chunks;
+        R.bRow = c->gRow;
+        R.bCol = c->gCol;
+        R.bVal = c->gVal;
+        R.m0 = c->m0;
+        R.ncells = n;
+        R.u = u;
+        R.alpha = alpha;
+        R.iters = iters;
+        R.iterGamma = iterGamma;
+        R.regIdx = regIdx;
+        R.status = status;
+        R.failCount = c->failCount;
+        R.stats = c->stats;
+        R.state = c->rState;
+        R.listA = c->rListA;
+        R.listB = c->rListB;
+        R.counts = c->rCounts;
+        R.hostCount = c->rHostCount;
+        R.buf = c->rBuf;
+        R.batch = c->rBatch;
+        R.errorFlag = c->errorFlag;
+        R.stream = c->stream;
+        R.launches = &c->launches;
+        R.maxRounds = 1LL << 24;
+        cudaEvent_t t0 = nullptr;
+        timing_begin(c, &t0);
+        cudaError_t e = launch_closure_rounds(R, c->gaunt);
+        timing_end(c, 0, t0);
+        if (e == cudaErrorLaunchTimeout)
+            return fail(C3D_ERR_TIMEOUT, "closure: round limit exceeded");
+        C3D_CUDA(e);
+        return C3D_OK;
+    }
     ClosureLaunch L{};
     L.P = &c->cp;
     L.chunks = c->chunks;
@@ -470,6 +576,15 @@ c3d_status c3d_set_gaunt(c3d_ctx *c, int nm2, const double *M2, const int *rowPt
     c->gCol = dcol;
     c->gVal = dval;
     c->gaunt = true;
+    c->nm2 = nm2;
+    return C3D_OK;
+}
+
+c3d_status c3d_set_engine(c3d_ctx *c, int engine)
+{
+    if (!c || engine < 0 || engine > 1)
+        return fail(C3D_ERR_INVALID, "c3d_set_engine: engine must be 0 (work list) or 1 (persistent)");
+    c->engine = engine;
     return C3D_OK;
 }
 
@@ -604,6 +719,10 @@ c3d_status c3d_closure_stats_get(c3d_ctx *c, c3d_closure_stats *st)
     st->maxIterGamma = (int)h[STAT_MAX_ITER_GAMMA];
     st->failed = (long long)h[STAT_FAILED];
     st->trials = (long long)h[STAT_TRIALS];
+    st->clkRefill = (long long)h[STAT_CLK_REFILL];
+    st->clkPass = (long long)h[STAT_CLK_PASS];
+    st->clkSerial = (long long)h[STAT_CLK_SERIAL];
+    st->passes = (long long)h[STAT_PASSES];
     for (int i = 0; i < 16; ++i)
         st->regHist[i] = (long long)h[STAT_REG_HIST + i];
     for (int i = 0; i < 64; ++i)

@@ -32,6 +32,10 @@ enum StatSlot : int {
     STAT_FAILED = 5,
     STAT_TRIALS = 6,     // line-search trial passes
     STAT_REG_HIST = 8,   // 16 bins
+    STAT_CLK_REFILL = 24, // SM clocks summed over warps: queue refill + cell set-up
+    STAT_CLK_PASS = 25,   // passes over the staged basis
+    STAT_CLK_SERIAL = 26, // per-cell Newton logic after each pass
+    STAT_PASSES = 27,     // passes (per CTA)
     STAT_ITER_HIST = 32, // 64 bins (last: >= 63)
     STAT_COUNT = 96,
 };

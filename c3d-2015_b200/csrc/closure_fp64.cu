@@ -27,660 +27,12 @@
 //   (packed lower triangle) with warp shuffles.
 #include "c3d_common.cuh"
 
-#include <cfloat>
 #include <cstdio>
 
-#ifndef M_PI
-#define M_PI 3.14159265358979323846
-#endif
+#include "closure_core.cuh"
 
 namespace c3d {
 
-namespace {
-
-constexpr int STAGES = 3;
-constexpr double EPS_HALF = DBL_EPSILON / 2;
-
-enum Need : int { NEED_NONE = 0, NEED_H = 1, NEED_TRIAL = 2 };
-
-struct SlotScalars {
-    long long cell;
-    long long passes;
-    double u0, alphaScale, rtol, f, t, maxFactor, gd, fquad, r, gamma, err;
-    int need, iter, totalIter, iterGamma, regIndex, maxIter, status, exhausted;
-};
-
-// Largest moment count (N+1)^2 whose padding to 8 gives NT tiles.
-__host__ __device__ constexpr int max_nm_for(int nt)
-{
-    return nt == 1 ? 4 : nt == 2 ? 16 : nt == 4 ? 25 : nt == 5 ? 36 : nt == 7 ? 49 : 8 * nt;
-}
-
-template <int NT> struct Cfg {
-    static constexpr int NMP = 8 * NT;
-    static constexpr int NML = max_nm_for(NT);
-    static constexpr int NPK = NML * (NML + 1) / 2;
-    static constexpr int ROWS = NMP + 1; // basis rows + weight row
-    static constexpr int CHUNK = ROWS * QCP;
-    static constexpr int NTILE = NT * (NT + 1) / 2;
-};
-
-template <int NT> struct Slot {
-    static constexpr int NMP = Cfg<NT>::NMP;
-    double u[NMP], alpha[NMP], alpha0[NMP], uOrig[NMP], g[NMP], d[NMP], alphaOld[NMP], rinv[NMP];
-    double L[Cfg<NT>::NPK];
-    SlotScalars s;
-};
-
-__device__ __forceinline__ int pidx(int i, int j) { return (i * (i + 1)) / 2 + j; }
-
-__device__ __forceinline__ double warp_sum(double v)
-{
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1)
-        v += __shfl_xor_sync(FULL_MASK, v, o);
-    return v;
-}
-
-__device__ __forceinline__ double warp_max(double v)
-{
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1)
-        v = fmax(v, __shfl_xor_sync(FULL_MASK, v, o));
-    return v;
-}
-
-// First index of the largest |x| (LAPACK idamax semantics).
-__device__ __forceinline__ int warp_iamax(double a0, double a1, int lane, int n)
-{
-    double best = (lane < n) ? fabs(a0) : -1.0;
-    int bi = lane;
-    if (lane + 32 < n) {
-        double b = fabs(a1);
-        if (b > best) {
-            best = b;
-            bi = lane + 32;
-        }
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        double ob = __shfl_xor_sync(FULL_MASK, best, o);
-        int oi = __shfl_xor_sync(FULL_MASK, bi, o);
-        if (ob > best || (ob == best && oi < bi)) {
-            best = ob;
-            bi = oi;
-        }
-    }
-    return bi;
-}
-
-__device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b)
-{
-    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-                 : "+d"(d0), "+d"(d1)
-                 : "d"(a), "d"(b));
-}
-
-// ---------------------------------------------------------------- mbarrier / bulk copy
-
-__device__ __forceinline__ uint32_t smem_u32(const void *p)
-{
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count));
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)),
-                 "r"(bytes)
-                 : "memory");
-}
-
-// Returns false if the phase did not complete within the iteration limit.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
-{
-    uint32_t addr = smem_u32(bar);
-    for (int it = 0; it < (1 << 26); ++it) {
-        uint32_t done;
-        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-                     " selp.u32 %0, 1, 0, p;\n}\n"
-                     : "=r"(done)
-                     : "r"(addr), "r"(parity)
-                     : "memory");
-        if (done)
-            return true;
-    }
-    return false;
-}
-
-__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
-{
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
-                     smem_u32(dst)),
-                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
-                 : "memory");
-}
-
-// ---------------------------------------------------------------- per-warp linear algebra
-
-// In-place right-looking Cholesky of the packed lower triangle; returns LAPACK info.
-template <int NT>
-__device__ int warp_cholesky(Slot<NT> &sl, int n, int lane)
-{
-    double *P = sl.L;
-    for (int j = 0; j < n; ++j) {
-        double ajj = P[pidx(j, j)];
-        if (!(ajj > 0.0))
-            return j + 1;
-        double ljj = sqrt(ajj);
-        double r = 1.0 / ljj;
-        __syncwarp();
-        if (lane == 0)
-            P[pidx(j, j)] = ljj;
-        for (int i = j + 1 + lane; i < n; i += 32)
-            P[pidx(i, j)] *= r;
-        __syncwarp();
-        // trailing update P(i,k) -= L(i,j) L(k,j), j < k <= i < n, flattened over the warp
-        int m = n - j - 1;
-        int total = m * (m + 1) / 2;
-        int ii = 0, kk = lane;
-        while (kk > ii) { // locate element number `lane` in row-major triangle order
-            kk -= ii + 1;
-            ++ii;
-        }
-        for (int e = lane; e < total; e += 32) {
-            int i = j + 1 + ii, k = j + 1 + kk;
-            P[pidx(i, k)] = fma(-P[pidx(i, j)], P[pidx(k, j)], P[pidx(i, k)]);
-            kk += 32;
-            while (kk > ii) {
-                kk -= ii + 1;
-                ++ii;
-            }
-        }
-        __syncwarp();
-    }
-    return 0;
-}
-
-// x <- (L L^T)^{-1} x, x distributed as x0 = x[lane], x1 = x[lane+32]; column-oriented
-// substitution (the order of the reference BLAS dtrsv and of src/utils.cpp:71-86).
-// exactDiv selects division by L_kk (as the reference's own dpotrs) instead of the
-// precomputed reciprocal.
-template <int NT>
-__device__ void warp_apply_inverse(const Slot<NT> &sl, int n, int lane, double &x0, double &x1,
-                                   bool exactDiv)
-{
-    const double *P = sl.L;
-    for (int k = 0; k < n; ++k) {
-        double v = (k < 32) ? x0 : x1;
-        double xk = __shfl_sync(FULL_MASK, v, k & 31);
-        xk = exactDiv ? xk / P[pidx(k, k)] : xk * sl.rinv[k];
-        if (lane == (k & 31)) {
-            if (k < 32)
-                x0 = xk;
-            else
-                x1 = xk;
-        }
-        if (lane > k && lane < n)
-            x0 = fma(-P[pidx(lane, k)], xk, x0);
-        if (lane + 32 > k && lane + 32 < n)
-            x1 = fma(-P[pidx(lane + 32, k)], xk, x1);
-    }
-    for (int k = n - 1; k >= 0; --k) {
-        double v = (k < 32) ? x0 : x1;
-        double xk = __shfl_sync(FULL_MASK, v, k & 31);
-        xk = exactDiv ? xk / P[pidx(k, k)] : xk * sl.rinv[k];
-        if (lane == (k & 31)) {
-            if (k < 32)
-                x0 = xk;
-            else
-                x1 = xk;
-        }
-        if (lane < k && lane < n)
-            x0 = fma(-P[pidx(k, lane)], xk, x0);
-        if (lane + 32 < k && lane + 32 < n)
-            x1 = fma(-P[pidx(k, lane + 32)], xk, x1);
-    }
-}
-
-__device__ __forceinline__ double vsum_abs(double x0, double x1, int lane, int n)
-{
-    double s = (lane < n ? fabs(x0) : 0.0) + (lane + 32 < n ? fabs(x1) : 0.0);
-    return warp_sum(s);
-}
-
-// Hager/Higham 1-norm estimate of (L L^T)^{-1} (N. J. Higham, ACM TOMS 14 (1988)
-// 381-396, Alg. 4.1 -- the algorithm of LAPACK's dlacn2 as driven by dpocon).
-// Returns 1/rcond with rcond = (1/est)/anorm.
-template <int NT>
-__device__ double warp_condest(const Slot<NT> &sl, int n, int lane, double anorm)
-{
-    if (anorm == 0.0)
-        return 1.0 / 0.0;
-    double x0 = 1.0 / (double)n, x1 = 1.0 / (double)n;
-    warp_apply_inverse(sl, n, lane, x0, x1, false);
-    double est;
-    if (n == 1) {
-        est = fabs(__shfl_sync(FULL_MASK, x0, 0));
-    } else {
-        est = vsum_abs(x0, x1, lane, n);
-        int s0 = x0 >= 0.0 ? 1 : -1, s1 = x1 >= 0.0 ? 1 : -1;
-        x0 = (double)s0;
-        x1 = (double)s1;
-        warp_apply_inverse(sl, n, lane, x0, x1, false);
-        int j = warp_iamax(x0, x1, lane, n);
-        int iter = 2;
-        for (;;) {
-            x0 = (lane == j) ? 1.0 : 0.0;
-            x1 = (lane + 32 == j) ? 1.0 : 0.0;
-            warp_apply_inverse(sl, n, lane, x0, x1, false);
-            double estold = est;
-            est = vsum_abs(x0, x1, lane, n);
-            bool diff = (lane < n && (x0 >= 0.0 ? 1 : -1) != s0) ||
-                        (lane + 32 < n && (x1 >= 0.0 ? 1 : -1) != s1);
-            bool same = !__any_sync(FULL_MASK, diff);
-            if (same || est <= estold)
-                break;
-            s0 = x0 >= 0.0 ? 1 : -1;
-            s1 = x1 >= 0.0 ? 1 : -1;
-            x0 = (double)s0;
-            x1 = (double)s1;
-            warp_apply_inverse(sl, n, lane, x0, x1, false);
-            int jlast = j;
-            j = warp_iamax(x0, x1, lane, n);
-            double xjl = __shfl_sync(FULL_MASK, jlast < 32 ? x0 : x1, jlast & 31);
-            double xj = fabs(__shfl_sync(FULL_MASK, j < 32 ? x0 : x1, j & 31));
-            if (xjl != xj && iter < 5) {
-                ++iter;
-                continue;
-            }
-            break;
-        }
-        x0 = ((lane & 1) ? -1.0 : 1.0) * (1.0 + (double)lane / (double)(n - 1));
-        x1 = (((lane + 32) & 1) ? -1.0 : 1.0) * (1.0 + (double)(lane + 32) / (double)(n - 1));
-        warp_apply_inverse(sl, n, lane, x0, x1, false);
-        double temp = 2.0 * (vsum_abs(x0, x1, lane, n) / (double)(3 * n));
-        if (temp > est)
-            est = temp;
-    }
-    if (est == 0.0)
-        return 1.0 / 0.0;
-    double rcond = (1.0 / est) / anorm;
-    return 1.0 / rcond;
-}
-
-__device__ __forceinline__ double warp_nrm2(const double *v, int n, int lane)
-{
-    double s = 0.0;
-    if (lane < n)
-        s = v[lane] * v[lane];
-    if (lane + 32 < n)
-        s = fma(v[lane + 32], v[lane + 32], s);
-    return sqrt(warp_sum(s));
-}
-
-// ---------------------------------------------------------------- Newton state machine
-
-struct Outputs {
-    double *u, *alpha;
-    int *iters, *iterGamma, *regIdx, *status;
-    unsigned long long *failCount; // cells finishing with a non-zero status
-    unsigned long long *stats;     // running counters, layout STAT_* (may be null)
-};
-
-template <int NT>
-__device__ void finalize(Slot<NT> &sl, const ClosureParams &P, const Outputs &O, int lane)
-{
-    const int nm = P.nm;
-    long long c = sl.s.cell;
-    __syncwarp();
-    if (sl.s.status != CELL_NONPOSITIVE_U0) {
-        // postProcess: rescale (src/opt/optBatch.cpp:334-344, src/opt/opt.cpp:352-354)
-        for (int i = lane; i < nm; i += 32) {
-            O.u[c * nm + i] = sl.u[i] * sl.s.u0;
-            double a = sl.alpha[i];
-            if (i == 0)
-                a = a + sl.s.alphaScale;
-            O.alpha[c * nm + i] = a;
-        }
-    }
-    if (lane == 0) {
-        if (O.iters) O.iters[c] = sl.s.totalIter;
-        if (O.iterGamma) O.iterGamma[c] = sl.s.iterGamma < 0 ? 0 : sl.s.iterGamma;
-        if (O.regIdx) O.regIdx[c] = sl.s.regIndex;
-        if (O.status) O.status[c] = sl.s.status;
-        if (sl.s.status != CELL_OK && O.failCount)
-            atomicAdd(O.failCount, 1ull);
-        if (O.stats) {
-            unsigned long long it = (unsigned long long)sl.s.totalIter;
-            unsigned long long ig = (unsigned long long)(sl.s.iterGamma < 0 ? 0 : sl.s.iterGamma);
-            atomicAdd(&O.stats[STAT_CELLS], 1ull);
-            atomicAdd(&O.stats[STAT_ITERS], it);
-            atomicAdd(&O.stats[STAT_ITER_GAMMA], ig);
-            atomicMax(&O.stats[STAT_MAX_ITER], it);
-            atomicMax(&O.stats[STAT_MAX_ITER_GAMMA], ig);
-            if (sl.s.status != CELL_OK)
-                atomicAdd(&O.stats[STAT_FAILED], 1ull);
-            atomicAdd(&O.stats[STAT_REG_HIST + (sl.s.regIndex & 15)], 1ull);
-            atomicAdd(&O.stats[STAT_ITER_HIST + (it < 63 ? it : 63)], 1ull);
-        }
-        sl.s.need = NEED_NONE;
-        sl.s.cell = -1;
-    }
-    __syncwarp();
-}
-
-// Regularise (src/opt/opt.cpp:251-279). Returns false if the ladder is exhausted.
-template <int NT>
-__device__ bool regularize(Slot<NT> &sl, const ClosureParams &P, int lane)
-{
-    const int nm = P.nm;
-    __syncwarp();
-    if (sl.s.regIndex >= P.nreg - 1)
-        return false;
-    int ri = sl.s.regIndex + 1;
-    double r = P.reg[ri];
-    for (int i = lane; i < nm; i += 32)
-        sl.u[i] = (i == 0) ? 1.0 : sl.uOrig[i] * (1.0 - r);
-    __syncwarp();
-    double rt = P.batched ? P.tol : warp_nrm2(sl.u, nm, lane) * P.tol;
-    for (int i = lane; i < nm; i += 32)
-        sl.alpha[i] = sl.alpha0[i];
-    __syncwarp();
-    if (lane == 0) {
-        sl.s.regIndex = ri;
-        sl.s.r = r;
-        sl.s.rtol = rt;
-        sl.s.iterGamma = 0;
-        sl.s.iter = 0;
-        sl.s.t = 1.0;
-        if (!P.batched && ri == P.nreg - 1)
-            sl.s.maxIter = 10 * sl.s.maxIter;
-    }
-    __syncwarp();
-    return true;
-}
-
-// Starts the next Newton iteration. When the iteration is bound to regularise
-// whatever H turns out to be (t == 0 after a failed line search, or the
-// iteration cap reached), the regularisation is applied here without the H pass.
-template <int NT>
-__device__ void begin_iteration(Slot<NT> &sl, const ClosureParams &P, const Outputs &O, int lane)
-{
-    for (;;) {
-        __syncwarp();
-        int maxIterEff = sl.s.maxIter;
-        if (P.batched && sl.s.regIndex == P.nreg - 1)
-            maxIterEff = 10 * P.maxIter;
-        int iter = sl.s.iter + 1, total = sl.s.totalIter + 1;
-        long long passes = sl.s.passes + 1;
-        __syncwarp();
-        if (lane == 0) {
-            sl.s.iter = iter;
-            sl.s.totalIter = total;
-            sl.s.passes = passes;
-        }
-        __syncwarp();
-        if (passes > P.passBudget) {
-            if (lane == 0)
-                sl.s.status = CELL_PASS_BUDGET;
-            finalize(sl, P, O, lane);
-            return;
-        }
-        if (total > 1 && (sl.s.t == 0.0 || iter >= maxIterEff)) {
-            if (!regularize(sl, P, lane)) {
-                if (lane == 0)
-                    sl.s.status = CELL_LADDER_EXHAUSTED;
-                finalize(sl, P, O, lane);
-                return;
-            }
-            continue;
-        }
-        if (lane == 0)
-            sl.s.need = NEED_H;
-        __syncwarp();
-        return;
-    }
-}
-
-template <int NT>
-__device__ void load_cell(Slot<NT> &sl, const ClosureParams &P, const Outputs &O, long long c,
-                          int lane)
-{
-    const int nm = P.nm;
-    constexpr int NMP = Cfg<NT>::NMP;
-    double u0 = O.u[c * nm];
-    double alphaScale = log(u0) * 2.0 * sqrt(M_PI);
-    for (int i = lane; i < NMP; i += 32) {
-        double ui = 0.0, ai = 0.0;
-        if (i < nm) {
-            ui = O.u[c * nm + i] / u0;
-            ai = O.alpha[c * nm + i];
-            if (i == 0)
-                ai = ai - alphaScale;
-        }
-        sl.u[i] = ui;
-        sl.uOrig[i] = ui;
-        sl.alpha[i] = ai;
-        sl.alpha0[i] = ai;
-        sl.g[i] = 0.0;
-        sl.d[i] = 0.0;
-    }
-    __syncwarp();
-    double rt = P.batched ? P.tol : warp_nrm2(sl.u, nm, lane) * P.tol;
-    if (lane == 0) {
-        sl.s.cell = c;
-        sl.s.passes = 0;
-        sl.s.u0 = u0;
-        sl.s.alphaScale = alphaScale;
-        sl.s.rtol = rt;
-        sl.s.t = 1.0;
-        sl.s.r = 0.0;
-        sl.s.gamma = 0.0;
-        sl.s.err = 0.0;
-        sl.s.iter = 0;
-        sl.s.totalIter = 0;
-        sl.s.iterGamma = 0;
-        sl.s.regIndex = 0;
-        sl.s.maxIter = P.maxIter;
-        sl.s.status = CELL_OK;
-    }
-    __syncwarp();
-    if (u0 <= 0) {
-        if (lane == 0)
-            sl.s.status = CELL_NONPOSITIVE_U0;
-        finalize(sl, P, O, lane);
-        return;
-    }
-    begin_iteration(sl, P, O, lane);
-}
-
-// Sets alpha = alphaOld + t d and requests a trial pass, or gives up with t = 0.
-template <int NT>
-__device__ void next_trial(Slot<NT> &sl, const ClosureParams &P, const Outputs &O, int lane);
-
-template <int NT>
-__device__ void next_trial(Slot<NT> &sl, const ClosureParams &P, const Outputs &O, int lane)
-{
-    const int nm = P.nm;
-    double t = sl.s.t;
-    __syncwarp();
-    if (t * sl.s.maxFactor > EPS_HALF) {
-        for (int i = lane; i < nm; i += 32)
-            sl.alpha[i] = __dadd_rn(sl.alphaOld[i], __dmul_rn(t, sl.d[i]));
-        __syncwarp();
-        if (lane == 0) {
-            sl.s.need = NEED_TRIAL;
-            if (O.stats)
-                atomicAdd(&O.stats[STAT_TRIALS], 1ull);
-        }
-        __syncwarp();
-    } else {
-        // backtracked all the way (src/opt/linesearch.cpp:76-78)
-        for (int i = lane; i < nm; i += 32)
-            sl.alpha[i] = sl.alphaOld[i];
-        __syncwarp();
-        if (lane == 0)
-            sl.s.t = 0.0;
-        __syncwarp();
-        begin_iteration(sl, P, O, lane);
-    }
-}
-
-template <int NT>
-__device__ void after_hessian(Slot<NT> &sl, const ClosureParams &P, const Outputs &O, int lane,
-                              double m0)
-{
-    const int nm = P.nm;
-    // g_i = H_i0 / m_0 - u_i ; f = H_00 / m_0^2 - alpha.u  (src/opt/fobj.cpp:121-129)
-    for (int i = lane; i < nm; i += 32)
-        sl.g[i] = sl.L[pidx(i, 0)] / m0 - sl.u[i];
-    __syncwarp();
-    double f = 0.0;
-    if (lane == 0) {
-        f = sl.L[0] / (m0 * m0);
-        for (int i = 0; i < nm; ++i)
-            f = __dsub_rn(f, __dmul_rn(sl.alpha[i], sl.u[i]));
-    }
-    f = __shfl_sync(FULL_MASK, f, 0);
-    // 1-norm: max row sum of |H| (src/utils.cpp:35-49)
-    double rs = 0.0, gmin = 1.0 / 0.0;
-    for (int i = lane; i < nm; i += 32) {
-        double s = 0.0;
-        for (int j = 0; j < nm; ++j)
-            s += fabs(j <= i ? sl.L[pidx(i, j)] : sl.L[pidx(j, i)]);
-        rs = fmax(rs, s);
-        gmin = fmin(gmin, 2.0 * sl.L[pidx(i, i)] - s); // Gershgorin: H_ii - sum_{j!=i} |H_ij|
-    }
-    double norm1 = warp_max(rs);
-    gmin = -warp_max(-gmin);
-    // All eigenvalues of H are >= gmin, so when gmin > 0, ||H^-1||_1 <= sqrt(n)/gmin and the
-    // 1-norm condition number is at most norm1 sqrt(n)/gmin. The Hager estimate can only be
-    // smaller, so if this bound is below condHMax/2 the reference's test `condest > condHMax`
-    // is false whatever the estimate; the estimate is then skipped.
-    bool condSure = gmin > 0.0 && norm1 * sqrt((double)nm) / gmin <= 0.5 * P.condHMax;
-    __syncwarp();
-    int info = warp_cholesky(sl, nm, lane);
-    double cond = 0.0;
-    if (info == 0) {
-        for (int i = lane; i < nm; i += 32)
-            sl.rinv[i] = 1.0 / sl.L[pidx(i, i)];
-        __syncwarp();
-        if (!condSure)
-            cond = warp_condest(sl, nm, lane, norm1);
-    }
-    __syncwarp();
-
-    bool bad = (info != 0) || (cond > P.condHMax);
-    if (sl.s.totalIter == 1 && bad) {
-        // isotropic restart (src/opt/opt.cpp:236-247)
-        double rt = P.batched ? P.tol : warp_nrm2(sl.u, nm, lane) * P.tol;
-        for (int i = lane; i < nm; i += 32) {
-            double a = (i == 0) ? 2.0 * sqrt(M_PI) * log(0.5 / sqrt(M_PI)) : 0.0;
-            sl.alpha0[i] = a;
-            sl.alpha[i] = a;
-        }
-        __syncwarp();
-        if (lane == 0) {
-            sl.s.rtol = rt;
-            sl.s.iter = 0;
-            sl.s.iterGamma = 0;
-            sl.s.t = 1.0;
-        }
-        __syncwarp();
-        begin_iteration(sl, P, O, lane);
-        return;
-    }
-    int maxIterEff = sl.s.maxIter;
-    if (P.batched && sl.s.regIndex == P.nreg - 1)
-        maxIterEff = 10 * P.maxIter;
-    if (sl.s.iter >= maxIterEff || bad || sl.s.t == 0.0) {
-        if (!regularize(sl, P, lane)) {
-            if (lane == 0)
-                sl.s.status = CELL_LADDER_EXHAUSTED;
-            finalize(sl, P, O, lane);
-            return;
-        }
-        begin_iteration(sl, P, O, lane);
-        return;
-    }
-    // d = -H^{-1} g
-    double x0 = lane < nm ? sl.g[lane] : 0.0;
-    double x1 = lane + 32 < nm ? sl.g[lane + 32] : 0.0;
-    warp_apply_inverse(sl, nm, lane, x0, x1, true);
-    if (lane < nm)
-        sl.d[lane] = -x0;
-    if (lane + 32 < nm)
-        sl.d[lane + 32] = -x1;
-    __syncwarp();
-    double err = warp_nrm2(sl.g, nm, lane);
-    double d1 = vsum_abs(x0, x1, lane, nm);
-    int pnOrder = (int)floor(sqrt((double)nm)) + 1;
-    double minf = sqrt((2 * pnOrder + 1) / (2 * M_PI));
-    double gamma = exp(2.0 * d1 * minf);
-    double tolEff = sl.s.rtol;
-    if (lane == 0) {
-        sl.s.err = err;
-        sl.s.gamma = gamma;
-    }
-    __syncwarp();
-    if (err <= tolEff && gamma <= P.tolGamma) {
-        finalize(sl, P, O, lane);
-        return;
-    }
-    // line search set-up (src/opt/linesearch.cpp:41-54)
-    double mf = 0.0;
-    for (int i = lane; i < nm; i += 32) {
-        sl.alphaOld[i] = sl.alpha[i];
-        mf = fmax(mf, fabs(sl.d[i]) / (fabs(sl.alpha[i]) + 1e-100));
-    }
-    mf = warp_max(mf);
-    double gd = 0.0;
-    __syncwarp();
-    if (lane == 0) {
-        for (int i = 0; i < nm; ++i)
-            gd = __dadd_rn(gd, __dmul_rn(sl.g[i], sl.d[i]));
-        if (err <= tolEff)
-            sl.s.iterGamma += 1;
-        sl.s.f = f;
-        sl.s.maxFactor = mf;
-        sl.s.gd = gd;
-        sl.s.t = 1.0;
-    }
-    __syncwarp();
-    next_trial(sl, P, O, lane);
-}
-
-template <int NT>
-__device__ void after_trial(Slot<NT> &sl, const ClosureParams &P, const Outputs &O, int lane,
-                            double fquad)
-{
-    const int nm = P.nm;
-    double fnew = 0.0;
-    if (lane == 0) {
-        fnew = fquad;
-        for (int i = 0; i < nm; ++i)
-            fnew = __dsub_rn(fnew, __dmul_rn(sl.alpha[i], sl.u[i]));
-    }
-    fnew = __shfl_sync(FULL_MASK, fnew, 0);
-    double t = sl.s.t;
-    bool accept = fnew <= __dadd_rn(sl.s.f, __dmul_rn(__dmul_rn(1e-3, t), sl.s.gd));
-    __syncwarp();
-    if (accept) {
-        begin_iteration(sl, P, O, lane);
-        return;
-    }
-    if (lane == 0)
-        sl.s.t = 0.5 * t;
-    __syncwarp();
-    next_trial(sl, P, O, lane);
-}
-
-} // namespace
 
 // ---------------------------------------------------------------- kernel
 
@@ -718,6 +70,7 @@ __global__ void __launch_bounds__(W * 32, 1)
 
     uint32_t seq = 0; // chunks consumed so far by this CTA (uniform)
     for (;;) {
+        long long tc0 = clock64();
         // refill an empty slot from the device work queue
         if (sl.s.need == NEED_NONE && !sl.s.exhausted) {
             for (;;) {
@@ -740,6 +93,7 @@ __global__ void __launch_bounds__(W * 32, 1)
         const int need = sl.s.need;
         if (!__syncthreads_or(need != NEED_NONE))
             break;
+        long long tc1 = clock64();
 
         // ------------------------------------------------ one pass over the basis
         double acc[Cfg<NT>::NTILE][2];
@@ -802,6 +156,7 @@ __global__ void __launch_bounds__(W * 32, 1)
             }
         }
         seq += nchunks;
+        long long tc2 = clock64();
 
         // ------------------------------------------------ per-warp Newton logic
         if (need == NEED_H) {
@@ -824,6 +179,14 @@ __global__ void __launch_bounds__(W * 32, 1)
             after_trial(sl, P, O, lane, fq);
         }
         __syncthreads();
+        if (lane == 0 && O.stats) {
+            long long tc3 = clock64();
+            atomicAdd(&O.stats[STAT_CLK_REFILL], (unsigned long long)(tc1 - tc0));
+            atomicAdd(&O.stats[STAT_CLK_PASS], (unsigned long long)(tc2 - tc1));
+            atomicAdd(&O.stats[STAT_CLK_SERIAL], (unsigned long long)(tc3 - tc2));
+            if (warp == 0)
+                atomicAdd(&O.stats[STAT_PASSES], 1ull);
+        }
     }
 }
 
@@ -838,8 +201,6 @@ __global__ void __launch_bounds__(W * 32, 1)
 // accumulate the moments of the CTA's W = 8 cells as one DMMA GEMM
 // (moments[k][cell] += M2^T[k][q] C[q][cell]) with the staged M2^T chunk as the shared
 // operand: ~7x fewer FLOPs than the direct lower triangle for M_6.
-constexpr int GSTAGES = 2;
-constexpr int CST = 12; // row stride of the coefficient tile (bank-conflict-free B fragments)
 
 template <int NT, int NT2, int W>
 __global__ void __launch_bounds__(W * 32, 1)
@@ -882,6 +243,7 @@ __global__ void __launch_bounds__(W * 32, 1)
 
     uint32_t seq = 0;
     for (;;) {
+        long long tc0 = clock64();
         if (sl.s.need == NEED_NONE && !sl.s.exhausted) {
             for (;;) {
                 unsigned long long c = 0;
@@ -903,6 +265,7 @@ __global__ void __launch_bounds__(W * 32, 1)
         const int need = sl.s.need;
         if (!__syncthreads_or(need != NEED_NONE))
             break;
+        long long tc1 = clock64();
         const bool anyH = __syncthreads_or(need == NEED_H);
 
         double acc[RT][2];
@@ -960,6 +323,7 @@ __global__ void __launch_bounds__(W * 32, 1)
             }
         }
         seq += nchunks;
+        long long tc2 = clock64();
 
         if (anyH) {
 #pragma unroll
@@ -1000,6 +364,14 @@ __global__ void __launch_bounds__(W * 32, 1)
             after_trial(sl, P, O, lane, fq);
         }
         __syncthreads();
+        if (lane == 0 && O.stats) {
+            long long tc3 = clock64();
+            atomicAdd(&O.stats[STAT_CLK_REFILL], (unsigned long long)(tc1 - tc0));
+            atomicAdd(&O.stats[STAT_CLK_PASS], (unsigned long long)(tc2 - tc1));
+            atomicAdd(&O.stats[STAT_CLK_SERIAL], (unsigned long long)(tc3 - tc2));
+            if (warp == 0)
+                atomicAdd(&O.stats[STAT_PASSES], 1ull);
+        }
     }
 }
 

@@ -1,0 +1,543 @@
+// Work-list form of the FP64 M_N closure: the reference's batched structure
+// (Optimization::opt with its stacks, src/opt/optBatch.cpp:350-472) on the device.
+//
+// A closure runs in rounds over a device work list of cells that need a quadrature
+// pass (a Hessian evaluation or a line-search trial):
+//   init kernel    per cell: scale u and alpha (preProcess, src/opt/optBatch.cpp:312-331),
+//                  start the first Newton iteration, append the cell to the work list;
+//   pass kernel    per listed cell: exponents alpha.m_q and either the extended moments
+//                  of the Gaunt form (one DMMA GEMM for the 8 cells of a CTA, shared
+//                  staged M2^T chunks) or the direct Hessian tiles, or the trial's f;
+//   Newton kernel  one warp per listed cell: assemble H, Cholesky, condition estimate,
+//                  direction, stop tests, Armijo (solveTheRest, src/opt/optBatch.cpp:143-283)
+//                  with the state machine shared with the persistent kernels; cells that
+//                  need another pass are appended to the next round's list.
+// Separating the passes (tensor-pipe work, small shared memory) from the per-cell logic
+// (latency-bound, one warp per cell) lets each run at its own occupancy; a cell that
+// needs many iterations only ever occupies the short lists of later rounds.
+#include "closure_core.cuh"
+
+#include <cstdio>
+
+namespace c3d {
+
+// Per-cell Newton state between rounds (the slot without the packed triangle).
+template <int NT> struct CellState {
+    static constexpr int NMP = Cfg<NT>::NMP;
+    double u[NMP], alpha[NMP], alpha0[NMP], uOrig[NMP], g[NMP], d[NMP], alphaOld[NMP];
+    SlotScalars s;
+};
+
+namespace {
+
+template <int NT>
+__device__ void state_to_slot(const CellState<NT> &st, Slot<NT> &sl, int lane)
+{
+    constexpr int NMP = Cfg<NT>::NMP;
+    for (int i = lane; i < NMP; i += 32) {
+        sl.u[i] = st.u[i];
+        sl.alpha[i] = st.alpha[i];
+        sl.alpha0[i] = st.alpha0[i];
+        sl.uOrig[i] = st.uOrig[i];
+        sl.g[i] = st.g[i];
+        sl.d[i] = st.d[i];
+        sl.alphaOld[i] = st.alphaOld[i];
+    }
+    if (lane == 0)
+        sl.s = st.s;
+    __syncwarp();
+}
+
+template <int NT>
+__device__ void slot_to_state(const Slot<NT> &sl, CellState<NT> &st, int lane)
+{
+    constexpr int NMP = Cfg<NT>::NMP;
+    __syncwarp();
+    for (int i = lane; i < NMP; i += 32) {
+        st.u[i] = sl.u[i];
+        st.alpha[i] = sl.alpha[i];
+        st.alpha0[i] = sl.alpha0[i];
+        st.uOrig[i] = sl.uOrig[i];
+        st.g[i] = sl.g[i];
+        st.d[i] = sl.d[i];
+        st.alphaOld[i] = sl.alphaOld[i];
+    }
+    if (lane == 0)
+        st.s = sl.s;
+}
+
+// Appends cell c to the list when it still needs a pass.
+template <int NT>
+__device__ void append_if_needed(const Slot<NT> &sl, long long c, int lane, int *listOut,
+                                 unsigned int *countOut)
+{
+    if (lane == 0 && sl.s.need != NEED_NONE) {
+        unsigned int pos = atomicAdd(countOut, 1u);
+        listOut[pos] = (int)c;
+    }
+}
+
+} // namespace
+
+constexpr int RW = 8; // warps (cells) per CTA in every round kernel
+
+template <int NT>
+__global__ void __launch_bounds__(RW * 32)
+    rounds_init_kernel(ClosureParams P, long long ncells, Outputs O, CellState<NT> *state,
+                       int *listOut, unsigned int *countOut)
+{
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    Slot<NT> *slots = reinterpret_cast<Slot<NT> *>(smem_raw);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const long long c = (long long)blockIdx.x * RW + warp;
+    if (c >= ncells)
+        return;
+    Slot<NT> &sl = slots[warp];
+    load_cell(sl, P, O, c, lane);
+    slot_to_state(sl, state[c], lane);
+    append_if_needed(sl, c, lane, listOut, countOut);
+}
+
+// Pass of the Gaunt form: per listed cell, exponents and then either the extended
+// moments (need H) into momBuf[pos] or the trial objective's quadrature sum (need TRIAL)
+// into its state.
+template <int NT, int NT2>
+__global__ void __launch_bounds__(RW * 32, 2)
+    rounds_pass_gaunt_kernel(ClosureParams P, const double *__restrict__ chunks,
+                             const int *__restrict__ list, int n, CellState<NT> *state,
+                             double *__restrict__ momBuf, int *errorFlag)
+{
+    constexpr int NMP = Cfg<NT>::NMP;
+    constexpr int NM2P = 8 * NT2;
+    constexpr int CH = (NM2P + 1) * QCP;
+    constexpr int RT = (NT2 + RW - 1) / RW;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    double *stage = reinterpret_cast<double *>(smem_raw);
+    double *cbuf = stage + GSTAGES * CH;       // QC x CST
+    double *alph = cbuf + QC * CST;            // RW x NMP
+    uint64_t *full = reinterpret_cast<uint64_t *>(alph + RW * NMP);
+    __shared__ int s_abort;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int nm = P.nm, nchunks = P.nchunks;
+    const uint32_t chunkBytes = CH * sizeof(double);
+    const int pos = blockIdx.x * RW + warp;
+    int need = NEED_NONE;
+    long long cell = -1;
+    if (pos < n) {
+        cell = list[pos];
+        need = state[cell].s.need;
+    }
+    for (int i = lane; i < NMP; i += 32)
+        alph[warp * NMP + i] = (cell >= 0 && i < nm) ? state[cell].alpha[i] : 0.0;
+    if (tid == 0) {
+        for (int s = 0; s < GSTAGES; ++s)
+            mbar_init(&full[s], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        s_abort = 0;
+        for (int k = 0; k < GSTAGES && k < nchunks; ++k) {
+            mbar_expect_tx(&full[k], chunkBytes);
+            bulk_g2s(stage + k * CH, chunks + (size_t)k * CH, chunkBytes, &full[k]);
+        }
+    }
+    __syncthreads();
+    const bool anyH = __syncthreads_or(need == NEED_H);
+    const double *al = alph + warp * NMP;
+    double acc[RT][2];
+#pragma unroll
+    for (int r = 0; r < RT; ++r)
+        acc[r][0] = acc[r][1] = 0.0;
+    double fpart = 0.0;
+    for (int k = 0; k < nchunks; ++k) {
+        uint32_t s = k % GSTAGES, parity = (k / GSTAGES) & 1u;
+        if (!mbar_wait(&full[s], parity))
+            s_abort = 1;
+        if (__syncthreads_or(s_abort)) {
+            if (tid == 0)
+                atomicExch(errorFlag, 1);
+            return;
+        }
+        const double *ch = stage + s * CH;
+        double c = 0.0;
+        if (need != NEED_NONE) {
+            double z = 0.0;
+            for (int i = 0; i < nm; ++i)
+                z = __dadd_rn(z, __dmul_rn(al[i], ch[i * QCP + lane]));
+            c = ch[NM2P * QCP + lane] * exp(z);
+            if (need == NEED_TRIAL)
+                fpart += c;
+        }
+        cbuf[lane * CST + warp] = (need == NEED_H) ? c : 0.0;
+        __syncthreads();
+        if (anyH) {
+#pragma unroll
+            for (int g = 0; g < QC / 4; ++g) {
+                double b = cbuf[(4 * g + (lane & 3)) * CST + (lane >> 2)];
+#pragma unroll
+                for (int r = 0; r < RT; ++r) {
+                    int rt = warp + r * RW;
+                    if (rt < NT2) {
+                        double a = ch[(8 * rt + (lane >> 2)) * QCP + 4 * g + (lane & 3)];
+                        dmma(acc[r][0], acc[r][1], a, b);
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        if (tid == 0 && k + GSTAGES < nchunks) {
+            mbar_expect_tx(&full[s], chunkBytes);
+            bulk_g2s(stage + s * CH, chunks + (size_t)(k + GSTAGES) * CH, chunkBytes, &full[s]);
+        }
+    }
+    if (anyH) {
+        const int base = blockIdx.x * RW;
+#pragma unroll
+        for (int r = 0; r < RT; ++r) {
+            int rt = warp + r * RW;
+            if (rt < NT2) {
+                int kk = 8 * rt + (lane >> 2), c0 = 2 * (lane & 3);
+                if (base + c0 < n)
+                    momBuf[(size_t)(base + c0) * NM2P + kk] = acc[r][0];
+                if (base + c0 + 1 < n)
+                    momBuf[(size_t)(base + c0 + 1) * NM2P + kk] = acc[r][1];
+            }
+        }
+    }
+    if (need == NEED_TRIAL) {
+        double fq = warp_sum(fpart);
+        if (lane == 0)
+            state[cell].s.fquad = fq;
+    }
+}
+
+// Pass of the direct form: per listed cell, the lower-triangle DMMA tiles of H (packed
+// into hBuf[pos]) or the trial's quadrature sum.
+template <int NT>
+__global__ void __launch_bounds__(RW * 32, 1)
+    rounds_pass_direct_kernel(ClosureParams P, const double *__restrict__ chunks,
+                              const int *__restrict__ list, int n, CellState<NT> *state,
+                              double *__restrict__ hBuf, int *errorFlag)
+{
+    constexpr int NMP = Cfg<NT>::NMP;
+    constexpr int NPK = Cfg<NT>::NPK;
+    constexpr int CH = Cfg<NT>::CHUNK;
+    constexpr int ST = 3;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    double *stage = reinterpret_cast<double *>(smem_raw);
+    double *alph = stage + ST * CH;
+    uint64_t *full = reinterpret_cast<uint64_t *>(alph + RW * NMP);
+    __shared__ int s_abort;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int nm = P.nm, nchunks = P.nchunks;
+    const uint32_t chunkBytes = CH * sizeof(double);
+    const int pos = blockIdx.x * RW + warp;
+    int need = NEED_NONE;
+    long long cell = -1;
+    if (pos < n) {
+        cell = list[pos];
+        need = state[cell].s.need;
+    }
+    for (int i = lane; i < NMP; i += 32)
+        alph[warp * NMP + i] = (cell >= 0 && i < nm) ? state[cell].alpha[i] : 0.0;
+    if (tid == 0) {
+        for (int s = 0; s < ST; ++s)
+            mbar_init(&full[s], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        s_abort = 0;
+        for (int k = 0; k < ST && k < nchunks; ++k) {
+            mbar_expect_tx(&full[k], chunkBytes);
+            bulk_g2s(stage + k * CH, chunks + (size_t)k * CH, chunkBytes, &full[k]);
+        }
+    }
+    __syncthreads();
+    const double *al = alph + warp * NMP;
+    double acc[Cfg<NT>::NTILE][2];
+#pragma unroll
+    for (int t = 0; t < Cfg<NT>::NTILE; ++t)
+        acc[t][0] = acc[t][1] = 0.0;
+    double fpart = 0.0;
+    for (int k = 0; k < nchunks; ++k) {
+        uint32_t s = k % ST, parity = (k / ST) & 1u;
+        if (!mbar_wait(&full[s], parity))
+            s_abort = 1;
+        if (__syncthreads_or(s_abort)) {
+            if (tid == 0)
+                atomicExch(errorFlag, 1);
+            return;
+        }
+        const double *ch = stage + s * CH;
+        if (need != NEED_NONE) {
+            double z = 0.0;
+            for (int i = 0; i < nm; ++i)
+                z = __dadd_rn(z, __dmul_rn(al[i], ch[i * QCP + lane]));
+            double c = ch[NMP * QCP + lane] * exp(z);
+            if (need == NEED_TRIAL) {
+                fpart += c;
+            } else {
+#pragma unroll
+                for (int g = 0; g < QC / 4; ++g) {
+                    double cq = __shfl_sync(FULL_MASK, c, 4 * g + (lane & 3));
+                    double m[NT], a[NT];
+#pragma unroll
+                    for (int I = 0; I < NT; ++I) {
+                        m[I] = ch[(8 * I + (lane >> 2)) * QCP + 4 * g + (lane & 3)];
+                        a[I] = cq * m[I];
+                    }
+#pragma unroll
+                    for (int I = 0; I < NT; ++I)
+#pragma unroll
+                        for (int J = 0; J <= I; ++J)
+                            dmma(acc[I * (I + 1) / 2 + J][0], acc[I * (I + 1) / 2 + J][1], a[I],
+                                 m[J]);
+                }
+            }
+        }
+        __syncthreads();
+        if (tid == 0 && k + ST < nchunks) {
+            mbar_expect_tx(&full[s], chunkBytes);
+            bulk_g2s(stage + s * CH, chunks + (size_t)(k + ST) * CH, chunkBytes, &full[s]);
+        }
+    }
+    if (need == NEED_H) {
+        double *H = hBuf + (size_t)pos * NPK;
+#pragma unroll
+        for (int I = 0; I < NT; ++I)
+#pragma unroll
+            for (int J = 0; J <= I; ++J) {
+                int row = 8 * I + (lane >> 2);
+#pragma unroll
+                for (int e2 = 0; e2 < 2; ++e2) {
+                    int col = 8 * J + 2 * (lane & 3) + e2;
+                    if (row < nm && col < nm && col <= row)
+                        H[pidx(row, col)] = acc[I * (I + 1) / 2 + J][e2];
+                }
+            }
+    } else if (need == NEED_TRIAL) {
+        double fq = warp_sum(fpart);
+        if (lane == 0)
+            state[cell].s.fquad = fq;
+    }
+}
+
+// Newton logic for the listed cells: one warp per cell, state staged in shared memory.
+// GAUNT: H_ij (i >= j) from the CSR of beta over the cell's moments (momBuf);
+// otherwise H packed in hBuf.
+template <int NT, int NT2, bool GAUNT>
+__global__ void __launch_bounds__(RW * 32, 2)
+    rounds_newton_kernel(ClosureParams P, double m0, const int *__restrict__ list, int n,
+                         CellState<NT> *state, const double *__restrict__ buf,
+                         const int *__restrict__ bRow, const int *__restrict__ bCol,
+                         const double *__restrict__ bVal, Outputs O, int *listOut,
+                         unsigned int *countOut)
+{
+    constexpr int NM2P = 8 * NT2;
+    constexpr int NPK = Cfg<NT>::NPK;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    Slot<NT> *slots = reinterpret_cast<Slot<NT> *>(smem_raw);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int pos = blockIdx.x * RW + warp;
+    if (pos >= n)
+        return;
+    const long long cell = list[pos];
+    Slot<NT> &sl = slots[warp];
+    state_to_slot(state[cell], sl, lane);
+    const int nm = P.nm;
+    const int npk = nm * (nm + 1) / 2;
+    if (sl.s.need == NEED_H) {
+        if (GAUNT) {
+            const double *mw = buf + (size_t)pos * NM2P;
+            int ii = 0, jj = lane;
+            while (jj > ii) {
+                jj -= ii + 1;
+                ++ii;
+            }
+            for (int e = lane; e < npk; e += 32) {
+                int idx = jj * nm + ii;
+                double h = 0.0;
+                for (int t = bRow[idx]; t < bRow[idx + 1]; ++t)
+                    h = __dadd_rn(h, __dmul_rn(mw[bCol[t]], bVal[t]));
+                sl.L[e] = h;
+                jj += 32;
+                while (jj > ii) {
+                    jj -= ii + 1;
+                    ++ii;
+                }
+            }
+        } else {
+            const double *H = buf + (size_t)pos * NPK;
+            for (int e = lane; e < npk; e += 32)
+                sl.L[e] = H[e];
+        }
+        __syncwarp();
+        after_hessian(sl, P, O, lane, m0);
+    } else if (sl.s.need == NEED_TRIAL) {
+        after_trial(sl, P, O, lane, sl.s.fquad);
+    }
+    slot_to_state(sl, state[cell], lane);
+    append_if_needed(sl, cell, lane, listOut, countOut);
+}
+
+// ---------------------------------------------------------------- host side
+
+struct RoundsLaunch {
+    const ClosureParams *P;
+    const double *chunks;      // direct: (NMP+1) x QCP chunks; Gaunt: (NM2P+1) x QCP chunks
+    const int *bRow, *bCol;    // Gaunt CSR (null for the direct form)
+    const double *bVal;
+    double m0;                 // M[0][0]
+    long long ncells;
+    double *u, *alpha;
+    int *iters, *iterGamma, *regIdx, *status;
+    unsigned long long *failCount, *stats;
+    void *state;               // ncells x rounds_state_bytes(nm)
+    int *listA, *listB;        // ncells each
+    unsigned int *counts;      // 2 device counters
+    unsigned int *hostCount;   // pinned
+    double *buf;               // batch x (NM2P or NPK) doubles
+    long long batch;           // list entries per pass/Newton launch pair
+    int *errorFlag;
+    cudaStream_t stream;
+    long long *launches;
+    long long maxRounds;
+};
+
+template <int NT> static size_t state_bytes_t() { return sizeof(CellState<NT>); }
+
+size_t rounds_state_bytes(int nm)
+{
+    switch ((nm + 7) / 8) {
+    case 1: return state_bytes_t<1>();
+    case 2: return state_bytes_t<2>();
+    case 3: return state_bytes_t<3>();
+    case 4: return state_bytes_t<4>();
+    case 5: return state_bytes_t<5>();
+    case 6: return state_bytes_t<6>();
+    case 7: return state_bytes_t<7>();
+    default: return state_bytes_t<8>();
+    }
+}
+
+// Doubles per list entry of the pass output buffer.
+size_t rounds_buf_doubles(int nm, int nm2, bool gaunt)
+{
+    if (gaunt)
+        return (size_t)8 * ((nm2 + 7) / 8);
+    int nml = max_nm_for((nm + 7) / 8);
+    return (size_t)nml * (nml + 1) / 2; // the template's packed triangle
+}
+
+template <int NT, int NT2, bool GAUNT> static cudaError_t rounds_t(const RoundsLaunch &R)
+{
+    const ClosureParams &P = *R.P;
+    CellState<NT> *state = reinterpret_cast<CellState<NT> *>(R.state);
+    cudaStream_t st = R.stream;
+    cudaError_t e;
+    size_t slotSmem = RW * sizeof(Slot<NT>);
+    e = cudaFuncSetAttribute(rounds_init_kernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)slotSmem);
+    if (e != cudaSuccess)
+        return e;
+    e = cudaFuncSetAttribute(rounds_newton_kernel<NT, NT2, GAUNT>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)slotSmem);
+    if (e != cudaSuccess)
+        return e;
+    size_t passSmem;
+    if (GAUNT) {
+        constexpr int NM2P = 8 * NT2;
+        passSmem = GSTAGES * (size_t)(NM2P + 1) * QCP * 8 + (size_t)QC * CST * 8 +
+                   (size_t)RW * Cfg<NT>::NMP * 8 + GSTAGES * 8;
+        e = cudaFuncSetAttribute(rounds_pass_gaunt_kernel<NT, NT2>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)passSmem);
+    } else {
+        passSmem = 3 * (size_t)Cfg<NT>::CHUNK * 8 + (size_t)RW * Cfg<NT>::NMP * 8 + 3 * 8;
+        e = cudaFuncSetAttribute(rounds_pass_direct_kernel<NT>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)passSmem);
+    }
+    if (e != cudaSuccess)
+        return e;
+    const double m0 = R.m0;
+    const Outputs O{R.u, R.alpha, R.iters, R.iterGamma, R.regIdx, R.status, R.failCount, R.stats};
+
+    // round 0: set-up of every cell
+    unsigned int *cA = R.counts, *cB = R.counts + 1;
+    int *listA = R.listA, *listB = R.listB;
+    e = cudaMemsetAsync(cA, 0, sizeof(unsigned int), st);
+    if (e != cudaSuccess)
+        return e;
+    rounds_init_kernel<NT><<<(unsigned)((R.ncells + RW - 1) / RW), RW * 32, slotSmem, st>>>(
+        P, R.ncells, O, state, listA, cA);
+    *R.launches += 2;
+    e = cudaMemcpyAsync(R.hostCount, cA, sizeof(unsigned int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess)
+        return e;
+    long long count = *R.hostCount;
+    long long rounds = 0;
+    while (count > 0) {
+        if (++rounds > R.maxRounds)
+            return cudaErrorLaunchTimeout;
+        e = cudaMemsetAsync(cB, 0, sizeof(unsigned int), st);
+        if (e != cudaSuccess)
+            return e;
+        for (long long off = 0; off < count; off += R.batch) {
+            int nb = (int)((count - off) < R.batch ? (count - off) : R.batch);
+            unsigned grid = (unsigned)((nb + RW - 1) / RW);
+            if (GAUNT)
+                rounds_pass_gaunt_kernel<NT, NT2><<<grid, RW * 32, passSmem, st>>>(
+                    P, R.chunks, listA + off, nb, state, R.buf, R.errorFlag);
+            else
+                rounds_pass_direct_kernel<NT><<<grid, RW * 32, passSmem, st>>>(
+                    P, R.chunks, listA + off, nb, state, R.buf, R.errorFlag);
+            rounds_newton_kernel<NT, NT2, GAUNT><<<grid, RW * 32, slotSmem, st>>>(
+                P, m0, listA + off, nb, state, R.buf, R.bRow, R.bCol, R.bVal, O, listB, cB);
+            *R.launches += 2;
+            e = cudaGetLastError();
+            if (e != cudaSuccess)
+                return e;
+        }
+        *R.launches += 1;
+        e = cudaMemcpyAsync(R.hostCount, cB, sizeof(unsigned int), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess)
+            e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess)
+            return e;
+        count = *R.hostCount;
+        int *t = listA;
+        listA = listB;
+        listB = t;
+        unsigned int *tc = cA;
+        cA = cB;
+        cB = tc;
+    }
+    return cudaSuccess;
+}
+
+cudaError_t launch_closure_rounds(const RoundsLaunch &R, bool gaunt)
+{
+    const int nm = R.P->nm;
+    if (gaunt) {
+        switch (nm) {
+        case 1: return rounds_t<1, 1, true>(R);
+        case 4: return rounds_t<1, 2, true>(R);
+        case 9: return rounds_t<2, 4, true>(R);
+        case 16: return rounds_t<2, 7, true>(R);
+        case 25: return rounds_t<4, 11, true>(R);
+        case 36: return rounds_t<5, 16, true>(R);
+        case 49: return rounds_t<7, 22, true>(R);
+        default: return cudaErrorInvalidValue;
+        }
+    }
+    switch ((nm + 7) / 8) {
+    case 1: return rounds_t<1, 1, false>(R);
+    case 2: return rounds_t<2, 1, false>(R);
+    case 3: return rounds_t<3, 1, false>(R);
+    case 4: return rounds_t<4, 1, false>(R);
+    case 5: return rounds_t<5, 1, false>(R);
+    case 6: return rounds_t<6, 1, false>(R);
+    case 7: return rounds_t<7, 1, false>(R);
+    case 8: return rounds_t<8, 1, false>(R);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+} // namespace c3d

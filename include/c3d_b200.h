@@ -102,6 +102,10 @@ typedef struct {
     long long totalIterGamma;
     long long failed;          /* cells with a non-zero status */
     long long trials;          /* line-search objective evaluations */
+    long long clkRefill;       /* SM clocks summed over warps: work-queue refill and set-up */
+    long long clkPass;         /* ... in passes over the staged basis (moments/Hessian/trials) */
+    long long clkSerial;       /* ... in the per-cell Newton logic between passes */
+    long long passes;          /* passes, summed over CTAs */
     long long regHist[16];     /* g_mnHistReg */
     long long iterHist[64];    /* cells per iteration count (last bin: >= 63) */
 } c3d_closure_stats;
@@ -154,6 +158,13 @@ c3d_status c3d_closure_stats_reset(c3d_ctx *ctx);
  * for the dense mode. NULL tables switch back to the direct form. N <= 6. */
 c3d_status c3d_set_gaunt(c3d_ctx *ctx, int nm2, const double *M2, const int *rowPtr,
                          const int *colInd, const double *val);
+
+/* Closure engine: 0 (default) runs rounds over a device work list -- a pass kernel for
+ * the quadrature sums of every listed cell, then a Newton kernel with one warp per cell,
+ * re-listing cells that need another pass (the reference's Optimization::opt stacks,
+ * src/opt/optBatch.cpp:350-472); 1 runs one persistent kernel whose warps pull cells
+ * from a device counter. Both compute the same per-cell arithmetic. */
+c3d_status c3d_set_engine(c3d_ctx *ctx, int engine);
 
 /* Standalone batched closure of n independent moment vectors (device
  * pointers u[n*nm], alpha[n*nm], solved in place; records may be NULL).

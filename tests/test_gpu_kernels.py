@@ -290,3 +290,25 @@ def test_gaunt_closure_matches_oracle(oracle, mode, N, Q):
     rel = np.linalg.norm(ag[ok] - ao[ok], axis=1) / np.linalg.norm(ao[ok], axis=1)
     assert rel.max() < 1e-10, rel.max()
     assert (out["totalIter"] > 1).sum() > 100
+
+
+@pytest.mark.parametrize("gaunt", [False, True])
+def test_engines_bit_identical(oracle, gaunt):
+    """Work-list rounds (engine 0) and the persistent kernel (engine 1) run the same per-cell
+    arithmetic, so multipliers, moments and iteration records agree bit for bit."""
+    S = _setup(oracle, N=2, Q=12, steps_before=2)
+    T = oracle.tables(2, 12, gaunt=True)
+    out = []
+    for engine in (0, 1):
+        ctx = _ctx(S)
+        ctx.set_engine(engine)
+        if gaunt:
+            row, col, val = _gaunt_csr(T, 1e-13)
+            ctx.set_gaunt(T["nm2"], T["M2"], row, col, val)
+        ctx.set_state(u=S["u"], alpha=S["alpha"], sig_t=S["sig"], sig_s=S["sig"])
+        ctx.step(S["dt"])
+        ctx.sync()
+        out.append(ctx.get_state() + (ctx.records()["iters"],))
+        ctx.close()
+    for a, b in zip(out[0], out[1]):
+        assert np.array_equal(a, b)
