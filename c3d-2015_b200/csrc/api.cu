@@ -614,7 +614,7 @@ c3d_status c3d_flux_kinetic(c3d_ctx *c, int alphaIsU)
                                  c->dx, c->dy, c->dz, c->theta, isPn, c->psi, c->flux, c->stream));
     timing_end(c, 1, t0);
     int nch = ceil_div(c->nq, c->qChunk);
-    c->launches += nch * (1 + ceil_div(c->qChunk, 64));
+    c->launches += 2 * nch;
     return C3D_OK;
 }
 

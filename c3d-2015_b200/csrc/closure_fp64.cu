@@ -125,12 +125,12 @@ __global__ void __launch_bounds__(W * 32, 1)
                 double z = 0.0;
                 for (int i = 0; i < nm; ++i)
                     z = __dadd_rn(z, __dmul_rn(sl.alpha[i], ch[i * QCP + lane]));
-                double e = exp(z);
-                double wq = ch[NMP * QCP + lane];
+                // c = w_q e^{z}; rounded product, then an unfused running sum (the same in
+                // every engine, whatever the compiler would contract)
+                double c = __dmul_rn(ch[NMP * QCP + lane], exp(z));
                 if (need == NEED_TRIAL) {
-                    fpart += wq * e;
+                    fpart = __dadd_rn(fpart, c);
                 } else {
-                    double c = wq * e;
 #pragma unroll
                     for (int g = 0; g < QC / 4; ++g) {
                         double cq = __shfl_sync(FULL_MASK, c, 4 * g + (lane & 3));
@@ -296,9 +296,9 @@ __global__ void __launch_bounds__(W * 32, 1)
                 double z = 0.0;
                 for (int i = 0; i < nm; ++i)
                     z = __dadd_rn(z, __dmul_rn(sl.alpha[i], ch[i * QCP + lane]));
-                c = ch[NM2P * QCP + lane] * exp(z);
+                c = __dmul_rn(ch[NM2P * QCP + lane], exp(z));
                 if (need == NEED_TRIAL)
-                    fpart += c;
+                    fpart = __dadd_rn(fpart, c);
             }
             cbuf[lane * CST + warp] = (need == NEED_H) ? c : 0.0;
             __syncthreads();

@@ -162,9 +162,9 @@ __global__ void __launch_bounds__(RW * 32, 2)
             double z = 0.0;
             for (int i = 0; i < nm; ++i)
                 z = __dadd_rn(z, __dmul_rn(al[i], ch[i * QCP + lane]));
-            c = ch[NM2P * QCP + lane] * exp(z);
+            c = __dmul_rn(ch[NM2P * QCP + lane], exp(z));
             if (need == NEED_TRIAL)
-                fpart += c;
+                fpart = __dadd_rn(fpart, c);
         }
         cbuf[lane * CST + warp] = (need == NEED_H) ? c : 0.0;
         __syncthreads();
@@ -269,9 +269,9 @@ __global__ void __launch_bounds__(RW * 32, 1)
             double z = 0.0;
             for (int i = 0; i < nm; ++i)
                 z = __dadd_rn(z, __dmul_rn(al[i], ch[i * QCP + lane]));
-            double c = ch[NMP * QCP + lane] * exp(z);
+            double c = __dmul_rn(ch[NMP * QCP + lane], exp(z));
             if (need == NEED_TRIAL) {
-                fpart += c;
+                fpart = __dadd_rn(fpart, c);
             } else {
 #pragma unroll
                 for (int g = 0; g < QC / 4; ++g) {

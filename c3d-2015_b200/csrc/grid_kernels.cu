@@ -276,6 +276,174 @@ __global__ void __launch_bounds__(128)
         flux[c * NM + m] = acc[m];
 }
 
+// ---------------------------------------------------------------- kinetic flux on the tensor pipe
+
+__device__ __forceinline__ void dmma_g(double &d0, double &d1, double a, double b)
+{
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+// psi[(q - q0) * nall + c] = exp(z) (M_N) or z (P_N) with z = alpha_c . m_q, for a tile of
+// 64 cells x 32 directions per CTA: Z = A M^T on the FP64 tensor pipe (m8n8k4; warp w owns
+// cells 8w..8w+7, four 8-direction tiles, K = moments in steps of 4).
+template <int NT>
+__global__ void __launch_bounds__(256)
+    ansatz_dmma_kernel(GridDims g, const double *__restrict__ alpha, const double *__restrict__ M,
+                       int q0, int nqc, int isPn, double *__restrict__ psi)
+{
+    constexpr int NMP = 8 * NT;
+    constexpr int KS = (NMP + 3) / 4;      // k-steps of 4 moments
+    constexpr int AS = 4 * KS + 4;         // row stride of the alpha tile (== 4 mod 16 doubles
+    constexpr int MS = 4 * KS + 4;         //   when 4*KS is a multiple of 16; conflict-light)
+    extern __shared__ double ansatzSmem[]; // sA[64 * AS], sM[32 * MS]
+    double *sA = ansatzSmem;
+    double *sM = ansatzSmem + 64 * AS;
+    const int nm = g.nm;
+    const long long nall = g.nall();
+    const long long c0 = (long long)blockIdx.x * 64;
+    const int qb = blockIdx.y * 32;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int e = tid; e < 64 * AS; e += 256) {
+        int r = e / AS, m = e % AS;
+        long long c = c0 + r;
+        sA[e] = (c < nall && m < nm) ? alpha[c * nm + m] : 0.0;
+    }
+    for (int e = tid; e < 32 * MS; e += 256) {
+        int r = e / MS, m = e % MS;
+        int q = qb + r;
+        sM[e] = (q < nqc && m < nm) ? M[(long long)(q0 + q) * nm + m] : 0.0;
+    }
+    __syncthreads();
+    double acc[4][2];
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+        acc[j][0] = acc[j][1] = 0.0;
+#pragma unroll
+    for (int kk = 0; kk < KS; ++kk) {
+        double a = sA[(8 * warp + (lane >> 2)) * AS + 4 * kk + (lane & 3)];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            double b = sM[(8 * j + (lane >> 2)) * MS + 4 * kk + (lane & 3)];
+            dmma_g(acc[j][0], acc[j][1], a, b);
+        }
+    }
+    const long long c = c0 + 8 * warp + (lane >> 2);
+    if (c >= nall)
+        return;
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+        for (int e2 = 0; e2 < 2; ++e2) {
+            int q = qb + 8 * j + 2 * (lane & 3) + e2;
+            if (q < nqc) {
+                double z = acc[j][e2];
+                psi[(long long)q * nall + c] = isPn ? z : exp(z);
+            }
+        }
+}
+
+// flux(c) (+)= sum_q m_q (Fx/dx + Fy/dy + Fz/dz) for 64 interior cells (consecutive in the
+// interior numbering) per CTA: per 32-direction chunk the limited upwind differences
+// S[q][cell] go to shared memory, then F += S^T M on the FP64 tensor pipe (warp w owns
+// cells 8w..8w+7 and every 8-moment tile).
+template <int NT>
+__global__ void __launch_bounds__(256)
+    kinetic_dmma_kernel(GridDims g, const double *__restrict__ psi, const double *__restrict__ M,
+                        const double *__restrict__ w, const double *__restrict__ xi,
+                        const double *__restrict__ eta, const double *__restrict__ mu, int q0,
+                        int nqc, double rdx, double rdy, double rdz, double theta,
+                        int accumulate, double *__restrict__ flux)
+{
+    constexpr int NMP = 8 * NT;
+    constexpr int CS = 68; // S tile row stride (cells)
+    constexpr int MS = NMP + 4 + ((NMP + 4) % 16 == 4 ? 0 : (20 - (NMP + 4) % 16) % 16);
+    __shared__ double sS[32 * CS];
+    __shared__ double sM[32 * MS];
+    __shared__ double sO[32 * 4];
+    __shared__ long long sCell[64];
+    const int nm = g.nm;
+    const long long nall = g.nall(), nint = g.ninterior();
+    const long long n0 = (long long)blockIdx.x * 64;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const long long sx = (long long)g.nyg() * g.nzg(), sy = g.nzg(), sz = 1;
+    if (tid < 64)
+        sCell[tid] = (n0 + tid < nint) ? interior_cell(g, n0 + tid) : -1;
+    double acc[NT][2];
+    const long long myc = n0 + 8 * warp + (lane >> 2);
+    __syncthreads();
+    if (accumulate && myc < nint) {
+        long long c = sCell[8 * warp + (lane >> 2)];
+#pragma unroll
+        for (int j = 0; j < NT; ++j)
+#pragma unroll
+            for (int e2 = 0; e2 < 2; ++e2) {
+                int m = 8 * j + 2 * (lane & 3) + e2;
+                acc[j][e2] = (m < nm) ? flux[c * nm + m] : 0.0;
+            }
+    } else {
+#pragma unroll
+        for (int j = 0; j < NT; ++j)
+            acc[j][0] = acc[j][1] = 0.0;
+    }
+    for (int qb = 0; qb < nqc; qb += 32) {
+        int nq = nqc - qb < 32 ? nqc - qb : 32;
+        __syncthreads();
+        for (int e = tid; e < 32 * MS; e += 256) {
+            int r = e / MS, m = e % MS;
+            sM[e] = (r < nq && m < nm) ? M[(long long)(q0 + qb + r) * nm + m] : 0.0;
+        }
+        if (tid < 32) {
+            int q = q0 + qb + tid;
+            bool ok = tid < nq;
+            sO[4 * tid + 0] = ok ? xi[q] : 0.0;
+            sO[4 * tid + 1] = ok ? eta[q] : 0.0;
+            sO[4 * tid + 2] = ok ? mu[q] : 0.0;
+            sO[4 * tid + 3] = ok ? w[q] : 0.0;
+        }
+        __syncthreads();
+        // stencil: thread handles cell (tid % 64) for directions tid/64 + 4i
+        {
+            const int cl = tid & 63;
+            const long long c = sCell[cl];
+            for (int qq = tid >> 6; qq < 32; qq += 4) {
+                double sv = 0.0;
+                if (c >= 0 && qq < nq) {
+                    const double *p = psi + (long long)(qb + qq) * nall;
+                    double wq = sO[4 * qq + 3];
+                    double fx = axis_flux(sO[4 * qq + 0], wq, theta, p, c, sx);
+                    double fy = axis_flux(sO[4 * qq + 1], wq, theta, p, c, sy);
+                    double fz = axis_flux(sO[4 * qq + 2], wq, theta, p, c, sz);
+                    sv = fx * rdx + fy * rdy + fz * rdz;
+                }
+                sS[qq * CS + cl] = sv;
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < 8; ++kk) {
+            double a = sS[(4 * kk + (lane & 3)) * CS + 8 * warp + (lane >> 2)];
+#pragma unroll
+            for (int j = 0; j < NT; ++j) {
+                double b = sM[(4 * kk + (lane & 3)) * MS + 8 * j + (lane >> 2)];
+                dmma_g(acc[j][0], acc[j][1], a, b);
+            }
+        }
+    }
+    if (myc >= nint)
+        return;
+    long long c = sCell[8 * warp + (lane >> 2)];
+#pragma unroll
+    for (int j = 0; j < NT; ++j)
+#pragma unroll
+        for (int e2 = 0; e2 < 2; ++e2) {
+            int m = 8 * j + 2 * (lane & 3) + e2;
+            if (m < nm)
+                flux[c * nm + m] = acc[j][e2];
+        }
+}
+
 // ---------------------------------------------------------------- P_N moment flux
 
 // One CTA handles CPB interior cells; phase 1 forms the six 4-point differences per
@@ -370,7 +538,7 @@ cudaError_t launch_rk(const GridDims &g, double *u, double *uOld, int mode, int 
     return cudaGetLastError();
 }
 
-template <int NM>
+template <int NT>
 static cudaError_t kinetic_t(const GridDims &g, const double *alpha, const double *M,
                              const double *w, const double *xi, const double *eta, const double *mu,
                              int nq, int qChunk, double dx, double dy, double dz, double theta,
@@ -378,17 +546,17 @@ static cudaError_t kinetic_t(const GridDims &g, const double *alpha, const doubl
 {
     for (int q0 = 0; q0 < nq; q0 += qChunk) {
         int nqc = nq - q0 < qChunk ? nq - q0 : qChunk;
-        // ansatz for directions [q0, q0+nqc), in sub-chunks sized for shared memory
-        const int sub = 64;
-        for (int s0 = 0; s0 < nqc; s0 += sub) {
-            int ns = nqc - s0 < sub ? nqc - s0 : sub;
-            size_t smA = ((size_t)ns * NM + 128 * NM) * sizeof(double);
-            cudaFuncSetAttribute(ansatz_kernel<NM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smA);
-            ansatz_kernel<NM><<<(int)((g.nall() + 127) / 128), 128, smA, st>>>(
-                g, alpha, M, q0 + s0, ns, isPn, psi + (long long)s0 * g.nall());
+        dim3 ga((unsigned)((g.nall() + 63) / 64), (unsigned)((nqc + 31) / 32));
+        constexpr int KS = (8 * NT + 3) / 4;
+        const size_t smem = (size_t)(64 + 32) * (4 * KS + 4) * sizeof(double);
+        if (smem > 48 * 1024) {
+            cudaError_t e = cudaFuncSetAttribute(ansatz_dmma_kernel<NT>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess)
+                return e;
         }
-        kinetic_stencil_kernel<NM><<<(int)((g.ninterior() + 127) / 128), 128, 0, st>>>(
+        ansatz_dmma_kernel<NT><<<ga, 256, smem, st>>>(g, alpha, M, q0, nqc, isPn, psi);
+        kinetic_dmma_kernel<NT><<<(unsigned)((g.ninterior() + 63) / 64), 256, 0, st>>>(
             g, psi, M, w, xi, eta, mu, q0, nqc, 1.0 / dx, 1.0 / dy, 1.0 / dz, theta, q0 > 0 ? 1 : 0,
             flux);
         cudaError_t e = cudaGetLastError();
@@ -404,23 +572,23 @@ cudaError_t launch_kinetic_flux(const GridDims &g, const double *alpha, const do
                                 double dz, double theta, int isPn, double *psi, double *flux,
                                 cudaStream_t st)
 {
-#define C3D_NM_CASE(N)                                                                             \
-    case N:                                                                                        \
-        return kinetic_t<N>(g, alpha, M, w, xi, eta, mu, nq, qChunk, dx, dy, dz, theta, isPn, psi, \
-                            flux, st);
-    switch (g.nm) {
-        C3D_NM_CASE(1)
-        C3D_NM_CASE(4)
-        C3D_NM_CASE(9)
-        C3D_NM_CASE(16)
-        C3D_NM_CASE(25)
-        C3D_NM_CASE(36)
-        C3D_NM_CASE(49)
-        C3D_NM_CASE(64)
+#define C3D_NT_CASE(NT)                                                                            \
+    case NT:                                                                                       \
+        return kinetic_t<NT>(g, alpha, M, w, xi, eta, mu, nq, qChunk, dx, dy, dz, theta, isPn,     \
+                             psi, flux, st);
+    switch ((g.nm + 7) / 8) {
+        C3D_NT_CASE(1)
+        C3D_NT_CASE(2)
+        C3D_NT_CASE(3)
+        C3D_NT_CASE(4)
+        C3D_NT_CASE(5)
+        C3D_NT_CASE(6)
+        C3D_NT_CASE(7)
+        C3D_NT_CASE(8)
     default:
         return cudaErrorInvalidValue;
     }
-#undef C3D_NM_CASE
+#undef C3D_NT_CASE
 }
 
 // Directions per materialised-ansatz chunk (bounded by the HBM budget only).
