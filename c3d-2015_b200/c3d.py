@@ -55,7 +55,8 @@ class ClosureStats(ctypes.Structure):
                 ("clkRefill", ctypes.c_longlong), ("clkPass", ctypes.c_longlong),
                 ("clkSerial", ctypes.c_longlong), ("passes", ctypes.c_longlong),
                 ("regHist", ctypes.c_longlong * 16),
-                ("iterHist", ctypes.c_longlong * 64)]
+                ("iterHist", ctypes.c_longlong * 64),
+                ("clkNewton", ctypes.c_longlong * 4)]
 
 
 _lib = None

@@ -727,6 +727,8 @@ c3d_status c3d_closure_stats_get(c3d_ctx *c, c3d_closure_stats *st)
         st->regHist[i] = (long long)h[STAT_REG_HIST + i];
     for (int i = 0; i < 64; ++i)
         st->iterHist[i] = (long long)h[STAT_ITER_HIST + i];
+    for (int i = 0; i < 4; ++i)
+        st->clkNewton[i] = (long long)h[STAT_CLK_NEWTON + i];
     return C3D_OK;
 }
 

@@ -36,6 +36,8 @@ enum StatSlot : int {
     STAT_CLK_PASS = 25,   // passes over the staged basis
     STAT_CLK_SERIAL = 26, // per-cell Newton logic after each pass
     STAT_PASSES = 27,     // passes (per CTA)
+    STAT_CLK_NEWTON = 28, // 4 slots, builds with C3D_NEWTON_CLOCKS only: SM clocks of the
+                          // Newton kernel's H assembly, g/f/norms, Cholesky, and the rest
     STAT_ITER_HIST = 32, // 64 bins (last: >= 63)
     STAT_COUNT = 96,
 };

@@ -22,6 +22,21 @@ constexpr double EPS_HALF = DBL_EPSILON / 2;
 
 enum Need : int { NEED_NONE = 0, NEED_H = 1, NEED_TRIAL = 2 };
 
+// Phase clocks of the per-cell Newton logic (profiling builds only).
+#ifdef C3D_NEWTON_CLOCKS
+#define C3D_NCLK_DECL long long nclk_ = clock64();
+#define C3D_NCLK(stats, slot, lane)                                                                \
+    do {                                                                                           \
+        long long t_ = clock64();                                                                  \
+        if ((lane) == 0 && (stats))                                                                \
+            atomicAdd(&(stats)[STAT_CLK_NEWTON + (slot)], (unsigned long long)(t_ - nclk_));       \
+        nclk_ = t_;                                                                                \
+    } while (0)
+#else
+#define C3D_NCLK_DECL
+#define C3D_NCLK(stats, slot, lane)
+#endif
+
 struct SlotScalars {
     long long cell;
     long long passes;
@@ -44,14 +59,34 @@ template <int NT> struct Cfg {
     static constexpr int NTILE = NT * (NT + 1) / 2;
 };
 
-template <int NT> struct Slot {
-    static constexpr int NMP = Cfg<NT>::NMP;
-    double u[NMP], alpha[NMP], alpha0[NMP], uOrig[NMP], g[NMP], d[NMP], alphaOld[NMP], rinv[NMP];
-    double L[Cfg<NT>::NPK];
-    SlotScalars s;
-};
+__host__ __device__ constexpr int pidx(int i, int j) { return (i * (i + 1)) / 2 + j; }
 
-__device__ __forceinline__ int pidx(int i, int j) { return (i * (i + 1)) / 2 + j; }
+// Tile (ib, jb), ib >= jb, of the lower triangle of 8x8 tiles, in row order.
+__host__ __device__ constexpr int tix(int ib, int jb) { return ib * (ib + 1) / 2 + jb; }
+
+// Per-warp state of one cell. The lower triangle of H (then of its Cholesky factor L) is
+// either packed row by row (TILED = false) or stored as the lower triangle of 8x8 tiles of
+// the matrix padded to 8 NT rows (TILED = true): tile (ib, jb) at 64 tix(ib, jb), row-major
+// inside the tile, which is also the accumulator layout of the m8n8k4 DMMA (lane l holds
+// elements 2l and 2l + 1). Padding rows are those of the identity. 16-byte alignment keeps
+// L of every slot in an array aligned for the double2 tile accesses.
+template <int NT, bool TILED = false> struct alignas(16) Slot {
+    static constexpr int NMP = Cfg<NT>::NMP;
+    static constexpr int NTILES = NT * (NT + 1) / 2;
+    static constexpr int LSIZE = TILED ? 64 * NTILES : Cfg<NT>::NPK;
+    static constexpr bool tiled = TILED;
+    static constexpr int nt = NT;
+    double u[NMP], alpha[NMP], alpha0[NMP], uOrig[NMP], g[NMP], d[NMP], alphaOld[NMP], rinv[NMP];
+    double L[LSIZE];
+    SlotScalars s;
+    // offset of element (i, j), i >= j
+    __device__ static __forceinline__ int lx(int i, int j)
+    {
+        if (TILED)
+            return 64 * tix(i >> 3, j >> 3) + 8 * (i & 7) + (j & 7);
+        return pidx(i, j);
+    }
+};
 
 __device__ __forceinline__ double warp_sum(double v)
 {
@@ -147,8 +182,8 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
 // ---------------------------------------------------------------- per-warp linear algebra
 
 // In-place right-looking Cholesky of the packed lower triangle; returns LAPACK info.
-template <int NT>
-__device__ int warp_cholesky(Slot<NT> &sl, int n, int lane)
+template <class S>
+__device__ int warp_cholesky_packed(S &sl, int n, int lane)
 {
     double *P = sl.L;
     for (int j = 0; j < n; ++j) {
@@ -185,19 +220,118 @@ __device__ int warp_cholesky(Slot<NT> &sl, int n, int lane)
     return 0;
 }
 
+// Blocked Cholesky of the tiled lower triangle (Slot<NT, true>); returns LAPACK info.
+// Per tile column kb: the 8 columns of the panel (diagonal tile and the tiles below it,
+// in registers, lane l holding elements 2l, 2l+1 of each) are factored right-looking with
+// warp shuffles; the trailing tiles (ib, jb), kb < jb <= ib, then receive
+// -L(ib,kb) L(jb,kb)^T as two m8n8k4 DMMAs each (the panel tiles in operand layout:
+// lane l holds L[l/4][4s + l%4] for k-step s, which is the A fragment of L(ib,kb) and the
+// B fragment of L(jb,kb)^T).
+template <class S>
+__device__ int warp_cholesky_tiled(S &sl, int n, int lane)
+{
+    constexpr int T = S::nt;
+    static_assert(sizeof(S) % 16 == 0 && (8 * 8 * S::NMP) % 16 == 0,
+                  "tiles must be 16-byte aligned in every slot");
+    double *A = sl.L;
+    const int r = lane >> 2, q = lane & 3;
+    const int c0 = 2 * q, c1 = 2 * q + 1;
+    int info = 0;
+#pragma unroll
+    for (int kb = 0; kb < T; ++kb) {
+        double p0[T], p1[T];
+#pragma unroll
+        for (int t = kb; t < T; ++t) {
+            double2 v = *reinterpret_cast<const double2 *>(&A[64 * tix(t, kb) + 2 * lane]);
+            p0[t] = v.x;
+            p1[t] = v.y;
+        }
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const int src = 4 * j + (j >> 1);
+            double ajj = __shfl_sync(FULL_MASK, (j & 1) ? p1[kb] : p0[kb], src);
+            // warp-uniform; padding pivots are 1. The loops run to the end (and then hold
+            // NaNs) so that they unroll completely and the panel stays in registers.
+            if (!(ajj > 0.0) && info == 0)
+                info = 8 * kb + j + 1;
+            double ljj = sqrt(ajj);
+            double rj = 1.0 / ljj;
+            // column j: the pivot, then the rows below it scaled by 1/L_jj
+            if (q == (j >> 1)) {
+                double &dv = (j & 1) ? p1[kb] : p0[kb];
+                if (r == j)
+                    dv = ljj;
+                else if (r > j)
+                    dv *= rj;
+#pragma unroll
+                for (int t = kb + 1; t < T; ++t) {
+                    double &v = (j & 1) ? p1[t] : p0[t];
+                    v *= rj;
+                }
+            }
+            // L(c, j) of the diagonal tile for this lane's columns c0, c1
+            double lc0 = __shfl_sync(FULL_MASK, (j & 1) ? p1[kb] : p0[kb], 4 * c0 + (j >> 1));
+            double lc1 = __shfl_sync(FULL_MASK, (j & 1) ? p1[kb] : p0[kb], 4 * c1 + (j >> 1));
+#pragma unroll
+            for (int t = kb; t < T; ++t) {
+                double lrj = __shfl_sync(FULL_MASK, (j & 1) ? p1[t] : p0[t], 4 * r + (j >> 1));
+                bool ok0 = c0 > j && (t > kb || c0 <= r);
+                bool ok1 = c1 > j && (t > kb || c1 <= r);
+                if (ok0)
+                    p0[t] = fma(-lrj, lc0, p0[t]);
+                if (ok1)
+                    p1[t] = fma(-lrj, lc1, p1[t]);
+            }
+        }
+        double f0[T], f1[T];
+#pragma unroll
+        for (int t = kb; t < T; ++t) {
+            *reinterpret_cast<double2 *>(&A[64 * tix(t, kb) + 2 * lane]) = make_double2(p0[t], p1[t]);
+            double x0 = __shfl_sync(FULL_MASK, p0[t], 4 * r + (q >> 1));
+            double x1 = __shfl_sync(FULL_MASK, p1[t], 4 * r + (q >> 1));
+            double y0 = __shfl_sync(FULL_MASK, p0[t], 4 * r + 2 + (q >> 1));
+            double y1 = __shfl_sync(FULL_MASK, p1[t], 4 * r + 2 + (q >> 1));
+            f0[t] = (q & 1) ? x1 : x0;
+            f1[t] = (q & 1) ? y1 : y0;
+        }
+#pragma unroll
+        for (int jb = kb + 1; jb < T; ++jb)
+#pragma unroll
+            for (int ib = jb; ib < T; ++ib) {
+                double2 *cp = reinterpret_cast<double2 *>(&A[64 * tix(ib, jb) + 2 * lane]);
+                double2 c = *cp;
+                dmma(c.x, c.y, -f0[ib], f0[jb]);
+                dmma(c.x, c.y, -f1[ib], f1[jb]);
+                *cp = c;
+            }
+        __syncwarp();
+    }
+    (void)n;
+    return info;
+}
+
+template <class S>
+__device__ __forceinline__ int warp_cholesky(S &sl, int n, int lane)
+{
+    if constexpr (S::tiled)
+        return warp_cholesky_tiled(sl, n, lane);
+    else
+        return warp_cholesky_packed(sl, n, lane);
+}
+
 // x <- (L L^T)^{-1} x, x distributed as x0 = x[lane], x1 = x[lane+32]; column-oriented
 // substitution (the order of the reference BLAS dtrsv and of src/utils.cpp:71-86).
 // exactDiv selects division by L_kk (as the reference's own dpotrs) instead of the
 // precomputed reciprocal.
-template <int NT>
-__device__ void warp_apply_inverse(const Slot<NT> &sl, int n, int lane, double &x0, double &x1,
+template <class S>
+__device__ void warp_apply_inverse(const S &sl, int n, int lane, double &x0, double &x1,
                                    bool exactDiv)
 {
     const double *P = sl.L;
     for (int k = 0; k < n; ++k) {
         double v = (k < 32) ? x0 : x1;
         double xk = __shfl_sync(FULL_MASK, v, k & 31);
-        xk = exactDiv ? xk / P[pidx(k, k)] : xk * sl.rinv[k];
+        xk = exactDiv ? xk / P[S::lx(k, k)] : xk * sl.rinv[k];
         if (lane == (k & 31)) {
             if (k < 32)
                 x0 = xk;
@@ -205,14 +339,14 @@ __device__ void warp_apply_inverse(const Slot<NT> &sl, int n, int lane, double &
                 x1 = xk;
         }
         if (lane > k && lane < n)
-            x0 = fma(-P[pidx(lane, k)], xk, x0);
+            x0 = fma(-P[S::lx(lane, k)], xk, x0);
         if (lane + 32 > k && lane + 32 < n)
-            x1 = fma(-P[pidx(lane + 32, k)], xk, x1);
+            x1 = fma(-P[S::lx(lane + 32, k)], xk, x1);
     }
     for (int k = n - 1; k >= 0; --k) {
         double v = (k < 32) ? x0 : x1;
         double xk = __shfl_sync(FULL_MASK, v, k & 31);
-        xk = exactDiv ? xk / P[pidx(k, k)] : xk * sl.rinv[k];
+        xk = exactDiv ? xk / P[S::lx(k, k)] : xk * sl.rinv[k];
         if (lane == (k & 31)) {
             if (k < 32)
                 x0 = xk;
@@ -220,9 +354,9 @@ __device__ void warp_apply_inverse(const Slot<NT> &sl, int n, int lane, double &
                 x1 = xk;
         }
         if (lane < k && lane < n)
-            x0 = fma(-P[pidx(k, lane)], xk, x0);
+            x0 = fma(-P[S::lx(k, lane)], xk, x0);
         if (lane + 32 < k && lane + 32 < n)
-            x1 = fma(-P[pidx(k, lane + 32)], xk, x1);
+            x1 = fma(-P[S::lx(k, lane + 32)], xk, x1);
     }
 }
 
@@ -235,8 +369,8 @@ __device__ __forceinline__ double vsum_abs(double x0, double x1, int lane, int n
 // Hager/Higham 1-norm estimate of (L L^T)^{-1} (N. J. Higham, ACM TOMS 14 (1988)
 // 381-396, Alg. 4.1 -- the algorithm of LAPACK's dlacn2 as driven by dpocon).
 // Returns 1/rcond with rcond = (1/est)/anorm.
-template <int NT>
-__device__ double warp_condest(const Slot<NT> &sl, int n, int lane, double anorm)
+template <class S>
+__device__ double warp_condest(const S &sl, int n, int lane, double anorm)
 {
     if (anorm == 0.0)
         return 1.0 / 0.0;
@@ -311,8 +445,8 @@ struct Outputs {
     unsigned long long *stats;     // running counters, layout STAT_* (may be null)
 };
 
-template <int NT>
-__device__ void finalize(Slot<NT> &sl, const ClosureParams &P, const Outputs &O, int lane)
+template <class S>
+__device__ void finalize(S &sl, const ClosureParams &P, const Outputs &O, int lane)
 {
     const int nm = P.nm;
     long long c = sl.s.cell;
@@ -354,8 +488,8 @@ __device__ void finalize(Slot<NT> &sl, const ClosureParams &P, const Outputs &O,
 }
 
 // Regularise (src/opt/opt.cpp:251-279). Returns false if the ladder is exhausted.
-template <int NT>
-__device__ bool regularize(Slot<NT> &sl, const ClosureParams &P, int lane)
+template <class S>
+__device__ bool regularize(S &sl, const ClosureParams &P, int lane)
 {
     const int nm = P.nm;
     __syncwarp();
@@ -387,8 +521,8 @@ __device__ bool regularize(Slot<NT> &sl, const ClosureParams &P, int lane)
 // Starts the next Newton iteration. When the iteration is bound to regularise
 // whatever H turns out to be (t == 0 after a failed line search, or the
 // iteration cap reached), the regularisation is applied here without the H pass.
-template <int NT>
-__device__ void begin_iteration(Slot<NT> &sl, const ClosureParams &P, const Outputs &O, int lane)
+template <class S>
+__device__ void begin_iteration(S &sl, const ClosureParams &P, const Outputs &O, int lane)
 {
     for (;;) {
         __syncwarp();
@@ -426,12 +560,12 @@ __device__ void begin_iteration(Slot<NT> &sl, const ClosureParams &P, const Outp
     }
 }
 
-template <int NT>
-__device__ void load_cell(Slot<NT> &sl, const ClosureParams &P, const Outputs &O, long long c,
+template <class S>
+__device__ void load_cell(S &sl, const ClosureParams &P, const Outputs &O, long long c,
                           int lane)
 {
     const int nm = P.nm;
-    constexpr int NMP = Cfg<NT>::NMP;
+    constexpr int NMP = S::NMP;
     double u0 = O.u[c * nm];
     double alphaScale = log(u0) * 2.0 * sqrt(M_PI);
     for (int i = lane; i < NMP; i += 32) {
@@ -479,11 +613,11 @@ __device__ void load_cell(Slot<NT> &sl, const ClosureParams &P, const Outputs &O
 }
 
 // Sets alpha = alphaOld + t d and requests a trial pass, or gives up with t = 0.
-template <int NT>
-__device__ void next_trial(Slot<NT> &sl, const ClosureParams &P, const Outputs &O, int lane);
+template <class S>
+__device__ void next_trial(S &sl, const ClosureParams &P, const Outputs &O, int lane);
 
-template <int NT>
-__device__ void next_trial(Slot<NT> &sl, const ClosureParams &P, const Outputs &O, int lane)
+template <class S>
+__device__ void next_trial(S &sl, const ClosureParams &P, const Outputs &O, int lane)
 {
     const int nm = P.nm;
     double t = sl.s.t;
@@ -510,14 +644,15 @@ __device__ void next_trial(Slot<NT> &sl, const ClosureParams &P, const Outputs &
     }
 }
 
-template <int NT>
-__device__ void after_hessian(Slot<NT> &sl, const ClosureParams &P, const Outputs &O, int lane,
+template <class S>
+__device__ void after_hessian(S &sl, const ClosureParams &P, const Outputs &O, int lane,
                               double m0)
 {
     const int nm = P.nm;
+    C3D_NCLK_DECL
     // g_i = H_i0 / m_0 - u_i ; f = H_00 / m_0^2 - alpha.u  (src/opt/fobj.cpp:121-129)
     for (int i = lane; i < nm; i += 32)
-        sl.g[i] = sl.L[pidx(i, 0)] / m0 - sl.u[i];
+        sl.g[i] = sl.L[S::lx(i, 0)] / m0 - sl.u[i];
     __syncwarp();
     double f = 0.0;
     if (lane == 0) {
@@ -531,9 +666,9 @@ __device__ void after_hessian(Slot<NT> &sl, const ClosureParams &P, const Output
     for (int i = lane; i < nm; i += 32) {
         double s = 0.0;
         for (int j = 0; j < nm; ++j)
-            s += fabs(j <= i ? sl.L[pidx(i, j)] : sl.L[pidx(j, i)]);
+            s += fabs(j <= i ? sl.L[S::lx(i, j)] : sl.L[S::lx(j, i)]);
         rs = fmax(rs, s);
-        gmin = fmin(gmin, 2.0 * sl.L[pidx(i, i)] - s); // Gershgorin: H_ii - sum_{j!=i} |H_ij|
+        gmin = fmin(gmin, 2.0 * sl.L[S::lx(i, i)] - s); // Gershgorin: H_ii - sum_{j!=i} |H_ij|
     }
     double norm1 = warp_max(rs);
     gmin = -warp_max(-gmin);
@@ -543,11 +678,13 @@ __device__ void after_hessian(Slot<NT> &sl, const ClosureParams &P, const Output
     // is false whatever the estimate; the estimate is then skipped.
     bool condSure = gmin > 0.0 && norm1 * sqrt((double)nm) / gmin <= 0.5 * P.condHMax;
     __syncwarp();
+    C3D_NCLK(O.stats, 1, lane);
     int info = warp_cholesky(sl, nm, lane);
+    C3D_NCLK(O.stats, 2, lane);
     double cond = 0.0;
     if (info == 0) {
         for (int i = lane; i < nm; i += 32)
-            sl.rinv[i] = 1.0 / sl.L[pidx(i, i)];
+            sl.rinv[i] = 1.0 / sl.L[S::lx(i, i)];
         __syncwarp();
         if (!condSure)
             cond = warp_condest(sl, nm, lane, norm1);
@@ -634,8 +771,8 @@ __device__ void after_hessian(Slot<NT> &sl, const ClosureParams &P, const Output
     next_trial(sl, P, O, lane);
 }
 
-template <int NT>
-__device__ void after_trial(Slot<NT> &sl, const ClosureParams &P, const Outputs &O, int lane,
+template <class S>
+__device__ void after_trial(S &sl, const ClosureParams &P, const Outputs &O, int lane,
                             double fquad)
 {
     const int nm = P.nm;

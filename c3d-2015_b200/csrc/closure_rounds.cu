@@ -30,8 +30,8 @@ template <int NT> struct CellState {
 
 namespace {
 
-template <int NT>
-__device__ void state_to_slot(const CellState<NT> &st, Slot<NT> &sl, int lane)
+template <int NT, class S>
+__device__ void state_to_slot(const CellState<NT> &st, S &sl, int lane)
 {
     constexpr int NMP = Cfg<NT>::NMP;
     for (int i = lane; i < NMP; i += 32) {
@@ -48,8 +48,8 @@ __device__ void state_to_slot(const CellState<NT> &st, Slot<NT> &sl, int lane)
     __syncwarp();
 }
 
-template <int NT>
-__device__ void slot_to_state(const Slot<NT> &sl, CellState<NT> &st, int lane)
+template <int NT, class S>
+__device__ void slot_to_state(const S &sl, CellState<NT> &st, int lane)
 {
     constexpr int NMP = Cfg<NT>::NMP;
     __syncwarp();
@@ -67,8 +67,8 @@ __device__ void slot_to_state(const Slot<NT> &sl, CellState<NT> &st, int lane)
 }
 
 // Appends cell c to the list when it still needs a pass.
-template <int NT>
-__device__ void append_if_needed(const Slot<NT> &sl, long long c, int lane, int *listOut,
+template <class S>
+__device__ void append_if_needed(const S &sl, long long c, int lane, int *listOut,
                                  unsigned int *countOut)
 {
     if (lane == 0 && sl.s.need != NEED_NONE) {
@@ -79,7 +79,10 @@ __device__ void append_if_needed(const Slot<NT> &sl, long long c, int lane, int 
 
 } // namespace
 
-constexpr int RW = 8; // warps (cells) per CTA in every round kernel
+constexpr int RW = 8;  // warps (cells) per CTA of the init and pass kernels
+constexpr int RWN = 4; // warps (cells) per CTA of the Newton kernel
+
+template <int NT> using TSlot = Slot<NT, true>;
 
 template <int NT>
 __global__ void __launch_bounds__(RW * 32)
@@ -218,7 +221,6 @@ __global__ void __launch_bounds__(RW * 32, 1)
                               double *__restrict__ hBuf, int *errorFlag)
 {
     constexpr int NMP = Cfg<NT>::NMP;
-    constexpr int NPK = Cfg<NT>::NPK;
     constexpr int CH = Cfg<NT>::CHUNK;
     constexpr int ST = 3;
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -298,18 +300,20 @@ __global__ void __launch_bounds__(RW * 32, 1)
         }
     }
     if (need == NEED_H) {
-        double *H = hBuf + (size_t)pos * NPK;
+        // tiles of the padded H, identity in the padding rows
+        double *H = hBuf + (size_t)pos * TSlot<NT>::LSIZE;
 #pragma unroll
         for (int I = 0; I < NT; ++I)
 #pragma unroll
             for (int J = 0; J <= I; ++J) {
-                int row = 8 * I + (lane >> 2);
-#pragma unroll
-                for (int e2 = 0; e2 < 2; ++e2) {
-                    int col = 8 * J + 2 * (lane & 3) + e2;
-                    if (row < nm && col < nm && col <= row)
-                        H[pidx(row, col)] = acc[I * (I + 1) / 2 + J][e2];
-                }
+                const int t = I * (I + 1) / 2 + J;
+                int row = 8 * I + (lane >> 2), col = 8 * J + 2 * (lane & 3);
+                double v0 = acc[t][0], v1 = acc[t][1];
+                if (row >= nm || col >= nm)
+                    v0 = (row == col) ? 1.0 : 0.0;
+                if (row >= nm || col + 1 >= nm)
+                    v1 = (row == col + 1) ? 1.0 : 0.0;
+                *reinterpret_cast<double2 *>(&H[64 * t + 2 * lane]) = make_double2(v0, v1);
             }
     } else if (need == NEED_TRIAL) {
         double fq = warp_sum(fpart);
@@ -318,11 +322,14 @@ __global__ void __launch_bounds__(RW * 32, 1)
     }
 }
 
-// Newton logic for the listed cells: one warp per cell, state staged in shared memory.
-// GAUNT: H_ij (i >= j) from the CSR of beta over the cell's moments (momBuf);
-// otherwise H packed in hBuf.
+// Newton logic for the listed cells: one warp per cell, RWN cells per CTA, state staged
+// in shared memory with H in the tiled layout (TSlot).
+// GAUNT: the CTA assembles H_ij = sum_k beta_ijk mom_k (i >= j, CSR of beta in the order of
+// src/opt/fobj.cpp:81-99) for its cells that need a Hessian in one sweep over the tile
+// elements, so that each CSR term is read once for RWN cells; otherwise the pass wrote H in
+// tiles to hBuf.
 template <int NT, int NT2, bool GAUNT>
-__global__ void __launch_bounds__(RW * 32, 2)
+__global__ void __launch_bounds__(RWN * 32)
     rounds_newton_kernel(ClosureParams P, double m0, const int *__restrict__ list, int n,
                          CellState<NT> *state, const double *__restrict__ buf,
                          const int *__restrict__ bRow, const int *__restrict__ bCol,
@@ -330,50 +337,84 @@ __global__ void __launch_bounds__(RW * 32, 2)
                          unsigned int *countOut)
 {
     constexpr int NM2P = 8 * NT2;
-    constexpr int NPK = Cfg<NT>::NPK;
+    constexpr int LS = TSlot<NT>::LSIZE;
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    Slot<NT> *slots = reinterpret_cast<Slot<NT> *>(smem_raw);
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int pos = blockIdx.x * RW + warp;
-    if (pos >= n)
-        return;
-    const long long cell = list[pos];
-    Slot<NT> &sl = slots[warp];
-    state_to_slot(state[cell], sl, lane);
-    const int nm = P.nm;
-    const int npk = nm * (nm + 1) / 2;
-    if (sl.s.need == NEED_H) {
-        if (GAUNT) {
-            const double *mw = buf + (size_t)pos * NM2P;
-            int ii = 0, jj = lane;
-            while (jj > ii) {
-                jj -= ii + 1;
-                ++ii;
-            }
-            for (int e = lane; e < npk; e += 32) {
-                int idx = jj * nm + ii;
-                double h = 0.0;
-                for (int t = bRow[idx]; t < bRow[idx + 1]; ++t)
-                    h = __dadd_rn(h, __dmul_rn(mw[bCol[t]], bVal[t]));
-                sl.L[e] = h;
-                jj += 32;
-                while (jj > ii) {
-                    jj -= ii + 1;
-                    ++ii;
-                }
-            }
-        } else {
-            const double *H = buf + (size_t)pos * NPK;
-            for (int e = lane; e < npk; e += 32)
-                sl.L[e] = H[e];
-        }
-        __syncwarp();
-        after_hessian(sl, P, O, lane, m0);
-    } else if (sl.s.need == NEED_TRIAL) {
-        after_trial(sl, P, O, lane, sl.s.fquad);
+    TSlot<NT> *slots = reinterpret_cast<TSlot<NT> *>(smem_raw);
+    double *sMom = reinterpret_cast<double *>(slots + RWN); // RWN x NM2P (GAUNT)
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int pos = blockIdx.x * RWN + warp;
+    const bool active = pos < n;
+    const long long cell = active ? list[pos] : -1;
+    TSlot<NT> &sl = slots[warp];
+    C3D_NCLK_DECL
+    if (active) {
+        state_to_slot(state[cell], sl, lane);
+    } else if (lane == 0) {
+        sl.s.need = NEED_NONE;
     }
+    const int nm = P.nm;
+    const bool needH = active && sl.s.need == NEED_H;
+    if (GAUNT) {
+        for (int k = lane; k < NM2P; k += 32)
+            sMom[warp * NM2P + k] = needH ? buf[(size_t)pos * NM2P + k] : 0.0;
+        __syncthreads();
+        if (__syncthreads_or(needH)) {
+            bool hw[RWN];
+#pragma unroll
+            for (int w = 0; w < RWN; ++w)
+                hw[w] = slots[w].s.need == NEED_H;
+            for (int e = tid; e < LS; e += RWN * 32) {
+                const int t = e >> 6, rr = (e >> 3) & 7, cc = e & 7;
+                int ib = 0;
+                while (tix(ib + 1, 0) <= t)
+                    ++ib;
+                const int jb = t - tix(ib, 0);
+                const int i = 8 * ib + rr, j = 8 * jb + cc;
+                double h[RWN];
+#pragma unroll
+                for (int w = 0; w < RWN; ++w)
+                    h[w] = 0.0;
+                if (ib == jb && cc > rr) {
+                    // upper half of a diagonal tile: unused
+                } else if (i >= nm || j >= nm) {
+#pragma unroll
+                    for (int w = 0; w < RWN; ++w)
+                        h[w] = (i == j) ? 1.0 : 0.0;
+                } else {
+                    const int idx = j * nm + i;
+                    const int tEnd = bRow[idx + 1];
+                    for (int tt = bRow[idx]; tt < tEnd; ++tt) {
+                        const int col = bCol[tt];
+                        const double v = bVal[tt];
+#pragma unroll
+                        for (int w = 0; w < RWN; ++w)
+                            h[w] = __dadd_rn(h[w], __dmul_rn(sMom[w * NM2P + col], v));
+                    }
+                }
+#pragma unroll
+                for (int w = 0; w < RWN; ++w)
+                    if (hw[w])
+                        slots[w].L[e] = h[w];
+            }
+        }
+        __syncthreads();
+    } else if (needH) {
+        const double2 *H = reinterpret_cast<const double2 *>(buf + (size_t)pos * LS);
+        double2 *L = reinterpret_cast<double2 *>(sl.L);
+        for (int e = lane; e < LS / 2; e += 32)
+            L[e] = H[e];
+        __syncwarp();
+    }
+    if (!active)
+        return;
+    C3D_NCLK(O.stats, 0, lane);
+    if (sl.s.need == NEED_H)
+        after_hessian(sl, P, O, lane, m0);
+    else if (sl.s.need == NEED_TRIAL)
+        after_trial(sl, P, O, lane, sl.s.fquad);
     slot_to_state(sl, state[cell], lane);
     append_if_needed(sl, cell, lane, listOut, countOut);
+    C3D_NCLK(O.stats, 3, lane);
 }
 
 // ---------------------------------------------------------------- host side
@@ -421,8 +462,8 @@ size_t rounds_buf_doubles(int nm, int nm2, bool gaunt)
 {
     if (gaunt)
         return (size_t)8 * ((nm2 + 7) / 8);
-    int nml = max_nm_for((nm + 7) / 8);
-    return (size_t)nml * (nml + 1) / 2; // the template's packed triangle
+    const int nt = (nm + 7) / 8;
+    return (size_t)64 * nt * (nt + 1) / 2; // the tiled lower triangle
 }
 
 template <int NT, int NT2, bool GAUNT> static cudaError_t rounds_t(const RoundsLaunch &R)
@@ -436,8 +477,9 @@ template <int NT, int NT2, bool GAUNT> static cudaError_t rounds_t(const RoundsL
                              (int)slotSmem);
     if (e != cudaSuccess)
         return e;
+    size_t newtonSmem = RWN * sizeof(TSlot<NT>) + (GAUNT ? (size_t)RWN * 8 * NT2 * 8 : 0);
     e = cudaFuncSetAttribute(rounds_newton_kernel<NT, NT2, GAUNT>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)slotSmem);
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)newtonSmem);
     if (e != cudaSuccess)
         return e;
     size_t passSmem;
@@ -488,7 +530,8 @@ template <int NT, int NT2, bool GAUNT> static cudaError_t rounds_t(const RoundsL
             else
                 rounds_pass_direct_kernel<NT><<<grid, RW * 32, passSmem, st>>>(
                     P, R.chunks, listA + off, nb, state, R.buf, R.errorFlag);
-            rounds_newton_kernel<NT, NT2, GAUNT><<<grid, RW * 32, slotSmem, st>>>(
+            rounds_newton_kernel<NT, NT2, GAUNT><<<(unsigned)((nb + RWN - 1) / RWN), RWN * 32,
+                                                   newtonSmem, st>>>(
                 P, m0, listA + off, nb, state, R.buf, R.bRow, R.bCol, R.bVal, O, listB, cB);
             *R.launches += 2;
             e = cudaGetLastError();
