@@ -56,7 +56,7 @@ class ClosureStats(ctypes.Structure):
                 ("clkSerial", ctypes.c_longlong), ("passes", ctypes.c_longlong),
                 ("regHist", ctypes.c_longlong * 16),
                 ("iterHist", ctypes.c_longlong * 64),
-                ("clkNewton", ctypes.c_longlong * 4)]
+                ("clkNewton", ctypes.c_longlong * 8)]
 
 
 _lib = None

@@ -35,8 +35,8 @@ cudaError_t launch_closure_gaunt(const ClosureLaunch &L, const GauntTables &G);
 struct RoundsLaunch {
     const ClosureParams *P;
     const double *chunks;
-    const int *bRow, *bCol;
-    const double *bVal;
+    const int2 *plan;          // Gaunt: per tile slot {first term, terms} (-1: identity)
+    const GauntTerm *terms;    // Gaunt: the beta terms in tile-slot order
     double m0;
     long long ncells;
     double *u, *alpha;
@@ -156,6 +156,8 @@ struct c3d_ctx {
     bool gaunt = false;
     double *gChunks = nullptr, *gVal = nullptr;
     int *gRow = nullptr, *gCol = nullptr;
+    int2 *gPlan = nullptr;         // tiled assembly plan of the work-list engine
+    GauntTerm *gTerms = nullptr;
     // optional event timing of the closure and flux launches (kind 0 closure, 1 flux)
     bool timing = false;
     std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> events;
@@ -192,7 +194,8 @@ static void free_ctx(c3d_ctx *c)
                     c->M,     c->w,      c->xi,       c->eta,     c->mu,     c->chunks,
                     c->pnops, c->psi,    c->iters,    c->iterGamma, c->regIdx, c->status,
                     c->counter, c->failCount, c->stats, c->errorFlag, c->gChunks, c->gVal,
-                    c->gRow, c->gCol, c->rState, c->rListA, c->rListB, c->rCounts, c->rBuf};
+                    c->gRow, c->gCol, c->gPlan, c->gTerms, c->rState, c->rListA, c->rListB,
+                    c->rCounts, c->rBuf};
     for (void *p : ptrs)
         if (p)
             cudaFree(p);
@@ -447,9 +450,8 @@ static c3d_status run_closure(c3d_ctx *c, long long n, double *u, double *alpha,
         RoundsLaunch R{};
         R.P = &c->cp;
         R.chunks = c->gaunt ? c->gChunks : c->chunks;
-        R.bRow = c->gRow;
-        R.bCol = c->gCol;
-        R.bVal = c->gVal;
+        R.plan = c->gPlan;
+        R.terms = c->gTerms;
         R.m0 = c->m0;
         R.ncells = n;
         R.u = u;
@@ -566,7 +568,51 @@ c3d_status c3d_set_gaunt(c3d_ctx *c, int nm2, const double *M2, const int *rowPt
     cudaMemcpy(drow, rowPtr, (size_t)(nm * nm + 1) * 4, cudaMemcpyHostToDevice);
     cudaMemcpy(dcol, colInd, (size_t)nnz * 4, cudaMemcpyHostToDevice);
     cudaMemcpy(dval, val, (size_t)nnz * 8, cudaMemcpyHostToDevice);
+    // assembly plan of the tiled Hessian (work-list engine): per slot of the lower
+    // triangle of 8x8 tiles, the CSR row of its (row >= col) element
+    const int nt = (nm + 7) / 8, ls = 64 * nt * (nt + 1) / 2;
+    std::vector<int2> plan(ls);
+    std::vector<GauntTerm> terms;
+    terms.reserve((size_t)nnz);
+    for (int e = 0; e < ls; ++e) {
+        const int t = e >> 6, rr = (e >> 3) & 7, cc = e & 7;
+        int ib = 0;
+        while ((ib + 1) * (ib + 2) / 2 <= t)
+            ++ib;
+        const int jb = t - ib * (ib + 1) / 2;
+        const int i = 8 * ib + rr, j = 8 * jb + cc;
+        plan[e] = make_int2((int)terms.size(), 0);
+        if (ib == jb && cc > rr)
+            continue;
+        if (i >= nm || j >= nm) {
+            plan[e].y = (i == j) ? -1 : 0;
+            continue;
+        }
+        const int idx = j * nm + i;
+        for (int k = rowPtr[idx]; k < rowPtr[idx + 1]; ++k)
+            terms.push_back(GauntTerm{val[k], colInd[k], 0});
+        plan[e].y = (int)terms.size() - plan[e].x;
+    }
+    int2 *dplan = nullptr;
+    GauntTerm *dterms = nullptr;
+    if (cudaMalloc(&dplan, plan.size() * sizeof(int2)) != cudaSuccess ||
+        cudaMalloc(&dterms, (terms.empty() ? 1 : terms.size()) * sizeof(GauntTerm)) != cudaSuccess) {
+        cudaGetLastError();
+        if (dplan) cudaFree(dplan);
+        cudaFree(dch);
+        cudaFree(drow);
+        cudaFree(dcol);
+        cudaFree(dval);
+        return fail(C3D_ERR_OOM, "c3d_set_gaunt: device allocation failed");
+    }
+    cudaMemcpy(dplan, plan.data(), plan.size() * sizeof(int2), cudaMemcpyHostToDevice);
+    if (!terms.empty())
+        cudaMemcpy(dterms, terms.data(), terms.size() * sizeof(GauntTerm), cudaMemcpyHostToDevice);
     C3D_CUDA(cudaDeviceSynchronize());
+    if (c->gPlan) cudaFree(c->gPlan);
+    if (c->gTerms) cudaFree(c->gTerms);
+    c->gPlan = dplan;
+    c->gTerms = dterms;
     if (c->gChunks) cudaFree(c->gChunks);
     if (c->gRow) cudaFree(c->gRow);
     if (c->gCol) cudaFree(c->gCol);
@@ -727,7 +773,7 @@ c3d_status c3d_closure_stats_get(c3d_ctx *c, c3d_closure_stats *st)
         st->regHist[i] = (long long)h[STAT_REG_HIST + i];
     for (int i = 0; i < 64; ++i)
         st->iterHist[i] = (long long)h[STAT_ITER_HIST + i];
-    for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < 8; ++i)
         st->clkNewton[i] = (long long)h[STAT_CLK_NEWTON + i];
     return C3D_OK;
 }

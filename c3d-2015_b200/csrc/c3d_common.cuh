@@ -36,10 +36,10 @@ enum StatSlot : int {
     STAT_CLK_PASS = 25,   // passes over the staged basis
     STAT_CLK_SERIAL = 26, // per-cell Newton logic after each pass
     STAT_PASSES = 27,     // passes (per CTA)
-    STAT_CLK_NEWTON = 28, // 4 slots, builds with C3D_NEWTON_CLOCKS only: SM clocks of the
-                          // Newton kernel's H assembly, g/f/norms, Cholesky, and the rest
     STAT_ITER_HIST = 32, // 64 bins (last: >= 63)
-    STAT_COUNT = 96,
+    STAT_CLK_NEWTON = 96, // 8 slots, builds with C3D_NEWTON_CLOCKS only: SM clocks of the
+                          // work-list Newton kernel's phases (c3d_closure_stats.clkNewton)
+    STAT_COUNT = 104,
 };
 
 // Closure options (the MN_* deck keys, src/init.cpp:252-258).
@@ -58,6 +58,14 @@ struct ClosureParams {
 };
 
 __host__ __device__ inline int ceil_div(int a, int b) { return (a + b - 1) / b; }
+
+// One term beta_ijk of the Gaunt-form Hessian for the tiled assembly: H element of a tile
+// slot += v * moment[col] (src/opt/fobj.cpp:81-99).
+struct __align__(16) GauntTerm {
+    double v;
+    int col;
+    int pad;
+};
 
 // Grid with two ghost layers per face; cell (i,j,k) with k fastest (src/global.h:15).
 struct GridDims {

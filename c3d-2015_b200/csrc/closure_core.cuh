@@ -324,9 +324,20 @@ __device__ __forceinline__ int warp_cholesky(S &sl, int n, int lane)
 // exactDiv selects division by L_kk (as the reference's own dpotrs) instead of the
 // precomputed reciprocal.
 template <class S>
+__device__ __noinline__ void warp_apply_inverse_tiled(const S &sl, int lane, double &x0, double &x1);
+
+template <class S>
 __device__ void warp_apply_inverse(const S &sl, int n, int lane, double &x0, double &x1,
                                    bool exactDiv)
 {
+    if constexpr (S::tiled) {
+        // the reciprocals serve both the estimate and the direction here: the blocked
+        // factor already rounds differently from the reference's unblocked one
+        (void)n;
+        (void)exactDiv;
+        warp_apply_inverse_tiled(sl, lane, x0, x1);
+        return;
+    }
     const double *P = sl.L;
     for (int k = 0; k < n; ++k) {
         double v = (k < 32) ? x0 : x1;
@@ -357,6 +368,93 @@ __device__ void warp_apply_inverse(const S &sl, int n, int lane, double &x0, dou
             x0 = fma(-P[S::lx(k, lane)], xk, x0);
         if (lane + 32 < k && lane + 32 < n)
             x1 = fma(-P[S::lx(k, lane + 32)], xk, x1);
+    }
+}
+
+// x <- (L L^T)^{-1} x on the tiled factor: tile-blocked substitution. Inside the diagonal
+// tile the steps are those of the column-oriented form with the precomputed reciprocals;
+// the tiles off the diagonal act as 8-column mat-vec updates of the rows below (forward) or
+// above (backward). Padding rows (L = I there, rinv = 1) keep finite values and never feed
+// the real rows.
+template <class S>
+__device__ __noinline__ void warp_apply_inverse_tiled(const S &sl, int lane, double &x0, double &x1)
+{
+    constexpr int T = S::nt;
+    constexpr int NMP = S::NMP;
+    const double *A = sl.L;
+#pragma unroll 1
+    for (int kb = 0; kb < T; ++kb) {
+        const double *D = A + 64 * tix(kb, kb);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const int row = 8 * kb + i;
+            double xi = __shfl_sync(FULL_MASK, row < 32 ? x0 : x1, row & 31) * sl.rinv[row];
+            if (lane == (row & 31)) {
+                if (row < 32)
+                    x0 = xi;
+                else
+                    x1 = xi;
+            }
+            if (lane > row && lane < 8 * kb + 8)
+                x0 = fma(-D[8 * (lane - 8 * kb) + i], xi, x0);
+            if (lane + 32 > row && lane + 32 < 8 * kb + 8)
+                x1 = fma(-D[8 * (lane + 32 - 8 * kb) + i], xi, x1);
+        }
+        if (kb + 1 < T) {
+            double y[8];
+#pragma unroll
+            for (int c = 0; c < 8; ++c)
+                y[c] = __shfl_sync(FULL_MASK, 8 * kb + c < 32 ? x0 : x1, (8 * kb + c) & 31);
+            if (lane >= 8 * kb + 8 && lane < NMP) {
+                const double *Lr = A + 64 * tix(lane >> 3, kb) + 8 * (lane & 7);
+#pragma unroll
+                for (int c = 0; c < 8; ++c)
+                    x0 = fma(-Lr[c], y[c], x0);
+            }
+            if (lane + 32 >= 8 * kb + 8 && lane + 32 < NMP) {
+                const double *Lr = A + 64 * tix((lane + 32) >> 3, kb) + 8 * (lane & 7);
+#pragma unroll
+                for (int c = 0; c < 8; ++c)
+                    x1 = fma(-Lr[c], y[c], x1);
+            }
+        }
+    }
+#pragma unroll 1
+    for (int kb = T - 1; kb >= 0; --kb) {
+        const double *D = A + 64 * tix(kb, kb);
+#pragma unroll
+        for (int i = 7; i >= 0; --i) {
+            const int row = 8 * kb + i;
+            double xi = __shfl_sync(FULL_MASK, row < 32 ? x0 : x1, row & 31) * sl.rinv[row];
+            if (lane == (row & 31)) {
+                if (row < 32)
+                    x0 = xi;
+                else
+                    x1 = xi;
+            }
+            if (lane >= 8 * kb && lane < row)
+                x0 = fma(-D[8 * i + (lane - 8 * kb)], xi, x0);
+            if (lane + 32 >= 8 * kb && lane + 32 < row)
+                x1 = fma(-D[8 * i + (lane + 32 - 8 * kb)], xi, x1);
+        }
+        if (kb > 0) {
+            double y[8];
+#pragma unroll
+            for (int c = 0; c < 8; ++c)
+                y[c] = __shfl_sync(FULL_MASK, 8 * kb + c < 32 ? x0 : x1, (8 * kb + c) & 31);
+            if (lane < 8 * kb) {
+                const double *Lc = A + 64 * tix(kb, lane >> 3) + (lane & 7);
+#pragma unroll
+                for (int c = 0; c < 8; ++c)
+                    x0 = fma(-Lc[8 * c], y[c], x0);
+            }
+            if (lane + 32 < 8 * kb) {
+                const double *Lc = A + 64 * tix(kb, (lane + 32) >> 3) + (lane & 7);
+#pragma unroll
+                for (int c = 0; c < 8; ++c)
+                    x1 = fma(-Lc[8 * c], y[c], x1);
+            }
+        }
     }
 }
 
@@ -665,8 +763,30 @@ __device__ void after_hessian(S &sl, const ClosureParams &P, const Outputs &O, i
     double rs = 0.0, gmin = 1.0 / 0.0;
     for (int i = lane; i < nm; i += 32) {
         double s = 0.0;
-        for (int j = 0; j < nm; ++j)
-            s += fabs(j <= i ? sl.L[S::lx(i, j)] : sl.L[S::lx(j, i)]);
+        if constexpr (S::tiled) {
+            // row i = the row segments of tiles (ib, jb <= ib) and the column segments of
+            // tiles (ib' > ib, ib); padding entries are 0
+            const int ib = i >> 3, r = i & 7;
+            for (int jb = 0; jb < ib; ++jb) {
+                const double *Lr = sl.L + 64 * tix(ib, jb) + 8 * r;
+#pragma unroll
+                for (int c = 0; c < 8; ++c)
+                    s += fabs(Lr[c]);
+            }
+            const double *D = sl.L + 64 * tix(ib, ib);
+#pragma unroll
+            for (int c = 0; c < 8; ++c)
+                s += fabs(c <= r ? D[8 * r + c] : D[8 * c + r]);
+            for (int ib2 = ib + 1; ib2 < S::nt; ++ib2) {
+                const double *Lc = sl.L + 64 * tix(ib2, ib) + r;
+#pragma unroll
+                for (int c = 0; c < 8; ++c)
+                    s += fabs(Lc[8 * c]);
+            }
+        } else {
+            for (int j = 0; j < nm; ++j)
+                s += fabs(j <= i ? sl.L[S::lx(i, j)] : sl.L[S::lx(j, i)]);
+        }
         rs = fmax(rs, s);
         gmin = fmin(gmin, 2.0 * sl.L[S::lx(i, i)] - s); // Gershgorin: H_ii - sum_{j!=i} |H_ij|
     }
@@ -683,13 +803,14 @@ __device__ void after_hessian(S &sl, const ClosureParams &P, const Outputs &O, i
     C3D_NCLK(O.stats, 2, lane);
     double cond = 0.0;
     if (info == 0) {
-        for (int i = lane; i < nm; i += 32)
+        for (int i = lane; i < (S::tiled ? S::NMP : nm); i += 32)
             sl.rinv[i] = 1.0 / sl.L[S::lx(i, i)];
         __syncwarp();
         if (!condSure)
             cond = warp_condest(sl, nm, lane, norm1);
     }
     __syncwarp();
+    C3D_NCLK(O.stats, 3, lane);
 
     bool bad = (info != 0) || (cond > P.condHMax);
     if (sl.s.totalIter == 1 && bad) {
@@ -733,6 +854,7 @@ __device__ void after_hessian(S &sl, const ClosureParams &P, const Outputs &O, i
     if (lane + 32 < nm)
         sl.d[lane + 32] = -x1;
     __syncwarp();
+    C3D_NCLK(O.stats, 4, lane);
     double err = warp_nrm2(sl.g, nm, lane);
     double d1 = vsum_abs(x0, x1, lane, nm);
     int pnOrder = (int)floor(sqrt((double)nm)) + 1;

@@ -30,8 +30,9 @@ template <int NT> struct CellState {
 
 namespace {
 
+// lineSearch = false skips g, d and alphaOld, which a Hessian visit recomputes before use.
 template <int NT, class S>
-__device__ void state_to_slot(const CellState<NT> &st, S &sl, int lane)
+__device__ void state_to_slot(const CellState<NT> &st, S &sl, int lane, bool lineSearch = true)
 {
     constexpr int NMP = Cfg<NT>::NMP;
     for (int i = lane; i < NMP; i += 32) {
@@ -39,9 +40,11 @@ __device__ void state_to_slot(const CellState<NT> &st, S &sl, int lane)
         sl.alpha[i] = st.alpha[i];
         sl.alpha0[i] = st.alpha0[i];
         sl.uOrig[i] = st.uOrig[i];
-        sl.g[i] = st.g[i];
-        sl.d[i] = st.d[i];
-        sl.alphaOld[i] = st.alphaOld[i];
+        if (lineSearch) {
+            sl.g[i] = st.g[i];
+            sl.d[i] = st.d[i];
+            sl.alphaOld[i] = st.alphaOld[i];
+        }
     }
     if (lane == 0)
         sl.s = st.s;
@@ -324,72 +327,57 @@ __global__ void __launch_bounds__(RW * 32, 1)
 
 // Newton logic for the listed cells: one warp per cell, RWN cells per CTA, state staged
 // in shared memory with H in the tiled layout (TSlot).
-// GAUNT: the CTA assembles H_ij = sum_k beta_ijk mom_k (i >= j, CSR of beta in the order of
-// src/opt/fobj.cpp:81-99) for its cells that need a Hessian in one sweep over the tile
-// elements, so that each CSR term is read once for RWN cells; otherwise the pass wrote H in
-// tiles to hBuf.
+// GAUNT: the CTA assembles H_ij = sum_k beta_ijk mom_k (i >= j, the CSR terms of beta in
+// the order of src/opt/fobj.cpp:81-99, laid out per tile slot by c3d_set_gaunt) for its
+// cells that need a Hessian in one sweep over the tile slots, so that each term is read once
+// for RWN cells. A cell's moments sit in its slot's g..rinv vectors, which a Hessian visit
+// recomputes afterwards. Otherwise the pass wrote H in tiles to hBuf.
 template <int NT, int NT2, bool GAUNT>
 __global__ void __launch_bounds__(RWN * 32)
     rounds_newton_kernel(ClosureParams P, double m0, const int *__restrict__ list, int n,
                          CellState<NT> *state, const double *__restrict__ buf,
-                         const int *__restrict__ bRow, const int *__restrict__ bCol,
-                         const double *__restrict__ bVal, Outputs O, int *listOut,
-                         unsigned int *countOut)
+                         const int2 *__restrict__ plan, const GauntTerm *__restrict__ terms,
+                         Outputs O, int *listOut, unsigned int *countOut)
 {
     constexpr int NM2P = 8 * NT2;
+    constexpr int NMP = Cfg<NT>::NMP;
     constexpr int LS = TSlot<NT>::LSIZE;
+    static_assert(!GAUNT || NM2P <= 4 * NMP, "moments must fit in g, d, alphaOld, rinv");
     extern __shared__ __align__(128) unsigned char smem_raw[];
     TSlot<NT> *slots = reinterpret_cast<TSlot<NT> *>(smem_raw);
-    double *sMom = reinterpret_cast<double *>(slots + RWN); // RWN x NM2P (GAUNT)
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int pos = blockIdx.x * RWN + warp;
     const bool active = pos < n;
     const long long cell = active ? list[pos] : -1;
+    const bool needH = active && state[cell].s.need == NEED_H;
     TSlot<NT> &sl = slots[warp];
     C3D_NCLK_DECL
     if (active) {
-        state_to_slot(state[cell], sl, lane);
+        state_to_slot(state[cell], sl, lane, !(GAUNT && needH));
     } else if (lane == 0) {
         sl.s.need = NEED_NONE;
     }
-    const int nm = P.nm;
-    const bool needH = active && sl.s.need == NEED_H;
     if (GAUNT) {
-        for (int k = lane; k < NM2P; k += 32)
-            sMom[warp * NM2P + k] = needH ? buf[(size_t)pos * NM2P + k] : 0.0;
-        __syncthreads();
+        double *mom = sl.g; // g, d, alphaOld, rinv are contiguous: NM2P <= 4 NMP doubles
+        if (needH)
+            for (int k = lane; k < NM2P; k += 32)
+                mom[k] = buf[(size_t)pos * NM2P + k];
         if (__syncthreads_or(needH)) {
             bool hw[RWN];
 #pragma unroll
             for (int w = 0; w < RWN; ++w)
                 hw[w] = slots[w].s.need == NEED_H;
             for (int e = tid; e < LS; e += RWN * 32) {
-                const int t = e >> 6, rr = (e >> 3) & 7, cc = e & 7;
-                int ib = 0;
-                while (tix(ib + 1, 0) <= t)
-                    ++ib;
-                const int jb = t - tix(ib, 0);
-                const int i = 8 * ib + rr, j = 8 * jb + cc;
+                const int2 pe = plan[e];
                 double h[RWN];
 #pragma unroll
                 for (int w = 0; w < RWN; ++w)
-                    h[w] = 0.0;
-                if (ib == jb && cc > rr) {
-                    // upper half of a diagonal tile: unused
-                } else if (i >= nm || j >= nm) {
+                    h[w] = pe.y < 0 ? 1.0 : 0.0;
+                for (int tt = pe.x; tt < pe.x + pe.y; ++tt) {
+                    const GauntTerm gt = terms[tt];
 #pragma unroll
                     for (int w = 0; w < RWN; ++w)
-                        h[w] = (i == j) ? 1.0 : 0.0;
-                } else {
-                    const int idx = j * nm + i;
-                    const int tEnd = bRow[idx + 1];
-                    for (int tt = bRow[idx]; tt < tEnd; ++tt) {
-                        const int col = bCol[tt];
-                        const double v = bVal[tt];
-#pragma unroll
-                        for (int w = 0; w < RWN; ++w)
-                            h[w] = __dadd_rn(h[w], __dmul_rn(sMom[w * NM2P + col], v));
-                    }
+                        h[w] = __dadd_rn(h[w], __dmul_rn(slots[w].g[gt.col], gt.v));
                 }
 #pragma unroll
                 for (int w = 0; w < RWN; ++w)
@@ -408,13 +396,16 @@ __global__ void __launch_bounds__(RWN * 32)
     if (!active)
         return;
     C3D_NCLK(O.stats, 0, lane);
-    if (sl.s.need == NEED_H)
+    if (sl.s.need == NEED_H) {
         after_hessian(sl, P, O, lane, m0);
-    else if (sl.s.need == NEED_TRIAL)
+        C3D_NCLK(O.stats, 5, lane);
+    } else if (sl.s.need == NEED_TRIAL) {
         after_trial(sl, P, O, lane, sl.s.fquad);
+        C3D_NCLK(O.stats, 7, lane);
+    }
     slot_to_state(sl, state[cell], lane);
     append_if_needed(sl, cell, lane, listOut, countOut);
-    C3D_NCLK(O.stats, 3, lane);
+    C3D_NCLK(O.stats, 6, lane);
 }
 
 // ---------------------------------------------------------------- host side
@@ -422,8 +413,8 @@ __global__ void __launch_bounds__(RWN * 32)
 struct RoundsLaunch {
     const ClosureParams *P;
     const double *chunks;      // direct: (NMP+1) x QCP chunks; Gaunt: (NM2P+1) x QCP chunks
-    const int *bRow, *bCol;    // Gaunt CSR (null for the direct form)
-    const double *bVal;
+    const int2 *plan;          // Gaunt: per tile slot {first term, terms} (-1: identity)
+    const GauntTerm *terms;    // Gaunt: the beta terms in tile-slot order
     double m0;                 // M[0][0]
     long long ncells;
     double *u, *alpha;
@@ -477,7 +468,7 @@ template <int NT, int NT2, bool GAUNT> static cudaError_t rounds_t(const RoundsL
                              (int)slotSmem);
     if (e != cudaSuccess)
         return e;
-    size_t newtonSmem = RWN * sizeof(TSlot<NT>) + (GAUNT ? (size_t)RWN * 8 * NT2 * 8 : 0);
+    size_t newtonSmem = RWN * sizeof(TSlot<NT>);
     e = cudaFuncSetAttribute(rounds_newton_kernel<NT, NT2, GAUNT>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)newtonSmem);
     if (e != cudaSuccess)
@@ -532,7 +523,7 @@ template <int NT, int NT2, bool GAUNT> static cudaError_t rounds_t(const RoundsL
                     P, R.chunks, listA + off, nb, state, R.buf, R.errorFlag);
             rounds_newton_kernel<NT, NT2, GAUNT><<<(unsigned)((nb + RWN - 1) / RWN), RWN * 32,
                                                    newtonSmem, st>>>(
-                P, m0, listA + off, nb, state, R.buf, R.bRow, R.bCol, R.bVal, O, listB, cB);
+                P, m0, listA + off, nb, state, R.buf, R.plan, R.terms, O, listB, cB);
             *R.launches += 2;
             e = cudaGetLastError();
             if (e != cudaSuccess)

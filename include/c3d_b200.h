@@ -108,8 +108,10 @@ typedef struct {
     long long passes;          /* passes, summed over CTAs */
     long long regHist[16];     /* g_mnHistReg */
     long long iterHist[64];    /* cells per iteration count (last bin: >= 63) */
-    long long clkNewton[4];    /* SM clocks of the work-list Newton kernel: H assembly, g/f and
-                                  norms, Cholesky, the rest; builds with C3D_NEWTON_CLOCKS only */
+    long long clkNewton[8];    /* SM clocks of the work-list Newton kernel, builds with
+                                  C3D_NEWTON_CLOCKS only: state load + H assembly, g/f/norms,
+                                  Cholesky, condition estimate, direction solve, after_hessian in
+                                  total, state store, line-search trial updates */
 } c3d_closure_stats;
 
 /* Creates a context on the current CUDA device with the tables M[nq*nm],
