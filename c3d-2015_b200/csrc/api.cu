@@ -65,12 +65,13 @@ cudaError_t launch_euler(const GridDims &g, double *u, const double *flux, const
                          const double *sigS, double dt, int numSMs, cudaStream_t st);
 cudaError_t launch_rk(const GridDims &g, double *u, double *uOld, int mode, int numSMs,
                       cudaStream_t st);
-cudaError_t launch_kinetic_flux(const GridDims &g, const double *alpha, const double *M,
-                                const double *w, const double *xi, const double *eta,
-                                const double *mu, int nq, int qChunk, double dx, double dy,
+cudaError_t launch_kinetic_flux(const GridDims &g, const double *alpha, const double *mfA,
+                                const double *mfP, int nq, int qChunk, double dx, double dy,
                                 double dz, double theta, int isPn, double *psi, double *flux,
-                                cudaStream_t st);
-int kinetic_max_chunk(int nm);
+                                int *errorFlag, cudaStream_t st);
+size_t flux_frag_doubles(int nm, int nq, int which);
+void flux_frags(int nm, int nq, const double *M, const double *w, const double *xi,
+                const double *eta, const double *mu, double *mfA, double *mfP);
 cudaError_t launch_moment_flux(const GridDims &g, const double *u, const double *ops, double dx,
                                double dy, double dz, double *flux, cudaStream_t st);
 } // namespace c3d
@@ -138,6 +139,7 @@ struct c3d_ctx {
     double *u = nullptr, *alpha = nullptr, *uOld = nullptr, *flux = nullptr;
     double *sigT = nullptr, *sigS = nullptr;
     double *M = nullptr, *w = nullptr, *xi = nullptr, *eta = nullptr, *mu = nullptr;
+    double *mfA = nullptr, *mfP = nullptr; // basis in the flux kernels' fragment order
     double *chunks = nullptr, *pnops = nullptr, *psi = nullptr;
     int *iters = nullptr, *iterGamma = nullptr, *regIdx = nullptr, *status = nullptr;
     unsigned long long *counter = nullptr, *failCount = nullptr, *stats = nullptr;
@@ -195,7 +197,7 @@ static void free_ctx(c3d_ctx *c)
                     c->pnops, c->psi,    c->iters,    c->iterGamma, c->regIdx, c->status,
                     c->counter, c->failCount, c->stats, c->errorFlag, c->gChunks, c->gVal,
                     c->gRow, c->gCol, c->gPlan, c->gTerms, c->rState, c->rListA, c->rListB,
-                    c->rCounts, c->rBuf};
+                    c->rCounts, c->rBuf, c->mfA, c->mfP};
     for (void *p : ptrs)
         if (p)
             cudaFree(p);
@@ -291,6 +293,9 @@ c3d_status c3d_create(const c3d_params *p, const double *M, const double *w, con
               alloc((void **)&c->stats, STAT_COUNT * 8);
     std::vector<double> ch = build_chunks(nm, nq, M, w);
     ok = ok && alloc((void **)&c->chunks, ch.size() * 8);
+    std::vector<double> mfA(flux_frag_doubles(nm, nq, 0)), mfP(flux_frag_doubles(nm, nq, 1));
+    flux_frags(nm, nq, M, w, xi, eta, mu, mfA.data(), mfP.data());
+    ok = ok && alloc((void **)&c->mfA, mfA.size() * 8) && alloc((void **)&c->mfP, mfP.size() * 8);
     if (ok && pnOps)
         ok = alloc((void **)&c->pnops, (size_t)6 * nm * nm * 8);
     if (!ok) {
@@ -303,6 +308,8 @@ c3d_status c3d_create(const c3d_params *p, const double *M, const double *w, con
     cudaMemcpy(c->eta, eta, nq * 8, cudaMemcpyHostToDevice);
     cudaMemcpy(c->mu, mu, nq * 8, cudaMemcpyHostToDevice);
     cudaMemcpy(c->chunks, ch.data(), ch.size() * 8, cudaMemcpyHostToDevice);
+    cudaMemcpy(c->mfA, mfA.data(), mfA.size() * 8, cudaMemcpyHostToDevice);
+    cudaMemcpy(c->mfP, mfP.data(), mfP.size() * 8, cudaMemcpyHostToDevice);
     if (pnOps)
         cudaMemcpy(c->pnops, pnOps, (size_t)6 * nm * nm * 8, cudaMemcpyHostToDevice);
     cudaMemset(c->u, 0, nall * nm * 8);
@@ -322,12 +329,11 @@ c3d_status c3d_create(const c3d_params *p, const double *M, const double *w, con
         return fail(C3D_ERR_CUDA, std::string("c3d_create: ") + cudaGetErrorString(e));
     }
     // direction chunk of the materialised ansatz: shared-memory and HBM budgets
-    int qc = kinetic_max_chunk(nm);
+    // (whole tiles of 32 unless one chunk covers every direction)
     long long byBudget = (long long)(c->psiBytes / ((size_t)nall * 8));
-    if (byBudget < qc)
-        qc = (int)(byBudget < 1 ? 1 : byBudget);
-    if (qc > nq)
-        qc = nq;
+    int qc = byBudget >= nq ? nq : (int)(byBudget / 32) * 32;
+    if (qc < 32)
+        qc = nq < 32 ? nq : 32;
     c->qChunk = qc;
     *out = c;
     return C3D_OK;
@@ -656,8 +662,9 @@ c3d_status c3d_flux_kinetic(c3d_ctx *c, int alphaIsU)
     int isPn = (c->solver == 0) ? 1 : 0;
     cudaEvent_t t0 = nullptr;
     timing_begin(c, &t0);
-    C3D_CUDA(launch_kinetic_flux(c->g, a, c->M, c->w, c->xi, c->eta, c->mu, c->nq, c->qChunk,
-                                 c->dx, c->dy, c->dz, c->theta, isPn, c->psi, c->flux, c->stream));
+    C3D_CUDA(launch_kinetic_flux(c->g, a, c->mfA, c->mfP, c->nq, c->qChunk,
+                                 c->dx, c->dy, c->dz, c->theta, isPn, c->psi, c->flux,
+                                 c->errorFlag, c->stream));
     timing_end(c, 1, t0);
     int nch = ceil_div(c->nq, c->qChunk);
     c->launches += 2 * nch;

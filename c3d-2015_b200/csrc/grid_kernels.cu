@@ -142,6 +142,7 @@ __global__ void rk_kernel(GridDims g, double *__restrict__ u, double *__restrict
 // psi[(q - q0) * nall + c] = exp(alpha_c . m_q) (M_N) or alpha_c . m_q (P_N), for all
 // cells c and q0 <= q < q0 + nqc. The dot product runs in the reference's order
 // (moment index ascending, unfused), src/flux_kinetic.cpp:21-37.
+// (moment index ascending, unfused), src/flux_kinetic.cpp:21-37.
 template <int NM>
 __global__ void __launch_bounds__(128)
     ansatz_kernel(GridDims g, const double *__restrict__ alpha, const double *__restrict__ M, int q0,
@@ -191,92 +192,17 @@ __device__ __forceinline__ double slopefit(double th, double l, double c, double
     return minmod(th * (r - c), minmod(0.5 * (r - l), th * (c - l)));
 }
 
-// Upwind MUSCL difference along one axis, src/flux_kinetic.cpp:130-189.
-__device__ __forceinline__ double axis_flux(double om, double w, double th, const double *p,
-                                            long long c, long long s)
-{
-    double k1, k2, k3, k4, f;
-    if (om > 0) {
-        k1 = p[c - 2 * s];
-        k2 = p[c - s];
-        k3 = p[c];
-        k4 = p[c + s];
-        f = k3 + 0.5 * slopefit(th, k2, k3, k4) - k2 - 0.5 * slopefit(th, k1, k2, k3);
-    } else {
-        k1 = p[c - s];
-        k2 = p[c];
-        k3 = p[c + s];
-        k4 = p[c + 2 * s];
-        f = k3 - 0.5 * slopefit(th, k2, k3, k4) - k2 + 0.5 * slopefit(th, k1, k2, k3);
-    }
-    return f * om * w;
-}
-
-// flux_m(c) (+)= sum_{q in chunk} m_q[m] (Fx/dx + Fy/dy + Fz/dz), one thread per interior
-// cell, moments in registers. Directions are staged through shared memory SUB at a time
-// (7 KB for M_6), so several blocks share an SM. 1/dx is precomputed (exact for the
-// power-of-two spacings of the benchmark grids, within one rounding otherwise).
-// accumulate = 0 on the first chunk.
-template <int NM>
-__global__ void __launch_bounds__(128)
-    kinetic_stencil_kernel(GridDims g, const double *__restrict__ psi, const double *__restrict__ M,
-                           const double *__restrict__ w, const double *__restrict__ xi,
-                           const double *__restrict__ eta, const double *__restrict__ mu, int q0,
-                           int nqc, double rdx, double rdy, double rdz, double theta,
-                           int accumulate, double *__restrict__ flux)
-{
-    constexpr int SUB = 16;
-    __shared__ double sM[SUB * NM];
-    __shared__ double sO[SUB * 4]; // xi, eta, mu, w
-    long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    const bool active = n < g.ninterior();
-    const long long nall = g.nall();
-    long long c = active ? interior_cell(g, n) : 0;
-    const long long sx = (long long)g.nyg() * g.nzg(), sy = g.nzg(), sz = 1;
-    double acc[NM];
-    if (accumulate && active) {
-#pragma unroll
-        for (int m = 0; m < NM; ++m)
-            acc[m] = flux[c * NM + m];
-    } else {
-#pragma unroll
-        for (int m = 0; m < NM; ++m)
-            acc[m] = 0.0;
-    }
-    for (int s0 = 0; s0 < nqc; s0 += SUB) {
-        int ns = nqc - s0 < SUB ? nqc - s0 : SUB;
-        __syncthreads();
-        for (int e = threadIdx.x; e < ns * NM; e += blockDim.x)
-            sM[e] = M[(long long)(q0 + s0) * NM + e];
-        for (int q = threadIdx.x; q < ns; q += blockDim.x) {
-            sO[4 * q + 0] = xi[q0 + s0 + q];
-            sO[4 * q + 1] = eta[q0 + s0 + q];
-            sO[4 * q + 2] = mu[q0 + s0 + q];
-            sO[4 * q + 3] = w[q0 + s0 + q];
-        }
-        __syncthreads();
-        if (!active)
-            continue;
-        for (int q = 0; q < ns; ++q) {
-            const double *p = psi + (long long)(s0 + q) * nall;
-            double wq = sO[4 * q + 3];
-            double fx = axis_flux(sO[4 * q + 0], wq, theta, p, c, sx);
-            double fy = axis_flux(sO[4 * q + 1], wq, theta, p, c, sy);
-            double fz = axis_flux(sO[4 * q + 2], wq, theta, p, c, sz);
-            double sv = fx * rdx + fy * rdy + fz * rdz;
-#pragma unroll
-            for (int m = 0; m < NM; ++m)
-                acc[m] = fma(sM[q * NM + m], sv, acc[m]);
-        }
-    }
-    if (!active)
-        return;
-#pragma unroll
-    for (int m = 0; m < NM; ++m)
-        flux[c * NM + m] = acc[m];
-}
-
 // ---------------------------------------------------------------- kinetic flux on the tensor pipe
+//
+// Directions come in tiles of 32. Per tile the host prepares (c3d_create) two copies of the
+// basis in m8n8k4 fragment order, so that a warp reads each fragment as 32 consecutive
+// doubles and a CTA stages a tile with one bulk copy:
+//   ansatz     [j 0..3][k-step 0..2NT-1][lane]  M[32t + 8j + lane/4][4k + lane%4]   (B of Z = A M^T)
+//   projection [k-step 0..7][j 0..NT-1][lane]   M[32t + 4k + lane%4][8j + lane/4]   (B of F += S M)
+//              followed by xi, eta, mu, w of the tile's 32 directions.
+// Directions past nq and moments past nm are zero.
+
+constexpr int FLUX_STAGES = 2;
 
 __device__ __forceinline__ void dmma_g(double &d0, double &d1, double a, double b)
 {
@@ -285,162 +211,211 @@ __device__ __forceinline__ void dmma_g(double &d0, double &d1, double a, double 
                  : "d"(a), "d"(b));
 }
 
-// psi[(q - q0) * nall + c] = exp(z) (M_N) or z (P_N) with z = alpha_c . m_q, for a tile of
-// 64 cells x 32 directions per CTA: Z = A M^T on the FP64 tensor pipe (m8n8k4; warp w owns
-// cells 8w..8w+7, four 8-direction tiles, K = moments in steps of 4).
-template <int NT>
-__global__ void __launch_bounds__(256)
-    ansatz_dmma_kernel(GridDims g, const double *__restrict__ alpha, const double *__restrict__ M,
-                       int q0, int nqc, int isPn, double *__restrict__ psi)
+__device__ __forceinline__ uint32_t smem_addr(const void *p)
 {
-    constexpr int NMP = 8 * NT;
-    constexpr int KS = (NMP + 3) / 4;      // k-steps of 4 moments
-    constexpr int AS = 4 * KS + 4;         // row stride of the alpha tile (== 4 mod 16 doubles
-    constexpr int MS = 4 * KS + 4;         //   when 4*KS is a multiple of 16; conflict-light)
-    extern __shared__ double ansatzSmem[]; // sA[64 * AS], sM[32 * MS]
-    double *sA = ansatzSmem;
-    double *sM = ansatzSmem + 64 * AS;
-    const int nm = g.nm;
-    const long long nall = g.nall();
-    const long long c0 = (long long)blockIdx.x * 64;
-    const int qb = blockIdx.y * 32;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (int e = tid; e < 64 * AS; e += 256) {
-        int r = e / AS, m = e % AS;
-        long long c = c0 + r;
-        sA[e] = (c < nall && m < nm) ? alpha[c * nm + m] : 0.0;
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void fbar_init(uint64_t *bar)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_addr(bar)));
+}
+__device__ __forceinline__ void fbar_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(bar)),
+                 "r"(bytes)
+                 : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+// false if the phase did not complete within the iteration limit
+__device__ __forceinline__ bool fbar_wait(uint64_t *bar, uint32_t parity)
+{
+    for (int it = 0; it < (1 << 26); ++it) {
+        uint32_t done;
+        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                     " selp.u32 %0, 1, 0, p;\n}\n"
+                     : "=r"(done)
+                     : "r"(smem_addr(bar)), "r"(parity)
+                     : "memory");
+        if (done)
+            return true;
     }
-    for (int e = tid; e < 32 * MS; e += 256) {
-        int r = e / MS, m = e % MS;
-        int q = qb + r;
-        sM[e] = (q < nqc && m < nm) ? M[(long long)(q0 + q) * nm + m] : 0.0;
-    }
-    __syncthreads();
-    double acc[4][2];
-#pragma unroll
-    for (int j = 0; j < 4; ++j)
-        acc[j][0] = acc[j][1] = 0.0;
-#pragma unroll
-    for (int kk = 0; kk < KS; ++kk) {
-        double a = sA[(8 * warp + (lane >> 2)) * AS + 4 * kk + (lane & 3)];
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            double b = sM[(8 * j + (lane >> 2)) * MS + 4 * kk + (lane & 3)];
-            dmma_g(acc[j][0], acc[j][1], a, b);
-        }
-    }
-    const long long c = c0 + 8 * warp + (lane >> 2);
-    if (c >= nall)
-        return;
-#pragma unroll
-    for (int j = 0; j < 4; ++j)
-#pragma unroll
-        for (int e2 = 0; e2 < 2; ++e2) {
-            int q = qb + 8 * j + 2 * (lane & 3) + e2;
-            if (q < nqc) {
-                double z = acc[j][e2];
-                psi[(long long)q * nall + c] = isPn ? z : exp(z);
-            }
-        }
+    return false;
 }
 
-// flux(c) (+)= sum_q m_q (Fx/dx + Fy/dy + Fz/dz) for 64 interior cells (consecutive in the
-// interior numbering) per CTA: per 32-direction chunk the limited upwind differences
-// S[q][cell] go to shared memory, then F += S^T M on the FP64 tensor pipe (warp w owns
-// cells 8w..8w+7 and every 8-moment tile).
+// psi[(q - q0) nall + c] = exp(alpha_c . m_q) (M_N) or alpha_c . m_q (P_N) for the directions
+// q0 <= q < q0 + nqc, q0 a multiple of 32. A CTA owns 64 cells (warp w: 8w..8w+7), keeps
+// their multipliers as A fragments in registers and walks the direction tiles of the chunk
+// (double-buffered bulk copies of the ansatz fragments): 8 NT DMMAs per 8 x 8 block.
 template <int NT>
 __global__ void __launch_bounds__(256)
-    kinetic_dmma_kernel(GridDims g, const double *__restrict__ psi, const double *__restrict__ M,
-                        const double *__restrict__ w, const double *__restrict__ xi,
-                        const double *__restrict__ eta, const double *__restrict__ mu, int q0,
-                        int nqc, double rdx, double rdy, double rdz, double theta,
-                        int accumulate, double *__restrict__ flux)
+    ansatz_dmma_kernel(GridDims g, const double *__restrict__ alpha, const double *__restrict__ mfA,
+                       int q0, int nqc, int isPn, double *__restrict__ psi, int *errorFlag)
 {
-    constexpr int NMP = 8 * NT;
+    constexpr int KS = 2 * NT;
+    constexpr int TILE = 4 * KS * 32;
+    __shared__ __align__(128) double sB[FLUX_STAGES][TILE];
+    __shared__ uint64_t bar[FLUX_STAGES];
+    __shared__ int sAbort;
+    const int nm = g.nm;
+    const long long nall = g.nall();
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const long long c = (long long)blockIdx.x * 64 + 8 * warp + (lane >> 2);
+    const int t0 = q0 >> 5, nt = (nqc + 31) >> 5;
+    if (tid == 0) {
+        sAbort = 0;
+        for (int s = 0; s < FLUX_STAGES; ++s)
+            fbar_init(&bar[s]);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        for (int s = 0; s < FLUX_STAGES && s < nt; ++s)
+            fbar_load(sB[s], mfA + (size_t)(t0 + s) * TILE, TILE * 8, &bar[s]);
+    }
+    double a[KS];
+#pragma unroll
+    for (int kk = 0; kk < KS; ++kk) {
+        int k = 4 * kk + (lane & 3);
+        a[kk] = (c < nall && k < nm) ? alpha[c * nm + k] : 0.0;
+    }
+    __syncthreads();
+    for (int t = 0; t < nt; ++t) {
+        const int s = t % FLUX_STAGES;
+        if (!fbar_wait(&bar[s], (t / FLUX_STAGES) & 1))
+            sAbort = 1;
+        if (__syncthreads_or(sAbort)) {
+            if (tid == 0)
+                atomicExch(errorFlag, 1);
+            return;
+        }
+        const double *B = sB[s];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            double z0 = 0.0, z1 = 0.0;
+#pragma unroll
+            for (int kk = 0; kk < KS; ++kk)
+                dmma_g(z0, z1, a[kk], B[(j * KS + kk) * 32 + lane]);
+            const int ql = 32 * t + 8 * j + 2 * (lane & 3); // direction within the chunk
+            if (c < nall) {
+                if (ql < nqc)
+                    psi[(long long)ql * nall + c] = isPn ? z0 : exp(z0);
+                if (ql + 1 < nqc)
+                    psi[(long long)(ql + 1) * nall + c] = isPn ? z1 : exp(z1);
+            }
+        }
+        __syncthreads();
+        if (tid == 0 && t + FLUX_STAGES < nt)
+            fbar_load(sB[s], mfA + (size_t)(t0 + t + FLUX_STAGES) * TILE, TILE * 8, &bar[s]);
+    }
+}
+
+// Limited upwind difference along one axis for either sign of the direction cosine,
+// src/flux_kinetic.cpp:130-189: with h = +1/2 (om > 0, values k1..k4 at offsets -2..1)
+// or h = -1/2 (om <= 0, offsets -1..2), f = ((k3 + h s(k2,k3,k4)) - k2) - h s(k1,k2,k3).
+__device__ __forceinline__ double axis_flux_bf(double om, double w, double th, const double *p,
+                                               long long c, long long st)
+{
+    const long long b = (om > 0) ? c - 2 * st : c - st;
+    const double k1 = p[b], k2 = p[b + st], k3 = p[b + 2 * st], k4 = p[b + 3 * st];
+    const double h = (om > 0) ? 0.5 : -0.5;
+    const double f = k3 + h * slopefit(th, k2, k3, k4) - k2 - h * slopefit(th, k1, k2, k3);
+    return f * om * w;
+}
+
+// flux(c) (+)= sum_q m_q (Fx/dx + Fy/dy + Fz/dz) for 64 interior cells per CTA (consecutive
+// in the interior numbering). Per direction tile: the limited upwind differences S[q][cell]
+// of the CTA (each thread 8 (cell, direction) pairs, loads issued two pairs at a time) go to
+// shared memory, then F += S^T M on the FP64 tensor pipe (warp w: cells 8w..8w+7, all moment
+// tiles), with the projection fragments and direction cosines staged by bulk copies.
+template <int NT>
+__global__ void __launch_bounds__(256)
+    kinetic_dmma_kernel(GridDims g, const double *__restrict__ psi, const double *__restrict__ mfP,
+                        int q0, int nqc, double rdx, double rdy, double rdz, double theta,
+                        int accumulate, double *__restrict__ flux, int *errorFlag)
+{
+    constexpr int TILE = 8 * NT * 32 + 128;
     constexpr int CS = 68; // S tile row stride (cells)
-    constexpr int MS = NMP + 4 + ((NMP + 4) % 16 == 4 ? 0 : (20 - (NMP + 4) % 16) % 16);
-    __shared__ double sS[32 * CS];
-    __shared__ double sM[32 * MS];
-    __shared__ double sO[32 * 4];
+    extern __shared__ __align__(128) double kinSmem[]; // sB[FLUX_STAGES][TILE], sS[32 * CS]
+    double(*sB)[TILE] = reinterpret_cast<double(*)[TILE]>(kinSmem);
+    double *sS = kinSmem + FLUX_STAGES * TILE;
     __shared__ long long sCell[64];
+    __shared__ uint64_t bar[FLUX_STAGES];
+    __shared__ int sAbort;
     const int nm = g.nm;
     const long long nall = g.nall(), nint = g.ninterior();
     const long long n0 = (long long)blockIdx.x * 64;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const long long sx = (long long)g.nyg() * g.nzg(), sy = g.nzg(), sz = 1;
+    const int t0 = q0 >> 5, nt = (nqc + 31) >> 5;
+    if (tid == 0) {
+        sAbort = 0;
+        for (int s = 0; s < FLUX_STAGES; ++s)
+            fbar_init(&bar[s]);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        for (int s = 0; s < FLUX_STAGES && s < nt; ++s)
+            fbar_load(sB[s], mfP + (size_t)(t0 + s) * TILE, TILE * 8, &bar[s]);
+    }
     if (tid < 64)
         sCell[tid] = (n0 + tid < nint) ? interior_cell(g, n0 + tid) : -1;
-    double acc[NT][2];
-    const long long myc = n0 + 8 * warp + (lane >> 2);
     __syncthreads();
-    if (accumulate && myc < nint) {
-        long long c = sCell[8 * warp + (lane >> 2)];
+    const long long myc = sCell[8 * warp + (lane >> 2)];
+    double acc[NT][2];
 #pragma unroll
-        for (int j = 0; j < NT; ++j)
+    for (int j = 0; j < NT; ++j)
 #pragma unroll
-            for (int e2 = 0; e2 < 2; ++e2) {
-                int m = 8 * j + 2 * (lane & 3) + e2;
-                acc[j][e2] = (m < nm) ? flux[c * nm + m] : 0.0;
+        for (int e2 = 0; e2 < 2; ++e2) {
+            int m = 8 * j + 2 * (lane & 3) + e2;
+            acc[j][e2] = (accumulate && myc >= 0 && m < nm) ? flux[myc * nm + m] : 0.0;
+        }
+    const int cl = tid & 63;
+    const long long c = sCell[cl];
+    for (int t = 0; t < nt; ++t) {
+        const int s = t % FLUX_STAGES;
+        if (!fbar_wait(&bar[s], (t / FLUX_STAGES) & 1))
+            sAbort = 1;
+        if (__syncthreads_or(sAbort)) {
+            if (tid == 0)
+                atomicExch(errorFlag, 1);
+            return;
+        }
+        const double *dirs = sB[s] + 8 * NT * 32; // xi, eta, mu, w per direction
+#pragma unroll 2
+        for (int i = 0; i < 8; ++i) {
+            const int qq = (tid >> 6) + 4 * i;
+            const int ql = 32 * t + qq;
+            double sv = 0.0;
+            if (c >= 0 && ql < nqc) {
+                const double *p = psi + (long long)ql * nall;
+                const double wq = dirs[qq + 96];
+                const double fx = axis_flux_bf(dirs[qq], wq, theta, p, c, sx);
+                const double fy = axis_flux_bf(dirs[qq + 32], wq, theta, p, c, sy);
+                const double fz = axis_flux_bf(dirs[qq + 64], wq, theta, p, c, sz);
+                sv = fx * rdx + fy * rdy + fz * rdz;
             }
-    } else {
-#pragma unroll
-        for (int j = 0; j < NT; ++j)
-            acc[j][0] = acc[j][1] = 0.0;
-    }
-    for (int qb = 0; qb < nqc; qb += 32) {
-        int nq = nqc - qb < 32 ? nqc - qb : 32;
-        __syncthreads();
-        for (int e = tid; e < 32 * MS; e += 256) {
-            int r = e / MS, m = e % MS;
-            sM[e] = (r < nq && m < nm) ? M[(long long)(q0 + qb + r) * nm + m] : 0.0;
-        }
-        if (tid < 32) {
-            int q = q0 + qb + tid;
-            bool ok = tid < nq;
-            sO[4 * tid + 0] = ok ? xi[q] : 0.0;
-            sO[4 * tid + 1] = ok ? eta[q] : 0.0;
-            sO[4 * tid + 2] = ok ? mu[q] : 0.0;
-            sO[4 * tid + 3] = ok ? w[q] : 0.0;
+            sS[qq * CS + cl] = sv;
         }
         __syncthreads();
-        // stencil: thread handles cell (tid % 64) for directions tid/64 + 4i
-        {
-            const int cl = tid & 63;
-            const long long c = sCell[cl];
-            for (int qq = tid >> 6; qq < 32; qq += 4) {
-                double sv = 0.0;
-                if (c >= 0 && qq < nq) {
-                    const double *p = psi + (long long)(qb + qq) * nall;
-                    double wq = sO[4 * qq + 3];
-                    double fx = axis_flux(sO[4 * qq + 0], wq, theta, p, c, sx);
-                    double fy = axis_flux(sO[4 * qq + 1], wq, theta, p, c, sy);
-                    double fz = axis_flux(sO[4 * qq + 2], wq, theta, p, c, sz);
-                    sv = fx * rdx + fy * rdy + fz * rdz;
-                }
-                sS[qq * CS + cl] = sv;
-            }
-        }
-        __syncthreads();
+        const double *B = sB[s];
 #pragma unroll
         for (int kk = 0; kk < 8; ++kk) {
-            double a = sS[(4 * kk + (lane & 3)) * CS + 8 * warp + (lane >> 2)];
+            const double a = sS[(4 * kk + (lane & 3)) * CS + 8 * warp + (lane >> 2)];
 #pragma unroll
-            for (int j = 0; j < NT; ++j) {
-                double b = sM[(4 * kk + (lane & 3)) * MS + 8 * j + (lane >> 2)];
-                dmma_g(acc[j][0], acc[j][1], a, b);
-            }
+            for (int j = 0; j < NT; ++j)
+                dmma_g(acc[j][0], acc[j][1], a, B[(kk * NT + j) * 32 + lane]);
         }
+        __syncthreads();
+        if (tid == 0 && t + FLUX_STAGES < nt)
+            fbar_load(sB[s], mfP + (size_t)(t0 + t + FLUX_STAGES) * TILE, TILE * 8, &bar[s]);
     }
-    if (myc >= nint)
+    if (myc < 0)
         return;
-    long long c = sCell[8 * warp + (lane >> 2)];
 #pragma unroll
     for (int j = 0; j < NT; ++j)
 #pragma unroll
         for (int e2 = 0; e2 < 2; ++e2) {
             int m = 8 * j + 2 * (lane & 3) + e2;
             if (m < nm)
-                flux[c * nm + m] = acc[j][e2];
+                flux[myc * nm + m] = acc[j][e2];
         }
 }
 
@@ -538,27 +513,62 @@ cudaError_t launch_rk(const GridDims &g, double *u, double *uOld, int mode, int 
     return cudaGetLastError();
 }
 
+// Fragment-order copies of the basis for the flux kernels (layouts above); nt = ceil(nq/32)
+// tiles each.
+size_t flux_frag_doubles(int nm, int nq, int which)
+{
+    const int NT = (nm + 7) / 8, nt = (nq + 31) / 32;
+    return (size_t)nt * (which == 0 ? 4 * 2 * NT * 32 : 8 * NT * 32 + 128);
+}
+
+void flux_frags(int nm, int nq, const double *M, const double *w, const double *xi,
+                const double *eta, const double *mu, double *mfA, double *mfP)
+{
+    const int NT = (nm + 7) / 8, KS = 2 * NT, nt = (nq + 31) / 32;
+    auto m = [&](int q, int k) { return (q < nq && k < nm) ? M[(size_t)q * nm + k] : 0.0; };
+    for (int t = 0; t < nt; ++t) {
+        double *A = mfA + (size_t)t * 4 * KS * 32;
+        for (int j = 0; j < 4; ++j)
+            for (int kk = 0; kk < KS; ++kk)
+                for (int l = 0; l < 32; ++l)
+                    A[(j * KS + kk) * 32 + l] = m(32 * t + 8 * j + l / 4, 4 * kk + l % 4);
+        double *P = mfP + (size_t)t * (8 * NT * 32 + 128);
+        for (int kk = 0; kk < 8; ++kk)
+            for (int j = 0; j < NT; ++j)
+                for (int l = 0; l < 32; ++l)
+                    P[(kk * NT + j) * 32 + l] = m(32 * t + 4 * kk + l % 4, 8 * j + l / 4);
+        double *D = P + 8 * NT * 32;
+        for (int qq = 0; qq < 32; ++qq) {
+            int q = 32 * t + qq;
+            D[qq] = q < nq ? xi[q] : 0.0;
+            D[32 + qq] = q < nq ? eta[q] : 0.0;
+            D[64 + qq] = q < nq ? mu[q] : 0.0;
+            D[96 + qq] = q < nq ? w[q] : 0.0;
+        }
+    }
+}
+
 template <int NT>
-static cudaError_t kinetic_t(const GridDims &g, const double *alpha, const double *M,
-                             const double *w, const double *xi, const double *eta, const double *mu,
-                             int nq, int qChunk, double dx, double dy, double dz, double theta,
-                             int isPn, double *psi, double *flux, cudaStream_t st)
+static cudaError_t kinetic_t(const GridDims &g, const double *alpha, const double *mfA,
+                             const double *mfP, int nq, int qChunk, double dx, double dy, double dz,
+                             double theta, int isPn, double *psi, double *flux, int *errorFlag,
+                             cudaStream_t st)
 {
     for (int q0 = 0; q0 < nq; q0 += qChunk) {
         int nqc = nq - q0 < qChunk ? nq - q0 : qChunk;
-        dim3 ga((unsigned)((g.nall() + 63) / 64), (unsigned)((nqc + 31) / 32));
-        constexpr int KS = (8 * NT + 3) / 4;
-        const size_t smem = (size_t)(64 + 32) * (4 * KS + 4) * sizeof(double);
-        if (smem > 48 * 1024) {
-            cudaError_t e = cudaFuncSetAttribute(ansatz_dmma_kernel<NT>,
-                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        ansatz_dmma_kernel<NT><<<(unsigned)((g.nall() + 63) / 64), 256, 0, st>>>(
+            g, alpha, mfA, q0, nqc, isPn, psi, errorFlag);
+        const size_t kinSmem = (size_t)(FLUX_STAGES * (8 * NT * 32 + 128) + 32 * 68) * 8;
+        if (kinSmem > 48 * 1024) {
+            cudaError_t e = cudaFuncSetAttribute(kinetic_dmma_kernel<NT>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)kinSmem);
             if (e != cudaSuccess)
                 return e;
         }
-        ansatz_dmma_kernel<NT><<<ga, 256, smem, st>>>(g, alpha, M, q0, nqc, isPn, psi);
-        kinetic_dmma_kernel<NT><<<(unsigned)((g.ninterior() + 63) / 64), 256, 0, st>>>(
-            g, psi, M, w, xi, eta, mu, q0, nqc, 1.0 / dx, 1.0 / dy, 1.0 / dz, theta, q0 > 0 ? 1 : 0,
-            flux);
+        kinetic_dmma_kernel<NT><<<(unsigned)((g.ninterior() + 63) / 64), 256, kinSmem, st>>>(
+            g, psi, mfP, q0, nqc, 1.0 / dx, 1.0 / dy, 1.0 / dz, theta, q0 > 0 ? 1 : 0, flux,
+            errorFlag);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess)
             return e;
@@ -566,16 +576,18 @@ static cudaError_t kinetic_t(const GridDims &g, const double *alpha, const doubl
     return cudaSuccess;
 }
 
-cudaError_t launch_kinetic_flux(const GridDims &g, const double *alpha, const double *M,
-                                const double *w, const double *xi, const double *eta,
-                                const double *mu, int nq, int qChunk, double dx, double dy,
+// qChunk: a multiple of 32 unless it covers all of nq.
+cudaError_t launch_kinetic_flux(const GridDims &g, const double *alpha, const double *mfA,
+                                const double *mfP, int nq, int qChunk, double dx, double dy,
                                 double dz, double theta, int isPn, double *psi, double *flux,
-                                cudaStream_t st)
+                                int *errorFlag, cudaStream_t st)
 {
+    if (qChunk < nq && (qChunk & 31))
+        return cudaErrorInvalidValue;
 #define C3D_NT_CASE(NT)                                                                            \
     case NT:                                                                                       \
-        return kinetic_t<NT>(g, alpha, M, w, xi, eta, mu, nq, qChunk, dx, dy, dz, theta, isPn,     \
-                             psi, flux, st);
+        return kinetic_t<NT>(g, alpha, mfA, mfP, nq, qChunk, dx, dy, dz, theta, isPn, psi, flux,   \
+                             errorFlag, st);
     switch ((g.nm + 7) / 8) {
         C3D_NT_CASE(1)
         C3D_NT_CASE(2)
@@ -589,13 +601,6 @@ cudaError_t launch_kinetic_flux(const GridDims &g, const double *alpha, const do
         return cudaErrorInvalidValue;
     }
 #undef C3D_NT_CASE
-}
-
-// Directions per materialised-ansatz chunk (bounded by the HBM budget only).
-int kinetic_max_chunk(int nm)
-{
-    (void)nm;
-    return 1 << 20;
 }
 
 cudaError_t launch_moment_flux(const GridDims &g, const double *u, const double *ops, double dx,
