@@ -28,7 +28,7 @@ HEADER_SYMBOLS = [
     "c3d_step", "c3d_sync", "c3d_closure_records", "c3d_closure_stats_get",
     "c3d_closure_stats_reset", "c3d_closure_vectors", "c3d_build_quadrature",
     "c3d_launch_count", "c3d_timing_enable", "c3d_timing_get", "c3d_closure_vectors_noalloc",
-    "c3d_set_gaunt", "c3d_set_engine",
+    "c3d_set_gaunt", "c3d_set_engine", "c3d_set_ghost_mirroring",
 ]
 
 
@@ -93,6 +93,7 @@ def lib():
         L.c3d_build_quadrature.argtypes = [ctypes.c_int, ctypes.c_int] + [_dp] * 6
         L.c3d_set_gaunt.argtypes = [vp, ctypes.c_int, _dp, _ip, _ip, _dp]
         L.c3d_set_engine.argtypes = [vp, ctypes.c_int]
+        L.c3d_set_ghost_mirroring.argtypes = [vp, ctypes.c_int]
         L.c3d_timing_enable.argtypes = [vp, ctypes.c_int]
         L.c3d_timing_get.argtypes = [vp, _dp, ctypes.POINTER(ctypes.c_longlong)]
         L.c3d_launch_count.argtypes = [vp]
@@ -243,6 +244,9 @@ class Context:
     def set_engine(self, engine):
         """0: work-list rounds (default), 1: persistent kernel."""
         check(lib().c3d_set_engine(self.h, engine), "c3d_set_engine")
+
+    def set_ghost_mirroring(self, on):
+        check(lib().c3d_set_ghost_mirroring(self.h, int(bool(on))), "c3d_set_ghost_mirroring")
 
     def set_gaunt(self, nm2, M2, row, col, val):
         """Gaunt form of the Hessian (CSR of beta); None switches back to the direct form."""

@@ -39,6 +39,7 @@ struct RoundsLaunch {
     const GauntTerm *terms;    // Gaunt: the beta terms in tile-slot order
     double m0;
     long long ncells;
+    const int *cellMap;        // closure cell i -> grid cell cellMap[i] (null: identity)
     double *u, *alpha;
     int *iters, *iterGamma, *regIdx, *status;
     unsigned long long *failCount, *stats;
@@ -70,6 +71,9 @@ cudaError_t launch_kinetic_flux(const GridDims &g, const double *alpha, const do
                                 double dz, double theta, int isPn, double *psi, double *flux,
                                 int *errorFlag, cudaStream_t st);
 size_t flux_frag_doubles(int nm, int nq, int which);
+cudaError_t launch_ghost_fill_int(const GridDims &g, int *a, int numSMs, cudaStream_t st);
+cudaError_t launch_ghost_mirror_check(const GridDims &g, const double *a, int *flag, int numSMs,
+                                      cudaStream_t st);
 void flux_frags(int nm, int nq, const double *M, const double *w, const double *xi,
                 const double *eta, const double *mu, double *mfA, double *mfP);
 cudaError_t launch_moment_flux(const GridDims &g, const double *u, const double *ops, double dx,
@@ -158,6 +162,14 @@ struct c3d_ctx {
     bool gaunt = false;
     double *gChunks = nullptr, *gVal = nullptr;
     int *gRow = nullptr, *gCol = nullptr;
+    // face-ghost mirroring: when every face ghost's multipliers equal its periodic image's
+    // (bitwise), the closure solves only the other cells (cellMap) and copies the face ghosts
+    int *cellMap = nullptr;
+    long long cellMapCount = 0;
+    int *mirrorFlag = nullptr;     // device
+    int *mirrorHost = nullptr;     // pinned
+    bool mirror = true;
+    long long mirroredClosures = 0;
     int2 *gPlan = nullptr;         // tiled assembly plan of the work-list engine
     GauntTerm *gTerms = nullptr;
     // optional event timing of the closure and flux launches (kind 0 closure, 1 flux)
@@ -197,13 +209,15 @@ static void free_ctx(c3d_ctx *c)
                     c->pnops, c->psi,    c->iters,    c->iterGamma, c->regIdx, c->status,
                     c->counter, c->failCount, c->stats, c->errorFlag, c->gChunks, c->gVal,
                     c->gRow, c->gCol, c->gPlan, c->gTerms, c->rState, c->rListA, c->rListB,
-                    c->rCounts, c->rBuf, c->mfA, c->mfP};
+                    c->rCounts, c->rBuf, c->mfA, c->mfP, c->cellMap, c->mirrorFlag};
     for (void *p : ptrs)
         if (p)
             cudaFree(p);
     timing_clear(c);
     if (c->rHostCount)
         cudaFreeHost(c->rHostCount);
+    if (c->mirrorHost)
+        cudaFreeHost(c->mirrorHost);
     if (c->ownStream && c->stream)
         cudaStreamDestroy(c->stream);
     delete c;
@@ -447,7 +461,7 @@ static c3d_status ensure_rounds(c3d_ctx *c, long long n)
 }
 
 static c3d_status run_closure(c3d_ctx *c, long long n, double *u, double *alpha, int *iters,
-                              int *iterGamma, int *regIdx, int *status)
+                              int *iterGamma, int *regIdx, int *status, const int *cellMap = nullptr)
 {
     if (c->engine == 0) {
         c3d_status s = ensure_rounds(c, n);
@@ -460,6 +474,7 @@ static c3d_status run_closure(c3d_ctx *c, long long n, double *u, double *alpha,
         R.terms = c->gTerms;
         R.m0 = c->m0;
         R.ncells = n;
+        R.cellMap = cellMap;
         R.u = u;
         R.alpha = alpha;
         R.iters = iters;
@@ -523,6 +538,53 @@ c3d_status c3d_closure(c3d_ctx *c)
         return fail(C3D_ERR_INVALID, "c3d_closure: null context");
     if (c->solver != 1)
         return fail(C3D_ERR_INVALID, "c3d_closure: the closure belongs to the M_N solver");
+    if (c->engine == 0 && c->mirror) {
+        // Face ghosts hold copies of their periodic images (src/comm.cpp:281-323); when their
+        // multipliers (the warm starts) are bitwise those of the images too, the per-cell
+        // solve of the reference gives them the images' results, so they are copied after
+        // solving the other cells instead. Edge and corner ghosts are solved as before.
+        if (!c->cellMap) {
+            std::vector<int> map;
+            const GridDims &g = c->g;
+            map.reserve((size_t)g.nall());
+            for (int i = 0; i < g.nxg(); ++i)
+                for (int j = 0; j < g.nyg(); ++j)
+                    for (int k = 0; k < g.nzg(); ++k) {
+                        int gi = (i >= 2 && i < g.nx + 2), gj = (j >= 2 && j < g.ny + 2),
+                            gk = (k >= 2 && k < g.nz + 2);
+                        if (gi + gj + gk != 2) // not a face ghost
+                            map.push_back((int)g.cell(i, j, k));
+                    }
+            if (cudaMalloc(&c->cellMap, map.size() * sizeof(int)) != cudaSuccess ||
+                cudaMalloc(&c->mirrorFlag, sizeof(int)) != cudaSuccess ||
+                cudaMallocHost(&c->mirrorHost, sizeof(int)) != cudaSuccess) {
+                cudaGetLastError();
+                return fail(C3D_ERR_OOM, "c3d_closure: device allocation failed");
+            }
+            C3D_CUDA(cudaMemcpy(c->cellMap, map.data(), map.size() * sizeof(int),
+                                cudaMemcpyHostToDevice));
+            c->cellMapCount = (long long)map.size();
+        }
+        C3D_CUDA(cudaMemsetAsync(c->mirrorFlag, 0, sizeof(int), c->stream));
+        C3D_CUDA(launch_ghost_mirror_check(c->g, c->alpha, c->mirrorFlag, c->numSMs, c->stream));
+        C3D_CUDA(cudaMemcpyAsync(c->mirrorHost, c->mirrorFlag, sizeof(int), cudaMemcpyDeviceToHost,
+                                 c->stream));
+        C3D_CUDA(cudaStreamSynchronize(c->stream));
+        c->launches += 1;
+        if (*c->mirrorHost == 0) {
+            c3d_status s = run_closure(c, c->cellMapCount, c->u, c->alpha, c->iters, c->iterGamma,
+                                       c->regIdx, c->status, c->cellMap);
+            if (s != C3D_OK)
+                return s;
+            C3D_CUDA(launch_ghost_fill(c->g, c->alpha, c->numSMs, c->stream));
+            C3D_CUDA(launch_ghost_fill(c->g, c->u, c->numSMs, c->stream));
+            for (int *a : {c->iters, c->iterGamma, c->regIdx, c->status})
+                C3D_CUDA(launch_ghost_fill_int(c->g, a, c->numSMs, c->stream));
+            c->launches += 6;
+            c->mirroredClosures++;
+            return C3D_OK;
+        }
+    }
     return run_closure(c, c->g.nall(), c->u, c->alpha, c->iters, c->iterGamma, c->regIdx, c->status);
 }
 
@@ -637,6 +699,14 @@ c3d_status c3d_set_engine(c3d_ctx *c, int engine)
     if (!c || engine < 0 || engine > 1)
         return fail(C3D_ERR_INVALID, "c3d_set_engine: engine must be 0 (work list) or 1 (persistent)");
     c->engine = engine;
+    return C3D_OK;
+}
+
+c3d_status c3d_set_ghost_mirroring(c3d_ctx *c, int on)
+{
+    if (!c)
+        return fail(C3D_ERR_INVALID, "c3d_set_ghost_mirroring: null context");
+    c->mirror = on != 0;
     return C3D_OK;
 }
 

@@ -82,5 +82,55 @@ struct GridDims {
     __host__ __device__ long long ninterior() const { return (long long)nx * ny * nz; }
 };
 
+// Interior-cell index (k fastest) -> grid cell index.
+__host__ __device__ inline long long interior_cell(const GridDims &g, long long n)
+{
+    int k = (int)(n % g.nz);
+    long long r = n / g.nz;
+    int j = (int)(r % g.ny);
+    int i = (int)(r / g.ny);
+    return g.cell(i + 2, j + 2, k + 2);
+}
+
+// Face ghost cells: 2 layers per face over the interior ranges of the other two axes (no
+// edges or corners), f in [0, 4 (ny nz + nx nz + nx ny)). dst is the ghost cell, src its
+// periodic image inside the domain (src/comm.cpp:281-323).
+__host__ __device__ inline long long ghost_faces(const GridDims &g)
+{
+    return 4LL * g.ny * g.nz + 4LL * g.nx * g.nz + 4LL * g.nx * g.ny;
+}
+__host__ __device__ inline void ghost_pair(const GridDims &g, long long f, long long &dst,
+                                           long long &src)
+{
+    const long long fx = 4LL * g.ny * g.nz, fy = 4LL * g.nx * g.nz;
+    if (f < fx) {
+        int side = (int)(f / (2LL * g.ny * g.nz)); // 0: low ghosts, 1: high ghosts
+        long long r = f % (2LL * g.ny * g.nz);
+        int l = (int)(r / ((long long)g.ny * g.nz));
+        long long r2 = r % ((long long)g.ny * g.nz);
+        int j = 2 + (int)(r2 / g.nz), k = 2 + (int)(r2 % g.nz);
+        dst = side == 0 ? g.cell(l, j, k) : g.cell(g.nx + 2 + l, j, k);
+        src = side == 0 ? g.cell(g.nx + l, j, k) : g.cell(2 + l, j, k);
+    } else if (f < fx + fy) {
+        f -= fx;
+        int side = (int)(f / (2LL * g.nx * g.nz));
+        long long r = f % (2LL * g.nx * g.nz);
+        int l = (int)(r / ((long long)g.nx * g.nz));
+        long long r2 = r % ((long long)g.nx * g.nz);
+        int i = 2 + (int)(r2 / g.nz), k = 2 + (int)(r2 % g.nz);
+        dst = side == 0 ? g.cell(i, l, k) : g.cell(i, g.ny + 2 + l, k);
+        src = side == 0 ? g.cell(i, g.ny + l, k) : g.cell(i, 2 + l, k);
+    } else {
+        f -= fx + fy;
+        int side = (int)(f / (2LL * g.nx * g.ny));
+        long long r = f % (2LL * g.nx * g.ny);
+        int l = (int)(r / ((long long)g.nx * g.ny));
+        long long r2 = r % ((long long)g.nx * g.ny);
+        int i = 2 + (int)(r2 / g.ny), j = 2 + (int)(r2 % g.ny);
+        dst = side == 0 ? g.cell(i, j, l) : g.cell(i, j, g.nz + 2 + l);
+        src = side == 0 ? g.cell(i, j, g.nz + l) : g.cell(i, j, 2 + l);
+    }
+}
+
 
 } // namespace c3d

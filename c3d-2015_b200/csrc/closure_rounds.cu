@@ -89,8 +89,8 @@ template <int NT> using TSlot = Slot<NT, true>;
 
 template <int NT>
 __global__ void __launch_bounds__(RW * 32)
-    rounds_init_kernel(ClosureParams P, long long ncells, Outputs O, CellState<NT> *state,
-                       int *listOut, unsigned int *countOut)
+    rounds_init_kernel(ClosureParams P, long long ncells, const int *__restrict__ cellMap,
+                       Outputs O, CellState<NT> *state, int *listOut, unsigned int *countOut)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     Slot<NT> *slots = reinterpret_cast<Slot<NT> *>(smem_raw);
@@ -99,7 +99,8 @@ __global__ void __launch_bounds__(RW * 32)
     if (c >= ncells)
         return;
     Slot<NT> &sl = slots[warp];
-    load_cell(sl, P, O, c, lane);
+    // the state and work lists use the closure's own numbering c; outputs the grid cell's
+    load_cell(sl, P, O, cellMap ? (long long)cellMap[c] : c, lane);
     slot_to_state(sl, state[c], lane);
     append_if_needed(sl, c, lane, listOut, countOut);
 }
@@ -417,6 +418,7 @@ struct RoundsLaunch {
     const GauntTerm *terms;    // Gaunt: the beta terms in tile-slot order
     double m0;                 // M[0][0]
     long long ncells;
+    const int *cellMap;        // closure cell i -> grid cell cellMap[i] (null: identity)
     double *u, *alpha;
     int *iters, *iterGamma, *regIdx, *status;
     unsigned long long *failCount, *stats;
@@ -497,7 +499,7 @@ template <int NT, int NT2, bool GAUNT> static cudaError_t rounds_t(const RoundsL
     if (e != cudaSuccess)
         return e;
     rounds_init_kernel<NT><<<(unsigned)((R.ncells + RW - 1) / RW), RW * 32, slotSmem, st>>>(
-        P, R.ncells, O, state, listA, cA);
+        P, R.ncells, R.cellMap, O, state, listA, cA);
     *R.launches += 2;
     e = cudaMemcpyAsync(R.hostCount, cA, sizeof(unsigned int), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess)

@@ -10,8 +10,9 @@
 // (nx+4)(ny+4)(nz+4) cells.
 //
 // Elementwise stages (ghost fill, Euler, average) reproduce the reference's
-// arithmetic bit for bit (unfused operations in its order). The flux sums
-// over directions in the reference's order, with fused multiply-adds.
+// arithmetic bit for bit (unfused operations in its order). The kinetic flux runs its
+// two contractions (exponents alpha.m_q, projection onto the moments) on the FP64 tensor
+// pipe, so its sums are reordered against the reference's (agreement to ~1e-15 relative).
 #include "c3d_common.cuh"
 
 namespace c3d {
@@ -21,61 +22,36 @@ namespace c3d {
 
 // Two periodic ghost layers per face over interior ranges of the other two axes
 // (no edges or corners). The three face groups read only interior cells, so
-// they run as one launch.
-__global__ void ghost_fill_kernel(GridDims g, double *__restrict__ u)
+// they run as one launch. T: double state arrays (ncomp = nm) or int per-cell records.
+template <typename T>
+__global__ void ghost_fill_kernel(GridDims g, T *__restrict__ u, int ncomp)
 {
-    const int nm = g.nm;
-    const long long fx = 4LL * g.ny * g.nz, fy = 4LL * g.nx * g.nz, fz = 4LL * g.nx * g.ny;
-    const long long total = (fx + fy + fz) * nm;
+    const long long total = ghost_faces(g) * ncomp;
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
          e += (long long)gridDim.x * blockDim.x) {
-        int m = (int)(e % nm);
-        long long f = e / nm;
+        int m = (int)(e % ncomp);
         long long dst, src;
-        if (f < fx) {
-            int side = (int)(f / (2LL * g.ny * g.nz)); // 0: low ghosts, 1: high ghosts
-            long long r = f % (2LL * g.ny * g.nz);
-            int l = (int)(r / ((long long)g.ny * g.nz));
-            long long r2 = r % ((long long)g.ny * g.nz);
-            int j = 2 + (int)(r2 / g.nz), k = 2 + (int)(r2 % g.nz);
-            if (side == 0) {
-                dst = g.cell(l, j, k);
-                src = g.cell(g.nx + l, j, k);
-            } else {
-                dst = g.cell(g.nx + 2 + l, j, k);
-                src = g.cell(2 + l, j, k);
-            }
-        } else if (f < fx + fy) {
-            f -= fx;
-            int side = (int)(f / (2LL * g.nx * g.nz));
-            long long r = f % (2LL * g.nx * g.nz);
-            int l = (int)(r / ((long long)g.nx * g.nz));
-            long long r2 = r % ((long long)g.nx * g.nz);
-            int i = 2 + (int)(r2 / g.nz), k = 2 + (int)(r2 % g.nz);
-            if (side == 0) {
-                dst = g.cell(i, l, k);
-                src = g.cell(i, g.ny + l, k);
-            } else {
-                dst = g.cell(i, g.ny + 2 + l, k);
-                src = g.cell(i, 2 + l, k);
-            }
-        } else {
-            f -= fx + fy;
-            int side = (int)(f / (2LL * g.nx * g.ny));
-            long long r = f % (2LL * g.nx * g.ny);
-            int l = (int)(r / ((long long)g.nx * g.ny));
-            long long r2 = r % ((long long)g.nx * g.ny);
-            int i = 2 + (int)(r2 / g.ny), j = 2 + (int)(r2 % g.ny);
-            if (side == 0) {
-                dst = g.cell(i, j, l);
-                src = g.cell(i, j, g.nz + l);
-            } else {
-                dst = g.cell(i, j, g.nz + 2 + l);
-                src = g.cell(i, j, 2 + l);
-            }
-        }
-        u[dst * nm + m] = u[src * nm + m];
+        ghost_pair(g, e / ncomp, dst, src);
+        u[dst * ncomp + m] = u[src * ncomp + m];
     }
+}
+
+// *flag = 1 if any face ghost of a differs (bitwise) from its periodic image.
+__global__ void ghost_mirror_check_kernel(GridDims g, const double *__restrict__ a, int ncomp,
+                                          int *flag)
+{
+    const long long total = ghost_faces(g) * ncomp;
+    const unsigned long long *b = reinterpret_cast<const unsigned long long *>(a);
+    bool diff = false;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        int m = (int)(e % ncomp);
+        long long dst, src;
+        ghost_pair(g, e / ncomp, dst, src);
+        diff |= b[dst * ncomp + m] != b[src * ncomp + m];
+    }
+    if (__syncthreads_or(diff) && threadIdx.x == 0)
+        atomicExch(flag, 1);
 }
 
 // ---------------------------------------------------------------- Euler / RK
@@ -89,15 +65,6 @@ __device__ __forceinline__ bool interior(const GridDims &g, long long c, int &i,
     return i >= 2 && i < g.nx + 2 && j >= 2 && j < g.ny + 2 && k >= 2 && k < g.nz + 2;
 }
 
-// Interior-cell index -> grid cell index.
-__device__ __forceinline__ long long interior_cell(const GridDims &g, long long n)
-{
-    int k = (int)(n % g.nz);
-    long long r = n / g.nz;
-    int j = (int)(r % g.ny);
-    int i = (int)(r / g.ny);
-    return g.cell(i + 2, j + 2, k + 2);
-}
 
 __global__ void euler_kernel(GridDims g, double *__restrict__ u, const double *__restrict__ flux,
                              const double *__restrict__ sigT, const double *__restrict__ sigS,
@@ -135,61 +102,6 @@ __global__ void rk_kernel(GridDims g, double *__restrict__ u, double *__restrict
         else
             u[x] = __dmul_rn(0.5, __dadd_rn(u[x], uOld[x]));
     }
-}
-
-// ---------------------------------------------------------------- kinetic flux
-
-// psi[(q - q0) * nall + c] = exp(alpha_c . m_q) (M_N) or alpha_c . m_q (P_N), for all
-// cells c and q0 <= q < q0 + nqc. The dot product runs in the reference's order
-// (moment index ascending, unfused), src/flux_kinetic.cpp:21-37.
-// (moment index ascending, unfused), src/flux_kinetic.cpp:21-37.
-template <int NM>
-__global__ void __launch_bounds__(128)
-    ansatz_kernel(GridDims g, const double *__restrict__ alpha, const double *__restrict__ M, int q0,
-                  int nqc, int isPn, double *__restrict__ psi)
-{
-    constexpr int TB = 128;
-    extern __shared__ double sh[];
-    double *sM = sh;             // nqc x NM
-    double *sA = sh + nqc * NM;  // TB x NM
-    const long long nall = g.nall();
-    for (int e = threadIdx.x; e < nqc * NM; e += TB)
-        sM[e] = M[(long long)q0 * NM + e];
-    long long c0 = (long long)blockIdx.x * TB;
-    long long n = nall - c0 < TB ? nall - c0 : TB;
-    for (long long e = threadIdx.x; e < n * NM; e += TB)
-        sA[e] = alpha[c0 * NM + e];
-    __syncthreads();
-    if (threadIdx.x >= n)
-        return;
-    double a[NM];
-#pragma unroll
-    for (int i = 0; i < NM; ++i)
-        a[i] = sA[threadIdx.x * NM + i];
-    long long c = c0 + threadIdx.x;
-    for (int q = 0; q < nqc; ++q) {
-        double z = 0.0;
-#pragma unroll
-        for (int i = 0; i < NM; ++i)
-            z = __dadd_rn(z, __dmul_rn(a[i], sM[q * NM + i]));
-        psi[(long long)q * nall + c] = isPn ? z : exp(z);
-    }
-}
-
-__device__ __forceinline__ double sgn1(double x) { return x >= 0.0 ? 1.0 : -1.0; }
-
-// minmod / slopefit, src/flux_kinetic.cpp:45-60 (MIN/MAX/SIGN macros of src/utils.h:12-14).
-__device__ __forceinline__ double minmod(double x, double y)
-{
-    double s = sgn1(x);
-    double ax = fabs(x), b = y * s;
-    double mn = ax < b ? ax : b;
-    double mx = 0.0 > mn ? 0.0 : mn;
-    return s * mx;
-}
-__device__ __forceinline__ double slopefit(double th, double l, double c, double r)
-{
-    return minmod(th * (r - c), minmod(0.5 * (r - l), th * (c - l)));
 }
 
 // ---------------------------------------------------------------- kinetic flux on the tensor pipe
@@ -309,16 +221,30 @@ __global__ void __launch_bounds__(256)
     }
 }
 
-// Limited upwind difference along one axis for either sign of the direction cosine,
-// src/flux_kinetic.cpp:130-189: with h = +1/2 (om > 0, values k1..k4 at offsets -2..1)
-// or h = -1/2 (om <= 0, offsets -1..2), f = ((k3 + h s(k2,k3,k4)) - k2) - h s(k1,k2,k3).
-__device__ __forceinline__ double axis_flux_bf(double om, double w, double th, const double *p,
-                                               long long c, long long st)
+// minmod of src/flux_kinetic.cpp:45-50 as a select: the same value (x when |x| < |y|, else
+// y, for operands of one sign; 0 otherwise), except possibly for the sign of a zero and for
+// operands whose product underflows.
+__device__ __forceinline__ double minmod_sel(double x, double y)
 {
-    const long long b = (om > 0) ? c - 2 * st : c - st;
-    const double k1 = p[b], k2 = p[b + st], k3 = p[b + 2 * st], k4 = p[b + 3 * st];
-    const double h = (om > 0) ? 0.5 : -0.5;
-    const double f = k3 + h * slopefit(th, k2, k3, k4) - k2 - h * slopefit(th, k1, k2, k3);
+    return (x * y > 0.0) ? (fabs(x) < fabs(y) ? x : y) : 0.0;
+}
+
+// Limited upwind difference along one axis for either sign of the direction cosine om,
+// src/flux_kinetic.cpp:130-189, times om w. With h = +1/2 (om > 0: values k1..k4 at offsets
+// -2..1) or h = -1/2 (om <= 0: offsets -1..2),
+//   f = ((k3 + h s(k2,k3,k4)) - k2) - h s(k1,k2,k3),  s(l,c,r) = slopefit (src/flux_kinetic.cpp:56-61);
+// h s is exact, so the fused forms below round as the reference's expression.
+__device__ __forceinline__ double axis_flux_bf(double om, double w, double th, const double *pc,
+                                               long long st)
+{
+    const bool pos = om > 0;
+    const double *b = pos ? pc - 2 * st : pc - st;
+    const double k1 = b[0], k2 = b[st], k3 = b[2 * st], k4 = b[3 * st];
+    const double h = pos ? 0.5 : -0.5;
+    const double t32 = th * (k3 - k2);
+    const double s1 = minmod_sel(th * (k4 - k3), minmod_sel(0.5 * (k4 - k2), t32));
+    const double s2 = minmod_sel(t32, minmod_sel(0.5 * (k3 - k1), th * (k2 - k1)));
+    const double f = fma(-h, s2, fma(h, s1, k3) - k2);
     return f * om * w;
 }
 
@@ -385,11 +311,11 @@ __global__ void __launch_bounds__(256)
             const int ql = 32 * t + qq;
             double sv = 0.0;
             if (c >= 0 && ql < nqc) {
-                const double *p = psi + (long long)ql * nall;
+                const double *pc = psi + (long long)ql * nall + c;
                 const double wq = dirs[qq + 96];
-                const double fx = axis_flux_bf(dirs[qq], wq, theta, p, c, sx);
-                const double fy = axis_flux_bf(dirs[qq + 32], wq, theta, p, c, sy);
-                const double fz = axis_flux_bf(dirs[qq + 64], wq, theta, p, c, sz);
+                const double fx = axis_flux_bf(dirs[qq], wq, theta, pc, sx);
+                const double fy = axis_flux_bf(dirs[qq + 32], wq, theta, pc, sy);
+                const double fz = axis_flux_bf(dirs[qq + 64], wq, theta, pc, sz);
                 sv = fx * rdx + fy * rdy + fz * rdz;
             }
             sS[qq * CS + cl] = sv;
@@ -493,8 +419,21 @@ static int grid_for(long long n, int threads, int numSMs)
 
 cudaError_t launch_ghost_fill(const GridDims &g, double *u, int numSMs, cudaStream_t st)
 {
-    long long total = (4LL * g.ny * g.nz + 4LL * g.nx * g.nz + 4LL * g.nx * g.ny) * g.nm;
-    ghost_fill_kernel<<<grid_for(total, 256, numSMs), 256, 0, st>>>(g, u);
+    ghost_fill_kernel<double><<<grid_for(ghost_faces(g) * g.nm, 256, numSMs), 256, 0, st>>>(g, u, g.nm);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ghost_fill_int(const GridDims &g, int *a, int numSMs, cudaStream_t st)
+{
+    ghost_fill_kernel<int><<<grid_for(ghost_faces(g), 256, numSMs), 256, 0, st>>>(g, a, 1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ghost_mirror_check(const GridDims &g, const double *a, int *flag, int numSMs,
+                                      cudaStream_t st)
+{
+    ghost_mirror_check_kernel<<<grid_for(ghost_faces(g) * g.nm, 256, numSMs), 256, 0, st>>>(
+        g, a, g.nm, flag);
     return cudaGetLastError();
 }
 
@@ -559,7 +498,8 @@ static cudaError_t kinetic_t(const GridDims &g, const double *alpha, const doubl
         ansatz_dmma_kernel<NT><<<(unsigned)((g.nall() + 63) / 64), 256, 0, st>>>(
             g, alpha, mfA, q0, nqc, isPn, psi, errorFlag);
         const size_t kinSmem = (size_t)(FLUX_STAGES * (8 * NT * 32 + 128) + 32 * 68) * 8;
-        if (kinSmem > 48 * 1024) {
+        // opt in above the 48 KB default for the dynamic part plus the ~1.3 KB static part
+        if (kinSmem > 46 * 1024) {
             cudaError_t e = cudaFuncSetAttribute(kinetic_dmma_kernel<NT>,
                                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                  (int)kinSmem);

@@ -167,8 +167,19 @@ c3d_status c3d_set_gaunt(c3d_ctx *ctx, int nm2, const double *M2, const int *row
  * the quadrature sums of every listed cell, then a Newton kernel with one warp per cell,
  * re-listing cells that need another pass (the reference's Optimization::opt stacks,
  * src/opt/optBatch.cpp:350-472); 1 runs one persistent kernel whose warps pull cells
- * from a device counter. Both compute the same per-cell arithmetic. */
+ * from a device counter. Both run the reference's per-cell algorithm; they differ in the
+ * blocking of the Cholesky factorisation and of the triangular solves (engine 0: 8x8 tiles
+ * with tensor-core trailing updates), so results agree to rounding. */
 c3d_status c3d_set_engine(c3d_ctx *ctx, int engine);
+
+/* Face-ghost mirroring of the grid closure (engine 0; on by default). The reference solves
+ * every cell, ghosts included (src/update.cpp:51-53, 119-123). A face ghost holds a copy of
+ * its periodic image's moments, so when its multipliers (the warm start) also equal the
+ * image's bit for bit -- checked on the device before each closure -- its solve would
+ * reproduce the image's; the closure then solves the other cells and copies multipliers,
+ * regularised moments and records to the face ghosts. Results are identical either way;
+ * closure statistics then count the solved cells only. No counterpart in the reference. */
+c3d_status c3d_set_ghost_mirroring(c3d_ctx *ctx, int on);
 
 /* Standalone batched closure of n independent moment vectors (device
  * pointers u[n*nm], alpha[n*nm], solved in place; records may be NULL).

@@ -327,3 +327,32 @@ def test_engines_match_oracle(oracle, engine, gaunt):
     rel = np.linalg.norm(ag[ok] - ao[ok], axis=1) / np.linalg.norm(ao[ok], axis=1)
     assert rel.max() < 1e-10, rel.max()
     assert (out["totalIter"] > 1).sum() > 100
+
+
+def test_ghost_mirroring_is_exact(oracle):
+    """Face-ghost mirroring (solve the non-face cells, copy the face ghosts from their
+    periodic images) gives bit-identical moments, multipliers and records to solving every
+    cell as the reference does, and engages when the face ghosts mirror their images."""
+    S = _setup(oracle, N=2, Q=12, steps_before=1)
+    n, nall = S["n"], S["nall"]
+    faces = 4 * 3 * n * n
+    u0, a0 = S["u"].copy(), S["alpha"].copy()
+    oracle.ghost_fill(S["g"], u0)  # face ghosts = periodic images, multipliers included
+    oracle.ghost_fill(S["g"], a0)
+    out = []
+    for on in (False, True):
+        ctx = _ctx(S)
+        ctx.set_ghost_mirroring(on)
+        ctx.set_state(u=u0, alpha=a0, sig_t=S["sig"], sig_s=S["sig"])
+        ctx.reset_stats()
+        for _ in range(2):
+            ctx.step(S["dt"])
+        ctx.sync()
+        u, a = ctx.get_state()
+        rec = ctx.records()
+        out.append((u, a, rec["iters"], rec["regIndex"], rec["status"], ctx.stats().cells))
+        ctx.close()
+    for x, y in zip(out[0][:5], out[1][:5]):
+        assert np.array_equal(x, y)
+    assert out[0][5] == 4 * nall             # 2 steps x 2 stages, every cell
+    assert out[1][5] == 4 * (nall - faces)   # face ghosts copied
