@@ -35,6 +35,7 @@ cudaError_t launch_closure_gaunt(const ClosureLaunch &L, const GauntTables &G);
 struct RoundsLaunch {
     const ClosureParams *P;
     const double *chunks;
+    int nm2;                   // Gaunt: extended moments (chunk rows: nm2 + the weight row)
     const int2 *plan;          // Gaunt: per tile slot {first term, terms} (-1: identity)
     const GauntTerm *terms;    // Gaunt: the beta terms in tile-slot order
     double m0;
@@ -170,6 +171,7 @@ struct c3d_ctx {
     int *mirrorHost = nullptr;     // pinned
     bool mirror = true;
     long long mirroredClosures = 0;
+    double *gChunksC = nullptr;    // work-list engine: chunks of nm2 M2 rows + the weight row
     int2 *gPlan = nullptr;         // tiled assembly plan of the work-list engine
     GauntTerm *gTerms = nullptr;
     // optional event timing of the closure and flux launches (kind 0 closure, 1 flux)
@@ -209,7 +211,8 @@ static void free_ctx(c3d_ctx *c)
                     c->pnops, c->psi,    c->iters,    c->iterGamma, c->regIdx, c->status,
                     c->counter, c->failCount, c->stats, c->errorFlag, c->gChunks, c->gVal,
                     c->gRow, c->gCol, c->gPlan, c->gTerms, c->rState, c->rListA, c->rListB,
-                    c->rCounts, c->rBuf, c->mfA, c->mfP, c->cellMap, c->mirrorFlag};
+                    c->rCounts, c->rBuf, c->mfA, c->mfP, c->cellMap, c->mirrorFlag,
+                    c->gChunksC};
     for (void *p : ptrs)
         if (p)
             cudaFree(p);
@@ -469,7 +472,8 @@ static c3d_status run_closure(c3d_ctx *c, long long n, double *u, double *alpha,
             return s;
         RoundsLaunch R{};
         R.P = &c->cp;
-        R.chunks = c->gaunt ? c->gChunks : c->chunks;
+        R.chunks = c->gaunt ? c->gChunksC : c->chunks;
+        R.nm2 = c->nm2;
         R.plan = c->gPlan;
         R.terms = c->gTerms;
         R.m0 = c->m0;
@@ -636,6 +640,30 @@ c3d_status c3d_set_gaunt(c3d_ctx *c, int nm2, const double *M2, const int *rowPt
     cudaMemcpy(drow, rowPtr, (size_t)(nm * nm + 1) * 4, cudaMemcpyHostToDevice);
     cudaMemcpy(dcol, colInd, (size_t)nnz * 4, cudaMemcpyHostToDevice);
     cudaMemcpy(dval, val, (size_t)nnz * 8, cudaMemcpyHostToDevice);
+    // compact chunks of the work-list engine: nm2 rows of M2, then the weights
+    const size_t perC = (size_t)(nm2 + 1) * QCP;
+    std::vector<double> chc((size_t)nch * perC, 0.0);
+    for (int k = 0; k < nch; ++k)
+        for (int qq = 0; qq < QC; ++qq) {
+            int q = k * QC + qq;
+            if (q >= nq)
+                break;
+            for (int r = 0; r < nm2; ++r)
+                chc[k * perC + (size_t)r * QCP + qq] = M2[(size_t)q * nm2 + r];
+            chc[k * perC + (size_t)nm2 * QCP + qq] = wh[q];
+        }
+    double *dchc = nullptr;
+    if (cudaMalloc(&dchc, chc.size() * 8) != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(dch);
+        cudaFree(drow);
+        cudaFree(dcol);
+        cudaFree(dval);
+        return fail(C3D_ERR_OOM, "c3d_set_gaunt: device allocation failed");
+    }
+    cudaMemcpy(dchc, chc.data(), chc.size() * 8, cudaMemcpyHostToDevice);
+    if (c->gChunksC) cudaFree(c->gChunksC);
+    c->gChunksC = dchc;
     // assembly plan of the tiled Hessian (work-list engine): per slot of the lower
     // triangle of 8x8 tiles, the CSR row of its (row >= col) element
     const int nt = (nm + 7) / 8, ls = 64 * nt * (nt + 1) / 2;

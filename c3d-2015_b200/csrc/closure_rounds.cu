@@ -105,37 +105,48 @@ __global__ void __launch_bounds__(RW * 32)
     append_if_needed(sl, c, lane, listOut, countOut);
 }
 
-// Pass of the Gaunt form: per listed cell, exponents and then either the extended
-// moments (need H) into momBuf[pos] or the trial objective's quadrature sum (need TRIAL)
-// into its state.
+// Pass of the Gaunt form over RWP = 16 listed cells per CTA (warp w: cells 2w, 2w + 1):
+// per staged chunk of QC directions, each lane forms the exponents alpha.m_q of both cells
+// for its direction (the reference's order: moment index ascending, unfused,
+// src/opt/fobj.cpp:64-79) and c_q = w_q e^{alpha.m_q}; then either the extended moments
+// mom_k = sum_q M2[k][q] c_q of the cells that need H, as a DMMA GEMM [nm2 x QC] x [QC x 16]
+// (each A fragment of M2 serves both 8-cell tiles), or the trial objective's quadrature sum.
+// Chunk layout (c3d_set_gaunt): nm2 rows of M2 then the weight row, row stride QCP.
+constexpr int RWP = 16;
+constexpr int CST2 = 20; // row stride (cells) of the coefficient tile: conflict-free B fragments
+
 template <int NT, int NT2>
 __global__ void __launch_bounds__(RW * 32, 2)
-    rounds_pass_gaunt_kernel(ClosureParams P, const double *__restrict__ chunks,
+    rounds_pass_gaunt_kernel(ClosureParams P, const double *__restrict__ chunks, int nm2,
                              const int *__restrict__ list, int n, CellState<NT> *state,
                              double *__restrict__ momBuf, int *errorFlag)
 {
-    constexpr int NMP = Cfg<NT>::NMP;
     constexpr int NM2P = 8 * NT2;
-    constexpr int CH = (NM2P + 1) * QCP;
     constexpr int RT = (NT2 + RW - 1) / RW;
     extern __shared__ __align__(128) unsigned char smem_raw[];
+    const int nm = P.nm, nchunks = P.nchunks;
+    const int CH = (nm2 + 1) * QCP; // doubles per chunk (multiple of 4: 16-byte copies)
     double *stage = reinterpret_cast<double *>(smem_raw);
-    double *cbuf = stage + GSTAGES * CH;       // QC x CST
-    double *alph = cbuf + QC * CST;            // RW x NMP
-    uint64_t *full = reinterpret_cast<uint64_t *>(alph + RW * NMP);
+    double *cbuf = stage + GSTAGES * CH; // QC x CST2
+    double *alph = cbuf + QC * CST2;     // RWP x nm
+    uint64_t *full = reinterpret_cast<uint64_t *>(alph + RWP * nm + (RWP * nm & 1));
     __shared__ int s_abort;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int nm = P.nm, nchunks = P.nchunks;
     const uint32_t chunkBytes = CH * sizeof(double);
-    const int pos = blockIdx.x * RW + warp;
-    int need = NEED_NONE;
-    long long cell = -1;
-    if (pos < n) {
-        cell = list[pos];
-        need = state[cell].s.need;
+    int need[2];
+    long long cell[2];
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+        const int pos = blockIdx.x * RWP + 2 * warp + e;
+        need[e] = NEED_NONE;
+        cell[e] = -1;
+        if (pos < n) {
+            cell[e] = list[pos];
+            need[e] = state[cell[e]].s.need;
+        }
+        for (int i = lane; i < nm; i += 32)
+            alph[(2 * warp + e) * nm + i] = cell[e] >= 0 ? state[cell[e]].alpha[i] : 0.0;
     }
-    for (int i = lane; i < NMP; i += 32)
-        alph[warp * NMP + i] = (cell >= 0 && i < nm) ? state[cell].alpha[i] : 0.0;
     if (tid == 0) {
         for (int s = 0; s < GSTAGES; ++s)
             mbar_init(&full[s], 1);
@@ -147,13 +158,14 @@ __global__ void __launch_bounds__(RW * 32, 2)
         }
     }
     __syncthreads();
-    const bool anyH = __syncthreads_or(need == NEED_H);
-    const double *al = alph + warp * NMP;
-    double acc[RT][2];
+    const bool anyH = __syncthreads_or(need[0] == NEED_H || need[1] == NEED_H);
+    const double *a0 = alph + (2 * warp) * nm, *a1 = a0 + nm;
+    double acc[RT][2][2];
 #pragma unroll
     for (int r = 0; r < RT; ++r)
-        acc[r][0] = acc[r][1] = 0.0;
-    double fpart = 0.0;
+        acc[r][0][0] = acc[r][0][1] = acc[r][1][0] = acc[r][1][1] = 0.0;
+    double fpart0 = 0.0, fpart1 = 0.0;
+    const bool any = need[0] != NEED_NONE || need[1] != NEED_NONE;
     for (int k = 0; k < nchunks; ++k) {
         uint32_t s = k % GSTAGES, parity = (k / GSTAGES) & 1u;
         if (!mbar_wait(&full[s], parity))
@@ -164,27 +176,42 @@ __global__ void __launch_bounds__(RW * 32, 2)
             return;
         }
         const double *ch = stage + s * CH;
-        double c = 0.0;
-        if (need != NEED_NONE) {
-            double z = 0.0;
-            for (int i = 0; i < nm; ++i)
-                z = __dadd_rn(z, __dmul_rn(al[i], ch[i * QCP + lane]));
-            c = __dmul_rn(ch[NM2P * QCP + lane], exp(z));
-            if (need == NEED_TRIAL)
-                fpart = __dadd_rn(fpart, c);
+        double c0 = 0.0, c1 = 0.0;
+        if (any) {
+            double z0 = 0.0, z1 = 0.0;
+            for (int i = 0; i < nm; ++i) {
+                const double m = ch[i * QCP + lane];
+                z0 = __dadd_rn(z0, __dmul_rn(a0[i], m));
+                z1 = __dadd_rn(z1, __dmul_rn(a1[i], m));
+            }
+            const double wq = ch[nm2 * QCP + lane];
+            if (need[0] != NEED_NONE) {
+                c0 = __dmul_rn(wq, exp(z0));
+                if (need[0] == NEED_TRIAL)
+                    fpart0 = __dadd_rn(fpart0, c0);
+            }
+            if (need[1] != NEED_NONE) {
+                c1 = __dmul_rn(wq, exp(z1));
+                if (need[1] == NEED_TRIAL)
+                    fpart1 = __dadd_rn(fpart1, c1);
+            }
         }
-        cbuf[lane * CST + warp] = (need == NEED_H) ? c : 0.0;
+        cbuf[lane * CST2 + 2 * warp] = (need[0] == NEED_H) ? c0 : 0.0;
+        cbuf[lane * CST2 + 2 * warp + 1] = (need[1] == NEED_H) ? c1 : 0.0;
         __syncthreads();
         if (anyH) {
 #pragma unroll
             for (int g = 0; g < QC / 4; ++g) {
-                double b = cbuf[(4 * g + (lane & 3)) * CST + (lane >> 2)];
+                const double b0 = cbuf[(4 * g + (lane & 3)) * CST2 + (lane >> 2)];
+                const double b1 = cbuf[(4 * g + (lane & 3)) * CST2 + 8 + (lane >> 2)];
 #pragma unroll
                 for (int r = 0; r < RT; ++r) {
-                    int rt = warp + r * RW;
+                    const int rt = warp + r * RW;
+                    const int row = 8 * rt + (lane >> 2);
                     if (rt < NT2) {
-                        double a = ch[(8 * rt + (lane >> 2)) * QCP + 4 * g + (lane & 3)];
-                        dmma(acc[r][0], acc[r][1], a, b);
+                        const double a = row < nm2 ? ch[row * QCP + 4 * g + (lane & 3)] : 0.0;
+                        dmma(acc[r][0][0], acc[r][0][1], a, b0);
+                        dmma(acc[r][1][0], acc[r][1][1], a, b1);
                     }
                 }
             }
@@ -196,23 +223,29 @@ __global__ void __launch_bounds__(RW * 32, 2)
         }
     }
     if (anyH) {
-        const int base = blockIdx.x * RW;
+        const int base = blockIdx.x * RWP;
 #pragma unroll
         for (int r = 0; r < RT; ++r) {
-            int rt = warp + r * RW;
+            const int rt = warp + r * RW;
             if (rt < NT2) {
-                int kk = 8 * rt + (lane >> 2), c0 = 2 * (lane & 3);
-                if (base + c0 < n)
-                    momBuf[(size_t)(base + c0) * NM2P + kk] = acc[r][0];
-                if (base + c0 + 1 < n)
-                    momBuf[(size_t)(base + c0 + 1) * NM2P + kk] = acc[r][1];
+                const int kk = 8 * rt + (lane >> 2);
+#pragma unroll
+                for (int t = 0; t < 2; ++t)
+#pragma unroll
+                    for (int e = 0; e < 2; ++e) {
+                        const int p = base + 8 * t + 2 * (lane & 3) + e;
+                        if (p < n)
+                            momBuf[(size_t)p * NM2P + kk] = acc[r][t][e];
+                    }
             }
         }
     }
-    if (need == NEED_TRIAL) {
-        double fq = warp_sum(fpart);
-        if (lane == 0)
-            state[cell].s.fquad = fq;
+    const double fq0 = warp_sum(fpart0), fq1 = warp_sum(fpart1);
+    if (lane == 0) {
+        if (need[0] == NEED_TRIAL)
+            state[cell[0]].s.fquad = fq0;
+        if (need[1] == NEED_TRIAL)
+            state[cell[1]].s.fquad = fq1;
     }
 }
 
@@ -414,6 +447,7 @@ __global__ void __launch_bounds__(RWN * 32)
 struct RoundsLaunch {
     const ClosureParams *P;
     const double *chunks;      // direct: (NMP+1) x QCP chunks; Gaunt: (NM2P+1) x QCP chunks
+    int nm2;                   // Gaunt: extended moments (chunk rows: nm2 + the weight row)
     const int2 *plan;          // Gaunt: per tile slot {first term, terms} (-1: identity)
     const GauntTerm *terms;    // Gaunt: the beta terms in tile-slot order
     double m0;                 // M[0][0]
@@ -477,9 +511,8 @@ template <int NT, int NT2, bool GAUNT> static cudaError_t rounds_t(const RoundsL
         return e;
     size_t passSmem;
     if (GAUNT) {
-        constexpr int NM2P = 8 * NT2;
-        passSmem = GSTAGES * (size_t)(NM2P + 1) * QCP * 8 + (size_t)QC * CST * 8 +
-                   (size_t)RW * Cfg<NT>::NMP * 8 + GSTAGES * 8;
+        passSmem = GSTAGES * (size_t)(R.nm2 + 1) * QCP * 8 + (size_t)QC * CST2 * 8 +
+                   (size_t)(RWP * P.nm + 1) * 8 + GSTAGES * 8;
         e = cudaFuncSetAttribute(rounds_pass_gaunt_kernel<NT, NT2>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)passSmem);
     } else {
@@ -518,8 +551,9 @@ template <int NT, int NT2, bool GAUNT> static cudaError_t rounds_t(const RoundsL
             int nb = (int)((count - off) < R.batch ? (count - off) : R.batch);
             unsigned grid = (unsigned)((nb + RW - 1) / RW);
             if (GAUNT)
-                rounds_pass_gaunt_kernel<NT, NT2><<<grid, RW * 32, passSmem, st>>>(
-                    P, R.chunks, listA + off, nb, state, R.buf, R.errorFlag);
+                rounds_pass_gaunt_kernel<NT, NT2><<<(unsigned)((nb + RWP - 1) / RWP), RW * 32,
+                                                    passSmem, st>>>(
+                    P, R.chunks, R.nm2, listA + off, nb, state, R.buf, R.errorFlag);
             else
                 rounds_pass_direct_kernel<NT><<<grid, RW * 32, passSmem, st>>>(
                     P, R.chunks, listA + off, nb, state, R.buf, R.errorFlag);
