@@ -79,6 +79,13 @@ template <int NT, bool TILED = false> struct alignas(16) Slot {
     double u[NMP], alpha[NMP], alpha0[NMP], uOrig[NMP], g[NMP], d[NMP], alphaOld[NMP], rinv[NMP];
     double L[LSIZE];
     SlotScalars s;
+    // g, d, alphaOld and rinv as one array of 4 NMP doubles (scratch between Hessian visits),
+    // addressed through the slot object so that it may span the four vectors
+    __device__ __forceinline__ double *scratch()
+    {
+        return reinterpret_cast<double *>(reinterpret_cast<unsigned char *>(this) +
+                                          4 * NMP * sizeof(double));
+    }
     // offset of element (i, j), i >= j
     __device__ static __forceinline__ int lx(int i, int j)
     {
@@ -376,6 +383,9 @@ __device__ void warp_apply_inverse(const S &sl, int n, int lane, double &x0, dou
 // the tiles off the diagonal act as 8-column mat-vec updates of the rows below (forward) or
 // above (backward). Padding rows (L = I there, rinv = 1) keep finite values and never feed
 // the real rows.
+// Kept out of line: inlined into its callers (direction and condition estimate), builds with
+// nvcc 12.9 for sm_100a gave iteration counts that differ from the oracle's on M_6 cells
+// (the M_6 closure parity test), while this form matches it.
 template <class S>
 __device__ __noinline__ void warp_apply_inverse_tiled(const S &sl, int lane, double &x0, double &x1)
 {

@@ -21,16 +21,17 @@
 
 namespace c3d {
 
-// Per-cell Newton state between rounds (the slot without the packed triangle).
+// Per-cell Newton state between rounds: the slot without the factor, the reciprocal
+// pivots and the gradient (recomputed from H on every Hessian visit, unused by trials).
 template <int NT> struct CellState {
     static constexpr int NMP = Cfg<NT>::NMP;
-    double u[NMP], alpha[NMP], alpha0[NMP], uOrig[NMP], g[NMP], d[NMP], alphaOld[NMP];
+    double u[NMP], alpha[NMP], alpha0[NMP], uOrig[NMP], d[NMP], alphaOld[NMP];
     SlotScalars s;
 };
 
 namespace {
 
-// lineSearch = false skips g, d and alphaOld, which a Hessian visit recomputes before use.
+// lineSearch = false skips d and alphaOld, which a Hessian visit recomputes before use.
 template <int NT, class S>
 __device__ void state_to_slot(const CellState<NT> &st, S &sl, int lane, bool lineSearch = true)
 {
@@ -41,7 +42,6 @@ __device__ void state_to_slot(const CellState<NT> &st, S &sl, int lane, bool lin
         sl.alpha0[i] = st.alpha0[i];
         sl.uOrig[i] = st.uOrig[i];
         if (lineSearch) {
-            sl.g[i] = st.g[i];
             sl.d[i] = st.d[i];
             sl.alphaOld[i] = st.alphaOld[i];
         }
@@ -61,7 +61,6 @@ __device__ void slot_to_state(const S &sl, CellState<NT> &st, int lane)
         st.alpha[i] = sl.alpha[i];
         st.alpha0[i] = sl.alpha0[i];
         st.uOrig[i] = sl.uOrig[i];
-        st.g[i] = sl.g[i];
         st.d[i] = sl.d[i];
         st.alphaOld[i] = sl.alphaOld[i];
     }
@@ -392,7 +391,7 @@ __global__ void __launch_bounds__(RWN * 32)
         sl.s.need = NEED_NONE;
     }
     if (GAUNT) {
-        double *mom = sl.g; // g, d, alphaOld, rinv are contiguous: NM2P <= 4 NMP doubles
+        double *mom = sl.scratch(); // g, d, alphaOld, rinv: NM2P <= 4 NMP doubles
         if (needH)
             for (int k = lane; k < NM2P; k += 32)
                 mom[k] = buf[(size_t)pos * NM2P + k];
@@ -411,7 +410,7 @@ __global__ void __launch_bounds__(RWN * 32)
                     const GauntTerm gt = terms[tt];
 #pragma unroll
                     for (int w = 0; w < RWN; ++w)
-                        h[w] = __dadd_rn(h[w], __dmul_rn(slots[w].g[gt.col], gt.v));
+                        h[w] = __dadd_rn(h[w], __dmul_rn(slots[w].scratch()[gt.col], gt.v));
                 }
 #pragma unroll
                 for (int w = 0; w < RWN; ++w)

@@ -1,0 +1,77 @@
+"""M_6 closure parity on cells near the realizability boundary.
+
+The 64^3 version of the M_6 benchmark workload (N=6, Q=28: 49 moments, 1568 directions,
+gaussian pulse of width 0.02 over a 1e-10 floor) is advanced three steps on the GPU; its
+cells -- the multi-iteration ones of the last closure plus a random sample -- are then
+solved again by both closure engines through c3d_closure_vectors and by the oracle, from
+the same moments and warm starts. Iteration counts must be identical except at rounding
+ties, and the multipliers agree to 1e-10. Parity at N <= 4 alone does not exercise the
+tiled factor, the condition estimate and the line search on such cells.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import c3d
+from oracle_lib import deck_text, make_opts, tie_cells
+from test_gpu_kernels import _gaunt_csr
+
+pytestmark = pytest.mark.gpu
+
+LADDER = [0.0, 1e-8, 1e-6, 1e-4, 1e-2, 1e-1]
+TOL = 1e-6
+
+
+def test_m6_cells_match_oracle(oracle, tmp_path):
+    import torch
+    deck = tmp_path / "input.deck"
+    deck.write_text(deck_text(NX=64, NY=64, NZ=64, MOMENT_ORDER=6, QUAD_ORDER=28, CFL_FACTOR=0.5,
+                              CROSS_SECTION=1.0, INIT_FLOOR=1e-10, GAUSS_SIGMA=0.02,
+                              INIT_COND="gaussian_psi", THETA=2.0, MN_TOL=TOL,
+                              MN_BATCHED="true", MN_USE_GAUNT_COEF="true",
+                              MN_USE_GAUNT_SPARSE="true",
+                              REG_LADDER=",".join(str(x) for x in LADDER),
+                              OMP_THREADS=os.cpu_count() or 1))
+    s = c3d.Solver(str(deck))
+    for _ in range(3):
+        s.update(s.max_dt)
+    s.sync()
+    s.pull()
+    nm = s.nm
+    A = s.arrays()
+    u = A["u"].reshape(-1, nm).copy()
+    a = A["alpha"].reshape(-1, nm).copy()
+    it = s.records()["iters"]
+    s.close()
+    multi = np.nonzero(it >= 2)[0]
+    assert len(multi) > 100
+    rng = np.random.default_rng(3)
+    pick = np.concatenate([multi[:3000], rng.choice(len(it), 2000, replace=False)])
+    T = oracle.tables(6, 28, gaunt=True)
+    row, col, val = _gaunt_csr(T, 1e-13)
+    uo, ao = u[pick].copy(), a[pick].copy()
+    ro = oracle.closure(make_opts(nm, T["nq"], nm2=T["nm2"], hess_mode=2, tol=TOL, ladder=LADDER),
+                        T, uo, ao)
+    ties = tie_cells(ro)
+    for engine in (0, 1):
+        ctx = c3d.Context(nx=1, ny=1, nz=1, nm=nm, nq=T["nq"], dx=1.0, dy=1.0, dz=1.0, M=T["M"],
+                          w=T["w"], xi=T["xi"], eta=T["eta"], mu=T["mu"], ladder=LADDER, tol=TOL)
+        ctx.set_engine(engine)
+        ctx.set_gaunt(T["nm2"], T["M2"], row, col, val)
+        du = torch.tensor(u[pick], device="cuda")
+        da = torch.tensor(a[pick], device="cuda")
+        itg = torch.zeros(len(pick), dtype=torch.int32, device="cuda")
+        stg = torch.zeros(len(pick), dtype=torch.int32, device="cuda")
+        torch.cuda.synchronize()
+        ctx.closure_vectors_device(len(pick), du.data_ptr(), da.data_ptr(), itg.data_ptr(), None,
+                                   None, stg.data_ptr())
+        ctx.sync()
+        itg, ag, stg = itg.cpu().numpy(), da.cpu().numpy(), stg.cpu().numpy()
+        ctx.close()
+        assert (stg == 0).all(), engine
+        mism = itg != ro["totalIter"]
+        assert not (mism & ~ties).any(), (engine, int((mism & ~ties).sum()))
+        ok = ~mism & (ro["status"] == 0)
+        rel = np.linalg.norm(ag[ok] - ao[ok], axis=1) / np.linalg.norm(ao[ok], axis=1)
+        assert rel.max() < 1e-10, (engine, rel.max())
