@@ -155,6 +155,17 @@ def closure_flops(nm, nq, iters, trials, hessian="gaunt"):
     return iters * per_iter + trials * per_trial
 
 
+def _hbm_peak_gbs():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"])
+    except Exception:
+        return 6650.0  # earlier measurement on this pool
+
+
+HBM_PEAK_GBS = _hbm_peak_gbs()
+
+
 def fp64_peak_tflops():
     """In-run FP64 reference: cuBLAS DGEMM 8192^3 through torch (burst, best of 5)."""
     import torch
@@ -413,7 +424,10 @@ def b200_arm(args):
         achieved = flops / max(1, closure_launches) / per_launch_s / 1e12
         roofline = dict(bound="tensor", pipe="fp64 (DMMA m8n8k4 + DFMA)", achieved=achieved,
                         peak=peak, unit="TFLOP/s", frac=achieved / peak if peak else None,
-                        traffic=profile_traffic("closure_fp64_m6_128"),
+                        traffic=(profile_traffic("closure_rounds_m6_64")
+                                 if args.engine == "rounds" and args.hessian == "gaunt" else None),
+                        traffic_source="profiles/closure_rounds_m6_64.txt: one closure's DRAM "
+                                       "bytes at 64^3 (ncu) scaled by solved cells to 128^3",
                         peak_source="in-run cuBLAS DGEMM 8192^3 via torch (FP64 is not in "
                                     "MEASURED_PEAKS.json)",
                         kernel=(("closure work-list rounds: rounds_pass_gaunt_kernel<7,22> + "
@@ -427,6 +441,20 @@ def b200_arm(args):
                         closure_ms_per_launch=ms[0] / max(1, closure_launches),
                         flux_ms_per_launch=ms[1] / max(1, int(cnt[1])),
                         closure_share_of_step=ms[0] / total_ms)
+        # the kinetic flux, second in the step: HBM view of the materialised-psi variant and
+        # its tensor-pipe work (exponents and projection)
+        nall_c = solver.nall
+        flux_ms = ms[1] / max(1, int(cnt[1]))
+        flux_bytes = 8.0 * (nall_c * nm + cells * nm + nall_c * nq + cells * nq)
+        flux_flops = 2.0 * nm * nq * (nall_c + cells)
+        flux_line = dict(ms_per_call=flux_ms, variant="materialised psi (FP64)",
+                         hbm_bytes_per_call=flux_bytes,
+                         achieved_gbs=flux_bytes / (flux_ms * 1e-3) / 1e9,
+                         hbm_peak_gbs=HBM_PEAK_GBS,
+                         hbm_frac=flux_bytes / (flux_ms * 1e-3) / 1e9 / HBM_PEAK_GBS,
+                         contraction_tflops=flux_flops / (flux_ms * 1e-3) / 1e12,
+                         note="FP64-pipe bound: exponents and projection on DMMA plus "
+                              "the limiter's FP64 arithmetic (profiles/kinetic_flux_m6_48.txt)")
         # CPU baseline: the reference closure on a bounded sample of this workload's cells
         cpu = None
         try:
@@ -456,7 +484,7 @@ def b200_arm(args):
                         mn_tol=MN_TOL, mn_batched=True, ladder=LADDER,
                         cells_per_step=2 * cells, l2="inputs larger than L2 (u, alpha 0.9 GB each)",
                         parallelism=f"replicas x{world}"),
-            roofline=roofline, cpu_baseline=cpu,
+            roofline=roofline, flux=flux_line, cpu_baseline=cpu,
             e2e=dict(value=e2e_value, unit=UNIT, h2d_bytes_per_step=2 * nv * 8,
                      d2h_bytes_per_step=2 * nv * 8, steps=e_steps),
             gpu_launches=int(launches), clocks=clk,
