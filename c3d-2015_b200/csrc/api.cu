@@ -36,8 +36,8 @@ struct RoundsLaunch {
     const ClosureParams *P;
     const double *chunks;
     int nm2;                   // Gaunt: extended moments (chunk rows: nm2 + the weight row)
-    const int2 *plan;          // Gaunt: per tile slot {first term, terms} (-1: identity)
-    const GauntTerm *terms;    // Gaunt: the beta terms in tile-slot order
+    const GauntTerm *gstream;  // Gaunt: assembly streams, entry s of thread t at s*128 + t
+    int streamLen;             // entries per thread
     double m0;
     long long ncells;
     const int *cellMap;        // closure cell i -> grid cell cellMap[i] (null: identity)
@@ -172,8 +172,8 @@ struct c3d_ctx {
     bool mirror = true;
     long long mirroredClosures = 0;
     double *gChunksC = nullptr;    // work-list engine: chunks of nm2 M2 rows + the weight row
-    int2 *gPlan = nullptr;         // tiled assembly plan of the work-list engine
-    GauntTerm *gTerms = nullptr;
+    GauntTerm *gStream = nullptr;  // tiled assembly streams of the work-list engine
+    int gStreamLen = 0;
     // optional event timing of the closure and flux launches (kind 0 closure, 1 flux)
     bool timing = false;
     std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> events;
@@ -210,7 +210,7 @@ static void free_ctx(c3d_ctx *c)
                     c->M,     c->w,      c->xi,       c->eta,     c->mu,     c->chunks,
                     c->pnops, c->psi,    c->iters,    c->iterGamma, c->regIdx, c->status,
                     c->counter, c->failCount, c->stats, c->errorFlag, c->gChunks, c->gVal,
-                    c->gRow, c->gCol, c->gPlan, c->gTerms, c->rState, c->rListA, c->rListB,
+                    c->gRow, c->gCol, c->gStream, c->rState, c->rListA, c->rListB,
                     c->rCounts, c->rBuf, c->mfA, c->mfP, c->cellMap, c->mirrorFlag,
                     c->gChunksC};
     for (void *p : ptrs)
@@ -474,8 +474,8 @@ static c3d_status run_closure(c3d_ctx *c, long long n, double *u, double *alpha,
         R.P = &c->cp;
         R.chunks = c->gaunt ? c->gChunksC : c->chunks;
         R.nm2 = c->nm2;
-        R.plan = c->gPlan;
-        R.terms = c->gTerms;
+        R.gstream = c->gStream;
+        R.streamLen = c->gStreamLen;
         R.m0 = c->m0;
         R.ncells = n;
         R.cellMap = cellMap;
@@ -664,51 +664,59 @@ c3d_status c3d_set_gaunt(c3d_ctx *c, int nm2, const double *M2, const int *rowPt
     cudaMemcpy(dchc, chc.data(), chc.size() * 8, cudaMemcpyHostToDevice);
     if (c->gChunksC) cudaFree(c->gChunksC);
     c->gChunksC = dchc;
-    // assembly plan of the tiled Hessian (work-list engine): per slot of the lower
-    // triangle of 8x8 tiles, the CSR row of its (row >= col) element
+    // assembly streams of the tiled Hessian (work-list engine). Thread t of the Newton
+    // kernel's CTA owns the tile slots e = t + 128 i of the lower triangle of 8x8 tiles; its
+    // stream lists, slot after slot, the CSR terms of beta for that slot's (row >= col)
+    // element in the reference's order, the last one marked with the slot (a slot without
+    // terms gets one zero term; identity padding slots one col = -1 entry). Streams are
+    // padded to a common length with no-op entries and interleaved across threads
+    // (entry s of thread t at s * 128 + t) so that a warp's loads coalesce.
     const int nt = (nm + 7) / 8, ls = 64 * nt * (nt + 1) / 2;
-    std::vector<int2> plan(ls);
-    std::vector<GauntTerm> terms;
-    terms.reserve((size_t)nnz);
+    std::vector<std::vector<GauntTerm>> lists(NEWTON_THREADS);
     for (int e = 0; e < ls; ++e) {
+        std::vector<GauntTerm> &st = lists[e % NEWTON_THREADS];
         const int t = e >> 6, rr = (e >> 3) & 7, cc = e & 7;
         int ib = 0;
         while ((ib + 1) * (ib + 2) / 2 <= t)
             ++ib;
         const int jb = t - ib * (ib + 1) / 2;
         const int i = 8 * ib + rr, j = 8 * jb + cc;
-        plan[e] = make_int2((int)terms.size(), 0);
-        if (ib == jb && cc > rr)
-            continue;
-        if (i >= nm || j >= nm) {
-            plan[e].y = (i == j) ? -1 : 0;
-            continue;
+        const size_t first = st.size();
+        if (!(ib == jb && cc > rr)) {
+            if (i >= nm || j >= nm) {
+                if (i == j)
+                    st.push_back(GauntTerm{1.0, -1, -1});
+            } else {
+                const int idx = j * nm + i;
+                for (int k = rowPtr[idx]; k < rowPtr[idx + 1]; ++k)
+                    st.push_back(GauntTerm{val[k], colInd[k], -1});
+            }
         }
-        const int idx = j * nm + i;
-        for (int k = rowPtr[idx]; k < rowPtr[idx + 1]; ++k)
-            terms.push_back(GauntTerm{val[k], colInd[k], 0});
-        plan[e].y = (int)terms.size() - plan[e].x;
+        if (st.size() == first)
+            st.push_back(GauntTerm{0.0, 0, -1});
+        st.back().slot = e;
     }
-    int2 *dplan = nullptr;
-    GauntTerm *dterms = nullptr;
-    if (cudaMalloc(&dplan, plan.size() * sizeof(int2)) != cudaSuccess ||
-        cudaMalloc(&dterms, (terms.empty() ? 1 : terms.size()) * sizeof(GauntTerm)) != cudaSuccess) {
+    size_t len = 0;
+    for (auto &st : lists)
+        len = st.size() > len ? st.size() : len;
+    std::vector<GauntTerm> stream(len * NEWTON_THREADS, GauntTerm{0.0, 0, -1});
+    for (int t = 0; t < NEWTON_THREADS; ++t)
+        for (size_t k = 0; k < lists[t].size(); ++k)
+            stream[k * NEWTON_THREADS + t] = lists[t][k];
+    GauntTerm *dstream = nullptr;
+    if (cudaMalloc(&dstream, stream.size() * sizeof(GauntTerm)) != cudaSuccess) {
         cudaGetLastError();
-        if (dplan) cudaFree(dplan);
         cudaFree(dch);
         cudaFree(drow);
         cudaFree(dcol);
         cudaFree(dval);
         return fail(C3D_ERR_OOM, "c3d_set_gaunt: device allocation failed");
     }
-    cudaMemcpy(dplan, plan.data(), plan.size() * sizeof(int2), cudaMemcpyHostToDevice);
-    if (!terms.empty())
-        cudaMemcpy(dterms, terms.data(), terms.size() * sizeof(GauntTerm), cudaMemcpyHostToDevice);
+    cudaMemcpy(dstream, stream.data(), stream.size() * sizeof(GauntTerm), cudaMemcpyHostToDevice);
     C3D_CUDA(cudaDeviceSynchronize());
-    if (c->gPlan) cudaFree(c->gPlan);
-    if (c->gTerms) cudaFree(c->gTerms);
-    c->gPlan = dplan;
-    c->gTerms = dterms;
+    if (c->gStream) cudaFree(c->gStream);
+    c->gStream = dstream;
+    c->gStreamLen = (int)len;
     if (c->gChunks) cudaFree(c->gChunks);
     if (c->gRow) cudaFree(c->gRow);
     if (c->gCol) cudaFree(c->gCol);

@@ -59,13 +59,18 @@ struct ClosureParams {
 
 __host__ __device__ inline int ceil_div(int a, int b) { return (a + b - 1) / b; }
 
-// One term beta_ijk of the Gaunt-form Hessian for the tiled assembly: H element of a tile
-// slot += v * moment[col] (src/opt/fobj.cpp:81-99).
+// One entry of the Gaunt-form Hessian assembly stream (src/opt/fobj.cpp:81-99): the
+// running H element += v * moment[col] (col = -1: the element is 1, an identity padding
+// slot); slot >= 0 ends tile slot `slot`, which then receives the element.
 struct __align__(16) GauntTerm {
     double v;
     int col;
-    int pad;
+    int slot;
 };
+
+// Threads of the work-list Newton kernel (4 cells of one warp each); the Gaunt assembly
+// streams are laid out for this many threads.
+constexpr int NEWTON_THREADS = 128;
 
 // Grid with two ghost layers per face; cell (i,j,k) with k fastest (src/global.h:15).
 struct GridDims {

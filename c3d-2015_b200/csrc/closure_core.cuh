@@ -255,6 +255,10 @@ __device__ int warp_cholesky_tiled(S &sl, int n, int lane)
         }
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
+            // padding columns (identity rows, zero couplings) would leave their entries
+            // unchanged: skip them (warp-uniform)
+            if (8 * kb + j >= n)
+                break;
             const int src = 4 * j + (j >> 1);
             double ajj = __shfl_sync(FULL_MASK, (j & 1) ? p1[kb] : p0[kb], src);
             // warp-uniform; padding pivots are 1. The loops run to the end (and then hold
@@ -313,7 +317,6 @@ __device__ int warp_cholesky_tiled(S &sl, int n, int lane)
             }
         __syncwarp();
     }
-    (void)n;
     return info;
 }
 
@@ -331,18 +334,19 @@ __device__ __forceinline__ int warp_cholesky(S &sl, int n, int lane)
 // exactDiv selects division by L_kk (as the reference's own dpotrs) instead of the
 // precomputed reciprocal.
 template <class S>
-__device__ __noinline__ void warp_apply_inverse_tiled(const S &sl, int lane, double &x0, double &x1);
+__device__ __noinline__ void warp_apply_inverse_tiled(const S &sl, int lane, double &x0,
+                                                      double &x1, double r0, double r1);
 
 template <class S>
 __device__ void warp_apply_inverse(const S &sl, int n, int lane, double &x0, double &x1,
-                                   bool exactDiv)
+                                   bool exactDiv, double r0 = 0.0, double r1 = 0.0)
 {
     if constexpr (S::tiled) {
         // the reciprocals serve both the estimate and the direction here: the blocked
         // factor already rounds differently from the reference's unblocked one
         (void)n;
         (void)exactDiv;
-        warp_apply_inverse_tiled(sl, lane, x0, x1);
+        warp_apply_inverse_tiled(sl, lane, x0, x1, r0, r1);
         return;
     }
     const double *P = sl.L;
@@ -379,15 +383,18 @@ __device__ void warp_apply_inverse(const S &sl, int n, int lane, double &x0, dou
 }
 
 // x <- (L L^T)^{-1} x on the tiled factor: tile-blocked substitution. Inside the diagonal
-// tile the steps are those of the column-oriented form with the precomputed reciprocals;
+// tile the steps are those of the column-oriented form with the reciprocal pivots r0, r1
+// of this lane's rows (lane, lane + 32), held in registers: the row's owner scales it and
+// broadcasts the result;
 // the tiles off the diagonal act as 8-column mat-vec updates of the rows below (forward) or
-// above (backward). Padding rows (L = I there, rinv = 1) keep finite values and never feed
+// above (backward). Padding rows (L = I there, reciprocal 1) keep finite values and never feed
 // the real rows.
-// Kept out of line: inlined into its callers (direction and condition estimate), builds with
-// nvcc 12.9 for sm_100a gave iteration counts that differ from the oracle's on M_6 cells
-// (the M_6 closure parity test), while this form matches it.
+// Kept out of line: inlined into after_hessian, builds with nvcc 12.9 for sm_100a gave
+// iteration counts that differ from the oracle's on M_6 cells (the M_6 closure parity
+// test), while this form matches it.
 template <class S>
-__device__ __noinline__ void warp_apply_inverse_tiled(const S &sl, int lane, double &x0, double &x1)
+__device__ __noinline__ void warp_apply_inverse_tiled(const S &sl, int lane, double &x0,
+                                                      double &x1, double r0, double r1)
 {
     constexpr int T = S::nt;
     constexpr int NMP = S::NMP;
@@ -398,7 +405,7 @@ __device__ __noinline__ void warp_apply_inverse_tiled(const S &sl, int lane, dou
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
             const int row = 8 * kb + i;
-            double xi = __shfl_sync(FULL_MASK, row < 32 ? x0 : x1, row & 31) * sl.rinv[row];
+            const double xi = __shfl_sync(FULL_MASK, row < 32 ? x0 * r0 : x1 * r1, row & 31);
             if (lane == (row & 31)) {
                 if (row < 32)
                     x0 = xi;
@@ -435,7 +442,7 @@ __device__ __noinline__ void warp_apply_inverse_tiled(const S &sl, int lane, dou
 #pragma unroll
         for (int i = 7; i >= 0; --i) {
             const int row = 8 * kb + i;
-            double xi = __shfl_sync(FULL_MASK, row < 32 ? x0 : x1, row & 31) * sl.rinv[row];
+            const double xi = __shfl_sync(FULL_MASK, row < 32 ? x0 * r0 : x1 * r1, row & 31);
             if (lane == (row & 31)) {
                 if (row < 32)
                     x0 = xi;
@@ -478,12 +485,13 @@ __device__ __forceinline__ double vsum_abs(double x0, double x1, int lane, int n
 // 381-396, Alg. 4.1 -- the algorithm of LAPACK's dlacn2 as driven by dpocon).
 // Returns 1/rcond with rcond = (1/est)/anorm.
 template <class S>
-__device__ double warp_condest(const S &sl, int n, int lane, double anorm)
+__device__ double warp_condest(const S &sl, int n, int lane, double anorm, double r0 = 0.0,
+                               double r1 = 0.0)
 {
     if (anorm == 0.0)
         return 1.0 / 0.0;
     double x0 = 1.0 / (double)n, x1 = 1.0 / (double)n;
-    warp_apply_inverse(sl, n, lane, x0, x1, false);
+    warp_apply_inverse(sl, n, lane, x0, x1, false, r0, r1);
     double est;
     if (n == 1) {
         est = fabs(__shfl_sync(FULL_MASK, x0, 0));
@@ -492,13 +500,13 @@ __device__ double warp_condest(const S &sl, int n, int lane, double anorm)
         int s0 = x0 >= 0.0 ? 1 : -1, s1 = x1 >= 0.0 ? 1 : -1;
         x0 = (double)s0;
         x1 = (double)s1;
-        warp_apply_inverse(sl, n, lane, x0, x1, false);
+        warp_apply_inverse(sl, n, lane, x0, x1, false, r0, r1);
         int j = warp_iamax(x0, x1, lane, n);
         int iter = 2;
         for (;;) {
             x0 = (lane == j) ? 1.0 : 0.0;
             x1 = (lane + 32 == j) ? 1.0 : 0.0;
-            warp_apply_inverse(sl, n, lane, x0, x1, false);
+            warp_apply_inverse(sl, n, lane, x0, x1, false, r0, r1);
             double estold = est;
             est = vsum_abs(x0, x1, lane, n);
             bool diff = (lane < n && (x0 >= 0.0 ? 1 : -1) != s0) ||
@@ -510,7 +518,7 @@ __device__ double warp_condest(const S &sl, int n, int lane, double anorm)
             s1 = x1 >= 0.0 ? 1 : -1;
             x0 = (double)s0;
             x1 = (double)s1;
-            warp_apply_inverse(sl, n, lane, x0, x1, false);
+            warp_apply_inverse(sl, n, lane, x0, x1, false, r0, r1);
             int jlast = j;
             j = warp_iamax(x0, x1, lane, n);
             double xjl = __shfl_sync(FULL_MASK, jlast < 32 ? x0 : x1, jlast & 31);
@@ -523,7 +531,7 @@ __device__ double warp_condest(const S &sl, int n, int lane, double anorm)
         }
         x0 = ((lane & 1) ? -1.0 : 1.0) * (1.0 + (double)lane / (double)(n - 1));
         x1 = (((lane + 32) & 1) ? -1.0 : 1.0) * (1.0 + (double)(lane + 32) / (double)(n - 1));
-        warp_apply_inverse(sl, n, lane, x0, x1, false);
+        warp_apply_inverse(sl, n, lane, x0, x1, false, r0, r1);
         double temp = 2.0 * (vsum_abs(x0, x1, lane, n) / (double)(3 * n));
         if (temp > est)
             est = temp;
@@ -812,12 +820,20 @@ __device__ void after_hessian(S &sl, const ClosureParams &P, const Outputs &O, i
     int info = warp_cholesky(sl, nm, lane);
     C3D_NCLK(O.stats, 2, lane);
     double cond = 0.0;
+    double r0 = 1.0, r1 = 1.0; // tiled: reciprocal pivots of rows lane, lane + 32
     if (info == 0) {
-        for (int i = lane; i < (S::tiled ? S::NMP : nm); i += 32)
-            sl.rinv[i] = 1.0 / sl.L[S::lx(i, i)];
+        if constexpr (S::tiled) {
+            if (lane < S::NMP)
+                r0 = 1.0 / sl.L[S::lx(lane, lane)];
+            if (lane + 32 < S::NMP)
+                r1 = 1.0 / sl.L[S::lx(lane + 32, lane + 32)];
+        } else {
+            for (int i = lane; i < nm; i += 32)
+                sl.rinv[i] = 1.0 / sl.L[S::lx(i, i)];
+        }
         __syncwarp();
         if (!condSure)
-            cond = warp_condest(sl, nm, lane, norm1);
+            cond = warp_condest(sl, nm, lane, norm1, r0, r1);
     }
     __syncwarp();
     C3D_NCLK(O.stats, 3, lane);
@@ -858,7 +874,7 @@ __device__ void after_hessian(S &sl, const ClosureParams &P, const Outputs &O, i
     // d = -H^{-1} g
     double x0 = lane < nm ? sl.g[lane] : 0.0;
     double x1 = lane + 32 < nm ? sl.g[lane + 32] : 0.0;
-    warp_apply_inverse(sl, nm, lane, x0, x1, true);
+    warp_apply_inverse(sl, nm, lane, x0, x1, true, r0, r1);
     if (lane < nm)
         sl.d[lane] = -x0;
     if (lane + 32 < nm)

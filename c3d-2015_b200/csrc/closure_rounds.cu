@@ -369,7 +369,7 @@ template <int NT, int NT2, bool GAUNT>
 __global__ void __launch_bounds__(RWN * 32)
     rounds_newton_kernel(ClosureParams P, double m0, const int *__restrict__ list, int n,
                          CellState<NT> *state, const double *__restrict__ buf,
-                         const int2 *__restrict__ plan, const GauntTerm *__restrict__ terms,
+                         const GauntTerm *__restrict__ stream, int streamLen,
                          Outputs O, int *listOut, unsigned int *countOut)
 {
     constexpr int NM2P = 8 * NT2;
@@ -400,22 +400,31 @@ __global__ void __launch_bounds__(RWN * 32)
 #pragma unroll
             for (int w = 0; w < RWN; ++w)
                 hw[w] = slots[w].s.need == NEED_H;
-            for (int e = tid; e < LS; e += RWN * 32) {
-                const int2 pe = plan[e];
-                double h[RWN];
+            static_assert(RWN * 32 == NEWTON_THREADS, "stream layout");
+            double h[RWN];
 #pragma unroll
-                for (int w = 0; w < RWN; ++w)
-                    h[w] = pe.y < 0 ? 1.0 : 0.0;
-                for (int tt = pe.x; tt < pe.x + pe.y; ++tt) {
-                    const GauntTerm gt = terms[tt];
+            for (int w = 0; w < RWN; ++w)
+                h[w] = 0.0;
+#pragma unroll 4
+            for (int k = 0; k < streamLen; ++k) {
+                const GauntTerm gt = stream[k * NEWTON_THREADS + tid];
+                if (gt.col >= 0) {
 #pragma unroll
                     for (int w = 0; w < RWN; ++w)
                         h[w] = __dadd_rn(h[w], __dmul_rn(slots[w].scratch()[gt.col], gt.v));
-                }
+                } else {
 #pragma unroll
-                for (int w = 0; w < RWN; ++w)
-                    if (hw[w])
-                        slots[w].L[e] = h[w];
+                    for (int w = 0; w < RWN; ++w)
+                        h[w] = 1.0;
+                }
+                if (gt.slot >= 0) {
+#pragma unroll
+                    for (int w = 0; w < RWN; ++w) {
+                        if (hw[w])
+                            slots[w].L[gt.slot] = h[w];
+                        h[w] = 0.0;
+                    }
+                }
             }
         }
         __syncthreads();
@@ -447,8 +456,8 @@ struct RoundsLaunch {
     const ClosureParams *P;
     const double *chunks;      // direct: (NMP+1) x QCP chunks; Gaunt: (NM2P+1) x QCP chunks
     int nm2;                   // Gaunt: extended moments (chunk rows: nm2 + the weight row)
-    const int2 *plan;          // Gaunt: per tile slot {first term, terms} (-1: identity)
-    const GauntTerm *terms;    // Gaunt: the beta terms in tile-slot order
+    const GauntTerm *gstream;  // Gaunt: assembly streams, entry s of thread t at s*128 + t
+    int streamLen;             // entries per thread
     double m0;                 // M[0][0]
     long long ncells;
     const int *cellMap;        // closure cell i -> grid cell cellMap[i] (null: identity)
@@ -558,7 +567,7 @@ template <int NT, int NT2, bool GAUNT> static cudaError_t rounds_t(const RoundsL
                     P, R.chunks, listA + off, nb, state, R.buf, R.errorFlag);
             rounds_newton_kernel<NT, NT2, GAUNT><<<(unsigned)((nb + RWN - 1) / RWN), RWN * 32,
                                                    newtonSmem, st>>>(
-                P, m0, listA + off, nb, state, R.buf, R.plan, R.terms, O, listB, cB);
+                P, m0, listA + off, nb, state, R.buf, R.gstream, R.streamLen, O, listB, cB);
             *R.launches += 2;
             e = cudaGetLastError();
             if (e != cudaSuccess)
