@@ -44,7 +44,8 @@ class Params(ctypes.Structure):
                 ("mnBatched", ctypes.c_int), ("mnMaxIter", ctypes.c_int),
                 ("mnTol", ctypes.c_double), ("mnTolGamma", ctypes.c_double),
                 ("mnCondHMax", ctypes.c_double), ("nreg", ctypes.c_int),
-                ("reg", ctypes.c_double * 16), ("psiBytes", ctypes.c_size_t)]
+                ("reg", ctypes.c_double * 16), ("psiBytes", ctypes.c_size_t),
+                ("mnReproject", ctypes.c_int)]
 
 
 class ClosureStats(ctypes.Structure):
@@ -147,7 +148,7 @@ class Context:
     def __init__(self, *, nx, ny, nz, nm, nq, dx, dy, dz, M, w, xi, eta, mu, theta=2.0, solver=1,
                  pn_kinetic=0, batched=True, max_iter=100, tol=1e-8, tol_gamma=1.1,
                  cond_h_max=1e10, ladder=(0.0, 1e-3, 1e-2, 1e-1, 5e-1), pn_ops=None, stream=None,
-                 psi_bytes=0):
+                 psi_bytes=0, reproject=False):
         L = lib()
         p = Params()
         p.nx, p.ny, p.nz, p.nm, p.nq = nx, ny, nz, nm, nq
@@ -159,6 +160,7 @@ class Context:
         for i, r in enumerate(ladder):
             p.reg[i] = r
         p.psiBytes = psi_bytes
+        p.mnReproject = int(bool(reproject))
         self.nx, self.ny, self.nz, self.nm, self.nq = nx, ny, nz, nm, nq
         self.nall = (nx + 4) * (ny + 4) * (nz + 4)
         self._keep = [np.ascontiguousarray(a, dtype=np.float64) for a in (M, w, xi, eta, mu)]

@@ -72,6 +72,8 @@ cudaError_t launch_kinetic_flux(const GridDims &g, const double *alpha, const do
                                 double dz, double theta, int isPn, double *psi, double *flux,
                                 int *errorFlag, cudaStream_t st);
 size_t flux_frag_doubles(int nm, int nq, int which);
+cudaError_t launch_reproject(const GridDims &g, double *u, double *alpha, const double *mfA,
+                             const double *mfP, int nq, int *errorFlag, cudaStream_t st);
 cudaError_t launch_ghost_fill_int(const GridDims &g, int *a, int numSMs, cudaStream_t st);
 cudaError_t launch_ghost_mirror_check(const GridDims &g, const double *a, int *flag, int numSMs,
                                       cudaStream_t st);
@@ -145,6 +147,7 @@ struct c3d_ctx {
     double *sigT = nullptr, *sigS = nullptr;
     double *M = nullptr, *w = nullptr, *xi = nullptr, *eta = nullptr, *mu = nullptr;
     double *mfA = nullptr, *mfP = nullptr; // basis in the flux kernels' fragment order
+    bool reproject = false;                // MN_REPROJECT
     double *chunks = nullptr, *pnops = nullptr, *psi = nullptr;
     int *iters = nullptr, *iterGamma = nullptr, *regIdx = nullptr, *status = nullptr;
     unsigned long long *counter = nullptr, *failCount = nullptr, *stats = nullptr;
@@ -288,6 +291,7 @@ c3d_status c3d_create(const c3d_params *p, const double *M, const double *w, con
         cp.reg[i] = p->reg[i];
     cp.passBudget = 1LL << 40;
     c->psiBytes = p->psiBytes ? p->psiBytes : (size_t)16 << 30;
+    c->reproject = p->mnReproject != 0;
 
     const long long nall = c->g.nall();
     const int nm = p->nm, nq = p->nq;
@@ -536,12 +540,25 @@ static c3d_status run_closure(c3d_ctx *c, long long n, double *u, double *alpha,
     return C3D_OK;
 }
 
+static c3d_status closure_grid(c3d_ctx *c);
+
 c3d_status c3d_closure(c3d_ctx *c)
 {
     if (!c)
         return fail(C3D_ERR_INVALID, "c3d_closure: null context");
     if (c->solver != 1)
         return fail(C3D_ERR_INVALID, "c3d_closure: the closure belongs to the M_N solver");
+    c3d_status s = closure_grid(c);
+    if (s != C3D_OK || !c->reproject)
+        return s;
+    C3D_CUDA(launch_reproject(c->g, c->u, c->alpha, c->mfA, c->mfP, c->nq, c->errorFlag,
+                              c->stream));
+    c->launches += 1;
+    return C3D_OK;
+}
+
+static c3d_status closure_grid(c3d_ctx *c)
+{
     if (c->engine == 0 && c->mirror) {
         // Face ghosts hold copies of their periodic images (src/comm.cpp:281-323); when their
         // multipliers (the warm starts) are bitwise those of the images too, the per-cell

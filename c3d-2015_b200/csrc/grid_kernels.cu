@@ -15,6 +15,10 @@
 // pipe, so its sums are reordered against the reference's (agreement to ~1e-15 relative).
 #include "c3d_common.cuh"
 
+#ifndef M_PI
+#define M_PI 3.14159265358979323846
+#endif
+
 namespace c3d {
 
 
@@ -139,6 +143,23 @@ __device__ __forceinline__ void fbar_load(void *dst, const void *src, uint32_t b
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
                      smem_addr(dst)),
                  "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+// Two bulk copies completing one phase of a barrier initialised for one arrival: a single
+// arrive.expect_tx with the combined byte count, then both copies.
+__device__ __forceinline__ void fbar_load2(void *dst0, const void *src0, uint32_t bytes0, void *dst1,
+                                           const void *src1, uint32_t bytes1, uint64_t *bar)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(bar)),
+                 "r"(bytes0 + bytes1)
+                 : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                     smem_addr(dst0)),
+                 "l"(src0), "r"(bytes0), "r"(smem_addr(bar))
+                 : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                     smem_addr(dst1)),
+                 "l"(src1), "r"(bytes1), "r"(smem_addr(bar))
                  : "memory");
 }
 // false if the phase did not complete within the iteration limit
@@ -450,6 +471,137 @@ cudaError_t launch_rk(const GridDims &g, double *u, double *uOld, int mode, int 
 {
     rk_kernel<<<grid_for(g.ninterior() * g.nm, 256, numSMs), 256, 0, st>>>(g, u, uOld, mode);
     return cudaGetLastError();
+}
+
+// Robustness re-projection after the closure (the note in the reference's readme.txt:
+// "one should calculate a new u^n so that u^n = <m exp(m^T alpha^n)> exactly ... and scale
+// u^n and alpha^n so that u_0^n does not change"): per cell u' = sum_q w_q m_q e^{alpha.m_q};
+// with s = u_0 / u'_0, u <- (u_0, s u'_1, ..., s u'_{nm-1}) and alpha_0 <- alpha_0 + log(s)/m_0
+// (m_0 = 1/(2 sqrt(pi)); e^{alpha.m} s = e^{alpha'.m}). A CTA owns 64 cells: per direction
+// tile the exponents (DMMA, multipliers as A fragments), c = w e^{z} into shared memory, then
+// the moments (DMMA with the projection fragments) -- the ansatz and projection layouts of
+// the kinetic flux.
+template <int NT>
+__global__ void __launch_bounds__(256)
+    reproject_kernel(GridDims g, double *__restrict__ u, double *__restrict__ alpha,
+                     const double *__restrict__ mfA, const double *__restrict__ mfP, int nq,
+                     int *errorFlag)
+{
+    constexpr int KS = 2 * NT;
+    constexpr int TA = 4 * KS * 32, TP = 8 * NT * 32 + 128;
+    constexpr int CS = 68;
+    extern __shared__ __align__(128) double rpSmem[]; // sA[2][TA], sP[2][TP], sC[32][CS]
+    double(*sA)[TA] = reinterpret_cast<double(*)[TA]>(rpSmem);
+    double(*sP)[TP] = reinterpret_cast<double(*)[TP]>(rpSmem + FLUX_STAGES * TA);
+    double *sC = rpSmem + FLUX_STAGES * (TA + TP);
+    __shared__ uint64_t bar[FLUX_STAGES];
+    __shared__ int sAbort;
+    const int nm = g.nm;
+    const long long nall = g.nall();
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const long long c = (long long)blockIdx.x * 64 + 8 * warp + (lane >> 2);
+    const int nt = (nq + 31) >> 5;
+    if (tid == 0) {
+        sAbort = 0;
+        for (int st = 0; st < FLUX_STAGES; ++st)
+            fbar_init(&bar[st]);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        for (int st = 0; st < FLUX_STAGES && st < nt; ++st)
+            fbar_load2(sA[st], mfA + (size_t)st * TA, TA * 8, sP[st], mfP + (size_t)st * TP,
+                       TP * 8, &bar[st]);
+    }
+    double a[KS];
+#pragma unroll
+    for (int kk = 0; kk < KS; ++kk) {
+        int k = 4 * kk + (lane & 3);
+        a[kk] = (c < nall && k < nm) ? alpha[c * nm + k] : 0.0;
+    }
+    double acc[NT][2];
+#pragma unroll
+    for (int j = 0; j < NT; ++j)
+        acc[j][0] = acc[j][1] = 0.0;
+    __syncthreads();
+    for (int t = 0; t < nt; ++t) {
+        const int st = t % FLUX_STAGES;
+        if (!fbar_wait(&bar[st], (t / FLUX_STAGES) & 1))
+            sAbort = 1;
+        if (__syncthreads_or(sAbort)) {
+            if (tid == 0)
+                atomicExch(errorFlag, 1);
+            return;
+        }
+        const double *w = sP[st] + 8 * NT * 32 + 96;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            double z0 = 0.0, z1 = 0.0;
+#pragma unroll
+            for (int kk = 0; kk < KS; ++kk)
+                dmma_g(z0, z1, a[kk], sA[st][(j * KS + kk) * 32 + lane]);
+            const int qq = 8 * j + 2 * (lane & 3);
+            sC[qq * CS + 8 * warp + (lane >> 2)] = w[qq] * exp(z0);
+            sC[(qq + 1) * CS + 8 * warp + (lane >> 2)] = w[qq + 1] * exp(z1);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < 8; ++kk) {
+            const double av = sC[(4 * kk + (lane & 3)) * CS + 8 * warp + (lane >> 2)];
+#pragma unroll
+            for (int j = 0; j < NT; ++j)
+                dmma_g(acc[j][0], acc[j][1], av, sP[st][(kk * NT + j) * 32 + lane]);
+        }
+        __syncthreads();
+        if (tid == 0 && t + FLUX_STAGES < nt)
+            fbar_load2(sA[st], mfA + (size_t)(t + FLUX_STAGES) * TA, TA * 8, sP[st],
+                       mfP + (size_t)(t + FLUX_STAGES) * TP, TP * 8, &bar[st]);
+    }
+    // lane 4r holds moment 0 of cell r of the warp's tile
+    const double un0 = __shfl_sync(0xffffffffu, acc[0][0], lane & ~3);
+    if (c >= nall)
+        return;
+    const double u0 = u[c * nm];
+    const double sc = u0 / un0;
+#pragma unroll
+    for (int j = 0; j < NT; ++j)
+#pragma unroll
+        for (int e2 = 0; e2 < 2; ++e2) {
+            int m = 8 * j + 2 * (lane & 3) + e2;
+            if (m > 0 && m < nm)
+                u[c * nm + m] = sc * acc[j][e2];
+        }
+    if ((lane & 3) == 0)
+        alpha[c * nm] += 2.0 * sqrt(M_PI) * log(sc);
+}
+
+template <int NT>
+static cudaError_t reproject_t(const GridDims &g, double *u, double *alpha, const double *mfA,
+                               const double *mfP, int nq, int *errorFlag, cudaStream_t st)
+{
+    constexpr int KS = 2 * NT;
+    const size_t smem =
+        (size_t)(FLUX_STAGES * (4 * KS * 32 + 8 * NT * 32 + 128) + 32 * 68) * sizeof(double);
+    cudaError_t e = cudaFuncSetAttribute(reproject_kernel<NT>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess)
+        return e;
+    reproject_kernel<NT><<<(unsigned)((g.nall() + 63) / 64), 256, smem, st>>>(g, u, alpha, mfA,
+                                                                             mfP, nq, errorFlag);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_reproject(const GridDims &g, double *u, double *alpha, const double *mfA,
+                             const double *mfP, int nq, int *errorFlag, cudaStream_t st)
+{
+    switch ((g.nm + 7) / 8) {
+    case 1: return reproject_t<1>(g, u, alpha, mfA, mfP, nq, errorFlag, st);
+    case 2: return reproject_t<2>(g, u, alpha, mfA, mfP, nq, errorFlag, st);
+    case 3: return reproject_t<3>(g, u, alpha, mfA, mfP, nq, errorFlag, st);
+    case 4: return reproject_t<4>(g, u, alpha, mfA, mfP, nq, errorFlag, st);
+    case 5: return reproject_t<5>(g, u, alpha, mfA, mfP, nq, errorFlag, st);
+    case 6: return reproject_t<6>(g, u, alpha, mfA, mfP, nq, errorFlag, st);
+    case 7: return reproject_t<7>(g, u, alpha, mfA, mfP, nq, errorFlag, st);
+    case 8: return reproject_t<8>(g, u, alpha, mfA, mfP, nq, errorFlag, st);
+    default: return cudaErrorInvalidValue;
+    }
 }
 
 // Fragment-order copies of the basis for the flux kernels (layouts above); nt = ceil(nq/32)

@@ -81,6 +81,7 @@ std::string parse_config(const InputDeck &d, Config &c)
         if (c.ladder.empty() || c.ladder.size() > 16)
             return "REG_LADDER must list 1 to 16 values";
     }
+    d.get("MN_REPROJECT", c.mnReproject);
     d.get("SIGMA_CHECKER_BLOCK", c.checkerBlock);
     d.get("SIGMA_S_HI", c.sigmaSHi);
     d.get("SIGMA_A_HI", c.sigmaAHi);
@@ -198,6 +199,7 @@ void Solver::prepare(const Config &cfg)
     P.mnMaxIter = c.mnMaxIter;
     P.mnTol = c.mnTol;
     P.mnTolGamma = c.mnTolGamma;
+    P.mnReproject = c.mnReproject ? 1 : 0;
     P.mnCondHMax = c.mnCondHMax;
     P.nreg = (int)c.ladder.size();
     for (size_t i = 0; i < c.ladder.size(); ++i)

@@ -13,6 +13,8 @@
 //   SIGMA_S_HI, SIGMA_A_HI     the odd blocks get sigma_s = SIGMA_S_HI, sigma_a = SIGMA_A_HI,
 //                              the even blocks sigma_s = CROSS_SECTION, sigma_a = 0;
 //                              sigma_t = sigma_s + sigma_a.
+//   MN_REPROJECT true        after each closure set u = <m e^{alpha.m}> keeping u_0 (the
+//                              robustness note of the reference's readme.txt)
 #pragma once
 #include "../../include/c3d_b200.h"
 #include "deck.h"
@@ -37,6 +39,7 @@ struct Config {
     double mnTol = 0, mnTolGamma = 0, mnCondHMax = 0;
     int mnMaxIter = 0;
     bool mnBatched = true, mnUseGaunt = false, mnUseGauntSparse = false;
+    bool mnReproject = false; // optional MN_REPROJECT (readme.txt robustness note)
     // optional keys
     int nsteps = -1;
     std::vector<double> ladder{0.0, 1e-3, 1e-2, 1e-1, 5e-1};

@@ -89,6 +89,9 @@ typedef struct {
     int nreg;                  /* regularisation ladder (reference: 5 values) */
     double reg[16];
     size_t psiBytes;           /* budget for the materialised ansatz (0 = default) */
+    int mnReproject;           /* 1: after each grid closure set u = <m e^{alpha.m}> with u_0
+                                  kept (the robustness note of the reference's readme.txt);
+                                  deck key MN_REPROJECT; no counterpart in the reference code */
 } c3d_params;
 
 /* Closure counters accumulated on the device since the last reset (the

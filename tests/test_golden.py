@@ -122,3 +122,31 @@ def test_gpu_pn_golden(tmp_path):
     rel = np.linalg.norm(x - ref) / np.linalg.norm(ref)
     assert rel < 1e-13, rel
     s.close()
+
+
+@pytest.mark.gpu
+def test_gpu_pn_kinetic_flux_matches_oracle(oracle, tmp_path):
+    """P_N with the kinetic flux (PN_USE_KINETIC_FLUX 1, src/update.cpp:242-245): the ansatz
+    is psi = alpha.m_q with u standing in for alpha; three steps against the oracle."""
+    from oracle_lib import deck_text, make_opts
+    s = c3d.Solver(_deck(tmp_path, deck_text(SOLVER="pn", NX=8, NY=6, NZ=7, MOMENT_ORDER=3,
+                                              QUAD_ORDER=8, INIT_COND="smooth",
+                                              PN_USE_KINETIC_FLUX=1)))
+    s.pull()
+    A = s.arrays()
+    u = A["u"].copy()
+    alpha = np.zeros_like(u)
+    T = oracle.tables(3, 8, pn=True)
+    g = oracle.grid(s.nx, s.ny, s.nz, s.nm, s.nq, s.dx, s.dy, s.dz, s.theta)
+    opts = make_opts(s.nm, s.nq)
+    for _ in range(3):
+        s.update(s.max_dt)
+        oracle.step(g, opts, T, u, alpha, A["sigT"], A["sigS"], s.max_dt, solver=0,
+                    pn_kinetic=1, records=False)
+    s.sync()
+    s.pull()
+    x = s.arrays()["u"].reshape(s.nx + 4, s.ny + 4, s.nz + 4, s.nm)[2:-2, 2:-2, 2:-2]
+    y = u.reshape(s.nx + 4, s.ny + 4, s.nz + 4, s.nm)[2:-2, 2:-2, 2:-2]
+    rel = np.linalg.norm(x - y) / np.linalg.norm(y)
+    assert rel < 1e-13, rel
+    s.close()

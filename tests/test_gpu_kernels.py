@@ -356,3 +356,36 @@ def test_ghost_mirroring_is_exact(oracle):
         assert np.array_equal(x, y)
     assert out[0][5] == 4 * nall             # 2 steps x 2 stages, every cell
     assert out[1][5] == 4 * (nall - faces)   # face ghosts copied
+
+
+def test_reprojection_mode(oracle):
+    """MN_REPROJECT (the robustness note of the reference's readme.txt): after the closure
+    u = <m e^{alpha.m}> with u_0 kept and alpha_0 shifted by 2 sqrt(pi) log(u_0 / u'_0);
+    checked against the same formulas in numpy on the plain closure's multipliers."""
+    S = _setup(oracle, N=2, Q=12, steps_before=1)
+    nm, nq, T = S["nm"], S["nq"], S["T"]
+    outs = []
+    for rp in (False, True):
+        ctx = _ctx(S, reproject=rp)
+        ctx.set_state(u=S["u"], alpha=S["alpha"], sig_t=S["sig"], sig_s=S["sig"])
+        ctx.closure()
+        ctx.sync()
+        outs.append(ctx.get_state())
+        ctx.close()
+    (u0, a0), (u1, a1) = outs
+    M = T["M"].reshape(nq, nm)
+    A, U = a0.reshape(-1, nm), u0.reshape(-1, nm)
+    un = (np.exp(A @ M.T) * T["w"]) @ M
+    s = U[:, 0] / un[:, 0]
+    ue = un * s[:, None]
+    ue[:, 0] = U[:, 0]
+    ae = A.copy()
+    ae[:, 0] += 2.0 * np.sqrt(np.pi) * np.log(s)
+    u1, a1 = u1.reshape(-1, nm), a1.reshape(-1, nm)
+    assert np.array_equal(u1[:, 0], U[:, 0])
+    assert np.linalg.norm(u1 - ue) <= 1e-13 * np.linalg.norm(ue)
+    assert np.abs(a1 - ae).max() <= 1e-12 * np.abs(ae).max()
+    # u is now the ansatz's own moments (to rounding)
+    ua = (np.exp(a1 @ M.T) * T["w"]) @ M
+    assert np.linalg.norm(u1 - ua) <= 1e-12 * np.linalg.norm(ua)
+    assert np.abs(s - 1.0).max() > 1e-12  # the closure's tolerance left something to fix
