@@ -20,6 +20,14 @@ C3D_OK = 0
 STATUS_NAMES = {0: "OK", 1: "INVALID", 2: "CUDA", 3: "NO_DEVICE", 4: "CLOSURE", 5: "TIMEOUT",
                 6: "OOM"}
 
+# the symbols include/c3d_solver.h declares
+SOLVER_SYMBOLS = [
+    "c3d_solver_create", "c3d_solver_prepare", "c3d_solver_destroy", "c3d_solver_update",
+    "c3d_solver_run", "c3d_solver_pull", "c3d_solver_push", "c3d_solver_context",
+    "c3d_solver_info", "c3d_solver_host_array", "c3d_solver_output_data",
+    "c3d_solver_checkpoint", "c3d_solver_restore",
+]
+
 # the symbols include/c3d_b200.h declares
 HEADER_SYMBOLS = [
     "c3d_last_error", "solveFluxKinetic_cuda", "solveH_cuda", "solveHInit_cuda", "c3d_create",
@@ -117,6 +125,9 @@ def lib():
         L.c3d_solver_info.argtypes = [vp, _ip, _dp]
         L.c3d_solver_host_array.argtypes = [vp, ctypes.c_int]
         L.c3d_solver_host_array.restype = _dp
+        L.c3d_solver_output_data.argtypes = [vp, ctypes.c_double, ctypes.c_char_p]
+        L.c3d_solver_checkpoint.argtypes = [vp, ctypes.c_double, ctypes.c_char_p]
+        L.c3d_solver_restore.argtypes = [vp, ctypes.c_char_p, _dp]
         _lib = L
     return _lib
 
@@ -325,6 +336,18 @@ class Solver:
 
     def push(self):
         check(lib().c3d_solver_push(self.h), "push")
+
+    def output_data(self, time, directory):
+        """outputData(time) of the reference into `directory` (.master + .pn)."""
+        check(lib().c3d_solver_output_data(self.h, time, str(directory).encode()), "output_data")
+
+    def checkpoint(self, time, path):
+        check(lib().c3d_solver_checkpoint(self.h, time, str(path).encode()), "checkpoint")
+
+    def restore(self, path):
+        t = ctypes.c_double(0.0)
+        check(lib().c3d_solver_restore(self.h, str(path).encode(), ctypes.byref(t)), "restore")
+        return t.value
 
     def sync(self):
         check(lib().c3d_sync(self.ctx_handle), "sync")

@@ -75,6 +75,9 @@ size_t flux_frag_doubles(int nm, int nq, int which);
 cudaError_t launch_reproject(const GridDims &g, double *u, double *alpha, const double *mfA,
                              const double *mfP, int nq, int *errorFlag, cudaStream_t st);
 cudaError_t launch_ghost_fill_int(const GridDims &g, int *a, int numSMs, cudaStream_t st);
+cudaError_t launch_ghost_stats(const GridDims &g, const int *iters, const int *iterGamma,
+                               const int *regIdx, const int *status, unsigned long long *stats,
+                               int numSMs, cudaStream_t st);
 cudaError_t launch_ghost_mirror_check(const GridDims &g, const double *a, int *flag, int numSMs,
                                       cudaStream_t st);
 void flux_frags(int nm, int nq, const double *M, const double *w, const double *xi,
@@ -601,7 +604,9 @@ static c3d_status closure_grid(c3d_ctx *c)
             C3D_CUDA(launch_ghost_fill(c->g, c->u, c->numSMs, c->stream));
             for (int *a : {c->iters, c->iterGamma, c->regIdx, c->status})
                 C3D_CUDA(launch_ghost_fill_int(c->g, a, c->numSMs, c->stream));
-            c->launches += 6;
+            C3D_CUDA(launch_ghost_stats(c->g, c->iters, c->iterGamma, c->regIdx, c->status,
+                                        c->stats, c->numSMs, c->stream));
+            c->launches += 7;
             c->mirroredClosures++;
             return C3D_OK;
         }

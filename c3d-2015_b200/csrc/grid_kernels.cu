@@ -40,6 +40,33 @@ __global__ void ghost_fill_kernel(GridDims g, T *__restrict__ u, int ncomp)
     }
 }
 
+// Closure statistics of the face ghosts whose records a mirrored closure copied from their
+// images: the same counters a solve adds (finalize, closure_core.cuh), so that the totals
+// equal those of solving every cell.
+__global__ void ghost_stats_kernel(GridDims g, const int *__restrict__ iters,
+                                   const int *__restrict__ iterGamma,
+                                   const int *__restrict__ regIdx, const int *__restrict__ status,
+                                   unsigned long long *stats)
+{
+    const long long total = ghost_faces(g);
+    for (long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x; f < total;
+         f += (long long)gridDim.x * blockDim.x) {
+        long long dst, src;
+        ghost_pair(g, f, dst, src);
+        const unsigned long long it = (unsigned long long)iters[dst];
+        const unsigned long long ig = (unsigned long long)iterGamma[dst];
+        atomicAdd(&stats[STAT_CELLS], 1ull);
+        atomicAdd(&stats[STAT_ITERS], it);
+        atomicAdd(&stats[STAT_ITER_GAMMA], ig);
+        atomicMax(&stats[STAT_MAX_ITER], it);
+        atomicMax(&stats[STAT_MAX_ITER_GAMMA], ig);
+        if (status[dst] != CELL_OK)
+            atomicAdd(&stats[STAT_FAILED], 1ull);
+        atomicAdd(&stats[STAT_REG_HIST + (regIdx[dst] & 15)], 1ull);
+        atomicAdd(&stats[STAT_ITER_HIST + (it < 63 ? it : 63)], 1ull);
+    }
+}
+
 // *flag = 1 if any face ghost of a differs (bitwise) from its periodic image.
 __global__ void ghost_mirror_check_kernel(GridDims g, const double *__restrict__ a, int ncomp,
                                           int *flag)
@@ -447,6 +474,15 @@ cudaError_t launch_ghost_fill(const GridDims &g, double *u, int numSMs, cudaStre
 cudaError_t launch_ghost_fill_int(const GridDims &g, int *a, int numSMs, cudaStream_t st)
 {
     ghost_fill_kernel<int><<<grid_for(ghost_faces(g), 256, numSMs), 256, 0, st>>>(g, a, 1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ghost_stats(const GridDims &g, const int *iters, const int *iterGamma,
+                               const int *regIdx, const int *status, unsigned long long *stats,
+                               int numSMs, cudaStream_t st)
+{
+    ghost_stats_kernel<<<grid_for(ghost_faces(g), 256, numSMs), 256, 0, st>>>(
+        g, iters, iterGamma, regIdx, status, stats);
     return cudaGetLastError();
 }
 

@@ -1,0 +1,113 @@
+// Output files of the reference (src/output.cpp:19-110): the text master file and the
+// binary .pn data file of one rank, plus a checkpoint of (u, alpha) that the reference
+// does not have. Formats are the reference's, byte for byte, so its readers (plot.py)
+// work unchanged.
+#include "output.h"
+
+#include <cstdint>
+#include <cstdio>
+
+namespace c3d_host {
+
+static bool put_i64(FILE *f, long long v)
+{
+    int64_t t = (int64_t)v;
+    return fwrite(&t, sizeof(t), 1, f) == 1;
+}
+static bool put_f64(FILE *f, double v) { return fwrite(&v, sizeof(v), 1, f) == 1; }
+
+bool write_output_data(const std::string &dir, double time, const Config &c, int nm,
+                       const double *u, const OutputStats &st, std::string &err)
+{
+    char name[512];
+    // master file (rank 0; one rank here)
+    snprintf(name, sizeof(name), "%s/out_%.6f.master", dir.c_str(), time);
+    FILE *f = fopen(name, "w");
+    if (!f) {
+        err = std::string("could not open ") + name;
+        return false;
+    }
+    fprintf(f, "%d\n%d\n%d\n", c.nx, c.ny, c.nz);
+    fprintf(f, "%f\n%f\n%f\n%f\n%f\n%f\n", c.ax, c.ay, c.az, c.bx, c.by, c.bz);
+    fprintf(f, "%d\n", nm);
+    fprintf(f, "1\n1\n1\n");
+    fprintf(f, "out_%.6f_%d.pn\n", time, 0);
+    fclose(f);
+
+    // data file: nx ny nz, the interior moments (i, j, k with k fastest), closure statistics
+    snprintf(name, sizeof(name), "%s/out_%.6f_%d.pn", dir.c_str(), time, 0);
+    f = fopen(name, "wb");
+    if (!f) {
+        err = std::string("could not open ") + name;
+        return false;
+    }
+    bool ok = put_i64(f, c.nx) && put_i64(f, c.ny) && put_i64(f, c.nz);
+    const long long nyg = c.ny + 4, nzg = c.nz + 4;
+    for (int i = 2; ok && i < c.nx + 2; ++i)
+        for (int j = 2; ok && j < c.ny + 2; ++j)
+            for (int k = 2; ok && k < c.nz + 2; ++k) {
+                const long long cell = k + nzg * (j + nyg * (long long)i);
+                ok = fwrite(u + cell * nm, sizeof(double), (size_t)nm, f) == (size_t)nm;
+            }
+    ok = ok && put_i64(f, st.maxIter) && put_i64(f, st.maxIterGamma) &&
+         put_f64(f, st.iterMean) && put_f64(f, st.iterGammaMean) && put_i64(f, st.numDualSolves);
+    for (size_t r = 0; ok && r < st.regHist.size(); ++r)
+        ok = put_i64(f, st.regHist[r]);
+    fclose(f);
+    if (!ok)
+        err = std::string("write failed: ") + name;
+    return ok;
+}
+
+static const char CKPT_MAGIC[8] = {'C', '3', 'D', 'C', 'K', 'P', 'T', '1'};
+
+bool write_checkpoint(const std::string &path, double time, const Config &c, int nm,
+                      const double *u, const double *alpha, std::string &err)
+{
+    FILE *f = fopen(path.c_str(), "wb");
+    if (!f) {
+        err = "could not open " + path;
+        return false;
+    }
+    const size_t n = (size_t)(c.nx + 4) * (c.ny + 4) * (c.nz + 4) * nm;
+    bool ok = fwrite(CKPT_MAGIC, 1, 8, f) == 8 && put_i64(f, c.nx) && put_i64(f, c.ny) &&
+              put_i64(f, c.nz) && put_i64(f, nm) && put_f64(f, time) &&
+              fwrite(u, sizeof(double), n, f) == n && fwrite(alpha, sizeof(double), n, f) == n;
+    fclose(f);
+    if (!ok)
+        err = "write failed: " + path;
+    return ok;
+}
+
+bool read_checkpoint(const std::string &path, const Config &c, int nm, double *u, double *alpha,
+                     double *time, std::string &err)
+{
+    FILE *f = fopen(path.c_str(), "rb");
+    if (!f) {
+        err = "could not open " + path;
+        return false;
+    }
+    char magic[8];
+    int64_t hdr[4];
+    double t = 0.0;
+    bool ok = fread(magic, 1, 8, f) == 8 && fread(hdr, sizeof(int64_t), 4, f) == 4 &&
+              fread(&t, sizeof(double), 1, f) == 1;
+    if (ok && (std::string(magic, 8) != std::string(CKPT_MAGIC, 8) || hdr[0] != c.nx ||
+               hdr[1] != c.ny || hdr[2] != c.nz || hdr[3] != nm)) {
+        err = "checkpoint " + path + " does not match this problem";
+        fclose(f);
+        return false;
+    }
+    const size_t n = (size_t)(c.nx + 4) * (c.ny + 4) * (c.nz + 4) * nm;
+    ok = ok && fread(u, sizeof(double), n, f) == n && fread(alpha, sizeof(double), n, f) == n;
+    fclose(f);
+    if (!ok) {
+        err = "read failed: " + path;
+        return false;
+    }
+    if (time)
+        *time = t;
+    return true;
+}
+
+} // namespace c3d_host

@@ -1,4 +1,6 @@
 #include "solver.h"
+#include "output.h"
+#include "../../include/c3d_solver.h"
 
 #include "tables.h"
 
@@ -290,16 +292,74 @@ c3d_status Solver::pull()
 
 c3d_status Solver::update(double dt) { return c3d_step(ctx_, dt); }
 
+c3d_status Solver::outputData(double time, const std::string &dir)
+{
+    OutputStats st;
+    st.regHist.assign(cfg_.ladder.size(), 0);
+    if (ctx_) {
+        c3d_status s = pull();
+        if (s != C3D_OK)
+            return s;
+        if (cfg_.solver == "mn") {
+            c3d_closure_stats cs;
+            if ((s = c3d_closure_stats_get(ctx_, &cs)) != C3D_OK)
+                return s;
+            st.maxIter = cs.maxIter;
+            st.maxIterGamma = cs.maxIterGamma;
+            st.numDualSolves = cs.cells;
+            st.iterMean = cs.cells ? (double)cs.totalIters / (double)cs.cells : 0.0;
+            st.iterGammaMean = cs.cells ? (double)cs.totalIterGamma / (double)cs.cells : 0.0;
+            for (size_t r = 0; r < st.regHist.size() && r < 16; ++r)
+                st.regHist[r] = cs.regHist[r];
+        }
+    }
+    std::string err;
+    if (!write_output_data(dir, time, cfg_, nm_, u.data(), st, err)) {
+        fprintf(stderr, "[c3d_b200] outputData: %s\n", err.c_str());
+        return C3D_ERR_INVALID;
+    }
+    return C3D_OK;
+}
+
+c3d_status Solver::checkpoint(const std::string &path, double time)
+{
+    if (ctx_) {
+        c3d_status s = pull();
+        if (s != C3D_OK)
+            return s;
+    }
+    std::string err;
+    if (!write_checkpoint(path, time, cfg_, nm_, u.data(), alpha.data(), err)) {
+        fprintf(stderr, "[c3d_b200] checkpoint: %s\n", err.c_str());
+        return C3D_ERR_INVALID;
+    }
+    return C3D_OK;
+}
+
+c3d_status Solver::restore(const std::string &path, double *time)
+{
+    std::string err;
+    if (!read_checkpoint(path, cfg_, nm_, u.data(), alpha.data(), time, err)) {
+        fprintf(stderr, "[c3d_b200] restore: %s\n", err.c_str());
+        return C3D_ERR_INVALID;
+    }
+    return ctx_ ? push() : C3D_OK;
+}
+
 c3d_status Solver::run(int *stepsTaken)
 {
     int steps = 0;
     c3d_status s = C3D_OK;
+    if (cfg_.outputData && (s = outputData(0.0, "output")) != C3D_OK)
+        return s;
     if (cfg_.nsteps >= 0) {
         for (int n = 0; n < cfg_.nsteps; ++n) {
             if ((s = update(maxDt_)) != C3D_OK)
                 return s;
             ++steps;
         }
+        if (cfg_.outputData && (s = outputData(cfg_.nsteps * maxDt_, "output")) != C3D_OK)
+            return s;
     } else {
         // src/main.cpp:57-76
         double t = 0.0, dt;
@@ -317,6 +377,8 @@ c3d_status Solver::run(int *stepsTaken)
                     return s;
                 ++steps;
             }
+            if (cfg_.outputData && (s = outputData(t, "output")) != C3D_OK)
+                return s;
             if (tOut > tFinal - 1e-14 * tFinal)
                 break;
         }
@@ -391,6 +453,21 @@ c3d_status c3d_solver_run(c3d_solver *s, int *steps) { return s ? s->s.run(steps
 c3d_status c3d_solver_pull(c3d_solver *s) { return s ? s->s.pull() : C3D_ERR_INVALID; }
 c3d_status c3d_solver_push(c3d_solver *s) { return s ? s->s.push() : C3D_ERR_INVALID; }
 c3d_ctx *c3d_solver_context(c3d_solver *s) { return s ? s->s.ctx() : nullptr; }
+
+c3d_status c3d_solver_output_data(c3d_solver *s, double time, const char *dir)
+{
+    return (s && dir) ? s->s.outputData(time, dir) : C3D_ERR_INVALID;
+}
+
+c3d_status c3d_solver_checkpoint(c3d_solver *s, double time, const char *path)
+{
+    return (s && path) ? s->s.checkpoint(path, time) : C3D_ERR_INVALID;
+}
+
+c3d_status c3d_solver_restore(c3d_solver *s, const char *path, double *time)
+{
+    return (s && path) ? s->s.restore(path, time) : C3D_ERR_INVALID;
+}
 
 /* iv: nx ny nz nm nq solver(0 pn/1 mn) nsteps ; dv: dx dy dz maxDt theta tFinal */
 void c3d_solver_info(c3d_solver *s, int *iv, double *dv)

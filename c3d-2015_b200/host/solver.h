@@ -66,6 +66,12 @@ public:
     c3d_status pull();
     // Copies the host arrays to the device (u, alpha, sigma_t, sigma_s).
     c3d_status push();
+    // outputData(time) of src/output.cpp:19-110 into dir (the reference uses "output"): the
+    // current state (pulled from the device when there is one) and closure statistics.
+    c3d_status outputData(double time, const std::string &dir);
+    // Checkpoint of (u, alpha) and the time; restore() loads it and pushes it to the device.
+    c3d_status checkpoint(const std::string &path, double time);
+    c3d_status restore(const std::string &path, double *time);
 
     const Config &config() const { return cfg_; }
     c3d_ctx *ctx() { return ctx_; }

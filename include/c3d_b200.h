@@ -180,8 +180,9 @@ c3d_status c3d_set_engine(c3d_ctx *ctx, int engine);
  * its periodic image's moments, so when its multipliers (the warm start) also equal the
  * image's bit for bit -- checked on the device before each closure -- its solve would
  * reproduce the image's; the closure then solves the other cells and copies multipliers,
- * regularised moments and records to the face ghosts. Results are identical either way;
- * closure statistics then count the solved cells only. No counterpart in the reference. */
+ * regularised moments and records to the face ghosts, whose records also enter the closure
+ * statistics. Results and statistics are identical either way. No counterpart in the
+ * reference. */
 c3d_status c3d_set_ghost_mirroring(c3d_ctx *ctx, int on);
 
 /* Standalone batched closure of n independent moment vectors (device

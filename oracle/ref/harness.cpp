@@ -109,6 +109,20 @@ double *c3dref_ptr(int which)
 /* The reference's own time step. */
 void c3dref_update(double dt) { update(dt); }
 
+/* The reference's outputData(time) (src/output.cpp:19-110) run in directory dir, which must
+ * hold an output/ subdirectory; returns 0 on success. */
+int c3dref_output_data(double time, const char *dir)
+{
+    char cwd[4096];
+    if (!getcwd(cwd, sizeof(cwd)) || chdir(dir) != 0)
+        return -1;
+    bool saved = g_outputData;
+    g_outputData = true;
+    outputData(time);
+    g_outputData = saved;
+    return chdir(cwd) == 0 ? 0 : -2;
+}
+
 void c3dref_comm() { communicateBoundaries(); }
 void c3dref_flux_kinetic(const double *alpha)
 {

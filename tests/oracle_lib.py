@@ -306,6 +306,20 @@ def _ref_worker(conn, deck, ladder, nsteps, overrides, record, want):  # noqa: C
         res["flux"] = arr(16, nall * nm).copy()
     if "pnops" in want:
         res["pnops"] = np.concatenate([arr(10 + k, nm * nm).copy() for k in range(6)])
+    if "output" in want:
+        # the reference's outputData(t) after the steps (t = nsteps * dt_max)
+        L.c3dref_output_data.argtypes = [ctypes.c_double, ctypes.c_char_p]
+        L.c3dref_output_data.restype = ctypes.c_int
+        t = nsteps * dt
+        with tempfile.TemporaryDirectory() as od:
+            os.makedirs(os.path.join(od, "output"))
+            rc = L.c3dref_output_data(t, od.encode())
+            assert rc == 0, rc
+            files = {}
+            for fn in os.listdir(os.path.join(od, "output")):
+                with open(os.path.join(od, "output", fn), "rb") as f:
+                    files[fn] = f.read()
+        res["output"] = (t, files)
     conn.send(res)
     conn.close()
 

@@ -1,5 +1,5 @@
-"""The C-ABI library loads without a GPU and exports every function include/c3d_b200.h
-declares (no compute calls here)."""
+"""The C-ABI library loads without a GPU and exports every function include/c3d_b200.h and
+include/c3d_solver.h declare (no compute calls here)."""
 import ctypes
 import os
 import re
@@ -9,8 +9,8 @@ import c3d
 REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
-def header_functions():
-    text = open(os.path.join(REPO, "include", "c3d_b200.h")).read()
+def header_functions(name="c3d_b200.h"):
+    text = open(os.path.join(REPO, "include", name)).read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
     names = re.findall(r"\b([A-Za-z_][A-Za-z0-9_]*)\s*\(", text)
     skip = {"if", "sizeof", "defined"}
@@ -24,6 +24,14 @@ def test_library_exports_header_symbols():
     missing = [n for n in declared if not hasattr(lib, n)]
     assert not missing, missing
     assert sorted(c3d.HEADER_SYMBOLS) == declared
+
+
+def test_library_exports_solver_header_symbols():
+    lib = ctypes.CDLL(c3d.LIB_PATH)
+    declared = [n for n in header_functions("c3d_solver.h") if n.startswith("c3d_solver_")]
+    missing = [n for n in declared if not hasattr(lib, n)]
+    assert not missing, missing
+    assert sorted(c3d.SOLVER_SYMBOLS) == declared
 
 
 def test_no_device_reports_error_not_abort():

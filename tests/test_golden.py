@@ -102,10 +102,7 @@ def test_gpu_c1_golden(tmp_path):
             assert rel < 1e-12, (k, rel)
     st = s.stats()
     assert st.failed == 0
-    # the deck's face ghosts start as copies of their images (the pulse is below the floor at
-    # the faces), so face-ghost mirroring copies them instead of solving them (records and
-    # moments above are the reference's either way)
-    assert st.cells == 2 * 20 * (nall - 12 * n * n)
+    assert st.cells == 2 * 20 * nall
     s.close()
 
 
