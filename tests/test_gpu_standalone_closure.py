@@ -1,0 +1,74 @@
+"""The standalone closure workload (moment vectors of every order N = 1..7 on the order's
+own tensor quadrature, 2(N+3) mu x 4(N+3) phi directions), solved back from the isotropic
+multipliers with the unbatched rules of opt() (src/opt/opt.cpp:139-355: |g| <= |u| tol,
+gamma <= 1.1) by the work-list engine, against the oracle: identical iteration counts
+except rounding ties; multipliers within 1e-7 relative (condition numbers of H reach ~1e10
+on these vectors, and the last Newton step turns rounding-level differences of the gradient
+into relative differences of alpha of up to cond * eps).
+
+Vectors: alpha_k ~ N(0, s^2) for k >= 1 with s log-uniform in [0.1, 5], alpha_0 set for unit
+density, u = <m e^{alpha.m}> in FP64 (seeded: numpy default_rng([2015, N]))."""
+import numpy as np
+import pytest
+
+import c3d
+from oracle_lib import make_opts, tie_cells
+
+pytestmark = pytest.mark.gpu
+
+LADDER = [0.0, 1e-3, 1e-2, 1e-1, 5e-1]
+TOL = 1e-8
+PER_N = 256
+
+
+def _vectors(N, n):
+    q = c3d.quadrature(N, 2 * (N + 3))
+    nm, nq = q["nm"], q["nq"]
+    M = q["M"].reshape(nq, nm)
+    rng = np.random.default_rng([2015, N])
+    s = np.exp(rng.uniform(np.log(0.1), np.log(5.0), n))
+    a = rng.standard_normal((n, nm)) * s[:, None]
+    a[:, 0] = 0.0
+    u = (np.exp(a @ M.T) * q["w"]) @ M
+    a[:, 0] = -2.0 * np.sqrt(np.pi) * np.log(u[:, 0])  # unit density (m_0 = 1/(2 sqrt(pi)))
+    u = (np.exp(a @ M.T) * q["w"]) @ M
+    a_iso = np.zeros_like(a)
+    a_iso[:, 0] = 2.0 * np.sqrt(np.pi) * np.log(u[:, 0] / (2.0 * np.sqrt(np.pi)))
+    return q, u, a, a_iso
+
+
+@pytest.mark.parametrize("N", [1, 2, 3, 4, 5, 6, 7])
+def test_standalone_closure_matches_oracle(oracle, N):
+    import torch
+    q, u, a_true, a_iso = _vectors(N, PER_N)
+    nm, nq = q["nm"], q["nq"]
+    T = oracle.tables(N, 2 * (N + 3))
+    assert np.array_equal(T["M"], q["M"])
+    ctx = c3d.Context(nx=1, ny=1, nz=1, nm=nm, nq=nq, dx=1.0, dy=1.0, dz=1.0, M=q["M"], w=q["w"],
+                      xi=q["xi"], eta=q["eta"], mu=q["mu"], batched=False, tol=TOL,
+                      ladder=LADDER)
+    du = torch.tensor(u, device="cuda")
+    da = torch.tensor(a_iso, device="cuda")
+    it = torch.zeros(PER_N, dtype=torch.int32, device="cuda")
+    rg = torch.zeros(PER_N, dtype=torch.int32, device="cuda")
+    st = torch.zeros(PER_N, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    ctx.closure_vectors_device(PER_N, du.data_ptr(), da.data_ptr(), it.data_ptr(), None,
+                               rg.data_ptr(), st.data_ptr())
+    ctx.sync()
+    ag, itg, rgg, stg = da.cpu().numpy(), it.cpu().numpy(), rg.cpu().numpy(), st.cpu().numpy()
+    ctx.close()
+    uo, ao = u.copy(), a_iso.copy()
+    ro = oracle.closure(make_opts(nm, nq, batched=False, tol=TOL, ladder=LADDER), T, uo, ao)
+    ties = tie_cells(ro)
+    assert np.array_equal(stg, ro["status"])
+    mism = itg != ro["totalIter"]
+    assert not (mism & ~ties).any(), (N, int((mism & ~ties).sum()))
+    ok = ~ties & (rgg == ro["regIndex"]) & (ro["status"] == 0)
+    rel = np.linalg.norm(ag[ok] - ao[ok], axis=1) / np.linalg.norm(ao[ok], axis=1)
+    assert rel.max() < 1e-7, (N, rel.max())
+    assert np.median(rel) < 1e-12, (N, np.median(rel))
+    # the unregularised solves recover the generating multipliers
+    clean = ok & (rgg == 0)
+    err = np.linalg.norm(ag[clean] - a_true[clean], axis=1) / np.linalg.norm(a_true[clean], axis=1)
+    assert clean.sum() > PER_N // 4 and np.median(err) < 1e-5, (N, clean.sum(), np.median(err))
