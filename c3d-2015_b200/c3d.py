@@ -25,7 +25,8 @@ SOLVER_SYMBOLS = [
     "c3d_solver_create", "c3d_solver_prepare", "c3d_solver_destroy", "c3d_solver_update",
     "c3d_solver_run", "c3d_solver_pull", "c3d_solver_push", "c3d_solver_context",
     "c3d_solver_info", "c3d_solver_host_array", "c3d_solver_output_data",
-    "c3d_solver_checkpoint", "c3d_solver_restore",
+    "c3d_solver_checkpoint", "c3d_solver_restore", "c3d_solver_output_timings",
+    "c3d_solver_output_opt_stats",
 ]
 
 # the symbols include/c3d_b200.h declares
@@ -36,7 +37,8 @@ HEADER_SYMBOLS = [
     "c3d_step", "c3d_sync", "c3d_closure_records", "c3d_closure_stats_get",
     "c3d_closure_stats_reset", "c3d_closure_vectors", "c3d_build_quadrature",
     "c3d_launch_count", "c3d_timing_enable", "c3d_timing_get", "c3d_closure_vectors_noalloc",
-    "c3d_set_gaunt", "c3d_set_engine", "c3d_set_ghost_mirroring",
+    "c3d_set_gaunt", "c3d_set_engine", "c3d_set_ghost_mirroring", "c3d_timing_events",
+    "c3d_closure_records_fp", "c3d_line_stats_enable", "c3d_line_stats_get",
 ]
 
 
@@ -128,6 +130,12 @@ def lib():
         L.c3d_solver_output_data.argtypes = [vp, ctypes.c_double, ctypes.c_char_p]
         L.c3d_solver_checkpoint.argtypes = [vp, ctypes.c_double, ctypes.c_char_p]
         L.c3d_solver_restore.argtypes = [vp, ctypes.c_char_p, _dp]
+        L.c3d_solver_output_timings.argtypes = [vp, ctypes.c_char_p]
+        L.c3d_solver_output_opt_stats.argtypes = [vp, ctypes.c_char_p]
+        L.c3d_timing_events.argtypes = [vp, _ip, _dp, ctypes.c_int]
+        L.c3d_closure_records_fp.argtypes = [vp, _dp, _dp]
+        L.c3d_line_stats_enable.argtypes = [vp, ctypes.c_int]
+        L.c3d_line_stats_get.argtypes = [vp, _dp, _ip]
         _lib = L
     return _lib
 
@@ -343,6 +351,13 @@ class Solver:
 
     def checkpoint(self, time, path):
         check(lib().c3d_solver_checkpoint(self.h, time, str(path).encode()), "checkpoint")
+
+    def output_timings(self, directory):
+        check(lib().c3d_solver_output_timings(self.h, str(directory).encode()), "output_timings")
+
+    def output_opt_stats(self, directory):
+        check(lib().c3d_solver_output_opt_stats(self.h, str(directory).encode()),
+              "output_opt_stats")
 
     def restore(self, path):
         t = ctypes.c_double(0.0)

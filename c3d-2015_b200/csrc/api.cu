@@ -20,6 +20,7 @@ struct ClosureLaunch {
     int *iters, *iterGamma, *regIdx, *status;
     unsigned long long *failCount;
     unsigned long long *stats;
+    double *gamma, *normG; // per-cell final gamma and |g| (may be null)
     int *errorFlag;
     int numSMs;
     cudaStream_t stream;
@@ -44,6 +45,7 @@ struct RoundsLaunch {
     double *u, *alpha;
     int *iters, *iterGamma, *regIdx, *status;
     unsigned long long *failCount, *stats;
+    double *gamma, *normG;     // per-cell final gamma and |g| (may be null)
     void *state;
     int *listA, *listB;
     unsigned int *counts;
@@ -75,6 +77,10 @@ size_t flux_frag_doubles(int nm, int nq, int which);
 cudaError_t launch_reproject(const GridDims &g, double *u, double *alpha, const double *mfA,
                              const double *mfP, int nq, int *errorFlag, cudaStream_t st);
 cudaError_t launch_ghost_fill_int(const GridDims &g, int *a, int numSMs, cudaStream_t st);
+cudaError_t launch_ghost_fill_1(const GridDims &g, double *a, int numSMs, cudaStream_t st);
+cudaError_t launch_line_log(const GridDims &g, const ClosureParams &P, const int *iters,
+                            const int *iterGamma, const int *regIdx, const double *gamma,
+                            const double *normG, double *out, cudaStream_t st);
 cudaError_t launch_ghost_stats(const GridDims &g, const int *iters, const int *iterGamma,
                                const int *regIdx, const int *status, unsigned long long *stats,
                                int numSMs, cudaStream_t st);
@@ -151,6 +157,10 @@ struct c3d_ctx {
     double *M = nullptr, *w = nullptr, *xi = nullptr, *eta = nullptr, *mu = nullptr;
     double *mfA = nullptr, *mfP = nullptr; // basis in the flux kernels' fragment order
     bool reproject = false;                // MN_REPROJECT
+    double *cellGamma = nullptr, *cellErr = nullptr; // per-cell final gamma and |g|
+    // x-line statistics log (the reference's g_optStats, src/update.cpp:66-75,147-155)
+    double *lineLog = nullptr;
+    int lineCap = 0, lineCount = 0;
     double *chunks = nullptr, *pnops = nullptr, *psi = nullptr;
     int *iters = nullptr, *iterGamma = nullptr, *regIdx = nullptr, *status = nullptr;
     unsigned long long *counter = nullptr, *failCount = nullptr, *stats = nullptr;
@@ -218,7 +228,7 @@ static void free_ctx(c3d_ctx *c)
                     c->counter, c->failCount, c->stats, c->errorFlag, c->gChunks, c->gVal,
                     c->gRow, c->gCol, c->gStream, c->rState, c->rListA, c->rListB,
                     c->rCounts, c->rBuf, c->mfA, c->mfP, c->cellMap, c->mirrorFlag,
-                    c->gChunksC};
+                    c->gChunksC, c->cellGamma, c->cellErr, c->lineLog};
     for (void *p : ptrs)
         if (p)
             cudaFree(p);
@@ -314,7 +324,8 @@ c3d_status c3d_create(const c3d_params *p, const double *M, const double *w, con
               alloc((void **)&c->iterGamma, nall * 4) && alloc((void **)&c->regIdx, nall * 4) &&
               alloc((void **)&c->status, nall * 4) && alloc((void **)&c->counter, 8) &&
               alloc((void **)&c->failCount, 8) && alloc((void **)&c->errorFlag, 4) &&
-              alloc((void **)&c->stats, STAT_COUNT * 8);
+              alloc((void **)&c->stats, STAT_COUNT * 8) && alloc((void **)&c->cellGamma, nall * 8) &&
+              alloc((void **)&c->cellErr, nall * 8);
     std::vector<double> ch = build_chunks(nm, nq, M, w);
     ok = ok && alloc((void **)&c->chunks, ch.size() * 8);
     std::vector<double> mfA(flux_frag_doubles(nm, nq, 0)), mfP(flux_frag_doubles(nm, nq, 1));
@@ -436,7 +447,10 @@ c3d_status c3d_ghost_fill(c3d_ctx *c)
 {
     if (!c)
         return fail(C3D_ERR_INVALID, "c3d_ghost_fill: null context");
+    cudaEvent_t t0 = nullptr;
+    timing_begin(c, &t0);
     C3D_CUDA(launch_ghost_fill(c->g, c->u, c->numSMs, c->stream));
+    timing_end(c, 2, t0);
     c->launches += 1;
     return C3D_OK;
 }
@@ -470,9 +484,14 @@ static c3d_status ensure_rounds(c3d_ctx *c, long long n)
     return C3D_OK;
 }
 
+// gridRecords: the closure covers the context's grid (directly or through cellMap), so the
+// per-cell gamma and |g| records of the context (nall entries) receive its results.
 static c3d_status run_closure(c3d_ctx *c, long long n, double *u, double *alpha, int *iters,
-                              int *iterGamma, int *regIdx, int *status, const int *cellMap = nullptr)
+                              int *iterGamma, int *regIdx, int *status, const int *cellMap = nullptr,
+                              bool gridRecords = false)
 {
+    double *recGamma = gridRecords ? c->cellGamma : nullptr;
+    double *recErr = gridRecords ? c->cellErr : nullptr;
     if (c->engine == 0) {
         c3d_status s = ensure_rounds(c, n);
         if (s != C3D_OK)
@@ -494,6 +513,8 @@ static c3d_status run_closure(c3d_ctx *c, long long n, double *u, double *alpha,
         R.status = status;
         R.failCount = c->failCount;
         R.stats = c->stats;
+        R.gamma = recGamma;
+        R.normG = recErr;
         R.state = c->rState;
         R.listA = c->rListA;
         R.listB = c->rListB;
@@ -505,10 +526,7 @@ static c3d_status run_closure(c3d_ctx *c, long long n, double *u, double *alpha,
         R.stream = c->stream;
         R.launches = &c->launches;
         R.maxRounds = 1LL << 24;
-        cudaEvent_t t0 = nullptr;
-        timing_begin(c, &t0);
         cudaError_t e = launch_closure_rounds(R, c->gaunt);
-        timing_end(c, 0, t0);
         if (e == cudaErrorLaunchTimeout)
             return fail(C3D_ERR_TIMEOUT, "closure: round limit exceeded");
         C3D_CUDA(e);
@@ -527,18 +545,17 @@ static c3d_status run_closure(c3d_ctx *c, long long n, double *u, double *alpha,
     L.status = status;
     L.failCount = c->failCount;
     L.stats = c->stats;
+    L.gamma = recGamma;
+    L.normG = recErr;
     L.errorFlag = c->errorFlag;
     L.numSMs = c->numSMs;
     L.stream = c->stream;
-    cudaEvent_t t0 = nullptr;
-    timing_begin(c, &t0);
     if (c->gaunt) {
         GauntTables G{c->gChunks, c->gRow, c->gCol, c->gVal};
         C3D_CUDA(launch_closure_gaunt(L, G));
     } else {
         C3D_CUDA(launch_closure_fp64(L));
     }
-    timing_end(c, 0, t0);
     c->launches += 2; // counter reset + closure kernel
     return C3D_OK;
 }
@@ -551,12 +568,24 @@ c3d_status c3d_closure(c3d_ctx *c)
         return fail(C3D_ERR_INVALID, "c3d_closure: null context");
     if (c->solver != 1)
         return fail(C3D_ERR_INVALID, "c3d_closure: the closure belongs to the M_N solver");
+    cudaEvent_t t0 = nullptr;
+    timing_begin(c, &t0);
     c3d_status s = closure_grid(c);
-    if (s != C3D_OK || !c->reproject)
+    if (s != C3D_OK)
         return s;
-    C3D_CUDA(launch_reproject(c->g, c->u, c->alpha, c->mfA, c->mfP, c->nq, c->errorFlag,
-                              c->stream));
-    c->launches += 1;
+    if (c->lineLog && c->lineCount < c->lineCap) {
+        C3D_CUDA(launch_line_log(c->g, c->cp, c->iters, c->iterGamma, c->regIdx, c->cellGamma,
+                                 c->cellErr, c->lineLog + (size_t)c->lineCount * c->g.nx * 5,
+                                 c->stream));
+        c->lineCount++;
+        c->launches += 1;
+    }
+    if (c->reproject) {
+        C3D_CUDA(launch_reproject(c->g, c->u, c->alpha, c->mfA, c->mfP, c->nq, c->errorFlag,
+                                  c->stream));
+        c->launches += 1;
+    }
+    timing_end(c, 0, t0);
     return C3D_OK;
 }
 
@@ -597,21 +626,24 @@ static c3d_status closure_grid(c3d_ctx *c)
         c->launches += 1;
         if (*c->mirrorHost == 0) {
             c3d_status s = run_closure(c, c->cellMapCount, c->u, c->alpha, c->iters, c->iterGamma,
-                                       c->regIdx, c->status, c->cellMap);
+                                       c->regIdx, c->status, c->cellMap, true);
             if (s != C3D_OK)
                 return s;
             C3D_CUDA(launch_ghost_fill(c->g, c->alpha, c->numSMs, c->stream));
             C3D_CUDA(launch_ghost_fill(c->g, c->u, c->numSMs, c->stream));
             for (int *a : {c->iters, c->iterGamma, c->regIdx, c->status})
                 C3D_CUDA(launch_ghost_fill_int(c->g, a, c->numSMs, c->stream));
+            for (double *a : {c->cellGamma, c->cellErr})
+                C3D_CUDA(launch_ghost_fill_1(c->g, a, c->numSMs, c->stream));
             C3D_CUDA(launch_ghost_stats(c->g, c->iters, c->iterGamma, c->regIdx, c->status,
                                         c->stats, c->numSMs, c->stream));
-            c->launches += 7;
+            c->launches += 9;
             c->mirroredClosures++;
             return C3D_OK;
         }
     }
-    return run_closure(c, c->g.nall(), c->u, c->alpha, c->iters, c->iterGamma, c->regIdx, c->status);
+    return run_closure(c, c->g.nall(), c->u, c->alpha, c->iters, c->iterGamma, c->regIdx, c->status,
+                       nullptr, true);
 }
 
 c3d_status c3d_set_gaunt(c3d_ctx *c, int nm2, const double *M2, const int *rowPtr,
@@ -814,7 +846,10 @@ c3d_status c3d_euler(c3d_ctx *c, double dt)
 {
     if (!c)
         return fail(C3D_ERR_INVALID, "c3d_euler: null context");
+    cudaEvent_t t0 = nullptr;
+    timing_begin(c, &t0);
     C3D_CUDA(launch_euler(c->g, c->u, c->flux, c->sigT, c->sigS, dt, c->numSMs, c->stream));
+    timing_end(c, 3, t0);
     c->launches += 1;
     return C3D_OK;
 }
@@ -885,6 +920,69 @@ c3d_status c3d_closure_records(c3d_ctx *c, int *iters, int *iterGamma, int *regI
     return C3D_OK;
 }
 
+c3d_status c3d_closure_records_fp(c3d_ctx *c, double *gamma, double *normG)
+{
+    if (!c)
+        return fail(C3D_ERR_INVALID, "c3d_closure_records_fp: null context");
+    const size_t b = c->g.nall() * 8;
+    C3D_CUDA(cudaStreamSynchronize(c->stream));
+    if (gamma)
+        C3D_CUDA(cudaMemcpy(gamma, c->cellGamma, b, cudaMemcpyDeviceToHost));
+    if (normG)
+        C3D_CUDA(cudaMemcpy(normG, c->cellErr, b, cudaMemcpyDeviceToHost));
+    return C3D_OK;
+}
+
+c3d_status c3d_line_stats_enable(c3d_ctx *c, int maxClosures)
+{
+    if (!c || maxClosures < 0)
+        return fail(C3D_ERR_INVALID, "c3d_line_stats_enable: bad argument");
+    if (c->lineLog) {
+        cudaFree(c->lineLog);
+        c->lineLog = nullptr;
+    }
+    c->lineCap = c->lineCount = 0;
+    if (maxClosures == 0)
+        return C3D_OK;
+    C3D_CUDA(cudaMalloc(&c->lineLog, (size_t)maxClosures * c->g.nx * 5 * sizeof(double)));
+    c->lineCap = maxClosures;
+    return C3D_OK;
+}
+
+c3d_status c3d_line_stats_get(c3d_ctx *c, double *out, int *count)
+{
+    if (!c || !count)
+        return fail(C3D_ERR_INVALID, "c3d_line_stats_get: null argument");
+    C3D_CUDA(cudaStreamSynchronize(c->stream));
+    *count = c->lineCount;
+    if (out && c->lineCount)
+        C3D_CUDA(cudaMemcpy(out, c->lineLog, (size_t)c->lineCount * c->g.nx * 5 * sizeof(double),
+                            cudaMemcpyDeviceToHost));
+    return C3D_OK;
+}
+
+int c3d_timing_events(c3d_ctx *c, int *kinds, double *ms, int maxEvents)
+{
+    if (!c)
+        return -1;
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess)
+        return -1;
+    int n = 0;
+    for (auto &e : c->events) {
+        if (n >= maxEvents)
+            break;
+        float t = 0.f;
+        if (cudaEventElapsedTime(&t, e.second.first, e.second.second) != cudaSuccess)
+            return -1;
+        if (kinds)
+            kinds[n] = e.first;
+        if (ms)
+            ms[n] = t;
+        ++n;
+    }
+    return n;
+}
+
 c3d_status c3d_closure_stats_get(c3d_ctx *c, c3d_closure_stats *st)
 {
     if (!c || !st)
@@ -941,6 +1039,8 @@ c3d_status c3d_timing_get(c3d_ctx *c, double *ms, long long *count)
     ms[0] = ms[1] = 0.0;
     long long n[2] = {0, 0};
     for (auto &e : c->events) {
+        if (e.first > 1)
+            continue;
         float t = 0.f;
         C3D_CUDA(cudaEventElapsedTime(&t, e.second.first, e.second.second));
         ms[e.first] += t;

@@ -559,6 +559,7 @@ struct Outputs {
     int *iters, *iterGamma, *regIdx, *status;
     unsigned long long *failCount; // cells finishing with a non-zero status
     unsigned long long *stats;     // running counters, layout STAT_* (may be null)
+    double *gamma, *normG;         // final gamma and |g| per cell (may be null)
 };
 
 template <class S>
@@ -582,6 +583,8 @@ __device__ void finalize(S &sl, const ClosureParams &P, const Outputs &O, int la
         if (O.iterGamma) O.iterGamma[c] = sl.s.iterGamma < 0 ? 0 : sl.s.iterGamma;
         if (O.regIdx) O.regIdx[c] = sl.s.regIndex;
         if (O.status) O.status[c] = sl.s.status;
+        if (O.gamma) O.gamma[c] = sl.s.gamma;
+        if (O.normG) O.normG[c] = sl.s.err;
         if (sl.s.status != CELL_OK && O.failCount)
             atomicAdd(O.failCount, 1ull);
         if (O.stats) {

@@ -481,6 +481,7 @@ struct ClosureLaunch {
     int *iters, *iterGamma, *regIdx, *status;
     unsigned long long *failCount;
     unsigned long long *stats;
+    double *gamma, *normG; // per-cell final gamma and |g| (may be null)
     int *errorFlag;
     int numSMs;
     cudaStream_t stream;
@@ -498,7 +499,8 @@ template <int NT, int W> static cudaError_t launch_closure_t(const ClosureLaunch
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess)
         return e;
-    Outputs O{L.u, L.alpha, L.iters, L.iterGamma, L.regIdx, L.status, L.failCount, L.stats};
+    Outputs O{L.u,      L.alpha,     L.iters, L.iterGamma, L.regIdx,
+              L.status, L.failCount, L.stats, L.gamma,     L.normG};
     long long maxCtas = (L.ncells + W - 1) / W;
     int grid = L.numSMs;
     if (maxCtas < grid)
@@ -537,7 +539,8 @@ static cudaError_t launch_gaunt_t(const ClosureLaunch &L, const GauntTables &G)
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess)
         return e;
-    Outputs O{L.u, L.alpha, L.iters, L.iterGamma, L.regIdx, L.status, L.failCount, L.stats};
+    Outputs O{L.u,      L.alpha,     L.iters, L.iterGamma, L.regIdx,
+              L.status, L.failCount, L.stats, L.gamma,     L.normG};
     long long maxCtas = (L.ncells + W - 1) / W;
     int grid = L.numSMs;
     if (maxCtas < grid)

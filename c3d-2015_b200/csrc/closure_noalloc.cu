@@ -36,6 +36,7 @@ struct ClosureLaunch {
     int *iters, *iterGamma, *regIdx, *status;
     unsigned long long *failCount;
     unsigned long long *stats;
+    double *gamma, *normG; // per-cell final gamma and |g| (may be null)
     int *errorFlag;
     int numSMs;
     cudaStream_t stream;

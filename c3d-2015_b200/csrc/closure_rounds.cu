@@ -464,6 +464,7 @@ struct RoundsLaunch {
     double *u, *alpha;
     int *iters, *iterGamma, *regIdx, *status;
     unsigned long long *failCount, *stats;
+    double *gamma, *normG;     // per-cell final gamma and |g| (may be null)
     void *state;               // ncells x rounds_state_bytes(nm)
     int *listA, *listB;        // ncells each
     unsigned int *counts;      // 2 device counters
@@ -531,7 +532,8 @@ template <int NT, int NT2, bool GAUNT> static cudaError_t rounds_t(const RoundsL
     if (e != cudaSuccess)
         return e;
     const double m0 = R.m0;
-    const Outputs O{R.u, R.alpha, R.iters, R.iterGamma, R.regIdx, R.status, R.failCount, R.stats};
+    const Outputs O{R.u,      R.alpha,     R.iters, R.iterGamma, R.regIdx,
+                    R.status, R.failCount, R.stats, R.gamma,     R.normG};
 
     // round 0: set-up of every cell
     unsigned int *cA = R.counts, *cB = R.counts + 1;

@@ -67,6 +67,26 @@ __global__ void ghost_stats_kernel(GridDims g, const int *__restrict__ iters,
     }
 }
 
+// One closure's records along the x-line (i, (ny+3)/2, (nz+3)/2) of interior cells:
+// {r, iter, iterGamma, gamma, normG} per cell (src/update.cpp:66-75 unbatched,
+// :147-155 batched, where the stored gamma is the gamma-iteration count).
+__global__ void line_log_kernel(GridDims g, ClosureParams P, const int *__restrict__ iters,
+                                const int *__restrict__ iterGamma, const int *__restrict__ regIdx,
+                                const double *__restrict__ gamma, const double *__restrict__ normG,
+                                double *__restrict__ out)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.nx)
+        return;
+    const long long c = g.cell(2 + i, (g.ny + 3) / 2, (g.nz + 3) / 2);
+    double *o = out + (size_t)i * 5;
+    o[0] = P.reg[regIdx[c] & 15];
+    o[1] = (double)iters[c];
+    o[2] = (double)iterGamma[c];
+    o[3] = P.batched ? (double)iterGamma[c] : gamma[c];
+    o[4] = normG[c];
+}
+
 // *flag = 1 if any face ghost of a differs (bitwise) from its periodic image.
 __global__ void ghost_mirror_check_kernel(GridDims g, const double *__restrict__ a, int ncomp,
                                           int *flag)
@@ -474,6 +494,21 @@ cudaError_t launch_ghost_fill(const GridDims &g, double *u, int numSMs, cudaStre
 cudaError_t launch_ghost_fill_int(const GridDims &g, int *a, int numSMs, cudaStream_t st)
 {
     ghost_fill_kernel<int><<<grid_for(ghost_faces(g), 256, numSMs), 256, 0, st>>>(g, a, 1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ghost_fill_1(const GridDims &g, double *a, int numSMs, cudaStream_t st)
+{
+    ghost_fill_kernel<double><<<grid_for(ghost_faces(g), 256, numSMs), 256, 0, st>>>(g, a, 1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_line_log(const GridDims &g, const ClosureParams &P, const int *iters,
+                            const int *iterGamma, const int *regIdx, const double *gamma,
+                            const double *normG, double *out, cudaStream_t st)
+{
+    line_log_kernel<<<(g.nx + 127) / 128, 128, 0, st>>>(g, P, iters, iterGamma, regIdx, gamma,
+                                                         normG, out);
     return cudaGetLastError();
 }
 

@@ -59,6 +59,57 @@ bool write_output_data(const std::string &dir, double time, const Config &c, int
     return ok;
 }
 
+bool write_timings(const std::string &dir, int numUpdates, const std::vector<double> &times,
+                   std::string &err)
+{
+    char name[512];
+    snprintf(name, sizeof(name), "%s/times.master", dir.c_str());
+    FILE *f = fopen(name, "w");
+    if (!f) {
+        err = std::string("could not open ") + name;
+        return false;
+    }
+    fprintf(f, "%d\n1\n1\n1\ntimes_%d.dat\n", numUpdates, 0);
+    fclose(f);
+    snprintf(name, sizeof(name), "%s/times_%d.dat", dir.c_str(), 0);
+    f = fopen(name, "wb");
+    if (!f) {
+        err = std::string("could not open ") + name;
+        return false;
+    }
+    const size_t n = (size_t)numUpdates * 8;
+    bool ok = n <= times.size() && fwrite(times.data(), sizeof(double), n, f) == n;
+    fclose(f);
+    if (!ok)
+        err = std::string("write failed: ") + name;
+    return ok;
+}
+
+bool write_opt_stats(const std::string &dir, int numUpdates, int nx, const std::vector<double> &log,
+                     std::string &err)
+{
+    char name[512];
+    snprintf(name, sizeof(name), "%s/stats_%d.dat", dir.c_str(), 0);
+    FILE *f = fopen(name, "wb");
+    if (!f) {
+        err = std::string("could not open ") + name;
+        return false;
+    }
+    bool ok = put_i64(f, numUpdates) && put_i64(f, nx);
+    const size_t recs = (size_t)numUpdates * 2 * nx;
+    for (size_t k = 0; ok && k < recs; ++k) {
+        const double *r = log.data() + 5 * k;
+        const bool have = 5 * k + 5 <= log.size();
+        ok = put_f64(f, have ? r[0] : 0.0) && put_i64(f, have ? (long long)r[1] : 0) &&
+             put_i64(f, have ? (long long)r[2] : 0) && put_f64(f, have ? r[3] : 0.0) &&
+             put_f64(f, have ? r[4] : 0.0);
+    }
+    fclose(f);
+    if (!ok)
+        err = std::string("write failed: ") + name;
+    return ok;
+}
+
 static const char CKPT_MAGIC[8] = {'C', '3', 'D', 'C', 'K', 'P', 'T', '1'};
 
 bool write_checkpoint(const std::string &path, double time, const Config &c, int nm,

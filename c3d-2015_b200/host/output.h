@@ -19,6 +19,18 @@ struct OutputStats {
 bool write_output_data(const std::string &dir, double time, const Config &c, int nm,
                        const double *u, const OutputStats &st, std::string &err);
 
+// outputTimings (src/output.cpp:116-178): <dir>/times.master and <dir>/times_0.dat with 8
+// seconds per update (per RK stage: ghost fill, closure, flux, Euler; src/update.cpp:217-262).
+bool write_timings(const std::string &dir, int numUpdates, const std::vector<double> &times,
+                   std::string &err);
+
+// outputOptStats (src/output.cpp:184-222): <dir>/stats_0.dat, int64 numUpdates, int64 nx, then
+// per closure (2 per update) and x-line cell the record {double r; int64 iter; int64 iterGamma;
+// double gamma; double normG} (OPTIMIZATION_STATS, src/global.h:53-60). log holds 5 doubles
+// per record in that order.
+bool write_opt_stats(const std::string &dir, int numUpdates, int nx, const std::vector<double> &log,
+                     std::string &err);
+
 // Checkpoint: "C3DCKPT1", int64 nx ny nz nm, double time, u and alpha of all cells.
 bool write_checkpoint(const std::string &path, double time, const Config &c, int nm,
                       const double *u, const double *alpha, std::string &err);

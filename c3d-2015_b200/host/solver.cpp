@@ -276,6 +276,16 @@ c3d_status Solver::init(const Config &cfg, void *stream)
                 return s;
         }
     }
+    if (cfg_.outputTimings && (s = c3d_timing_enable(ctx_, 1)) != C3D_OK)
+        return s;
+    if (cfg_.outputOptStats && cfg_.solver == "mn") {
+        // room for every closure of the run (the reference sizes g_optStats from TFINAL,
+        // src/init.cpp:558-568)
+        long long steps = cfg_.nsteps >= 0 ? cfg_.nsteps
+                                           : (long long)std::ceil(cfg_.tFinal / maxDt_) + 2;
+        if ((s = c3d_line_stats_enable(ctx_, (int)(2 * steps + 2))) != C3D_OK)
+            return s;
+    }
     return push();
 }
 
@@ -290,7 +300,68 @@ c3d_status Solver::pull()
     return c3d_get_state(ctx_, u.data(), alpha.empty() ? nullptr : alpha.data(), 0);
 }
 
-c3d_status Solver::update(double dt) { return c3d_step(ctx_, dt); }
+c3d_status Solver::update(double dt)
+{
+    c3d_status s = c3d_step(ctx_, dt);
+    if (s != C3D_OK)
+        return s;
+    ++numUpdates_;
+    return cfg_.outputTimings ? record_update_times() : C3D_OK;
+}
+
+// The 8 timers of one update (src/update.cpp:217-262): per RK stage communicateBoundaries,
+// solveOptimization (0 for P_N), the flux and the Euler stage, in seconds, from the
+// context's stage events (synchronises).
+c3d_status Solver::record_update_times()
+{
+    std::vector<int> kinds(64);
+    std::vector<double> ms(64);
+    int n = c3d_timing_events(ctx_, kinds.data(), ms.data(), (int)kinds.size());
+    if (n < 0)
+        return C3D_ERR_CUDA;
+    double t[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    int stage = 0;
+    static const int slot[4] = {1, 2, 0, 3}; // kind: closure, flux, ghost fill, Euler
+    for (int e = 0; e < n; ++e) {
+        if (kinds[e] < 0 || kinds[e] > 3)
+            continue;
+        t[4 * stage + slot[kinds[e]]] += 1e-3 * ms[e];
+        if (kinds[e] == 3 && stage == 0)
+            stage = 1; // the first Euler stage ends RK stage 1
+    }
+    updateTimes_.insert(updateTimes_.end(), t, t + 8);
+    return c3d_timing_enable(ctx_, 1); // clears the events for the next update
+}
+
+c3d_status Solver::outputTimings(const std::string &dir)
+{
+    std::string err;
+    if (!write_timings(dir, numUpdates_, updateTimes_, err)) {
+        fprintf(stderr, "[c3d_b200] outputTimings: %s\n", err.c_str());
+        return C3D_ERR_INVALID;
+    }
+    return C3D_OK;
+}
+
+c3d_status Solver::outputOptStats(const std::string &dir)
+{
+    std::vector<double> log;
+    if (ctx_ && cfg_.solver == "mn") {
+        int count = 0;
+        c3d_status s = c3d_line_stats_get(ctx_, nullptr, &count);
+        if (s != C3D_OK)
+            return s;
+        log.resize((size_t)count * cfg_.nx * 5);
+        if ((s = c3d_line_stats_get(ctx_, log.data(), &count)) != C3D_OK)
+            return s;
+    }
+    std::string err;
+    if (!write_opt_stats(dir, numUpdates_, cfg_.nx, log, err)) {
+        fprintf(stderr, "[c3d_b200] outputOptStats: %s\n", err.c_str());
+        return C3D_ERR_INVALID;
+    }
+    return C3D_OK;
+}
 
 c3d_status Solver::outputData(double time, const std::string &dir)
 {
@@ -385,7 +456,14 @@ c3d_status Solver::run(int *stepsTaken)
     }
     if (stepsTaken)
         *stepsTaken = steps;
-    return c3d_sync(ctx_);
+    if ((s = c3d_sync(ctx_)) != C3D_OK)
+        return s;
+    // src/main.cpp:98-103
+    if (cfg_.outputTimings && (s = outputTimings("output")) != C3D_OK)
+        return s;
+    if (cfg_.outputOptStats && (s = outputOptStats("output")) != C3D_OK)
+        return s;
+    return C3D_OK;
 }
 
 } // namespace c3d_host
@@ -467,6 +545,16 @@ c3d_status c3d_solver_checkpoint(c3d_solver *s, double time, const char *path)
 c3d_status c3d_solver_restore(c3d_solver *s, const char *path, double *time)
 {
     return (s && path) ? s->s.restore(path, time) : C3D_ERR_INVALID;
+}
+
+c3d_status c3d_solver_output_timings(c3d_solver *s, const char *dir)
+{
+    return (s && dir) ? s->s.outputTimings(dir) : C3D_ERR_INVALID;
+}
+
+c3d_status c3d_solver_output_opt_stats(c3d_solver *s, const char *dir)
+{
+    return (s && dir) ? s->s.outputOptStats(dir) : C3D_ERR_INVALID;
 }
 
 /* iv: nx ny nz nm nq solver(0 pn/1 mn) nsteps ; dv: dx dy dz maxDt theta tFinal */

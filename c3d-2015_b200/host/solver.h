@@ -72,6 +72,11 @@ public:
     // Checkpoint of (u, alpha) and the time; restore() loads it and pushes it to the device.
     c3d_status checkpoint(const std::string &path, double time);
     c3d_status restore(const std::string &path, double *time);
+    // outputTimings / outputOptStats of src/output.cpp:116-222 for the updates run so far
+    // (the per-update timers and x-line statistics are recorded when the deck sets
+    // OUTPUT_TIMINGS / OUTPUT_OPT_STATS).
+    c3d_status outputTimings(const std::string &dir);
+    c3d_status outputOptStats(const std::string &dir);
 
     const Config &config() const { return cfg_; }
     c3d_ctx *ctx() { return ctx_; }
@@ -96,6 +101,9 @@ private:
     int nm_ = 0, nq_ = 0, nm2_ = 0;
     void prepare_gaunt();
     double dx_ = 0, dy_ = 0, dz_ = 0, maxDt_ = 0;
+    int numUpdates_ = 0;
+    std::vector<double> updateTimes_; // 8 seconds per update (OUTPUT_TIMINGS)
+    c3d_status record_update_times();
 };
 
 } // namespace c3d_host

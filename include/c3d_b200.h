@@ -234,11 +234,27 @@ c3d_status c3d_closure_vectors_noalloc(int nm, int nq, const double *M, const do
                                        long long n, double *u, double *alpha, int *iters,
                                        int *status, const c3d_closure_opts *opts, void *stream);
 
-/* Event timing on the context's stream around every closure and kinetic-flux
- * launch (off by default). c3d_timing_get returns the summed milliseconds
- * ms[0] closure, ms[1] kinetic flux and the launch counts since enabling. */
+/* Event timing on the context's stream around every grid closure (kind 0), kinetic flux
+ * (1), ghost fill (2) and Euler stage (3) (off by default). c3d_timing_get returns the
+ * summed milliseconds ms[0] closure, ms[1] kinetic flux and their counts since enabling;
+ * c3d_timing_events copies up to maxEvents (kind, ms) pairs in launch order and returns
+ * their number (-1 on error). They feed the reference's per-update timers
+ * (src/update.cpp:217-262). */
 c3d_status c3d_timing_enable(c3d_ctx *ctx, int on);
 c3d_status c3d_timing_get(c3d_ctx *ctx, double *ms, long long *count);
+int c3d_timing_events(c3d_ctx *ctx, int *kinds, double *ms, int maxEvents);
+
+/* Per-cell final gamma and |g| of the last closure (host arrays of nall doubles; either may
+ * be NULL). */
+c3d_status c3d_closure_records_fp(c3d_ctx *ctx, double *gamma, double *normG);
+
+/* x-line statistics of the reference (g_optStats, src/update.cpp:66-75,147-155): after
+ * each grid closure, for the interior cells (i, (ny+3)/2, (nz+3)/2) the records
+ * {r, iter, iterGamma, gamma, normG} (5 doubles per cell; gamma holds iterGamma under the
+ * batched rules, as the reference's batched path stores it) are appended to a device log of
+ * up to maxClosures closures (0 disables). c3d_line_stats_get copies count*nx*5 doubles. */
+c3d_status c3d_line_stats_enable(c3d_ctx *ctx, int maxClosures);
+c3d_status c3d_line_stats_get(c3d_ctx *ctx, double *out, int *count);
 
 #ifdef __cplusplus
 }

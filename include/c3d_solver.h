@@ -51,6 +51,13 @@ double *c3d_solver_host_array(c3d_solver *s, int which);
  * the reference's formats. */
 c3d_status c3d_solver_output_data(c3d_solver *s, double time, const char *dir);
 
+/* outputTimings / outputOptStats of src/output.cpp:116-222 into directory dir:
+ * times.master + times_0.dat (8 seconds per update: per RK stage ghost fill, closure, flux,
+ * Euler) and stats_0.dat (per closure the x-line records {r, iter, iterGamma, gamma, normG});
+ * recorded during the run when the deck sets OUTPUT_TIMINGS / OUTPUT_OPT_STATS true. */
+c3d_status c3d_solver_output_timings(c3d_solver *s, const char *dir);
+c3d_status c3d_solver_output_opt_stats(c3d_solver *s, const char *dir);
+
 /* Checkpoint of (u, alpha) of all cells and the time ("C3DCKPT1", int64 nx ny nz nm,
  * double time, u, alpha); restore loads one written for the same grid and moment count.
  * No counterpart in the reference. */

@@ -109,6 +109,18 @@ double *c3dref_ptr(int which)
 /* The reference's own time step. */
 void c3dref_update(double dt) { update(dt); }
 
+/* The reference's outputOptStats() and outputTimings() (src/output.cpp:116-222) run in
+ * directory dir (with an output/ subdirectory); returns 0 on success. */
+int c3dref_output_stats(const char *dir)
+{
+    char cwd[4096];
+    if (!getcwd(cwd, sizeof(cwd)) || chdir(dir) != 0)
+        return -1;
+    outputOptStats();
+    outputTimings();
+    return chdir(cwd) == 0 ? 0 : -2;
+}
+
 /* The reference's outputData(time) (src/output.cpp:19-110) run in directory dir, which must
  * hold an output/ subdirectory; returns 0 on success. */
 int c3dref_output_data(double time, const char *dir)

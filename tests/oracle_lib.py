@@ -320,6 +320,19 @@ def _ref_worker(conn, deck, ladder, nsteps, overrides, record, want):  # noqa: C
                 with open(os.path.join(od, "output", fn), "rb") as f:
                     files[fn] = f.read()
         res["output"] = (t, files)
+    if "stats_files" in want:
+        # outputOptStats / outputTimings after the steps (decks with OUTPUT_OPT_STATS and
+        # OUTPUT_TIMINGS true)
+        L.c3dref_output_stats.argtypes = [ctypes.c_char_p]
+        L.c3dref_output_stats.restype = ctypes.c_int
+        with tempfile.TemporaryDirectory() as od:
+            os.makedirs(os.path.join(od, "output"))
+            assert L.c3dref_output_stats(od.encode()) == 0
+            files = {}
+            for fn in os.listdir(os.path.join(od, "output")):
+                with open(os.path.join(od, "output", fn), "rb") as f:
+                    files[fn] = f.read()
+        res["stats_files"] = files
     conn.send(res)
     conn.close()
 

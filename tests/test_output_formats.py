@@ -112,3 +112,41 @@ def test_checkpoint_round_trip(tmp_path):
     assert np.array_equal(s2.arrays()["u"], a)
     s.close()
     s2.close()
+
+
+@pytest.mark.gpu
+def test_stats_and_timing_files_match_reference(tmp_path):
+    """OUTPUT_OPT_STATS / OUTPUT_TIMINGS: stats_0.dat (the x-line records of every closure)
+    with the reference's iteration counts, gamma-iteration counts and ladder values, |g| to
+    1e-6 relative; times.master identical and times_0.dat with 8 positive-or-zero seconds per
+    update (the timers themselves are machine-dependent)."""
+    deck = deck_text(NX=8, NY=8, NZ=8, MOMENT_ORDER=2, QUAD_ORDER=12, MN_TOL=1e-6,
+                     GAUSS_SIGMA=0.2, INIT_FLOOR=1e-4, OUTPUT_OPT_STATS="true",
+                     OUTPUT_TIMINGS="true")
+    ref = run_reference(deck, nsteps=3, record=False, want=("stats_files",))
+    files = ref["stats_files"]
+    s = c3d.Solver(_write(tmp_path, deck))
+    for _ in range(3):
+        s.update(s.max_dt)
+    s.sync()
+    out = tmp_path / "out"
+    out.mkdir()
+    s.output_opt_stats(out)
+    s.output_timings(out)
+    mine = {fn: (out / fn).read_bytes() for fn in os.listdir(out)}
+    assert sorted(mine) == sorted(files)
+    assert mine["times.master"] == files["times.master"]
+    tm = np.frombuffer(mine["times_0.dat"], np.float64)
+    assert tm.size == 3 * 8 and (tm >= 0).all() and tm[1] > 0 and tm[2] > 0
+    rec = np.dtype([("r", "f8"), ("iter", "i8"), ("iterGamma", "i8"), ("gamma", "f8"),
+                    ("normG", "f8")])
+    h0 = np.frombuffer(files["stats_0.dat"][:16], np.int64)
+    h1 = np.frombuffer(mine["stats_0.dat"][:16], np.int64)
+    assert np.array_equal(h0, h1) and h1[0] == 3 and h1[1] == 8
+    r0 = np.frombuffer(files["stats_0.dat"][16:], rec)
+    r1 = np.frombuffer(mine["stats_0.dat"][16:], rec)
+    assert r0.size == r1.size == 3 * 2 * 8
+    for k in ("r", "iter", "iterGamma", "gamma"):
+        assert np.array_equal(r0[k], r1[k]), k
+    assert np.abs(r1["normG"] - r0["normG"]).max() <= 1e-6 * np.abs(r0["normG"]).max()
+    s.close()
