@@ -334,8 +334,8 @@ __device__ __forceinline__ int warp_cholesky(S &sl, int n, int lane)
 // exactDiv selects division by L_kk (as the reference's own dpotrs) instead of the
 // precomputed reciprocal.
 template <class S>
-__device__ __noinline__ void warp_apply_inverse_tiled(const S &sl, int lane, double &x0,
-                                                      double &x1, double r0, double r1);
+__device__ __forceinline__ void warp_apply_inverse_tiled(const S &sl, int lane, double &x0,
+                                                         double &x1, double r0, double r1);
 
 template <class S>
 __device__ void warp_apply_inverse(const S &sl, int n, int lane, double &x0, double &x1,
@@ -389,17 +389,14 @@ __device__ void warp_apply_inverse(const S &sl, int n, int lane, double &x0, dou
 // the tiles off the diagonal act as 8-column mat-vec updates of the rows below (forward) or
 // above (backward). Padding rows (L = I there, reciprocal 1) keep finite values and never feed
 // the real rows.
-// Kept out of line: inlined into after_hessian, builds with nvcc 12.9 for sm_100a gave
-// iteration counts that differ from the oracle's on M_6 cells (the M_6 closure parity
-// test), while this form matches it.
 template <class S>
-__device__ __noinline__ void warp_apply_inverse_tiled(const S &sl, int lane, double &x0,
-                                                      double &x1, double r0, double r1)
+__device__ __forceinline__ void warp_apply_inverse_tiled(const S &sl, int lane, double &x0,
+                                                         double &x1, double r0, double r1)
 {
     constexpr int T = S::nt;
     constexpr int NMP = S::NMP;
     const double *A = sl.L;
-#pragma unroll 1
+#pragma unroll
     for (int kb = 0; kb < T; ++kb) {
         const double *D = A + 64 * tix(kb, kb);
 #pragma unroll
@@ -436,7 +433,7 @@ __device__ __noinline__ void warp_apply_inverse_tiled(const S &sl, int lane, dou
             }
         }
     }
-#pragma unroll 1
+#pragma unroll
     for (int kb = T - 1; kb >= 0; --kb) {
         const double *D = A + 64 * tix(kb, kb);
 #pragma unroll
