@@ -38,7 +38,8 @@ HEADER_SYMBOLS = [
     "c3d_closure_stats_reset", "c3d_closure_vectors", "c3d_build_quadrature",
     "c3d_launch_count", "c3d_timing_enable", "c3d_timing_get", "c3d_closure_vectors_noalloc",
     "c3d_set_gaunt", "c3d_set_engine", "c3d_set_ghost_mirroring", "c3d_timing_events",
-    "c3d_closure_records_fp", "c3d_line_stats_enable", "c3d_line_stats_get",
+    "c3d_closure_records_fp", "c3d_line_stats_enable", "c3d_line_stats_get", "c3d_stage",
+    "c3d_set_x_halo_external", "c3d_copy_x_planes",
 ]
 
 
@@ -136,6 +137,10 @@ def lib():
         L.c3d_closure_records_fp.argtypes = [vp, _dp, _dp]
         L.c3d_line_stats_enable.argtypes = [vp, ctypes.c_int]
         L.c3d_line_stats_get.argtypes = [vp, _dp, _ip]
+        L.c3d_stage.argtypes = [vp, ctypes.c_int, ctypes.c_double]
+        L.c3d_set_x_halo_external.argtypes = [vp, ctypes.c_int]
+        L.c3d_copy_x_planes.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp,
+                                        ctypes.c_int, ctypes.c_int]
         _lib = L
     return _lib
 
@@ -239,6 +244,17 @@ class Context:
 
     def euler(self, dt):
         check(lib().c3d_euler(self.h, dt), "c3d_euler")
+
+    def stage(self, stage, dt):
+        check(lib().c3d_stage(self.h, stage, dt), "c3d_stage")
+
+    def set_x_halo_external(self, on=True):
+        check(lib().c3d_set_x_halo_external(self.h, int(bool(on))), "c3d_set_x_halo_external")
+
+    def copy_x_planes(self, field, i0, count, buf_ptr, to_buf, device):
+        """x-planes i0..i0+count-1 of u (field 0) or alpha (1) to/from a raw buffer."""
+        check(lib().c3d_copy_x_planes(self.h, field, i0, count, ctypes.c_void_p(buf_ptr),
+                                      int(bool(to_buf)), int(bool(device))), "c3d_copy_x_planes")
 
     def step(self, dt):
         check(lib().c3d_step(self.h, dt), "c3d_step")

@@ -64,7 +64,8 @@ bool closure_gaunt_supported(int nm);
 int closure_gaunt_nm2p(int nm2);
 cudaError_t launch_hessian_batch(int nm, int nchunks, const double *chunks, const double *alphas,
                                  long long n, double *hs, int *errorFlag, cudaStream_t st);
-cudaError_t launch_ghost_fill(const GridDims &g, double *u, int numSMs, cudaStream_t st);
+cudaError_t launch_ghost_fill(const GridDims &g, double *u, int numSMs, cudaStream_t st,
+                              bool skipX = false);
 cudaError_t launch_euler(const GridDims &g, double *u, const double *flux, const double *sigT,
                          const double *sigS, double dt, int numSMs, cudaStream_t st);
 cudaError_t launch_rk(const GridDims &g, double *u, double *uOld, int mode, int numSMs,
@@ -157,6 +158,7 @@ struct c3d_ctx {
     double *M = nullptr, *w = nullptr, *xi = nullptr, *eta = nullptr, *mu = nullptr;
     double *mfA = nullptr, *mfP = nullptr; // basis in the flux kernels' fragment order
     bool reproject = false;                // MN_REPROJECT
+    bool xHaloExternal = false;            // x ghosts filled by the caller (x-slab decomposition)
     double *cellGamma = nullptr, *cellErr = nullptr; // per-cell final gamma and |g|
     // x-line statistics log (the reference's g_optStats, src/update.cpp:66-75,147-155)
     double *lineLog = nullptr;
@@ -449,7 +451,7 @@ c3d_status c3d_ghost_fill(c3d_ctx *c)
         return fail(C3D_ERR_INVALID, "c3d_ghost_fill: null context");
     cudaEvent_t t0 = nullptr;
     timing_begin(c, &t0);
-    C3D_CUDA(launch_ghost_fill(c->g, c->u, c->numSMs, c->stream));
+    C3D_CUDA(launch_ghost_fill(c->g, c->u, c->numSMs, c->stream, c->xHaloExternal));
     timing_end(c, 2, t0);
     c->launches += 1;
     return C3D_OK;
@@ -591,7 +593,7 @@ c3d_status c3d_closure(c3d_ctx *c)
 
 static c3d_status closure_grid(c3d_ctx *c)
 {
-    if (c->engine == 0 && c->mirror) {
+    if (c->engine == 0 && c->mirror && !c->xHaloExternal) {
         // Face ghosts hold copies of their periodic images (src/comm.cpp:281-323); when their
         // multipliers (the warm starts) are bitwise those of the images too, the per-cell
         // solve of the reference gives them the images' results, so they are copied after
@@ -854,33 +856,70 @@ c3d_status c3d_euler(c3d_ctx *c, double dt)
     return C3D_OK;
 }
 
+c3d_status c3d_stage(c3d_ctx *c, int stage, double dt)
+{
+    if (!c || stage < 0 || stage > 1)
+        return fail(C3D_ERR_INVALID, "c3d_stage: bad argument");
+    c3d_status s;
+    if (stage == 0) {
+        C3D_CUDA(launch_rk(c->g, c->u, c->uOld, 0, c->numSMs, c->stream));
+        c->launches += 1;
+    }
+    if ((s = c3d_ghost_fill(c)) != C3D_OK)
+        return s;
+    if (c->solver == 1) {
+        if ((s = c3d_closure(c)) != C3D_OK)
+            return s;
+        if ((s = c3d_flux_kinetic(c, 0)) != C3D_OK)
+            return s;
+    } else if (!c->pnKinetic) {
+        if ((s = c3d_flux_moment(c)) != C3D_OK)
+            return s;
+    } else {
+        if ((s = c3d_flux_kinetic(c, 1)) != C3D_OK)
+            return s;
+    }
+    if ((s = c3d_euler(c, dt)) != C3D_OK)
+        return s;
+    if (stage == 1) {
+        C3D_CUDA(launch_rk(c->g, c->u, c->uOld, 1, c->numSMs, c->stream));
+        c->launches += 1;
+    }
+    return C3D_OK;
+}
+
 c3d_status c3d_step(c3d_ctx *c, double dt)
 {
     if (!c)
         return fail(C3D_ERR_INVALID, "c3d_step: null context");
-    c3d_status s;
-    C3D_CUDA(launch_rk(c->g, c->u, c->uOld, 0, c->numSMs, c->stream));
-    c->launches += 1;
-    for (int stage = 0; stage < 2; ++stage) {
-        if ((s = c3d_ghost_fill(c)) != C3D_OK)
-            return s;
-        if (c->solver == 1) {
-            if ((s = c3d_closure(c)) != C3D_OK)
-                return s;
-            if ((s = c3d_flux_kinetic(c, 0)) != C3D_OK)
-                return s;
-        } else if (!c->pnKinetic) {
-            if ((s = c3d_flux_moment(c)) != C3D_OK)
-                return s;
-        } else {
-            if ((s = c3d_flux_kinetic(c, 1)) != C3D_OK)
-                return s;
-        }
-        if ((s = c3d_euler(c, dt)) != C3D_OK)
-            return s;
-    }
-    C3D_CUDA(launch_rk(c->g, c->u, c->uOld, 1, c->numSMs, c->stream));
-    c->launches += 1;
+    c3d_status s = c3d_stage(c, 0, dt);
+    return s == C3D_OK ? c3d_stage(c, 1, dt) : s;
+}
+
+c3d_status c3d_set_x_halo_external(c3d_ctx *c, int on)
+{
+    if (!c)
+        return fail(C3D_ERR_INVALID, "c3d_set_x_halo_external: null context");
+    c->xHaloExternal = on != 0;
+    return C3D_OK;
+}
+
+c3d_status c3d_copy_x_planes(c3d_ctx *c, int field, int i0, int count, void *buf, int toBuf,
+                             int where)
+{
+    if (!c || !buf || field < 0 || field > 1 || count < 0 || i0 < 0 || i0 + count > c->g.nxg())
+        return fail(C3D_ERR_INVALID, "c3d_copy_x_planes: bad argument");
+    const size_t plane = (size_t)c->g.nyg() * c->g.nzg() * c->g.nm;
+    double *a = (field == 0 ? c->u : c->alpha) + (size_t)i0 * plane;
+    const size_t bytes = (size_t)count * plane * sizeof(double);
+    cudaMemcpyKind k = where ? cudaMemcpyDeviceToDevice
+                             : (toBuf ? cudaMemcpyDeviceToHost : cudaMemcpyHostToDevice);
+    if (toBuf)
+        C3D_CUDA(cudaMemcpyAsync(buf, a, bytes, k, c->stream));
+    else
+        C3D_CUDA(cudaMemcpyAsync(a, buf, bytes, k, c->stream));
+    if (!where)
+        C3D_CUDA(cudaStreamSynchronize(c->stream));
     return C3D_OK;
 }
 

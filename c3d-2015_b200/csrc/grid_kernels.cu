@@ -27,15 +27,17 @@ namespace c3d {
 // Two periodic ghost layers per face over interior ranges of the other two axes
 // (no edges or corners). The three face groups read only interior cells, so
 // they run as one launch. T: double state arrays (ncomp = nm) or int per-cell records.
+// f0 > 0 skips the first f0 faces: f0 = 4 ny nz leaves the x faces to the caller (x-slab
+// decomposition, whose x ghosts come from the neighbouring slabs).
 template <typename T>
-__global__ void ghost_fill_kernel(GridDims g, T *__restrict__ u, int ncomp)
+__global__ void ghost_fill_kernel(GridDims g, T *__restrict__ u, int ncomp, long long f0)
 {
-    const long long total = ghost_faces(g) * ncomp;
+    const long long total = (ghost_faces(g) - f0) * ncomp;
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
          e += (long long)gridDim.x * blockDim.x) {
         int m = (int)(e % ncomp);
         long long dst, src;
-        ghost_pair(g, e / ncomp, dst, src);
+        ghost_pair(g, f0 + e / ncomp, dst, src);
         u[dst * ncomp + m] = u[src * ncomp + m];
     }
 }
@@ -485,21 +487,24 @@ static int grid_for(long long n, int threads, int numSMs)
     return b < 1 ? 1 : (int)b;
 }
 
-cudaError_t launch_ghost_fill(const GridDims &g, double *u, int numSMs, cudaStream_t st)
+cudaError_t launch_ghost_fill(const GridDims &g, double *u, int numSMs, cudaStream_t st,
+                              bool skipX)
 {
-    ghost_fill_kernel<double><<<grid_for(ghost_faces(g) * g.nm, 256, numSMs), 256, 0, st>>>(g, u, g.nm);
+    const long long f0 = skipX ? 4LL * g.ny * g.nz : 0;
+    ghost_fill_kernel<double><<<grid_for((ghost_faces(g) - f0) * g.nm, 256, numSMs), 256, 0, st>>>(
+        g, u, g.nm, f0);
     return cudaGetLastError();
 }
 
 cudaError_t launch_ghost_fill_int(const GridDims &g, int *a, int numSMs, cudaStream_t st)
 {
-    ghost_fill_kernel<int><<<grid_for(ghost_faces(g), 256, numSMs), 256, 0, st>>>(g, a, 1);
+    ghost_fill_kernel<int><<<grid_for(ghost_faces(g), 256, numSMs), 256, 0, st>>>(g, a, 1, 0);
     return cudaGetLastError();
 }
 
 cudaError_t launch_ghost_fill_1(const GridDims &g, double *a, int numSMs, cudaStream_t st)
 {
-    ghost_fill_kernel<double><<<grid_for(ghost_faces(g), 256, numSMs), 256, 0, st>>>(g, a, 1);
+    ghost_fill_kernel<double><<<grid_for(ghost_faces(g), 256, numSMs), 256, 0, st>>>(g, a, 1, 0);
     return cudaGetLastError();
 }
 

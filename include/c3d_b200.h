@@ -146,6 +146,24 @@ c3d_status c3d_flux_moment(c3d_ctx *ctx);                  /* solveFluxMoment */
 c3d_status c3d_euler(c3d_ctx *ctx, double dt);             /* eulerStep */
 /* One SSP-RK2 step, update(dt). */
 c3d_status c3d_step(c3d_ctx *ctx, double dt);
+
+/* One RK stage of update(dt) (src/update.cpp:204-274): stage 0 saves u, then ghost fill,
+ * closure, flux and Euler stage; stage 1 does the same and ends with the RK average.
+ * c3d_step is stage 0 then stage 1. The x-slab decomposition exchanges halos between them. */
+c3d_status c3d_stage(c3d_ctx *ctx, int stage, double dt);
+
+/* x-slab decomposition (replacing the MPI halo exchange, src/comm.cpp:170-276, with slabs
+ * as in src/init.cpp:125-186): with on = 1 the ghost fill leaves the two x ghost planes on
+ * each side to the caller, who fills them from the neighbouring slabs before each stage;
+ * face-ghost mirroring is off for such a context. */
+c3d_status c3d_set_x_halo_external(c3d_ctx *ctx, int on);
+
+/* Copies the x-planes i0 .. i0+count-1 (ghost indices 0 .. nx+3; each plane (ny+4)(nz+4) nm
+ * doubles, contiguous) of u (field 0) or alpha (field 1) to (toBuf = 1) or from (toBuf = 0)
+ * buf: a device buffer (where = 1, ordered on the context's stream) or a host buffer
+ * (where = 0, synchronous). */
+c3d_status c3d_copy_x_planes(c3d_ctx *ctx, int field, int i0, int count, void *buf, int toBuf,
+                             int where);
 /* Waits for the context's stream; reports device-side failures. */
 c3d_status c3d_sync(c3d_ctx *ctx);
 
