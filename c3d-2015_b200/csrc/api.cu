@@ -731,7 +731,9 @@ c3d_status c3d_set_gaunt(c3d_ctx *c, int nm2, const double *M2, const int *rowPt
     std::vector<std::vector<GauntTerm>> lists(NEWTON_THREADS);
     for (int e = 0; e < ls; ++e) {
         std::vector<GauntTerm> &st = lists[e % NEWTON_THREADS];
-        const int t = e >> 6, rr = (e >> 3) & 7, cc = e & 7;
+        // storage offset e & 63 inside tile e >> 6 -> element (rr, cc), the inverse of toff
+        const int t = e >> 6, rr = (e >> 3) & 7;
+        const int cc = 2 * (((e >> 1) & 3) ^ ((rr >> 1) & 3)) + (e & 1);
         int ib = 0;
         while ((ib + 1) * (ib + 2) / 2 <= t)
             ++ib;

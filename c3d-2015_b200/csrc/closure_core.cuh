@@ -64,11 +64,22 @@ __host__ __device__ constexpr int pidx(int i, int j) { return (i * (i + 1)) / 2 
 // Tile (ib, jb), ib >= jb, of the lower triangle of 8x8 tiles, in row order.
 __host__ __device__ constexpr int tix(int ib, int jb) { return ib * (ib + 1) / 2 + jb; }
 
+// Offset of element (r, c) inside a tile: row-major by pairs of columns, the pair index of
+// row r XOR-ed with (r / 2) & 3. A pair (r, 2q), (r, 2q + 1) stays 16-byte aligned (the
+// Cholesky and DMMA accumulator accesses), and the 8 elements of a column land in 8
+// distinct 8-byte bank groups (the substitutions and row norms read columns).
+__host__ __device__ constexpr int toff(int r, int c)
+{
+    return 8 * r + 2 * ((c >> 1) ^ ((r >> 1) & 3)) + (c & 1);
+}
+// Offset of the pair lane l holds in the m8n8 accumulator layout (row l / 4, pair l % 4).
+__host__ __device__ constexpr int tpair(int l) { return toff(l >> 2, 2 * (l & 3)); }
+
 // Per-warp state of one cell. The lower triangle of H (then of its Cholesky factor L) is
 // either packed row by row (TILED = false) or stored as the lower triangle of 8x8 tiles of
-// the matrix padded to 8 NT rows (TILED = true): tile (ib, jb) at 64 tix(ib, jb), row-major
-// inside the tile, which is also the accumulator layout of the m8n8k4 DMMA (lane l holds
-// elements 2l and 2l + 1). Padding rows are those of the identity. 16-byte alignment keeps
+// the matrix padded to 8 NT rows (TILED = true): tile (ib, jb) at 64 tix(ib, jb), inside the
+// tile element (r, c) at toff(r, c); lane l of the m8n8k4 DMMA accumulator layout holds the
+// pair at tpair(l). Padding rows are those of the identity. 16-byte alignment keeps
 // L of every slot in an array aligned for the double2 tile accesses.
 template <int NT, bool TILED = false> struct alignas(16) Slot {
     static constexpr int NMP = Cfg<NT>::NMP;
@@ -90,7 +101,7 @@ template <int NT, bool TILED = false> struct alignas(16) Slot {
     __device__ static __forceinline__ int lx(int i, int j)
     {
         if (TILED)
-            return 64 * tix(i >> 3, j >> 3) + 8 * (i & 7) + (j & 7);
+            return 64 * tix(i >> 3, j >> 3) + toff(i & 7, j & 7);
         return pidx(i, j);
     }
 };
@@ -249,7 +260,7 @@ __device__ int warp_cholesky_tiled(S &sl, int n, int lane)
         double p0[T], p1[T];
 #pragma unroll
         for (int t = kb; t < T; ++t) {
-            double2 v = *reinterpret_cast<const double2 *>(&A[64 * tix(t, kb) + 2 * lane]);
+            double2 v = *reinterpret_cast<const double2 *>(&A[64 * tix(t, kb) + tpair(lane)]);
             p0[t] = v.x;
             p1[t] = v.y;
         }
@@ -297,7 +308,8 @@ __device__ int warp_cholesky_tiled(S &sl, int n, int lane)
         double f0[T], f1[T];
 #pragma unroll
         for (int t = kb; t < T; ++t) {
-            *reinterpret_cast<double2 *>(&A[64 * tix(t, kb) + 2 * lane]) = make_double2(p0[t], p1[t]);
+            *reinterpret_cast<double2 *>(&A[64 * tix(t, kb) + tpair(lane)]) =
+                make_double2(p0[t], p1[t]);
             double x0 = __shfl_sync(FULL_MASK, p0[t], 4 * r + (q >> 1));
             double x1 = __shfl_sync(FULL_MASK, p1[t], 4 * r + (q >> 1));
             double y0 = __shfl_sync(FULL_MASK, p0[t], 4 * r + 2 + (q >> 1));
@@ -309,7 +321,7 @@ __device__ int warp_cholesky_tiled(S &sl, int n, int lane)
         for (int jb = kb + 1; jb < T; ++jb)
 #pragma unroll
             for (int ib = jb; ib < T; ++ib) {
-                double2 *cp = reinterpret_cast<double2 *>(&A[64 * tix(ib, jb) + 2 * lane]);
+                double2 *cp = reinterpret_cast<double2 *>(&A[64 * tix(ib, jb) + tpair(lane)]);
                 double2 c = *cp;
                 dmma(c.x, c.y, -f0[ib], f0[jb]);
                 dmma(c.x, c.y, -f1[ib], f1[jb]);
@@ -410,9 +422,9 @@ __device__ __forceinline__ void warp_apply_inverse_tiled(const S &sl, int lane, 
                     x1 = xi;
             }
             if (lane > row && lane < 8 * kb + 8)
-                x0 = fma(-D[8 * (lane - 8 * kb) + i], xi, x0);
+                x0 = fma(-D[toff(lane - 8 * kb, i)], xi, x0);
             if (lane + 32 > row && lane + 32 < 8 * kb + 8)
-                x1 = fma(-D[8 * (lane + 32 - 8 * kb) + i], xi, x1);
+                x1 = fma(-D[toff(lane + 32 - 8 * kb, i)], xi, x1);
         }
         if (kb + 1 < T) {
             double y[8];
@@ -420,16 +432,16 @@ __device__ __forceinline__ void warp_apply_inverse_tiled(const S &sl, int lane, 
             for (int c = 0; c < 8; ++c)
                 y[c] = __shfl_sync(FULL_MASK, 8 * kb + c < 32 ? x0 : x1, (8 * kb + c) & 31);
             if (lane >= 8 * kb + 8 && lane < NMP) {
-                const double *Lr = A + 64 * tix(lane >> 3, kb) + 8 * (lane & 7);
+                const double *Lt = A + 64 * tix(lane >> 3, kb);
 #pragma unroll
                 for (int c = 0; c < 8; ++c)
-                    x0 = fma(-Lr[c], y[c], x0);
+                    x0 = fma(-Lt[toff(lane & 7, c)], y[c], x0);
             }
             if (lane + 32 >= 8 * kb + 8 && lane + 32 < NMP) {
-                const double *Lr = A + 64 * tix((lane + 32) >> 3, kb) + 8 * (lane & 7);
+                const double *Lt = A + 64 * tix((lane + 32) >> 3, kb);
 #pragma unroll
                 for (int c = 0; c < 8; ++c)
-                    x1 = fma(-Lr[c], y[c], x1);
+                    x1 = fma(-Lt[toff(lane & 7, c)], y[c], x1);
             }
         }
     }
@@ -447,9 +459,9 @@ __device__ __forceinline__ void warp_apply_inverse_tiled(const S &sl, int lane, 
                     x1 = xi;
             }
             if (lane >= 8 * kb && lane < row)
-                x0 = fma(-D[8 * i + (lane - 8 * kb)], xi, x0);
+                x0 = fma(-D[toff(i, lane - 8 * kb)], xi, x0);
             if (lane + 32 >= 8 * kb && lane + 32 < row)
-                x1 = fma(-D[8 * i + (lane + 32 - 8 * kb)], xi, x1);
+                x1 = fma(-D[toff(i, lane + 32 - 8 * kb)], xi, x1);
         }
         if (kb > 0) {
             double y[8];
@@ -457,16 +469,16 @@ __device__ __forceinline__ void warp_apply_inverse_tiled(const S &sl, int lane, 
             for (int c = 0; c < 8; ++c)
                 y[c] = __shfl_sync(FULL_MASK, 8 * kb + c < 32 ? x0 : x1, (8 * kb + c) & 31);
             if (lane < 8 * kb) {
-                const double *Lc = A + 64 * tix(kb, lane >> 3) + (lane & 7);
+                const double *Lt = A + 64 * tix(kb, lane >> 3);
 #pragma unroll
                 for (int c = 0; c < 8; ++c)
-                    x0 = fma(-Lc[8 * c], y[c], x0);
+                    x0 = fma(-Lt[toff(c, lane & 7)], y[c], x0);
             }
             if (lane + 32 < 8 * kb) {
-                const double *Lc = A + 64 * tix(kb, (lane + 32) >> 3) + (lane & 7);
+                const double *Lt = A + 64 * tix(kb, (lane + 32) >> 3);
 #pragma unroll
                 for (int c = 0; c < 8; ++c)
-                    x1 = fma(-Lc[8 * c], y[c], x1);
+                    x1 = fma(-Lt[toff(c, lane & 7)], y[c], x1);
             }
         }
     }
@@ -786,20 +798,20 @@ __device__ void after_hessian(S &sl, const ClosureParams &P, const Outputs &O, i
             // tiles (ib' > ib, ib); padding entries are 0
             const int ib = i >> 3, r = i & 7;
             for (int jb = 0; jb < ib; ++jb) {
-                const double *Lr = sl.L + 64 * tix(ib, jb) + 8 * r;
+                const double *Lt = sl.L + 64 * tix(ib, jb);
 #pragma unroll
                 for (int c = 0; c < 8; ++c)
-                    s += fabs(Lr[c]);
+                    s += fabs(Lt[toff(r, c)]);
             }
             const double *D = sl.L + 64 * tix(ib, ib);
 #pragma unroll
             for (int c = 0; c < 8; ++c)
-                s += fabs(c <= r ? D[8 * r + c] : D[8 * c + r]);
+                s += fabs(c <= r ? D[toff(r, c)] : D[toff(c, r)]);
             for (int ib2 = ib + 1; ib2 < S::nt; ++ib2) {
-                const double *Lc = sl.L + 64 * tix(ib2, ib) + r;
+                const double *Lt = sl.L + 64 * tix(ib2, ib);
 #pragma unroll
                 for (int c = 0; c < 8; ++c)
-                    s += fabs(Lc[8 * c]);
+                    s += fabs(Lt[toff(c, r)]);
             }
         } else {
             for (int j = 0; j < nm; ++j)

@@ -349,7 +349,7 @@ __global__ void __launch_bounds__(RW * 32, 1)
                     v0 = (row == col) ? 1.0 : 0.0;
                 if (row >= nm || col + 1 >= nm)
                     v1 = (row == col + 1) ? 1.0 : 0.0;
-                *reinterpret_cast<double2 *>(&H[64 * t + 2 * lane]) = make_double2(v0, v1);
+                *reinterpret_cast<double2 *>(&H[64 * t + tpair(lane)]) = make_double2(v0, v1);
             }
     } else if (need == NEED_TRIAL) {
         double fq = warp_sum(fpart);
