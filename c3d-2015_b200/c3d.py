@@ -29,6 +29,12 @@ SOLVER_SYMBOLS = [
     "c3d_solver_output_opt_stats",
 ]
 
+# the symbols include/c3d_serve.h declares
+SERVE_SYMBOLS = [
+    "c3d_server_create", "c3d_server_submit", "c3d_server_wait", "c3d_server_stats",
+    "c3d_server_estimate", "c3d_server_destroy",
+]
+
 # the symbols include/c3d_b200.h declares
 HEADER_SYMBOLS = [
     "c3d_last_error", "solveFluxKinetic_cuda", "solveH_cuda", "solveHInit_cuda", "c3d_create",
@@ -131,6 +137,13 @@ def lib():
         L.c3d_solver_output_data.argtypes = [vp, ctypes.c_double, ctypes.c_char_p]
         L.c3d_solver_checkpoint.argtypes = [vp, ctypes.c_double, ctypes.c_char_p]
         L.c3d_solver_restore.argtypes = [vp, ctypes.c_char_p, _dp]
+        L.c3d_server_create.argtypes = [ctypes.c_int, ctypes.c_size_t, ctypes.POINTER(vp)]
+        L.c3d_server_submit.argtypes = [vp, ctypes.c_char_p, ctypes.POINTER(ctypes.c_longlong)]
+        L.c3d_server_wait.argtypes = [vp, ctypes.c_longlong, _ip, _dp, ctypes.c_longlong, _dp,
+                                      _ip]
+        L.c3d_server_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong), _ip]
+        L.c3d_server_estimate.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_longlong)]
+        L.c3d_server_destroy.argtypes = [vp]
         L.c3d_solver_output_timings.argtypes = [vp, ctypes.c_char_p]
         L.c3d_solver_output_opt_stats.argtypes = [vp, ctypes.c_char_p]
         L.c3d_timing_events.argtypes = [vp, _ip, _dp, ctypes.c_int]
@@ -408,3 +421,53 @@ class Solver:
         check(lib().c3d_closure_records(self.ctx_handle, _p(it), _p(ig), _p(rg), _p(st)),
               "records")
         return dict(iters=it, iterGamma=ig, regIndex=rg, status=st)
+
+
+class Server:
+    """Serving loop (include/c3d_serve.h): problems given as deck text, admitted against a
+    device-memory budget and run concurrently, one context and host thread each."""
+
+    def __init__(self, workers=4, hbm_budget=0):
+        h = ctypes.c_void_p()
+        check(lib().c3d_server_create(workers, hbm_budget, ctypes.byref(h)), "c3d_server_create")
+        self.h = h
+
+    def submit(self, deck_text):
+        i = ctypes.c_longlong(0)
+        check(lib().c3d_server_submit(self.h, deck_text.encode(), ctypes.byref(i)), "submit")
+        return i.value
+
+    def wait(self, rid):
+        """(status, interior moments [nx, ny, nz, nm], latency seconds, steps)."""
+        L = lib()
+        dims = (ctypes.c_int * 4)()
+        lat = ctypes.c_double(0.0)
+        steps = ctypes.c_int(0)
+        L.c3d_server_wait(self.h, rid, dims, None, 0, None, None)
+        u = np.zeros(dims[0] * dims[1] * dims[2] * dims[3])
+        st = L.c3d_server_wait(self.h, rid, dims, u.ctypes.data_as(_dp), u.size,
+                               ctypes.byref(lat), ctypes.byref(steps))
+        return st, u.reshape(dims[0], dims[1], dims[2], dims[3]), lat.value, steps.value
+
+    def stats(self):
+        pb = ctypes.c_longlong(0)
+        pa = ctypes.c_int(0)
+        check(lib().c3d_server_stats(self.h, ctypes.byref(pb), ctypes.byref(pa)), "stats")
+        return pb.value, pa.value
+
+    @staticmethod
+    def estimate(deck_text):
+        b = ctypes.c_longlong(0)
+        check(lib().c3d_server_estimate(deck_text.encode(), ctypes.byref(b)), "estimate")
+        return b.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().c3d_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

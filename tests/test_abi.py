@@ -50,3 +50,19 @@ def test_no_device_reports_error_not_abort():
         assert "NO_DEVICE" in str(e) or "CUDA" in str(e)
     else:
         raise AssertionError("context creation without a device must fail")
+
+
+def test_library_exports_serve_header_symbols():
+    lib = ctypes.CDLL(c3d.LIB_PATH)
+    declared = [n for n in header_functions("c3d_serve.h") if n.startswith("c3d_server_")]
+    missing = [n for n in declared if not hasattr(lib, n)]
+    assert not missing, missing
+    assert sorted(c3d.SERVE_SYMBOLS) == declared
+
+
+def test_serve_footprint_estimate():
+    """The admission test's device-memory estimate grows with the grid and the order."""
+    from oracle_lib import deck_text
+    small = c3d.Server.estimate(deck_text(NX=8, NY=8, NZ=8, MOMENT_ORDER=1, QUAD_ORDER=4))
+    big = c3d.Server.estimate(deck_text(NX=32, NY=32, NZ=32, MOMENT_ORDER=5, QUAD_ORDER=16))
+    assert 0 < small < big
