@@ -127,8 +127,10 @@ __global__ void __launch_bounds__(RW * 32, 2)
     const int CH = (nm2 + 1) * QCP; // doubles per chunk (multiple of 4: 16-byte copies)
     double *stage = reinterpret_cast<double *>(smem_raw);
     double *cbuf = stage + GSTAGES * CH; // QC x CST2
-    double *alph = cbuf + QC * CST2;     // RWP x nm
-    uint64_t *full = reinterpret_cast<uint64_t *>(alph + RWP * nm + (RWP * nm & 1));
+    // multipliers of warp w's two cells interleaved, (cell 2w, cell 2w + 1) per moment: one
+    // 16-byte broadcast load feeds both cells' exponents
+    double2 *alph = reinterpret_cast<double2 *>(cbuf + QC * CST2); // RW x nm
+    uint64_t *full = reinterpret_cast<uint64_t *>(alph + RW * nm);
     __shared__ int s_abort;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t chunkBytes = CH * sizeof(double);
@@ -143,8 +145,13 @@ __global__ void __launch_bounds__(RW * 32, 2)
             cell[e] = list[pos];
             need[e] = state[cell[e]].s.need;
         }
-        for (int i = lane; i < nm; i += 32)
-            alph[(2 * warp + e) * nm + i] = cell[e] >= 0 ? state[cell[e]].alpha[i] : 0.0;
+        for (int i = lane; i < nm; i += 32) {
+            const double a = cell[e] >= 0 ? state[cell[e]].alpha[i] : 0.0;
+            if (e == 0)
+                alph[warp * nm + i].x = a;
+            else
+                alph[warp * nm + i].y = a;
+        }
     }
     if (tid == 0) {
         for (int s = 0; s < GSTAGES; ++s)
@@ -158,7 +165,7 @@ __global__ void __launch_bounds__(RW * 32, 2)
     }
     __syncthreads();
     const bool anyH = __syncthreads_or(need[0] == NEED_H || need[1] == NEED_H);
-    const double *a0 = alph + (2 * warp) * nm, *a1 = a0 + nm;
+    const double2 *aw = alph + warp * nm;
     double acc[RT][2][2];
 #pragma unroll
     for (int r = 0; r < RT; ++r)
@@ -180,8 +187,9 @@ __global__ void __launch_bounds__(RW * 32, 2)
             double z0 = 0.0, z1 = 0.0;
             for (int i = 0; i < nm; ++i) {
                 const double m = ch[i * QCP + lane];
-                z0 = __dadd_rn(z0, __dmul_rn(a0[i], m));
-                z1 = __dadd_rn(z1, __dmul_rn(a1[i], m));
+                const double2 a = aw[i];
+                z0 = __dadd_rn(z0, __dmul_rn(a.x, m));
+                z1 = __dadd_rn(z1, __dmul_rn(a.y, m));
             }
             const double wq = ch[nm2 * QCP + lane];
             if (need[0] != NEED_NONE) {
