@@ -45,7 +45,7 @@ HEADER_SYMBOLS = [
     "c3d_launch_count", "c3d_timing_enable", "c3d_timing_get", "c3d_closure_vectors_noalloc",
     "c3d_set_gaunt", "c3d_set_engine", "c3d_set_ghost_mirroring", "c3d_timing_events",
     "c3d_closure_records_fp", "c3d_line_stats_enable", "c3d_line_stats_get", "c3d_stage",
-    "c3d_set_x_halo_external", "c3d_copy_x_planes",
+    "c3d_set_x_halo_external", "c3d_copy_x_planes", "c3d_set_precision",
 ]
 
 
@@ -74,7 +74,9 @@ class ClosureStats(ctypes.Structure):
                 ("clkSerial", ctypes.c_longlong), ("passes", ctypes.c_longlong),
                 ("regHist", ctypes.c_longlong * 16),
                 ("iterHist", ctypes.c_longlong * 64),
-                ("clkNewton", ctypes.c_longlong * 8)]
+                ("clkNewton", ctypes.c_longlong * 8), ("hessBf16", ctypes.c_longlong),
+                ("hessTf32x3", ctypes.c_longlong), ("hessFp64", ctypes.c_longlong),
+                ("escalated", ctypes.c_longlong)]
 
 
 _lib = None
@@ -111,6 +113,8 @@ def lib():
         L.c3d_build_quadrature.argtypes = [ctypes.c_int, ctypes.c_int] + [_dp] * 6
         L.c3d_set_gaunt.argtypes = [vp, ctypes.c_int, _dp, _ip, _ip, _dp]
         L.c3d_set_engine.argtypes = [vp, ctypes.c_int]
+        L.c3d_set_precision.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                        ctypes.c_int]
         L.c3d_set_ghost_mirroring.argtypes = [vp, ctypes.c_int]
         L.c3d_timing_enable.argtypes = [vp, ctypes.c_int]
         L.c3d_timing_get.argtypes = [vp, _dp, ctypes.POINTER(ctypes.c_longlong)]
@@ -294,6 +298,14 @@ class Context:
     def set_engine(self, engine):
         """0: work-list rounds (default), 1: persistent kernel."""
         check(lib().c3d_set_engine(self.h, engine), "c3d_set_engine")
+
+    def set_precision(self, mode, cond_bf16=0.0, cond_mixed_max=0.0, mixed_iter_max=0):
+        """0: FP64 closure (default, the drop-in); 1: mixed precision -- Hessian moments on
+        the tensor cores in BF16 / 3xTF32 with FP32 accumulation, FP64 gradient, objective,
+        factorisation and fallback (Gaunt form, engine 0). Zeros select the defaults
+        (1e4, 1e7, 8)."""
+        check(lib().c3d_set_precision(self.h, int(mode), float(cond_bf16), float(cond_mixed_max),
+                                      int(mixed_iter_max)), "c3d_set_precision")
 
     def set_ghost_mirroring(self, on):
         check(lib().c3d_set_ghost_mirroring(self.h, int(bool(on))), "c3d_set_ghost_mirroring")

@@ -1,6 +1,7 @@
 // C ABI of libc3d_b200.so (declarations and contracts in include/c3d_b200.h).
 #include "../../include/c3d_b200.h"
 #include "c3d_common.cuh"
+#include "rounds_launch.h"
 
 #include <cmath>
 #include <cstdio>
@@ -33,33 +34,6 @@ struct GauntTables {
     const double *val;
 };
 cudaError_t launch_closure_gaunt(const ClosureLaunch &L, const GauntTables &G);
-struct RoundsLaunch {
-    const ClosureParams *P;
-    const double *chunks;
-    int nm2;                   // Gaunt: extended moments (chunk rows: nm2 + the weight row)
-    const GauntTerm *gstream;  // Gaunt: assembly streams, entry s of thread t at s*128 + t
-    int streamLen;             // entries per thread
-    double m0;
-    long long ncells;
-    const int *cellMap;        // closure cell i -> grid cell cellMap[i] (null: identity)
-    double *u, *alpha;
-    int *iters, *iterGamma, *regIdx, *status;
-    unsigned long long *failCount, *stats;
-    double *gamma, *normG;     // per-cell final gamma and |g| (may be null)
-    void *state;
-    int *listA, *listB;
-    unsigned int *counts;
-    unsigned int *hostCount;
-    double *buf;
-    long long batch;
-    int *errorFlag;
-    cudaStream_t stream;
-    long long *launches;
-    long long maxRounds;
-};
-cudaError_t launch_closure_rounds(const RoundsLaunch &R, bool gaunt);
-size_t rounds_state_bytes(int nm);
-size_t rounds_buf_doubles(int nm, int nm2, bool gaunt);
 bool closure_gaunt_supported(int nm);
 int closure_gaunt_nm2p(int nm2);
 cudaError_t launch_hessian_batch(int nm, int nchunks, const double *chunks, const double *alphas,
@@ -192,6 +166,12 @@ struct c3d_ctx {
     double *gChunksC = nullptr;    // work-list engine: chunks of nm2 M2 rows + the weight row
     GauntTerm *gStream = nullptr;  // tiled assembly streams of the work-list engine
     int gStreamLen = 0;
+    // mixed-precision closure (c3d_set_precision): staged chunks of the mixed pass -- FP64
+    // rows (the nm rows of M2 of degree <= N, then the weights) and the A operand in BF16 and
+    // in TF32 hi + lo -- and the per-cell condition records that seed each cell's precision
+    double *mixF64 = nullptr;
+    unsigned char *mixA[2] = {nullptr, nullptr};
+    float *cellCond = nullptr;
     // optional event timing of the closure and flux launches (kind 0 closure, 1 flux)
     bool timing = false;
     std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> events;
@@ -230,7 +210,8 @@ static void free_ctx(c3d_ctx *c)
                     c->counter, c->failCount, c->stats, c->errorFlag, c->gChunks, c->gVal,
                     c->gRow, c->gCol, c->gStream, c->rState, c->rListA, c->rListB,
                     c->rCounts, c->rBuf, c->mfA, c->mfP, c->cellMap, c->mirrorFlag,
-                    c->gChunksC, c->cellGamma, c->cellErr, c->lineLog};
+                    c->gChunksC, c->cellGamma, c->cellErr, c->lineLog, c->mixF64,
+                    c->mixA[0], c->mixA[1], c->cellCond};
     for (void *p : ptrs)
         if (p)
             cudaFree(p);
@@ -327,7 +308,7 @@ c3d_status c3d_create(const c3d_params *p, const double *M, const double *w, con
               alloc((void **)&c->status, nall * 4) && alloc((void **)&c->counter, 8) &&
               alloc((void **)&c->failCount, 8) && alloc((void **)&c->errorFlag, 4) &&
               alloc((void **)&c->stats, STAT_COUNT * 8) && alloc((void **)&c->cellGamma, nall * 8) &&
-              alloc((void **)&c->cellErr, nall * 8);
+              alloc((void **)&c->cellErr, nall * 8) && alloc((void **)&c->cellCond, nall * 4);
     std::vector<double> ch = build_chunks(nm, nq, M, w);
     ok = ok && alloc((void **)&c->chunks, ch.size() * 8);
     std::vector<double> mfA(flux_frag_doubles(nm, nq, 0)), mfP(flux_frag_doubles(nm, nq, 1));
@@ -360,6 +341,10 @@ c3d_status c3d_create(const c3d_params *p, const double *M, const double *w, con
     cudaMemset(c->failCount, 0, 8);
     cudaMemset(c->errorFlag, 0, 4);
     cudaMemset(c->stats, 0, STAT_COUNT * 8);
+    {
+        std::vector<float> none((size_t)nall, -1.0f); // no condition record yet
+        cudaMemcpy(c->cellCond, none.data(), (size_t)nall * 4, cudaMemcpyHostToDevice);
+    }
     cudaError_t e = cudaDeviceSynchronize();
     if (e != cudaSuccess) {
         free_ctx(c);
@@ -460,7 +445,7 @@ c3d_status c3d_ghost_fill(c3d_ctx *c)
 // Work-list buffers for n cells (grown on demand).
 static c3d_status ensure_rounds(c3d_ctx *c, long long n)
 {
-    size_t per = rounds_buf_doubles(c->g.nm, c->nm2, c->gaunt);
+    size_t per = rounds_buf_doubles(c->g.nm, c->nm2, c->gaunt, c->gaunt && c->cp.mixed);
     long long batch = n < (1LL << 20) ? n : (1LL << 20);
     if (n <= c->rCells && per <= c->rBufPer && batch <= c->rBatch)
         return C3D_OK;
@@ -474,12 +459,13 @@ static c3d_status ensure_rounds(c3d_ctx *c, long long n)
     c->rBuf = nullptr;
     c->rCells = c->rBatch = 0;
     C3D_CUDA(cudaMalloc(&c->rState, (size_t)n * rounds_state_bytes(c->g.nm)));
-    C3D_CUDA(cudaMalloc(&c->rListA, (size_t)n * sizeof(int)));
-    C3D_CUDA(cudaMalloc(&c->rListB, (size_t)n * sizeof(int)));
-    C3D_CUDA(cudaMalloc(&c->rCounts, 4 * sizeof(unsigned int)));
+    // one list per precision level (the FP64 closure uses the first)
+    C3D_CUDA(cudaMalloc(&c->rListA, 3 * (size_t)n * sizeof(int)));
+    C3D_CUDA(cudaMalloc(&c->rListB, 3 * (size_t)n * sizeof(int)));
+    C3D_CUDA(cudaMalloc(&c->rCounts, 8 * sizeof(unsigned int)));
     C3D_CUDA(cudaMalloc(&c->rBuf, (size_t)batch * per * sizeof(double)));
     if (!c->rHostCount)
-        C3D_CUDA(cudaMallocHost(&c->rHostCount, sizeof(unsigned int)));
+        C3D_CUDA(cudaMallocHost(&c->rHostCount, 4 * sizeof(unsigned int)));
     c->rCells = n;
     c->rBatch = batch;
     c->rBufPer = per;
@@ -517,6 +503,10 @@ static c3d_status run_closure(c3d_ctx *c, long long n, double *u, double *alpha,
         R.stats = c->stats;
         R.gamma = recGamma;
         R.normG = recErr;
+        R.cond = gridRecords ? c->cellCond : nullptr;
+        R.mixF64 = c->mixF64;
+        R.mixA[0] = c->mixA[0];
+        R.mixA[1] = c->mixA[1];
         R.state = c->rState;
         R.listA = c->rListA;
         R.listB = c->rListB;
@@ -648,14 +638,91 @@ static c3d_status closure_grid(c3d_ctx *c)
                        nullptr, true);
 }
 
+// Round to nearest even (BF16) and to nearest with ties away (TF32, as cvt.rna), on the
+// FP32 bit pattern; finite inputs.
+static uint16_t host_bf16(float x)
+{
+    uint32_t b;
+    std::memcpy(&b, &x, 4);
+    b += 0x7FFFu + ((b >> 16) & 1u);
+    return (uint16_t)(b >> 16);
+}
+static uint32_t host_tf32(float x)
+{
+    uint32_t b;
+    std::memcpy(&b, &x, 4);
+    return (b + 0x1000u) & 0xFFFFE000u;
+}
+
+// Staged chunks of the mixed-precision pass (closure_rounds.cu): per 32-direction chunk the
+// nm rows of M2 of degree <= N and the weight row in FP64 (row stride QCP), and the A
+// operand -- M2's rows padded to max(nm2p, 128) -- in the tensor cores' K-major core-matrix
+// layout: element (r, q) at (r / 8) SBO + (q es / 16) 128 + (r % 8) 16 + (q es) % 16 with
+// SBO = 128 (QC es / 16); BF16 (es 2), and TF32 (es 4) hi then lo = tf32(M2 - hi).
+static c3d_status build_mixed_chunks(c3d_ctx *c, int nm2, const double *M2,
+                                     const std::vector<double> &wh)
+{
+    const int nm = c->g.nm, nq = c->nq, nch = ceil_div(nq, QC);
+    const size_t perF = (size_t)(nm + 1) * QCP;
+    std::vector<double> f((size_t)nch * perF, 0.0);
+    const size_t ab[2] = {mixed_a_chunk_bytes(nm2, 0), mixed_a_chunk_bytes(nm2, 1)};
+    const int nm2p = 8 * ((nm2 + 7) / 8), na = nm2p < 128 ? 128 : nm2p;
+    std::vector<unsigned char> a0((size_t)nch * ab[0], 0), a1((size_t)nch * ab[1], 0);
+    const size_t tfPiece = (size_t)na * QC * 4;
+    for (int k = 0; k < nch; ++k)
+        for (int qq = 0; qq < QC; ++qq) {
+            const int q = k * QC + qq;
+            if (q >= nq)
+                break;
+            for (int r = 0; r < nm; ++r)
+                f[k * perF + (size_t)r * QCP + qq] = M2[(size_t)q * nm2 + r];
+            f[k * perF + (size_t)nm * QCP + qq] = wh[q];
+            for (int r = 0; r < nm2; ++r) {
+                const double v = M2[(size_t)q * nm2 + r];
+                const size_t o16 = (size_t)(r / 8) * (QC * 2 / 16) * 128 + (qq * 2 / 16) * 128 +
+                                   (r % 8) * 16 + (qq * 2) % 16;
+                const uint16_t h = host_bf16((float)v);
+                std::memcpy(&a0[k * ab[0] + o16], &h, 2);
+                const size_t o32 = (size_t)(r / 8) * (QC * 4 / 16) * 128 + (qq * 4 / 16) * 128 +
+                                   (r % 8) * 16 + (qq * 4) % 16;
+                const uint32_t hi = host_tf32((float)v);
+                float hf;
+                std::memcpy(&hf, &hi, 4);
+                const uint32_t lo = host_tf32((float)(v - (double)hf));
+                std::memcpy(&a1[k * ab[1] + o32], &hi, 4);
+                std::memcpy(&a1[k * ab[1] + tfPiece + o32], &lo, 4);
+            }
+        }
+    double *df = nullptr;
+    unsigned char *da0 = nullptr, *da1 = nullptr;
+    if (cudaMalloc(&df, f.size() * 8) != cudaSuccess || cudaMalloc(&da0, a0.size()) != cudaSuccess ||
+        cudaMalloc(&da1, a1.size()) != cudaSuccess) {
+        cudaGetLastError();
+        if (df) cudaFree(df);
+        if (da0) cudaFree(da0);
+        return fail(C3D_ERR_OOM, "c3d_set_gaunt: device allocation failed");
+    }
+    C3D_CUDA(cudaMemcpy(df, f.data(), f.size() * 8, cudaMemcpyHostToDevice));
+    C3D_CUDA(cudaMemcpy(da0, a0.data(), a0.size(), cudaMemcpyHostToDevice));
+    C3D_CUDA(cudaMemcpy(da1, a1.data(), a1.size(), cudaMemcpyHostToDevice));
+    if (c->mixF64) cudaFree(c->mixF64);
+    if (c->mixA[0]) cudaFree(c->mixA[0]);
+    if (c->mixA[1]) cudaFree(c->mixA[1]);
+    c->mixF64 = df;
+    c->mixA[0] = da0;
+    c->mixA[1] = da1;
+    return C3D_OK;
+}
+
 c3d_status c3d_set_gaunt(c3d_ctx *c, int nm2, const double *M2, const int *rowPtr,
                          const int *colInd, const double *val)
 {
     if (!c)
         return fail(C3D_ERR_INVALID, "c3d_set_gaunt: null context");
     if (!M2 || !rowPtr || !colInd || !val) {
-        // back to the direct form
+        // back to the direct form (FP64: the mixed closure needs the Gaunt form)
         c->gaunt = false;
+        c->cp.mixed = 0;
         return C3D_OK;
     }
     const int nm = c->g.nm, nq = c->nq;
@@ -785,6 +852,21 @@ c3d_status c3d_set_gaunt(c3d_ctx *c, int nm2, const double *M2, const int *rowPt
     c->gVal = dval;
     c->gaunt = true;
     c->nm2 = nm2;
+    return build_mixed_chunks(c, nm2, M2, wh);
+}
+
+c3d_status c3d_set_precision(c3d_ctx *c, int mode, double condBf16, double condMixedMax,
+                             int mixedIterMax)
+{
+    if (!c || mode < 0 || mode > 1)
+        return fail(C3D_ERR_INVALID, "c3d_set_precision: mode must be 0 (FP64) or 1 (mixed)");
+    if (mode == 1 && (!c->gaunt || c->engine != 0))
+        return fail(C3D_ERR_INVALID,
+                    "c3d_set_precision: the mixed closure needs the Gaunt form and engine 0");
+    c->cp.mixed = mode;
+    c->cp.condBf16 = condBf16 > 0 ? condBf16 : 1e4;
+    c->cp.condMixMax = condMixedMax > 0 ? condMixedMax : 1e7;
+    c->cp.mixIterMax = mixedIterMax > 0 ? mixedIterMax : 8;
     return C3D_OK;
 }
 
@@ -793,6 +875,8 @@ c3d_status c3d_set_engine(c3d_ctx *c, int engine)
     if (!c || engine < 0 || engine > 1)
         return fail(C3D_ERR_INVALID, "c3d_set_engine: engine must be 0 (work list) or 1 (persistent)");
     c->engine = engine;
+    if (engine != 0)
+        c->cp.mixed = 0; // the persistent kernels are FP64 only
     return C3D_OK;
 }
 
@@ -1049,6 +1133,10 @@ c3d_status c3d_closure_stats_get(c3d_ctx *c, c3d_closure_stats *st)
         st->iterHist[i] = (long long)h[STAT_ITER_HIST + i];
     for (int i = 0; i < 8; ++i)
         st->clkNewton[i] = (long long)h[STAT_CLK_NEWTON + i];
+    st->hessBf16 = (long long)h[STAT_H_BF16];
+    st->hessTf32x3 = (long long)h[STAT_H_TF32X3];
+    st->hessFp64 = (long long)h[STAT_H_FP64];
+    st->escalated = (long long)h[STAT_ESCALATED];
     return C3D_OK;
 }
 

@@ -36,6 +36,10 @@ enum StatSlot : int {
     STAT_CLK_PASS = 25,   // passes over the staged basis
     STAT_CLK_SERIAL = 26, // per-cell Newton logic after each pass
     STAT_PASSES = 27,     // passes (per CTA)
+    STAT_H_BF16 = 28,     // mixed-precision closure: Hessian visits with BF16 moments,
+    STAT_H_TF32X3 = 29,   //   with 3xTF32 split moments,
+    STAT_H_FP64 = 30,     //   with FP64 moments,
+    STAT_ESCALATED = 31,  //   and visits redone in FP64 (factorisation failed or non-finite)
     STAT_ITER_HIST = 32, // 64 bins (last: >= 63)
     STAT_CLK_NEWTON = 96, // 8 slots, builds with C3D_NEWTON_CLOCKS only: SM clocks of the
                           // work-list Newton kernel's phases (c3d_closure_stats.clkNewton)
@@ -55,6 +59,15 @@ struct ClosureParams {
     double condHMax;
     double reg[MAX_REG];
     long long passBudget; // safety bound on H/line-search passes per cell
+    // mixed-precision closure (work-list engine, Gaunt form): the Hessian's extended moments
+    // in BF16 (condition estimate <= condBf16) or 3xTF32 split products (<= condMixMax) with
+    // FP32 accumulation; FP64 moments beyond, after mixIterMax iterations at one
+    // regularisation level, and for the rest of the closure once a reduced-precision
+    // factorisation fails. Gradient, objective and line search stay FP64.
+    int mixed;
+    int mixIterMax;
+    double condBf16;
+    double condMixMax;
 };
 
 __host__ __device__ inline int ceil_div(int a, int b) { return (a + b - 1) / b; }

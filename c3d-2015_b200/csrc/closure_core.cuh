@@ -42,6 +42,12 @@ struct SlotScalars {
     long long passes;
     double u0, alphaScale, rtol, f, t, maxFactor, gd, fquad, r, gamma, err;
     int need, iter, totalIter, iterGamma, regIndex, maxIter, status, exhausted;
+    // mixed precision: condition estimate of the last Hessian (-1: none yet; +inf: the
+    // factorisation failed), FP64 moments forced for the rest of the closure, and the binary
+    // exponent of the largest w_q e^{alpha.m_q} of the last reduced-precision pass (the
+    // per-cell shift of the next one)
+    double cnd;
+    int fp64, cshift;
 };
 
 // Largest moment count (N+1)^2 whose padding to 8 gives NT tiles.
@@ -569,6 +575,8 @@ struct Outputs {
     unsigned long long *failCount; // cells finishing with a non-zero status
     unsigned long long *stats;     // running counters, layout STAT_* (may be null)
     double *gamma, *normG;         // final gamma and |g| per cell (may be null)
+    float *cond;                   // condition estimate of the last Hessian per cell, read at
+                                   // set-up as the mixed closure's first precision hint (may be null)
 };
 
 template <class S>
@@ -594,6 +602,7 @@ __device__ void finalize(S &sl, const ClosureParams &P, const Outputs &O, int la
         if (O.status) O.status[c] = sl.s.status;
         if (O.gamma) O.gamma[c] = sl.s.gamma;
         if (O.normG) O.normG[c] = sl.s.err;
+        if (O.cond) O.cond[c] = (float)sl.s.cnd;
         if (sl.s.status != CELL_OK && O.failCount)
             atomicAdd(O.failCount, 1ull);
         if (O.stats) {
@@ -729,6 +738,9 @@ __device__ void load_cell(S &sl, const ClosureParams &P, const Outputs &O, long 
         sl.s.regIndex = 0;
         sl.s.maxIter = P.maxIter;
         sl.s.status = CELL_OK;
+        sl.s.cnd = O.cond ? (double)O.cond[c] : -1.0;
+        sl.s.fp64 = 0;
+        sl.s.cshift = 0;
     }
     __syncwarp();
     if (u0 <= 0) {
@@ -772,19 +784,37 @@ __device__ void next_trial(S &sl, const ClosureParams &P, const Outputs &O, int 
     }
 }
 
+// A reduced-precision Hessian visit is redone with FP64 moments (same iteration); the cell
+// keeps FP64 moments for the rest of the closure.
+template <class S>
+__device__ void escalate_fp64(S &sl, const Outputs &O, int lane)
+{
+    __syncwarp();
+    if (lane == 0) {
+        sl.s.fp64 = 1;
+        sl.s.passes += 1;
+        sl.s.need = NEED_H;
+        if (O.stats)
+            atomicAdd(&O.stats[STAT_ESCALATED], 1ull);
+    }
+    __syncwarp();
+}
+
+// gext (mixed precision): the FP64 moments <m_i e^{alpha.m}> and fqext = <e^{alpha.m}> of
+// the pass, from which g and f are formed instead of from row 0 of the reduced-precision H.
 template <class S>
 __device__ void after_hessian(S &sl, const ClosureParams &P, const Outputs &O, int lane,
-                              double m0)
+                              double m0, const double *gext = nullptr, double fqext = 0.0)
 {
     const int nm = P.nm;
     C3D_NCLK_DECL
     // g_i = H_i0 / m_0 - u_i ; f = H_00 / m_0^2 - alpha.u  (src/opt/fobj.cpp:121-129)
     for (int i = lane; i < nm; i += 32)
-        sl.g[i] = sl.L[S::lx(i, 0)] / m0 - sl.u[i];
+        sl.g[i] = gext ? __dsub_rn(gext[i], sl.u[i]) : sl.L[S::lx(i, 0)] / m0 - sl.u[i];
     __syncwarp();
     double f = 0.0;
     if (lane == 0) {
-        f = sl.L[0] / (m0 * m0);
+        f = gext ? fqext : sl.L[0] / (m0 * m0);
         for (int i = 0; i < nm; ++i)
             f = __dsub_rn(f, __dmul_rn(sl.alpha[i], sl.u[i]));
     }
@@ -827,6 +857,8 @@ __device__ void after_hessian(S &sl, const ClosureParams &P, const Outputs &O, i
     // smaller, so if this bound is below condHMax/2 the reference's test `condest > condHMax`
     // is false whatever the estimate; the estimate is then skipped.
     bool condSure = gmin > 0.0 && norm1 * sqrt((double)nm) / gmin <= 0.5 * P.condHMax;
+    if (lane == 0) // the condition record: the Gershgorin bound, or the estimate below
+        sl.s.cnd = condSure ? norm1 * sqrt((double)nm) / gmin : 0.0;
     __syncwarp();
     C3D_NCLK(O.stats, 1, lane);
     int info = warp_cholesky(sl, nm, lane);
@@ -850,7 +882,13 @@ __device__ void after_hessian(S &sl, const ClosureParams &P, const Outputs &O, i
     __syncwarp();
     C3D_NCLK(O.stats, 3, lane);
 
+    if (lane == 0 && (info != 0 || !condSure))
+        sl.s.cnd = info != 0 ? 1.0 / 0.0 : cond;
     bool bad = (info != 0) || (cond > P.condHMax);
+    if (gext && bad) {
+        escalate_fp64(sl, O, lane);
+        return;
+    }
     if (sl.s.totalIter == 1 && bad) {
         // isotropic restart (src/opt/opt.cpp:236-247)
         double rt = P.batched ? P.tol : warp_nrm2(sl.u, nm, lane) * P.tol;

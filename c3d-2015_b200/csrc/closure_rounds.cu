@@ -16,7 +16,10 @@
 // (latency-bound, one warp per cell) lets each run at its own occupancy; a cell that
 // needs many iterations only ever occupies the short lists of later rounds.
 #include "closure_core.cuh"
+#include "rounds_launch.h"
+#include "umma.cuh"
 
+#include <cuda_bf16.h>
 #include <cstdio>
 
 namespace c3d {
@@ -68,14 +71,44 @@ __device__ void slot_to_state(const S &sl, CellState<NT> &st, int lane)
         st.s = sl.s;
 }
 
-// Appends cell c to the list when it still needs a pass.
+// The work lists of one round: 0 trials and FP64 Hessian passes, 1 BF16 Hessian passes,
+// 2 3xTF32 Hessian passes (lists 1 and 2: mixed-precision closure only).
+constexpr int NLISTS = 3;
+struct Lists {
+    int *list[NLISTS];
+    unsigned int *count[NLISTS];
+};
+
+// The list of a cell's next pass. Mixed precision: the Hessian's moments in BF16 when the
+// last condition estimate is <= condBf16, in 3xTF32 up to condMixMax or when there is no
+// estimate yet, else (and after mixIterMax iterations at one regularisation level, or once a
+// reduced-precision factorisation failed) in FP64.
+template <class S> __device__ int route_list(const S &sl, const ClosureParams &P)
+{
+    if (sl.s.need != NEED_H || !P.mixed || sl.s.fp64 || sl.s.iter > P.mixIterMax)
+        return 0;
+    const double c = sl.s.cnd;
+    if (c < 0.0)
+        return 2;
+    if (c <= P.condBf16)
+        return 1;
+    if (c <= P.condMixMax)
+        return 2;
+    return 0;
+}
+
+// Appends cell c to its list when it still needs a pass.
 template <class S>
-__device__ void append_if_needed(const S &sl, long long c, int lane, int *listOut,
-                                 unsigned int *countOut)
+__device__ void append_if_needed(const S &sl, const ClosureParams &P, long long c, int lane,
+                                 const Lists &out)
 {
     if (lane == 0 && sl.s.need != NEED_NONE) {
-        unsigned int pos = atomicAdd(countOut, 1u);
-        listOut[pos] = (int)c;
+        // selects, not an indexed parameter array (which would be copied to local memory)
+        const int l = route_list(sl, P);
+        unsigned int *cnt = l == 0 ? out.count[0] : l == 1 ? out.count[1] : out.count[2];
+        int *lst = l == 0 ? out.list[0] : l == 1 ? out.list[1] : out.list[2];
+        unsigned int pos = atomicAdd(cnt, 1u);
+        lst[pos] = (int)c;
     }
 }
 
@@ -89,7 +122,7 @@ template <int NT> using TSlot = Slot<NT, true>;
 template <int NT>
 __global__ void __launch_bounds__(RW * 32)
     rounds_init_kernel(ClosureParams P, long long ncells, const int *__restrict__ cellMap,
-                       Outputs O, CellState<NT> *state, int *listOut, unsigned int *countOut)
+                       Outputs O, CellState<NT> *state, Lists out)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     Slot<NT> *slots = reinterpret_cast<Slot<NT> *>(smem_raw);
@@ -101,7 +134,7 @@ __global__ void __launch_bounds__(RW * 32)
     // the state and work lists use the closure's own numbering c; outputs the grid cell's
     load_cell(sl, P, O, cellMap ? (long long)cellMap[c] : c, lane);
     slot_to_state(sl, state[c], lane);
-    append_if_needed(sl, c, lane, listOut, countOut);
+    append_if_needed(sl, P, c, lane, out);
 }
 
 // Pass of the Gaunt form over RWP = 16 listed cells per CTA (warp w: cells 2w, 2w + 1):
@@ -366,22 +399,283 @@ __global__ void __launch_bounds__(RW * 32, 1)
     }
 }
 
+// ---------------------------------------------------------------- mixed-precision pass
+// Pass of the mixed-precision closure over MXC = 16 listed cells per CTA that need a Hessian
+// (warp w: cells 2w, 2w + 1; lane: direction of the staged 32-direction chunk):
+//   FP64   exponents alpha.m_q (moment index ascending, unfused), c_q = w_q e^{alpha.m_q},
+//          f's sum over q, and the first-order moments <m_i e^{alpha.m}> (i < nm) as a DMMA
+//          GEMM [nm x QC] x [QC x 16] -- the gradient and objective of the FP64 stopping test
+//          and line search;
+//   tcgen05 the extended moments mom_k = sum_q M2[k][q] c_q of the Gaunt Hessian as
+//          D[128 x 16] += A[128 x K] B[16 x K]^T per M = 128 row tile (A: the staged M2 rows
+//          in BF16, or hi and lo TF32 parts; B: the cells' c_q scaled by 2^-shift, the
+//          cell's largest c of its previous pass, in the same format), FP32 accumulators in
+//          tensor memory. 3xTF32: A_hi B_hi + A_hi B_lo + A_lo B_hi.
+// One thread issues the MMAs of a chunk once the CTA has written its B tile; their commit
+// releases the chunk's stage and B buffer. Staged chunk: the nm rows of M2 of degree <= N
+// and the weight row (FP64, row stride QCP), then the A operand (c3d_set_gaunt).
+// Output entry (stride NM2P + NMP + 8 doubles): the nm2 moments, the nm FP64 moments, f's sum.
+template <int KIND> struct MixKind;
+template <> struct MixKind<0> { // BF16
+    static constexpr int ES = 2, NP = 1, KI = 16;
+    static constexpr uint32_t FMT = 1;
+};
+template <> struct MixKind<1> { // 3xTF32
+    static constexpr int ES = 4, NP = 2, KI = 8;
+    static constexpr uint32_t FMT = 2;
+};
+constexpr int MXC = 16;
+
+template <int NT2> struct MixRows {
+    static constexpr int NM2P = 8 * NT2;
+    static constexpr int NA = NM2P < 128 ? 128 : NM2P; // staged A rows (zero beyond nm2)
+    static constexpr int MT = NM2P <= 128 ? 1 : 2;     // M = 128 row tiles
+    static constexpr int ROW1 = NM2P - 128;            // first row of tile 1 (overlaps tile 0)
+    static_assert(NM2P <= 256, "two row tiles");
+};
+
+__host__ __device__ constexpr int mix_entry_doubles(int nmp, int nm2p) { return nm2p + nmp + 8; }
+
+template <int NT, int NT2, int KIND>
+__global__ void __launch_bounds__(RW * 32, KIND == 0 ? 2 : 1)
+    rounds_pass_mixed_kernel(ClosureParams P, const double *__restrict__ f64c,
+                             const unsigned char *__restrict__ ac, const int *__restrict__ list,
+                             int n, CellState<NT> *state, double *__restrict__ out, int *errorFlag)
+{
+    using K = MixKind<KIND>;
+    using R = MixRows<NT2>;
+    constexpr int NMP = 8 * NT;
+    constexpr int KG = QC * K::ES / 16, SBO = KG * 128;
+    constexpr uint32_t APB = R::NA * QC * K::ES, BPB = MXC * QC * K::ES;
+    constexpr int ESTR = mix_entry_doubles(NMP, R::NM2P);
+    constexpr uint32_t IDESC = umma_idesc(K::FMT, 128, MXC);
+    static_assert(NT <= RW, "one FP64 row tile per warp");
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    const int nm = P.nm, nchunks = P.nchunks;
+    const uint32_t f64Bytes = (uint32_t)(nm + 1) * QCP * 8;
+    const uint32_t f64Pad = (f64Bytes + 127u) & ~127u;
+    const uint32_t stg = f64Pad + K::NP * APB;
+    unsigned char *bbuf = smem_raw + GSTAGES * stg; // GSTAGES x NP x BPB
+    double *cbuf = reinterpret_cast<double *>(bbuf + GSTAGES * K::NP * BPB); // QC x CST2
+    double2 *alph = reinterpret_cast<double2 *>(cbuf + QC * CST2);          // RW x nm
+    uint64_t *full = reinterpret_cast<uint64_t *>(alph + RW * nm);
+    uint64_t *mmab = full + GSTAGES;
+    uint64_t *fin = mmab + GSTAGES;
+    __shared__ uint32_t s_tmem;
+    __shared__ int s_abort;
+    __shared__ int s_shift[MXC];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int base = blockIdx.x * MXC;
+    long long cell[2];
+    double scale[2];
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+        const int pos = base + 2 * warp + e;
+        cell[e] = pos < n ? list[pos] : -1;
+        for (int i = lane; i < nm; i += 32) {
+            const double a = cell[e] >= 0 ? state[cell[e]].alpha[i] : 0.0;
+            if (e == 0)
+                alph[warp * nm + i].x = a;
+            else
+                alph[warp * nm + i].y = a;
+        }
+        const int sh = cell[e] >= 0 ? state[cell[e]].s.cshift : 0;
+        if (lane == 0)
+            s_shift[2 * warp + e] = sh;
+        scale[e] = ldexp(1.0, -sh);
+    }
+    if (tid == 0) {
+        for (int s = 0; s < GSTAGES; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&mmab[s], 1);
+        }
+        mbar_init(fin, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        s_abort = 0;
+        for (int k = 0; k < GSTAGES && k < nchunks; ++k) {
+            unsigned char *st = smem_raw + k * stg;
+            mbar_expect_tx(&full[k], f64Bytes + K::NP * APB);
+            bulk_g2s(st, f64c + (size_t)k * (nm + 1) * QCP, f64Bytes, &full[k]);
+            bulk_g2s(st + f64Pad, ac + (size_t)k * K::NP * APB, K::NP * APB, &full[k]);
+        }
+    }
+    if (warp == 0)
+        tmem_alloc(&s_tmem, 32);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = s_tmem;
+    const double2 *aw = alph + warp * nm;
+    double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+    double fpart0 = 0.0, fpart1 = 0.0, cmax0 = 0.0, cmax1 = 0.0;
+    for (int k = 0; k < nchunks; ++k) {
+        const uint32_t s = k % GSTAGES, parity = (k / GSTAGES) & 1u;
+        if (!mbar_wait(&full[s], parity))
+            s_abort = 1;
+        if (__syncthreads_or(s_abort))
+            break;
+        const unsigned char *stb = smem_raw + s * stg;
+        const double *ch = reinterpret_cast<const double *>(stb);
+        double z0 = 0.0, z1 = 0.0;
+        for (int i = 0; i < nm; ++i) {
+            const double m = ch[i * QCP + lane];
+            const double2 a = aw[i];
+            z0 = __dadd_rn(z0, __dmul_rn(a.x, m));
+            z1 = __dadd_rn(z1, __dmul_rn(a.y, m));
+        }
+        const double wq = ch[nm * QCP + lane];
+        const double c0 = cell[0] >= 0 ? __dmul_rn(wq, exp(z0)) : 0.0;
+        const double c1 = cell[1] >= 0 ? __dmul_rn(wq, exp(z1)) : 0.0;
+        fpart0 = __dadd_rn(fpart0, c0);
+        fpart1 = __dadd_rn(fpart1, c1);
+        cmax0 = fmax(cmax0, c0);
+        cmax1 = fmax(cmax1, c1);
+        cbuf[lane * CST2 + 2 * warp] = c0;
+        cbuf[lane * CST2 + 2 * warp + 1] = c1;
+        // B tile: cell row nn, direction column lane
+        unsigned char *bt = bbuf + s * K::NP * BPB;
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+            const int nn = 2 * warp + e;
+            const double v = (e == 0 ? c0 : c1) * scale[e];
+            const uint32_t off = (nn >> 3) * SBO + ((lane * K::ES) >> 4) * 128 + (nn & 7) * 16 +
+                                 ((lane * K::ES) & 15);
+            if constexpr (KIND == 0) {
+                *reinterpret_cast<__nv_bfloat16 *>(bt + off) = __float2bfloat16_rn((float)v);
+            } else {
+                const uint32_t hi = to_tf32((float)v);
+                const float lo = (float)(v - (double)__uint_as_float(hi));
+                *reinterpret_cast<uint32_t *>(bt + off) = hi;
+                *reinterpret_cast<uint32_t *>(bt + BPB + off) = to_tf32(lo);
+            }
+        }
+        fence_async_smem();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+            const uint32_t aAddr = umma_smem_u32(stb + f64Pad), bAddr = umma_smem_u32(bt);
+#pragma unroll
+            for (int j = 0; j < QC / K::KI; ++j)
+#pragma unroll
+                for (int t = 0; t < R::MT; ++t) {
+                    const uint32_t d = tmem + 16 * t;
+                    const uint32_t a0 = aAddr + (t == 0 ? 0 : (R::ROW1 / 8) * SBO) + 256 * j;
+                    const uint32_t b0 = bAddr + 256 * j;
+                    umma_issue<KIND == 1>(d, umma_desc(a0, SBO), umma_desc(b0, SBO), IDESC,
+                                          (k > 0 || j > 0) ? 1u : 0u);
+                    if constexpr (KIND == 1) {
+                        umma_issue<true>(d, umma_desc(a0, SBO), umma_desc(b0 + BPB, SBO), IDESC, 1u);
+                        umma_issue<true>(d, umma_desc(a0 + APB, SBO), umma_desc(b0, SBO), IDESC, 1u);
+                    }
+                }
+            umma_commit(&mmab[s]);
+        }
+        // FP64 first-order moments: warp w, rows 8w .. 8w + 7
+        if (warp < NT) {
+            const int row = 8 * warp + (lane >> 2);
+#pragma unroll
+            for (int g = 0; g < QC / 4; ++g) {
+                const double b0 = cbuf[(4 * g + (lane & 3)) * CST2 + (lane >> 2)];
+                const double b1 = cbuf[(4 * g + (lane & 3)) * CST2 + 8 + (lane >> 2)];
+                const double a = row < nm ? ch[row * QCP + 4 * g + (lane & 3)] : 0.0;
+                dmma(acc[0][0], acc[0][1], a, b0);
+                dmma(acc[1][0], acc[1][1], a, b1);
+            }
+        }
+        __syncthreads();
+        if (tid == 0 && k + GSTAGES < nchunks) {
+            // the MMAs of chunk k have read stage s and B buffer s
+            if (!mbar_wait(&mmab[s], parity)) {
+                s_abort = 1;
+            } else {
+                unsigned char *st = smem_raw + s * stg;
+                const int kn = k + GSTAGES;
+                mbar_expect_tx(&full[s], f64Bytes + K::NP * APB);
+                bulk_g2s(st, f64c + (size_t)kn * (nm + 1) * QCP, f64Bytes, &full[s]);
+                bulk_g2s(st + f64Pad, ac + (size_t)kn * K::NP * APB, K::NP * APB, &full[s]);
+            }
+        }
+    }
+    // every MMA complete before the accumulators are read and the columns freed
+    if (tid == 0) {
+        umma_commit(fin);
+        if (!mbar_wait(fin, 0))
+            s_abort = 1;
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const bool ok = s_abort == 0;
+    if (!ok && tid == 0)
+        atomicExch(errorFlag, 1);
+    if (ok) {
+        const int qw = warp & 3, t = warp >> 2;
+        if (t < R::MT) {
+            uint32_t r[16];
+            tmem_ld16(tmem + ((uint32_t)(32 * qw) << 16) + 16 * t, r);
+            const int row = (t == 0 ? 0 : R::ROW1) + 32 * qw + lane;
+            if (row < R::NM2P && (t == 0 || row >= 128)) {
+#pragma unroll
+                for (int j = 0; j < MXC; ++j)
+                    if (base + j < n)
+                        out[(size_t)(base + j) * ESTR + row] =
+                            ldexp((double)__uint_as_float(r[j]), s_shift[j]);
+            }
+        }
+        if (warp < NT) {
+            const int kk = 8 * warp + (lane >> 2);
+#pragma unroll
+            for (int tt = 0; tt < 2; ++tt)
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    const int p = base + 8 * tt + 2 * (lane & 3) + e;
+                    if (p < n)
+                        out[(size_t)p * ESTR + R::NM2P + kk] = acc[tt][e];
+                }
+        }
+        const double fq0 = warp_sum(fpart0), fq1 = warp_sum(fpart1);
+        const double cm0 = warp_max(cmax0), cm1 = warp_max(cmax1);
+        if (lane == 0) {
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                const int p = base + 2 * warp + e;
+                if (p < n) {
+                    out[(size_t)p * ESTR + R::NM2P + NMP] = e == 0 ? fq0 : fq1;
+                    const double cm = e == 0 ? cm0 : cm1;
+                    int sh = (cm > 0.0 && cm < 1.0 / 0.0) ? ilogb(cm) : 0;
+                    state[cell[e]].s.cshift = sh < -120 ? -120 : sh > 120 ? 120 : sh;
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        tmem_dealloc(tmem, 32);
+    }
+}
+
 // Newton logic for the listed cells: one warp per cell, RWN cells per CTA, state staged
 // in shared memory with H in the tiled layout (TSlot).
+// MIX: the list of a mixed-precision pass (entries of mix_entry_doubles): H from the
+// reduced-precision moments, g and f from the pass's FP64 moments; a visit whose moments are
+// not all finite is redone in FP64. level: the list (0 FP64 and trials, 1 BF16, 2 3xTF32).
 // GAUNT: the CTA assembles H_ij = sum_k beta_ijk mom_k (i >= j, the CSR terms of beta in
 // the order of src/opt/fobj.cpp:81-99, laid out per tile slot by c3d_set_gaunt) for its
 // cells that need a Hessian in one sweep over the tile slots, so that each term is read once
 // for RWN cells. A cell's moments sit in its slot's g..rinv vectors, which a Hessian visit
 // recomputes afterwards. Otherwise the pass wrote H in tiles to hBuf.
-template <int NT, int NT2, bool GAUNT>
+template <int NT, int NT2, bool GAUNT, bool MIX>
 __global__ void __launch_bounds__(RWN * 32)
     rounds_newton_kernel(ClosureParams P, double m0, const int *__restrict__ list, int n,
                          CellState<NT> *state, const double *__restrict__ buf,
                          const GauntTerm *__restrict__ stream, int streamLen,
-                         Outputs O, int *listOut, unsigned int *countOut)
+                         Outputs O, Lists out, int level)
 {
     constexpr int NM2P = 8 * NT2;
     constexpr int NMP = Cfg<NT>::NMP;
+    constexpr int BSTR = MIX ? mix_entry_doubles(NMP, NM2P) : NM2P;
     constexpr int LS = TSlot<NT>::LSIZE;
     static_assert(!GAUNT || NM2P <= 4 * NMP, "moments must fit in g, d, alphaOld, rinv");
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -398,11 +692,18 @@ __global__ void __launch_bounds__(RWN * 32)
     } else if (lane == 0) {
         sl.s.need = NEED_NONE;
     }
+    bool nonFinite = false;
     if (GAUNT) {
         double *mom = sl.scratch(); // g, d, alphaOld, rinv: NM2P <= 4 NMP doubles
-        if (needH)
-            for (int k = lane; k < NM2P; k += 32)
-                mom[k] = buf[(size_t)pos * NM2P + k];
+        if (needH) {
+            bool nf = false;
+            for (int k = lane; k < NM2P; k += 32) {
+                const double v = buf[(size_t)pos * BSTR + k];
+                nf |= MIX && !isfinite(v);
+                mom[k] = v;
+            }
+            nonFinite = __any_sync(FULL_MASK, nf);
+        }
         if (__syncthreads_or(needH)) {
             bool hw[RWN];
 #pragma unroll
@@ -447,43 +748,28 @@ __global__ void __launch_bounds__(RWN * 32)
         return;
     C3D_NCLK(O.stats, 0, lane);
     if (sl.s.need == NEED_H) {
-        after_hessian(sl, P, O, lane, m0);
+        if (P.mixed && lane == 0 && O.stats)
+            atomicAdd(&O.stats[level == 1 ? STAT_H_BF16 : level == 2 ? STAT_H_TF32X3 : STAT_H_FP64],
+                      1ull);
+        if (MIX && nonFinite) {
+            escalate_fp64(sl, O, lane);
+        } else if (MIX) {
+            const double *e = buf + (size_t)pos * BSTR + NM2P;
+            after_hessian(sl, P, O, lane, m0, e, e[NMP]);
+        } else {
+            after_hessian(sl, P, O, lane, m0);
+        }
         C3D_NCLK(O.stats, 5, lane);
     } else if (sl.s.need == NEED_TRIAL) {
         after_trial(sl, P, O, lane, sl.s.fquad);
         C3D_NCLK(O.stats, 7, lane);
     }
     slot_to_state(sl, state[cell], lane);
-    append_if_needed(sl, cell, lane, listOut, countOut);
+    append_if_needed(sl, P, cell, lane, out);
     C3D_NCLK(O.stats, 6, lane);
 }
 
 // ---------------------------------------------------------------- host side
-
-struct RoundsLaunch {
-    const ClosureParams *P;
-    const double *chunks;      // direct: (NMP+1) x QCP chunks; Gaunt: (NM2P+1) x QCP chunks
-    int nm2;                   // Gaunt: extended moments (chunk rows: nm2 + the weight row)
-    const GauntTerm *gstream;  // Gaunt: assembly streams, entry s of thread t at s*128 + t
-    int streamLen;             // entries per thread
-    double m0;                 // M[0][0]
-    long long ncells;
-    const int *cellMap;        // closure cell i -> grid cell cellMap[i] (null: identity)
-    double *u, *alpha;
-    int *iters, *iterGamma, *regIdx, *status;
-    unsigned long long *failCount, *stats;
-    double *gamma, *normG;     // per-cell final gamma and |g| (may be null)
-    void *state;               // ncells x rounds_state_bytes(nm)
-    int *listA, *listB;        // ncells each
-    unsigned int *counts;      // 2 device counters
-    unsigned int *hostCount;   // pinned
-    double *buf;               // batch x (NM2P or NPK) doubles
-    long long batch;           // list entries per pass/Newton launch pair
-    int *errorFlag;
-    cudaStream_t stream;
-    long long *launches;
-    long long maxRounds;
-};
 
 template <int NT> static size_t state_bytes_t() { return sizeof(CellState<NT>); }
 
@@ -502,12 +788,31 @@ size_t rounds_state_bytes(int nm)
 }
 
 // Doubles per list entry of the pass output buffer.
-size_t rounds_buf_doubles(int nm, int nm2, bool gaunt)
+size_t rounds_buf_doubles(int nm, int nm2, bool gaunt, bool mixed)
 {
-    if (gaunt)
-        return (size_t)8 * ((nm2 + 7) / 8);
     const int nt = (nm + 7) / 8;
+    if (gaunt) {
+        const int nm2p = 8 * ((nm2 + 7) / 8);
+        return (size_t)(mixed ? mix_entry_doubles(8 * nt, nm2p) : nm2p);
+    }
     return (size_t)64 * nt * (nt + 1) / 2; // the tiled lower triangle
+}
+
+// Bytes of one staged chunk of the mixed pass's A operand (format 0 BF16, 1 TF32 hi + lo).
+size_t mixed_a_chunk_bytes(int nm2, int fmt)
+{
+    const int nm2p = 8 * ((nm2 + 7) / 8);
+    const int na = nm2p < 128 ? 128 : nm2p;
+    return (size_t)na * QC * (fmt == 0 ? 2 : 8);
+}
+
+template <int NT, int KIND> static size_t mixed_pass_smem(const ClosureParams &P, int nm2)
+{
+    using K = MixKind<KIND>;
+    const size_t f64Pad = ((size_t)(P.nm + 1) * QCP * 8 + 127) & ~(size_t)127;
+    const size_t stg = f64Pad + mixed_a_chunk_bytes(nm2, KIND);
+    return GSTAGES * stg + GSTAGES * (size_t)K::NP * MXC * QC * K::ES + (size_t)QC * CST2 * 8 +
+           (size_t)RW * P.nm * 16 + (2 * GSTAGES + 1) * 8;
 }
 
 template <int NT, int NT2, bool GAUNT> static cudaError_t rounds_t(const RoundsLaunch &R)
@@ -515,6 +820,7 @@ template <int NT, int NT2, bool GAUNT> static cudaError_t rounds_t(const RoundsL
     const ClosureParams &P = *R.P;
     CellState<NT> *state = reinterpret_cast<CellState<NT> *>(R.state);
     cudaStream_t st = R.stream;
+    const bool mixed = GAUNT && P.mixed;
     cudaError_t e;
     size_t slotSmem = RW * sizeof(Slot<NT>);
     e = cudaFuncSetAttribute(rounds_init_kernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -522,16 +828,30 @@ template <int NT, int NT2, bool GAUNT> static cudaError_t rounds_t(const RoundsL
     if (e != cudaSuccess)
         return e;
     size_t newtonSmem = RWN * sizeof(TSlot<NT>);
-    e = cudaFuncSetAttribute(rounds_newton_kernel<NT, NT2, GAUNT>,
+    e = cudaFuncSetAttribute(rounds_newton_kernel<NT, NT2, GAUNT, false>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)newtonSmem);
     if (e != cudaSuccess)
         return e;
-    size_t passSmem;
+    size_t passSmem, mixSmem[2] = {0, 0};
     if (GAUNT) {
         passSmem = GSTAGES * (size_t)(R.nm2 + 1) * QCP * 8 + (size_t)QC * CST2 * 8 +
                    (size_t)(RWP * P.nm + 1) * 8 + GSTAGES * 8;
         e = cudaFuncSetAttribute(rounds_pass_gaunt_kernel<NT, NT2>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)passSmem);
+        if (e == cudaSuccess && mixed) {
+            e = cudaFuncSetAttribute(rounds_newton_kernel<NT, NT2, GAUNT, true>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)newtonSmem);
+            mixSmem[0] = mixed_pass_smem<NT, 0>(P, R.nm2);
+            mixSmem[1] = mixed_pass_smem<NT, 1>(P, R.nm2);
+            if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(rounds_pass_mixed_kernel<NT, NT2, 0>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)mixSmem[0]);
+            if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(rounds_pass_mixed_kernel<NT, NT2, 1>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)mixSmem[1]);
+        }
     } else {
         passSmem = 3 * (size_t)Cfg<NT>::CHUNK * 8 + (size_t)RW * Cfg<NT>::NMP * 8 + 3 * 8;
         e = cudaFuncSetAttribute(rounds_pass_direct_kernel<NT>,
@@ -541,61 +861,81 @@ template <int NT, int NT2, bool GAUNT> static cudaError_t rounds_t(const RoundsL
         return e;
     const double m0 = R.m0;
     const Outputs O{R.u,      R.alpha,     R.iters, R.iterGamma, R.regIdx,
-                    R.status, R.failCount, R.stats, R.gamma,     R.normG};
+                    R.status, R.failCount, R.stats, R.gamma,     R.normG, R.cond};
 
     // round 0: set-up of every cell
-    unsigned int *cA = R.counts, *cB = R.counts + 1;
-    int *listA = R.listA, *listB = R.listB;
-    e = cudaMemsetAsync(cA, 0, sizeof(unsigned int), st);
+    Lists A, B;
+    for (int l = 0; l < NLISTS; ++l) {
+        A.list[l] = R.listA + (size_t)l * R.ncells;
+        B.list[l] = R.listB + (size_t)l * R.ncells;
+        A.count[l] = R.counts + l;
+        B.count[l] = R.counts + NLISTS + l;
+    }
+    e = cudaMemsetAsync(A.count[0], 0, NLISTS * sizeof(unsigned int), st);
     if (e != cudaSuccess)
         return e;
     rounds_init_kernel<NT><<<(unsigned)((R.ncells + RW - 1) / RW), RW * 32, slotSmem, st>>>(
-        P, R.ncells, R.cellMap, O, state, listA, cA);
+        P, R.ncells, R.cellMap, O, state, A);
     *R.launches += 2;
-    e = cudaMemcpyAsync(R.hostCount, cA, sizeof(unsigned int), cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess)
-        e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess)
-        return e;
-    long long count = *R.hostCount;
     long long rounds = 0;
-    while (count > 0) {
-        if (++rounds > R.maxRounds)
-            return cudaErrorLaunchTimeout;
-        e = cudaMemsetAsync(cB, 0, sizeof(unsigned int), st);
-        if (e != cudaSuccess)
-            return e;
-        for (long long off = 0; off < count; off += R.batch) {
-            int nb = (int)((count - off) < R.batch ? (count - off) : R.batch);
-            unsigned grid = (unsigned)((nb + RW - 1) / RW);
-            if (GAUNT)
-                rounds_pass_gaunt_kernel<NT, NT2><<<(unsigned)((nb + RWP - 1) / RWP), RW * 32,
-                                                    passSmem, st>>>(
-                    P, R.chunks, R.nm2, listA + off, nb, state, R.buf, R.errorFlag);
-            else
-                rounds_pass_direct_kernel<NT><<<grid, RW * 32, passSmem, st>>>(
-                    P, R.chunks, listA + off, nb, state, R.buf, R.errorFlag);
-            rounds_newton_kernel<NT, NT2, GAUNT><<<(unsigned)((nb + RWN - 1) / RWN), RWN * 32,
-                                                   newtonSmem, st>>>(
-                P, m0, listA + off, nb, state, R.buf, R.gstream, R.streamLen, O, listB, cB);
-            *R.launches += 2;
-            e = cudaGetLastError();
-            if (e != cudaSuccess)
-                return e;
-        }
-        *R.launches += 1;
-        e = cudaMemcpyAsync(R.hostCount, cB, sizeof(unsigned int), cudaMemcpyDeviceToHost, st);
+    for (;;) {
+        e = cudaMemcpyAsync(R.hostCount, A.count[0], NLISTS * sizeof(unsigned int),
+                            cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess)
             e = cudaStreamSynchronize(st);
         if (e != cudaSuccess)
             return e;
-        count = *R.hostCount;
-        int *t = listA;
-        listA = listB;
-        listB = t;
-        unsigned int *tc = cA;
-        cA = cB;
-        cB = tc;
+        long long cnt[NLISTS], total = 0;
+        for (int l = 0; l < NLISTS; ++l)
+            total += (cnt[l] = R.hostCount[l]);
+        if (total == 0)
+            break;
+        if (++rounds > R.maxRounds)
+            return cudaErrorLaunchTimeout;
+        e = cudaMemsetAsync(B.count[0], 0, NLISTS * sizeof(unsigned int), st);
+        if (e != cudaSuccess)
+            return e;
+        *R.launches += 1;
+        for (int l = 0; l < NLISTS; ++l) {
+            const int *la = A.list[l];
+            for (long long off = 0; off < cnt[l]; off += R.batch) {
+                int nb = (int)((cnt[l] - off) < R.batch ? (cnt[l] - off) : R.batch);
+                if (l > 0) {
+                    // mixed-precision Hessian passes (Gaunt form only)
+                    if constexpr (GAUNT) {
+                        const unsigned grid = (unsigned)((nb + MXC - 1) / MXC);
+                        if (l == 1)
+                            rounds_pass_mixed_kernel<NT, NT2, 0><<<grid, RW * 32, mixSmem[0], st>>>(
+                                P, R.mixF64, R.mixA[0], la + off, nb, state, R.buf, R.errorFlag);
+                        else
+                            rounds_pass_mixed_kernel<NT, NT2, 1><<<grid, RW * 32, mixSmem[1], st>>>(
+                                P, R.mixF64, R.mixA[1], la + off, nb, state, R.buf, R.errorFlag);
+                        rounds_newton_kernel<NT, NT2, GAUNT, true>
+                            <<<(unsigned)((nb + RWN - 1) / RWN), RWN * 32, newtonSmem, st>>>(
+                                P, m0, la + off, nb, state, R.buf, R.gstream, R.streamLen, O, B, l);
+                    }
+                } else {
+                    if (GAUNT)
+                        rounds_pass_gaunt_kernel<NT, NT2>
+                            <<<(unsigned)((nb + RWP - 1) / RWP), RW * 32, passSmem, st>>>(
+                                P, R.chunks, R.nm2, la + off, nb, state, R.buf, R.errorFlag);
+                    else
+                        rounds_pass_direct_kernel<NT><<<(unsigned)((nb + RW - 1) / RW), RW * 32,
+                                                        passSmem, st>>>(
+                            P, R.chunks, la + off, nb, state, R.buf, R.errorFlag);
+                    rounds_newton_kernel<NT, NT2, GAUNT, false>
+                        <<<(unsigned)((nb + RWN - 1) / RWN), RWN * 32, newtonSmem, st>>>(
+                            P, m0, la + off, nb, state, R.buf, R.gstream, R.streamLen, O, B, 0);
+                }
+                *R.launches += 2;
+                e = cudaGetLastError();
+                if (e != cudaSuccess)
+                    return e;
+            }
+        }
+        Lists t = A;
+        A = B;
+        B = t;
     }
     return cudaSuccess;
 }

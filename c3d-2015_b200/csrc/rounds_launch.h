@@ -1,0 +1,45 @@
+// Host-side description of one work-list closure (closure_rounds.cu), shared by the
+// context code that fills it.
+#pragma once
+#include "c3d_common.cuh"
+
+#include <cstddef>
+
+namespace c3d {
+
+struct RoundsLaunch {
+    const ClosureParams *P;
+    const double *chunks;      // direct: (NMP+1) x QCP chunks; Gaunt: (NM2P+1) x QCP chunks
+    int nm2;                   // Gaunt: extended moments (chunk rows: nm2 + the weight row)
+    const GauntTerm *gstream;  // Gaunt: assembly streams, entry s of thread t at s*128 + t
+    int streamLen;             // entries per thread
+    double m0;                 // M[0][0]
+    long long ncells;
+    const int *cellMap;        // closure cell i -> grid cell cellMap[i] (null: identity)
+    double *u, *alpha;
+    int *iters, *iterGamma, *regIdx, *status;
+    unsigned long long *failCount, *stats;
+    double *gamma, *normG;     // per-cell final gamma and |g| (may be null)
+    float *cond;               // per-cell condition estimate records (may be null)
+    void *state;               // ncells x rounds_state_bytes(nm)
+    int *listA, *listB;        // NLISTS x ncells each (one list per precision level)
+    unsigned int *counts;      // 2 NLISTS device counters
+    unsigned int *hostCount;   // NLISTS pinned
+    double *buf;               // batch x rounds_buf_doubles doubles
+    long long batch;           // list entries per pass/Newton launch pair
+    // mixed precision (P->mixed): FP64 rows (nm rows of M2 + weights) and the A operand
+    // chunks of each format (BF16; TF32 hi then lo)
+    const double *mixF64;
+    const unsigned char *mixA[2];
+    int *errorFlag;
+    cudaStream_t stream;
+    long long *launches;
+    long long maxRounds;
+};
+
+cudaError_t launch_closure_rounds(const RoundsLaunch &R, bool gaunt);
+size_t rounds_state_bytes(int nm);
+size_t rounds_buf_doubles(int nm, int nm2, bool gaunt, bool mixed);
+size_t mixed_a_chunk_bytes(int nm2, int fmt);
+
+} // namespace c3d

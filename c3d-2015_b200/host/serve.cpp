@@ -33,13 +33,16 @@ long long footprint(const c3d_host::Config &c)
     const long long nq = 2LL * c.quadOrder * c.quadOrder;
     const long long psiCap = (16LL << 30) / 8 / (nall > 0 ? nall : 1);
     const long long psiDirs = nq < psiCap ? nq : psiCap;
-    long long b = 4 * nall * nm * 8 + 2 * nall * 8 + 4 * nall * 4 + 2 * nall * 8;
+    long long b = 4 * nall * nm * 8 + 2 * nall * 8 + 5 * nall * 4 + 2 * nall * 8;
     b += psiDirs * nall * 8;
     if (c.solver == "mn") {
         const long long batch = nall < (1LL << 20) ? nall : (1LL << 20);
         const long long nm2 = (2LL * c.momentOrder + 1) * (2 * c.momentOrder + 1);
-        const long long per = c.mnUseGaunt ? 8 * ((nm2 + 7) / 8) : 64 * ((nmp / 8) * (nmp / 8 + 1) / 2);
-        b += nall * (6 * nmp * 8 + 160) + 3 * nall * 4 + batch * per * 8;
+        const long long nm2p = 8 * ((nm2 + 7) / 8);
+        const long long per = c.mnUseGaunt ? (c.mnMixed ? nm2p + nmp + 8 : nm2p)
+                                           : 64 * ((nmp / 8) * (nmp / 8 + 1) / 2);
+        // state, the work lists (one per precision level, two generations), the face map
+        b += nall * (6 * nmp * 8 + 176) + 7 * nall * 4 + batch * per * 8;
         b += nq * (nm2 + 1) * 8 * 2;
     }
     b += nq * nm * 8 * 4;

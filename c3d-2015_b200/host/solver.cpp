@@ -84,6 +84,10 @@ std::string parse_config(const InputDeck &d, Config &c)
             return "REG_LADDER must list 1 to 16 values";
     }
     d.get("MN_REPROJECT", c.mnReproject);
+    d.get("MN_MIXED_PRECISION", c.mnMixed);
+    d.get("MN_MIXED_COND_BF16", c.mnMixedCondBf16);
+    d.get("MN_MIXED_COND_MAX", c.mnMixedCondMax);
+    d.get("MN_MIXED_ITER_MAX", c.mnMixedIterMax);
     d.get("SIGMA_CHECKER_BLOCK", c.checkerBlock);
     d.get("SIGMA_S_HI", c.sigmaSHi);
     d.get("SIGMA_A_HI", c.sigmaAHi);
@@ -276,6 +280,10 @@ c3d_status Solver::init(const Config &cfg, void *stream)
                 return s;
         }
     }
+    if (cfg_.solver == "mn" && cfg_.mnMixed &&
+        (s = c3d_set_precision(ctx_, 1, cfg_.mnMixedCondBf16, cfg_.mnMixedCondMax,
+                               cfg_.mnMixedIterMax)) != C3D_OK)
+        return s;
     if (cfg_.outputTimings && (s = c3d_timing_enable(ctx_, 1)) != C3D_OK)
         return s;
     if (cfg_.outputOptStats && cfg_.solver == "mn") {

@@ -15,6 +15,9 @@
 //                              sigma_t = sigma_s + sigma_a.
 //   MN_REPROJECT true        after each closure set u = <m e^{alpha.m}> keeping u_0 (the
 //                              robustness note of the reference's readme.txt)
+//   MN_MIXED_PRECISION true  mixed-precision closure (c3d_set_precision mode 1; needs
+//                              MN_USE_GAUNT_COEF true and N <= 6), thresholds
+//                              MN_MIXED_COND_BF16, MN_MIXED_COND_MAX, MN_MIXED_ITER_MAX
 #pragma once
 #include "../../include/c3d_b200.h"
 #include "deck.h"
@@ -40,6 +43,9 @@ struct Config {
     int mnMaxIter = 0;
     bool mnBatched = true, mnUseGaunt = false, mnUseGauntSparse = false;
     bool mnReproject = false; // optional MN_REPROJECT (readme.txt robustness note)
+    bool mnMixed = false;     // optional MN_MIXED_PRECISION
+    double mnMixedCondBf16 = 0.0, mnMixedCondMax = 0.0;
+    int mnMixedIterMax = 0;
     // optional keys
     int nsteps = -1;
     std::vector<double> ladder{0.0, 1e-3, 1e-2, 1e-1, 5e-1};

@@ -115,6 +115,10 @@ typedef struct {
                                   C3D_NEWTON_CLOCKS only: state load + H assembly, g/f/norms,
                                   Cholesky, condition estimate, direction solve, after_hessian in
                                   total, state store, line-search trial updates */
+    long long hessBf16;        /* mixed precision (c3d_set_precision): Hessian visits with BF16 */
+    long long hessTf32x3;      /*   ... with 3xTF32 split products */
+    long long hessFp64;        /*   ... with FP64 moments */
+    long long escalated;       /*   reduced-precision visits redone in FP64 */
 } c3d_closure_stats;
 
 /* Creates a context on the current CUDA device with the tables M[nq*nm],
@@ -192,6 +196,20 @@ c3d_status c3d_set_gaunt(c3d_ctx *ctx, int nm2, const double *M2, const int *row
  * blocking of the Cholesky factorisation and of the triangular solves (engine 0: 8x8 tiles
  * with tensor-core trailing updates), so results agree to rounding. */
 c3d_status c3d_set_engine(c3d_ctx *ctx, int engine);
+
+/* Precision of the closure (work-list engine, Gaunt form; no counterpart in the reference).
+ * mode 0 (default): FP64 throughout, the drop-in. mode 1: mixed -- an inexact Newton whose
+ * Hessian's extended moments run on the tensor cores in BF16 (cell's last condition
+ * estimate <= condBf16, default 1e4) or as 3xTF32 split products (<= condMixedMax, default
+ * 1e7, and for a cell's first Hessian without a record), with FP32 accumulation and a
+ * per-cell exponent shift of e^{alpha.m}; beyond, after mixedIterMax (default 8) iterations at
+ * one regularisation level, and for the rest of the closure once a reduced-precision
+ * factorisation fails or its moments are not finite, the cell's Hessian is FP64. The
+ * gradient of the stopping test, the objective of the line search and the factorisation stay
+ * FP64, so converged cells satisfy the same residual test as in mode 0; iteration counts
+ * and multipliers differ within the tolerance. Values <= 0 select the defaults. */
+c3d_status c3d_set_precision(c3d_ctx *ctx, int mode, double condBf16, double condMixedMax,
+                             int mixedIterMax);
 
 /* Face-ghost mirroring of the grid closure (engine 0; on by default). The reference solves
  * every cell, ghosts included (src/update.cpp:51-53, 119-123). A face ghost holds a copy of

@@ -1,0 +1,166 @@
+"""Mixed-precision closure (c3d_set_precision mode 1) against the FP64 closure.
+
+The mixed closure computes the Hessian's extended moments on the tensor cores (BF16, or
+3xTF32 split products, FP32 accumulation) and keeps the gradient, the objective, the
+factorisation and the stopping test in FP64. Every converged cell therefore satisfies the
+FP64 residual test |<m e^{alpha.m}> - u| / u_0 <= MN_TOL -- checked here in numpy from the
+returned multipliers and moments -- while iteration counts and multipliers may differ from
+the FP64 closure within what that tolerance allows.
+
+Cells: the 64^3 version of the M_6 benchmark workload (49 moments, 1568 directions, gaussian
+pulse of width 0.02 over a 1e-10 floor) advanced three steps by the FP64 solver; the
+multi-iteration cells of its last closure plus a random sample are solved again from the
+same moments and warm starts by both closures.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import c3d
+from oracle_lib import deck_text
+from test_gpu_kernels import _gaunt_csr
+
+pytestmark = pytest.mark.gpu
+
+LADDER = [0.0, 1e-8, 1e-6, 1e-4, 1e-2, 1e-1]
+TOL = 1e-6
+
+
+def _deck(tmp_path, n, mixed, steps=None, name="input.deck"):
+    kw = dict(NX=n, NY=n, NZ=n, MOMENT_ORDER=6, QUAD_ORDER=28, CFL_FACTOR=0.5, CROSS_SECTION=1.0,
+              INIT_FLOOR=1e-10, GAUSS_SIGMA=0.02, INIT_COND="gaussian_psi", THETA=2.0, MN_TOL=TOL,
+              MN_BATCHED="true", MN_USE_GAUNT_COEF="true", MN_USE_GAUNT_SPARSE="true",
+              REG_LADDER=",".join(str(x) for x in LADDER), OMP_THREADS=os.cpu_count() or 1)
+    if mixed:
+        kw["MN_MIXED_PRECISION"] = "true"
+    p = tmp_path / name
+    p.write_text(deck_text(**kw))
+    return str(p)
+
+
+@pytest.fixture(scope="module")
+def m6_cells(oracle, tmp_path_factory):
+    s = c3d.Solver(_deck(tmp_path_factory.mktemp("m6"), 64, False))
+    for _ in range(3):
+        s.update(s.max_dt)
+    s.sync()
+    s.pull()
+    nm = s.nm
+    A = s.arrays()
+    u = A["u"].reshape(-1, nm).copy()
+    a = A["alpha"].reshape(-1, nm).copy()
+    it = s.records()["iters"]
+    s.close()
+    multi = np.nonzero(it >= 2)[0]
+    rng = np.random.default_rng(5)
+    pick = np.concatenate([multi[:3000], rng.choice(len(it), 2000, replace=False)])
+    T = oracle.tables(6, 28, gaunt=True)
+    return dict(u=u[pick], a=a[pick], T=T, nm=nm, nmulti=len(multi))
+
+
+def _solve(S, mode, cond_bf16=0.0, cond_max=0.0):
+    import torch
+    T, nm = S["T"], S["nm"]
+    n = len(S["u"])
+    ctx = c3d.Context(nx=1, ny=1, nz=1, nm=nm, nq=T["nq"], dx=1.0, dy=1.0, dz=1.0, M=T["M"],
+                      w=T["w"], xi=T["xi"], eta=T["eta"], mu=T["mu"], ladder=LADDER, tol=TOL)
+    row, col, val = _gaunt_csr(T, 1e-13)
+    ctx.set_gaunt(T["nm2"], T["M2"], row, col, val)
+    ctx.set_precision(mode, cond_bf16, cond_max)
+    du = torch.tensor(S["u"], device="cuda")
+    da = torch.tensor(S["a"], device="cuda")
+    it = torch.zeros(n, dtype=torch.int32, device="cuda")
+    rg = torch.zeros(n, dtype=torch.int32, device="cuda")
+    st = torch.zeros(n, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    ctx.reset_stats()
+    ctx.closure_vectors_device(n, du.data_ptr(), da.data_ptr(), it.data_ptr(), None,
+                               rg.data_ptr(), st.data_ptr())
+    ctx.sync()
+    stats = _d(ctx.stats())
+    ctx.close()
+    return dict(u=du.cpu().numpy(), a=da.cpu().numpy(), it=it.cpu().numpy(), rg=rg.cpu().numpy(),
+                st=st.cpu().numpy(), stats=stats)
+
+
+def _d(stats):
+    return {k: getattr(stats, k) for k, t in stats._fields_ if not hasattr(t, "_length_")}
+
+
+def _residual(T, u, a):
+    """|<m e^{alpha.m}> - u|_2 / u_0 per cell (the scaled problem's stopping-test norm)."""
+    M = T["M"].reshape(T["nq"], -1)
+    mom = (np.exp(a @ M.T) * T["w"]) @ M
+    return np.linalg.norm(mom - u, axis=1) / u[:, 0]
+
+
+def test_mixed_closure_meets_fp64_residual(m6_cells):
+    S = m6_cells
+    f = _solve(S, 0)
+    m = _solve(S, 1)
+    assert (f["st"] == 0).all() and (m["st"] == 0).all()
+    assert S["nmulti"] > 100
+    # equal residual: both closures stop on the same FP64 test
+    rf = _residual(S["T"], f["u"], f["a"])
+    rm = _residual(S["T"], m["u"], m["a"])
+    assert rf.max() <= TOL * 1.001, rf.max()
+    assert rm.max() <= TOL * 1.001, rm.max()
+    # the same regularisation almost everywhere
+    same_reg = (f["rg"] == m["rg"]).mean()
+    assert same_reg >= 0.99, same_reg
+    ok = f["rg"] == m["rg"]
+    rel = np.linalg.norm(m["a"][ok] - f["a"][ok], axis=1) / np.linalg.norm(f["a"][ok], axis=1)
+    assert np.median(rel) < 1e-6, np.median(rel)
+    # the tensor-core levels carry the Hessians; iterations stay comparable
+    st = m["stats"]
+    assert st["hessBf16"] + st["hessTf32x3"] > 0.5 * st["totalIters"], st
+    assert m["it"].mean() <= 1.5 * f["it"].mean(), (m["it"].mean(), f["it"].mean())
+    print(f"\nmixed vs FP64 on {len(rel)} cells: alpha rel diff median {np.median(rel):.2e} "
+          f"max {rel.max():.2e}; iterations {m['it'].mean():.3f} vs {f['it'].mean():.3f}; "
+          f"Hessians BF16 {st['hessBf16']} 3xTF32 {st['hessTf32x3']} FP64 {st['hessFp64']} "
+          f"escalated {st['escalated']}")
+
+
+@pytest.mark.parametrize("levels", ["bf16", "fp64"])
+def test_mixed_precision_routing(m6_cells, levels):
+    """Thresholds route the Hessians: with no condition bound every Hessian after the
+    first (3xTF32, no record yet) is BF16 unless a factorisation fails; with zero bounds
+    they are FP64. Either way every cell meets the FP64 residual."""
+    S = m6_cells
+    if levels == "bf16":
+        m = _solve(S, 1, 1e300, 1e300)
+    else:
+        m = _solve(S, 1, 1e-300, 1e-300)
+    st = m["stats"]
+    assert (m["st"] == 0).all()
+    assert _residual(S["T"], m["u"], m["a"]).max() <= TOL * 1.001
+    n = len(S["u"])
+    assert st["hessTf32x3"] >= n  # first visits
+    if levels == "bf16":
+        assert st["hessBf16"] > 0
+    else:
+        assert st["hessBf16"] == 0 and st["hessFp64"] > 0
+
+
+def test_mixed_grid_steps_track_fp64(tmp_path):
+    """Five steps of the 32^3 M_6 deck with the mixed and the FP64 closure: no failed cell,
+    and the moments stay close (the multipliers differ within the Newton tolerance, which
+    enters the fluxes)."""
+    out = {}
+    for mixed in (False, True):
+        s = c3d.Solver(_deck(tmp_path, 32, mixed, name=f"d{int(mixed)}.deck"))
+        for _ in range(5):
+            s.update(s.max_dt)
+        s.sync()
+        s.pull()
+        st = _d(s.stats())
+        out[mixed] = (s.arrays()["u"].copy(), st)
+        s.close()
+    uf, sf = out[False]
+    um, sm = out[True]
+    assert sf["failed"] == 0 and sm["failed"] == 0
+    assert sm["hessBf16"] + sm["hessTf32x3"] > 0
+    rel = np.linalg.norm(um - uf) / np.linalg.norm(uf)
+    print(f"\n32^3 M_6, 5 steps: moments rel L2 mixed vs FP64 {rel:.2e}")
+    assert rel < 1e-6, rel
