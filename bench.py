@@ -8,11 +8,18 @@ interior cell in one stage, so a step on an n^3 grid is 2 n^3 cell-solves.
 
 Default workload (one GPU): M_6 (49 moments) on a 128^3 periodic grid, 1568-point
 quadrature (28 mu x 56 phi), isotropic gaussian pulse of width 0.02 with floor
-1e-10, sigma_s = 1, sigma_a = 0, SSP-RK2 at CFL 0.5, MN_TOL 1e-8 (batched rules),
+1e-10, sigma_s = 1, sigma_a = 0, SSP-RK2 at CFL 0.5, MN_TOL 1e-6 (batched rules),
 ladder {0, 1e-8, 1e-6, 1e-4, 1e-2, 1e-1}. Synthetic input generated from the deck.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                    [--config c1|c2|c3]
+                    [--config c1|c2|c3] [--precision mixed|fp64] [--no-compare]
+
+The reported arm runs the closure in the configuration's mixed precision (the Gaunt
+moments on the tensor cores in BF16 / 3xTF32, everything that decides convergence in
+FP64) unless --precision fp64 selects the plain FP64 drop-in. Both arms are timed from
+the same start state in every run (precision_compare: throughputs, their ratio, and the
+moments' and multipliers' relative L2 difference after the timed steps); both stop on the
+same FP64 residual test.
 
 --gpus N > 1 runs under torchrun: N independent replicas (weak scaling), one per
 GPU; time is the max over ranks. --impl reference times the reference's own CPU
@@ -141,6 +148,21 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------ FLOP model
+def closure_flops_mixed(nm, nq, st):
+    """The mixed closure's work: FP64 FLOPs (per Hessian visit the exponent 2 nm nq, nq exps,
+    the FP64 moments 2 nm nq and Cholesky nm^3/3 -- FP64-moment visits also the extended
+    moments 2 nm2 nq; per line-search trial 2 nm nq + 2 nq) and the reduced-precision
+    tensor-core FLOPs (2 nm2p nq per BF16 visit, 3x that per 3xTF32 visit)."""
+    N = int(round(nm ** 0.5)) - 1
+    nm2 = (2 * N + 1) ** 2
+    nm2p = 8 * ((nm2 + 7) // 8)
+    visits = st.totalIters + st.escalated
+    fp64 = (visits * (4 * nm * nq + nq + nm ** 3 / 3.0) + st.hessFp64 * 2 * nm2 * nq
+            + st.trials * (2 * nm * nq + 2 * nq))
+    low = 2 * nm2p * nq * (st.hessBf16 + 3 * st.hessTf32x3)
+    return fp64, low
+
+
 def closure_flops(nm, nq, iters, trials, hessian="gaunt"):
     """Algorithmic FP64 FLOPs of the dual solves. Per Newton iteration: the exponent
     2 nm nq and nq exps (counted 1 FLOP each), the Hessian -- direct form: lower triangle
@@ -349,53 +371,91 @@ def b200_arm(args):
         elif st_ != 0:
             c3d.check(st_, "sync")
 
-    # warm-up
-    for _ in range(args.warmup):
-        solver.update(dt)
-    sync_count()
-
-    peak = fp64_peak_tflops() if rank == 0 else None
-
-    # timed region: K device-resident steps
-    L.c3d_closure_stats_reset(ctxh)
-    L.c3d_timing_enable(ctxh, 1)
-    launches0 = L.c3d_launch_count(ctxh)
-    clocks = ClockSampler(local)
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    clocks.start()
-    time.sleep(0.3)
-    evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
-    evs[0].record(stream)
-    for k in range(args.steps):
-        solver.update(dt)
-        evs[k + 1].record(stream)
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    clk = clocks.stop()
-    launches = L.c3d_launch_count(ctxh) - launches0
-    sync_count()
-    step_ms = [evs[k].elapsed_time(evs[k + 1]) for k in range(args.steps)]
-    total_ms = evs[0].elapsed_time(evs[-1])
-    ms = np.zeros(2)
-    cnt = (ctypes.c_longlong * 2)()
-    L.c3d_timing_get(ctxh, ms.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), cnt)
-    L.c3d_timing_enable(ctxh, 0)
-    st = solver.stats()
-    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    max_ms = float(t.item())
-    cells = interior_cells(cfg)
-    value = world * cells * 2 * args.steps / (max_ms * 1e-3)
-
-    # end-to-end: host buffers through the C ABI, copies inside the timed region
     nv = solver.nall * nm
     hu = torch.empty(nv, dtype=torch.float64).pin_memory()
     ha = torch.empty(nv, dtype=torch.float64).pin_memory()
-    L.c3d_get_state(ctxh, ctypes.c_void_p(hu.data_ptr()), ctypes.c_void_p(ha.data_ptr()), 0)
+    precision = 1 if args.precision == "mixed" else 0
+
+    def set_precision(mode):
+        c3d.check(L.c3d_set_precision(ctxh, mode, 0.0, 0.0, 0), "precision")
+
+    def save_state(u_, a_):
+        c3d.check(L.c3d_get_state(ctxh, ctypes.c_void_p(u_.data_ptr()),
+                                  ctypes.c_void_p(a_.data_ptr()), 0), "get_state")
+
+    def load_state(u_, a_):
+        c3d.check(L.c3d_set_state(ctxh, ctypes.c_void_p(u_.data_ptr()),
+                                  ctypes.c_void_p(a_.data_ptr()), None, None, 0), "set_state")
+
+    # warm-up (FP64), then the start state S of both timed arms
+    set_precision(0)
+    for _ in range(args.warmup):
+        solver.update(dt)
+    sync_count()
+    u_s = torch.empty(nv, dtype=torch.float64).pin_memory()
+    a_s = torch.empty(nv, dtype=torch.float64).pin_memory()
+    save_state(u_s, a_s)
+    if precision == 1:
+        # the mixed kernels' first launches, from S (untimed)
+        set_precision(1)
+        for _ in range(args.warmup):
+            solver.update(dt)
+        sync_count()
+
+    peak = fp64_peak_tflops() if rank == 0 else None
+
+    def timed(mode, sample_clocks):
+        """K device-resident steps from S with the given closure precision."""
+        set_precision(mode)
+        load_state(u_s, a_s)
+        L.c3d_closure_stats_reset(ctxh)
+        L.c3d_timing_enable(ctxh, 1)
+        launches0 = L.c3d_launch_count(ctxh)
+        clocks = ClockSampler(local) if sample_clocks else None
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        if clocks:
+            clocks.start()
+            time.sleep(0.3)
+        evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+        evs[0].record(stream)
+        for k in range(args.steps):
+            solver.update(dt)
+            evs[k + 1].record(stream)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        clk = clocks.stop() if clocks else None
+        launches = L.c3d_launch_count(ctxh) - launches0
+        sync_count()
+        step_ms = [evs[k].elapsed_time(evs[k + 1]) for k in range(args.steps)]
+        total_ms = evs[0].elapsed_time(evs[-1])
+        ms = np.zeros(2)
+        cnt = (ctypes.c_longlong * 2)()
+        L.c3d_timing_get(ctxh, ms.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), cnt)
+        L.c3d_timing_enable(ctxh, 0)
+        st = solver.stats()
+        t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        uo = torch.empty(nv, dtype=torch.float64)
+        ao = torch.empty(nv, dtype=torch.float64)
+        save_state(uo, ao)
+        torch.cuda.synchronize()
+        return dict(max_ms=float(t.item()), step_ms=step_ms, ms=ms, cnt=cnt, launches=launches,
+                    clk=clk, st=st, u=uo.numpy(), a=ao.numpy())
+
+    cells = interior_cells(cfg)
+    other = timed(1 - precision, False) if args.compare else None
+    head = timed(precision, True)
+    max_ms, step_ms, ms, cnt = head["max_ms"], head["step_ms"], head["ms"], head["cnt"]
+    launches, clk, st = head["launches"], head["clk"], head["st"]
+    total_ms = max_ms
+    value = world * cells * 2 * args.steps / (max_ms * 1e-3)
+
+    # end-to-end: host buffers through the C ABI, copies inside the timed region
+    save_state(hu, ha)
     e_steps = max(1, min(args.steps, 3))
     torch.cuda.synchronize()
     if world > 1:
@@ -404,11 +464,9 @@ def b200_arm(args):
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(e_steps):
-        c3d.check(L.c3d_set_state(ctxh, ctypes.c_void_p(hu.data_ptr()),
-                                  ctypes.c_void_p(ha.data_ptr()), None, None, 0), "set_state")
+        load_state(hu, ha)
         solver.update(dt)
-        c3d.check(L.c3d_get_state(ctxh, ctypes.c_void_p(hu.data_ptr()),
-                                  ctypes.c_void_p(ha.data_ptr()), 0), "get_state")
+        save_state(hu, ha)
     e1.record(stream)
     torch.cuda.synchronize()
     sync_count()
@@ -419,10 +477,18 @@ def b200_arm(args):
 
     if rank == 0:
         closure_launches = int(cnt[0])
-        flops = closure_flops(nm, nq, st.totalIters, st.trials, args.hessian)
+        low = None
+        if precision == 1:
+            flops, low = closure_flops_mixed(nm, nq, st)
+        else:
+            flops = closure_flops(nm, nq, st.totalIters, st.trials, args.hessian)
         per_launch_s = ms[0] * 1e-3 / max(1, closure_launches)
         achieved = flops / max(1, closure_launches) / per_launch_s / 1e12
-        roofline = dict(bound="tensor", pipe="fp64 (DMMA m8n8k4 + DFMA)", achieved=achieved,
+        roofline = dict(bound="tensor",
+                        pipe=("fp64 (DMMA m8n8k4 + DFMA); the mixed closure's BF16 / 3xTF32 "
+                              "moments run on tcgen05 beside it (lowp_tflops)" if precision == 1
+                              else "fp64 (DMMA m8n8k4 + DFMA)"),
+                        achieved=achieved,
                         peak=peak, unit="TFLOP/s", frac=achieved / peak if peak else None,
                         traffic=(profile_traffic("closure_rounds_m6_64")
                                  if args.engine == "rounds" and args.hessian == "gaunt" else None),
@@ -441,6 +507,37 @@ def b200_arm(args):
                         closure_ms_per_launch=ms[0] / max(1, closure_launches),
                         flux_ms_per_launch=ms[1] / max(1, int(cnt[1])),
                         closure_share_of_step=ms[0] / total_ms)
+        if low is not None:
+            roofline["lowp_tflops"] = low / max(1, closure_launches) / per_launch_s / 1e12
+            roofline["kernel"] = ("closure work-list rounds: rounds_pass_mixed_kernel<7,22,0|1> "
+                                  "(tcgen05) + rounds_pass_gaunt_kernel<7,22> (trials, FP64 "
+                                  "Hessians) + rounds_newton_kernel")
+            roofline["traffic"] = None
+        compare = None
+        if other is not None:
+            fp, mx = (other, head) if precision == 1 else (head, other)
+            vf = world * cells * 2 * args.steps / (fp["max_ms"] * 1e-3)
+            vm = world * cells * 2 * args.steps / (mx["max_ms"] * 1e-3)
+            du = np.linalg.norm(mx["u"] - fp["u"]) / np.linalg.norm(fp["u"])
+            da = np.linalg.norm(mx["a"] - fp["a"]) / np.linalg.norm(fp["a"])
+            sm = mx["st"]
+            compare = dict(
+                fp64=dict(value=vf, ms_per_step=fp["max_ms"] / args.steps,
+                          closure_ms_per_launch=fp["ms"][0] / max(1, int(fp["cnt"][0])),
+                          newton_iters_per_solve=fp["st"].totalIters / max(1, fp["st"].cells),
+                          failed_cells=int(fp["st"].failed)),
+                mixed=dict(value=vm, ms_per_step=mx["max_ms"] / args.steps,
+                           closure_ms_per_launch=mx["ms"][0] / max(1, int(mx["cnt"][0])),
+                           newton_iters_per_solve=sm.totalIters / max(1, sm.cells),
+                           failed_cells=int(sm.failed),
+                           hessians=dict(bf16=int(sm.hessBf16), tf32x3=int(sm.hessTf32x3),
+                                         fp64=int(sm.hessFp64), redone_fp64=int(sm.escalated))),
+                mixed_over_fp64=vm / vf,
+                residual="equal: both closures stop on the FP64 test |<m e^{alpha.m}> - u| <= "
+                         "MN_TOL with gamma <= MN_TOL_GAMMA",
+                moments_rel_l2=du, alpha_rel_l2=da,
+                accuracy_note=f"u and alpha after the {args.steps} timed steps from the same "
+                              "start state, mixed vs FP64 (all cells incl. ghosts)")
         # the kinetic flux, second in the step: HBM view of the materialised-psi variant and
         # its tensor-pipe work (exponents and projection)
         nall_c = solver.nall
@@ -476,15 +573,20 @@ def b200_arm(args):
         line = dict(
             metric=METRIC, value=value, unit=UNIT, n_gpus=world, steps=args.steps,
             warmup=args.warmup, ms_per_step=max_ms / args.steps, higher_is_better=True,
-            scaling="weak", vs_baseline=None, dtype="f64", data="synthetic",
-            config=dict(workload=c["desc"], config=cfg, form="plain FP64 drop-in",
+            scaling="weak", vs_baseline=None,
+            dtype="f64 + bf16/tf32 (tcgen05, FP32 accumulate)" if precision == 1 else "f64",
+            data="synthetic",
+            config=dict(workload=c["desc"], config=cfg,
+                        form=("mixed precision: Gaunt moments BF16 / 3xTF32 on tcgen05 with "
+                              "FP32 accumulation, FP64 gradient, objective, factorisation and "
+                              "fallback" if precision == 1 else "plain FP64 drop-in"),
                         hessian=("Gaunt sparse (MN_USE_GAUNT_COEF/SPARSE true, the reference "
                                  "deck's default)" if args.hessian == "gaunt" else "direct"),
                         engine=args.engine,
                         mn_tol=MN_TOL, mn_batched=True, ladder=LADDER,
                         cells_per_step=2 * cells, l2="inputs larger than L2 (u, alpha 0.9 GB each)",
                         parallelism=f"replicas x{world}"),
-            roofline=roofline, flux=flux_line, cpu_baseline=cpu,
+            roofline=roofline, flux=flux_line, cpu_baseline=cpu, precision_compare=compare,
             e2e=dict(value=e2e_value, unit=UNIT, h2d_bytes_per_step=2 * nv * 8,
                      d2h_bytes_per_step=2 * nv * 8, steps=e_steps),
             gpu_launches=int(launches), clocks=clk,
@@ -510,7 +612,17 @@ def main():
     ap.add_argument("--config", default="c3", choices=sorted(CONFIGS))
     ap.add_argument("--hessian", default="gaunt", choices=["gaunt", "direct"])
     ap.add_argument("--engine", default="rounds", choices=["rounds", "persistent"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
+                    help="closure precision of the reported arm (mixed: the configuration's "
+                         "form; fp64: the drop-in)")
+    ap.add_argument("--no-compare", dest="compare", action="store_false",
+                    help="skip the other precision's arm")
+    ap.set_defaults(compare=True)
     args = ap.parse_args()
+    if args.engine != "rounds" or args.hessian != "gaunt":
+        # the mixed closure is built on the work-list engine's Gaunt form
+        args.precision = "fp64"
+        args.compare = False
     if args.impl == "reference":
         reference_arm(args)
     else:

@@ -46,6 +46,7 @@ HEADER_SYMBOLS = [
     "c3d_set_gaunt", "c3d_set_engine", "c3d_set_ghost_mirroring", "c3d_timing_events",
     "c3d_closure_records_fp", "c3d_line_stats_enable", "c3d_line_stats_get", "c3d_stage",
     "c3d_set_x_halo_external", "c3d_copy_x_planes", "c3d_set_precision",
+    "c3d_set_certificate",
 ]
 
 
@@ -76,7 +77,7 @@ class ClosureStats(ctypes.Structure):
                 ("iterHist", ctypes.c_longlong * 64),
                 ("clkNewton", ctypes.c_longlong * 8), ("hessBf16", ctypes.c_longlong),
                 ("hessTf32x3", ctypes.c_longlong), ("hessFp64", ctypes.c_longlong),
-                ("escalated", ctypes.c_longlong)]
+                ("escalated", ctypes.c_longlong), ("certified", ctypes.c_longlong)]
 
 
 _lib = None
@@ -115,6 +116,7 @@ def lib():
         L.c3d_set_engine.argtypes = [vp, ctypes.c_int]
         L.c3d_set_precision.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                         ctypes.c_int]
+        L.c3d_set_certificate.argtypes = [vp, ctypes.c_int]
         L.c3d_set_ghost_mirroring.argtypes = [vp, ctypes.c_int]
         L.c3d_timing_enable.argtypes = [vp, ctypes.c_int]
         L.c3d_timing_get.argtypes = [vp, _dp, ctypes.POINTER(ctypes.c_longlong)]
@@ -306,6 +308,11 @@ class Context:
         (1e4, 1e7, 8)."""
         check(lib().c3d_set_precision(self.h, int(mode), float(cond_bf16), float(cond_mixed_max),
                                       int(mixed_iter_max)), "c3d_set_precision")
+
+    def set_certificate(self, on):
+        """First-visit convergence certificate (default on): exact; off gives gamma records
+        of the full iteration."""
+        check(lib().c3d_set_certificate(self.h, int(bool(on))), "c3d_set_certificate")
 
     def set_ghost_mirroring(self, on):
         check(lib().c3d_set_ghost_mirroring(self.h, int(bool(on))), "c3d_set_ghost_mirroring")

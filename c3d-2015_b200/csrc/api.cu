@@ -3,6 +3,7 @@
 #include "c3d_common.cuh"
 #include "rounds_launch.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -172,6 +173,12 @@ struct c3d_ctx {
     double *mixF64 = nullptr;
     unsigned char *mixA[2] = {nullptr, nullptr};
     float *cellCond = nullptr;
+    // convergence certificate of first visits (c3d_set_certificate): the Gaunt terms of H's
+    // column 0 (g0n per row) for the FP64 gradient, and whether they lie in the probe's rows
+    GauntTerm *g0 = nullptr;
+    int g0n = 0;
+    bool g0Valid = false;
+    bool certificate = true;
     // optional event timing of the closure and flux launches (kind 0 closure, 1 flux)
     bool timing = false;
     std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> events;
@@ -211,7 +218,7 @@ static void free_ctx(c3d_ctx *c)
                     c->gRow, c->gCol, c->gStream, c->rState, c->rListA, c->rListB,
                     c->rCounts, c->rBuf, c->mfA, c->mfP, c->cellMap, c->mirrorFlag,
                     c->gChunksC, c->cellGamma, c->cellErr, c->lineLog, c->mixF64,
-                    c->mixA[0], c->mixA[1], c->cellCond};
+                    c->mixA[0], c->mixA[1], c->cellCond, c->g0};
     for (void *p : ptrs)
         if (p)
             cudaFree(p);
@@ -460,8 +467,8 @@ static c3d_status ensure_rounds(c3d_ctx *c, long long n)
     c->rCells = c->rBatch = 0;
     C3D_CUDA(cudaMalloc(&c->rState, (size_t)n * rounds_state_bytes(c->g.nm)));
     // one list per precision level (the FP64 closure uses the first)
-    C3D_CUDA(cudaMalloc(&c->rListA, 3 * (size_t)n * sizeof(int)));
-    C3D_CUDA(cudaMalloc(&c->rListB, 3 * (size_t)n * sizeof(int)));
+    C3D_CUDA(cudaMalloc(&c->rListA, 4 * (size_t)n * sizeof(int)));
+    C3D_CUDA(cudaMalloc(&c->rListB, 4 * (size_t)n * sizeof(int)));
     C3D_CUDA(cudaMalloc(&c->rCounts, 8 * sizeof(unsigned int)));
     C3D_CUDA(cudaMalloc(&c->rBuf, (size_t)batch * per * sizeof(double)));
     if (!c->rHostCount)
@@ -507,6 +514,11 @@ static c3d_status run_closure(c3d_ctx *c, long long n, double *u, double *alpha,
         R.mixF64 = c->mixF64;
         R.mixA[0] = c->mixA[0];
         R.mixA[1] = c->mixA[1];
+        R.g0 = c->g0;
+        R.g0n = c->g0n;
+        // the certificate's gamma record is a bound: off while the x-line log records gammas
+        c->cp.probe = c->gaunt && c->certificate && c->lineCap == 0 &&
+                      (c->cp.mixed || c->g0Valid) && c->cp.gramLo > 0.0;
         R.state = c->rState;
         R.listA = c->rListA;
         R.listB = c->rListB;
@@ -524,6 +536,7 @@ static c3d_status run_closure(c3d_ctx *c, long long n, double *u, double *alpha,
         C3D_CUDA(e);
         return C3D_OK;
     }
+    c->cp.probe = 0; // the persistent kernels always form H
     ClosureLaunch L{};
     L.P = &c->cp;
     L.chunks = c->chunks;
@@ -714,6 +727,58 @@ static c3d_status build_mixed_chunks(c3d_ctx *c, int nm2, const double *M2,
     return C3D_OK;
 }
 
+// Tables of the first-visit convergence certificate: the Gaunt terms of H's column 0 (CSR
+// row i of element (i, 0), in order; rows padded to the longest with col -2) -- valid when
+// they reference only moments of the probe's rows (< nm) -- and the Gershgorin bounds of the
+// quadrature's Gram matrix G = sum_q w_q m_q m_q^T (the first nm rows of M2 are the basis).
+static c3d_status build_certificate(c3d_ctx *c, int nm2, const double *M2,
+                                    const std::vector<double> &wh, const int *rowPtr,
+                                    const int *colInd, const double *val)
+{
+    const int nm = c->g.nm, nq = c->nq;
+    int g0n = 1;
+    bool valid = true;
+    for (int i = 0; i < nm; ++i) {
+        g0n = std::max(g0n, rowPtr[i + 1] - rowPtr[i]);
+        for (int k = rowPtr[i]; k < rowPtr[i + 1]; ++k)
+            valid = valid && colInd[k] >= 0 && colInd[k] < nm;
+    }
+    std::vector<GauntTerm> t((size_t)nm * g0n, GauntTerm{0.0, -2, -1});
+    for (int i = 0; i < nm; ++i)
+        for (int k = rowPtr[i]; k < rowPtr[i + 1]; ++k)
+            t[(size_t)i * g0n + (k - rowPtr[i])] = GauntTerm{val[k], colInd[k], -1};
+    std::vector<double> G((size_t)nm * nm, 0.0);
+    for (int q = 0; q < nq; ++q)
+        for (int i = 0; i < nm; ++i)
+            for (int j = 0; j < nm; ++j)
+                G[(size_t)i * nm + j] += wh[q] * M2[(size_t)q * nm2 + i] * M2[(size_t)q * nm2 + j];
+    double lo = 1.0 / 0.0, hi = 0.0;
+    for (int i = 0; i < nm; ++i) {
+        double off = 0.0;
+        for (int j = 0; j < nm; ++j)
+            if (j != i)
+                off += std::fabs(G[(size_t)i * nm + j]);
+        lo = std::min(lo, G[(size_t)i * nm + i] - off);
+        hi = std::max(hi, G[(size_t)i * nm + i] + off);
+    }
+    // rounding of the host sums: a relative margin far above nq eps
+    lo *= 1.0 - 1e-9;
+    hi *= 1.0 + 1e-9;
+    GauntTerm *d = nullptr;
+    if (cudaMalloc(&d, t.size() * sizeof(GauntTerm)) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(C3D_ERR_OOM, "c3d_set_gaunt: device allocation failed");
+    }
+    C3D_CUDA(cudaMemcpy(d, t.data(), t.size() * sizeof(GauntTerm), cudaMemcpyHostToDevice));
+    if (c->g0) cudaFree(c->g0);
+    c->g0 = d;
+    c->g0n = g0n;
+    c->g0Valid = valid;
+    c->cp.gramLo = lo;
+    c->cp.gramHi = hi;
+    return C3D_OK;
+}
+
 c3d_status c3d_set_gaunt(c3d_ctx *c, int nm2, const double *M2, const int *rowPtr,
                          const int *colInd, const double *val)
 {
@@ -852,7 +917,10 @@ c3d_status c3d_set_gaunt(c3d_ctx *c, int nm2, const double *M2, const int *rowPt
     c->gVal = dval;
     c->gaunt = true;
     c->nm2 = nm2;
-    return build_mixed_chunks(c, nm2, M2, wh);
+    c3d_status s = build_mixed_chunks(c, nm2, M2, wh);
+    if (s != C3D_OK)
+        return s;
+    return build_certificate(c, nm2, M2, wh, rowPtr, colInd, val);
 }
 
 c3d_status c3d_set_precision(c3d_ctx *c, int mode, double condBf16, double condMixedMax,
@@ -867,6 +935,14 @@ c3d_status c3d_set_precision(c3d_ctx *c, int mode, double condBf16, double condM
     c->cp.condBf16 = condBf16 > 0 ? condBf16 : 1e4;
     c->cp.condMixMax = condMixedMax > 0 ? condMixedMax : 1e7;
     c->cp.mixIterMax = mixedIterMax > 0 ? mixedIterMax : 8;
+    return C3D_OK;
+}
+
+c3d_status c3d_set_certificate(c3d_ctx *c, int on)
+{
+    if (!c)
+        return fail(C3D_ERR_INVALID, "c3d_set_certificate: null context");
+    c->certificate = on != 0;
     return C3D_OK;
 }
 
@@ -1137,6 +1213,7 @@ c3d_status c3d_closure_stats_get(c3d_ctx *c, c3d_closure_stats *st)
     st->hessTf32x3 = (long long)h[STAT_H_TF32X3];
     st->hessFp64 = (long long)h[STAT_H_FP64];
     st->escalated = (long long)h[STAT_ESCALATED];
+    st->certified = (long long)h[STAT_CERTIFIED];
     return C3D_OK;
 }
 

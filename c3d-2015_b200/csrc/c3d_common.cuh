@@ -31,6 +31,7 @@ enum StatSlot : int {
     STAT_MAX_ITER_GAMMA = 4,
     STAT_FAILED = 5,
     STAT_TRIALS = 6,     // line-search trial passes
+    STAT_CERTIFIED = 7,  // first visits ended by the probe's convergence certificate
     STAT_REG_HIST = 8,   // 16 bins
     STAT_CLK_REFILL = 24, // SM clocks summed over warps: queue refill + cell set-up
     STAT_CLK_PASS = 25,   // passes over the staged basis
@@ -68,6 +69,13 @@ struct ClosureParams {
     int mixIterMax;
     double condBf16;
     double condMixMax;
+    // convergence certificate of a cell's first Hessian visit (work-list engine, Gaunt form):
+    // a probe pass computes the first-order moments and the extreme values of e^{alpha.m}
+    // over the quadrature; H >= e_min G with G = sum_q w_q m_q m_q^T, whose eigenvalues lie
+    // in [gramLo, gramHi] (Gershgorin), bounds the condition estimate and |d| = |H^-1 g|,
+    // so a cell whose visit would end converged is finalized without H (see after_probe)
+    int probe;
+    double gramLo, gramHi;
 };
 
 __host__ __device__ inline int ceil_div(int a, int b) { return (a + b - 1) / b; }

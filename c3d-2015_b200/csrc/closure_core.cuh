@@ -20,7 +20,7 @@ constexpr int GSTAGES = 2; // stages of the (larger) Gaunt chunks
 constexpr int CST = 12;    // row stride of the coefficient tile (bank-conflict-free B fragments)
 constexpr double EPS_HALF = DBL_EPSILON / 2;
 
-enum Need : int { NEED_NONE = 0, NEED_H = 1, NEED_TRIAL = 2 };
+enum Need : int { NEED_NONE = 0, NEED_H = 1, NEED_TRIAL = 2, NEED_PROBE = 3 };
 
 // Phase clocks of the per-cell Newton logic (profiling builds only).
 #ifdef C3D_NEWTON_CLOCKS
@@ -691,7 +691,7 @@ __device__ void begin_iteration(S &sl, const ClosureParams &P, const Outputs &O,
             continue;
         }
         if (lane == 0)
-            sl.s.need = NEED_H;
+            sl.s.need = (P.probe && total == 1) ? NEED_PROBE : NEED_H;
         __syncwarp();
         return;
     }
@@ -967,6 +967,78 @@ __device__ void after_hessian(S &sl, const ClosureParams &P, const Outputs &O, i
     }
     __syncwarp();
     next_trial(sl, P, O, lane);
+}
+
+// First visit of a cell after the probe pass. pm: the probe's entry -- the first-order
+// moments mom_i (i < NMP, rows of M2 = the basis), then f's sum, e_min and e_max of
+// e^{alpha.m_q}. g is formed as the full visit would form it: FP64 closure, from the Gaunt
+// terms of the Hessian's column 0 (g0: g0n terms per row in the reference's CSR order, col
+// -2 padding; H_i0 = sum_t v_t mom_col_t, g_i = H_i0 / m_0 - u_i, src/opt/fobj.cpp:121-129);
+// mixed closure (g0 null), g_i = mom_i - u_i. The full visit ends the cell converged
+// (src/opt/optBatch.cpp:185-250) when info = 0, cond <= condHMax, |g| <= rtol and
+// gamma = exp(2 minf |d|_1) <= tolGamma. With lambda_min(H) >= e_min gramLo and
+// lambda_max(H) <= e_max gramHi (exact arithmetic; halved for rounding): the 1-norm condition
+// estimate is at most nm kappa_2 <= nm e_max gramHi / (e_min gramLo), kept below condHMax / 4
+// (Cholesky of such an H succeeds); |d|_1 <= sqrt(nm) |g|_2 / lambda_min, and the gamma
+// exponent is kept below half of log(tolGamma). A cell meeting these is finalized with the
+// same multipliers, moments and counts as the full visit would give (its gamma record is the
+// bound); any other goes on to the Hessian pass of the same iteration.
+template <class S>
+__device__ void after_probe(S &sl, const ClosureParams &P, const Outputs &O, int lane, double m0,
+                            const double *pm, const GauntTerm *g0, int g0n)
+{
+    const int nm = P.nm;
+    constexpr int NMP = S::NMP;
+    for (int i = lane; i < nm; i += 32) {
+        double gi;
+        if (g0) {
+            double h = 0.0;
+            for (int t = 0; t < g0n; ++t) {
+                const GauntTerm e = g0[i * g0n + t];
+                if (e.col >= 0)
+                    h = __dadd_rn(h, __dmul_rn(pm[e.col], e.v));
+            }
+            gi = h / m0 - sl.u[i];
+        } else {
+            gi = __dsub_rn(pm[i], sl.u[i]);
+        }
+        sl.g[i] = gi;
+    }
+    __syncwarp();
+    const double err = warp_nrm2(sl.g, nm, lane);
+    const double emin = pm[NMP + 1], emax = pm[NMP + 2];
+    int maxIterEff = sl.s.maxIter;
+    if (P.batched && sl.s.regIndex == P.nreg - 1)
+        maxIterEff = 10 * P.maxIter;
+    bool ok = err <= sl.s.rtol && sl.s.iter < maxIterEff && sl.s.t != 0.0 && P.tolGamma > 1.0 &&
+              emin > 0.0 && emax < 1.0 / 0.0 && P.gramLo > 0.0;
+    double k1 = 0.0, gexp = 0.0;
+    if (ok) {
+        const double lam = 0.5 * emin * P.gramLo;
+        k1 = nm * (emax * P.gramHi) / lam;
+        const int pnOrder = (int)floor(sqrt((double)nm)) + 1;
+        const double minf = sqrt((2 * pnOrder + 1) / (2 * M_PI));
+        gexp = 2.0 * minf * sqrt((double)nm) * err / lam;
+        ok = k1 <= 0.25 * P.condHMax && gexp <= 0.5 * log(P.tolGamma);
+    }
+    __syncwarp();
+    if (ok) {
+        if (lane == 0) {
+            sl.s.err = err;
+            sl.s.gamma = exp(gexp);
+            sl.s.cnd = k1;
+            if (O.stats)
+                atomicAdd(&O.stats[STAT_CERTIFIED], 1ull);
+        }
+        __syncwarp();
+        finalize(sl, P, O, lane);
+        return;
+    }
+    if (lane == 0) {
+        sl.s.passes += 1;
+        sl.s.need = NEED_H;
+    }
+    __syncwarp();
 }
 
 template <class S>

@@ -21,6 +21,7 @@
 
 #include <cuda_bf16.h>
 #include <cstdio>
+#include <type_traits>
 
 namespace c3d {
 
@@ -72,8 +73,9 @@ __device__ void slot_to_state(const S &sl, CellState<NT> &st, int lane)
 }
 
 // The work lists of one round: 0 trials and FP64 Hessian passes, 1 BF16 Hessian passes,
-// 2 3xTF32 Hessian passes (lists 1 and 2: mixed-precision closure only).
-constexpr int NLISTS = 3;
+// 2 3xTF32 Hessian passes (lists 1 and 2: mixed-precision closure only), 3 first visits
+// through the probe pass (convergence certificate).
+constexpr int NLISTS = 4;
 struct Lists {
     int *list[NLISTS];
     unsigned int *count[NLISTS];
@@ -85,6 +87,8 @@ struct Lists {
 // reduced-precision factorisation failed) in FP64.
 template <class S> __device__ int route_list(const S &sl, const ClosureParams &P)
 {
+    if (sl.s.need == NEED_PROBE)
+        return 3;
     if (sl.s.need != NEED_H || !P.mixed || sl.s.fp64 || sl.s.iter > P.mixIterMax)
         return 0;
     const double c = sl.s.cnd;
@@ -105,8 +109,11 @@ __device__ void append_if_needed(const S &sl, const ClosureParams &P, long long 
     if (lane == 0 && sl.s.need != NEED_NONE) {
         // selects, not an indexed parameter array (which would be copied to local memory)
         const int l = route_list(sl, P);
-        unsigned int *cnt = l == 0 ? out.count[0] : l == 1 ? out.count[1] : out.count[2];
-        int *lst = l == 0 ? out.list[0] : l == 1 ? out.list[1] : out.list[2];
+        unsigned int *cnt = l == 0   ? out.count[0]
+                            : l == 1 ? out.count[1]
+                            : l == 2 ? out.count[2]
+                                     : out.count[3];
+        int *lst = l == 0 ? out.list[0] : l == 1 ? out.list[1] : l == 2 ? out.list[2] : out.list[3];
         unsigned int pos = atomicAdd(cnt, 1u);
         lst[pos] = (int)c;
     }
@@ -118,6 +125,16 @@ constexpr int RW = 8;  // warps (cells) per CTA of the init and pass kernels
 constexpr int RWN = 4; // warps (cells) per CTA of the Newton kernel
 
 template <int NT> using TSlot = Slot<NT, true>;
+
+// Per-warp state of a first visit after the probe pass: the vectors and scalars of Slot
+// without the factor (the probe's Newton kernel forms no Hessian).
+template <int NT> struct alignas(16) ProbeSlot {
+    static constexpr int NMP = Cfg<NT>::NMP;
+    double u[NMP], alpha[NMP], alpha0[NMP], uOrig[NMP], g[NMP], d[NMP], alphaOld[NMP];
+    SlotScalars s;
+};
+template <int NT, int MODE>
+using NewtonSlot = typename std::conditional<MODE == 2, ProbeSlot<NT>, TSlot<NT>>::type;
 
 template <int NT>
 __global__ void __launch_bounds__(RW * 32)
@@ -133,7 +150,8 @@ __global__ void __launch_bounds__(RW * 32)
     Slot<NT> &sl = slots[warp];
     // the state and work lists use the closure's own numbering c; outputs the grid cell's
     load_cell(sl, P, O, cellMap ? (long long)cellMap[c] : c, lane);
-    slot_to_state(sl, state[c], lane);
+    if (sl.s.need != NEED_NONE)
+        slot_to_state(sl, state[c], lane);
     append_if_needed(sl, P, c, lane, out);
 }
 
@@ -424,6 +442,10 @@ template <> struct MixKind<1> { // 3xTF32
     static constexpr int ES = 4, NP = 2, KI = 8;
     static constexpr uint32_t FMT = 2;
 };
+template <> struct MixKind<2> { // probe: the FP64 part alone
+    static constexpr int ES = 8, NP = 0, KI = 8;
+    static constexpr uint32_t FMT = 0;
+};
 constexpr int MXC = 16;
 
 template <int NT2> struct MixRows {
@@ -435,9 +457,13 @@ template <int NT2> struct MixRows {
 };
 
 __host__ __device__ constexpr int mix_entry_doubles(int nmp, int nm2p) { return nm2p + nmp + 8; }
+// Probe entry (KIND 2): the NMP first-order moments, f's sum, e_min, e_max.
+__host__ __device__ constexpr int probe_entry_doubles(int nmp) { return nmp + 8; }
 
+// KIND 2 is the probe pass of a cell's first visit (the convergence certificate): the FP64
+// part alone, with the extreme values of e^{alpha.m_q} over the chunk's directions.
 template <int NT, int NT2, int KIND>
-__global__ void __launch_bounds__(RW * 32, KIND == 0 ? 2 : 1)
+__global__ void __launch_bounds__(RW * 32, KIND == 1 ? 1 : 2)
     rounds_pass_mixed_kernel(ClosureParams P, const double *__restrict__ f64c,
                              const unsigned char *__restrict__ ac, const int *__restrict__ list,
                              int n, CellState<NT> *state, double *__restrict__ out, int *errorFlag)
@@ -447,7 +473,8 @@ __global__ void __launch_bounds__(RW * 32, KIND == 0 ? 2 : 1)
     constexpr int NMP = 8 * NT;
     constexpr int KG = QC * K::ES / 16, SBO = KG * 128;
     constexpr uint32_t APB = R::NA * QC * K::ES, BPB = MXC * QC * K::ES;
-    constexpr int ESTR = mix_entry_doubles(NMP, R::NM2P);
+    constexpr bool TC = KIND < 2; // tensor-core moments
+    constexpr int ESTR = TC ? mix_entry_doubles(NMP, R::NM2P) : probe_entry_doubles(NMP);
     constexpr uint32_t IDESC = umma_idesc(K::FMT, 128, MXC);
     static_assert(NT <= RW, "one FP64 row tile per warp");
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -496,18 +523,21 @@ __global__ void __launch_bounds__(RW * 32, KIND == 0 ? 2 : 1)
             unsigned char *st = smem_raw + k * stg;
             mbar_expect_tx(&full[k], f64Bytes + K::NP * APB);
             bulk_g2s(st, f64c + (size_t)k * (nm + 1) * QCP, f64Bytes, &full[k]);
-            bulk_g2s(st + f64Pad, ac + (size_t)k * K::NP * APB, K::NP * APB, &full[k]);
+            if constexpr (TC)
+                bulk_g2s(st + f64Pad, ac + (size_t)k * K::NP * APB, K::NP * APB, &full[k]);
         }
     }
-    if (warp == 0)
-        tmem_alloc(&s_tmem, 32);
+    if constexpr (TC)
+        if (warp == 0)
+            tmem_alloc(&s_tmem, 32);
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    const uint32_t tmem = s_tmem;
+    const uint32_t tmem = TC ? s_tmem : 0u;
     const double2 *aw = alph + warp * nm;
     double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
     double fpart0 = 0.0, fpart1 = 0.0, cmax0 = 0.0, cmax1 = 0.0;
+    double emin0 = 1.0 / 0.0, emin1 = 1.0 / 0.0, emax0 = 0.0, emax1 = 0.0;
     for (int k = 0; k < nchunks; ++k) {
         const uint32_t s = k % GSTAGES, parity = (k / GSTAGES) & 1u;
         if (!mbar_wait(&full[s], parity))
@@ -524,18 +554,26 @@ __global__ void __launch_bounds__(RW * 32, KIND == 0 ? 2 : 1)
             z1 = __dadd_rn(z1, __dmul_rn(a.y, m));
         }
         const double wq = ch[nm * QCP + lane];
-        const double c0 = cell[0] >= 0 ? __dmul_rn(wq, exp(z0)) : 0.0;
-        const double c1 = cell[1] >= 0 ? __dmul_rn(wq, exp(z1)) : 0.0;
+        const double ez0 = exp(z0), ez1 = exp(z1);
+        const double c0 = cell[0] >= 0 ? __dmul_rn(wq, ez0) : 0.0;
+        const double c1 = cell[1] >= 0 ? __dmul_rn(wq, ez1) : 0.0;
         fpart0 = __dadd_rn(fpart0, c0);
         fpart1 = __dadd_rn(fpart1, c1);
-        cmax0 = fmax(cmax0, c0);
-        cmax1 = fmax(cmax1, c1);
+        if constexpr (TC) {
+            cmax0 = fmax(cmax0, c0);
+            cmax1 = fmax(cmax1, c1);
+        } else {
+            emin0 = fmin(emin0, ez0);
+            emin1 = fmin(emin1, ez1);
+            emax0 = fmax(emax0, ez0);
+            emax1 = fmax(emax1, ez1);
+        }
         cbuf[lane * CST2 + 2 * warp] = c0;
         cbuf[lane * CST2 + 2 * warp + 1] = c1;
         // B tile: cell row nn, direction column lane
         unsigned char *bt = bbuf + s * K::NP * BPB;
 #pragma unroll
-        for (int e = 0; e < 2; ++e) {
+        for (int e = 0; e < (TC ? 2 : 0); ++e) {
             const int nn = 2 * warp + e;
             const double v = (e == 0 ? c0 : c1) * scale[e];
             const uint32_t off = (nn >> 3) * SBO + ((lane * K::ES) >> 4) * 128 + (nn & 7) * 16 +
@@ -549,9 +587,10 @@ __global__ void __launch_bounds__(RW * 32, KIND == 0 ? 2 : 1)
                 *reinterpret_cast<uint32_t *>(bt + BPB + off) = to_tf32(lo);
             }
         }
-        fence_async_smem();
+        if constexpr (TC)
+            fence_async_smem();
         __syncthreads();
-        if (tid == 0) {
+        if (TC && tid == 0) {
             tc_fence_after();
             const uint32_t aAddr = umma_smem_u32(stb + f64Pad), bAddr = umma_smem_u32(bt);
 #pragma unroll
@@ -585,19 +624,20 @@ __global__ void __launch_bounds__(RW * 32, KIND == 0 ? 2 : 1)
         __syncthreads();
         if (tid == 0 && k + GSTAGES < nchunks) {
             // the MMAs of chunk k have read stage s and B buffer s
-            if (!mbar_wait(&mmab[s], parity)) {
+            if (TC && !mbar_wait(&mmab[s], parity)) {
                 s_abort = 1;
             } else {
                 unsigned char *st = smem_raw + s * stg;
                 const int kn = k + GSTAGES;
                 mbar_expect_tx(&full[s], f64Bytes + K::NP * APB);
                 bulk_g2s(st, f64c + (size_t)kn * (nm + 1) * QCP, f64Bytes, &full[s]);
-                bulk_g2s(st + f64Pad, ac + (size_t)kn * K::NP * APB, K::NP * APB, &full[s]);
+                if constexpr (TC)
+                    bulk_g2s(st + f64Pad, ac + (size_t)kn * K::NP * APB, K::NP * APB, &full[s]);
             }
         }
     }
     // every MMA complete before the accumulators are read and the columns freed
-    if (tid == 0) {
+    if (TC && tid == 0) {
         umma_commit(fin);
         if (!mbar_wait(fin, 0))
             s_abort = 1;
@@ -610,7 +650,7 @@ __global__ void __launch_bounds__(RW * 32, KIND == 0 ? 2 : 1)
         atomicExch(errorFlag, 1);
     if (ok) {
         const int qw = warp & 3, t = warp >> 2;
-        if (t < R::MT) {
+        if (TC && t < R::MT) {
             uint32_t r[16];
             tmem_ld16(tmem + ((uint32_t)(32 * qw) << 16) + 16 * t, r);
             const int row = (t == 0 ? 0 : R::ROW1) + 32 * qw + lane;
@@ -630,70 +670,95 @@ __global__ void __launch_bounds__(RW * 32, KIND == 0 ? 2 : 1)
                 for (int e = 0; e < 2; ++e) {
                     const int p = base + 8 * tt + 2 * (lane & 3) + e;
                     if (p < n)
-                        out[(size_t)p * ESTR + R::NM2P + kk] = acc[tt][e];
+                        out[(size_t)p * ESTR + (TC ? R::NM2P : 0) + kk] = acc[tt][e];
                 }
         }
         const double fq0 = warp_sum(fpart0), fq1 = warp_sum(fpart1);
-        const double cm0 = warp_max(cmax0), cm1 = warp_max(cmax1);
+        double x0, x1, y0 = 0.0, y1 = 0.0;
+        if constexpr (TC) {
+            x0 = warp_max(cmax0);
+            x1 = warp_max(cmax1);
+        } else {
+            x0 = -warp_max(-emin0);
+            x1 = -warp_max(-emin1);
+            y0 = warp_max(emax0);
+            y1 = warp_max(emax1);
+        }
         if (lane == 0) {
 #pragma unroll
             for (int e = 0; e < 2; ++e) {
                 const int p = base + 2 * warp + e;
                 if (p < n) {
-                    out[(size_t)p * ESTR + R::NM2P + NMP] = e == 0 ? fq0 : fq1;
-                    const double cm = e == 0 ? cm0 : cm1;
-                    int sh = (cm > 0.0 && cm < 1.0 / 0.0) ? ilogb(cm) : 0;
-                    state[cell[e]].s.cshift = sh < -120 ? -120 : sh > 120 ? 120 : sh;
+                    double *o = out + (size_t)p * ESTR + (TC ? R::NM2P : 0) + NMP;
+                    o[0] = e == 0 ? fq0 : fq1;
+                    if constexpr (TC) {
+                        const double cm = e == 0 ? x0 : x1;
+                        int sh = (cm > 0.0 && cm < 1.0 / 0.0) ? ilogb(cm) : 0;
+                        state[cell[e]].s.cshift = sh < -120 ? -120 : sh > 120 ? 120 : sh;
+                    } else {
+                        o[1] = e == 0 ? x0 : x1;
+                        o[2] = e == 0 ? y0 : y1;
+                    }
                 }
             }
         }
     }
-    tc_fence_before();
-    __syncthreads();
-    if (warp == 0) {
-        tc_fence_after();
-        tmem_dealloc(tmem, 32);
+    if constexpr (TC) {
+        tc_fence_before();
+        __syncthreads();
+        if (warp == 0) {
+            tc_fence_after();
+            tmem_dealloc(tmem, 32);
+        }
     }
 }
 
 // Newton logic for the listed cells: one warp per cell, RWN cells per CTA, state staged
 // in shared memory with H in the tiled layout (TSlot).
-// MIX: the list of a mixed-precision pass (entries of mix_entry_doubles): H from the
-// reduced-precision moments, g and f from the pass's FP64 moments; a visit whose moments are
-// not all finite is redone in FP64. level: the list (0 FP64 and trials, 1 BF16, 2 3xTF32).
+// MODE 0: FP64 Hessians and trials. MODE 1: the list of a mixed-precision pass (entries of
+// mix_entry_doubles): H from the reduced-precision moments, g and f from the pass's FP64
+// moments; a visit whose moments are not all finite is redone in FP64. MODE 2: first visits
+// after the probe pass (entries of probe_entry_doubles; g0: the Gaunt terms of H's column 0,
+// g0n per row, null in the mixed closure), no Hessian. level: the list (0 FP64 and trials,
+// 1 BF16, 2 3xTF32, 3 probe).
 // GAUNT: the CTA assembles H_ij = sum_k beta_ijk mom_k (i >= j, the CSR terms of beta in
 // the order of src/opt/fobj.cpp:81-99, laid out per tile slot by c3d_set_gaunt) for its
 // cells that need a Hessian in one sweep over the tile slots, so that each term is read once
 // for RWN cells. A cell's moments sit in its slot's g..rinv vectors, which a Hessian visit
 // recomputes afterwards. Otherwise the pass wrote H in tiles to hBuf.
-template <int NT, int NT2, bool GAUNT, bool MIX>
+template <int NT, int NT2, bool GAUNT, int MODE>
 __global__ void __launch_bounds__(RWN * 32)
     rounds_newton_kernel(ClosureParams P, double m0, const int *__restrict__ list, int n,
                          CellState<NT> *state, const double *__restrict__ buf,
                          const GauntTerm *__restrict__ stream, int streamLen,
-                         Outputs O, Lists out, int level)
+                         Outputs O, Lists out, int level, const GauntTerm *__restrict__ g0,
+                         int g0n)
 {
+    constexpr bool MIX = MODE == 1;
     constexpr int NM2P = 8 * NT2;
     constexpr int NMP = Cfg<NT>::NMP;
-    constexpr int BSTR = MIX ? mix_entry_doubles(NMP, NM2P) : NM2P;
+    constexpr int BSTR = MODE == 1 ? mix_entry_doubles(NMP, NM2P)
+                                   : MODE == 2 ? probe_entry_doubles(NMP) : NM2P;
     constexpr int LS = TSlot<NT>::LSIZE;
     static_assert(!GAUNT || NM2P <= 4 * NMP, "moments must fit in g, d, alphaOld, rinv");
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    TSlot<NT> *slots = reinterpret_cast<TSlot<NT> *>(smem_raw);
+    using SlotT = NewtonSlot<NT, MODE>;
+    SlotT *slots = reinterpret_cast<SlotT *>(smem_raw);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int pos = blockIdx.x * RWN + warp;
     const bool active = pos < n;
     const long long cell = active ? list[pos] : -1;
-    const bool needH = active && state[cell].s.need == NEED_H;
-    TSlot<NT> &sl = slots[warp];
+    const bool needH = MODE != 2 && active && state[cell].s.need == NEED_H;
+    SlotT &sl = slots[warp];
     C3D_NCLK_DECL
     if (active) {
-        state_to_slot(state[cell], sl, lane, !(GAUNT && needH));
+        state_to_slot(state[cell], sl, lane, MODE != 2 && !(GAUNT && needH));
     } else if (lane == 0) {
         sl.s.need = NEED_NONE;
     }
     bool nonFinite = false;
-    if (GAUNT) {
+    if constexpr (MODE == 2) {
+    } else if (GAUNT) {
         double *mom = sl.scratch(); // g, d, alphaOld, rinv: NM2P <= 4 NMP doubles
         if (needH) {
             bool nf = false;
@@ -747,15 +812,20 @@ __global__ void __launch_bounds__(RWN * 32)
     if (!active)
         return;
     C3D_NCLK(O.stats, 0, lane);
-    if (sl.s.need == NEED_H) {
+    if constexpr (MODE == 2) {
+        if (sl.s.need == NEED_PROBE)
+            after_probe(sl, P, O, lane, m0, buf + (size_t)pos * BSTR, g0, g0n);
+    } else if (sl.s.need == NEED_H) {
         if (P.mixed && lane == 0 && O.stats)
             atomicAdd(&O.stats[level == 1 ? STAT_H_BF16 : level == 2 ? STAT_H_TF32X3 : STAT_H_FP64],
                       1ull);
-        if (MIX && nonFinite) {
-            escalate_fp64(sl, O, lane);
-        } else if (MIX) {
-            const double *e = buf + (size_t)pos * BSTR + NM2P;
-            after_hessian(sl, P, O, lane, m0, e, e[NMP]);
+        if constexpr (MIX) {
+            if (nonFinite) {
+                escalate_fp64(sl, O, lane);
+            } else {
+                const double *e = buf + (size_t)pos * BSTR + NM2P;
+                after_hessian(sl, P, O, lane, m0, e, e[NMP]);
+            }
         } else {
             after_hessian(sl, P, O, lane, m0);
         }
@@ -764,7 +834,9 @@ __global__ void __launch_bounds__(RWN * 32)
         after_trial(sl, P, O, lane, sl.s.fquad);
         C3D_NCLK(O.stats, 7, lane);
     }
-    slot_to_state(sl, state[cell], lane);
+    // a finished cell's state is not read again
+    if (sl.s.need != NEED_NONE)
+        slot_to_state(sl, state[cell], lane);
     append_if_needed(sl, P, cell, lane, out);
     C3D_NCLK(O.stats, 6, lane);
 }
@@ -793,7 +865,9 @@ size_t rounds_buf_doubles(int nm, int nm2, bool gaunt, bool mixed)
     const int nt = (nm + 7) / 8;
     if (gaunt) {
         const int nm2p = 8 * ((nm2 + 7) / 8);
-        return (size_t)(mixed ? mix_entry_doubles(8 * nt, nm2p) : nm2p);
+        const size_t e = (size_t)(mixed ? mix_entry_doubles(8 * nt, nm2p) : nm2p);
+        const size_t pr = (size_t)probe_entry_doubles(8 * nt);
+        return e > pr ? e : pr;
     }
     return (size_t)64 * nt * (nt + 1) / 2; // the tiled lower triangle
 }
@@ -810,7 +884,7 @@ template <int NT, int KIND> static size_t mixed_pass_smem(const ClosureParams &P
 {
     using K = MixKind<KIND>;
     const size_t f64Pad = ((size_t)(P.nm + 1) * QCP * 8 + 127) & ~(size_t)127;
-    const size_t stg = f64Pad + mixed_a_chunk_bytes(nm2, KIND);
+    const size_t stg = f64Pad + (KIND < 2 ? mixed_a_chunk_bytes(nm2, KIND) : 0);
     return GSTAGES * stg + GSTAGES * (size_t)K::NP * MXC * QC * K::ES + (size_t)QC * CST2 * 8 +
            (size_t)RW * P.nm * 16 + (2 * GSTAGES + 1) * 8;
 }
@@ -828,18 +902,30 @@ template <int NT, int NT2, bool GAUNT> static cudaError_t rounds_t(const RoundsL
     if (e != cudaSuccess)
         return e;
     size_t newtonSmem = RWN * sizeof(TSlot<NT>);
-    e = cudaFuncSetAttribute(rounds_newton_kernel<NT, NT2, GAUNT, false>,
+    e = cudaFuncSetAttribute(rounds_newton_kernel<NT, NT2, GAUNT, 0>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)newtonSmem);
     if (e != cudaSuccess)
         return e;
-    size_t passSmem, mixSmem[2] = {0, 0};
+    const bool probe = GAUNT && P.probe;
+    const size_t probeSmem = RWN * sizeof(ProbeSlot<NT>);
+    size_t passSmem, mixSmem[3] = {0, 0, 0};
     if (GAUNT) {
         passSmem = GSTAGES * (size_t)(R.nm2 + 1) * QCP * 8 + (size_t)QC * CST2 * 8 +
                    (size_t)(RWP * P.nm + 1) * 8 + GSTAGES * 8;
         e = cudaFuncSetAttribute(rounds_pass_gaunt_kernel<NT, NT2>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)passSmem);
+        if (e == cudaSuccess && probe) {
+            e = cudaFuncSetAttribute(rounds_newton_kernel<NT, NT2, GAUNT, 2>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)probeSmem);
+            mixSmem[2] = mixed_pass_smem<NT, 2>(P, R.nm2);
+            if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(rounds_pass_mixed_kernel<NT, NT2, 2>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)mixSmem[2]);
+        }
         if (e == cudaSuccess && mixed) {
-            e = cudaFuncSetAttribute(rounds_newton_kernel<NT, NT2, GAUNT, true>,
+            e = cudaFuncSetAttribute(rounds_newton_kernel<NT, NT2, GAUNT, 1>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)newtonSmem);
             mixSmem[0] = mixed_pass_smem<NT, 0>(P, R.nm2);
             mixSmem[1] = mixed_pass_smem<NT, 1>(P, R.nm2);
@@ -900,7 +986,18 @@ template <int NT, int NT2, bool GAUNT> static cudaError_t rounds_t(const RoundsL
             const int *la = A.list[l];
             for (long long off = 0; off < cnt[l]; off += R.batch) {
                 int nb = (int)((cnt[l] - off) < R.batch ? (cnt[l] - off) : R.batch);
-                if (l > 0) {
+                if (l == 3) {
+                    // probe passes of first visits (Gaunt form only)
+                    if constexpr (GAUNT) {
+                        const unsigned grid = (unsigned)((nb + MXC - 1) / MXC);
+                        rounds_pass_mixed_kernel<NT, NT2, 2><<<grid, RW * 32, mixSmem[2], st>>>(
+                            P, R.mixF64, nullptr, la + off, nb, state, R.buf, R.errorFlag);
+                        rounds_newton_kernel<NT, NT2, GAUNT, 2>
+                            <<<(unsigned)((nb + RWN - 1) / RWN), RWN * 32, probeSmem, st>>>(
+                                P, m0, la + off, nb, state, R.buf, R.gstream, R.streamLen, O, B, l,
+                                mixed ? nullptr : R.g0, R.g0n);
+                    }
+                } else if (l > 0) {
                     // mixed-precision Hessian passes (Gaunt form only)
                     if constexpr (GAUNT) {
                         const unsigned grid = (unsigned)((nb + MXC - 1) / MXC);
@@ -910,9 +1007,10 @@ template <int NT, int NT2, bool GAUNT> static cudaError_t rounds_t(const RoundsL
                         else
                             rounds_pass_mixed_kernel<NT, NT2, 1><<<grid, RW * 32, mixSmem[1], st>>>(
                                 P, R.mixF64, R.mixA[1], la + off, nb, state, R.buf, R.errorFlag);
-                        rounds_newton_kernel<NT, NT2, GAUNT, true>
+                        rounds_newton_kernel<NT, NT2, GAUNT, 1>
                             <<<(unsigned)((nb + RWN - 1) / RWN), RWN * 32, newtonSmem, st>>>(
-                                P, m0, la + off, nb, state, R.buf, R.gstream, R.streamLen, O, B, l);
+                                P, m0, la + off, nb, state, R.buf, R.gstream, R.streamLen, O, B, l,
+                                nullptr, 0);
                     }
                 } else {
                     if (GAUNT)
@@ -923,9 +1021,10 @@ template <int NT, int NT2, bool GAUNT> static cudaError_t rounds_t(const RoundsL
                         rounds_pass_direct_kernel<NT><<<(unsigned)((nb + RW - 1) / RW), RW * 32,
                                                         passSmem, st>>>(
                             P, R.chunks, la + off, nb, state, R.buf, R.errorFlag);
-                    rounds_newton_kernel<NT, NT2, GAUNT, false>
+                    rounds_newton_kernel<NT, NT2, GAUNT, 0>
                         <<<(unsigned)((nb + RWN - 1) / RWN), RWN * 32, newtonSmem, st>>>(
-                            P, m0, la + off, nb, state, R.buf, R.gstream, R.streamLen, O, B, 0);
+                            P, m0, la + off, nb, state, R.buf, R.gstream, R.streamLen, O, B, 0,
+                            nullptr, 0);
                 }
                 *R.launches += 2;
                 e = cudaGetLastError();

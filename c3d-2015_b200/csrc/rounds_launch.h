@@ -31,6 +31,10 @@ struct RoundsLaunch {
     // chunks of each format (BF16; TF32 hi then lo)
     const double *mixF64;
     const unsigned char *mixA[2];
+    // probe of first visits (P->probe): the Gaunt terms of H's column 0, g0n per row (col -2:
+    // padding), for the FP64 closure's gradient
+    const GauntTerm *g0;
+    int g0n;
     int *errorFlag;
     cudaStream_t stream;
     long long *launches;

@@ -41,8 +41,8 @@ long long footprint(const c3d_host::Config &c)
         const long long nm2p = 8 * ((nm2 + 7) / 8);
         const long long per = c.mnUseGaunt ? (c.mnMixed ? nm2p + nmp + 8 : nm2p)
                                            : 64 * ((nmp / 8) * (nmp / 8 + 1) / 2);
-        // state, the work lists (one per precision level, two generations), the face map
-        b += nall * (6 * nmp * 8 + 176) + 7 * nall * 4 + batch * per * 8;
+        // state, the work lists (four kinds of pass, two generations), the face map
+        b += nall * (6 * nmp * 8 + 176) + 9 * nall * 4 + batch * per * 8;
         b += nq * (nm2 + 1) * 8 * 2;
     }
     b += nq * nm * 8 * 4;

@@ -119,6 +119,7 @@ typedef struct {
     long long hessTf32x3;      /*   ... with 3xTF32 split products */
     long long hessFp64;        /*   ... with FP64 moments */
     long long escalated;       /*   reduced-precision visits redone in FP64 */
+    long long certified;       /* first visits ended by the convergence certificate */
 } c3d_closure_stats;
 
 /* Creates a context on the current CUDA device with the tables M[nq*nm],
@@ -210,6 +211,18 @@ c3d_status c3d_set_engine(c3d_ctx *ctx, int engine);
  * and multipliers differ within the tolerance. Values <= 0 select the defaults. */
 c3d_status c3d_set_precision(c3d_ctx *ctx, int mode, double condBf16, double condMixedMax,
                              int mixedIterMax);
+
+/* Convergence certificate of a cell's first Newton iteration (work-list engine, Gaunt form;
+ * on by default; no counterpart in the reference). The first visit runs a probe pass --
+ * exponents, e^{alpha.m}, the first-order moments and the extreme values e_min, e_max of
+ * e^{alpha.m} over the quadrature -- instead of the Hessian pass. Since H >= e_min G with G the
+ * quadrature's Gram matrix, |H^-1 g| and the condition estimate are bounded without H; a cell
+ * whose gradient passes the stopping test with these bounds inside the test's thresholds (by
+ * factors of 2 and 4) ends exactly as the full iteration would end it -- same multipliers,
+ * moments, counts and status -- and is finalized without forming or factoring H; its gamma
+ * record is then the bound. Other cells continue with the Hessian pass of the same
+ * iteration. Off while the x-line statistics log (which records gamma) is enabled. */
+c3d_status c3d_set_certificate(c3d_ctx *ctx, int on);
 
 /* Face-ghost mirroring of the grid closure (engine 0; on by default). The reference solves
  * every cell, ghosts included (src/update.cpp:51-53, 119-123). A face ghost holds a copy of
