@@ -156,25 +156,27 @@ def closure_flops_mixed(nm, nq, st):
     N = int(round(nm ** 0.5)) - 1
     nm2 = (2 * N + 1) ** 2
     nm2p = 8 * ((nm2 + 7) // 8)
-    visits = st.totalIters + st.escalated
+    visits = st.totalIters + st.escalated - st.certified
     fp64 = (visits * (4 * nm * nq + nq + nm ** 3 / 3.0) + st.hessFp64 * 2 * nm2 * nq
-            + st.trials * (2 * nm * nq + 2 * nq))
+            + st.certified * (4 * nm * nq + nq) + st.trials * (2 * nm * nq + 2 * nq))
     low = 2 * nm2p * nq * (st.hessBf16 + 3 * st.hessTf32x3)
     return fp64, low
 
 
-def closure_flops(nm, nq, iters, trials, hessian="gaunt"):
+def closure_flops(nm, nq, iters, trials, hessian="gaunt", certified=0):
     """Algorithmic FP64 FLOPs of the dual solves. Per Newton iteration: the exponent
     2 nm nq and nq exps (counted 1 FLOP each), the Hessian -- direct form: lower triangle
     nm(nm+1)/2 nq FMAs; Gaunt form: the nm2 = (2N+1)^2 extended moments 2 nm2 nq (the
-    sparse beta contraction, ~1% of that, is not counted) -- and Cholesky nm^3/3. Per
-    line-search trial 2 nm nq + 2 nq."""
+    sparse beta contraction, ~1% of that, is not counted) -- and Cholesky nm^3/3. An
+    iteration ended by the convergence certificate: the exponent, the exps and the
+    first-order moments 2 nm nq. Per line-search trial 2 nm nq + 2 nq."""
     N = int(round(nm ** 0.5)) - 1
     nm2 = (2 * N + 1) ** 2
     hess = nm * (nm + 1) * nq if hessian == "direct" else 2 * nm2 * nq
     per_iter = hess + 2 * nm * nq + nq + nm ** 3 / 3.0
+    per_cert = 4 * nm * nq + nq
     per_trial = 2 * nm * nq + 2 * nq
-    return iters * per_iter + trials * per_trial
+    return (iters - certified) * per_iter + certified * per_cert + trials * per_trial
 
 
 def _hbm_peak_gbs():
@@ -481,7 +483,7 @@ def b200_arm(args):
         if precision == 1:
             flops, low = closure_flops_mixed(nm, nq, st)
         else:
-            flops = closure_flops(nm, nq, st.totalIters, st.trials, args.hessian)
+            flops = closure_flops(nm, nq, st.totalIters, st.trials, args.hessian, st.certified)
         per_launch_s = ms[0] * 1e-3 / max(1, closure_launches)
         achieved = flops / max(1, closure_launches) / per_launch_s / 1e12
         roofline = dict(bound="tensor",
@@ -496,7 +498,8 @@ def b200_arm(args):
                                        "bytes at 64^3 (ncu) scaled by solved cells to 128^3",
                         peak_source="in-run cuBLAS DGEMM 8192^3 via torch (FP64 is not in "
                                     "MEASURED_PEAKS.json)",
-                        kernel=(("closure work-list rounds: rounds_pass_gaunt_kernel<7,22> + "
+                        kernel=(("closure work-list rounds: rounds_pass_mixed_kernel<7,22,2> "
+                                 "(first-visit probe) + rounds_pass_gaunt_kernel<7,22> + "
                                  "rounds_newton_kernel" if args.hessian == "gaunt" else
                                  "closure work-list rounds: rounds_pass_direct_kernel<7> + "
                                  "rounds_newton_kernel") if args.engine == "rounds" else
@@ -509,10 +512,10 @@ def b200_arm(args):
                         closure_share_of_step=ms[0] / total_ms)
         if low is not None:
             roofline["lowp_tflops"] = low / max(1, closure_launches) / per_launch_s / 1e12
-            roofline["kernel"] = ("closure work-list rounds: rounds_pass_mixed_kernel<7,22,0|1> "
-                                  "(tcgen05) + rounds_pass_gaunt_kernel<7,22> (trials, FP64 "
-                                  "Hessians) + rounds_newton_kernel")
-            roofline["traffic"] = None
+            roofline["kernel"] = ("closure work-list rounds: rounds_pass_mixed_kernel<7,22,2> "
+                                  "(first-visit probe), <7,22,0|1> (tcgen05 Hessian moments), "
+                                  "rounds_pass_gaunt_kernel<7,22> (trials, FP64 Hessians) + "
+                                  "rounds_newton_kernel")
         compare = None
         if other is not None:
             fp, mx = (other, head) if precision == 1 else (head, other)

@@ -462,8 +462,13 @@ __host__ __device__ constexpr int probe_entry_doubles(int nmp) { return nmp + 8;
 
 // KIND 2 is the probe pass of a cell's first visit (the convergence certificate): the FP64
 // part alone, with the extreme values of e^{alpha.m_q} over the chunk's directions.
-template <int NT, int NT2, int KIND>
-__global__ void __launch_bounds__(RW * 32, KIND == 1 ? 1 : 2)
+// ZD (the mixed closure's passes): the exponents of the chunk as a DMMA GEMM
+// Z[32 x 16] = M_chunk^T [32 x nm] alpha [nm x 16] (warp w: directions 8 (w % 4) .., cells
+// 8 (w / 4) ..) staged through shared memory, instead of the reference's unfused order.
+constexpr int ZS = 18; // row stride (cells) of the exponent tile: 16-byte pairs, 8-lane phases
+                       // conflict-free
+template <int NT, int NT2, int KIND, bool ZD>
+__global__ void __launch_bounds__(RW * 32, KIND == 1 ? 1 : KIND == 2 ? 3 : 2)
     rounds_pass_mixed_kernel(ClosureParams P, const double *__restrict__ f64c,
                              const unsigned char *__restrict__ ac, const int *__restrict__ list,
                              int n, CellState<NT> *state, double *__restrict__ out, int *errorFlag)
@@ -485,7 +490,8 @@ __global__ void __launch_bounds__(RW * 32, KIND == 1 ? 1 : 2)
     unsigned char *bbuf = smem_raw + GSTAGES * stg; // GSTAGES x NP x BPB
     double *cbuf = reinterpret_cast<double *>(bbuf + GSTAGES * K::NP * BPB); // QC x CST2
     double2 *alph = reinterpret_cast<double2 *>(cbuf + QC * CST2);          // RW x nm
-    uint64_t *full = reinterpret_cast<uint64_t *>(alph + RW * nm);
+    double *zbuf = reinterpret_cast<double *>(alph + RW * nm);              // ZD: QC x ZS
+    uint64_t *full = reinterpret_cast<uint64_t *>(zbuf + (ZD ? QC * ZS : 0));
     uint64_t *mmab = full + GSTAGES;
     uint64_t *fin = mmab + GSTAGES;
     __shared__ uint32_t s_tmem;
@@ -547,11 +553,35 @@ __global__ void __launch_bounds__(RW * 32, KIND == 1 ? 1 : 2)
         const unsigned char *stb = smem_raw + s * stg;
         const double *ch = reinterpret_cast<const double *>(stb);
         double z0 = 0.0, z1 = 0.0;
-        for (int i = 0; i < nm; ++i) {
-            const double m = ch[i * QCP + lane];
-            const double2 a = aw[i];
-            z0 = __dadd_rn(z0, __dmul_rn(a.x, m));
-            z1 = __dadd_rn(z1, __dmul_rn(a.y, m));
+        if constexpr (ZD) {
+            // A[dir r][k] = M2[k][8 dt + r], B[k][cell n] = alpha_n[k] (zero for k >= nm)
+            const int dt = warp & 3, ct = warp >> 2, r = lane >> 2, kq = lane & 3;
+            const int nb = 8 * ct + r;
+            const double2 *ab = alph + (nb >> 1) * nm;
+            double d0 = 0.0, d1 = 0.0;
+            for (int ks = 0; ks < (nm + 3) / 4; ++ks) {
+                const int k = 4 * ks + kq;
+                double a = 0.0, b = 0.0;
+                if (k < nm) {
+                    a = ch[k * QCP + 8 * dt + r];
+                    const double2 v = ab[k];
+                    b = (nb & 1) ? v.y : v.x;
+                }
+                dmma(d0, d1, a, b);
+            }
+            *reinterpret_cast<double2 *>(&zbuf[(8 * dt + r) * ZS + 8 * ct + 2 * kq]) =
+                make_double2(d0, d1);
+            __syncthreads();
+            const double2 zz = *reinterpret_cast<const double2 *>(&zbuf[lane * ZS + 2 * warp]);
+            z0 = zz.x;
+            z1 = zz.y;
+        } else {
+            for (int i = 0; i < nm; ++i) {
+                const double m = ch[i * QCP + lane];
+                const double2 a = aw[i];
+                z0 = __dadd_rn(z0, __dmul_rn(a.x, m));
+                z1 = __dadd_rn(z1, __dmul_rn(a.y, m));
+            }
         }
         const double wq = ch[nm * QCP + lane];
         const double ez0 = exp(z0), ez1 = exp(z1);
@@ -880,13 +910,13 @@ size_t mixed_a_chunk_bytes(int nm2, int fmt)
     return (size_t)na * QC * (fmt == 0 ? 2 : 8);
 }
 
-template <int NT, int KIND> static size_t mixed_pass_smem(const ClosureParams &P, int nm2)
+template <int NT, int KIND, bool ZD> static size_t mixed_pass_smem(const ClosureParams &P, int nm2)
 {
     using K = MixKind<KIND>;
     const size_t f64Pad = ((size_t)(P.nm + 1) * QCP * 8 + 127) & ~(size_t)127;
     const size_t stg = f64Pad + (KIND < 2 ? mixed_a_chunk_bytes(nm2, KIND) : 0);
     return GSTAGES * stg + GSTAGES * (size_t)K::NP * MXC * QC * K::ES + (size_t)QC * CST2 * 8 +
-           (size_t)RW * P.nm * 16 + (2 * GSTAGES + 1) * 8;
+           (size_t)RW * P.nm * 16 + (ZD ? (size_t)QC * ZS * 8 : 0) + (2 * GSTAGES + 1) * 8;
 }
 
 template <int NT, int NT2, bool GAUNT> static cudaError_t rounds_t(const RoundsLaunch &R)
@@ -918,23 +948,27 @@ template <int NT, int NT2, bool GAUNT> static cudaError_t rounds_t(const RoundsL
             e = cudaFuncSetAttribute(rounds_newton_kernel<NT, NT2, GAUNT, 2>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)probeSmem);
-            mixSmem[2] = mixed_pass_smem<NT, 2>(P, R.nm2);
+            mixSmem[2] = mixed ? mixed_pass_smem<NT, 2, true>(P, R.nm2)
+                               : mixed_pass_smem<NT, 2, false>(P, R.nm2);
             if (e == cudaSuccess)
-                e = cudaFuncSetAttribute(rounds_pass_mixed_kernel<NT, NT2, 2>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)mixSmem[2]);
+                e = mixed ? cudaFuncSetAttribute(rounds_pass_mixed_kernel<NT, NT2, 2, true>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)mixSmem[2])
+                          : cudaFuncSetAttribute(rounds_pass_mixed_kernel<NT, NT2, 2, false>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)mixSmem[2]);
         }
         if (e == cudaSuccess && mixed) {
             e = cudaFuncSetAttribute(rounds_newton_kernel<NT, NT2, GAUNT, 1>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)newtonSmem);
-            mixSmem[0] = mixed_pass_smem<NT, 0>(P, R.nm2);
-            mixSmem[1] = mixed_pass_smem<NT, 1>(P, R.nm2);
+            mixSmem[0] = mixed_pass_smem<NT, 0, true>(P, R.nm2);
+            mixSmem[1] = mixed_pass_smem<NT, 1, true>(P, R.nm2);
             if (e == cudaSuccess)
-                e = cudaFuncSetAttribute(rounds_pass_mixed_kernel<NT, NT2, 0>,
+                e = cudaFuncSetAttribute(rounds_pass_mixed_kernel<NT, NT2, 0, true>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)mixSmem[0]);
             if (e == cudaSuccess)
-                e = cudaFuncSetAttribute(rounds_pass_mixed_kernel<NT, NT2, 1>,
+                e = cudaFuncSetAttribute(rounds_pass_mixed_kernel<NT, NT2, 1, true>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)mixSmem[1]);
         }
@@ -990,8 +1024,14 @@ template <int NT, int NT2, bool GAUNT> static cudaError_t rounds_t(const RoundsL
                     // probe passes of first visits (Gaunt form only)
                     if constexpr (GAUNT) {
                         const unsigned grid = (unsigned)((nb + MXC - 1) / MXC);
-                        rounds_pass_mixed_kernel<NT, NT2, 2><<<grid, RW * 32, mixSmem[2], st>>>(
-                            P, R.mixF64, nullptr, la + off, nb, state, R.buf, R.errorFlag);
+                        if (mixed)
+                            rounds_pass_mixed_kernel<NT, NT2, 2, true>
+                                <<<grid, RW * 32, mixSmem[2], st>>>(P, R.mixF64, nullptr, la + off,
+                                                                    nb, state, R.buf, R.errorFlag);
+                        else
+                            rounds_pass_mixed_kernel<NT, NT2, 2, false>
+                                <<<grid, RW * 32, mixSmem[2], st>>>(P, R.mixF64, nullptr, la + off,
+                                                                    nb, state, R.buf, R.errorFlag);
                         rounds_newton_kernel<NT, NT2, GAUNT, 2>
                             <<<(unsigned)((nb + RWN - 1) / RWN), RWN * 32, probeSmem, st>>>(
                                 P, m0, la + off, nb, state, R.buf, R.gstream, R.streamLen, O, B, l,
@@ -1002,10 +1042,10 @@ template <int NT, int NT2, bool GAUNT> static cudaError_t rounds_t(const RoundsL
                     if constexpr (GAUNT) {
                         const unsigned grid = (unsigned)((nb + MXC - 1) / MXC);
                         if (l == 1)
-                            rounds_pass_mixed_kernel<NT, NT2, 0><<<grid, RW * 32, mixSmem[0], st>>>(
+                            rounds_pass_mixed_kernel<NT, NT2, 0, true><<<grid, RW * 32, mixSmem[0], st>>>(
                                 P, R.mixF64, R.mixA[0], la + off, nb, state, R.buf, R.errorFlag);
                         else
-                            rounds_pass_mixed_kernel<NT, NT2, 1><<<grid, RW * 32, mixSmem[1], st>>>(
+                            rounds_pass_mixed_kernel<NT, NT2, 1, true><<<grid, RW * 32, mixSmem[1], st>>>(
                                 P, R.mixF64, R.mixA[1], la + off, nb, state, R.buf, R.errorFlag);
                         rounds_newton_kernel<NT, NT2, GAUNT, 1>
                             <<<(unsigned)((nb + RWN - 1) / RWN), RWN * 32, newtonSmem, st>>>(
