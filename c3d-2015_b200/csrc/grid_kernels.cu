@@ -415,6 +415,175 @@ __global__ void __launch_bounds__(256)
         }
 }
 
+// The limited upwind difference of axis_flux_bf from the five values at offsets -2..2 of
+// the cell along the axis (the same operations in the same order).
+__device__ __forceinline__ double axis_flux_vals(double om, double w, double th, double m2,
+                                                 double m1, double c0, double p1, double p2)
+{
+    const bool pos = om > 0;
+    const double k1 = pos ? m2 : m1, k2 = pos ? m1 : c0, k3 = pos ? c0 : p1, k4 = pos ? p1 : p2;
+    const double h = pos ? 0.5 : -0.5;
+    const double t32 = th * (k3 - k2);
+    const double s1 = minmod_sel(th * (k4 - k3), minmod_sel(0.5 * (k4 - k2), t32));
+    const double s2 = minmod_sel(t32, minmod_sel(0.5 * (k3 - k1), th * (k2 - k1)));
+    const double f = fma(-h, s2, fma(h, s1, k3) - k2);
+    return f * om * w;
+}
+
+// The kinetic flux of kinetic_dmma_kernel with psi staged in shared memory. A CTA owns one
+// run of L consecutive interior cells along z (i, j, k0 .. k0 + L - 1; L = min(64, nz), L
+// even, nz a multiple of L) and walks its direction chunk in sub-stages of KDS = 8
+// directions. Per direction a sub-stage holds nine contiguous runs of psi, brought in by
+// 1-D bulk copies on one mbarrier: the cell run with two halo cells on either side (L + 4
+// values) and the runs of the four x- and four y-neighbour lines (i +- 1, 2 and j +- 1, 2;
+// L values each). Two sub-stages are in flight; the copies of sub-stage u + 2 are issued as
+// soon as u's projection is done. Each thread forms the limited differences of two
+// (cell, direction) pairs from shared memory, then the CTA projects the sub-stage's S tile
+// onto the moments with DMMAs (k-steps 2v, 2v + 1 of the 32-direction fragment tile), so the
+// flux is the same, operation for operation, as kinetic_dmma_kernel's.
+constexpr int KDS = 8;                  // directions per sub-stage
+constexpr int KRUN = 64;                // longest cell run per CTA
+constexpr int KPER = (KRUN + 4) + 8 * KRUN; // doubles staged per direction
+template <int NT>
+__global__ void __launch_bounds__(256)
+    kinetic_staged_kernel(GridDims g, const double *__restrict__ psi, const double *__restrict__ mfP,
+                          int q0, int nqc, int L, double rdx, double rdy, double rdz, double theta,
+                          int accumulate, double *__restrict__ flux, int *errorFlag)
+{
+    constexpr int TILE = 8 * NT * 32 + 128;
+    constexpr int CS = 68;
+    extern __shared__ __align__(128) double kinSmem[];
+    double *sP = kinSmem;                          // 2 x KDS x KPER
+    double(*sB)[TILE] = reinterpret_cast<double(*)[TILE]>(kinSmem + 2 * KDS * KPER);
+    double *sS = kinSmem + 2 * KDS * KPER + FLUX_STAGES * TILE; // KDS x CS
+    __shared__ uint64_t bar[FLUX_STAGES], pbar[2];
+    __shared__ int sAbort;
+    const int nm = g.nm;
+    const long long nall = g.nall();
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    static_assert(KDS * 32 == 256, "one warp per direction of a sub-stage");
+    const int nkb = g.nz / L;
+    const int kb = blockIdx.x % nkb;
+    const int j = 2 + (blockIdx.x / nkb) % g.ny;
+    const int i = 2 + blockIdx.x / (nkb * g.ny);
+    const int k0 = 2 + kb * L;
+    const int t0 = q0 >> 5, nt = (nqc + 31) >> 5, nu = (nqc + KDS - 1) / KDS;
+    // run r of a direction: 0 the cell run with its z halo, 1-4 x offsets -2, -1, +1, +2,
+    // 5-8 y offsets -2, -1, +1, +2 (start cell and offset in a direction's stage)
+    __shared__ long long sRun[9];
+    __shared__ int sOff[9];
+    if (tid < 9) {
+        const int r = tid, o = (r - 1) & 3, d = o < 2 ? o - 2 : o - 1;
+        sRun[r] = r == 0 ? g.cell(i, j, k0 - 2) : r <= 4 ? g.cell(i + d, j, k0) : g.cell(i, j + d, k0);
+        sOff[r] = r == 0 ? 0 : (L + 4) + (r - 1) * L;
+    }
+    const uint32_t perDir = (uint32_t)((L + 4) + 8 * L) * 8;
+    // every warp: warp d arrives on sub-stage u's barrier with the bytes of direction d and
+    // its lanes 0..8 copy the nine runs (arrival count KDS)
+    auto issue = [&](int u) {
+        const int nd = min(KDS, nqc - KDS * u), d = warp;
+        uint64_t *b = &pbar[u & 1];
+        if (lane == 0)
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(
+                             smem_addr(b)),
+                         "r"(d < nd ? perDir : 0u)
+                         : "memory");
+        __syncwarp();
+        if (d < nd && lane < 9) {
+            const double *src = psi + (long long)(KDS * u + d) * nall + sRun[lane];
+            double *dst = sP + ((u & 1) * KDS + d) * KPER + sOff[lane];
+            const uint32_t bytes = (uint32_t)(lane == 0 ? L + 4 : L) * 8;
+            asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                             smem_addr(dst)),
+                         "l"(src), "r"(bytes), "r"(smem_addr(b))
+                         : "memory");
+        }
+    };
+    if (tid == 0) {
+        sAbort = 0;
+        for (int s = 0; s < FLUX_STAGES; ++s)
+            fbar_init(&bar[s]);
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(&pbar[0])),
+                     "r"(KDS));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(&pbar[1])),
+                     "r"(KDS));
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        for (int s = 0; s < FLUX_STAGES && s < nt; ++s)
+            fbar_load(sB[s], mfP + (size_t)(t0 + s) * TILE, TILE * 8, &bar[s]);
+    }
+    __syncthreads();
+    for (int u = 0; u < 2 && u < nu; ++u)
+        issue(u);
+    const int cw = 8 * warp + (lane >> 2); // the warp's projection cells
+    const long long myc = cw < L ? g.cell(i, j, k0 + cw) : -1;
+    double acc[NT][2];
+#pragma unroll
+    for (int jj = 0; jj < NT; ++jj)
+#pragma unroll
+        for (int e2 = 0; e2 < 2; ++e2) {
+            int m = 8 * jj + 2 * (lane & 3) + e2;
+            acc[jj][e2] = (accumulate && myc >= 0 && m < nm) ? flux[myc * nm + m] : 0.0;
+        }
+    for (int u = 0; u < nu; ++u) {
+        const int t = u >> 2, v = u & 3, s = t % FLUX_STAGES;
+        // a timed-out wait is agreed on at the barrier after the stencil (the data of that
+        // sub-stage are then not used)
+        bool ok = fbar_wait(&pbar[u & 1], (u >> 1) & 1);
+        if (v == 0)
+            ok = ok && fbar_wait(&bar[s], (t / FLUX_STAGES) & 1);
+        const double *dirs = sB[s] + 8 * NT * 32;
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            const int pr = tid + 256 * r, cl = pr & 63, d = pr >> 6;
+            const int qq = KDS * v + d, ql = KDS * u + d;
+            double sv = 0.0;
+            if (cl < L && ql < nqc) {
+                const double *P = sP + ((u & 1) * KDS + d) * KPER;
+                const double *xr = P + (L + 4), *yr = xr + 4 * L;
+                const double wq = dirs[qq + 96];
+                const double c0 = P[cl + 2];
+                const double fx = axis_flux_vals(dirs[qq], wq, theta, xr[cl], xr[L + cl], c0,
+                                                 xr[2 * L + cl], xr[3 * L + cl]);
+                const double fy = axis_flux_vals(dirs[qq + 32], wq, theta, yr[cl], yr[L + cl], c0,
+                                                 yr[2 * L + cl], yr[3 * L + cl]);
+                const double fz = axis_flux_vals(dirs[qq + 64], wq, theta, P[cl], P[cl + 1], c0,
+                                                 P[cl + 3], P[cl + 4]);
+                sv = fx * rdx + fy * rdy + fz * rdz;
+            }
+            sS[d * CS + cl] = sv;
+        }
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0)
+                atomicExch(errorFlag, 1);
+            return;
+        }
+        const double *B = sB[s];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int kk = 2 * v + h;
+            const double a = sS[(4 * h + (lane & 3)) * CS + 8 * warp + (lane >> 2)];
+#pragma unroll
+            for (int jj = 0; jj < NT; ++jj)
+                dmma_g(acc[jj][0], acc[jj][1], a, B[(kk * NT + jj) * 32 + lane]);
+        }
+        __syncthreads();
+        if (u + 2 < nu)
+            issue(u + 2);
+        if (tid == 0 && v == 3 && t + FLUX_STAGES < nt)
+            fbar_load(sB[s], mfP + (size_t)(t0 + t + FLUX_STAGES) * TILE, TILE * 8, &bar[s]);
+    }
+    if (myc < 0)
+        return;
+#pragma unroll
+    for (int jj = 0; jj < NT; ++jj)
+#pragma unroll
+        for (int e2 = 0; e2 < 2; ++e2) {
+            int m = 8 * jj + 2 * (lane & 3) + e2;
+            if (m < nm)
+                flux[myc * nm + m] = acc[jj][e2];
+        }
+}
+
 // ---------------------------------------------------------------- P_N moment flux
 
 // One CTA handles CPB interior cells; phase 1 forms the six 4-point differences per
@@ -725,6 +894,25 @@ static cudaError_t kinetic_t(const GridDims &g, const double *alpha, const doubl
         int nqc = nq - q0 < qChunk ? nq - q0 : qChunk;
         ansatz_dmma_kernel<NT><<<(unsigned)((g.nall() + 63) / 64), 256, 0, st>>>(
             g, alpha, mfA, q0, nqc, isPn, psi, errorFlag);
+        // staged psi when the z lines split into even runs of at most 64 cells
+        const int L = g.nz < KRUN ? g.nz : KRUN;
+        if (L % 2 == 0 && g.nz % L == 0) {
+            const size_t smem = (size_t)(2 * KDS * KPER + FLUX_STAGES * (8 * NT * 32 + 128) +
+                                         KDS * 68) * 8;
+            cudaError_t e = cudaFuncSetAttribute(kinetic_staged_kernel<NT>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)smem);
+            if (e != cudaSuccess)
+                return e;
+            kinetic_staged_kernel<NT>
+                <<<(unsigned)((long long)g.nx * g.ny * (g.nz / L)), 256, smem, st>>>(
+                    g, psi, mfP, q0, nqc, L, 1.0 / dx, 1.0 / dy, 1.0 / dz, theta, q0 > 0 ? 1 : 0,
+                    flux, errorFlag);
+            e = cudaGetLastError();
+            if (e != cudaSuccess)
+                return e;
+            continue;
+        }
         const size_t kinSmem = (size_t)(FLUX_STAGES * (8 * NT * 32 + 128) + 32 * 68) * 8;
         // opt in above the 48 KB default for the dynamic part plus the ~1.3 KB static part
         if (kinSmem > 46 * 1024) {
