@@ -467,11 +467,23 @@ __host__ __device__ constexpr int probe_entry_doubles(int nmp) { return nmp + 8;
 // 8 (w / 4) ..) staged through shared memory, instead of the reference's unfused order.
 constexpr int ZS = 18; // row stride (cells) of the exponent tile: 16-byte pairs, 8-lane phases
                        // conflict-free
+
+// The first round of a closure with the convergence certificate: no list and no set-up
+// kernel; list position p is closure cell off + p, its grid cell cellMap[off + p] (or the
+// same index), and the probe pass reads the grid's moments and multipliers directly (the
+// scaling of load_cell, src/opt/optBatch.cpp:312-331), the probe's Newton kernel sets the cell
+// up with load_cell.
+struct FirstRound {
+    long long off;
+    const int *cellMap;
+    const double *u, *alpha;
+};
 template <int NT, int NT2, int KIND, bool ZD>
 __global__ void __launch_bounds__(RW * 32, KIND == 1 ? 1 : KIND == 2 ? 3 : 2)
     rounds_pass_mixed_kernel(ClosureParams P, const double *__restrict__ f64c,
                              const unsigned char *__restrict__ ac, const int *__restrict__ list,
-                             int n, CellState<NT> *state, double *__restrict__ out, int *errorFlag)
+                             int n, CellState<NT> *state, double *__restrict__ out, int *errorFlag,
+                             FirstRound first)
 {
     using K = MixKind<KIND>;
     using R = MixRows<NT2>;
@@ -504,15 +516,30 @@ __global__ void __launch_bounds__(RW * 32, KIND == 1 ? 1 : KIND == 2 ? 3 : 2)
 #pragma unroll
     for (int e = 0; e < 2; ++e) {
         const int pos = base + 2 * warp + e;
-        cell[e] = pos < n ? list[pos] : -1;
+        cell[e] = pos < n ? (list ? list[pos] : first.off + pos) : -1;
+        long long gc = -1;
+        double ascale = 0.0;
+        if (!list && cell[e] >= 0) {
+            gc = first.cellMap ? first.cellMap[cell[e]] : cell[e];
+            ascale = log(first.u[gc * nm]) * 2.0 * sqrt(M_PI);
+        }
         for (int i = lane; i < nm; i += 32) {
-            const double a = cell[e] >= 0 ? state[cell[e]].alpha[i] : 0.0;
+            double a = 0.0;
+            if (cell[e] >= 0) {
+                if (list) {
+                    a = state[cell[e]].alpha[i];
+                } else {
+                    a = first.alpha[gc * nm + i];
+                    if (i == 0)
+                        a = a - ascale;
+                }
+            }
             if (e == 0)
                 alph[warp * nm + i].x = a;
             else
                 alph[warp * nm + i].y = a;
         }
-        const int sh = cell[e] >= 0 ? state[cell[e]].s.cshift : 0;
+        const int sh = (cell[e] >= 0 && list) ? state[cell[e]].s.cshift : 0;
         if (lane == 0)
             s_shift[2 * warp + e] = sh;
         scale[e] = ldexp(1.0, -sh);
@@ -762,7 +789,7 @@ __global__ void __launch_bounds__(RWN * 32)
                          CellState<NT> *state, const double *__restrict__ buf,
                          const GauntTerm *__restrict__ stream, int streamLen,
                          Outputs O, Lists out, int level, const GauntTerm *__restrict__ g0,
-                         int g0n)
+                         int g0n, FirstRound first)
 {
     constexpr bool MIX = MODE == 1;
     constexpr int NM2P = 8 * NT2;
@@ -777,12 +804,15 @@ __global__ void __launch_bounds__(RWN * 32)
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int pos = blockIdx.x * RWN + warp;
     const bool active = pos < n;
-    const long long cell = active ? list[pos] : -1;
+    const long long cell = active ? (list ? list[pos] : first.off + pos) : -1;
     const bool needH = MODE != 2 && active && state[cell].s.need == NEED_H;
     SlotT &sl = slots[warp];
     C3D_NCLK_DECL
     if (active) {
-        state_to_slot(state[cell], sl, lane, MODE != 2 && !(GAUNT && needH));
+        if (MODE == 2 && !list)
+            load_cell(sl, P, O, first.cellMap ? (long long)first.cellMap[cell] : cell, lane);
+        else
+            state_to_slot(state[cell], sl, lane, MODE != 2 && !(GAUNT && needH));
     } else if (lane == 0) {
         sl.s.need = NEED_NONE;
     }
@@ -994,9 +1024,32 @@ template <int NT, int NT2, bool GAUNT> static cudaError_t rounds_t(const RoundsL
     e = cudaMemsetAsync(A.count[0], 0, NLISTS * sizeof(unsigned int), st);
     if (e != cudaSuccess)
         return e;
-    rounds_init_kernel<NT><<<(unsigned)((R.ncells + RW - 1) / RW), RW * 32, slotSmem, st>>>(
-        P, R.ncells, R.cellMap, O, state, A);
-    *R.launches += 2;
+    if (probe) {
+        // set-up and probe pass of every cell in one round (the certificate's first round)
+        if constexpr (GAUNT) {
+            for (long long off = 0; off < R.ncells; off += R.batch) {
+                const int nb = (int)((R.ncells - off) < R.batch ? (R.ncells - off) : R.batch);
+                const FirstRound fr{off, R.cellMap, R.u, R.alpha};
+                const unsigned grid = (unsigned)((nb + MXC - 1) / MXC);
+                if (mixed)
+                    rounds_pass_mixed_kernel<NT, NT2, 2, true><<<grid, RW * 32, mixSmem[2], st>>>(
+                        P, R.mixF64, nullptr, nullptr, nb, state, R.buf, R.errorFlag, fr);
+                else
+                    rounds_pass_mixed_kernel<NT, NT2, 2, false><<<grid, RW * 32, mixSmem[2], st>>>(
+                        P, R.mixF64, nullptr, nullptr, nb, state, R.buf, R.errorFlag, fr);
+                rounds_newton_kernel<NT, NT2, GAUNT, 2>
+                    <<<(unsigned)((nb + RWN - 1) / RWN), RWN * 32, probeSmem, st>>>(
+                        P, m0, nullptr, nb, state, R.buf, R.gstream, R.streamLen, O, A, 3,
+                        mixed ? nullptr : R.g0, R.g0n, fr);
+                *R.launches += 2;
+            }
+        }
+    } else {
+        rounds_init_kernel<NT><<<(unsigned)((R.ncells + RW - 1) / RW), RW * 32, slotSmem, st>>>(
+            P, R.ncells, R.cellMap, O, state, A);
+        *R.launches += 1;
+    }
+    *R.launches += 1;
     long long rounds = 0;
     for (;;) {
         e = cudaMemcpyAsync(R.hostCount, A.count[0], NLISTS * sizeof(unsigned int),
@@ -1027,15 +1080,15 @@ template <int NT, int NT2, bool GAUNT> static cudaError_t rounds_t(const RoundsL
                         if (mixed)
                             rounds_pass_mixed_kernel<NT, NT2, 2, true>
                                 <<<grid, RW * 32, mixSmem[2], st>>>(P, R.mixF64, nullptr, la + off,
-                                                                    nb, state, R.buf, R.errorFlag);
+                                                                    nb, state, R.buf, R.errorFlag, FirstRound{});
                         else
                             rounds_pass_mixed_kernel<NT, NT2, 2, false>
                                 <<<grid, RW * 32, mixSmem[2], st>>>(P, R.mixF64, nullptr, la + off,
-                                                                    nb, state, R.buf, R.errorFlag);
+                                                                    nb, state, R.buf, R.errorFlag, FirstRound{});
                         rounds_newton_kernel<NT, NT2, GAUNT, 2>
                             <<<(unsigned)((nb + RWN - 1) / RWN), RWN * 32, probeSmem, st>>>(
                                 P, m0, la + off, nb, state, R.buf, R.gstream, R.streamLen, O, B, l,
-                                mixed ? nullptr : R.g0, R.g0n);
+                                mixed ? nullptr : R.g0, R.g0n, FirstRound{});
                     }
                 } else if (l > 0) {
                     // mixed-precision Hessian passes (Gaunt form only)
@@ -1043,14 +1096,14 @@ template <int NT, int NT2, bool GAUNT> static cudaError_t rounds_t(const RoundsL
                         const unsigned grid = (unsigned)((nb + MXC - 1) / MXC);
                         if (l == 1)
                             rounds_pass_mixed_kernel<NT, NT2, 0, true><<<grid, RW * 32, mixSmem[0], st>>>(
-                                P, R.mixF64, R.mixA[0], la + off, nb, state, R.buf, R.errorFlag);
+                                P, R.mixF64, R.mixA[0], la + off, nb, state, R.buf, R.errorFlag, FirstRound{});
                         else
                             rounds_pass_mixed_kernel<NT, NT2, 1, true><<<grid, RW * 32, mixSmem[1], st>>>(
-                                P, R.mixF64, R.mixA[1], la + off, nb, state, R.buf, R.errorFlag);
+                                P, R.mixF64, R.mixA[1], la + off, nb, state, R.buf, R.errorFlag, FirstRound{});
                         rounds_newton_kernel<NT, NT2, GAUNT, 1>
                             <<<(unsigned)((nb + RWN - 1) / RWN), RWN * 32, newtonSmem, st>>>(
                                 P, m0, la + off, nb, state, R.buf, R.gstream, R.streamLen, O, B, l,
-                                nullptr, 0);
+                                nullptr, 0, FirstRound{});
                     }
                 } else {
                     if (GAUNT)
@@ -1064,7 +1117,7 @@ template <int NT, int NT2, bool GAUNT> static cudaError_t rounds_t(const RoundsL
                     rounds_newton_kernel<NT, NT2, GAUNT, 0>
                         <<<(unsigned)((nb + RWN - 1) / RWN), RWN * 32, newtonSmem, st>>>(
                             P, m0, la + off, nb, state, R.buf, R.gstream, R.streamLen, O, B, 0,
-                            nullptr, 0);
+                            nullptr, 0, FirstRound{});
                 }
                 *R.launches += 2;
                 e = cudaGetLastError();
