@@ -415,19 +415,28 @@ __global__ void __launch_bounds__(256)
         }
 }
 
-// The limited upwind difference of axis_flux_bf from the five values at offsets -2..2 of
-// the cell along the axis (the same operations in the same order).
-__device__ __forceinline__ double axis_flux_vals(double om, double w, double th, double m2,
-                                                 double m1, double c0, double p1, double p2)
+// The limited upwind difference of axis_flux_bf from the four values k1..k4 of the upwind
+// stencil (offsets -2..1 for h = 1/2, om > 0; -1..2 for h = -1/2): the same operations in
+// the same order.
+__device__ __forceinline__ double axis_flux_k(double om, double w, double th, double h,
+                                              double k1, double k2, double k3, double k4)
 {
-    const bool pos = om > 0;
-    const double k1 = pos ? m2 : m1, k2 = pos ? m1 : c0, k3 = pos ? c0 : p1, k4 = pos ? p1 : p2;
-    const double h = pos ? 0.5 : -0.5;
     const double t32 = th * (k3 - k2);
     const double s1 = minmod_sel(th * (k4 - k3), minmod_sel(0.5 * (k4 - k2), t32));
     const double s2 = minmod_sel(t32, minmod_sel(0.5 * (k3 - k1), th * (k2 - k1)));
     const double f = fma(-h, s2, fma(h, s1, k3) - k2);
     return f * om * w;
+}
+// The same along one axis of the staged runs: lo2, lo1, hi1, hi2 are the runs at offsets -2,
+// -1, +1, +2 (index cl), c the cell's own value. The sign of om is the same for all threads
+// of a warp (one direction per warp), so the branch does not diverge.
+__device__ __forceinline__ double axis_flux_run(double om, double w, double th, const double *lo2,
+                                                const double *lo1, double c, const double *hi1,
+                                                const double *hi2, int cl)
+{
+    if (om > 0)
+        return axis_flux_k(om, w, th, 0.5, lo2[cl], lo1[cl], c, hi1[cl]);
+    return axis_flux_k(om, w, th, -0.5, lo1[cl], c, hi1[cl], hi2[cl]);
 }
 
 // The kinetic flux of kinetic_dmma_kernel with psi staged in shared memory. A CTA owns one
@@ -462,10 +471,24 @@ __global__ void __launch_bounds__(256)
     const long long nall = g.nall();
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     static_assert(KDS * 32 == 256, "one warp per direction of a sub-stage");
-    const int nkb = g.nz / L;
-    const int kb = blockIdx.x % nkb;
-    const int j = 2 + (blockIdx.x / nkb) % g.ny;
-    const int i = 2 + blockIdx.x / (nkb * g.ny);
+    // block order: z run index slowest; the (i, j) lines in tiles of 16 x 16 (row-major,
+    // partial tiles at the edges), so that CTAs running at the same time stage each other's
+    // neighbour lines from L2
+    int i, j, kb;
+    {
+        constexpr int TI = 16, TJ = 16;
+        const long long lines = (long long)g.nx * g.ny;
+        kb = (int)(blockIdx.x / lines);
+        const long long r = blockIdx.x % lines, rowBlock = (long long)TI * g.ny;
+        const int ti = (int)(r / rowBlock);
+        const long long r2 = r % rowBlock;
+        const int hi = min(TI, g.nx - ti * TI);
+        const int tj = (int)(r2 / ((long long)hi * TJ));
+        const int r3 = (int)(r2 % ((long long)hi * TJ));
+        const int wj = min(TJ, g.ny - tj * TJ);
+        i = 2 + ti * TI + r3 / wj;
+        j = 2 + tj * TJ + r3 % wj;
+    }
     const int k0 = 2 + kb * L;
     const int t0 = q0 >> 5, nt = (nqc + 31) >> 5, nu = (nqc + KDS - 1) / KDS;
     // run r of a direction: 0 the cell run with its z halo, 1-4 x offsets -2, -1, +1, +2,
@@ -542,12 +565,12 @@ __global__ void __launch_bounds__(256)
                 const double *xr = P + (L + 4), *yr = xr + 4 * L;
                 const double wq = dirs[qq + 96];
                 const double c0 = P[cl + 2];
-                const double fx = axis_flux_vals(dirs[qq], wq, theta, xr[cl], xr[L + cl], c0,
-                                                 xr[2 * L + cl], xr[3 * L + cl]);
-                const double fy = axis_flux_vals(dirs[qq + 32], wq, theta, yr[cl], yr[L + cl], c0,
-                                                 yr[2 * L + cl], yr[3 * L + cl]);
-                const double fz = axis_flux_vals(dirs[qq + 64], wq, theta, P[cl], P[cl + 1], c0,
-                                                 P[cl + 3], P[cl + 4]);
+                const double fx = axis_flux_run(dirs[qq], wq, theta, xr, xr + L, c0, xr + 2 * L,
+                                                xr + 3 * L, cl);
+                const double fy = axis_flux_run(dirs[qq + 32], wq, theta, yr, yr + L, c0,
+                                                yr + 2 * L, yr + 3 * L, cl);
+                const double fz = axis_flux_run(dirs[qq + 64], wq, theta, P, P + 1, c0, P + 3,
+                                                P + 4, cl);
                 sv = fx * rdx + fy * rdy + fz * rdz;
             }
             sS[d * CS + cl] = sv;
