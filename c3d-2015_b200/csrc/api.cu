@@ -46,9 +46,10 @@ cudaError_t launch_euler(const GridDims &g, double *u, const double *flux, const
 cudaError_t launch_rk(const GridDims &g, double *u, double *uOld, int mode, int numSMs,
                       cudaStream_t st);
 cudaError_t launch_kinetic_flux(const GridDims &g, const double *alpha, const double *mfA,
-                                const double *mfP, int nq, int qChunk, double dx, double dy,
-                                double dz, double theta, int isPn, double *psi, double *flux,
-                                int *errorFlag, cudaStream_t st);
+                                const double *mfP, const double *xi, const double *eta, int nq,
+                                int qChunk, double dx, double dy, double dz, double theta,
+                                int isPn, double *psi, double *flux, int *errorFlag,
+                                cudaStream_t st);
 size_t flux_frag_doubles(int nm, int nq, int which);
 cudaError_t launch_reproject(const GridDims &g, double *u, double *alpha, const double *mfA,
                              const double *mfP, int nq, int *errorFlag, cudaStream_t st);
@@ -986,7 +987,7 @@ c3d_status c3d_flux_kinetic(c3d_ctx *c, int alphaIsU)
     int isPn = (c->solver == 0) ? 1 : 0;
     cudaEvent_t t0 = nullptr;
     timing_begin(c, &t0);
-    C3D_CUDA(launch_kinetic_flux(c->g, a, c->mfA, c->mfP, c->nq, c->qChunk,
+    C3D_CUDA(launch_kinetic_flux(c->g, a, c->mfA, c->mfP, c->xi, c->eta, c->nq, c->qChunk,
                                  c->dx, c->dy, c->dz, c->theta, isPn, c->psi, c->flux,
                                  c->errorFlag, c->stream));
     timing_end(c, 1, t0);

@@ -442,35 +442,43 @@ __device__ __forceinline__ double axis_flux_run(double om, double w, double th, 
 // The kinetic flux of kinetic_dmma_kernel with psi staged in shared memory. A CTA owns one
 // run of L consecutive interior cells along z (i, j, k0 .. k0 + L - 1; L = min(64, nz), L
 // even, nz a multiple of L) and walks its direction chunk in sub-stages of KDS = 8
-// directions. Per direction a sub-stage holds nine contiguous runs of psi, brought in by
-// 1-D bulk copies on one mbarrier: the cell run with two halo cells on either side (L + 4
-// values) and the runs of the four x- and four y-neighbour lines (i +- 1, 2 and j +- 1, 2;
-// L values each). Two sub-stages are in flight; the copies of sub-stage u + 2 are issued as
-// soon as u's projection is done. Each thread forms the limited differences of two
-// (cell, direction) pairs from shared memory, then the CTA projects the sub-stage's S tile
-// onto the moments with DMMAs (k-steps 2v, 2v + 1 of the 32-direction fragment tile), so the
-// flux is the same, operation for operation, as kinetic_dmma_kernel's.
-constexpr int KDS = 8;                  // directions per sub-stage
-constexpr int KRUN = 64;                // longest cell run per CTA
-constexpr int KPER = (KRUN + 4) + 8 * KRUN; // doubles staged per direction
+// directions, two in flight. Per direction a sub-stage holds seven contiguous runs of psi,
+// brought in by 1-D bulk copies: the cell run with two halo cells on either side (L + 4
+// values) and the three x- and three y-neighbour lines the upwind stencil of that direction
+// reads (offsets -2, -1, +1 for a positive cosine, -1, +1, +2 otherwise; L values each), and
+// the sub-stage's two projection k-steps and its directions' cosines and weights; warp d
+// copies direction d (warp 0 also the projection data), each warp arriving on the stage's
+// mbarrier with its bytes. Each thread forms the limited differences of two (cell,
+// direction) pairs from shared memory (a warp-uniform branch on the sign of the cosine),
+// then the CTA projects the sub-stage's S tile onto the moments with DMMAs (k-steps 2v,
+// 2v + 1 of the 32-direction fragment tile, in order), so the flux is the same, operation for
+// operation, as kinetic_dmma_kernel's.
+constexpr int KDS = 8;                      // directions per sub-stage
+constexpr int KRUN = 64;                    // longest cell run per CTA
+constexpr int KPER = (KRUN + 4) + 6 * KRUN; // doubles staged per direction
+template <int NT> struct KinStage {
+    static constexpr int FRAG = 2 * NT * 32;                    // two projection k-steps
+    static constexpr int DOUBLES = KDS * KPER + FRAG + 4 * KDS; // + xi, eta, mu, w of KDS dirs
+};
 template <int NT>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 3)
     kinetic_staged_kernel(GridDims g, const double *__restrict__ psi, const double *__restrict__ mfP,
+                          const double *__restrict__ xiAll, const double *__restrict__ etaAll,
                           int q0, int nqc, int L, double rdx, double rdy, double rdz, double theta,
                           int accumulate, double *__restrict__ flux, int *errorFlag)
 {
-    constexpr int TILE = 8 * NT * 32 + 128;
+    constexpr int TILE = 8 * NT * 32 + 128; // one 32-direction tile of mfP
+    constexpr int SD = KinStage<NT>::DOUBLES, FRAG = KinStage<NT>::FRAG;
     constexpr int CS = 68;
+    static_assert((SD * 8) % 16 == 0 && (KPER * 8) % 16 == 0, "stage alignment");
+    static_assert(KDS * 32 == 256, "one warp per direction of a sub-stage");
     extern __shared__ __align__(128) double kinSmem[];
-    double *sP = kinSmem;                          // 2 x KDS x KPER
-    double(*sB)[TILE] = reinterpret_cast<double(*)[TILE]>(kinSmem + 2 * KDS * KPER);
-    double *sS = kinSmem + 2 * KDS * KPER + FLUX_STAGES * TILE; // KDS x CS
-    __shared__ uint64_t bar[FLUX_STAGES], pbar[2];
-    __shared__ int sAbort;
+    double *sS = kinSmem + 2 * SD; // KDS x CS
+    __shared__ uint64_t pbar[2];
+    __shared__ long long sRun[9];
     const int nm = g.nm;
     const long long nall = g.nall();
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    static_assert(KDS * 32 == 256, "one warp per direction of a sub-stage");
     // block order: z run index slowest; the (i, j) lines in tiles of 16 x 16 (row-major,
     // partial tiles at the edges), so that CTAs running at the same time stage each other's
     // neighbour lines from L2
@@ -490,49 +498,72 @@ __global__ void __launch_bounds__(256)
         j = 2 + tj * TJ + r3 % wj;
     }
     const int k0 = 2 + kb * L;
-    const int t0 = q0 >> 5, nt = (nqc + 31) >> 5, nu = (nqc + KDS - 1) / KDS;
-    // run r of a direction: 0 the cell run with its z halo, 1-4 x offsets -2, -1, +1, +2,
-    // 5-8 y offsets -2, -1, +1, +2 (start cell and offset in a direction's stage)
-    __shared__ long long sRun[9];
-    __shared__ int sOff[9];
+    const int t0 = q0 >> 5, nu = (nqc + KDS - 1) / KDS;
+    // start cell of run r: 0 the cell run with its z halo, 1-4 x offsets -2, -1, +1, +2,
+    // 5-8 y offsets -2, -1, +1, +2
     if (tid < 9) {
         const int r = tid, o = (r - 1) & 3, d = o < 2 ? o - 2 : o - 1;
         sRun[r] = r == 0 ? g.cell(i, j, k0 - 2) : r <= 4 ? g.cell(i + d, j, k0) : g.cell(i, j + d, k0);
-        sOff[r] = r == 0 ? 0 : (L + 4) + (r - 1) * L;
     }
-    const uint32_t perDir = (uint32_t)((L + 4) + 8 * L) * 8;
-    // every warp: warp d arrives on sub-stage u's barrier with the bytes of direction d and
-    // its lanes 0..8 copy the nine runs (arrival count KDS)
+    const uint32_t perDir = (uint32_t)((L + 4) + 6 * L) * 8;
+    // a direction's stage: the cell run, then x slots 0-2, then y slots 0-2 (offsets -2, -1,
+    // +1 for a positive cosine, -1, +1, +2 otherwise)
     auto issue = [&](int u) {
         const int nd = min(KDS, nqc - KDS * u), d = warp;
+        double *st = kinSmem + (u & 1) * SD;
         uint64_t *b = &pbar[u & 1];
+        uint32_t bytes = d < nd ? perDir : 0u;
+        if (d == 0)
+            bytes += (FRAG + 4 * KDS) * 8;
         if (lane == 0)
             asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(
                              smem_addr(b)),
-                         "r"(d < nd ? perDir : 0u)
+                         "r"(bytes)
                          : "memory");
         __syncwarp();
-        if (d < nd && lane < 9) {
-            const double *src = psi + (long long)(KDS * u + d) * nall + sRun[lane];
-            double *dst = sP + ((u & 1) * KDS + d) * KPER + sOff[lane];
-            const uint32_t bytes = (uint32_t)(lane == 0 ? L + 4 : L) * 8;
+        const double *src = nullptr;
+        double *dst = nullptr;
+        uint32_t nb = 0;
+        if (d < nd && lane < 7) {
+            const int ql = KDS * u + d;
+            int r = 0, off = 0;
+            if (lane >= 1 && lane <= 3) {
+                const int sl = lane - 1;
+                r = (xiAll[q0 + ql] > 0 ? 1 : 2) + sl; // runs 1-4: offsets -2, -1, +1, +2
+                off = (L + 4) + sl * L;
+            } else if (lane >= 4) {
+                const int sl = lane - 4;
+                r = (etaAll[q0 + ql] > 0 ? 5 : 6) + sl;
+                off = (L + 4) + (3 + sl) * L;
+            }
+            src = psi + (long long)ql * nall + sRun[r];
+            dst = st + d * KPER + off;
+            nb = (uint32_t)(r == 0 ? L + 4 : L) * 8;
+        } else if (d == 0 && lane >= 7 && lane <= 11) {
+            const int ql = KDS * u;
+            const double *tile = mfP + (size_t)(t0 + (ql >> 5)) * TILE;
+            const int v = (ql & 31) / KDS;
+            if (lane == 7) {
+                src = tile + v * FRAG;
+                dst = st + KDS * KPER;
+                nb = FRAG * 8;
+            } else {
+                src = tile + 8 * NT * 32 + 32 * (lane - 8) + KDS * v; // xi, eta, mu, w
+                dst = st + KDS * KPER + FRAG + KDS * (lane - 8);
+                nb = KDS * 8;
+            }
+        }
+        if (nb)
             asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
                              smem_addr(dst)),
-                         "l"(src), "r"(bytes), "r"(smem_addr(b))
+                         "l"(src), "r"(nb), "r"(smem_addr(b))
                          : "memory");
-        }
     };
     if (tid == 0) {
-        sAbort = 0;
-        for (int s = 0; s < FLUX_STAGES; ++s)
-            fbar_init(&bar[s]);
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(&pbar[0])),
-                     "r"(KDS));
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(&pbar[1])),
-                     "r"(KDS));
+        for (int s = 0; s < 2; ++s)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(&pbar[s])),
+                         "r"(KDS));
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-        for (int s = 0; s < FLUX_STAGES && s < nt; ++s)
-            fbar_load(sB[s], mfP + (size_t)(t0 + s) * TILE, TILE * 8, &bar[s]);
     }
     __syncthreads();
     for (int u = 0; u < 2 && u < nu; ++u)
@@ -548,29 +579,31 @@ __global__ void __launch_bounds__(256)
             acc[jj][e2] = (accumulate && myc >= 0 && m < nm) ? flux[myc * nm + m] : 0.0;
         }
     for (int u = 0; u < nu; ++u) {
-        const int t = u >> 2, v = u & 3, s = t % FLUX_STAGES;
+        const double *st = kinSmem + (u & 1) * SD;
         // a timed-out wait is agreed on at the barrier after the stencil (the data of that
         // sub-stage are then not used)
-        bool ok = fbar_wait(&pbar[u & 1], (u >> 1) & 1);
-        if (v == 0)
-            ok = ok && fbar_wait(&bar[s], (t / FLUX_STAGES) & 1);
-        const double *dirs = sB[s] + 8 * NT * 32;
+        const bool ok = fbar_wait(&pbar[u & 1], (u >> 1) & 1);
+        const double *dirs = st + KDS * KPER + FRAG; // xi[KDS], eta[KDS], mu[KDS], w[KDS]
 #pragma unroll
         for (int r = 0; r < 2; ++r) {
             const int pr = tid + 256 * r, cl = pr & 63, d = pr >> 6;
-            const int qq = KDS * v + d, ql = KDS * u + d;
+            const int ql = KDS * u + d;
             double sv = 0.0;
             if (cl < L && ql < nqc) {
-                const double *P = sP + ((u & 1) * KDS + d) * KPER;
-                const double *xr = P + (L + 4), *yr = xr + 4 * L;
-                const double wq = dirs[qq + 96];
+                const double *P = st + d * KPER;
+                const double *xr = P + (L + 4), *yr = xr + 3 * L;
+                const double wq = dirs[3 * KDS + d];
                 const double c0 = P[cl + 2];
-                const double fx = axis_flux_run(dirs[qq], wq, theta, xr, xr + L, c0, xr + 2 * L,
-                                                xr + 3 * L, cl);
-                const double fy = axis_flux_run(dirs[qq + 32], wq, theta, yr, yr + L, c0,
-                                                yr + 2 * L, yr + 3 * L, cl);
-                const double fz = axis_flux_run(dirs[qq + 64], wq, theta, P, P + 1, c0, P + 3,
-                                                P + 4, cl);
+                const double ox = dirs[d], oy = dirs[KDS + d], oz = dirs[2 * KDS + d];
+                const double fx = ox > 0 ? axis_flux_k(ox, wq, theta, 0.5, xr[cl], xr[L + cl], c0,
+                                                       xr[2 * L + cl])
+                                         : axis_flux_k(ox, wq, theta, -0.5, xr[cl], c0,
+                                                       xr[L + cl], xr[2 * L + cl]);
+                const double fy = oy > 0 ? axis_flux_k(oy, wq, theta, 0.5, yr[cl], yr[L + cl], c0,
+                                                       yr[2 * L + cl])
+                                         : axis_flux_k(oy, wq, theta, -0.5, yr[cl], c0,
+                                                       yr[L + cl], yr[2 * L + cl]);
+                const double fz = axis_flux_run(oz, wq, theta, P, P + 1, c0, P + 3, P + 4, cl);
                 sv = fx * rdx + fy * rdy + fz * rdz;
             }
             sS[d * CS + cl] = sv;
@@ -580,20 +613,17 @@ __global__ void __launch_bounds__(256)
                 atomicExch(errorFlag, 1);
             return;
         }
-        const double *B = sB[s];
+        const double *B = st + KDS * KPER;
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
-            const int kk = 2 * v + h;
             const double a = sS[(4 * h + (lane & 3)) * CS + 8 * warp + (lane >> 2)];
 #pragma unroll
             for (int jj = 0; jj < NT; ++jj)
-                dmma_g(acc[jj][0], acc[jj][1], a, B[(kk * NT + jj) * 32 + lane]);
+                dmma_g(acc[jj][0], acc[jj][1], a, B[(h * NT + jj) * 32 + lane]);
         }
         __syncthreads();
         if (u + 2 < nu)
             issue(u + 2);
-        if (tid == 0 && v == 3 && t + FLUX_STAGES < nt)
-            fbar_load(sB[s], mfP + (size_t)(t0 + t + FLUX_STAGES) * TILE, TILE * 8, &bar[s]);
     }
     if (myc < 0)
         return;
@@ -909,9 +939,9 @@ void flux_frags(int nm, int nq, const double *M, const double *w, const double *
 
 template <int NT>
 static cudaError_t kinetic_t(const GridDims &g, const double *alpha, const double *mfA,
-                             const double *mfP, int nq, int qChunk, double dx, double dy, double dz,
-                             double theta, int isPn, double *psi, double *flux, int *errorFlag,
-                             cudaStream_t st)
+                             const double *mfP, const double *xi, const double *eta, int nq,
+                             int qChunk, double dx, double dy, double dz, double theta, int isPn,
+                             double *psi, double *flux, int *errorFlag, cudaStream_t st)
 {
     for (int q0 = 0; q0 < nq; q0 += qChunk) {
         int nqc = nq - q0 < qChunk ? nq - q0 : qChunk;
@@ -920,8 +950,7 @@ static cudaError_t kinetic_t(const GridDims &g, const double *alpha, const doubl
         // staged psi when the z lines split into even runs of at most 64 cells
         const int L = g.nz < KRUN ? g.nz : KRUN;
         if (L % 2 == 0 && g.nz % L == 0) {
-            const size_t smem = (size_t)(2 * KDS * KPER + FLUX_STAGES * (8 * NT * 32 + 128) +
-                                         KDS * 68) * 8;
+            const size_t smem = (size_t)(2 * KinStage<NT>::DOUBLES + KDS * 68) * 8;
             cudaError_t e = cudaFuncSetAttribute(kinetic_staged_kernel<NT>,
                                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                  (int)smem);
@@ -929,8 +958,8 @@ static cudaError_t kinetic_t(const GridDims &g, const double *alpha, const doubl
                 return e;
             kinetic_staged_kernel<NT>
                 <<<(unsigned)((long long)g.nx * g.ny * (g.nz / L)), 256, smem, st>>>(
-                    g, psi, mfP, q0, nqc, L, 1.0 / dx, 1.0 / dy, 1.0 / dz, theta, q0 > 0 ? 1 : 0,
-                    flux, errorFlag);
+                    g, psi, mfP, xi, eta, q0, nqc, L, 1.0 / dx, 1.0 / dy, 1.0 / dz, theta,
+                    q0 > 0 ? 1 : 0, flux, errorFlag);
             e = cudaGetLastError();
             if (e != cudaSuccess)
                 return e;
@@ -957,16 +986,17 @@ static cudaError_t kinetic_t(const GridDims &g, const double *alpha, const doubl
 
 // qChunk: a multiple of 32 unless it covers all of nq.
 cudaError_t launch_kinetic_flux(const GridDims &g, const double *alpha, const double *mfA,
-                                const double *mfP, int nq, int qChunk, double dx, double dy,
-                                double dz, double theta, int isPn, double *psi, double *flux,
-                                int *errorFlag, cudaStream_t st)
+                                const double *mfP, const double *xi, const double *eta, int nq,
+                                int qChunk, double dx, double dy, double dz, double theta,
+                                int isPn, double *psi, double *flux, int *errorFlag,
+                                cudaStream_t st)
 {
     if (qChunk < nq && (qChunk & 31))
         return cudaErrorInvalidValue;
 #define C3D_NT_CASE(NT)                                                                            \
     case NT:                                                                                       \
-        return kinetic_t<NT>(g, alpha, mfA, mfP, nq, qChunk, dx, dy, dz, theta, isPn, psi, flux,   \
-                             errorFlag, st);
+        return kinetic_t<NT>(g, alpha, mfA, mfP, xi, eta, nq, qChunk, dx, dy, dz, theta, isPn,   \
+                             psi, flux, errorFlag, st);
     switch ((g.nm + 7) / 8) {
         C3D_NT_CASE(1)
         C3D_NT_CASE(2)
