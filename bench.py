@@ -41,7 +41,7 @@ import numpy as np
 REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(REPO, "c3d-2015_b200"))
 
-METRIC = "M_N Newton cell-solves/s"
+METRIC = "M_N Newton cell-solves/s mixed vs FP64 at equal residual; p50/p99 latency"
 UNIT = "cell-solves/s"
 LADDER = "0,1e-8,1e-6,1e-4,1e-2,1e-1"
 
@@ -553,8 +553,9 @@ def b200_arm(args):
                          hbm_peak_gbs=HBM_PEAK_GBS,
                          hbm_frac=flux_bytes / (flux_ms * 1e-3) / 1e9 / HBM_PEAK_GBS,
                          contraction_tflops=flux_flops / (flux_ms * 1e-3) / 1e12,
-                         note="FP64-pipe bound: exponents and projection on DMMA plus "
-                              "the limiter's FP64 arithmetic (profiles/kinetic_flux_m6_48.txt)")
+                         note="FP64-pipe and issue bound: exponents and projection on DMMA "
+                              "plus the limiter's FP64 arithmetic on shared-memory staged psi "
+                              "(profiles/kinetic_flux_m6_64.txt)")
         # CPU baseline: the reference closure on a bounded sample of this workload's cells
         cpu = None
         try:
