@@ -330,6 +330,109 @@ def reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------------------ standalone closure
+STANDALONE_PER_N = (1 << 20) // 7   # 2^20 moment vectors, order N uniform over 1..7
+STANDALONE_TOL = 1e-8
+STANDALONE_LADDER = "0,1e-3,1e-2,1e-1,5e-1"
+
+
+def standalone_vectors(c3d, N, n):
+    """The batched standalone closure workload for one order N: on the order's tensor
+    quadrature (2(N+3) mu x 4(N+3) phi), multipliers alpha_k ~ N(0, s^2) for k >= 1 with s
+    log-uniform in [0.1, 5] and alpha_0 set for unit density; u = <m e^{alpha.m}> in FP64;
+    the solve starts from the isotropic multipliers of u. Seeded: numpy default_rng([2015, N])."""
+    q = c3d.quadrature(N, 2 * (N + 3))
+    nm, nq = q["nm"], q["nq"]
+    M = q["M"].reshape(nq, nm)
+    rng = np.random.default_rng([2015, N])
+    sc = np.exp(rng.uniform(np.log(0.1), np.log(5.0), n))
+    a = rng.standard_normal((n, nm)) * sc[:, None]
+    a[:, 0] = 0.0
+    u = (np.exp(a @ M.T) * q["w"]) @ M
+    a[:, 0] = -2.0 * np.sqrt(np.pi) * np.log(u[:, 0])
+    u = (np.exp(a @ M.T) * q["w"]) @ M
+    a_iso = np.zeros_like(a)
+    a_iso[:, 0] = 2.0 * np.sqrt(np.pi) * np.log(u[:, 0] / (2.0 * np.sqrt(np.pi)))
+    return q, u, a_iso
+
+
+def standalone_closure(torch, c3d, stream):
+    """FP64 vs mixed closure of the standalone workload (one context per order; the mixed
+    closure needs the Gaunt form, N <= 6, so N = 7 runs FP64 in both arms). Unbatched rules
+    (|g| <= |u| MN_TOL, gamma <= 1.1), MN_TOL 1e-8. Device-resident vectors, CUDA events
+    around each c3d_closure_vectors call after an untimed solve of the same vectors. For
+    N <= 2 the mixed closure keeps FP64 Hessians (c3d_set_precision)."""
+    L = c3d.lib()
+    per_n, tot = [], {0: [0, 0.0], 1: [0, 0.0]}
+    diffs = []
+    for N in range(1, 8):
+        q, u, a_iso = standalone_vectors(c3d, N, STANDALONE_PER_N)
+        n = len(u)
+        with tempfile.TemporaryDirectory() as tmp:
+            deck = os.path.join(tmp, "input.deck")
+            kv = dict(SOLVER="mn", TFINAL="1", OUTDT="1000", OUTPUT_DATA="false",
+                      OUTPUT_OPT_STATS="false", OUTPUT_TIMINGS="false", NX=2, NY=2, NZ=2,
+                      MPIX=1, MPIY=1, MPIZ=1, AX=-1, AY=-1, AZ=-1, BX=1, BY=1, BZ=1,
+                      MOMENT_ORDER=N, QUAD_ORDER=2 * (N + 3), CFL_FACTOR=0.5, CROSS_SECTION=1.0,
+                      INIT_FLOOR=1e-4, GAUSS_SIGMA=0.1, INIT_COND="gaussian_psi", THETA=2.0,
+                      OMP_THREADS=1, PN_USE_KINETIC_FLUX=0, MN_TOL=STANDALONE_TOL,
+                      MN_TOL_GAMMA=1.1, MN_COND_H_MAX=1e10, MN_MAX_ITER=100, MN_BATCHED="false",
+                      MN_USE_GAUNT_COEF="true" if N <= 6 else "false",
+                      MN_USE_GAUNT_SPARSE="true" if N <= 6 else "false", CUDA_KINETIC="true",
+                      CUDA_BATCHED="true", CUDA_BATCH_SIZE=50, REG_LADDER=STANDALONE_LADDER)
+            with open(deck, "w") as f:
+                f.write("".join(f"{k} {v}\n" for k, v in kv.items()))
+            solver = c3d.Solver(deck, stream=ctypes.c_void_p(stream.cuda_stream))
+        h = solver.ctx_handle
+        row = dict(N=N, nm=q["nm"], nq=q["nq"], vectors=n)
+        alphas = {}
+        for mode in (0, 1):
+            c3d.check(L.c3d_set_precision(h, mode if N <= 6 else 0, 0.0, 0.0, 0), "precision")
+            for warm in (True, False):
+                # the untimed pass is the full solve too: every kernel the timed one launches
+                # (rare-path rounds included) is loaded before the events
+                m = n
+                du = torch.tensor(u[:m], device="cuda")
+                da = torch.tensor(a_iso[:m], device="cuda")
+                it = torch.zeros(m, dtype=torch.int32, device="cuda")
+                stt = torch.zeros(m, dtype=torch.int32, device="cuda")
+                torch.cuda.synchronize()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                c3d.check(L.c3d_closure_vectors(h, m, ctypes.c_void_p(du.data_ptr()),
+                                                ctypes.c_void_p(da.data_ptr()),
+                                                ctypes.c_void_p(it.data_ptr()), None, None,
+                                                ctypes.c_void_p(stt.data_ptr())), "closure")
+                e1.record(stream)
+                torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            key = "fp64" if mode == 0 else "mixed"
+            row[key] = dict(solves_per_s=n / (ms * 1e-3), ms=ms,
+                            iters_per_solve=float(it.double().mean()),
+                            failed=int((stt != 0).sum()))
+            tot[mode][0] += n
+            tot[mode][1] += ms
+            alphas[mode] = da.cpu().numpy()
+        d = np.linalg.norm(alphas[1] - alphas[0], axis=1) / np.linalg.norm(alphas[0], axis=1)
+        row["alpha_rel_diff_median"] = float(np.median(d))
+        diffs.append(d)
+        row["mixed_over_fp64"] = row["mixed"]["solves_per_s"] / row["fp64"]["solves_per_s"]
+        per_n.append(row)
+        solver.close()
+    dall = np.concatenate(diffs)
+    f64 = tot[0][0] / (tot[0][1] * 1e-3)
+    mix = tot[1][0] / (tot[1][1] * 1e-3)
+    return dict(
+        workload=f"{7 * STANDALONE_PER_N} moment vectors, N uniform over 1..7 "
+                 f"({STANDALONE_PER_N} per order), tensor quadrature 2(N+3) x 4(N+3), "
+                 "seeded multipliers, solved from the isotropic start (unbatched rules, MN_TOL "
+                 "1e-8); N = 7 runs FP64 in both arms (the mixed closure needs the Gaunt form)",
+        fp64_solves_per_s=f64, mixed_solves_per_s=mix, mixed_over_fp64=mix / f64,
+        alpha_rel_diff_median=float(np.median(dall)),
+        alpha_rel_diff_p99=float(np.percentile(dall, 99)), per_order=per_n)
+
+
 # ------------------------------------------------------------------ B200 arm
 def b200_arm(args):
     import torch
@@ -574,6 +677,12 @@ def b200_arm(args):
             cpu = dict(value=None, unit=UNIT, cores=os.cpu_count(), kind="reference",
                        sample=f"failed: {ex}")
         hist = {str(i): int(st.iterHist[i]) for i in range(64) if st.iterHist[i]}
+        standalone = None
+        if args.standalone and world == 1:
+            try:
+                standalone = standalone_closure(torch, c3d, stream)
+            except Exception as ex:  # reported, not fatal
+                standalone = dict(error=str(ex))
         line = dict(
             metric=METRIC, value=value, unit=UNIT, n_gpus=world, steps=args.steps,
             warmup=args.warmup, ms_per_step=max_ms / args.steps, higher_is_better=True,
@@ -591,6 +700,7 @@ def b200_arm(args):
                         cells_per_step=2 * cells, l2="inputs larger than L2 (u, alpha 0.9 GB each)",
                         parallelism=f"replicas x{world}"),
             roofline=roofline, flux=flux_line, cpu_baseline=cpu, precision_compare=compare,
+            standalone_closure=standalone,
             e2e=dict(value=e2e_value, unit=UNIT, h2d_bytes_per_step=2 * nv * 8,
                      d2h_bytes_per_step=2 * nv * 8, steps=e_steps),
             gpu_launches=int(launches), clocks=clk,
@@ -622,6 +732,9 @@ def main():
     ap.add_argument("--no-compare", dest="compare", action="store_false",
                     help="skip the other precision's arm")
     ap.set_defaults(compare=True)
+    ap.add_argument("--no-standalone", dest="standalone", action="store_false",
+                    help="skip the standalone-closure comparison (2^20 vectors, N = 1..7)")
+    ap.set_defaults(standalone=True)
     args = ap.parse_args()
     if args.engine != "rounds" or args.hessian != "gaunt":
         # the mixed closure is built on the work-list engine's Gaunt form

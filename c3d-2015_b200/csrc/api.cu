@@ -936,6 +936,10 @@ c3d_status c3d_set_precision(c3d_ctx *c, int mode, double condBf16, double condM
     c->cp.condBf16 = condBf16 > 0 ? condBf16 : 1e4;
     c->cp.condMixMax = condMixedMax > 0 ? condMixedMax : 1e7;
     c->cp.mixIterMax = mixedIterMax > 0 ? mixedIterMax : 8;
+    // N <= 2 (at most 32 extended moments): the 128-row tensor-core tile would be mostly
+    // padding and the FP64 moment pass is as cheap, so the Hessians stay FP64
+    if (mode == 1 && closure_gaunt_nm2p(c->nm2) <= 32)
+        c->cp.mixIterMax = 0;
     return C3D_OK;
 }
 

@@ -48,6 +48,7 @@ struct SlotScalars {
     // per-cell shift of the next one)
     double cnd;
     int fp64, cshift;
+    int hprec; // precision of the last Hessian: 0 FP64, 1 BF16, 2 3xTF32
 };
 
 // Largest moment count (N+1)^2 whose padding to 8 gives NT tiles.
@@ -741,6 +742,7 @@ __device__ void load_cell(S &sl, const ClosureParams &P, const Outputs &O, long 
         sl.s.cnd = O.cond ? (double)O.cond[c] : -1.0;
         sl.s.fp64 = 0;
         sl.s.cshift = 0;
+        sl.s.hprec = 0;
     }
     __syncwarp();
     if (u0 <= 0) {
@@ -777,8 +779,18 @@ __device__ void next_trial(S &sl, const ClosureParams &P, const Outputs &O, int 
         for (int i = lane; i < nm; i += 32)
             sl.alpha[i] = sl.alphaOld[i];
         __syncwarp();
-        if (lane == 0)
-            sl.s.t = 0.0;
+        // mixed precision: a direction from a reduced-precision Hessian is not the reference's
+        // Newton direction; the iteration is redone from alphaOld with FP64 moments instead of
+        // regularising
+        const bool redo = P.mixed && sl.s.hprec != 0;
+        if (lane == 0) {
+            sl.s.t = redo ? 1.0 : 0.0;
+            if (redo) {
+                sl.s.fp64 = 1;
+                if (O.stats)
+                    atomicAdd(&O.stats[STAT_ESCALATED], 1ull);
+            }
+        }
         __syncwarp();
         begin_iteration(sl, P, O, lane);
     }

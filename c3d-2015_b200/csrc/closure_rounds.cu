@@ -876,9 +876,14 @@ __global__ void __launch_bounds__(RWN * 32)
         if (sl.s.need == NEED_PROBE)
             after_probe(sl, P, O, lane, m0, buf + (size_t)pos * BSTR, g0, g0n);
     } else if (sl.s.need == NEED_H) {
-        if (P.mixed && lane == 0 && O.stats)
-            atomicAdd(&O.stats[level == 1 ? STAT_H_BF16 : level == 2 ? STAT_H_TF32X3 : STAT_H_FP64],
-                      1ull);
+        if (lane == 0) {
+            sl.s.hprec = MIX ? level : 0;
+            if (P.mixed && O.stats)
+                atomicAdd(&O.stats[level == 1   ? STAT_H_BF16
+                                   : level == 2 ? STAT_H_TF32X3
+                                                : STAT_H_FP64],
+                          1ull);
+        }
         if constexpr (MIX) {
             if (nonFinite) {
                 escalate_fp64(sl, O, lane);

@@ -208,7 +208,8 @@ c3d_status c3d_set_engine(c3d_ctx *ctx, int engine);
  * factorisation fails or its moments are not finite, the cell's Hessian is FP64. The
  * gradient of the stopping test, the objective of the line search and the factorisation stay
  * FP64, so converged cells satisfy the same residual test as in mode 0; iteration counts
- * and multipliers differ within the tolerance. Values <= 0 select the defaults. */
+ * and multipliers differ within the tolerance. Values <= 0 select the defaults. For N <= 2
+ * the Hessian moments stay FP64 (the tensor-core tile would be mostly padding). */
 c3d_status c3d_set_precision(c3d_ctx *ctx, int mode, double condBf16, double condMixedMax,
                              int mixedIterMax);
 
