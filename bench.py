@@ -357,8 +357,8 @@ def standalone_vectors(c3d, N, n):
 
 
 def standalone_closure(torch, c3d, stream):
-    """FP64 vs mixed closure of the standalone workload (one context per order; the mixed
-    closure needs the Gaunt form, N <= 6, so N = 7 runs FP64 in both arms). Unbatched rules
+    """FP64 vs mixed closure of the standalone workload (one context per order, Gaunt form).
+    Unbatched rules
     (|g| <= |u| MN_TOL, gamma <= 1.1), MN_TOL 1e-8. Device-resident vectors, CUDA events
     around each c3d_closure_vectors call after an untimed solve of the same vectors. For
     N <= 2 the mixed closure keeps FP64 Hessians (c3d_set_precision)."""
@@ -377,8 +377,7 @@ def standalone_closure(torch, c3d, stream):
                       INIT_FLOOR=1e-4, GAUSS_SIGMA=0.1, INIT_COND="gaussian_psi", THETA=2.0,
                       OMP_THREADS=1, PN_USE_KINETIC_FLUX=0, MN_TOL=STANDALONE_TOL,
                       MN_TOL_GAMMA=1.1, MN_COND_H_MAX=1e10, MN_MAX_ITER=100, MN_BATCHED="false",
-                      MN_USE_GAUNT_COEF="true" if N <= 6 else "false",
-                      MN_USE_GAUNT_SPARSE="true" if N <= 6 else "false", CUDA_KINETIC="true",
+                      MN_USE_GAUNT_COEF="true", MN_USE_GAUNT_SPARSE="true", CUDA_KINETIC="true",
                       CUDA_BATCHED="true", CUDA_BATCH_SIZE=50, REG_LADDER=STANDALONE_LADDER)
             with open(deck, "w") as f:
                 f.write("".join(f"{k} {v}\n" for k, v in kv.items()))
@@ -387,7 +386,7 @@ def standalone_closure(torch, c3d, stream):
         row = dict(N=N, nm=q["nm"], nq=q["nq"], vectors=n)
         alphas = {}
         for mode in (0, 1):
-            c3d.check(L.c3d_set_precision(h, mode if N <= 6 else 0, 0.0, 0.0, 0), "precision")
+            c3d.check(L.c3d_set_precision(h, mode, 0.0, 0.0, 0), "precision")
             for warm in (True, False):
                 # the untimed pass is the full solve too: every kernel the timed one launches
                 # (rare-path rounds included) is loaded before the events
@@ -427,7 +426,7 @@ def standalone_closure(torch, c3d, stream):
         workload=f"{7 * STANDALONE_PER_N} moment vectors, N uniform over 1..7 "
                  f"({STANDALONE_PER_N} per order), tensor quadrature 2(N+3) x 4(N+3), "
                  "seeded multipliers, solved from the isotropic start (unbatched rules, MN_TOL "
-                 "1e-8); N = 7 runs FP64 in both arms (the mixed closure needs the Gaunt form)",
+                 "1e-8)",
         fp64_solves_per_s=f64, mixed_solves_per_s=mix, mixed_over_fp64=mix / f64,
         alpha_rel_diff_median=float(np.median(dall)),
         alpha_rel_diff_p99=float(np.percentile(dall, 99)), per_order=per_n)

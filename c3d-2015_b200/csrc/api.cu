@@ -556,7 +556,9 @@ static c3d_status run_closure(c3d_ctx *c, long long n, double *u, double *alpha,
     L.errorFlag = c->errorFlag;
     L.numSMs = c->numSMs;
     L.stream = c->stream;
-    if (c->gaunt) {
+    if (c->gaunt && closure_gaunt_supported(c->g.nm)) {
+        // (the persistent Gaunt kernels cover N <= 6; N = 7 forms H by direct quadrature,
+        // the same H up to rounding)
         GauntTables G{c->gChunks, c->gRow, c->gCol, c->gVal};
         C3D_CUDA(launch_closure_gaunt(L, G));
     } else {
@@ -795,8 +797,8 @@ c3d_status c3d_set_gaunt(c3d_ctx *c, int nm2, const double *M2, const int *rowPt
     int n2 = (int)std::lround(std::sqrt((double)nm));
     if (nm2 != (2 * n2 - 1) * (2 * n2 - 1))
         return fail(C3D_ERR_INVALID, "c3d_set_gaunt: nm2 must be (2N+1)^2");
-    if (!closure_gaunt_supported(nm))
-        return fail(C3D_ERR_INVALID, "c3d_set_gaunt: the Gaunt form is provided for N <= 6");
+    if (!rounds_gaunt_supported(nm))
+        return fail(C3D_ERR_INVALID, "c3d_set_gaunt: the Gaunt form is provided for N <= 7");
     const int nm2p = closure_gaunt_nm2p(nm2);
     const int nch = ceil_div(nq, QC);
     const size_t per = (size_t)(nm2p + 1) * QCP;

@@ -1137,6 +1137,13 @@ template <int NT, int NT2, bool GAUNT> static cudaError_t rounds_t(const RoundsL
     return cudaSuccess;
 }
 
+// Moment counts with a work-list Gaunt form (N <= 7).
+bool rounds_gaunt_supported(int nm)
+{
+    return nm == 1 || nm == 4 || nm == 9 || nm == 16 || nm == 25 || nm == 36 || nm == 49 ||
+           nm == 64;
+}
+
 cudaError_t launch_closure_rounds(const RoundsLaunch &R, bool gaunt)
 {
     const int nm = R.P->nm;
@@ -1149,6 +1156,7 @@ cudaError_t launch_closure_rounds(const RoundsLaunch &R, bool gaunt)
         case 25: return rounds_t<4, 11, true>(R);
         case 36: return rounds_t<5, 16, true>(R);
         case 49: return rounds_t<7, 22, true>(R);
+        case 64: return rounds_t<8, 29, true>(R);
         default: return cudaErrorInvalidValue;
         }
     }

@@ -45,5 +45,6 @@ cudaError_t launch_closure_rounds(const RoundsLaunch &R, bool gaunt);
 size_t rounds_state_bytes(int nm);
 size_t rounds_buf_doubles(int nm, int nm2, bool gaunt, bool mixed);
 size_t mixed_a_chunk_bytes(int nm2, int fmt);
+bool rounds_gaunt_supported(int nm);
 
 } // namespace c3d

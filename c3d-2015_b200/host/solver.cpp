@@ -269,8 +269,8 @@ c3d_status Solver::init(const Config &cfg, void *stream)
     if (s != C3D_OK)
         return s;
     if (cfg_.solver == "mn" && cfg_.mnUseGaunt) {
-        if (nm_ > 49) {
-            fprintf(stderr, "[c3d_b200] MN_USE_GAUNT_COEF: Gaunt form provided for N <= 6; the "
+        if (nm_ > 64) {
+            fprintf(stderr, "[c3d_b200] MN_USE_GAUNT_COEF: Gaunt form provided for N <= 7; the "
                             "closure forms H by direct quadrature (same H up to rounding)\n");
         } else {
             prepare_gaunt();

@@ -185,7 +185,8 @@ c3d_status c3d_closure_stats_reset(c3d_ctx *ctx);
  * H_ij = sum_k beta_ijk mom_k in CSR order. M2[nq*nm2] and the CSR table
  * rowPtr[nm*nm+1], colInd[nnz], val[nnz] indexed by i*nm+j are host arrays (copied);
  * keep |beta| > 1e-13 for MN_USE_GAUNT_SPARSE true (src/init.cpp:318-336), all nonzeros
- * for the dense mode. NULL tables switch back to the direct form. N <= 6. */
+ * for the dense mode. NULL tables switch back to the direct form. N <= 7 (the persistent
+ * engine forms H by direct quadrature for N = 7). */
 c3d_status c3d_set_gaunt(c3d_ctx *ctx, int nm2, const double *M2, const int *rowPtr,
                          const int *colInd, const double *val);
 

@@ -168,7 +168,7 @@ def test_mixed_grid_steps_track_fp64(tmp_path):
     assert rel < 1e-6, rel
 
 
-@pytest.mark.parametrize("N", [1, 2, 3, 4, 5, 6])
+@pytest.mark.parametrize("N", [1, 2, 3, 4, 5, 6, 7])
 def test_mixed_standalone_orders(oracle, N):
     """The standalone closure workload (moment vectors of order N on the order's tensor
     quadrature, solved from the isotropic start with the unbatched rules, MN_TOL 1e-8) in
@@ -178,8 +178,8 @@ def test_mixed_standalone_orders(oracle, N):
     tolerance the Armijo test between the two fails at rounding level on some vectors, which
     then regularise; the mixed closure forms both from the same FP64 quadrature sum), and
     every converged vector meets the FP64 stopping test |g| <= |u| MN_TOL (numpy). Covers the
-    tensor-core pass with one zero-padded 128-row tile (3 <= N <= 5); N <= 2 keeps FP64
-    Hessians."""
+    tensor-core pass with one zero-padded 128-row tile (3 <= N <= 5) and with two overlapping
+    tiles (N = 6, 7); N <= 2 keeps FP64 Hessians."""
     import torch
     from test_gpu_standalone_closure import _vectors
     tol, ladder, n = 1e-8, [0.0, 1e-3, 1e-2, 1e-1, 5e-1], 256
