@@ -491,6 +491,13 @@ def b200_arm(args):
         c3d.check(L.c3d_set_state(ctxh, ctypes.c_void_p(u_.data_ptr()),
                                   ctypes.c_void_p(a_.data_ptr()), None, None, 0), "set_state")
 
+    # flux autotuner (direction chunk, z run per CTA), on the initial state
+    tq, tr, tms = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+    c3d.check(L.c3d_autotune(ctxh, ctypes.byref(tq), ctypes.byref(tr), ctypes.byref(tms)),
+              "autotune")
+    tuned = dict(q_chunk=tq.value, z_run=tr.value or min(64, CONFIGS[cfg]["n"]),
+                 flux_ms=tms.value)
+
     # warm-up (FP64), then the start state S of both timed arms
     set_precision(0)
     for _ in range(args.warmup):
@@ -697,6 +704,7 @@ def b200_arm(args):
                         engine=args.engine,
                         mn_tol=MN_TOL, mn_batched=True, ladder=LADDER,
                         cells_per_step=2 * cells, l2="inputs larger than L2 (u, alpha 0.9 GB each)",
+                        flux_autotune=tuned,
                         parallelism=f"replicas x{world}"),
             roofline=roofline, flux=flux_line, cpu_baseline=cpu, precision_compare=compare,
             standalone_closure=standalone,

@@ -46,7 +46,7 @@ HEADER_SYMBOLS = [
     "c3d_set_gaunt", "c3d_set_engine", "c3d_set_ghost_mirroring", "c3d_timing_events",
     "c3d_closure_records_fp", "c3d_line_stats_enable", "c3d_line_stats_get", "c3d_stage",
     "c3d_set_x_halo_external", "c3d_copy_x_planes", "c3d_set_precision",
-    "c3d_set_certificate",
+    "c3d_set_certificate", "c3d_autotune",
 ]
 
 
@@ -117,6 +117,8 @@ def lib():
         L.c3d_set_precision.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                         ctypes.c_int]
         L.c3d_set_certificate.argtypes = [vp, ctypes.c_int]
+        L.c3d_autotune.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                   ctypes.POINTER(ctypes.c_double)]
         L.c3d_set_ghost_mirroring.argtypes = [vp, ctypes.c_int]
         L.c3d_timing_enable.argtypes = [vp, ctypes.c_int]
         L.c3d_timing_get.argtypes = [vp, _dp, ctypes.POINTER(ctypes.c_longlong)]
@@ -313,6 +315,14 @@ class Context:
         """First-visit convergence certificate (default on): exact; off gives gamma records
         of the full iteration."""
         check(lib().c3d_set_certificate(self.h, int(bool(on))), "c3d_set_certificate")
+
+    def autotune(self):
+        """Times the kinetic flux per candidate direction chunk and z run length and keeps the
+        fastest; returns (qChunk, runLen, ms per flux call)."""
+        q, r, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+        check(lib().c3d_autotune(self.h, ctypes.byref(q), ctypes.byref(r), ctypes.byref(ms)),
+              "c3d_autotune")
+        return q.value, r.value, ms.value
 
     def set_ghost_mirroring(self, on):
         check(lib().c3d_set_ghost_mirroring(self.h, int(bool(on))), "c3d_set_ghost_mirroring")

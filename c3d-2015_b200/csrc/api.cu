@@ -47,8 +47,8 @@ cudaError_t launch_rk(const GridDims &g, double *u, double *uOld, int mode, int 
                       cudaStream_t st);
 cudaError_t launch_kinetic_flux(const GridDims &g, const double *alpha, const double *mfA,
                                 const double *mfP, const double *xi, const double *eta, int nq,
-                                int qChunk, double dx, double dy, double dz, double theta,
-                                int isPn, double *psi, double *flux, int *errorFlag,
+                                int qChunk, int runLen, double dx, double dy, double dz,
+                                double theta, int isPn, double *psi, double *flux, int *errorFlag,
                                 cudaStream_t st);
 size_t flux_frag_doubles(int nm, int nq, int which);
 cudaError_t launch_reproject(const GridDims &g, double *u, double *alpha, const double *mfA,
@@ -127,6 +127,8 @@ struct c3d_ctx {
     ClosureParams cp{};
     size_t psiBytes = 0;
     int qChunk = 0;
+    int runLen = 0;     // z run per CTA of the staged kinetic kernel (0: min(64, nz))
+    size_t psiAlloc = 0; // bytes of the psi buffer
     long long launches = 0;
     // device buffers
     double *u = nullptr, *alpha = nullptr, *uOld = nullptr, *flux = nullptr;
@@ -985,20 +987,98 @@ c3d_status c3d_flux_kinetic(c3d_ctx *c, int alphaIsU)
 {
     if (!c)
         return fail(C3D_ERR_INVALID, "c3d_flux_kinetic: null context");
-    if (!c->psi) {
-        size_t bytes = (size_t)c->qChunk * c->g.nall() * 8;
-        C3D_CUDA(cudaMalloc(&c->psi, bytes));
+    const size_t need = (size_t)c->qChunk * c->g.nall() * 8;
+    if (!c->psi || c->psiAlloc < need) {
+        if (c->psi)
+            cudaFree(c->psi);
+        c->psi = nullptr;
+        c->psiAlloc = 0;
+        C3D_CUDA(cudaMalloc(&c->psi, need));
+        c->psiAlloc = need;
     }
     const double *a = alphaIsU ? c->u : c->alpha;
     int isPn = (c->solver == 0) ? 1 : 0;
     cudaEvent_t t0 = nullptr;
     timing_begin(c, &t0);
     C3D_CUDA(launch_kinetic_flux(c->g, a, c->mfA, c->mfP, c->xi, c->eta, c->nq, c->qChunk,
-                                 c->dx, c->dy, c->dz, c->theta, isPn, c->psi, c->flux,
+                                 c->runLen, c->dx, c->dy, c->dz, c->theta, isPn, c->psi, c->flux,
                                  c->errorFlag, c->stream));
     timing_end(c, 1, t0);
     int nch = ceil_div(c->nq, c->qChunk);
     c->launches += 2 * nch;
+    return C3D_OK;
+}
+
+// Flux autotuner: times the kinetic flux (one warm-up call, then the mean of two timed
+// calls, CUDA events on the context's stream) for each direction chunk -- the largest the psi
+// budget allows, and the balanced splits into 2 .. 4 more chunks -- and each z run length of
+// the staged kernel (64 and 32 cells per CTA where nz allows), and keeps the fastest. The
+// flux buffer is overwritten; the state is not touched.
+c3d_status c3d_autotune(c3d_ctx *c, int *qChunk, int *runLen, double *msPerCall)
+{
+    if (!c)
+        return fail(C3D_ERR_INVALID, "c3d_autotune: null context");
+    const int nq = c->nq;
+    const long long nall = c->g.nall();
+    long long byBudget = (long long)(c->psiBytes / ((size_t)nall * 8));
+    int qmax = byBudget >= nq ? nq : (int)(byBudget / 32) * 32;
+    if (qmax < 32)
+        qmax = nq < 32 ? nq : 32;
+    std::vector<int> qs{qmax};
+    const int k0 = ceil_div(nq, qmax);
+    for (int k = k0 + (qmax == nq ? 1 : 0); k <= k0 + 3; ++k) {
+        int q = 32 * ceil_div(ceil_div(nq, k), 32);
+        if (q < qmax && q >= 32 && std::find(qs.begin(), qs.end(), q) == qs.end())
+            qs.push_back(q);
+    }
+    std::vector<int> ls{0};
+    if (c->g.nz % 32 == 0 && c->g.nz > 32)
+        ls.push_back(32);
+    const int q0 = c->qChunk, l0 = c->runLen;
+    const bool timing = c->timing;
+    c->timing = false;
+    cudaEvent_t e0, e1;
+    C3D_CUDA(cudaEventCreate(&e0));
+    C3D_CUDA(cudaEventCreate(&e1));
+    double best = 1e300;
+    int bq = q0, bl = l0;
+    for (int q : qs)
+        for (int l : ls) {
+            c->qChunk = q;
+            c->runLen = l;
+            c3d_status s = c3d_flux_kinetic(c, 0);
+            if (s != C3D_OK) {
+                c->qChunk = q0;
+                c->runLen = l0;
+                c->timing = timing;
+                return s;
+            }
+            C3D_CUDA(cudaEventRecord(e0, c->stream));
+            for (int r = 0; r < 2; ++r)
+                if ((s = c3d_flux_kinetic(c, 0)) != C3D_OK) {
+                    c->qChunk = q0;
+                    c->runLen = l0;
+                    c->timing = timing;
+                    return s;
+                }
+            C3D_CUDA(cudaEventRecord(e1, c->stream));
+            C3D_CUDA(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            C3D_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            if (ms / 2 < best) {
+                best = ms / 2;
+                bq = q;
+                bl = l;
+            }
+        }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    c->timing = timing;
+    c->qChunk = bq;
+    c->runLen = bl;
+    if (qChunk) *qChunk = bq;
+    if (runLen) *runLen = bl;
+    if (msPerCall) *msPerCall = best;
     return C3D_OK;
 }
 

@@ -940,16 +940,18 @@ void flux_frags(int nm, int nq, const double *M, const double *w, const double *
 template <int NT>
 static cudaError_t kinetic_t(const GridDims &g, const double *alpha, const double *mfA,
                              const double *mfP, const double *xi, const double *eta, int nq,
-                             int qChunk, double dx, double dy, double dz, double theta, int isPn,
-                             double *psi, double *flux, int *errorFlag, cudaStream_t st)
+                             int qChunk, int runLen, double dx, double dy, double dz,
+                             double theta, int isPn, double *psi, double *flux, int *errorFlag,
+                             cudaStream_t st)
 {
     for (int q0 = 0; q0 < nq; q0 += qChunk) {
         int nqc = nq - q0 < qChunk ? nq - q0 : qChunk;
         ansatz_dmma_kernel<NT><<<(unsigned)((g.nall() + 63) / 64), 256, 0, st>>>(
             g, alpha, mfA, q0, nqc, isPn, psi, errorFlag);
-        // staged psi when the z lines split into even runs of at most 64 cells
-        const int L = g.nz < KRUN ? g.nz : KRUN;
-        if (L % 2 == 0 && g.nz % L == 0) {
+        // staged psi when the z lines split into even runs of at most 64 cells (runLen: the
+        // run length chosen by the autotuner, 0 for min(64, nz))
+        const int L = runLen > 0 ? runLen : (g.nz < KRUN ? g.nz : KRUN);
+        if (L % 2 == 0 && L <= KRUN && g.nz % L == 0) {
             const size_t smem = (size_t)(2 * KinStage<NT>::DOUBLES + KDS * 68) * 8;
             cudaError_t e = cudaFuncSetAttribute(kinetic_staged_kernel<NT>,
                                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -987,16 +989,16 @@ static cudaError_t kinetic_t(const GridDims &g, const double *alpha, const doubl
 // qChunk: a multiple of 32 unless it covers all of nq.
 cudaError_t launch_kinetic_flux(const GridDims &g, const double *alpha, const double *mfA,
                                 const double *mfP, const double *xi, const double *eta, int nq,
-                                int qChunk, double dx, double dy, double dz, double theta,
-                                int isPn, double *psi, double *flux, int *errorFlag,
+                                int qChunk, int runLen, double dx, double dy, double dz,
+                                double theta, int isPn, double *psi, double *flux, int *errorFlag,
                                 cudaStream_t st)
 {
     if (qChunk < nq && (qChunk & 31))
         return cudaErrorInvalidValue;
 #define C3D_NT_CASE(NT)                                                                            \
     case NT:                                                                                       \
-        return kinetic_t<NT>(g, alpha, mfA, mfP, xi, eta, nq, qChunk, dx, dy, dz, theta, isPn,   \
-                             psi, flux, errorFlag, st);
+        return kinetic_t<NT>(g, alpha, mfA, mfP, xi, eta, nq, qChunk, runLen, dx, dy, dz, theta, \
+                             isPn, psi, flux, errorFlag, st);
     switch ((g.nm + 7) / 8) {
         C3D_NT_CASE(1)
         C3D_NT_CASE(2)

@@ -88,6 +88,7 @@ std::string parse_config(const InputDeck &d, Config &c)
     d.get("MN_MIXED_COND_BF16", c.mnMixedCondBf16);
     d.get("MN_MIXED_COND_MAX", c.mnMixedCondMax);
     d.get("MN_MIXED_ITER_MAX", c.mnMixedIterMax);
+    d.get("FLUX_AUTOTUNE", c.fluxAutotune);
     d.get("SIGMA_CHECKER_BLOCK", c.checkerBlock);
     d.get("SIGMA_S_HI", c.sigmaSHi);
     d.get("SIGMA_A_HI", c.sigmaAHi);
@@ -294,7 +295,11 @@ c3d_status Solver::init(const Config &cfg, void *stream)
         if ((s = c3d_line_stats_enable(ctx_, (int)(2 * steps + 2))) != C3D_OK)
             return s;
     }
-    return push();
+    if ((s = push()) != C3D_OK)
+        return s;
+    if (cfg_.solver == "mn" && cfg_.fluxAutotune && (s = c3d_autotune(ctx_, nullptr, nullptr, nullptr)) != C3D_OK)
+        return s;
+    return C3D_OK;
 }
 
 c3d_status Solver::push()

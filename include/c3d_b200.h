@@ -226,6 +226,14 @@ c3d_status c3d_set_precision(c3d_ctx *ctx, int mode, double condBf16, double con
  * iteration. Off while the x-line statistics log (which records gamma) is enabled. */
 c3d_status c3d_set_certificate(c3d_ctx *ctx, int on);
 
+/* Flux autotuner (no counterpart in the reference): times the kinetic flux of the context's
+ * current multipliers for each candidate direction chunk (the largest the psi budget allows
+ * and the balanced splits into up to 3 more chunks) and z run length per CTA of the staged
+ * kernel (64, and 32 where nz is a multiple of 32), then keeps the fastest for later calls.
+ * The flux buffer is overwritten; u and alpha are not touched. Outputs may be NULL
+ * (runLen 0: min(64, nz)). */
+c3d_status c3d_autotune(c3d_ctx *ctx, int *qChunk, int *runLen, double *msPerCall);
+
 /* Face-ghost mirroring of the grid closure (engine 0; on by default). The reference solves
  * every cell, ghosts included (src/update.cpp:51-53, 119-123). A face ghost holds a copy of
  * its periodic image's moments, so when its multipliers (the warm start) also equal the
