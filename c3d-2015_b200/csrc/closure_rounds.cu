@@ -788,7 +788,7 @@ __global__ void __launch_bounds__(RWN * 32)
     rounds_newton_kernel(ClosureParams P, double m0, const int *__restrict__ list, int n,
                          CellState<NT> *state, const double *__restrict__ buf,
                          const GauntTerm *__restrict__ stream, int streamLen,
-                         Outputs O, Lists out, int level, const GauntTerm *__restrict__ g0,
+                         Outputs Og, Lists out, int level, const GauntTerm *__restrict__ g0,
                          int g0n, FirstRound first)
 {
     constexpr bool MIX = MODE == 1;
@@ -802,6 +802,15 @@ __global__ void __launch_bounds__(RWN * 32)
     using SlotT = NewtonSlot<NT, MODE>;
     SlotT *slots = reinterpret_cast<SlotT *>(smem_raw);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    // the CTA's closure counters, added to the context's once at the end (one global atomic
+    // per counter and CTA instead of several per finished cell)
+    __shared__ unsigned long long sStat[STAT_COUNT];
+    for (int q = tid; q < STAT_COUNT; q += RWN * 32)
+        sStat[q] = 0;
+    __syncthreads();
+    Outputs O = Og;
+    if (Og.stats)
+        O.stats = sStat;
     const int pos = blockIdx.x * RWN + warp;
     const bool active = pos < n;
     const long long cell = active ? (list ? list[pos] : first.off + pos) : -1;
@@ -869,8 +878,7 @@ __global__ void __launch_bounds__(RWN * 32)
             L[e] = H[e];
         __syncwarp();
     }
-    if (!active)
-        return;
+    if (active) {
     C3D_NCLK(O.stats, 0, lane);
     if constexpr (MODE == 2) {
         if (sl.s.need == NEED_PROBE)
@@ -904,6 +912,18 @@ __global__ void __launch_bounds__(RWN * 32)
         slot_to_state(sl, state[cell], lane);
     append_if_needed(sl, P, cell, lane, out);
     C3D_NCLK(O.stats, 6, lane);
+    }
+    __syncthreads();
+    if (Og.stats)
+        for (int q = tid; q < STAT_COUNT; q += RWN * 32) {
+            const unsigned long long v = sStat[q];
+            if (v == 0)
+                continue;
+            if (q == STAT_MAX_ITER || q == STAT_MAX_ITER_GAMMA)
+                atomicMax(&Og.stats[q], v);
+            else
+                atomicAdd(&Og.stats[q], v);
+        }
 }
 
 // ---------------------------------------------------------------- host side
