@@ -50,6 +50,11 @@ __global__ void ghost_stats_kernel(GridDims g, const int *__restrict__ iters,
                                    const int *__restrict__ regIdx, const int *__restrict__ status,
                                    unsigned long long *stats)
 {
+    // the CTA's counters in shared memory, added to the context's once per CTA
+    __shared__ unsigned long long sStat[STAT_COUNT];
+    for (int q = threadIdx.x; q < STAT_COUNT; q += blockDim.x)
+        sStat[q] = 0;
+    __syncthreads();
     const long long total = ghost_faces(g);
     for (long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x; f < total;
          f += (long long)gridDim.x * blockDim.x) {
@@ -57,15 +62,25 @@ __global__ void ghost_stats_kernel(GridDims g, const int *__restrict__ iters,
         ghost_pair(g, f, dst, src);
         const unsigned long long it = (unsigned long long)iters[dst];
         const unsigned long long ig = (unsigned long long)iterGamma[dst];
-        atomicAdd(&stats[STAT_CELLS], 1ull);
-        atomicAdd(&stats[STAT_ITERS], it);
-        atomicAdd(&stats[STAT_ITER_GAMMA], ig);
-        atomicMax(&stats[STAT_MAX_ITER], it);
-        atomicMax(&stats[STAT_MAX_ITER_GAMMA], ig);
+        atomicAdd(&sStat[STAT_CELLS], 1ull);
+        atomicAdd(&sStat[STAT_ITERS], it);
+        atomicAdd(&sStat[STAT_ITER_GAMMA], ig);
+        atomicMax(&sStat[STAT_MAX_ITER], it);
+        atomicMax(&sStat[STAT_MAX_ITER_GAMMA], ig);
         if (status[dst] != CELL_OK)
-            atomicAdd(&stats[STAT_FAILED], 1ull);
-        atomicAdd(&stats[STAT_REG_HIST + (regIdx[dst] & 15)], 1ull);
-        atomicAdd(&stats[STAT_ITER_HIST + (it < 63 ? it : 63)], 1ull);
+            atomicAdd(&sStat[STAT_FAILED], 1ull);
+        atomicAdd(&sStat[STAT_REG_HIST + (regIdx[dst] & 15)], 1ull);
+        atomicAdd(&sStat[STAT_ITER_HIST + (it < 63 ? it : 63)], 1ull);
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < STAT_COUNT; q += blockDim.x) {
+        const unsigned long long v = sStat[q];
+        if (v == 0)
+            continue;
+        if (q == STAT_MAX_ITER || q == STAT_MAX_ITER_GAMMA)
+            atomicMax(&stats[q], v);
+        else
+            atomicAdd(&stats[q], v);
     }
 }
 
