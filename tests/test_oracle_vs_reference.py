@@ -20,7 +20,7 @@ from oracle_lib import (REF_SO, deck_text, make_opts, run_reference, tie_cells)
 
 pytestmark = pytest.mark.skipif(not os.path.exists(REF_SO), reason="reference build absent")
 
-BASELINE_LADDER = [0.0, 1e-8, 1e-6, 1e-4, 1e-2, 1e-1]
+DECK_LADDER = [0.0, 1e-8, 1e-6, 1e-4, 1e-2, 1e-1]
 
 
 def _write(tmp_path, text):
@@ -118,7 +118,7 @@ def test_pn_steps_bit_exact(oracle, kinetic):
 
 
 @pytest.mark.parametrize("batched,ladder,gaunt", [(True, None, 0), (False, None, 0),
-                                                   (True, BASELINE_LADDER, 0), (True, None, 2),
+                                                   (True, DECK_LADDER, 0), (True, None, 2),
                                                    (True, None, 1)])
 def test_closure_steps_vs_reference(oracle, batched, ladder, gaunt):
     """gaunt: 0 direct H, 1 dense Gaunt, 2 sparse Gaunt (MN_USE_GAUNT_COEF/_SPARSE)."""
