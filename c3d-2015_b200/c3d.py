@@ -46,7 +46,8 @@ HEADER_SYMBOLS = [
     "c3d_set_gaunt", "c3d_set_engine", "c3d_set_ghost_mirroring", "c3d_timing_events",
     "c3d_closure_records_fp", "c3d_line_stats_enable", "c3d_line_stats_get", "c3d_stage",
     "c3d_set_x_halo_external", "c3d_copy_x_planes", "c3d_set_precision",
-    "c3d_set_certificate", "c3d_autotune",
+    "c3d_set_certificate", "c3d_autotune", "c3d_closure_vectors_noalloc_check",
+    "c3d_set_limits",
 ]
 
 
@@ -120,6 +121,7 @@ def lib():
         L.c3d_autotune.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                                    ctypes.POINTER(ctypes.c_double)]
         L.c3d_set_ghost_mirroring.argtypes = [vp, ctypes.c_int]
+        L.c3d_set_limits.argtypes = [vp, ctypes.c_longlong, ctypes.c_longlong]
         L.c3d_timing_enable.argtypes = [vp, ctypes.c_int]
         L.c3d_timing_get.argtypes = [vp, _dp, ctypes.POINTER(ctypes.c_longlong)]
         L.c3d_launch_count.argtypes = [vp]
@@ -323,6 +325,11 @@ class Context:
         check(lib().c3d_autotune(self.h, ctypes.byref(q), ctypes.byref(r), ctypes.byref(ms)),
               "c3d_autotune")
         return q.value, r.value, ms.value
+
+    def set_limits(self, max_rounds=0, pass_budget=0):
+        """Work-list rounds per closure and passes per cell before the closure gives up
+        (C3D_ERR_TIMEOUT / cell status 3); 0 restores the defaults."""
+        check(lib().c3d_set_limits(self.h, int(max_rounds), int(pass_budget)), "c3d_set_limits")
 
     def set_ghost_mirroring(self, on):
         check(lib().c3d_set_ghost_mirroring(self.h, int(bool(on))), "c3d_set_ghost_mirroring")

@@ -39,6 +39,11 @@ bool closure_gaunt_supported(int nm);
 int closure_gaunt_nm2p(int nm2);
 cudaError_t launch_hessian_batch(int nm, int nchunks, const double *chunks, const double *alphas,
                                  long long n, double *hs, int *errorFlag, cudaStream_t st);
+size_t gaunt_batch_smem(int nm, int nm2p);
+cudaError_t launch_gaunt_batch(int nm, int nm2, int nm2p, int nchunks, const double *chunks,
+                               const double *alphas, long long n, const double *betaT,
+                               const int *rowPtr, const int *colInd, const double *val,
+                               int sparse, double *hs, int *errorFlag, cudaStream_t st);
 cudaError_t launch_ghost_fill(const GridDims &g, double *u, int numSMs, cudaStream_t st,
                               bool skipX = false);
 cudaError_t launch_euler(const GridDims &g, double *u, const double *flux, const double *sigT,
@@ -147,6 +152,7 @@ struct c3d_ctx {
     int *errorFlag = nullptr;
     double m0 = 0.0; // M[0][0]
     int engine = 0;  // 0: work-list rounds, 1: persistent kernels
+    long long maxRounds = 1LL << 24; // work-list rounds per closure before C3D_ERR_TIMEOUT
     // work-list buffers (sized on first use)
     void *rState = nullptr;
     int *rListA = nullptr, *rListB = nullptr;
@@ -532,7 +538,7 @@ static c3d_status run_closure(c3d_ctx *c, long long n, double *u, double *alpha,
         R.errorFlag = c->errorFlag;
         R.stream = c->stream;
         R.launches = &c->launches;
-        R.maxRounds = 1LL << 24;
+        R.maxRounds = c->maxRounds;
         cudaError_t e = launch_closure_rounds(R, c->gaunt);
         if (e == cudaErrorLaunchTimeout)
             return fail(C3D_ERR_TIMEOUT, "closure: round limit exceeded");
@@ -965,6 +971,15 @@ c3d_status c3d_set_engine(c3d_ctx *c, int engine)
     return C3D_OK;
 }
 
+c3d_status c3d_set_limits(c3d_ctx *c, long long maxRounds, long long passBudget)
+{
+    if (!c)
+        return fail(C3D_ERR_INVALID, "c3d_set_limits: null context");
+    c->maxRounds = maxRounds > 0 ? maxRounds : (1LL << 24);
+    c->cp.passBudget = passBudget > 0 ? passBudget : (1LL << 40);
+    return C3D_OK;
+}
+
 c3d_status c3d_set_ghost_mirroring(c3d_ctx *c, int on)
 {
     if (!c)
@@ -1354,66 +1369,185 @@ static std::mutex g_refMutex;
 static struct {
     int nm = 0, nq = 0, nchunks = 0;
     double *chunks = nullptr, *alphas = nullptr, *hs = nullptr;
-    long long cap = 0;
+    long long cap = 0; // batch buffers hold cap vectors of up to capNm moments
+    int capNm = 0;
     int *errorFlag = nullptr;
+    // Gaunt form (solveHInit_cuda with useGaunt): staged chunks of M^T, M2^T and the weights,
+    // dense beta transposed (betaT[k nm^2 + i nm + j]) and the CSR table of |beta| > 1e-13
+    int nm2 = 0, nm2p = 0, gnchunks = 0;
+    double *gchunks = nullptr, *betaT = nullptr, *betaVal = nullptr;
+    int *betaRow = nullptr, *betaCol = nullptr;
 } g_h;
+
+static void ref_free(void *&p)
+{
+    if (p)
+        cudaFree(p);
+    p = nullptr;
+}
+
+// Host staging for a device table; returns false (and prints) on a CUDA error.
+static bool ref_upload(void **dst, const void *src, size_t bytes, const char *what)
+{
+    void *d = nullptr;
+    cudaError_t e = cudaMalloc(&d, bytes > 0 ? bytes : 1);
+    if (e == cudaSuccess && bytes > 0)
+        e = cudaMemcpy(d, src, bytes, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        if (d)
+            cudaFree(d);
+        cudaGetLastError();
+        fprintf(stderr, "[c3d_b200] solveHInit_cuda: %s: %s\n", what, cudaGetErrorString(e));
+        return false;
+    }
+    *dst = d;
+    return true;
+}
 
 void solveHInit_cuda(int nm, int nm2, int nq, int batchSize, double *w, double *p, double *p2,
                      double *beta, double *betaVal, int *betaColInd, int *betaRowPtr, int useGaunt)
 {
-    (void)nm2; (void)p2; (void)beta; (void)betaVal; (void)betaColInd; (void)betaRowPtr;
     std::lock_guard<std::mutex> lk(g_refMutex);
-    if (useGaunt) {
-        fprintf(stderr, "[c3d_b200] solveHInit_cuda: Gaunt-coefficient Hessians are not provided; "
-                        "use MN_USE_GAUNT_COEF false\n");
-        return;
-    }
-    if (nm < 1 || nm > 64 || nq < 1) {
+    if (nm < 1 || nm > 64 || nq < 1 || !w || !p) {
         fprintf(stderr, "[c3d_b200] solveHInit_cuda: unsupported sizes nm=%d nq=%d\n", nm, nq);
         return;
     }
+    // direct form: chunks of M^T and the weights
     std::vector<double> ch = build_chunks(nm, nq, p, w);
-    if (g_h.chunks)
-        cudaFree(g_h.chunks);
-    g_h.nm = nm;
-    g_h.nq = nq;
+    ref_free((void *&)g_h.chunks);
+    g_h.nm = g_h.nq = 0;
+    if (!ref_upload((void **)&g_h.chunks, ch.data(), ch.size() * 8, "basis"))
+        return;
     g_h.nchunks = ceil_div(nq, QC);
-    cudaMalloc(&g_h.chunks, ch.size() * 8);
-    cudaMemcpy(g_h.chunks, ch.data(), ch.size() * 8, cudaMemcpyHostToDevice);
     if (!g_h.errorFlag) {
-        cudaMalloc(&g_h.errorFlag, 4);
-        cudaMemset(g_h.errorFlag, 0, 4);
+        if (cudaMalloc(&g_h.errorFlag, 4) != cudaSuccess || cudaMemset(g_h.errorFlag, 0, 4) != cudaSuccess) {
+            cudaGetLastError();
+            g_h.errorFlag = nullptr;
+            fprintf(stderr, "[c3d_b200] solveHInit_cuda: device allocation failed\n");
+            return;
+        }
     }
     long long cap = batchSize > 0 ? batchSize : 1;
-    if (cap > g_h.cap) {
-        if (g_h.alphas) cudaFree(g_h.alphas);
-        if (g_h.hs) cudaFree(g_h.hs);
-        cudaMalloc(&g_h.alphas, cap * nm * 8);
-        cudaMalloc(&g_h.hs, cap * nm * nm * 8);
+    if (cap > g_h.cap || nm > g_h.capNm) {
+        ref_free((void *&)g_h.alphas);
+        ref_free((void *&)g_h.hs);
+        g_h.cap = 0;
+        g_h.capNm = 0;
+        if (cudaMalloc(&g_h.alphas, cap * nm * 8) != cudaSuccess ||
+            cudaMalloc(&g_h.hs, cap * nm * nm * 8) != cudaSuccess) {
+            cudaGetLastError();
+            ref_free((void *&)g_h.alphas);
+            ref_free((void *&)g_h.hs);
+            fprintf(stderr, "[c3d_b200] solveHInit_cuda: device allocation of the batch failed\n");
+            return;
+        }
         g_h.cap = cap;
+        g_h.capNm = nm;
     }
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess)
-        fprintf(stderr, "[c3d_b200] solveHInit_cuda: %s\n", cudaGetErrorString(e));
+    // Gaunt form (src/cuda/cuda_solveH.cu:44-104 takes the same tables)
+    ref_free((void *&)g_h.gchunks);
+    ref_free((void *&)g_h.betaT);
+    ref_free((void *&)g_h.betaVal);
+    ref_free((void *&)g_h.betaRow);
+    ref_free((void *&)g_h.betaCol);
+    g_h.nm2 = g_h.nm2p = g_h.gnchunks = 0;
+    if (useGaunt) {
+        const int nm2p = 8 * ceil_div(nm2, 8);
+        if (nm2 < 1 || !p2 || gaunt_batch_smem(nm, nm2p) == 0) {
+            fprintf(stderr, "[c3d_b200] solveHInit_cuda: unsupported Gaunt sizes nm=%d nm2=%d\n",
+                    nm, nm2);
+            return;
+        }
+        const int rows = nm + nm2p + 1, nch = ceil_div(nq, QC);
+        std::vector<double> gch((size_t)nch * rows * QCP, 0.0);
+        for (int k = 0; k < nch; ++k)
+            for (int qq = 0; qq < QC && k * QC + qq < nq; ++qq) {
+                const int q = k * QC + qq;
+                double *c = gch.data() + (size_t)k * rows * QCP;
+                for (int i = 0; i < nm; ++i)
+                    c[i * QCP + qq] = p[(size_t)q * nm + i];
+                for (int i = 0; i < nm2; ++i)
+                    c[(nm + i) * QCP + qq] = p2[(size_t)q * nm2 + i];
+                c[(nm + nm2p) * QCP + qq] = w[q];
+            }
+        if (!ref_upload((void **)&g_h.gchunks, gch.data(), gch.size() * 8, "Gaunt basis"))
+            return;
+        if (beta) {
+            const size_t nmm = (size_t)nm * nm;
+            std::vector<double> bt(nmm * nm2);
+            for (size_t ij = 0; ij < nmm; ++ij)
+                for (int k = 0; k < nm2; ++k)
+                    bt[(size_t)k * nmm + ij] = beta[ij * nm2 + k];
+            if (!ref_upload((void **)&g_h.betaT, bt.data(), bt.size() * 8, "dense beta"))
+                return;
+        }
+        if (betaVal && betaColInd && betaRowPtr) {
+            const int nnz = betaRowPtr[nm * nm];
+            if (!ref_upload((void **)&g_h.betaRow, betaRowPtr, (size_t)(nm * nm + 1) * 4, "beta rows") ||
+                !ref_upload((void **)&g_h.betaCol, betaColInd, (size_t)nnz * 4, "beta columns") ||
+                !ref_upload((void **)&g_h.betaVal, betaVal, (size_t)nnz * 8, "beta values"))
+                return;
+        }
+        g_h.nm2 = nm2;
+        g_h.nm2p = nm2p;
+        g_h.gnchunks = nch;
+    }
+    g_h.nm = nm;
+    g_h.nq = nq;
+}
+
+// Fills hs with NaN so that a failed call cannot pass for a computed batch.
+static void ref_poison(double *hs, long long count)
+{
+    if (hs && count > 0)
+        std::fill(hs, hs + count, std::nan(""));
 }
 
 void solveH_cuda(int nm, int nm2, int nq, int batchSize, double *alphas, double *hs, int useGaunt,
                  int useGauntSparse)
 {
-    (void)nm2; (void)useGauntSparse;
     std::lock_guard<std::mutex> lk(g_refMutex);
-    if (useGaunt || !g_h.chunks || nm != g_h.nm || nq != g_h.nq || batchSize > g_h.cap) {
-        fprintf(stderr, "[c3d_b200] solveH_cuda: not initialised for this size (call solveHInit_cuda "
-                        "with MN_USE_GAUNT_COEF false)\n");
+    const long long count = batchSize > 0 ? (long long)batchSize * nm * nm : 0;
+    if (batchSize <= 0)
+        return;
+    bool ready = g_h.chunks && nm == g_h.nm && nq == g_h.nq && batchSize <= g_h.cap && alphas && hs;
+    if (ready && useGaunt)
+        ready = g_h.gchunks && nm2 == g_h.nm2 && (useGauntSparse ? g_h.betaVal != nullptr
+                                                                 : g_h.betaT != nullptr);
+    if (!ready) {
+        fprintf(stderr, "[c3d_b200] solveH_cuda: not initialised for nm=%d nm2=%d nq=%d batch=%d "
+                        "useGaunt=%d sparse=%d (call solveHInit_cuda with the same sizes and "
+                        "tables); hs set to NaN\n",
+                nm, nm2, nq, batchSize, useGaunt, useGauntSparse);
+        ref_poison(hs, count);
         return;
     }
-    cudaMemcpy(g_h.alphas, alphas, (size_t)batchSize * nm * 8, cudaMemcpyHostToDevice);
-    cudaError_t e = launch_hessian_batch(nm, g_h.nchunks, g_h.chunks, g_h.alphas, batchSize, g_h.hs,
-                                         g_h.errorFlag, 0);
+    cudaError_t e = cudaMemcpy(g_h.alphas, alphas, (size_t)batchSize * nm * 8, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        if (useGaunt)
+            e = launch_gaunt_batch(nm, g_h.nm2, g_h.nm2p, g_h.gnchunks, g_h.gchunks, g_h.alphas,
+                                   batchSize, g_h.betaT, g_h.betaRow, g_h.betaCol, g_h.betaVal,
+                                   useGauntSparse ? 1 : 0, g_h.hs, g_h.errorFlag, 0);
+        else
+            e = launch_hessian_batch(nm, g_h.nchunks, g_h.chunks, g_h.alphas, batchSize, g_h.hs,
+                                     g_h.errorFlag, 0);
+    }
     if (e == cudaSuccess)
-        e = cudaMemcpy(hs, g_h.hs, (size_t)batchSize * nm * nm * 8, cudaMemcpyDeviceToHost);
-    if (e != cudaSuccess)
-        fprintf(stderr, "[c3d_b200] solveH_cuda: %s\n", cudaGetErrorString(e));
+        e = cudaMemcpy(hs, g_h.hs, (size_t)count * 8, cudaMemcpyDeviceToHost);
+    int flag = 0;
+    if (e == cudaSuccess)
+        e = cudaMemcpy(&flag, g_h.errorFlag, 4, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        fprintf(stderr, "[c3d_b200] solveH_cuda: %s; hs set to NaN\n", cudaGetErrorString(e));
+        ref_poison(hs, count);
+        return;
+    }
+    if (flag) {
+        cudaMemset(g_h.errorFlag, 0, 4);
+        fprintf(stderr, "[c3d_b200] solveH_cuda: a bounded device wait gave up; hs set to NaN\n");
+        ref_poison(hs, count);
+    }
 }
 
 static struct {

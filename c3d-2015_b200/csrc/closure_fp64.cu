@@ -470,6 +470,123 @@ __global__ void __launch_bounds__(W * 32, 1)
         }
 }
 
+// Gaunt-form batched Hessians (src/opt/fobj.cpp:34-102 with useGaunt; the reference's
+// solveH_cuda with useGaunt = 1, src/cuda/cuda_solveH.cu:224-241). Eight vectors per CTA:
+// per staged chunk of QC directions each warp forms one vector's w_q e^{alpha.m_q} (exponent
+// summed in the reference's order, unfused), then the extended moments
+// mom_k = sum_q w_q e^{alpha.m_q} p2_qk accumulate on the FP64 tensor pipe as an
+// [8 vectors x nm2p] tile (A = the weights, B = the staged p2 rows; each warp owns every
+// eighth 8-column tile). H_ij = sum_k beta_ijk mom_k follows for j >= i and is mirrored, as
+// the CPU path does: over all nm2 harmonics in ascending order (dense beta, stored
+// transposed, betaT[k nm^2 + i nm + j]) or over the CSR row of (i, j) in its order.
+// Chunk layout (rows of QCP doubles): the nm rows of M^T, the nm2p rows of M2^T (zero past
+// nm2), the weight row.
+template <int TPW>
+__global__ void __launch_bounds__(256, 1)
+    gaunt_batch_kernel(int nm, int nm2, int nm2p, int nchunks, const double *__restrict__ chunks,
+                       const double *__restrict__ alphas, long long n,
+                       const double *__restrict__ betaT, const int *__restrict__ rowPtr,
+                       const int *__restrict__ colInd, const double *__restrict__ val, int sparse,
+                       double *__restrict__ hs, int *errorFlag)
+{
+    constexpr int GB = 8; // vectors per CTA: the DMMA row tile
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    const int CH = (nm + nm2p + 1) * QCP;
+    double *stage = reinterpret_cast<double *>(smem_raw); // GSTAGES chunks
+    double *sAlpha = stage + GSTAGES * CH;                 // GB x nm
+    double *sT = sAlpha + GB * nm;                         // GB x QCP weights of the chunk
+    double *sMom = sT + GB * QCP;                          // GB x nm2p extended moments
+    uint64_t *full = reinterpret_cast<uint64_t *>(sMom + GB * nm2p);
+    __shared__ int s_abort;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const long long b0 = (long long)blockIdx.x * GB;
+    const uint32_t chunkBytes = CH * sizeof(double);
+    const int ntiles = nm2p / 8;
+    for (int e = tid; e < GB * nm; e += blockDim.x) {
+        long long b = b0 + e / nm;
+        sAlpha[e] = b < n ? alphas[b * nm + e % nm] : 0.0;
+    }
+    if (tid == 0) {
+        for (int s = 0; s < GSTAGES; ++s)
+            mbar_init(&full[s], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        s_abort = 0;
+        for (int k = 0; k < GSTAGES && k < nchunks; ++k) {
+            mbar_expect_tx(&full[k], chunkBytes);
+            bulk_g2s(stage + k * CH, chunks + (size_t)k * CH, chunkBytes, &full[k]);
+        }
+    }
+    __syncthreads();
+    double acc[TPW][2];
+#pragma unroll
+    for (int t = 0; t < TPW; ++t)
+        acc[t][0] = acc[t][1] = 0.0;
+    for (int k = 0; k < nchunks; ++k) {
+        uint32_t s = k % GSTAGES, parity = (k / GSTAGES) & 1u;
+        if (!mbar_wait(&full[s], parity))
+            s_abort = 1;
+        if (__syncthreads_or(s_abort)) {
+            if (tid == 0)
+                atomicExch(errorFlag, 1);
+            return;
+        }
+        const double *ch = stage + s * CH;
+        {
+            const double *al = sAlpha + warp * nm;
+            double z = 0.0;
+            for (int i = 0; i < nm; ++i)
+                z = __dadd_rn(z, __dmul_rn(al[i], ch[i * QCP + lane]));
+            sT[warp * QCP + lane] = exp(z) * ch[(nm + nm2p) * QCP + lane];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int g = 0; g < QC / 4; ++g) {
+            double a = sT[(lane >> 2) * QCP + 4 * g + (lane & 3)];
+#pragma unroll
+            for (int t = 0; t < TPW; ++t) {
+                int j = warp + 8 * t;
+                if (j < ntiles)
+                    dmma(acc[t][0], acc[t][1], a,
+                         ch[(nm + 8 * j + (lane >> 2)) * QCP + 4 * g + (lane & 3)]);
+            }
+        }
+        __syncthreads();
+        if (tid == 0 && k + GSTAGES < nchunks) {
+            mbar_expect_tx(&full[s], chunkBytes);
+            bulk_g2s(stage + s * CH, chunks + (size_t)(k + GSTAGES) * CH, chunkBytes, &full[s]);
+        }
+    }
+#pragma unroll
+    for (int t = 0; t < TPW; ++t) {
+        int j = warp + 8 * t;
+        if (j < ntiles) {
+            int col = 8 * j + 2 * (lane & 3);
+            sMom[(lane >> 2) * nm2p + col] = acc[t][0];
+            sMom[(lane >> 2) * nm2p + col + 1] = acc[t][1];
+        }
+    }
+    __syncthreads();
+    const int nmm = nm * nm;
+    for (int e = tid; e < GB * nmm; e += blockDim.x) {
+        int c = e / nmm, ij = e % nmm, i = ij / nm, j = ij % nm;
+        long long b = b0 + c;
+        if (b >= n || j < i)
+            continue;
+        const double *mom = sMom + c * nm2p;
+        double h = 0.0;
+        if (sparse) {
+            for (int p = rowPtr[ij]; p < rowPtr[ij + 1]; ++p)
+                h = __dadd_rn(h, __dmul_rn(mom[colInd[p]], val[p]));
+        } else {
+            for (int kk = 0; kk < nm2; ++kk)
+                h = __dadd_rn(h, __dmul_rn(mom[kk], betaT[(size_t)kk * nmm + ij]));
+        }
+        double *H = hs + b * (long long)nmm;
+        H[i * nm + j] = h;
+        H[j * nm + i] = h;
+    }
+}
+
 // ---------------------------------------------------------------- host launcher
 
 struct ClosureLaunch {
@@ -589,6 +706,38 @@ static cudaError_t launch_hessian_t(int nm, int nchunks, const double *chunks, c
     if (grid < 1)
         return cudaSuccess;
     kern<<<(unsigned)grid, W * 32, smem, st>>>(nm, nchunks, chunks, alphas, n, hs, errorFlag);
+    return cudaGetLastError();
+}
+
+// Shared memory of gaunt_batch_kernel (0 if the sizes do not fit).
+size_t gaunt_batch_smem(int nm, int nm2p)
+{
+    size_t b = ((size_t)GSTAGES * (nm + nm2p + 1) * QCP + 8 * (size_t)(nm + QCP + nm2p)) *
+                   sizeof(double) + GSTAGES * sizeof(uint64_t);
+    return b <= 227 * 1024 ? b : 0;
+}
+
+cudaError_t launch_gaunt_batch(int nm, int nm2, int nm2p, int nchunks, const double *chunks,
+                               const double *alphas, long long n, const double *betaT,
+                               const int *rowPtr, const int *colInd, const double *val,
+                               int sparse, double *hs, int *errorFlag, cudaStream_t st)
+{
+    size_t smem = gaunt_batch_smem(nm, nm2p);
+    int tpw = (nm2p / 8 + 7) / 8;
+    if (smem == 0 || nm < 1 || nm > 64 || nm2p % 8 != 0 || tpw < 1 || tpw > 4)
+        return cudaErrorInvalidValue;
+    if (n < 1)
+        return cudaSuccess;
+    void (*kern)(int, int, int, int, const double *, const double *, long long, const double *,
+                 const int *, const int *, const double *, int, double *, int *) =
+        tpw == 1 ? gaunt_batch_kernel<1> : tpw == 2 ? gaunt_batch_kernel<2>
+                                         : tpw == 3 ? gaunt_batch_kernel<3> : gaunt_batch_kernel<4>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess)
+        return e;
+    long long grid = (n + 7) / 8;
+    kern<<<(unsigned)grid, 256, smem, st>>>(nm, nm2, nm2p, nchunks, chunks, alphas, n, betaT, rowPtr,
+                                            colInd, val, sparse, hs, errorFlag);
     return cudaGetLastError();
 }
 

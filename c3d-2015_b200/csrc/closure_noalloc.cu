@@ -22,6 +22,7 @@
 #include "../../include/c3d_b200.h"
 #include "c3d_common.cuh"
 
+#include <cmath>
 #include <cstdio>
 #include <mutex>
 #include <string>
@@ -147,6 +148,15 @@ c3d_status c3d_closure_vectors_noalloc(int nm, int nq, const double *M, const do
         set_last_error("c3d_closure_vectors_noalloc: ladder length must be in [1, 16]");
         return C3D_ERR_INVALID;
     }
+    // Without these checks a cell would run to the pass budget (maxIter < 1) or never meet
+    // its stopping test (tol <= 0), and the caller would only see status -1 or 3.
+    auto positive = [](double v) { return std::isfinite(v) && v > 0.0; };
+    if (opts->maxIter < 1 || !positive(opts->tol) || !positive(opts->condHMax) ||
+        (opts->batched && !positive(opts->tolGamma))) {
+        set_last_error("c3d_closure_vectors_noalloc: maxIter must be >= 1 and tol, tolGamma and "
+                       "condHMax positive and finite");
+        return C3D_ERR_INVALID;
+    }
     if (n == 0)
         return C3D_OK;
     unsigned char *base = nullptr;
@@ -206,6 +216,51 @@ c3d_status c3d_closure_vectors_noalloc(int nm, int nq, const double *M, const do
     if (e != cudaSuccess) {
         set_last_error(std::string("c3d_closure_vectors_noalloc: ") + cudaGetErrorString(e));
         return C3D_ERR_CUDA;
+    }
+    return C3D_OK;
+}
+
+// Outcome of the last c3d_closure_vectors_noalloc call on this device: synchronises the
+// stream, then reads the kernel's error flag and failure count out of the static array
+// (cudaMemcpyFromSymbol into host variables; nothing is allocated) and clears both.
+c3d_status c3d_closure_vectors_noalloc_check(void *stream, long long *failed)
+{
+    if (failed)
+        *failed = 0;
+    unsigned char *base = nullptr;
+    int numSMs = 1;
+    c3d_status s = noalloc_scratch_ptr(&base, &numSMs);
+    if (s != C3D_OK)
+        return s;
+    cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);
+    int flag = 0;
+    unsigned long long nfail = 0;
+    if (e == cudaSuccess)
+        e = cudaMemcpyFromSymbol(&flag, g_noalloc_scratch, sizeof(int), OFF_ERROR,
+                                 cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess)
+        e = cudaMemcpyFromSymbol(&nfail, g_noalloc_scratch, sizeof(nfail), OFF_FAIL,
+                                 cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && (flag || nfail)) {
+        const unsigned char zero[16] = {};
+        e = cudaMemcpyToSymbol(g_noalloc_scratch, zero, sizeof(zero), OFF_FAIL,
+                               cudaMemcpyHostToDevice);
+    }
+    if (e != cudaSuccess) {
+        set_last_error(std::string("c3d_closure_vectors_noalloc_check: ") + cudaGetErrorString(e));
+        return C3D_ERR_CUDA;
+    }
+    if (failed)
+        *failed = (long long)nfail;
+    if (flag) {
+        set_last_error("c3d_closure_vectors_noalloc: a bounded device wait gave up; cells whose "
+                       "status is -1 were not solved");
+        return C3D_ERR_TIMEOUT;
+    }
+    if (nfail) {
+        set_last_error("c3d_closure_vectors_noalloc: " + std::to_string(nfail) +
+                       " cell(s) failed: u0 <= 0 or regularisation ladder exhausted");
+        return C3D_ERR_CLOSURE;
     }
     return C3D_OK;
 }

@@ -56,14 +56,19 @@ void solveFluxKinetic_cuda(int nx, int ny, int nz, int nm, int nq, double dx, do
 
 /* Batched Hessians H_b = sum_q w_q exp(alpha_b . m_q) m_q m_q^T for batchSize
  * multiplier vectors (host, batchSize*nm), written to hs (host, batchSize*nm*nm,
- * row-major, symmetric). Replaces src/cuda/cuda_headers.h:15-17. Only the
- * direct quadrature form is provided (useGaunt must be 0). */
+ * row-major, symmetric). Replaces src/cuda/cuda_headers.h:15-17. useGaunt = 1 forms
+ * H from the extended moments over p2 and beta (src/cuda/cuda_solveH.cu:224-241):
+ * dense beta with useGauntSparse = 0, the CSR table with 1. If the sizes or tables
+ * were not set up by solveHInit_cuda, or the device fails, a message goes to stderr
+ * and hs is filled with NaN (never left unwritten). */
 void solveH_cuda(int nm, int nm2, int nq, int batchSize, double *alphas, double *hs, int useGaunt,
                  int useGauntSparse);
 
 /* One-time set-up for solveH_cuda (tables to the device); replaces
  * src/cuda/cuda_headers.h:19-21. p2/beta/betaVal/betaColInd/betaRowPtr may be
- * NULL when useGaunt is 0. */
+ * NULL when useGaunt is 0; with useGaunt = 1, beta (dense, [nm*nm][nm2]) serves
+ * useGauntSparse = 0 and the CSR arrays serve useGauntSparse = 1 (either may be NULL
+ * if that mode is not used). nm <= 64, nm2 <= 232. */
 void solveHInit_cuda(int nm, int nm2, int nq, int batchSize, double *w, double *p, double *p2,
                      double *beta, double *betaVal, int *betaColInd, int *betaRowPtr, int useGaunt);
 
@@ -234,6 +239,14 @@ c3d_status c3d_set_certificate(c3d_ctx *ctx, int on);
  * (runLen 0: min(64, nz)). */
 c3d_status c3d_autotune(c3d_ctx *ctx, int *qChunk, int *runLen, double *msPerCall);
 
+/* Safety bounds of the closure (no counterpart in the reference, which loops until each cell
+ * converges or aborts): at most maxRounds work-list rounds per closure (engine 0; default
+ * 2^24), after which the closure returns C3D_ERR_TIMEOUT with the unfinished cells' state
+ * left as it was, and at most passBudget Hessian and line-search passes per cell (default
+ * 2^40), after which the cell ends with status 3 and c3d_sync reports C3D_ERR_CLOSURE.
+ * Values <= 0 restore the defaults. */
+c3d_status c3d_set_limits(c3d_ctx *ctx, long long maxRounds, long long passBudget);
+
 /* Face-ghost mirroring of the grid closure (engine 0; on by default). The reference solves
  * every cell, ghosts included (src/update.cpp:51-53, 119-123). A face ghost holds a copy of
  * its periodic image's moments, so when its multipliers (the warm start) also equal the
@@ -288,10 +301,21 @@ typedef struct {
  * C3D_ERR_INVALID. The first call on a device looks up that array's device address
  * (cudaGetSymbolAddress), so make that first call before any stream capture. All
  * calls share the array: calls that overlap on the GPU race, so order them (one
- * stream). Stream-ordered; returns without synchronising. */
+ * stream). Stream-ordered; returns without synchronising. opts must hold maxIter >= 1
+ * and positive finite tol, condHMax (and tolGamma under the batched rules). Status per
+ * cell: 0 converged, 1 u0 <= 0, 2 ladder exhausted, -1 not reached because a bounded
+ * device wait gave up; c3d_closure_vectors_noalloc_check reports the call's outcome. */
 c3d_status c3d_closure_vectors_noalloc(int nm, int nq, const double *M, const double *w,
                                        long long n, double *u, double *alpha, int *iters,
                                        int *status, const c3d_closure_opts *opts, void *stream);
+
+/* Outcome of the last c3d_closure_vectors_noalloc call on the current device, read out of
+ * the same static array (allocates nothing): waits for stream, then returns
+ * C3D_ERR_TIMEOUT if a bounded device wait gave up (the kernel stopped early; unsolved
+ * cells keep their inputs), C3D_ERR_CLOSURE if cells failed (their number in *failed, which
+ * may be NULL), else C3D_OK, and clears both records. Call it after each call whose
+ * outcome matters, before the next call. */
+c3d_status c3d_closure_vectors_noalloc_check(void *stream, long long *failed);
 
 /* Event timing on the context's stream around every grid closure (kind 0), kinetic flux
  * (1), ghost fill (2) and Euler stage (3) (off by default). c3d_timing_get returns the

@@ -249,6 +249,56 @@ def test_reference_entry_points(oracle):
     assert (fg[ghost] == 0).all()
 
 
+@pytest.mark.parametrize("N,Q", [(2, 12), (4, 12), (6, 10), (7, 12)])
+def test_reference_solveH_gaunt(oracle, N, Q):
+    """solveH_cuda with useGaunt = 1 (the reference deck's default, MN_USE_GAUNT_COEF true),
+    dense beta (useGauntSparse 0) and CSR beta (1), against the oracle's Gaunt Hessian
+    (src/opt/fobj.cpp:34-102) to 1e-13; the batch is ragged (not a multiple of 8)."""
+    import ctypes
+    T = oracle.tables(N, Q, gaunt=True)
+    nm, nm2, nq = T["nm"], T["nm2"], T["nq"]
+    L = c3d.lib()
+    dp = ctypes.POINTER(ctypes.c_double)
+    ip = ctypes.POINTER(ctypes.c_int)
+    B = 53
+    rng = np.random.default_rng(N)
+    al = rng.standard_normal((B, nm)) * 0.3
+    al[:, 0] = rng.uniform(-2.0, 1.0, B)
+    L.solveHInit_cuda(nm, nm2, nq, B, T["w"].ctypes.data_as(dp), T["M"].ctypes.data_as(dp),
+                      T["M2"].ctypes.data_as(dp), T["beta"].ctypes.data_as(dp),
+                      T["betaVal"].ctypes.data_as(dp), T["betaCol"].ctypes.data_as(ip),
+                      T["betaRow"].ctypes.data_as(ip), 1)
+    for sparse, mode in ((0, 1), (1, 2)):
+        hs = np.full(B * nm * nm, -7.0)
+        L.solveH_cuda(nm, nm2, nq, B, al.ctypes.data_as(dp), hs.ctypes.data_as(dp), 1, sparse)
+        hs = hs.reshape(B, nm, nm)
+        assert np.isfinite(hs).all()
+        opts = make_opts(nm, nq, nm2=nm2, hess_mode=mode)
+        for b in range(B):
+            ho = oracle.hessian(opts, T, al[b].copy())
+            assert np.allclose(hs[b], ho, rtol=1e-13, atol=1e-14 * np.abs(ho).max()), (sparse, b)
+            assert np.array_equal(hs[b], hs[b].T)
+
+
+def test_reference_solveH_uninitialised_sizes_poison():
+    """A call whose sizes were not set up by solveHInit_cuda leaves no stale values: hs is
+    filled with NaN (and a message goes to stderr) instead of being left unwritten."""
+    import ctypes
+    q = c3d.quadrature(1, 4)
+    nm, nq = q["nm"], q["nq"]
+    L = c3d.lib()
+    dp = ctypes.POINTER(ctypes.c_double)
+    L.solveHInit_cuda(nm, 0, nq, 4, q["w"].ctypes.data_as(dp), q["M"].ctypes.data_as(dp), None,
+                      None, None, None, None, 0)
+    al = np.zeros(4 * nm)
+    hs = np.zeros(4 * nm * nm)
+    L.solveH_cuda(nm, 9, nq, 4, al.ctypes.data_as(dp), hs.ctypes.data_as(dp), 1, 1)
+    assert np.isnan(hs).all()
+    hs[:] = 0.0
+    L.solveH_cuda(nm, 0, nq, 4, al.ctypes.data_as(dp), hs.ctypes.data_as(dp), 0, 0)
+    assert np.isfinite(hs).all() and (hs != 0).any()
+
+
 def _gaunt_csr(T, threshold):
     nm, nm2 = T["nm"], T["nm2"]
     beta = T["beta"].reshape(nm * nm, nm2)

@@ -10,7 +10,10 @@ The test allocates the inputs and outputs (the caller's job), calls the entry po
 through the C ABI twice in a row on different vectors, and checks each call against the
 context-based c3d_closure_vectors on the same inputs: identical Newton iteration counts
 and statuses, multipliers and moments within 1e-10 relative (the tolerance of the
-closure parity tests). This file is named to be collected last.
+closure parity tests). It also checks that a call leaves the device's free memory and
+torch's reserved pool unchanged, runs the largest sizes the static array accepts
+(nm = 64, nq = 2048, which fill it to its last byte), and reads a call's outcome with
+c3d_closure_vectors_noalloc_check. This file is named to be collected last.
 """
 import ctypes
 
@@ -64,31 +67,65 @@ def _existing(q, u, a0):
     return out
 
 
-def _noalloc(q, u, a0, dM, dw):
-    import torch
+def _lib():
     L = c3d.lib()
     L.c3d_closure_vectors_noalloc.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
                                               ctypes.c_void_p, ctypes.c_longlong,
                                               ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                               ctypes.c_void_p, ctypes.POINTER(ClosureOpts),
                                               ctypes.c_void_p]
-    n, nm = u.shape
-    du = torch.tensor(u, device="cuda")
-    da = torch.tensor(a0, device="cuda")
-    it = torch.zeros(n, dtype=torch.int32, device="cuda")
-    st = torch.zeros(n, dtype=torch.int32, device="cuda")
+    L.c3d_closure_vectors_noalloc_check.argtypes = [ctypes.c_void_p,
+                                                    ctypes.POINTER(ctypes.c_longlong)]
+    return L
+
+
+def _opts():
     o = ClosureOpts()
     o.batched, o.maxIter, o.tol, o.tolGamma, o.condHMax = 1, 100, 1e-8, 1.1, 1e10
     o.nreg = len(LADDER)
     for i, r in enumerate(LADDER):
         o.reg[i] = r
+    return o
+
+
+def _check(L, stream):
+    failed = ctypes.c_longlong(-1)
+    rc = L.c3d_closure_vectors_noalloc_check(stream, ctypes.byref(failed))
+    return rc, failed.value
+
+
+def _noalloc(q, u, a0, dM, dw):
+    import torch
+    L = _lib()
+    n, nm = u.shape
+    du = torch.tensor(u, device="cuda")
+    da = torch.tensor(a0, device="cuda")
+    it = torch.zeros(n, dtype=torch.int32, device="cuda")
+    st = torch.zeros(n, dtype=torch.int32, device="cuda")
+    o = _opts()
     stream = torch.cuda.current_stream()
     rc = L.c3d_closure_vectors_noalloc(nm, q["nq"], dM.data_ptr(), dw.data_ptr(), n,
                                        du.data_ptr(), da.data_ptr(), it.data_ptr(),
                                        st.data_ptr(), ctypes.byref(o), stream.cuda_stream)
     c3d.check(rc, "c3d_closure_vectors_noalloc")
+    rc, failed = _check(L, stream.cuda_stream)
+    c3d.check(rc, "c3d_closure_vectors_noalloc_check")
+    assert failed == 0
     torch.cuda.synchronize()
     return du.cpu().numpy(), da.cpu().numpy(), it.cpu().numpy(), st.cpu().numpy()
+
+
+def _compare(q, n, seed, dM, dw):
+    u, a0 = _vectors(q, n, seed)
+    ue, ae, ite, ste = _existing(q, u, a0)
+    un, an, itn, stn = _noalloc(q, u, a0, dM, dw)
+    assert (stn == ste).all()
+    assert (stn >= 0).all()
+    assert np.array_equal(itn, ite)
+    for x, y in ((an, ae), (un, ue)):
+        rel = np.linalg.norm(x - y, axis=1) / np.linalg.norm(y, axis=1)
+        assert rel.max() <= 1e-10, rel.max()
+    return ite
 
 
 def test_noalloc_matches_existing_entry_point_twice():
@@ -97,31 +134,97 @@ def test_noalloc_matches_existing_entry_point_twice():
     dM = torch.tensor(q["M"], device="cuda")
     dw = torch.tensor(q["w"], device="cuda")
     for call, seed in enumerate((11, 12)):  # two calls in a row, different vectors
-        u, a0 = _vectors(q, 3000, seed)
-        ue, ae, ite, ste = _existing(q, u, a0)
-        un, an, itn, stn = _noalloc(q, u, a0, dM, dw)
-        assert (stn == ste).all(), call
-        assert (stn >= 0).all(), call
-        assert np.array_equal(itn, ite), call
-        for x, y in ((an, ae), (un, ue)):
-            rel = np.linalg.norm(x - y, axis=1) / np.linalg.norm(y, axis=1)
-            assert rel.max() <= 1e-10, (call, rel.max())
-        assert ite.max() > 1  # the vectors need real Newton work
+        ite = _compare(q, 3000, seed, dM, dw)
+        assert ite.max() > 1, call  # the vectors need real Newton work
+
+
+def test_noalloc_largest_sizes():
+    """nm = 64 (M_7) and nq = 2048 (Q = 32): the basis fills the static array to its end."""
+    import torch
+    q = c3d.quadrature(7, 32)
+    assert (q["nm"], q["nq"]) == (64, 2048)
+    dM = torch.tensor(q["M"], device="cuda")
+    dw = torch.tensor(q["w"], device="cuda")
+    for seed in (21, 22):
+        _compare(q, 300, seed, dM, dw)
+
+
+def test_noalloc_allocates_nothing():
+    """After a first call, a second call changes neither the device's free memory
+    (cudaMemGetInfo) nor torch's reserved pool."""
+    import torch
+    L = _lib()
+    q = c3d.quadrature(4, 20)
+    u, a0 = _vectors(q, 2000, 31)
+    n, nm = u.shape
+    dM = torch.tensor(q["M"], device="cuda")
+    dw = torch.tensor(q["w"], device="cuda")
+    du = torch.tensor(u, device="cuda")
+    da = torch.tensor(a0, device="cuda")
+    it = torch.zeros(n, dtype=torch.int32, device="cuda")
+    st = torch.zeros(n, dtype=torch.int32, device="cuda")
+    o = _opts()
+    stream = torch.cuda.current_stream().cuda_stream
+
+    def call():
+        rc = L.c3d_closure_vectors_noalloc(nm, q["nq"], dM.data_ptr(), dw.data_ptr(), n,
+                                           du.data_ptr(), da.data_ptr(), it.data_ptr(),
+                                           st.data_ptr(), ctypes.byref(o), stream)
+        c3d.check(rc, "c3d_closure_vectors_noalloc")
+        c3d.check(_check(L, stream)[0], "c3d_closure_vectors_noalloc_check")
+
+    call()  # first call: set-up (symbol address) and module loading
+    du.copy_(torch.tensor(u, device="cuda"))
+    da.copy_(torch.tensor(a0, device="cuda"))
+    torch.cuda.synchronize()
+    free1, reserved1 = torch.cuda.mem_get_info()[0], torch.cuda.memory_reserved()
+    call()
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free1
+    assert torch.cuda.memory_reserved() == reserved1
+    assert (st.cpu().numpy() == 0).all()
+
+
+def test_noalloc_reports_failed_cells():
+    """A vector with u0 <= 0 gets status 1 and the call's outcome is C3D_ERR_CLOSURE with
+    one failed cell; the check clears the record, so the next check reports C3D_OK."""
+    import torch
+    L = _lib()
+    q = c3d.quadrature(2, 12)
+    u, a0 = _vectors(q, 64, 41)
+    u[5, 0] = -1.0
+    n, nm = u.shape
+    dM = torch.tensor(q["M"], device="cuda")
+    dw = torch.tensor(q["w"], device="cuda")
+    du = torch.tensor(u, device="cuda")
+    da = torch.tensor(a0, device="cuda")
+    st = torch.zeros(n, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    rc = L.c3d_closure_vectors_noalloc(nm, q["nq"], dM.data_ptr(), dw.data_ptr(), n,
+                                       du.data_ptr(), da.data_ptr(), None, st.data_ptr(),
+                                       ctypes.byref(_opts()), stream)
+    c3d.check(rc, "c3d_closure_vectors_noalloc")
+    rc, failed = _check(L, stream)
+    assert rc == 4 and failed == 1, (rc, failed)  # C3D_ERR_CLOSURE
+    s = st.cpu().numpy()
+    assert s[5] == 1 and (np.delete(s, 5) == 0).all()
+    assert _check(L, stream) == (0, 0)
 
 
 def test_noalloc_rejects_sizes_beyond_scratch():
     import torch
-    L = c3d.lib()
-    L.c3d_closure_vectors_noalloc.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
-                                              ctypes.c_void_p, ctypes.c_longlong,
-                                              ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
-                                              ctypes.c_void_p, ctypes.POINTER(ClosureOpts),
-                                              ctypes.c_void_p]
-    o = ClosureOpts()
-    o.nreg, o.maxIter = 1, 10
+    L = _lib()
+    o = _opts()
     buf = torch.zeros(16, dtype=torch.float64, device="cuda")
     p = buf.data_ptr()
     rc = L.c3d_closure_vectors_noalloc(81, 800, p, p, 1, p, p, None, None, ctypes.byref(o), None)
     assert rc == 1 and "nm must be in [1, 64]" in L.c3d_last_error().decode()
     rc = L.c3d_closure_vectors_noalloc(25, 4096, p, p, 1, p, p, None, None, ctypes.byref(o), None)
     assert rc == 1 and "2048" in L.c3d_last_error().decode()
+    for field, bad in (("maxIter", 0), ("tol", 0.0), ("tol", float("nan")), ("condHMax", -1.0),
+                       ("tolGamma", float("inf"))):
+        o = _opts()
+        setattr(o, field, bad)
+        rc = L.c3d_closure_vectors_noalloc(25, 800, p, p, 1, p, p, None, None, ctypes.byref(o),
+                                           None)
+        assert rc == 1 and "positive and finite" in L.c3d_last_error().decode(), field
