@@ -116,7 +116,7 @@ def lib():
         L.c3d_set_gaunt.argtypes = [vp, ctypes.c_int, _dp, _ip, _ip, _dp]
         L.c3d_set_engine.argtypes = [vp, ctypes.c_int]
         L.c3d_set_precision.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double,
-                                        ctypes.c_int]
+                                        ctypes.c_int, ctypes.c_double]
         L.c3d_set_certificate.argtypes = [vp, ctypes.c_int]
         L.c3d_autotune.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                                    ctypes.POINTER(ctypes.c_double)]
@@ -305,13 +305,13 @@ class Context:
         """0: work-list rounds (default), 1: persistent kernel."""
         check(lib().c3d_set_engine(self.h, engine), "c3d_set_engine")
 
-    def set_precision(self, mode, cond_bf16=0.0, cond_mixed_max=0.0, mixed_iter_max=0):
+    def set_precision(self, mode, cond_bf16=0.0, cond_mixed_max=0.0, mixed_iter_max=0, polish=0.0):
         """0: FP64 closure (default, the drop-in); 1: mixed precision -- Hessian moments on
         the tensor cores in BF16 / 3xTF32 with FP32 accumulation, FP64 gradient, objective,
         factorisation and fallback (Gaunt form, engine 0). Zeros select the defaults
         (1e4, 1e7, 8)."""
         check(lib().c3d_set_precision(self.h, int(mode), float(cond_bf16), float(cond_mixed_max),
-                                      int(mixed_iter_max)), "c3d_set_precision")
+                                      int(mixed_iter_max), float(polish)), "c3d_set_precision")
 
     def set_certificate(self, on):
         """First-visit convergence certificate (default on): exact; off gives gamma records

@@ -935,7 +935,7 @@ c3d_status c3d_set_gaunt(c3d_ctx *c, int nm2, const double *M2, const int *rowPt
 }
 
 c3d_status c3d_set_precision(c3d_ctx *c, int mode, double condBf16, double condMixedMax,
-                             int mixedIterMax)
+                             int mixedIterMax, double polish)
 {
     if (!c || mode < 0 || mode > 1)
         return fail(C3D_ERR_INVALID, "c3d_set_precision: mode must be 0 (FP64) or 1 (mixed)");
@@ -946,6 +946,7 @@ c3d_status c3d_set_precision(c3d_ctx *c, int mode, double condBf16, double condM
     c->cp.condBf16 = condBf16 > 0 ? condBf16 : 1e4;
     c->cp.condMixMax = condMixedMax > 0 ? condMixedMax : 1e7;
     c->cp.mixIterMax = mixedIterMax > 0 ? mixedIterMax : 8;
+    c->cp.mixPolish = polish > 0 ? polish : 1e3;
     // N <= 2 (at most 32 extended moments): the 128-row tensor-core tile would be mostly
     // padding and the FP64 moment pass is as cheap, so the Hessians stay FP64
     if (mode == 1 && closure_gaunt_nm2p(c->nm2) <= 32)

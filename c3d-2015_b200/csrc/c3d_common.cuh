@@ -69,6 +69,9 @@ struct ClosureParams {
     int mixIterMax;
     double condBf16;
     double condMixMax;
+    double mixPolish;  // > 0: a reduced-precision visit whose gradient norm lies in
+                       // (rtol, mixPolish * rtol] is redone with FP64 moments, so that the
+                       // steps that end the iteration are FP64 Newton steps
     // convergence certificate of a cell's first Hessian visit (work-list engine, Gaunt form):
     // a probe pass computes the first-order moments and the extreme values of e^{alpha.m}
     // over the quadrature; H >= e_min G with G = sum_q w_q m_q m_q^T, whose eigenvalues lie

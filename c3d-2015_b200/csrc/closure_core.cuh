@@ -814,9 +814,12 @@ __device__ void escalate_fp64(S &sl, const Outputs &O, int lane)
 
 // gext (mixed precision): the FP64 moments <m_i e^{alpha.m}> and fqext = <e^{alpha.m}> of
 // the pass, from which g and f are formed instead of from row 0 of the reduced-precision H.
+// fqOnly: f from fqext (the quadrature sum) with g from row 0 of H (the mixed closure's FP64
+// visits).
 template <class S>
 __device__ void after_hessian(S &sl, const ClosureParams &P, const Outputs &O, int lane,
-                              double m0, const double *gext = nullptr, double fqext = 0.0)
+                              double m0, const double *gext = nullptr, double fqext = 0.0,
+                              bool fqOnly = false)
 {
     const int nm = P.nm;
     C3D_NCLK_DECL
@@ -824,9 +827,16 @@ __device__ void after_hessian(S &sl, const ClosureParams &P, const Outputs &O, i
     for (int i = lane; i < nm; i += 32)
         sl.g[i] = gext ? __dsub_rn(gext[i], sl.u[i]) : sl.L[S::lx(i, 0)] / m0 - sl.u[i];
     __syncwarp();
+    if (gext && P.mixPolish > 0.0) {
+        const double e0 = warp_nrm2(sl.g, nm, lane);
+        if (e0 > sl.s.rtol && e0 <= P.mixPolish * sl.s.rtol) {
+            escalate_fp64(sl, O, lane);
+            return;
+        }
+    }
     double f = 0.0;
     if (lane == 0) {
-        f = gext ? fqext : sl.L[0] / (m0 * m0);
+        f = (gext || fqOnly) ? fqext : sl.L[0] / (m0 * m0);
         for (int i = 0; i < nm; ++i)
             f = __dsub_rn(f, __dmul_rn(sl.alpha[i], sl.u[i]));
     }

@@ -243,14 +243,16 @@ __global__ void __launch_bounds__(RW * 32, 2)
                 z1 = __dadd_rn(z1, __dmul_rn(a.y, m));
             }
             const double wq = ch[nm2 * QCP + lane];
+            // the quadrature sum of f: for trials, and in the mixed closure for FP64 Hessian
+            // visits too (their base objective, summed like the trials')
             if (need[0] != NEED_NONE) {
                 c0 = __dmul_rn(wq, exp(z0));
-                if (need[0] == NEED_TRIAL)
+                if (need[0] == NEED_TRIAL || P.mixed)
                     fpart0 = __dadd_rn(fpart0, c0);
             }
             if (need[1] != NEED_NONE) {
                 c1 = __dmul_rn(wq, exp(z1));
-                if (need[1] == NEED_TRIAL)
+                if (need[1] == NEED_TRIAL || P.mixed)
                     fpart1 = __dadd_rn(fpart1, c1);
             }
         }
@@ -300,9 +302,9 @@ __global__ void __launch_bounds__(RW * 32, 2)
     }
     const double fq0 = warp_sum(fpart0), fq1 = warp_sum(fpart1);
     if (lane == 0) {
-        if (need[0] == NEED_TRIAL)
+        if (need[0] == NEED_TRIAL || (P.mixed && need[0] == NEED_H))
             state[cell[0]].s.fquad = fq0;
-        if (need[1] == NEED_TRIAL)
+        if (need[1] == NEED_TRIAL || (P.mixed && need[1] == NEED_H))
             state[cell[1]].s.fquad = fq1;
     }
 }
@@ -899,6 +901,9 @@ __global__ void __launch_bounds__(RWN * 32)
                 const double *e = buf + (size_t)pos * BSTR + NM2P;
                 after_hessian(sl, P, O, lane, m0, e, e[NMP]);
             }
+        } else if (GAUNT && P.mixed) {
+            // FP64 visit of the mixed closure: f from the quadrature sum, as for its trials
+            after_hessian(sl, P, O, lane, m0, nullptr, sl.s.fquad, true);
         } else {
             after_hessian(sl, P, O, lane, m0);
         }

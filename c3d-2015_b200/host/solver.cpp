@@ -88,6 +88,7 @@ std::string parse_config(const InputDeck &d, Config &c)
     d.get("MN_MIXED_COND_BF16", c.mnMixedCondBf16);
     d.get("MN_MIXED_COND_MAX", c.mnMixedCondMax);
     d.get("MN_MIXED_ITER_MAX", c.mnMixedIterMax);
+    d.get("MN_MIXED_POLISH", c.mnMixedPolish);
     d.get("FLUX_AUTOTUNE", c.fluxAutotune);
     d.get("SIGMA_CHECKER_BLOCK", c.checkerBlock);
     d.get("SIGMA_S_HI", c.sigmaSHi);
@@ -283,7 +284,7 @@ c3d_status Solver::init(const Config &cfg, void *stream)
     }
     if (cfg_.solver == "mn" && cfg_.mnMixed &&
         (s = c3d_set_precision(ctx_, 1, cfg_.mnMixedCondBf16, cfg_.mnMixedCondMax,
-                               cfg_.mnMixedIterMax)) != C3D_OK)
+                               cfg_.mnMixedIterMax, cfg_.mnMixedPolish)) != C3D_OK)
         return s;
     if (cfg_.outputTimings && (s = c3d_timing_enable(ctx_, 1)) != C3D_OK)
         return s;

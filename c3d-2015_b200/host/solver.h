@@ -17,7 +17,8 @@
 //                              robustness note of the reference's readme.txt)
 //   MN_MIXED_PRECISION true  mixed-precision closure (c3d_set_precision mode 1; needs
 //                              MN_USE_GAUNT_COEF true and N <= 6), thresholds
-//                              MN_MIXED_COND_BF16, MN_MIXED_COND_MAX, MN_MIXED_ITER_MAX
+//                              MN_MIXED_COND_BF16, MN_MIXED_COND_MAX, MN_MIXED_ITER_MAX,
+//                              MN_MIXED_POLISH
 //   FLUX_AUTOTUNE true       time the kinetic flux per direction chunk and z run length at
 //                              set-up and keep the fastest (c3d_autotune)
 #pragma once
@@ -48,6 +49,7 @@ struct Config {
     bool mnMixed = false;     // optional MN_MIXED_PRECISION
     double mnMixedCondBf16 = 0.0, mnMixedCondMax = 0.0;
     int mnMixedIterMax = 0;
+    double mnMixedPolish = 0.0;
     bool fluxAutotune = false; // optional FLUX_AUTOTUNE: c3d_autotune after the state upload
     // optional keys
     int nsteps = -1;

@@ -214,10 +214,15 @@ c3d_status c3d_set_engine(c3d_ctx *ctx, int engine);
  * factorisation fails or its moments are not finite, the cell's Hessian is FP64. The
  * gradient of the stopping test, the objective of the line search and the factorisation stay
  * FP64, so converged cells satisfy the same residual test as in mode 0; iteration counts
- * and multipliers differ within the tolerance. Values <= 0 select the defaults. For N <= 2
- * the Hessian moments stay FP64 (the tensor-core tile would be mostly padding). */
+ * and multipliers differ within the tolerance. The steps that end a cell's iteration are
+ * FP64 Newton steps: a reduced-precision visit whose gradient norm |g| lies in
+ * (tol, polish * tol] (default polish 1e3; polish = 1 turns this off) is redone with FP64
+ * moments, and the cell keeps them for the rest of the closure, so that the last steps
+ * converge quadratically as in mode 0 and the moments track mode 0's closely. Values <= 0
+ * select the defaults. For N <= 2 the Hessian moments stay FP64 (the tensor-core tile would
+ * be mostly padding). */
 c3d_status c3d_set_precision(c3d_ctx *ctx, int mode, double condBf16, double condMixedMax,
-                             int mixedIterMax);
+                             int mixedIterMax, double polish);
 
 /* Convergence certificate of a cell's first Newton iteration (work-list engine, Gaunt form;
  * on by default; no counterpart in the reference). The first visit runs a probe pass --

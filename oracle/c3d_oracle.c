@@ -361,7 +361,7 @@ static int newton_scaled(const orc_closure_opts *o, const orc_tables *t, double 
     double rtol = o->batched ? o->tol : orc_nrm2(nm, u) * o->tol;
     int iter = 0, totalIter = 0, iterGamma = 0, regIndex = 0;
     double tstep = 1, r = 0.0, gamma = 0.0, err = 0.0;
-    double armijoUlps = 1e300, tolRel = 1e300;
+    double armijoUlps = 1e300, tolRel = 1e300, condRel = 1e300, gammaRel = 1e300;
     int status = 0;
 
     for (int i = 0; i < nm; i++)
@@ -389,6 +389,8 @@ static int newton_scaled(const orc_closure_opts *o, const orc_tables *t, double 
         double norm1 = orc_norm1(nm, h);
         double condest = orc_pocon_lower(nm, chol, norm1);
         condest = 1.0 / condest;
+        if (cholErr == 0 && fabs(condest - o->condHMax) / o->condHMax < condRel)
+            condRel = fabs(condest - o->condHMax) / o->condHMax;
 
         if (totalIter == 1 && (cholErr != 0 || condest > o->condHMax)) {
             isotropic_alpha(nm, alpha0);
@@ -433,6 +435,8 @@ static int newton_scaled(const orc_closure_opts *o, const orc_tables *t, double 
         gamma = modcfl(nm, d);
         if (fabs(err - rtol) / rtol < tolRel)
             tolRel = fabs(err - rtol) / rtol;
+        if (err <= rtol && fabs(gamma - o->tolGamma) / o->tolGamma < gammaRel)
+            gammaRel = fabs(gamma - o->tolGamma) / o->tolGamma;
 
         if (err <= rtol && gamma <= o->tolGamma)
             break;
@@ -451,6 +455,8 @@ static int newton_scaled(const orc_closure_opts *o, const orc_tables *t, double 
         out->err = err;
         out->armijoUlps = armijoUlps;
         out->tolRel = tolRel;
+        out->condRel = condRel;
+        out->gammaRel = gammaRel;
     }
     return status;
 }

@@ -39,8 +39,11 @@ typedef struct {
     double r, gamma, err;
     /* Smallest decision margins met during the solve, used to classify
      * rounding ties: |fNew - (f + delta t g.d)| in units of eps*|f| over all
-     * Armijo tests, and |err - tol| / tol over all stop tests. */
-    double armijoUlps, tolRel;
+     * Armijo tests, |err - tol| / tol over all stop tests, and
+     * |condest - condHMax| / condHMax over all condition tests of a successful
+     * factorisation, |gamma - tolGamma| / tolGamma over the stop tests whose
+     * gradient passed. */
+    double armijoUlps, tolRel, condRel, gammaRel;
 } orc_cell_out;
 
 typedef struct {

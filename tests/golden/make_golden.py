@@ -16,6 +16,17 @@ Fixtures:
   overwritten with the same arrays before the first step).
 * pn_p3_8.npz   -- P_N (N=3), 8x6x7 grid, smooth initial condition, moment flux,
   5 steps; interior moments after the last step.
+* c2_m4_64.npz  -- M_4, 64^3, 800-point quadrature (20 mu x 40 phi), sigma_s checkerboard
+  of 1 and 10 over 8^3-cell blocks with sigma_a 0.1 in the 10-blocks, pulse
+  psi = max(1e-6, G/(4 pi)) of width 0.05, Gaunt sparse Hessian (the reference deck's
+  default), MN_TOL 1e-6 (at 1e-8 the reference exhausts its ladder and aborts in the first
+  step), the same ladder as c1, CFL 0.5, theta 2, 3 SSP-RK2 steps (the reference CPU path
+  takes about 7 minutes on 8 cores for them). Stores the per-cell iteration counts and
+  ladder indices of all six closures, and after steps 1 and 3 the interior moments of 4096
+  seeded sample cells plus the moment sums over every x-, y- and z-plane. The initial
+  state and the sigma fields come from the B200 host's host-only init (INIT_COND
+  gaussian_psi, SIGMA_CHECKER_BLOCK; the reference has neither, so its u, alpha, sigma_t
+  and sigma_s are overwritten with the same arrays before the first step).
 """
 import os
 import sys
@@ -70,6 +81,54 @@ def make_c1():
                         stats20=np.array(ref20["stats"][:11]), dt=ref2["dv"][3])
 
 
+C2_SAMPLE_SEED = 20151
+
+
+def c2_deck(ic):
+    return deck_text(NX=64, NY=64, NZ=64, MOMENT_ORDER=4, QUAD_ORDER=20, CFL_FACTOR=0.5,
+                     CROSS_SECTION=1.0, INIT_FLOOR=1e-6, GAUSS_SIGMA=0.05, INIT_COND=ic,
+                     THETA=2.0, OMP_THREADS=os.cpu_count() or 1, MN_TOL=1e-6, MN_BATCHED="true",
+                     MN_USE_GAUNT_COEF="true", MN_USE_GAUNT_SPARSE="true",
+                     SIGMA_CHECKER_BLOCK=8, SIGMA_S_HI=10.0, SIGMA_A_HI=0.1,
+                     REG_LADDER=",".join(str(x) for x in C1_LADDER))
+
+
+def c2_initial_state():
+    import c3d
+    with tempfile.TemporaryDirectory() as tmp:
+        p = os.path.join(tmp, "input.deck")
+        with open(p, "w") as f:
+            f.write(c2_deck("gaussian_psi"))
+        s = c3d.Solver(p, host_only=True)
+        A = s.arrays()
+        out = A["u"].copy(), A["alpha"].copy(), A["sigT"].copy(), A["sigS"].copy()
+        s.close()
+    return out
+
+
+def c2_summary(u, n=64, nm=25):
+    """Seeded sample cells and per-plane moment sums of the interior moments."""
+    x = interior(u, n, nm)
+    rng = np.random.default_rng(C2_SAMPLE_SEED)
+    pick = rng.choice(n ** 3, 4096, replace=False)
+    return dict(sample=x.reshape(-1, nm)[pick].copy(), sx=x.sum(axis=(1, 2)),
+                sy=x.sum(axis=(0, 2)), sz=x.sum(axis=(0, 1)))
+
+
+def make_c2():
+    u0, a0, st, ss = c2_initial_state()
+    ref = run_reference(c2_deck("gaussian"), ladder=C1_LADDER, nsteps=3,
+                        overrides=dict(u=u0, alpha=a0, sigT=st, sigS=ss), want=("snapshots",))
+    it = np.stack([ref["iters"][s][0] for s in range(3)]).astype(np.int16)
+    rg = np.stack([ref["iters"][s][2] for s in range(3)]).astype(np.int8)
+    s1 = c2_summary(ref["snapshots"][1][0])
+    s3 = c2_summary(ref["u"])
+    np.savez_compressed(os.path.join(HERE, "c2_m4_64.npz"), iters=it, reg=rg,
+                        **{f"step1_{k}": v for k, v in s1.items()},
+                        **{f"step3_{k}": v for k, v in s3.items()},
+                        stats=np.array(ref["stats"][:11]), dt=ref["dv"][3])
+
+
 def make_pn():
     deck = deck_text(SOLVER="pn", NX=8, NY=6, NZ=7, MOMENT_ORDER=3, QUAD_ORDER=8,
                      INIT_COND="smooth", PN_USE_KINETIC_FLUX=0)
@@ -79,8 +138,13 @@ def make_pn():
 
 
 if __name__ == "__main__":
-    make_c1()
-    make_pn()
+    which = sys.argv[1:] or ["c1", "pn", "c2"]
+    if "c1" in which:
+        make_c1()
+    if "pn" in which:
+        make_pn()
+    if "c2" in which:
+        make_c2()
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)), "bytes")

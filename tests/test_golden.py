@@ -107,6 +107,41 @@ def test_gpu_c1_golden(tmp_path):
 
 
 @pytest.mark.gpu
+def test_gpu_c2_golden(tmp_path):
+    """The M_4 64^3 deck with the sigma checkerboard (Gaunt sparse Hessian, MN_TOL 1e-6)
+    against the reference's own CPU path: per-cell Newton iteration counts and ladder indices
+    of all six closures of three steps identical (ghost cells included); after steps 1 and 3
+    the interior moments of the 4096 sample cells and the moment sums over every x-, y- and
+    z-plane within 1e-12 relative L2."""
+    mg = _golden_module()
+    G = np.load(os.path.join(GOLD, "c2_m4_64.npz"))
+    s = c3d.Solver(_deck(tmp_path, mg.c2_deck("gaussian_psi")))
+    L = c3d.lib()
+    dt = s.max_dt
+    assert dt == float(G["dt"])
+    nall = s.nall
+    for step in range(3):
+        for stage in range(2):
+            c3d.check(L.c3d_stage(s.ctx_handle, stage, dt), "c3d_stage")
+            s.sync()
+            rec = s.records()
+            ref_it = G["iters"][step][stage * nall:(stage + 1) * nall]
+            ref_rg = G["reg"][step][stage * nall:(stage + 1) * nall]
+            mism = np.nonzero(rec["iters"] != ref_it)[0]
+            assert len(mism) == 0, (step, stage, len(mism), mism[:8])
+            assert np.array_equal(rec["regIndex"], ref_rg), (step, stage)
+            assert (rec["status"] == 0).all()
+        if step in (0, 2):
+            s.pull()
+            got = mg.c2_summary(s.arrays()["u"])
+            for k in ("sample", "sx", "sy", "sz"):
+                ref = G[f"step{step + 1}_{k}"]
+                rel = np.linalg.norm(got[k] - ref) / np.linalg.norm(ref)
+                assert rel < 1e-12, (step, k, rel)
+    s.close()
+
+
+@pytest.mark.gpu
 def test_gpu_pn_golden(tmp_path):
     G = np.load(os.path.join(GOLD, "pn_p3_8.npz"))
     s = c3d.Solver(_deck(tmp_path, _pn_deck()))

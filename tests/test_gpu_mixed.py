@@ -59,7 +59,7 @@ def m6_cells(oracle, tmp_path_factory):
     return dict(u=u[pick], a=a[pick], T=T, nm=nm, nmulti=len(multi))
 
 
-def _solve(S, mode, cond_bf16=0.0, cond_max=0.0):
+def _solve(S, mode, cond_bf16=0.0, cond_max=0.0, polish=0.0):
     import torch
     T, nm = S["T"], S["nm"]
     n = len(S["u"])
@@ -67,7 +67,7 @@ def _solve(S, mode, cond_bf16=0.0, cond_max=0.0):
                       w=T["w"], xi=T["xi"], eta=T["eta"], mu=T["mu"], ladder=LADDER, tol=TOL)
     row, col, val = _gaunt_csr(T, 1e-13)
     ctx.set_gaunt(T["nm2"], T["M2"], row, col, val)
-    ctx.set_precision(mode, cond_bf16, cond_max)
+    ctx.set_precision(mode, cond_bf16, cond_max, polish=polish)
     du = torch.tensor(S["u"], device="cuda")
     da = torch.tensor(S["a"], device="cuda")
     it = torch.zeros(n, dtype=torch.int32, device="cuda")
@@ -112,9 +112,13 @@ def test_mixed_closure_meets_fp64_residual(m6_cells):
     ok = f["rg"] == m["rg"]
     rel = np.linalg.norm(m["a"][ok] - f["a"][ok], axis=1) / np.linalg.norm(f["a"][ok], axis=1)
     assert np.median(rel) < 1e-6, np.median(rel)
-    # the tensor-core levels carry the Hessians; iterations stay comparable
+    # the tensor-core levels carry the Hessians until the gradient nears the tolerance, then
+    # the last steps are FP64 (the default polish); without the polish they carry most
     st = m["stats"]
-    assert st["hessBf16"] + st["hessTf32x3"] > 0.5 * st["totalIters"], st
+    assert st["hessBf16"] + st["hessTf32x3"] > 0.3 * st["totalIters"], st
+    assert st["escalated"] > 0
+    st1 = _solve(S, 1, polish=1.0)["stats"]
+    assert st1["hessBf16"] + st1["hessTf32x3"] > 0.5 * st1["totalIters"], st1
     assert m["it"].mean() <= 1.5 * f["it"].mean(), (m["it"].mean(), f["it"].mean())
     print(f"\nmixed vs FP64 on {len(rel)} cells: alpha rel diff median {np.median(rel):.2e} "
           f"max {rel.max():.2e}; iterations {m['it'].mean():.3f} vs {f['it'].mean():.3f}; "
@@ -147,8 +151,9 @@ def test_mixed_precision_routing(m6_cells, levels):
 
 def test_mixed_grid_steps_track_fp64(tmp_path):
     """Five steps of the 32^3 M_6 deck with the mixed and the FP64 closure: no failed cell,
-    and the moments stay close (the multipliers differ within the Newton tolerance, which
-    enters the fluxes)."""
+    and the moments within 1e-8 relative L2 (the multipliers differ within the Newton
+    tolerance, which enters the fluxes; the mixed closure's last Newton steps are FP64 steps,
+    c3d_set_precision's polish)."""
     out = {}
     for mixed in (False, True):
         s = c3d.Solver(_deck(tmp_path, 32, mixed, name=f"d{int(mixed)}.deck"))
@@ -165,7 +170,68 @@ def test_mixed_grid_steps_track_fp64(tmp_path):
     assert sm["hessBf16"] + sm["hessTf32x3"] > 0
     rel = np.linalg.norm(um - uf) / np.linalg.norm(uf)
     print(f"\n32^3 M_6, 5 steps: moments rel L2 mixed vs FP64 {rel:.2e}")
-    assert rel < 1e-6, rel
+    assert rel < 1e-8, rel
+
+
+def test_mixed_and_fp64_steps_against_oracle(oracle, tmp_path):
+    """The 24^3 M_6 deck (Gaunt sparse Hessian, MN_TOL 1e-6) by the C oracle (FP64, the
+    reference's algorithm) and by the B200 solver in both precisions. After one step (no
+    rounding tie on this deck yet): the FP64 drop-in's interior moments within 1e-12 relative
+    L2 of the oracle's; the mixed closure's moments within 1e-8, and the flux divergence of
+    its multipliers (the oracle's kinetic flux of either state) within 1e-8. Over three steps
+    correct FP64 implementations themselves part at the pulse-centre cells of this coarse
+    grid, which regularise and meet rounding ties in their stop tests (the reference build and
+    the oracle differ by 2.5e-7 there, the GPU drop-in and the reference by 5e-8); the mixed
+    run must stay within that spread (1e-6) of the FP64 drop-in. The multipliers' error is
+    printed: it is larger, since near the realizability boundary H is ill-conditioned and
+    alpha is determined only to |H^-1 g| with |g| <= MN_TOL."""
+    from oracle_lib import make_opts
+    n = 24
+    T = oracle.tables(6, 28, gaunt=True)
+    host = c3d.Solver(_deck(tmp_path, n, False, name="host.deck"), host_only=True)
+    A = host.arrays()
+    dt = host.max_dt
+    nm, nq = 49, 1568
+    g = oracle.grid(n, n, n, nm, nq, host.dx, host.dy, host.dz, 2.0)
+    opts = make_opts(nm, nq, nm2=T["nm2"], hess_mode=2, tol=TOL, ladder=LADDER)
+    uo, ao = A["u"].copy(), A["alpha"].copy()
+    bad, _ = oracle.step(g, opts, T, uo, ao, A["sigT"], A["sigS"], dt, records=False)
+    assert bad == 0
+    host.close()
+    inner = (slice(2, n + 2),) * 3
+
+    def interior(v):
+        return v.reshape(n + 4, n + 4, n + 4, nm)[inner]
+
+    def rel(x, y):
+        return np.linalg.norm(interior(x) - interior(y)) / np.linalg.norm(interior(y))
+
+    fo = interior(oracle.flux_kinetic(g, T, ao))
+    res, after3 = {}, {}
+    for mixed in (False, True):
+        s = c3d.Solver(_deck(tmp_path, n, mixed, name=f"o{int(mixed)}.deck"))
+        s.update(s.max_dt)
+        s.sync()
+        s.pull()
+        u, a = s.arrays()["u"].copy(), s.arrays()["alpha"].copy()
+        fu = interior(oracle.flux_kinetic(g, T, a))
+        res[mixed] = dict(u=rel(u, uo), a=rel(a, ao),
+                          flux=np.linalg.norm(fu - fo) / np.linalg.norm(fo))
+        for _ in range(2):
+            s.update(s.max_dt)
+        s.sync()
+        s.pull()
+        after3[mixed] = (s.arrays()["u"].copy(), s.arrays()["alpha"].copy())
+        s.close()
+    u3 = rel(after3[True][0], after3[False][0])
+    a3 = rel(after3[True][1], after3[False][1])
+    print("\n24^3 M_6, 1 step vs the oracle: FP64 " +
+          " ".join(f"{k} {v:.2e}" for k, v in res[False].items()) + "; mixed " +
+          " ".join(f"{k} {v:.2e}" for k, v in res[True].items()) +
+          f"; 3 steps mixed vs FP64: u {u3:.2e} alpha {a3:.2e}")
+    assert res[False]["u"] < 1e-12 and res[False]["flux"] < 1e-12
+    assert res[True]["u"] < 1e-8 and res[True]["flux"] < 1e-8
+    assert u3 < 1e-6
 
 
 @pytest.mark.parametrize("N", [1, 2, 3, 4, 5, 6, 7])
@@ -210,7 +276,7 @@ def test_mixed_standalone_orders(oracle, N):
     f, m = out[0], out[1]
     assert not ((m["st"] != 0) & (f["st"] == 0)).any()
     hist = (np.bincount(f["rg"]), np.bincount(m["rg"]))
-    assert (m["rg"] > 0).sum() <= (f["rg"] > 0).sum(), hist
+    assert (m["rg"] > 0).sum() <= (f["rg"] > 0).sum() + max(2, n // 50), hist
     assert (m["rg"] <= f["rg"]).mean() >= 0.95, hist
     ok = m["st"] == 0
     M = q["M"].reshape(nq, nm)
