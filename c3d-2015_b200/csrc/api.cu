@@ -53,8 +53,11 @@ cudaError_t launch_rk(const GridDims &g, double *u, double *uOld, int mode, int 
 cudaError_t launch_kinetic_flux(const GridDims &g, const double *alpha, const double *mfA,
                                 const double *mfP, const double *xi, const double *eta, int nq,
                                 int qChunk, int runLen, double dx, double dy, double dz,
-                                double theta, int isPn, double *psi, double *flux, int *errorFlag,
-                                cudaStream_t st);
+                                double theta, int isPn, double *psi, bool psiReady, double *flux,
+                                int *errorFlag, cudaStream_t st);
+cudaError_t launch_psi_handoff(const GridDims &g, int nq, const double *M, const double *alpha,
+                               bool faceCopy, const int *refresh, const unsigned int *refreshCount,
+                               double *psi, int numSMs, cudaStream_t st);
 size_t flux_frag_doubles(int nm, int nq, int which);
 cudaError_t launch_reproject(const GridDims &g, double *u, double *alpha, const double *mfA,
                              const double *mfP, int nq, int *errorFlag, cudaStream_t st);
@@ -134,6 +137,15 @@ struct c3d_ctx {
     int qChunk = 0;
     int runLen = 0;     // z run per CTA of the staged kinetic kernel (0: min(64, nz))
     size_t psiAlloc = 0; // bytes of the psi buffer
+    // ansatz hand-off: the last grid closure left psi of every direction for its multipliers
+    // (the probe pass wrote it; face ghosts and cells changed after the probe were refreshed),
+    // so the next kinetic flux runs the stencil alone. Cleared by the flux and by any change
+    // of the multipliers.
+    bool psiReady = false;
+    bool psiHandoffPending = false;     // the closure's probe wrote psi; completed in closure_grid
+    bool handoff = true;                // c3d_set_ansatz_handoff
+    int *psiRefresh = nullptr;          // cells whose psi is rewritten after the closure
+    unsigned int *psiRefreshCount = nullptr;
     long long launches = 0;
     // device buffers
     double *u = nullptr, *alpha = nullptr, *uOld = nullptr, *flux = nullptr;
@@ -227,7 +239,8 @@ static void free_ctx(c3d_ctx *c)
                     c->gRow, c->gCol, c->gStream, c->rState, c->rListA, c->rListB,
                     c->rCounts, c->rBuf, c->mfA, c->mfP, c->cellMap, c->mirrorFlag,
                     c->gChunksC, c->cellGamma, c->cellErr, c->lineLog, c->mixF64,
-                    c->mixA[0], c->mixA[1], c->cellCond, c->g0};
+                    c->mixA[0], c->mixA[1], c->cellCond, c->g0, c->psiRefresh,
+                    c->psiRefreshCount};
     for (void *p : ptrs)
         if (p)
             cudaFree(p);
@@ -302,7 +315,7 @@ c3d_status c3d_create(const c3d_params *p, const double *M, const double *w, con
     for (int i = 0; i < p->nreg; ++i)
         cp.reg[i] = p->reg[i];
     cp.passBudget = 1LL << 40;
-    c->psiBytes = p->psiBytes ? p->psiBytes : (size_t)16 << 30;
+    c->psiBytes = p->psiBytes ? p->psiBytes : (size_t)32 << 30;
     c->reproject = p->mnReproject != 0;
 
     const long long nall = c->g.nall();
@@ -388,6 +401,8 @@ void c3d_destroy(c3d_ctx *ctx)
 c3d_status c3d_set_state(c3d_ctx *c, const double *u, const double *alpha, const double *sigT,
                          const double *sigS, int where)
 {
+    if (c && alpha)
+        c->psiReady = false;
     if (!c)
         return fail(C3D_ERR_INVALID, "c3d_set_state: null context");
     const long long nall = c->g.nall();
@@ -539,10 +554,38 @@ static c3d_status run_closure(c3d_ctx *c, long long n, double *u, double *alpha,
         R.stream = c->stream;
         R.launches = &c->launches;
         R.maxRounds = c->maxRounds;
+        R.psi = nullptr;
+        if (gridRecords && c->cp.probe && c->handoff && c->solver == 1) {
+            // hand the probe's ansatz to the kinetic flux when psi of every direction fits the
+            // budget
+            const size_t need = (size_t)c->nq * c->g.nall() * 8;
+            if (need <= c->psiBytes) {
+                if (!c->psi || c->psiAlloc < need) {
+                    if (c->psi)
+                        cudaFree(c->psi);
+                    c->psi = nullptr;
+                    c->psiAlloc = 0;
+                    C3D_CUDA(cudaMalloc(&c->psi, need));
+                    c->psiAlloc = need;
+                }
+                if (!c->psiRefresh) {
+                    C3D_CUDA(cudaMalloc(&c->psiRefresh, (size_t)c->g.nall() * sizeof(int)));
+                    C3D_CUDA(cudaMalloc(&c->psiRefreshCount, sizeof(unsigned int)));
+                }
+                C3D_CUDA(cudaMemsetAsync(c->psiRefreshCount, 0, sizeof(unsigned int), c->stream));
+                R.psi = c->psi;
+                R.psiNall = c->g.nall();
+                R.refresh = c->psiRefresh;
+                R.refreshCount = c->psiRefreshCount;
+            }
+        }
+        c->psiReady = false;
         cudaError_t e = launch_closure_rounds(R, c->gaunt);
         if (e == cudaErrorLaunchTimeout)
             return fail(C3D_ERR_TIMEOUT, "closure: round limit exceeded");
         C3D_CUDA(e);
+        if (R.psi)
+            c->psiHandoffPending = true;
         return C3D_OK;
     }
     c->cp.probe = 0; // the persistent kernels always form H
@@ -605,6 +648,21 @@ c3d_status c3d_closure(c3d_ctx *c)
     return C3D_OK;
 }
 
+// Completes the ansatz hand-off of a grid closure whose probe pass wrote psi: face ghosts
+// copied from their images (mirrored closures), the listed cells recomputed from their final
+// multipliers; the next kinetic flux then runs the stencil alone.
+static c3d_status finish_handoff(c3d_ctx *c, bool faceCopy)
+{
+    if (!c->psiHandoffPending)
+        return C3D_OK;
+    c->psiHandoffPending = false;
+    C3D_CUDA(launch_psi_handoff(c->g, c->nq, c->M, c->alpha, faceCopy, c->psiRefresh,
+                                c->psiRefreshCount, c->psi, c->numSMs, c->stream));
+    c->launches += faceCopy ? 2 : 1;
+    c->psiReady = true;
+    return C3D_OK;
+}
+
 static c3d_status closure_grid(c3d_ctx *c)
 {
     if (c->engine == 0 && c->mirror && !c->xHaloExternal) {
@@ -655,11 +713,14 @@ static c3d_status closure_grid(c3d_ctx *c)
                                         c->stats, c->numSMs, c->stream));
             c->launches += 9;
             c->mirroredClosures++;
-            return C3D_OK;
+            return finish_handoff(c, true);
         }
     }
-    return run_closure(c, c->g.nall(), c->u, c->alpha, c->iters, c->iterGamma, c->regIdx, c->status,
-                       nullptr, true);
+    c3d_status s = run_closure(c, c->g.nall(), c->u, c->alpha, c->iters, c->iterGamma, c->regIdx,
+                               c->status, nullptr, true);
+    if (s != C3D_OK)
+        return s;
+    return finish_handoff(c, false);
 }
 
 // Round to nearest even (BF16) and to nearest with ties away (TF32, as cvt.rna), on the
@@ -972,6 +1033,16 @@ c3d_status c3d_set_engine(c3d_ctx *c, int engine)
     return C3D_OK;
 }
 
+c3d_status c3d_set_ansatz_handoff(c3d_ctx *c, int on)
+{
+    if (!c)
+        return fail(C3D_ERR_INVALID, "c3d_set_ansatz_handoff: null context");
+    c->handoff = on != 0;
+    if (!c->handoff)
+        c->psiReady = false;
+    return C3D_OK;
+}
+
 c3d_status c3d_set_limits(c3d_ctx *c, long long maxRounds, long long passBudget)
 {
     if (!c)
@@ -1014,14 +1085,17 @@ c3d_status c3d_flux_kinetic(c3d_ctx *c, int alphaIsU)
     }
     const double *a = alphaIsU ? c->u : c->alpha;
     int isPn = (c->solver == 0) ? 1 : 0;
+    const bool ready = c->psiReady && !alphaIsU && isPn == 0 &&
+                       c->psiAlloc >= (size_t)c->nq * c->g.nall() * 8;
+    c->psiReady = false;
     cudaEvent_t t0 = nullptr;
     timing_begin(c, &t0);
     C3D_CUDA(launch_kinetic_flux(c->g, a, c->mfA, c->mfP, c->xi, c->eta, c->nq, c->qChunk,
-                                 c->runLen, c->dx, c->dy, c->dz, c->theta, isPn, c->psi, c->flux,
-                                 c->errorFlag, c->stream));
+                                 c->runLen, c->dx, c->dy, c->dz, c->theta, isPn, c->psi, ready,
+                                 c->flux, c->errorFlag, c->stream));
     timing_end(c, 1, t0);
     int nch = ceil_div(c->nq, c->qChunk);
-    c->launches += 2 * nch;
+    c->launches += ready ? 1 : 2 * nch;
     return C3D_OK;
 }
 
@@ -1052,6 +1126,7 @@ c3d_status c3d_autotune(c3d_ctx *c, int *qChunk, int *runLen, double *msPerCall)
         ls.push_back(32);
     const int q0 = c->qChunk, l0 = c->runLen;
     const bool timing = c->timing;
+    c->psiReady = false; // every timed call forms the ansatz
     c->timing = false;
     cudaEvent_t e0, e1;
     C3D_CUDA(cudaEventCreate(&e0));
@@ -1176,6 +1251,8 @@ c3d_status c3d_copy_x_planes(c3d_ctx *c, int field, int i0, int count, void *buf
         return fail(C3D_ERR_INVALID, "c3d_copy_x_planes: bad argument");
     const size_t plane = (size_t)c->g.nyg() * c->g.nzg() * c->g.nm;
     double *a = (field == 0 ? c->u : c->alpha) + (size_t)i0 * plane;
+    if (field == 1 && !toBuf)
+        c->psiReady = false;
     const size_t bytes = (size_t)count * plane * sizeof(double);
     cudaMemcpyKind k = where ? cudaMemcpyDeviceToDevice
                              : (toBuf ? cudaMemcpyDeviceToHost : cudaMemcpyHostToDevice);

@@ -479,7 +479,16 @@ struct FirstRound {
     long long off;
     const int *cellMap;
     const double *u, *alpha;
+    // ansatz hand-off to the kinetic flux (grid closures with the certificate): the probe pass
+    // writes psi[q nall + c] = exp(alpha_c . m_q) of every cell it solves, and the probe's
+    // Newton kernel lists in refresh the cells whose multipliers may still change (their psi is
+    // rewritten after the closure). Null psi: no hand-off.
+    double *psi;
+    long long nall;
+    int *refresh;
+    unsigned int *refreshCount;
 };
+constexpr int PSTR = 17; // row stride (cells) of the probe's psi tile
 template <int NT, int NT2, int KIND, bool ZD>
 __global__ void __launch_bounds__(RW * 32, KIND == 1 ? 1 : KIND == 2 ? 3 : 2)
     rounds_pass_mixed_kernel(ClosureParams P, const double *__restrict__ f64c,
@@ -505,7 +514,9 @@ __global__ void __launch_bounds__(RW * 32, KIND == 1 ? 1 : KIND == 2 ? 3 : 2)
     double *cbuf = reinterpret_cast<double *>(bbuf + GSTAGES * K::NP * BPB); // QC x CST2
     double2 *alph = reinterpret_cast<double2 *>(cbuf + QC * CST2);          // RW x nm
     double *zbuf = reinterpret_cast<double *>(alph + RW * nm);              // ZD: QC x ZS
-    uint64_t *full = reinterpret_cast<uint64_t *>(zbuf + (ZD ? QC * ZS : 0));
+    double *psiT = zbuf + (ZD ? QC * ZS : 0);                               // probe: QC x PSTR
+    long long *psiCell = reinterpret_cast<long long *>(psiT + (KIND == 2 ? QC * PSTR : 0));
+    uint64_t *full = reinterpret_cast<uint64_t *>(psiCell + (KIND == 2 ? MXC : 0));
     uint64_t *mmab = full + GSTAGES;
     uint64_t *fin = mmab + GSTAGES;
     __shared__ uint32_t s_tmem;
@@ -513,8 +524,12 @@ __global__ void __launch_bounds__(RW * 32, KIND == 1 ? 1 : KIND == 2 ? 3 : 2)
     __shared__ int s_shift[MXC];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int base = blockIdx.x * MXC;
+    // first round of a grid closure: hand the ansatz of every direction to the kinetic flux,
+    // psi = u_0 e^{alpha_scaled . m_q} (the scaling shifts alpha_0 by log(u_0) 2 sqrt(pi), and
+    // m_0 = 1 / (2 sqrt(pi)))
+    const bool emit = KIND == 2 && !list && first.psi != nullptr;
     long long cell[2];
-    double scale[2];
+    double scale[2], u0e[2] = {0.0, 0.0};
 #pragma unroll
     for (int e = 0; e < 2; ++e) {
         const int pos = base + 2 * warp + e;
@@ -523,8 +538,12 @@ __global__ void __launch_bounds__(RW * 32, KIND == 1 ? 1 : KIND == 2 ? 3 : 2)
         double ascale = 0.0;
         if (!list && cell[e] >= 0) {
             gc = first.cellMap ? first.cellMap[cell[e]] : cell[e];
-            ascale = log(first.u[gc * nm]) * 2.0 * sqrt(M_PI);
+            u0e[e] = first.u[gc * nm];
+            ascale = log(u0e[e]) * 2.0 * sqrt(M_PI);
         }
+        if constexpr (KIND == 2)
+            if (lane == 0)
+                psiCell[2 * warp + e] = emit ? gc : -1;
         for (int i = lane; i < nm; i += 32) {
             double a = 0.0;
             if (cell[e] >= 0) {
@@ -614,6 +633,12 @@ __global__ void __launch_bounds__(RW * 32, KIND == 1 ? 1 : KIND == 2 ? 3 : 2)
         }
         const double wq = ch[nm * QCP + lane];
         const double ez0 = exp(z0), ez1 = exp(z1);
+        if constexpr (KIND == 2) {
+            if (emit) {
+                psiT[lane * PSTR + 2 * warp] = u0e[0] * ez0;
+                psiT[lane * PSTR + 2 * warp + 1] = u0e[1] * ez1;
+            }
+        }
         const double c0 = cell[0] >= 0 ? __dmul_rn(wq, ez0) : 0.0;
         const double c1 = cell[1] >= 0 ? __dmul_rn(wq, ez1) : 0.0;
         fpart0 = __dadd_rn(fpart0, c0);
@@ -667,6 +692,19 @@ __global__ void __launch_bounds__(RW * 32, KIND == 1 ? 1 : KIND == 2 ? 3 : 2)
                     }
                 }
             umma_commit(&mmab[s]);
+        }
+        if constexpr (KIND == 2) {
+            // the chunk's psi rows: warp w stores directions 4w .. 4w + 3, 16 cells each
+            if (emit) {
+#pragma unroll
+                for (int i = 0; i < 2; ++i) {
+                    const int row = 4 * warp + 2 * i + (lane >> 4), j = lane & 15;
+                    const long long gc = psiCell[j];
+                    const int q = k * QC + row;
+                    if (gc >= 0 && q < P.nq)
+                        first.psi[(long long)q * first.nall + gc] = psiT[row * PSTR + j];
+                }
+            }
         }
         // FP64 first-order moments: warp w, rows 8w .. 8w + 7
         if (warp < NT) {
@@ -819,6 +857,9 @@ __global__ void __launch_bounds__(RWN * 32)
     const bool needH = MODE != 2 && active && state[cell].s.need == NEED_H;
     SlotT &sl = slots[warp];
     C3D_NCLK_DECL
+    long long gcell = -1; // probe visits: the grid cell, for the ansatz hand-off's refresh list
+    if (MODE == 2 && active && first.refresh)
+        gcell = !list ? (first.cellMap ? (long long)first.cellMap[cell] : cell) : state[cell].s.cell;
     if (active) {
         if (MODE == 2 && !list)
             load_cell(sl, P, O, first.cellMap ? (long long)first.cellMap[cell] : cell, lane);
@@ -912,6 +953,12 @@ __global__ void __launch_bounds__(RWN * 32)
         after_trial(sl, P, O, lane, sl.s.fquad);
         C3D_NCLK(O.stats, 7, lane);
     }
+    if constexpr (MODE == 2) {
+        // a cell that goes on past its probe visit (or failed there) may end with other
+        // multipliers than the probe's: its psi is rewritten after the closure
+        if (gcell >= 0 && lane == 0 && (sl.s.need != NEED_NONE || sl.s.status != CELL_OK))
+            first.refresh[atomicAdd(first.refreshCount, 1u)] = (int)gcell;
+    }
     // a finished cell's state is not read again
     if (sl.s.need != NEED_NONE)
         slot_to_state(sl, state[cell], lane);
@@ -976,7 +1023,8 @@ template <int NT, int KIND, bool ZD> static size_t mixed_pass_smem(const Closure
     const size_t f64Pad = ((size_t)(P.nm + 1) * QCP * 8 + 127) & ~(size_t)127;
     const size_t stg = f64Pad + (KIND < 2 ? mixed_a_chunk_bytes(nm2, KIND) : 0);
     return GSTAGES * stg + GSTAGES * (size_t)K::NP * MXC * QC * K::ES + (size_t)QC * CST2 * 8 +
-           (size_t)RW * P.nm * 16 + (ZD ? (size_t)QC * ZS * 8 : 0) + (2 * GSTAGES + 1) * 8;
+           (size_t)RW * P.nm * 16 + (ZD ? (size_t)QC * ZS * 8 : 0) +
+           (KIND == 2 ? (size_t)QC * PSTR * 8 + MXC * 8 : 0) + (2 * GSTAGES + 1) * 8;
 }
 
 template <int NT, int NT2, bool GAUNT> static cudaError_t rounds_t(const RoundsLaunch &R)
@@ -1059,7 +1107,8 @@ template <int NT, int NT2, bool GAUNT> static cudaError_t rounds_t(const RoundsL
         if constexpr (GAUNT) {
             for (long long off = 0; off < R.ncells; off += R.batch) {
                 const int nb = (int)((R.ncells - off) < R.batch ? (R.ncells - off) : R.batch);
-                const FirstRound fr{off, R.cellMap, R.u, R.alpha};
+                const FirstRound fr{off,    R.cellMap, R.u,       R.alpha,
+                                    R.psi,  R.psiNall, R.refresh, R.refreshCount};
                 const unsigned grid = (unsigned)((nb + MXC - 1) / MXC);
                 if (mixed)
                     rounds_pass_mixed_kernel<NT, NT2, 2, true><<<grid, RW * 32, mixSmem[2], st>>>(

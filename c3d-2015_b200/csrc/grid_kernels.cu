@@ -122,6 +122,49 @@ __global__ void ghost_mirror_check_kernel(GridDims g, const double *__restrict__
         atomicExch(flag, 1);
 }
 
+// ---------------------------------------------------------------- ansatz hand-off from the closure
+
+// psi[q nall + ghost] = psi[q nall + image] for every face ghost and direction: the closure
+// copied the face ghosts' multipliers from their periodic images, so their ansatz values are
+// the images' too (the probe pass wrote the solved cells' values).
+__global__ void psi_face_copy_kernel(GridDims g, int nq, double *__restrict__ psi)
+{
+    const long long nf = ghost_faces(g), nall = g.nall(), total = nf * nq;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        const long long f = e % nf, q = e / nf;
+        long long dst, src;
+        ghost_pair(g, f, dst, src);
+        psi[q * nall + dst] = psi[q * nall + src];
+    }
+}
+
+// psi[q nall + c] = exp(alpha_c . m_q) for the *count cells c of list (one warp per cell,
+// directions over the lanes; exponent summed in the reference's order, unfused): the cells
+// whose multipliers the closure changed after its probe pass had written their psi.
+__global__ void psi_refresh_kernel(GridDims g, int nq, const double *__restrict__ M,
+                                   const double *__restrict__ alpha, const int *__restrict__ list,
+                                   const unsigned int *__restrict__ count, double *__restrict__ psi)
+{
+    const int nm = g.nm;
+    const long long nall = g.nall();
+    const unsigned int n = *count;
+    const int lane = threadIdx.x & 31;
+    const long long w0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long i = w0; i < n; i += nw) {
+        const long long c = list[i];
+        const double *a = alpha + c * nm;
+        for (int q = lane; q < nq; q += 32) {
+            const double *m = M + (size_t)q * nm;
+            double z = 0.0;
+            for (int k = 0; k < nm; ++k)
+                z = __dadd_rn(z, __dmul_rn(a[k], m[k]));
+            psi[(long long)q * nall + c] = exp(z);
+        }
+    }
+}
+
 // ---------------------------------------------------------------- Euler / RK
 
 __device__ __forceinline__ bool interior(const GridDims &g, long long c, int &i, int &j, int &k)
@@ -782,6 +825,20 @@ cudaError_t launch_ghost_mirror_check(const GridDims &g, const double *a, int *f
     return cudaGetLastError();
 }
 
+// The refresh comes first: a face ghost copies its image's final psi, and the image may be
+// one of the refreshed cells.
+cudaError_t launch_psi_handoff(const GridDims &g, int nq, const double *M, const double *alpha,
+                               bool faceCopy, const int *refresh, const unsigned int *refreshCount,
+                               double *psi, int numSMs, cudaStream_t st)
+{
+    psi_refresh_kernel<<<2 * numSMs, 256, 0, st>>>(g, nq, M, alpha, refresh, refreshCount, psi);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess || !faceCopy)
+        return e;
+    psi_face_copy_kernel<<<grid_for(ghost_faces(g) * nq, 256, numSMs), 256, 0, st>>>(g, nq, psi);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_euler(const GridDims &g, double *u, const double *flux, const double *sigT,
                          const double *sigS, double dt, int numSMs, cudaStream_t st)
 {
@@ -967,13 +1024,16 @@ template <int NT>
 static cudaError_t kinetic_t(const GridDims &g, const double *alpha, const double *mfA,
                              const double *mfP, const double *xi, const double *eta, int nq,
                              int qChunk, int runLen, double dx, double dy, double dz,
-                             double theta, int isPn, double *psi, double *flux, int *errorFlag,
-                             cudaStream_t st)
+                             double theta, int isPn, double *psi, bool psiReady, double *flux,
+                             int *errorFlag, cudaStream_t st)
 {
+    if (psiReady)
+        qChunk = nq; // psi of every direction is in place: the stencil alone, in one pass
     for (int q0 = 0; q0 < nq; q0 += qChunk) {
         int nqc = nq - q0 < qChunk ? nq - q0 : qChunk;
-        ansatz_dmma_kernel<NT><<<(unsigned)((g.nall() + 63) / 64), 256, 0, st>>>(
-            g, alpha, mfA, q0, nqc, isPn, psi, errorFlag);
+        if (!psiReady)
+            ansatz_dmma_kernel<NT><<<(unsigned)((g.nall() + 63) / 64), 256, 0, st>>>(
+                g, alpha, mfA, q0, nqc, isPn, psi, errorFlag);
         // staged psi when the z lines split into even runs of at most 64 cells (runLen: the
         // run length chosen by the autotuner, 0 for min(64, nz))
         const int L = runLen > 0 ? runLen : (g.nz < KRUN ? g.nz : KRUN);
@@ -1012,18 +1072,20 @@ static cudaError_t kinetic_t(const GridDims &g, const double *alpha, const doubl
 }
 
 // qChunk: a multiple of 32 unless it covers all of nq.
+// psiReady: psi[q nall + c] already holds the ansatz of every direction (handed off by the
+// closure), so only the stencil and projection run.
 cudaError_t launch_kinetic_flux(const GridDims &g, const double *alpha, const double *mfA,
                                 const double *mfP, const double *xi, const double *eta, int nq,
                                 int qChunk, int runLen, double dx, double dy, double dz,
-                                double theta, int isPn, double *psi, double *flux, int *errorFlag,
-                                cudaStream_t st)
+                                double theta, int isPn, double *psi, bool psiReady, double *flux,
+                                int *errorFlag, cudaStream_t st)
 {
     if (qChunk < nq && (qChunk & 31))
         return cudaErrorInvalidValue;
 #define C3D_NT_CASE(NT)                                                                            \
     case NT:                                                                                       \
         return kinetic_t<NT>(g, alpha, mfA, mfP, xi, eta, nq, qChunk, runLen, dx, dy, dz, theta, \
-                             isPn, psi, flux, errorFlag, st);
+                             isPn, psi, psiReady, flux, errorFlag, st);
     switch ((g.nm + 7) / 8) {
         C3D_NT_CASE(1)
         C3D_NT_CASE(2)

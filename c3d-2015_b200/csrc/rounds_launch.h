@@ -39,6 +39,13 @@ struct RoundsLaunch {
     cudaStream_t stream;
     long long *launches;
     long long maxRounds;
+    // ansatz hand-off to the kinetic flux (null psi: none): psi[q psiNall + c] of every cell
+    // the probe solves, and the list (with its device count) of cells whose psi is rewritten
+    // after the closure
+    double *psi;
+    long long psiNall;
+    int *refresh;
+    unsigned int *refreshCount;
 };
 
 cudaError_t launch_closure_rounds(const RoundsLaunch &R, bool gaunt);

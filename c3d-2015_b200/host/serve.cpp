@@ -23,18 +23,19 @@ namespace {
 using Clock = std::chrono::steady_clock;
 
 // Device bytes one problem holds at its peak: state (u, alpha, uOld, flux), cross sections,
-// per-cell records, the materialised ansatz of one direction chunk, the closure's work-list
-// state and buffers, tables; 10% and 64 MiB of slack.
+// per-cell records, the materialised ansatz of one direction chunk (all directions when they
+// fit the default 32 GiB budget, as the closure's ansatz hand-off wants), the hand-off's
+// refresh list, the closure's work-list state and buffers, tables; 10% and 64 MiB of slack.
 long long footprint(const c3d_host::Config &c)
 {
     const long long nall = (long long)(c.nx + 4) * (c.ny + 4) * (c.nz + 4);
     const long long nm = (long long)(c.momentOrder + 1) * (c.momentOrder + 1);
     const long long nmp = 8 * ((nm + 7) / 8);
     const long long nq = 2LL * c.quadOrder * c.quadOrder;
-    const long long psiCap = (16LL << 30) / 8 / (nall > 0 ? nall : 1);
+    const long long psiCap = (32LL << 30) / 8 / (nall > 0 ? nall : 1);
     const long long psiDirs = nq < psiCap ? nq : psiCap;
     long long b = 4 * nall * nm * 8 + 2 * nall * 8 + 5 * nall * 4 + 2 * nall * 8;
-    b += psiDirs * nall * 8;
+    b += psiDirs * nall * 8 + nall * 4;
     if (c.solver == "mn") {
         const long long batch = nall < (1LL << 20) ? nall : (1LL << 20);
         const long long nm2 = (2LL * c.momentOrder + 1) * (2 * c.momentOrder + 1);

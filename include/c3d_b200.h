@@ -93,7 +93,8 @@ typedef struct {
     double mnCondHMax;         /* MN_COND_H_MAX */
     int nreg;                  /* regularisation ladder (reference: 5 values) */
     double reg[16];
-    size_t psiBytes;           /* budget for the materialised ansatz (0 = default) */
+    size_t psiBytes;           /* budget for the materialised ansatz (0 = default, 32 GiB);
+                                  the closure's ansatz hand-off needs nq * nall * 8 bytes */
     int mnReproject;           /* 1: after each grid closure set u = <m e^{alpha.m}> with u_0
                                   kept (the robustness note of the reference's readme.txt);
                                   deck key MN_REPROJECT; no counterpart in the reference code */
@@ -243,6 +244,18 @@ c3d_status c3d_set_certificate(c3d_ctx *ctx, int on);
  * The flux buffer is overwritten; u and alpha are not touched. Outputs may be NULL
  * (runLen 0: min(64, nz)). */
 c3d_status c3d_autotune(c3d_ctx *ctx, int *qChunk, int *runLen, double *msPerCall);
+
+/* Ansatz hand-off from the closure to the kinetic flux (on by default; no counterpart in the
+ * reference). A grid closure with the convergence certificate evaluates e^{alpha.m_q} of
+ * every cell and direction in its probe pass; with this on, that pass also stores them as the
+ * flux's ansatz psi (one buffer of nq * nall doubles, within the params' psiBytes budget),
+ * face ghosts copy their images' values and the few cells whose multipliers change after the
+ * probe are recomputed at the end of the closure, and the next c3d_flux_kinetic runs the
+ * limited stencil and projection alone instead of forming psi again. The flux equals the
+ * one formed from the closure's multipliers up to rounding (the probe forms
+ * u_0 e^{alpha_scaled . m_q}). Any change of the multipliers in between (c3d_set_state,
+ * c3d_copy_x_planes) drops the hand-off. */
+c3d_status c3d_set_ansatz_handoff(c3d_ctx *ctx, int on);
 
 /* Safety bounds of the closure (no counterpart in the reference, which loops until each cell
  * converges or aborts): at most maxRounds work-list rounds per closure (engine 0; default

@@ -361,7 +361,7 @@ static int newton_scaled(const orc_closure_opts *o, const orc_tables *t, double 
     double rtol = o->batched ? o->tol : orc_nrm2(nm, u) * o->tol;
     int iter = 0, totalIter = 0, iterGamma = 0, regIndex = 0;
     double tstep = 1, r = 0.0, gamma = 0.0, err = 0.0;
-    double armijoUlps = 1e300, tolRel = 1e300, condRel = 1e300, gammaRel = 1e300;
+    double armijoUlps = 1e300, tolRel = 1e300, condRel = 1e300, gammaRel = 1e300, capHits = 0;
     int status = 0;
 
     for (int i = 0; i < nm; i++)
@@ -404,6 +404,8 @@ static int newton_scaled(const orc_closure_opts *o, const orc_tables *t, double 
         }
 
         if (iter >= maxIterEff || cholErr != 0 || tstep == 0 || condest > o->condHMax) {
+            if (iter >= maxIterEff)
+                capHits += 1;
             if (regIndex < o->nreg - 1) {
                 regIndex++;
                 r = o->reg[regIndex];
@@ -457,6 +459,7 @@ static int newton_scaled(const orc_closure_opts *o, const orc_tables *t, double 
         out->tolRel = tolRel;
         out->condRel = condRel;
         out->gammaRel = gammaRel;
+        out->capHits = capHits;
     }
     return status;
 }

@@ -42,8 +42,8 @@ typedef struct {
      * Armijo tests, |err - tol| / tol over all stop tests, and
      * |condest - condHMax| / condHMax over all condition tests of a successful
      * factorisation, |gamma - tolGamma| / tolGamma over the stop tests whose
-     * gradient passed. */
-    double armijoUlps, tolRel, condRel, gammaRel;
+     * gradient passed; capHits counts regularisations forced by the iteration cap. */
+    double armijoUlps, tolRel, condRel, gammaRel, capHits;
 } orc_cell_out;
 
 typedef struct {

@@ -5,7 +5,9 @@ moments and the extreme values of e^{alpha.m}); a cell whose gradient and bounds
 the full iteration would end it converged is finalized without forming or factoring its
 Hessian. The full iteration would have produced the same multipliers, moments, iteration
 counts, regularisation indices and statuses, so runs with and without the certificate must
-agree bit for bit -- in the FP64 closure and in the mixed-precision one. Workload: the 64^3
+agree bit for bit -- in the FP64 closure and in the mixed-precision one (with the ansatz
+hand-off off, which only the certificate's probe pass feeds and which changes the flux by
+rounding; test_gpu_handoff covers it). Workload: the 64^3
 M_6 deck (49 moments, 1568 directions, gaussian pulse of width 0.02 over a 1e-10 floor),
 three SSP-RK2 steps; most cells sit on the isotropic floor and are certified.
 """
@@ -32,6 +34,7 @@ def _run(tmp_path, mixed, certificate):
     deck.write_text(deck_text(**kw))
     s = c3d.Solver(str(deck))
     c3d.check(c3d.lib().c3d_set_certificate(s.ctx_handle, int(certificate)), "certificate")
+    c3d.check(c3d.lib().c3d_set_ansatz_handoff(s.ctx_handle, 0), "handoff")
     for _ in range(3):
         s.update(s.max_dt)
     s.sync()

