@@ -47,7 +47,7 @@ HEADER_SYMBOLS = [
     "c3d_closure_records_fp", "c3d_line_stats_enable", "c3d_line_stats_get", "c3d_stage",
     "c3d_set_x_halo_external", "c3d_copy_x_planes", "c3d_set_precision",
     "c3d_set_certificate", "c3d_autotune", "c3d_closure_vectors_noalloc_check",
-    "c3d_set_limits", "c3d_set_ansatz_handoff",
+    "c3d_set_limits", "c3d_set_ansatz_handoff", "c3d_set_graphs",
 ]
 
 
@@ -121,8 +121,9 @@ def lib():
         L.c3d_autotune.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                                    ctypes.POINTER(ctypes.c_double)]
         L.c3d_set_ghost_mirroring.argtypes = [vp, ctypes.c_int]
-        L.c3d_set_limits.argtypes = [vp, ctypes.c_longlong, ctypes.c_longlong]
+        L.c3d_set_limits.argtypes = [vp, ctypes.c_longlong, ctypes.c_longlong, ctypes.c_longlong]
         L.c3d_set_ansatz_handoff.argtypes = [vp, ctypes.c_int]
+        L.c3d_set_graphs.argtypes = [vp, ctypes.c_int]
         L.c3d_timing_enable.argtypes = [vp, ctypes.c_int]
         L.c3d_timing_get.argtypes = [vp, _dp, ctypes.POINTER(ctypes.c_longlong)]
         L.c3d_launch_count.argtypes = [vp]
@@ -327,10 +328,15 @@ class Context:
               "c3d_autotune")
         return q.value, r.value, ms.value
 
-    def set_limits(self, max_rounds=0, pass_budget=0):
+    def set_limits(self, max_rounds=0, pass_budget=0, batch=0):
         """Work-list rounds per closure and passes per cell before the closure gives up
-        (C3D_ERR_TIMEOUT / cell status 3); 0 restores the defaults."""
-        check(lib().c3d_set_limits(self.h, int(max_rounds), int(pass_budget)), "c3d_set_limits")
+        (C3D_ERR_TIMEOUT / cell status 3), list entries per launch; 0 restores the defaults."""
+        check(lib().c3d_set_limits(self.h, int(max_rounds), int(pass_budget), int(batch)),
+              "c3d_set_limits")
+
+    def set_graphs(self, on):
+        """Closure rounds as one device-resident CUDA graph (default) or host-driven."""
+        check(lib().c3d_set_graphs(self.h, int(bool(on))), "c3d_set_graphs")
 
     def set_ansatz_handoff(self, on):
         """Closure probe's ansatz handed to the next kinetic flux (default on)."""

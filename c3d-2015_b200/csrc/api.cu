@@ -165,12 +165,16 @@ struct c3d_ctx {
     double m0 = 0.0; // M[0][0]
     int engine = 0;  // 0: work-list rounds, 1: persistent kernels
     long long maxRounds = 1LL << 24; // work-list rounds per closure before C3D_ERR_TIMEOUT
+    long long maxBatch = 1LL << 20;  // list entries per pass/Newton launch
+    void *roundsGraph = nullptr;     // the closure as one CUDA graph (c3d_set_graphs)
+    bool graphs = true;
+    unsigned long long *launchDev = nullptr; // kernels launched by device-side round loops
     // work-list buffers (sized on first use)
     void *rState = nullptr;
     int *rListA = nullptr, *rListB = nullptr;
     unsigned int *rCounts = nullptr, *rHostCount = nullptr;
     double *rBuf = nullptr;
-    long long rCells = 0, rBatch = 0;
+    long long rCells = 0, rBatch = 0, rBatchUse = 0; // rBatch: buffer capacity, rBatchUse: in use
     size_t rBufPer = 0;
     int nm2 = 0;
     // Gaunt form of the Hessian (c3d_set_gaunt)
@@ -244,6 +248,10 @@ static void free_ctx(c3d_ctx *c)
     for (void *p : ptrs)
         if (p)
             cudaFree(p);
+    if (c->launchDev)
+        cudaFree(c->launchDev);
+    if (c->roundsGraph)
+        rounds_graph_free(c->roundsGraph);
     timing_clear(c);
     if (c->rHostCount)
         cudaFreeHost(c->rHostCount);
@@ -477,9 +485,11 @@ c3d_status c3d_ghost_fill(c3d_ctx *c)
 static c3d_status ensure_rounds(c3d_ctx *c, long long n)
 {
     size_t per = rounds_buf_doubles(c->g.nm, c->nm2, c->gaunt, c->gaunt && c->cp.mixed);
-    long long batch = n < (1LL << 20) ? n : (1LL << 20);
-    if (n <= c->rCells && per <= c->rBufPer && batch <= c->rBatch)
+    long long batch = n < c->maxBatch ? n : c->maxBatch;
+    if (n <= c->rCells && per <= c->rBufPer && batch <= c->rBatch) {
+        c->rBatchUse = batch;
         return C3D_OK;
+    }
     void *ptrs[] = {c->rState, c->rListA, c->rListB, c->rCounts, c->rBuf};
     for (void *p : ptrs)
         if (p)
@@ -493,12 +503,13 @@ static c3d_status ensure_rounds(c3d_ctx *c, long long n)
     // one list per precision level (the FP64 closure uses the first)
     C3D_CUDA(cudaMalloc(&c->rListA, 4 * (size_t)n * sizeof(int)));
     C3D_CUDA(cudaMalloc(&c->rListB, 4 * (size_t)n * sizeof(int)));
-    C3D_CUDA(cudaMalloc(&c->rCounts, 8 * sizeof(unsigned int)));
+    C3D_CUDA(cudaMalloc(&c->rCounts, 16 * sizeof(unsigned int)));
     C3D_CUDA(cudaMalloc(&c->rBuf, (size_t)batch * per * sizeof(double)));
     if (!c->rHostCount)
         C3D_CUDA(cudaMallocHost(&c->rHostCount, 4 * sizeof(unsigned int)));
     c->rCells = n;
     c->rBatch = batch;
+    c->rBatchUse = batch;
     c->rBufPer = per;
     return C3D_OK;
 }
@@ -549,11 +560,23 @@ static c3d_status run_closure(c3d_ctx *c, long long n, double *u, double *alpha,
         R.counts = c->rCounts;
         R.hostCount = c->rHostCount;
         R.buf = c->rBuf;
-        R.batch = c->rBatch;
+        R.batch = c->rBatchUse;
         R.errorFlag = c->errorFlag;
         R.stream = c->stream;
         R.launches = &c->launches;
         R.maxRounds = c->maxRounds;
+        R.graphs = nullptr;
+        R.launchDev = nullptr;
+        if (c->graphs) {
+            if (!c->roundsGraph)
+                c->roundsGraph = rounds_graph_new();
+            if (!c->launchDev) {
+                C3D_CUDA(cudaMalloc(&c->launchDev, sizeof(unsigned long long)));
+                C3D_CUDA(cudaMemset(c->launchDev, 0, sizeof(unsigned long long)));
+            }
+            R.graphs = c->roundsGraph;
+            R.launchDev = c->launchDev;
+        }
         R.psi = nullptr;
         if (gridRecords && c->cp.probe && c->handoff && c->solver == 1) {
             // hand the probe's ansatz to the kinetic flux when psi of every direction fits the
@@ -1033,6 +1056,14 @@ c3d_status c3d_set_engine(c3d_ctx *c, int engine)
     return C3D_OK;
 }
 
+c3d_status c3d_set_graphs(c3d_ctx *c, int on)
+{
+    if (!c)
+        return fail(C3D_ERR_INVALID, "c3d_set_graphs: null context");
+    c->graphs = on != 0;
+    return C3D_OK;
+}
+
 c3d_status c3d_set_ansatz_handoff(c3d_ctx *c, int on)
 {
     if (!c)
@@ -1043,12 +1074,14 @@ c3d_status c3d_set_ansatz_handoff(c3d_ctx *c, int on)
     return C3D_OK;
 }
 
-c3d_status c3d_set_limits(c3d_ctx *c, long long maxRounds, long long passBudget)
+c3d_status c3d_set_limits(c3d_ctx *c, long long maxRounds, long long passBudget,
+                          long long batch)
 {
     if (!c)
         return fail(C3D_ERR_INVALID, "c3d_set_limits: null context");
     c->maxRounds = maxRounds > 0 ? maxRounds : (1LL << 24);
     c->cp.passBudget = passBudget > 0 ? passBudget : (1LL << 40);
+    c->maxBatch = batch > 0 ? batch : (1LL << 20);
     return C3D_OK;
 }
 
@@ -1274,8 +1307,11 @@ c3d_status c3d_sync(c3d_ctx *c)
     unsigned long long failed = 0;
     C3D_CUDA(cudaMemcpy(&flag, c->errorFlag, 4, cudaMemcpyDeviceToHost));
     C3D_CUDA(cudaMemcpy(&failed, c->failCount, 8, cudaMemcpyDeviceToHost));
-    if (flag)
-        return fail(C3D_ERR_TIMEOUT, "a bounded device wait gave up");
+    if (flag) {
+        cudaMemset(c->errorFlag, 0, 4);
+        return fail(C3D_ERR_TIMEOUT, flag == 2 ? "closure: round limit exceeded"
+                                               : "a bounded device wait gave up");
+    }
     if (failed) {
         cudaMemset(c->failCount, 0, 8);
         return fail(C3D_ERR_CLOSURE, std::to_string(failed) +
@@ -1405,7 +1441,17 @@ c3d_status c3d_closure_stats_reset(c3d_ctx *c)
     return C3D_OK;
 }
 
-long long c3d_launch_count(c3d_ctx *c) { return c ? c->launches : 0; }
+long long c3d_launch_count(c3d_ctx *c)
+{
+    if (!c)
+        return 0;
+    unsigned long long dev = 0;
+    if (c->launchDev) {
+        cudaStreamSynchronize(c->stream);
+        cudaMemcpy(&dev, c->launchDev, sizeof(dev), cudaMemcpyDeviceToHost);
+    }
+    return c->launches + (long long)dev;
+}
 
 c3d_status c3d_timing_enable(c3d_ctx *c, int on)
 {

@@ -16,6 +16,8 @@
 // (latency-bound, one warp per cell) lets each run at its own occupancy; a cell that
 // needs many iterations only ever occupies the short lists of later rounds.
 #include "closure_core.cuh"
+
+#include <vector>
 #include "rounds_launch.h"
 #include "umma.cuh"
 
@@ -124,6 +126,13 @@ __device__ void append_if_needed(const S &sl, const ClosureParams &P, long long 
 constexpr int RW = 8;  // warps (cells) per CTA of the init and pass kernels
 constexpr int RWN = 4; // warps (cells) per CTA of the Newton kernel
 
+// Entries a round kernel works on: n, or with nDev (the list's device counter, as the
+// graph-resident round loop launches them) the smaller of n and *nDev.
+__device__ __forceinline__ int round_entries(int n, const unsigned int *nDev)
+{
+    return nDev ? (int)min((unsigned int)n, *nDev) : n;
+}
+
 template <int NT> using TSlot = Slot<NT, true>;
 
 // Per-warp state of a first visit after the probe pass: the vectors and scalars of Slot
@@ -168,9 +177,12 @@ constexpr int CST2 = 20; // row stride (cells) of the coefficient tile: conflict
 template <int NT, int NT2>
 __global__ void __launch_bounds__(RW * 32, 2)
     rounds_pass_gaunt_kernel(ClosureParams P, const double *__restrict__ chunks, int nm2,
-                             const int *__restrict__ list, int n, CellState<NT> *state,
-                             double *__restrict__ momBuf, int *errorFlag)
+                             const int *__restrict__ list, int n, const unsigned int *nDev,
+                             CellState<NT> *state, double *__restrict__ momBuf, int *errorFlag)
 {
+    n = round_entries(n, nDev);
+    if (blockIdx.x * RWP >= n)
+        return;
     constexpr int NM2P = 8 * NT2;
     constexpr int RT = (NT2 + RW - 1) / RW;
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -314,9 +326,12 @@ __global__ void __launch_bounds__(RW * 32, 2)
 template <int NT>
 __global__ void __launch_bounds__(RW * 32, 1)
     rounds_pass_direct_kernel(ClosureParams P, const double *__restrict__ chunks,
-                              const int *__restrict__ list, int n, CellState<NT> *state,
-                              double *__restrict__ hBuf, int *errorFlag)
+                              const int *__restrict__ list, int n, const unsigned int *nDev,
+                              CellState<NT> *state, double *__restrict__ hBuf, int *errorFlag)
 {
+    n = round_entries(n, nDev);
+    if (blockIdx.x * RW >= n)
+        return;
     constexpr int NMP = Cfg<NT>::NMP;
     constexpr int CH = Cfg<NT>::CHUNK;
     constexpr int ST = 3;
@@ -493,9 +508,12 @@ template <int NT, int NT2, int KIND, bool ZD>
 __global__ void __launch_bounds__(RW * 32, KIND == 1 ? 1 : KIND == 2 ? 3 : 2)
     rounds_pass_mixed_kernel(ClosureParams P, const double *__restrict__ f64c,
                              const unsigned char *__restrict__ ac, const int *__restrict__ list,
-                             int n, CellState<NT> *state, double *__restrict__ out, int *errorFlag,
-                             FirstRound first)
+                             int n, const unsigned int *nDev, CellState<NT> *state,
+                             double *__restrict__ out, int *errorFlag, FirstRound first)
 {
+    n = round_entries(n, nDev);
+    if (blockIdx.x * MXC >= n)
+        return;
     using K = MixKind<KIND>;
     using R = MixRows<NT2>;
     constexpr int NMP = 8 * NT;
@@ -826,11 +844,15 @@ __global__ void __launch_bounds__(RW * 32, KIND == 1 ? 1 : KIND == 2 ? 3 : 2)
 template <int NT, int NT2, bool GAUNT, int MODE>
 __global__ void __launch_bounds__(RWN * 32)
     rounds_newton_kernel(ClosureParams P, double m0, const int *__restrict__ list, int n,
-                         CellState<NT> *state, const double *__restrict__ buf,
+                         const unsigned int *nDev, CellState<NT> *state,
+                         const double *__restrict__ buf,
                          const GauntTerm *__restrict__ stream, int streamLen,
                          Outputs Og, Lists out, int level, const GauntTerm *__restrict__ g0,
                          int g0n, FirstRound first)
 {
+    n = round_entries(n, nDev);
+    if (blockIdx.x * RWN >= n)
+        return;
     constexpr bool MIX = MODE == 1;
     constexpr int NM2P = 8 * NT2;
     constexpr int NMP = Cfg<NT>::NMP;
@@ -1027,6 +1049,168 @@ template <int NT, int KIND, bool ZD> static size_t mixed_pass_smem(const Closure
            (KIND == 2 ? (size_t)QC * PSTR * 8 + MXC * 8 : 0) + (2 * GSTAGES + 1) * 8;
 }
 
+// ---------------------------------------------------------------- graph-resident round loop
+//
+// A closure is one CUDA graph: round 0 (set-up, or the certificate's probe round) then a
+// conditional WHILE node whose body runs two rounds (lists A -> B, then B -> A) and sets the
+// loop condition on the device, so no round waits for the host. Within a round, each list's
+// pass and Newton kernels sit in a SWITCH node whose branch -- one of four launch sizes
+// (up to 512, 8192, 65536 and `cap` entries) or none for an empty list -- a control kernel
+// picks from the list's device counter; entries past `cap` are carried to the next round's
+// list. The kernels read their entry count from the counter (round_entries).
+
+constexpr int NTIER = 4;
+__host__ __device__ inline long long tier_entries(int t, long long cap)
+{
+    const long long t0 = t == 0 ? 512 : t == 1 ? 8192 : 65536;
+    return t < 3 && t0 < cap ? t0 : cap;
+}
+
+struct TierHandles {
+    cudaGraphConditionalHandle h[NLISTS];
+};
+
+// Picks each used list's launch size (SWITCH branch; NTIER = none) from its counter; bit l of
+// mask marks list l as used.
+__global__ void rounds_tier_kernel(const Lists in, TierHandles th, unsigned int mask, long long cap,
+                                   unsigned long long *launches)
+{
+    if (threadIdx.x != 0)
+        return;
+    unsigned long long l2 = 1;
+    for (int l = 0; l < NLISTS; ++l) {
+        if (!((mask >> l) & 1u))
+            continue;
+        const long long c = (long long)*in.count[l];
+        int t = NTIER;
+        for (int k = NTIER - 1; k >= 0; --k)
+            if (c > 0 && c <= tier_entries(k, cap))
+                t = k;
+        if (c > cap)
+            t = NTIER - 1;
+        cudaGraphSetConditional(th.h[l], (unsigned int)t);
+        l2 += t < NTIER ? 2 : 0;
+    }
+    if (launches)
+        atomicAdd(launches, l2 + 1); // + the carry kernel
+}
+
+// Entries past cap stay for the next round: appended to that round's list.
+__global__ void rounds_carry_kernel(const Lists in, Lists out, unsigned int mask, long long cap)
+{
+    __shared__ unsigned int base[NLISTS];
+    for (int l = 0; l < NLISTS; ++l) {
+        if (!((mask >> l) & 1u))
+            continue;
+        const long long c = (long long)*in.count[l];
+        if (c <= cap)
+            continue; // uniform over the block
+        if (threadIdx.x == 0)
+            base[l] = atomicAdd(out.count[l], (unsigned int)(c - cap));
+        __syncthreads();
+        for (long long i = cap + threadIdx.x; i < c; i += blockDim.x)
+            out.list[l][base[l] + (i - cap)] = in.list[l][i];
+        __syncthreads();
+    }
+}
+
+// Loop condition after the body's two rounds: more work and the round limit not reached;
+// past the limit the closure stops with errorFlag 2 (c3d_sync: C3D_ERR_TIMEOUT).
+__global__ void rounds_cond_kernel(const Lists in, unsigned int mask, unsigned int *rounds,
+                                   long long maxRounds, int *errorFlag,
+                                   cudaGraphConditionalHandle loop, unsigned long long *launches)
+{
+    if (threadIdx.x != 0)
+        return;
+    unsigned long long total = 0;
+    for (int l = 0; l < NLISTS; ++l)
+        if ((mask >> l) & 1u)
+            total += *in.count[l];
+    const unsigned int r = *rounds + 2;
+    *rounds = r;
+    bool more = total > 0;
+    if (more && (long long)r >= maxRounds) {
+        atomicExch(errorFlag, 2);
+        more = false;
+    }
+    cudaGraphSetConditional(loop, more ? 1u : 0u);
+    if (launches)
+        atomicAdd(launches, 1ull);
+}
+
+// Appends a conditional node after the current dependencies of the graph being captured on st.
+static cudaError_t capture_conditional(cudaStream_t st, cudaGraphConditionalHandle h,
+                                       cudaGraphConditionalNodeType type, unsigned int size,
+                                       cudaGraph_t **bodies)
+{
+    cudaStreamCaptureStatus status;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t ndeps = 0;
+    cudaError_t e = cudaStreamGetCaptureInfo(st, &status, nullptr, &g, &deps, &ndeps);
+    if (e != cudaSuccess)
+        return e;
+    if (status != cudaStreamCaptureStatusActive)
+        return cudaErrorStreamCaptureInvalidated;
+    cudaGraphNodeParams p = {};
+    p.type = cudaGraphNodeTypeConditional;
+    p.conditional.handle = h;
+    p.conditional.type = type;
+    p.conditional.size = size;
+    cudaGraphNode_t node;
+    e = cudaGraphAddNode(&node, g, deps, ndeps, &p);
+    if (e != cudaSuccess)
+        return e;
+    e = cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies);
+    *bodies = p.conditional.phGraph_out;
+    return e;
+}
+
+// The instantiated closure graph of one configuration (rebuilt when any launch parameter
+// changes), with the streams its capture uses.
+struct RoundsGraph {
+    std::vector<unsigned char> key;
+    cudaGraphExec_t exec = nullptr;
+    cudaStream_t cs[3] = {nullptr, nullptr, nullptr};
+    ~RoundsGraph()
+    {
+        if (exec)
+            cudaGraphExecDestroy(exec);
+        for (cudaStream_t s : cs)
+            if (s)
+                cudaStreamDestroy(s);
+    }
+};
+
+template <class T> static void key_add(std::vector<unsigned char> &k, const T &v)
+{
+    const unsigned char *b = reinterpret_cast<const unsigned char *>(&v);
+    k.insert(k.end(), b, b + sizeof(T));
+}
+
+static std::vector<unsigned char> rounds_key(const RoundsLaunch &R, bool gaunt)
+{
+    std::vector<unsigned char> k;
+    key_add(k, *R.P);
+    const void *ptrs[] = {R.chunks, R.gstream, R.cellMap, R.u, R.alpha, R.iters, R.iterGamma,
+                          R.regIdx, R.status, R.failCount, R.stats, R.gamma, R.normG, R.cond,
+                          R.state, R.listA, R.listB, R.counts, R.buf, R.mixF64, R.mixA[0],
+                          R.mixA[1], R.g0, R.errorFlag, R.psi, R.refresh, R.refreshCount,
+                          R.launchDev};
+    for (const void *p : ptrs)
+        key_add(k, p);
+    key_add(k, R.nm2);
+    key_add(k, R.streamLen);
+    key_add(k, R.m0);
+    key_add(k, R.ncells);
+    key_add(k, R.batch);
+    key_add(k, R.g0n);
+    key_add(k, R.psiNall);
+    key_add(k, R.maxRounds);
+    key_add(k, gaunt);
+    return k;
+}
+
 template <int NT, int NT2, bool GAUNT> static cudaError_t rounds_t(const RoundsLaunch &R)
 {
     const ClosureParams &P = *R.P;
@@ -1091,7 +1275,6 @@ template <int NT, int NT2, bool GAUNT> static cudaError_t rounds_t(const RoundsL
     const Outputs O{R.u,      R.alpha,     R.iters, R.iterGamma, R.regIdx,
                     R.status, R.failCount, R.stats, R.gamma,     R.normG, R.cond};
 
-    // round 0: set-up of every cell
     Lists A, B;
     for (int l = 0; l < NLISTS; ++l) {
         A.list[l] = R.listA + (size_t)l * R.ncells;
@@ -1099,35 +1282,218 @@ template <int NT, int NT2, bool GAUNT> static cudaError_t rounds_t(const RoundsL
         A.count[l] = R.counts + l;
         B.count[l] = R.counts + NLISTS + l;
     }
-    e = cudaMemsetAsync(A.count[0], 0, NLISTS * sizeof(unsigned int), st);
-    if (e != cudaSuccess)
-        return e;
-    if (probe) {
-        // set-up and probe pass of every cell in one round (the certificate's first round)
-        if constexpr (GAUNT) {
-            for (long long off = 0; off < R.ncells; off += R.batch) {
-                const int nb = (int)((R.ncells - off) < R.batch ? (R.ncells - off) : R.batch);
-                const FirstRound fr{off,    R.cellMap, R.u,       R.alpha,
-                                    R.psi,  R.psiNall, R.refresh, R.refreshCount};
+    // the lists a round can fill: FP64 Hessian passes, the mixed closure's BF16 and 3xTF32
+    // ones, and probe passes (first visits; set up with the probe kernels' launch attributes)
+    const unsigned int usedLists = 1u | (mixed ? 6u : 0u) | (probe ? 8u : 0u);
+
+    // pass + Newton kernels of list l: entries la[0 .. nb) (with nDev, at most *nDev of them),
+    // the cells still in need appended to out
+    auto launch_list = [&](int l, const int *la, int nb, const unsigned int *nDev, const Lists &out,
+                           cudaStream_t s) {
+        if (l == 3) {
+            // probe passes of first visits (Gaunt form only)
+            if constexpr (GAUNT) {
                 const unsigned grid = (unsigned)((nb + MXC - 1) / MXC);
                 if (mixed)
-                    rounds_pass_mixed_kernel<NT, NT2, 2, true><<<grid, RW * 32, mixSmem[2], st>>>(
-                        P, R.mixF64, nullptr, nullptr, nb, state, R.buf, R.errorFlag, fr);
+                    rounds_pass_mixed_kernel<NT, NT2, 2, true><<<grid, RW * 32, mixSmem[2], s>>>(
+                        P, R.mixF64, nullptr, la, nb, nDev, state, R.buf, R.errorFlag,
+                        FirstRound{});
                 else
-                    rounds_pass_mixed_kernel<NT, NT2, 2, false><<<grid, RW * 32, mixSmem[2], st>>>(
-                        P, R.mixF64, nullptr, nullptr, nb, state, R.buf, R.errorFlag, fr);
+                    rounds_pass_mixed_kernel<NT, NT2, 2, false><<<grid, RW * 32, mixSmem[2], s>>>(
+                        P, R.mixF64, nullptr, la, nb, nDev, state, R.buf, R.errorFlag,
+                        FirstRound{});
                 rounds_newton_kernel<NT, NT2, GAUNT, 2>
-                    <<<(unsigned)((nb + RWN - 1) / RWN), RWN * 32, probeSmem, st>>>(
-                        P, m0, nullptr, nb, state, R.buf, R.gstream, R.streamLen, O, A, 3,
-                        mixed ? nullptr : R.g0, R.g0n, fr);
-                *R.launches += 2;
+                    <<<(unsigned)((nb + RWN - 1) / RWN), RWN * 32, probeSmem, s>>>(
+                        P, m0, la, nb, nDev, state, R.buf, R.gstream, R.streamLen, O, out, l,
+                        mixed ? nullptr : R.g0, R.g0n, FirstRound{});
             }
+        } else if (l > 0) {
+            // mixed-precision Hessian passes (Gaunt form only)
+            if constexpr (GAUNT) {
+                const unsigned grid = (unsigned)((nb + MXC - 1) / MXC);
+                if (l == 1)
+                    rounds_pass_mixed_kernel<NT, NT2, 0, true><<<grid, RW * 32, mixSmem[0], s>>>(
+                        P, R.mixF64, R.mixA[0], la, nb, nDev, state, R.buf, R.errorFlag,
+                        FirstRound{});
+                else
+                    rounds_pass_mixed_kernel<NT, NT2, 1, true><<<grid, RW * 32, mixSmem[1], s>>>(
+                        P, R.mixF64, R.mixA[1], la, nb, nDev, state, R.buf, R.errorFlag,
+                        FirstRound{});
+                rounds_newton_kernel<NT, NT2, GAUNT, 1>
+                    <<<(unsigned)((nb + RWN - 1) / RWN), RWN * 32, newtonSmem, s>>>(
+                        P, m0, la, nb, nDev, state, R.buf, R.gstream, R.streamLen, O, out, l,
+                        nullptr, 0, FirstRound{});
+            }
+        } else {
+            if (GAUNT)
+                rounds_pass_gaunt_kernel<NT, NT2>
+                    <<<(unsigned)((nb + RWP - 1) / RWP), RW * 32, passSmem, s>>>(
+                        P, R.chunks, R.nm2, la, nb, nDev, state, R.buf, R.errorFlag);
+            else
+                rounds_pass_direct_kernel<NT>
+                    <<<(unsigned)((nb + RW - 1) / RW), RW * 32, passSmem, s>>>(
+                        P, R.chunks, la, nb, nDev, state, R.buf, R.errorFlag);
+            rounds_newton_kernel<NT, NT2, GAUNT, 0>
+                <<<(unsigned)((nb + RWN - 1) / RWN), RWN * 32, newtonSmem, s>>>(
+                    P, m0, la, nb, nDev, state, R.buf, R.gstream, R.streamLen, O, out, 0, nullptr,
+                    0, FirstRound{});
         }
-    } else {
-        rounds_init_kernel<NT><<<(unsigned)((R.ncells + RW - 1) / RW), RW * 32, slotSmem, st>>>(
-            P, R.ncells, R.cellMap, O, state, A);
-        *R.launches += 1;
+        return cudaGetLastError();
+    };
+
+    // round 0: set-up of every cell (with the certificate: set-up and probe pass in one round)
+    auto round0 = [&](cudaStream_t s) -> cudaError_t {
+        cudaError_t e0 = cudaMemsetAsync(A.count[0], 0, NLISTS * sizeof(unsigned int), s);
+        if (e0 != cudaSuccess)
+            return e0;
+        if (probe) {
+            if constexpr (GAUNT) {
+                for (long long off = 0; off < R.ncells; off += R.batch) {
+                    const int nb = (int)((R.ncells - off) < R.batch ? (R.ncells - off) : R.batch);
+                    const FirstRound fr{off,    R.cellMap, R.u,       R.alpha,
+                                        R.psi,  R.psiNall, R.refresh, R.refreshCount};
+                    const unsigned grid = (unsigned)((nb + MXC - 1) / MXC);
+                    if (mixed)
+                        rounds_pass_mixed_kernel<NT, NT2, 2, true><<<grid, RW * 32, mixSmem[2], s>>>(
+                            P, R.mixF64, nullptr, nullptr, nb, nullptr, state, R.buf, R.errorFlag,
+                            fr);
+                    else
+                        rounds_pass_mixed_kernel<NT, NT2, 2, false><<<grid, RW * 32, mixSmem[2], s>>>(
+                            P, R.mixF64, nullptr, nullptr, nb, nullptr, state, R.buf, R.errorFlag,
+                            fr);
+                    rounds_newton_kernel<NT, NT2, GAUNT, 2>
+                        <<<(unsigned)((nb + RWN - 1) / RWN), RWN * 32, probeSmem, s>>>(
+                            P, m0, nullptr, nb, nullptr, state, R.buf, R.gstream, R.streamLen, O,
+                            A, 3, mixed ? nullptr : R.g0, R.g0n, fr);
+                    *R.launches += 2;
+                }
+            }
+        } else {
+            rounds_init_kernel<NT><<<(unsigned)((R.ncells + RW - 1) / RW), RW * 32, slotSmem, s>>>(
+                P, R.ncells, R.cellMap, O, state, A);
+            *R.launches += 1;
+        }
+        return cudaGetLastError();
+    };
+
+    if (R.graphs) {
+        RoundsGraph *G = reinterpret_cast<RoundsGraph *>(R.graphs);
+        std::vector<unsigned char> key = rounds_key(R, GAUNT);
+        const long long round0Launches = probe ? 2 * ((R.ncells + R.batch - 1) / R.batch) : 1;
+        if (!G->exec || G->key != key) {
+            if (G->exec) {
+                cudaGraphExecDestroy(G->exec);
+                G->exec = nullptr;
+            }
+            for (int i = 0; i < 3; ++i)
+                if (!G->cs[i] && (e = cudaStreamCreateWithFlags(&G->cs[i], cudaStreamNonBlocking)) !=
+                                     cudaSuccess)
+                    return e;
+            const long long cap = R.batch;
+            cudaGraph_t top = nullptr;
+            if ((e = cudaGraphCreate(&top, 0)) != cudaSuccess)
+                return e;
+            cudaGraphConditionalHandle hLoop;
+            TierHandles th[2];
+            e = cudaGraphConditionalHandleCreate(&hLoop, top, 1, cudaGraphCondAssignDefault);
+            // one handle per SWITCH node the graph has (a handle without its node makes the
+            // graph invalid)
+            for (int hr = 0; hr < 2 && e == cudaSuccess; ++hr)
+                for (int l = 0; l < NLISTS && e == cudaSuccess; ++l)
+                    if ((usedLists >> l) & 1u)
+                        e = cudaGraphConditionalHandleCreate(&th[hr].h[l], top, NTIER,
+                                                             cudaGraphCondAssignDefault);
+            if (e == cudaSuccess)
+                e = cudaStreamBeginCaptureToGraph(G->cs[0], top, nullptr, nullptr, 0,
+                                                  cudaStreamCaptureModeRelaxed);
+            if (e == cudaSuccess) {
+                const long long launches0 = *R.launches;
+                cudaError_t ec = cudaMemsetAsync(R.counts + 2 * NLISTS, 0, sizeof(unsigned int),
+                                                 G->cs[0]);
+                if (ec == cudaSuccess)
+                    ec = round0(G->cs[0]);
+                *R.launches = launches0;
+                cudaGraph_t *loopBody = nullptr;
+                if (ec == cudaSuccess)
+                    ec = capture_conditional(G->cs[0], hLoop, cudaGraphCondTypeWhile, 1, &loopBody);
+                if (ec == cudaSuccess)
+                    ec = cudaStreamBeginCaptureToGraph(G->cs[1], loopBody[0], nullptr, nullptr, 0,
+                                                       cudaStreamCaptureModeRelaxed);
+                if (ec == cudaSuccess) {
+                    for (int hr = 0; hr < 2 && ec == cudaSuccess; ++hr) {
+                        const Lists &X = hr == 0 ? A : B, &Y = hr == 0 ? B : A;
+                        ec = cudaMemsetAsync(Y.count[0], 0, NLISTS * sizeof(unsigned int),
+                                             G->cs[1]);
+                        if (ec == cudaSuccess) {
+                            rounds_tier_kernel<<<1, 32, 0, G->cs[1]>>>(X, th[hr], usedLists, cap,
+                                                                      R.launchDev);
+                            ec = cudaGetLastError();
+                        }
+                        for (int l = 0; l < NLISTS && ec == cudaSuccess; ++l) {
+                            if (!((usedLists >> l) & 1u))
+                                continue;
+                            cudaGraph_t *tiers = nullptr;
+                            ec = capture_conditional(G->cs[1], th[hr].h[l], cudaGraphCondTypeSwitch,
+                                                     NTIER, &tiers);
+                            for (int t = 0; t < NTIER && ec == cudaSuccess; ++t) {
+                                ec = cudaStreamBeginCaptureToGraph(G->cs[2], tiers[t], nullptr,
+                                                                   nullptr, 0,
+                                                                   cudaStreamCaptureModeRelaxed);
+                                if (ec == cudaSuccess) {
+                                    cudaError_t el = launch_list(
+                                        l, X.list[l], (int)tier_entries(t, cap), X.count[l], Y,
+                                        G->cs[2]);
+                                    cudaGraph_t body = nullptr;
+                                    ec = cudaStreamEndCapture(G->cs[2], &body);
+                                    if (ec == cudaSuccess)
+                                        ec = el;
+                                }
+                            }
+                        }
+                        if (ec == cudaSuccess) {
+                            rounds_carry_kernel<<<1, 1024, 0, G->cs[1]>>>(X, Y, usedLists, cap);
+                            ec = cudaGetLastError();
+                        }
+                    }
+                    if (ec == cudaSuccess) {
+                        rounds_cond_kernel<<<1, 32, 0, G->cs[1]>>>(
+                            A, usedLists, R.counts + 2 * NLISTS, R.maxRounds, R.errorFlag, hLoop,
+                            R.launchDev);
+                        ec = cudaGetLastError();
+                    }
+                    cudaGraph_t body = nullptr;
+                    cudaError_t eb = cudaStreamEndCapture(G->cs[1], &body);
+                    if (ec == cudaSuccess)
+                        ec = eb;
+                }
+                cudaGraph_t topOut = nullptr;
+                e = cudaStreamEndCapture(G->cs[0], &topOut);
+                if (e == cudaSuccess)
+                    e = ec;
+            }
+            if (e == cudaSuccess)
+                e = cudaGraphInstantiate(&G->exec, top, 0);
+            cudaGraphDestroy(top);
+            if (e != cudaSuccess) {
+                // a failed capture may leave its streams unusable: start over with new ones
+                G->exec = nullptr;
+                for (cudaStream_t &cs : G->cs) {
+                    if (cs)
+                        cudaStreamDestroy(cs);
+                    cs = nullptr;
+                }
+                cudaGetLastError();
+                return e;
+            }
+            G->key = key;
+        }
+        *R.launches += round0Launches + 1;
+        return cudaGraphLaunch(G->exec, st);
     }
+
+    // host-driven rounds: the host reads the list counts after each round
+    if ((e = round0(st)) != cudaSuccess)
+        return e;
     *R.launches += 1;
     long long rounds = 0;
     for (;;) {
@@ -1149,59 +1515,11 @@ template <int NT, int NT2, bool GAUNT> static cudaError_t rounds_t(const RoundsL
             return e;
         *R.launches += 1;
         for (int l = 0; l < NLISTS; ++l) {
-            const int *la = A.list[l];
             for (long long off = 0; off < cnt[l]; off += R.batch) {
                 int nb = (int)((cnt[l] - off) < R.batch ? (cnt[l] - off) : R.batch);
-                if (l == 3) {
-                    // probe passes of first visits (Gaunt form only)
-                    if constexpr (GAUNT) {
-                        const unsigned grid = (unsigned)((nb + MXC - 1) / MXC);
-                        if (mixed)
-                            rounds_pass_mixed_kernel<NT, NT2, 2, true>
-                                <<<grid, RW * 32, mixSmem[2], st>>>(P, R.mixF64, nullptr, la + off,
-                                                                    nb, state, R.buf, R.errorFlag, FirstRound{});
-                        else
-                            rounds_pass_mixed_kernel<NT, NT2, 2, false>
-                                <<<grid, RW * 32, mixSmem[2], st>>>(P, R.mixF64, nullptr, la + off,
-                                                                    nb, state, R.buf, R.errorFlag, FirstRound{});
-                        rounds_newton_kernel<NT, NT2, GAUNT, 2>
-                            <<<(unsigned)((nb + RWN - 1) / RWN), RWN * 32, probeSmem, st>>>(
-                                P, m0, la + off, nb, state, R.buf, R.gstream, R.streamLen, O, B, l,
-                                mixed ? nullptr : R.g0, R.g0n, FirstRound{});
-                    }
-                } else if (l > 0) {
-                    // mixed-precision Hessian passes (Gaunt form only)
-                    if constexpr (GAUNT) {
-                        const unsigned grid = (unsigned)((nb + MXC - 1) / MXC);
-                        if (l == 1)
-                            rounds_pass_mixed_kernel<NT, NT2, 0, true><<<grid, RW * 32, mixSmem[0], st>>>(
-                                P, R.mixF64, R.mixA[0], la + off, nb, state, R.buf, R.errorFlag, FirstRound{});
-                        else
-                            rounds_pass_mixed_kernel<NT, NT2, 1, true><<<grid, RW * 32, mixSmem[1], st>>>(
-                                P, R.mixF64, R.mixA[1], la + off, nb, state, R.buf, R.errorFlag, FirstRound{});
-                        rounds_newton_kernel<NT, NT2, GAUNT, 1>
-                            <<<(unsigned)((nb + RWN - 1) / RWN), RWN * 32, newtonSmem, st>>>(
-                                P, m0, la + off, nb, state, R.buf, R.gstream, R.streamLen, O, B, l,
-                                nullptr, 0, FirstRound{});
-                    }
-                } else {
-                    if (GAUNT)
-                        rounds_pass_gaunt_kernel<NT, NT2>
-                            <<<(unsigned)((nb + RWP - 1) / RWP), RW * 32, passSmem, st>>>(
-                                P, R.chunks, R.nm2, la + off, nb, state, R.buf, R.errorFlag);
-                    else
-                        rounds_pass_direct_kernel<NT><<<(unsigned)((nb + RW - 1) / RW), RW * 32,
-                                                        passSmem, st>>>(
-                            P, R.chunks, la + off, nb, state, R.buf, R.errorFlag);
-                    rounds_newton_kernel<NT, NT2, GAUNT, 0>
-                        <<<(unsigned)((nb + RWN - 1) / RWN), RWN * 32, newtonSmem, st>>>(
-                            P, m0, la + off, nb, state, R.buf, R.gstream, R.streamLen, O, B, 0,
-                            nullptr, 0, FirstRound{});
-                }
-                *R.launches += 2;
-                e = cudaGetLastError();
-                if (e != cudaSuccess)
+                if ((e = launch_list(l, A.list[l] + off, nb, nullptr, B, st)) != cudaSuccess)
                     return e;
+                *R.launches += 2;
             }
         }
         Lists t = A;
@@ -1210,6 +1528,9 @@ template <int NT, int NT2, bool GAUNT> static cudaError_t rounds_t(const RoundsL
     }
     return cudaSuccess;
 }
+
+void *rounds_graph_new() { return new RoundsGraph(); }
+void rounds_graph_free(void *g) { delete reinterpret_cast<RoundsGraph *>(g); }
 
 // Moment counts with a work-list Gaunt form (N <= 7).
 bool rounds_gaunt_supported(int nm)

@@ -46,6 +46,10 @@ struct RoundsLaunch {
     long long psiNall;
     int *refresh;
     unsigned int *refreshCount;
+    // graph-resident round loop (rounds_graph_new; null: host-driven rounds) and the device
+    // counter of the kernels its loop launches
+    void *graphs;
+    unsigned long long *launchDev;
 };
 
 cudaError_t launch_closure_rounds(const RoundsLaunch &R, bool gaunt);
@@ -53,5 +57,7 @@ size_t rounds_state_bytes(int nm);
 size_t rounds_buf_doubles(int nm, int nm2, bool gaunt, bool mixed);
 size_t mixed_a_chunk_bytes(int nm2, int fmt);
 bool rounds_gaunt_supported(int nm);
+void *rounds_graph_new();
+void rounds_graph_free(void *g);
 
 } // namespace c3d

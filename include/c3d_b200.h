@@ -245,6 +245,19 @@ c3d_status c3d_set_certificate(c3d_ctx *ctx, int on);
  * (runLen 0: min(64, nz)). */
 c3d_status c3d_autotune(c3d_ctx *ctx, int *qChunk, int *runLen, double *msPerCall);
 
+/* The work-list closure as one CUDA graph (engine 0; on by default; no counterpart in the
+ * reference, whose host loop hands the GPU one Hessian batch at a time,
+ * src/opt/optBatch.cpp:350-472). Round 0, then a conditional WHILE node whose body runs two
+ * rounds and sets its own condition on the device; each list's kernels sit in a SWITCH node
+ * whose branch (launch size, or none for an empty list) a control kernel picks from the
+ * list's device counter. A closure then needs no host round trip: c3d_closure enqueues one
+ * graph launch on the context's stream (built on the first call and again whenever the
+ * closure's parameters or buffers change). The round limit of c3d_set_limits is checked on
+ * the device and reported by c3d_sync as C3D_ERR_TIMEOUT ("closure: round limit exceeded").
+ * off: the host reads the list counts after every round (c3d_closure itself returns
+ * C3D_ERR_TIMEOUT at the limit). Results are identical either way. */
+c3d_status c3d_set_graphs(c3d_ctx *ctx, int on);
+
 /* Ansatz hand-off from the closure to the kinetic flux (on by default; no counterpart in the
  * reference). A grid closure with the convergence certificate evaluates e^{alpha.m_q} of
  * every cell and direction in its probe pass; with this on, that pass also stores them as the
@@ -261,9 +274,12 @@ c3d_status c3d_set_ansatz_handoff(c3d_ctx *ctx, int on);
  * converges or aborts): at most maxRounds work-list rounds per closure (engine 0; default
  * 2^24), after which the closure returns C3D_ERR_TIMEOUT with the unfinished cells' state
  * left as it was, and at most passBudget Hessian and line-search passes per cell (default
- * 2^40), after which the cell ends with status 3 and c3d_sync reports C3D_ERR_CLOSURE.
- * Values <= 0 restore the defaults. */
-c3d_status c3d_set_limits(c3d_ctx *ctx, long long maxRounds, long long passBudget);
+ * 2^40), after which the cell ends with status 3 and c3d_sync reports C3D_ERR_CLOSURE, and at
+ * most batch list entries per pass and Newton launch (default 2^20; the pass output buffer
+ * holds that many; longer lists run in several launches, or carry over between the graph's
+ * rounds). Values <= 0 restore the defaults. */
+c3d_status c3d_set_limits(c3d_ctx *ctx, long long maxRounds, long long passBudget,
+                          long long batch);
 
 /* Face-ghost mirroring of the grid closure (engine 0; on by default). The reference solves
  * every cell, ghosts included (src/update.cpp:51-53, 119-123). A face ghost holds a copy of
@@ -286,7 +302,8 @@ c3d_status c3d_closure_vectors(c3d_ctx *ctx, long long n, double *u, double *alp
 void c3d_build_quadrature(int momentOrder, int quadOrder, double *w, double *xi, double *eta,
                           double *mu, double *M, double *M2);
 
-/* Number of kernel launches issued by this context so far. */
+/* Number of kernel launches issued by this context so far (synchronises the context's stream
+ * to add those of device-side round loops). */
 long long c3d_launch_count(c3d_ctx *ctx);
 
 /* ------------------------------------------------------------------ allocation-free closure */

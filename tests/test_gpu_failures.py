@@ -10,8 +10,9 @@ a status code, and the context stays usable afterwards:
   cannot finish in two iterations get status 2 (ladder exhausted), the rest converge with
   the oracle's multipliers;
 * a pass budget of one: cells that need a second pass end with status 3;
-* a limit of one work-list round: the closure returns C3D_ERR_TIMEOUT, and a closure
-  with the default limits then finishes the same state.
+* a limit of one work-list round: C3D_ERR_TIMEOUT -- from c3d_sync when the round loop
+  runs on the device (c3d_set_graphs on, the default), from c3d_closure itself when the host
+  drives the rounds -- and a closure with the default limits then finishes the same state.
 """
 import numpy as np
 import pytest
@@ -93,7 +94,8 @@ def test_pass_budget_ends_cells_with_status_3(oracle):
     ctx.close()
 
 
-def test_round_limit_returns_timeout_and_recovers(oracle):
+@pytest.mark.parametrize("graphs", [True, False])
+def test_round_limit_returns_timeout_and_recovers(oracle, graphs):
     S = _setup(oracle, steps_before=2)
     nm = S["nm"]
     ref = _ctx(S)
@@ -105,10 +107,12 @@ def test_round_limit_returns_timeout_and_recovers(oracle):
     ref.close()
 
     ctx = _ctx(S)
+    ctx.set_graphs(graphs)
     ctx.set_limits(max_rounds=1)
     ctx.set_state(u=S["u"], alpha=S["alpha"], sig_t=S["sig"], sig_s=S["sig"])
     with pytest.raises(c3d.C3DError, match="TIMEOUT"):
         ctx.closure()
+        ctx.sync()
     # cells the first round finished hold their results, the others their inputs
     ctx.set_limits()
     ctx.closure()
