@@ -356,7 +356,7 @@ def standalone_vectors(c3d, N, n):
     return q, u, a_iso
 
 
-def standalone_closure(torch, c3d, stream):
+def standalone_closure(torch, c3d, stream, graphs=True):
     """FP64 vs mixed closure of the standalone workload (one context per order, Gaunt form).
     Unbatched rules
     (|g| <= |u| MN_TOL, gamma <= 1.1), MN_TOL 1e-8. Device-resident vectors, CUDA events
@@ -383,6 +383,7 @@ def standalone_closure(torch, c3d, stream):
                 f.write("".join(f"{k} {v}\n" for k, v in kv.items()))
             solver = c3d.Solver(deck, stream=ctypes.c_void_p(stream.cuda_stream))
         h = solver.ctx_handle
+        c3d.check(L.c3d_set_graphs(h, 1 if graphs else 0), "graphs")
         row = dict(N=N, nm=q["nm"], nq=q["nq"], vectors=n)
         alphas = {}
         for mode in (0, 1):
@@ -469,6 +470,7 @@ def b200_arm(args):
     ctxh = solver.ctx_handle
     L = c3d.lib()
     c3d.check(L.c3d_set_engine(ctxh, 0 if args.engine == "rounds" else 1), "engine")
+    c3d.check(L.c3d_set_graphs(ctxh, 1 if args.graphs else 0), "graphs")
     dt = solver.max_dt
     nm, nq = solver.nm, solver.nq
 
@@ -521,12 +523,16 @@ def b200_arm(args):
 
     peak = fp64_peak_tflops() if rank == 0 else None
 
-    def timed(mode, sample_clocks):
-        """K device-resident steps from S with the given closure precision."""
+    def timed(mode, sample_clocks, breakdown=False, steps=None):
+        """Device-resident steps from S with the given closure precision: each RK stage one
+        CUDA graph launch, or with breakdown (CUDA events around the closure and flux launches)
+        stage by stage."""
+        nsteps = steps or args.steps
         set_precision(mode)
         load_state(u_s, a_s)
         L.c3d_closure_stats_reset(ctxh)
-        L.c3d_timing_enable(ctxh, 1)
+        L.c3d_timing_enable(ctxh, 1 if breakdown else 0)
+        syncs0 = solver.stats().hostSyncs
         launches0 = L.c3d_launch_count(ctxh)
         clocks = ClockSampler(local) if sample_clocks else None
         if world > 1:
@@ -535,9 +541,9 @@ def b200_arm(args):
         if clocks:
             clocks.start()
             time.sleep(0.3)
-        evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+        evs = [torch.cuda.Event(enable_timing=True) for _ in range(nsteps + 1)]
         evs[0].record(stream)
-        for k in range(args.steps):
+        for k in range(nsteps):
             solver.update(dt)
             evs[k + 1].record(stream)
         torch.cuda.synchronize()
@@ -546,13 +552,14 @@ def b200_arm(args):
         clk = clocks.stop() if clocks else None
         launches = L.c3d_launch_count(ctxh) - launches0
         sync_count()
-        step_ms = [evs[k].elapsed_time(evs[k + 1]) for k in range(args.steps)]
+        step_ms = [evs[k].elapsed_time(evs[k + 1]) for k in range(nsteps)]
         total_ms = evs[0].elapsed_time(evs[-1])
         ms = np.zeros(2)
         cnt = (ctypes.c_longlong * 2)()
         L.c3d_timing_get(ctxh, ms.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), cnt)
         L.c3d_timing_enable(ctxh, 0)
         st = solver.stats()
+        syncs = st.hostSyncs - syncs0
         t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
         if world > 1:
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -563,12 +570,23 @@ def b200_arm(args):
         c3d.check(L.c3d_get_flux(ctxh, ctypes.c_void_p(fo.data_ptr()), 0), "get_flux")
         torch.cuda.synchronize()
         return dict(max_ms=float(t.item()), step_ms=step_ms, ms=ms, cnt=cnt, launches=launches,
-                    clk=clk, st=st, u=uo.numpy(), a=ao.numpy(), f=fo.numpy())
+                    clk=clk, st=st, u=uo.numpy(), a=ao.numpy(), f=fo.numpy(), syncs=syncs,
+                    steps=nsteps)
 
     cells = interior_cells(cfg)
+    if args.compare:
+        # the other arm's graphs, instantiated from S untimed (the timed arm's were built by
+        # the warm-up)
+        set_precision(1 - precision)
+        load_state(u_s, a_s)
+        solver.update(dt)
+        sync_count()
     other = timed(1 - precision, False) if args.compare else None
     head = timed(precision, True)
-    max_ms, step_ms, ms, cnt = head["max_ms"], head["step_ms"], head["ms"], head["cnt"]
+    # closure / flux split: a short run with CUDA events around each launch (stage by stage)
+    split = timed(precision, False, breakdown=True, steps=min(2, args.steps))
+    max_ms, step_ms = head["max_ms"], head["step_ms"]
+    ms, cnt = split["ms"], split["cnt"]
     launches, clk, st = head["launches"], head["clk"], head["st"]
     total_ms = max_ms
     value = world * cells * 2 * args.steps / (max_ms * 1e-3)
@@ -596,11 +614,12 @@ def b200_arm(args):
 
     if rank == 0:
         closure_launches = int(cnt[0])
+        sst = split["st"]  # counters of the split run, whose closures the events time
         low = None
         if precision == 1:
-            flops, low = closure_flops_mixed(nm, nq, st)
+            flops, low = closure_flops_mixed(nm, nq, sst)
         else:
-            flops = closure_flops(nm, nq, st.totalIters, st.trials, args.hessian, st.certified)
+            flops = closure_flops(nm, nq, sst.totalIters, sst.trials, args.hessian, sst.certified)
         per_launch_s = ms[0] * 1e-3 / max(1, closure_launches)
         achieved = flops / max(1, closure_launches) / per_launch_s / 1e12
         roofline = dict(bound="tensor",
@@ -626,7 +645,7 @@ def b200_arm(args):
                         flops_per_launch=flops / max(1, closure_launches),
                         closure_ms_per_launch=ms[0] / max(1, closure_launches),
                         flux_ms_per_launch=ms[1] / max(1, int(cnt[1])),
-                        closure_share_of_step=ms[0] / total_ms)
+                        closure_share_of_step=ms[0] / split["max_ms"])
         if low is not None:
             roofline["lowp_tflops"] = low / max(1, closure_launches) / per_launch_s / 1e12
             roofline["kernel"] = ("closure work-list rounds: rounds_pass_mixed_kernel<7,22,2> "
@@ -697,7 +716,7 @@ def b200_arm(args):
         standalone = None
         if args.standalone and world == 1:
             try:
-                standalone = standalone_closure(torch, c3d, stream)
+                standalone = standalone_closure(torch, c3d, stream, args.graphs)
             except Exception as ex:  # reported, not fatal
                 standalone = dict(error=str(ex))
         line = dict(
@@ -722,6 +741,16 @@ def b200_arm(args):
             e2e=dict(value=e2e_value, unit=UNIT, h2d_bytes_per_step=2 * nv * 8,
                      d2h_bytes_per_step=2 * nv * 8, steps=e_steps),
             gpu_launches=int(launches), clocks=clk,
+            stage_graphs=dict(launches_per_step=launches / args.steps,
+                              host_syncs_per_step=head["syncs"] / args.steps,
+                              note="each RK stage is one CUDA graph launch (closure rounds in a "
+                                   "device-side conditional loop); launches counted by the "
+                                   "library, device-side loop kernels included"),
+            closure_only=dict(value=cells / (ms[0] / max(1, closure_launches) * 1e-3), unit=UNIT,
+                              ms_per_closure=ms[0] / max(1, closure_launches),
+                              note="interior cell-solves per second of the closure alone (the "
+                                   "same quantity as cpu_baseline, which times the reference's "
+                                   "closure only)"),
             latency_ms=dict(p50=float(np.percentile(step_ms, 50)),
                             p99=float(np.percentile(step_ms, 99)), unit="ms per RK2 step"),
             iter_histogram=hist, newton_iters_per_solve=st.totalIters / max(1, st.cells),
@@ -750,6 +779,9 @@ def main():
     ap.add_argument("--config", default="c3", choices=sorted(CONFIGS))
     ap.add_argument("--hessian", default="gaunt", choices=["gaunt", "direct"])
     ap.add_argument("--engine", default="rounds", choices=["rounds", "persistent"])
+    ap.add_argument("--no-graphs", dest="graphs", action="store_false",
+                    help="launch the stages kernel by kernel with host-driven closure rounds "
+                         "(for profilers that do not look inside CUDA graphs' conditional nodes)")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
                     help="closure precision of the reported arm (mixed: the configuration's "
                          "form; fp64: the drop-in)")

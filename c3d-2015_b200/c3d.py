@@ -78,7 +78,8 @@ class ClosureStats(ctypes.Structure):
                 ("iterHist", ctypes.c_longlong * 64),
                 ("clkNewton", ctypes.c_longlong * 8), ("hessBf16", ctypes.c_longlong),
                 ("hessTf32x3", ctypes.c_longlong), ("hessFp64", ctypes.c_longlong),
-                ("escalated", ctypes.c_longlong), ("certified", ctypes.c_longlong)]
+                ("escalated", ctypes.c_longlong), ("certified", ctypes.c_longlong),
+                ("hostSyncs", ctypes.c_longlong)]
 
 
 _lib = None

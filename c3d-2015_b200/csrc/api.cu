@@ -147,6 +147,7 @@ struct c3d_ctx {
     int *psiRefresh = nullptr;          // cells whose psi is rewritten after the closure
     unsigned int *psiRefreshCount = nullptr;
     long long launches = 0;
+    long long hostSyncs = 0; // host waits inside the stages (c3d_closure_stats.hostSyncs)
     // device buffers
     double *u = nullptr, *alpha = nullptr, *uOld = nullptr, *flux = nullptr;
     double *sigT = nullptr, *sigS = nullptr;
@@ -168,6 +169,16 @@ struct c3d_ctx {
     long long maxBatch = 1LL << 20;  // list entries per pass/Newton launch
     void *roundsGraph = nullptr;     // the closure as one CUDA graph (c3d_set_graphs)
     bool graphs = true;
+    // each RK stage as one CUDA graph (c3d_set_graphs): instantiated per stage and rebuilt
+    // when its key (dt, options, buffers) changes; sc: the streams its capture uses
+    struct StageGraph {
+        std::vector<unsigned char> key;
+        cudaGraphExec_t exec = nullptr;
+        long long launches = 0;
+        unsigned long long used = 0;
+    } sg[8]; // the last few stage configurations (both stages, e.g. of two precisions)
+    unsigned long long sgTick = 0;
+    cudaStream_t sc[4] = {nullptr, nullptr, nullptr, nullptr};
     unsigned long long *launchDev = nullptr; // kernels launched by device-side round loops
     // work-list buffers (sized on first use)
     void *rState = nullptr;
@@ -236,6 +247,8 @@ static void timing_clear(c3d_ctx *c)
 
 static void free_ctx(c3d_ctx *c)
 {
+    if (c->stream)
+        cudaStreamSynchronize(c->stream); // graphs and buffers may still be in use
     void *ptrs[] = {c->u,     c->alpha,  c->uOld,     c->flux,    c->sigT,   c->sigS,
                     c->M,     c->w,      c->xi,       c->eta,     c->mu,     c->chunks,
                     c->pnops, c->psi,    c->iters,    c->iterGamma, c->regIdx, c->status,
@@ -252,6 +265,12 @@ static void free_ctx(c3d_ctx *c)
         cudaFree(c->launchDev);
     if (c->roundsGraph)
         rounds_graph_free(c->roundsGraph);
+    for (auto &g : c->sg)
+        if (g.exec)
+            cudaGraphExecDestroy(g.exec);
+    for (cudaStream_t s : c->sc)
+        if (s)
+            cudaStreamDestroy(s);
     timing_clear(c);
     if (c->rHostCount)
         cudaFreeHost(c->rHostCount);
@@ -516,17 +535,20 @@ static c3d_status ensure_rounds(c3d_ctx *c, long long n)
 
 // gridRecords: the closure covers the context's grid (directly or through cellMap), so the
 // per-cell gamma and |g| records of the context (nall entries) receive its results.
-static c3d_status run_closure(c3d_ctx *c, long long n, double *u, double *alpha, int *iters,
-                              int *iterGamma, int *regIdx, int *status, const int *cellMap = nullptr,
-                              bool gridRecords = false)
+// The work-list closure of n cells (engine 0): buffers sized, the launch description filled;
+// the hand-off's refresh count is cleared on st (the stream the closure will run on, or the
+// stream capturing it).
+static c3d_status rounds_setup(c3d_ctx *c, long long n, double *u, double *alpha, int *iters,
+                               int *iterGamma, int *regIdx, int *status, const int *cellMap,
+                               bool gridRecords, cudaStream_t st, RoundsLaunch &R)
 {
     double *recGamma = gridRecords ? c->cellGamma : nullptr;
     double *recErr = gridRecords ? c->cellErr : nullptr;
-    if (c->engine == 0) {
+    {
         c3d_status s = ensure_rounds(c, n);
         if (s != C3D_OK)
             return s;
-        RoundsLaunch R{};
+        R = RoundsLaunch{};
         R.P = &c->cp;
         R.chunks = c->gaunt ? c->gChunksC : c->chunks;
         R.nm2 = c->nm2;
@@ -564,6 +586,7 @@ static c3d_status run_closure(c3d_ctx *c, long long n, double *u, double *alpha,
         R.errorFlag = c->errorFlag;
         R.stream = c->stream;
         R.launches = &c->launches;
+        R.hostSyncs = &c->hostSyncs;
         R.maxRounds = c->maxRounds;
         R.graphs = nullptr;
         R.launchDev = nullptr;
@@ -595,13 +618,30 @@ static c3d_status run_closure(c3d_ctx *c, long long n, double *u, double *alpha,
                     C3D_CUDA(cudaMalloc(&c->psiRefresh, (size_t)c->g.nall() * sizeof(int)));
                     C3D_CUDA(cudaMalloc(&c->psiRefreshCount, sizeof(unsigned int)));
                 }
-                C3D_CUDA(cudaMemsetAsync(c->psiRefreshCount, 0, sizeof(unsigned int), c->stream));
+                C3D_CUDA(cudaMemsetAsync(c->psiRefreshCount, 0, sizeof(unsigned int), st));
                 R.psi = c->psi;
                 R.psiNall = c->g.nall();
                 R.refresh = c->psiRefresh;
                 R.refreshCount = c->psiRefreshCount;
             }
         }
+        R.stream = st;
+    }
+    return C3D_OK;
+}
+
+static c3d_status run_closure(c3d_ctx *c, long long n, double *u, double *alpha, int *iters,
+                              int *iterGamma, int *regIdx, int *status, const int *cellMap = nullptr,
+                              bool gridRecords = false)
+{
+    double *recGamma = gridRecords ? c->cellGamma : nullptr;
+    double *recErr = gridRecords ? c->cellErr : nullptr;
+    if (c->engine == 0) {
+        RoundsLaunch R;
+        c3d_status s = rounds_setup(c, n, u, alpha, iters, iterGamma, regIdx, status, cellMap,
+                                    gridRecords, c->stream, R);
+        if (s != C3D_OK)
+            return s;
         c->psiReady = false;
         cudaError_t e = launch_closure_rounds(R, c->gaunt);
         if (e == cudaErrorLaunchTimeout)
@@ -686,13 +726,10 @@ static c3d_status finish_handoff(c3d_ctx *c, bool faceCopy)
     return C3D_OK;
 }
 
-static c3d_status closure_grid(c3d_ctx *c)
+// The closure cells of a mirrored closure: every cell but the face ghosts.
+static c3d_status ensure_cellmap(c3d_ctx *c)
 {
-    if (c->engine == 0 && c->mirror && !c->xHaloExternal) {
-        // Face ghosts hold copies of their periodic images (src/comm.cpp:281-323); when their
-        // multipliers (the warm starts) are bitwise those of the images too, the per-cell
-        // solve of the reference gives them the images' results, so they are copied after
-        // solving the other cells instead. Edge and corner ghosts are solved as before.
+    {
         if (!c->cellMap) {
             std::vector<int> map;
             const GridDims &g = c->g;
@@ -715,11 +752,26 @@ static c3d_status closure_grid(c3d_ctx *c)
                                 cudaMemcpyHostToDevice));
             c->cellMapCount = (long long)map.size();
         }
+    }
+    return C3D_OK;
+}
+
+static c3d_status closure_grid(c3d_ctx *c)
+{
+    if (c->engine == 0 && c->mirror && !c->xHaloExternal) {
+        // Face ghosts hold copies of their periodic images (src/comm.cpp:281-323); when their
+        // multipliers (the warm starts) are bitwise those of the images too, the per-cell
+        // solve of the reference gives them the images' results, so they are copied after
+        // solving the other cells instead. Edge and corner ghosts are solved as before.
+        c3d_status sm = ensure_cellmap(c);
+        if (sm != C3D_OK)
+            return sm;
         C3D_CUDA(cudaMemsetAsync(c->mirrorFlag, 0, sizeof(int), c->stream));
         C3D_CUDA(launch_ghost_mirror_check(c->g, c->alpha, c->mirrorFlag, c->numSMs, c->stream));
         C3D_CUDA(cudaMemcpyAsync(c->mirrorHost, c->mirrorFlag, sizeof(int), cudaMemcpyDeviceToHost,
                                  c->stream));
         C3D_CUDA(cudaStreamSynchronize(c->stream));
+        c->hostSyncs++;
         c->launches += 1;
         if (*c->mirrorHost == 0) {
             c3d_status s = run_closure(c, c->cellMapCount, c->u, c->alpha, c->iters, c->iterGamma,
@@ -1229,11 +1281,225 @@ c3d_status c3d_euler(c3d_ctx *c, double dt)
     return C3D_OK;
 }
 
+// Sets an IF node's condition: mirrored closure when no face ghost's multipliers differ from
+// its image's.
+__global__ void mirror_if_kernel(const int *flag, cudaGraphConditionalHandle h)
+{
+    if (threadIdx.x == 0)
+        cudaGraphSetConditional(h, *flag == 0 ? 1u : 0u);
+}
+
+// One M_N RK stage of update() as a CUDA graph: [RK save,] ghost fill, the closure (with
+// face-ghost mirroring: the mirror check picks, through an IF node, the mirrored closure with
+// its ghost copies or the closure of every cell), the ansatz hand-off, the kinetic flux and
+// the Euler stage[, RK average]. Nothing in it waits for the host. *used is false when the
+// context's options need the stage run launch by launch (timing events, the x-line log,
+// re-projection, the persistent engine, P_N).
+static c3d_status stage_graph(c3d_ctx *c, int stage, double dt, bool *used)
+{
+    *used = false;
+    if (!c->graphs || c->engine != 0 || c->timing || c->lineCap != 0 || c->reproject ||
+        c->solver != 1)
+        return C3D_OK;
+    const bool mirrorPath = c->mirror && !c->xHaloExternal;
+    // buffers first (nothing is allocated while capturing)
+    if (mirrorPath) {
+        c3d_status sm = ensure_cellmap(c);
+        if (sm != C3D_OK)
+            return sm;
+    }
+    RoundsLaunch Rall;
+    c3d_status s = rounds_setup(c, c->g.nall(), c->u, c->alpha, c->iters, c->iterGamma,
+                                c->regIdx, c->status, nullptr, true, c->stream, Rall);
+    if (s != C3D_OK)
+        return s;
+    if (!c->launchDev) {
+        C3D_CUDA(cudaMalloc(&c->launchDev, sizeof(unsigned long long)));
+        C3D_CUDA(cudaMemset(c->launchDev, 0, sizeof(unsigned long long)));
+        Rall.launchDev = c->launchDev;
+    }
+    const bool handoff = Rall.psi != nullptr;
+    if (!handoff) {
+        const size_t need = (size_t)c->qChunk * c->g.nall() * 8;
+        if (!c->psi || c->psiAlloc < need) {
+            if (c->psi)
+                cudaFree(c->psi);
+            c->psi = nullptr;
+            c->psiAlloc = 0;
+            C3D_CUDA(cudaMalloc(&c->psi, need));
+            c->psiAlloc = need;
+        }
+    }
+    std::vector<unsigned char> key;
+    auto skey = [](std::vector<unsigned char> &k, const auto &v) {
+        const unsigned char *b = reinterpret_cast<const unsigned char *>(&v);
+        k.insert(k.end(), b, b + sizeof(v));
+    };
+    skey(key, stage);
+    skey(key, dt);
+    skey(key, c->cp);
+    skey(key, mirrorPath);
+    skey(key, c->gaunt);
+    skey(key, handoff);
+    skey(key, c->qChunk);
+    skey(key, c->runLen);
+    skey(key, c->maxRounds);
+    skey(key, c->rBatchUse);
+    const void *ptrs[] = {c->psi, c->rState, c->rBuf, c->rListA, c->rCounts, c->cellMap,
+                          c->gChunksC, c->chunks, c->gStream, c->mixF64, c->mixA[0],
+                          c->mixA[1], c->g0, c->psiRefresh, c->launchDev};
+    for (const void *p : ptrs)
+        skey(key, p);
+    c3d_ctx::StageGraph *Gp = nullptr;
+    for (auto &g : c->sg)
+        if (g.exec && g.key == key)
+            Gp = &g;
+    if (!Gp) {
+        Gp = &c->sg[0];
+        for (auto &g : c->sg)
+            if (g.used < Gp->used)
+                Gp = &g;
+    }
+    auto &G = *Gp;
+    if (!G.exec || G.key != key) {
+        std::lock_guard<std::mutex> lk(graph_build_mutex());
+        if (G.exec) {
+            // the previous graph may still run on the stream: it is destroyed once idle
+            C3D_CUDA(cudaStreamSynchronize(c->stream));
+            cudaGraphExecDestroy(G.exec);
+            G.exec = nullptr;
+        }
+        for (cudaStream_t &x : c->sc)
+            if (!x)
+                C3D_CUDA(cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking));
+        cudaGraph_t top = nullptr;
+        C3D_CUDA(cudaGraphCreate(&top, 0));
+        long long launches = 0;
+        const long long l0 = c->launches;
+        cudaError_t e = cudaStreamBeginCaptureToGraph(c->sc[0], top, nullptr, nullptr, 0,
+                                                      cudaStreamCaptureModeRelaxed);
+        cudaError_t ec = cudaSuccess;
+        if (e == cudaSuccess) {
+            cudaStream_t s0 = c->sc[0];
+            if (stage == 0)
+                ec = launch_rk(c->g, c->u, c->uOld, 0, c->numSMs, s0);
+            if (ec == cudaSuccess)
+                ec = launch_ghost_fill(c->g, c->u, c->numSMs, s0, c->xHaloExternal);
+            launches += (stage == 0) + 1;
+            // the closure on stream sc[k] (its bodies on the next two) and what follows it
+            auto closure = [&](bool mirrored, int k) -> cudaError_t {
+                RoundsLaunch R;
+                c3d_status rs = mirrored
+                                    ? rounds_setup(c, c->cellMapCount, c->u, c->alpha, c->iters,
+                                                   c->iterGamma, c->regIdx, c->status, c->cellMap,
+                                                   true, c->sc[k], R)
+                                    : rounds_setup(c, c->g.nall(), c->u, c->alpha, c->iters,
+                                                   c->iterGamma, c->regIdx, c->status, nullptr,
+                                                   true, c->sc[k], R);
+                if (rs != C3D_OK)
+                    return cudaErrorInvalidValue;
+                R.captureTop = top;
+                R.captureStreams = &c->sc[k];
+                cudaError_t er = launch_closure_rounds(R, c->gaunt);
+                cudaStream_t sk = c->sc[k];
+                if (er == cudaSuccess && mirrored) {
+                    er = launch_ghost_fill(c->g, c->alpha, c->numSMs, sk);
+                    if (er == cudaSuccess)
+                        er = launch_ghost_fill(c->g, c->u, c->numSMs, sk);
+                    for (int *a : {c->iters, c->iterGamma, c->regIdx, c->status})
+                        if (er == cudaSuccess)
+                            er = launch_ghost_fill_int(c->g, a, c->numSMs, sk);
+                    for (double *a : {c->cellGamma, c->cellErr})
+                        if (er == cudaSuccess)
+                            er = launch_ghost_fill_1(c->g, a, c->numSMs, sk);
+                    if (er == cudaSuccess)
+                        er = launch_ghost_stats(c->g, c->iters, c->iterGamma, c->regIdx, c->status,
+                                                c->stats, c->numSMs, sk);
+                }
+                if (er == cudaSuccess && R.psi)
+                    er = launch_psi_handoff(c->g, c->nq, c->M, c->alpha, mirrored, c->psiRefresh,
+                                            c->psiRefreshCount, c->psi, c->numSMs, sk);
+                return er;
+            };
+            if (ec == cudaSuccess && mirrorPath) {
+                ec = cudaMemsetAsync(c->mirrorFlag, 0, sizeof(int), s0);
+                if (ec == cudaSuccess)
+                    ec = launch_ghost_mirror_check(c->g, c->alpha, c->mirrorFlag, c->numSMs, s0);
+                cudaGraphConditionalHandle hIf;
+                if (ec == cudaSuccess)
+                    ec = cudaGraphConditionalHandleCreate(&hIf, top, 0, cudaGraphCondAssignDefault);
+                if (ec == cudaSuccess) {
+                    mirror_if_kernel<<<1, 32, 0, s0>>>(c->mirrorFlag, hIf);
+                    ec = cudaGetLastError();
+                }
+                cudaGraph_t *bodies = nullptr;
+                if (ec == cudaSuccess)
+                    ec = capture_conditional(s0, hIf, cudaGraphCondTypeIf, 2, &bodies);
+                for (int b = 0; b < 2 && ec == cudaSuccess; ++b) {
+                    ec = cudaStreamBeginCaptureToGraph(c->sc[1], bodies[b], nullptr, nullptr, 0,
+                                                       cudaStreamCaptureModeRelaxed);
+                    if (ec == cudaSuccess) {
+                        cudaError_t eb = closure(b == 0, 1);
+                        cudaGraph_t out = nullptr;
+                        ec = cudaStreamEndCapture(c->sc[1], &out);
+                        if (ec == cudaSuccess)
+                            ec = eb;
+                    }
+                }
+                launches += 3 + 9;
+            } else if (ec == cudaSuccess) {
+                ec = closure(false, 0);
+            }
+            if (ec == cudaSuccess)
+                ec = launch_kinetic_flux(c->g, c->alpha, c->mfA, c->mfP, c->xi, c->eta, c->nq,
+                                         c->qChunk, c->runLen, c->dx, c->dy, c->dz, c->theta, 0,
+                                         c->psi, handoff, c->flux, c->errorFlag, s0);
+            if (ec == cudaSuccess)
+                ec = launch_euler(c->g, c->u, c->flux, c->sigT, c->sigS, dt, c->numSMs, s0);
+            if (ec == cudaSuccess && stage == 1)
+                ec = launch_rk(c->g, c->u, c->uOld, 1, c->numSMs, s0);
+            launches += (handoff ? 1 + 2 : 2 * ceil_div(c->nq, c->qChunk)) + 1 + (stage == 1);
+            cudaGraph_t out = nullptr;
+            e = cudaStreamEndCapture(s0, &out);
+            if (e == cudaSuccess)
+                e = ec;
+        }
+        if (e == cudaSuccess)
+            e = cudaGraphInstantiate(&G.exec, top, 0);
+        cudaGraphDestroy(top);
+        G.launches = launches + (c->launches - l0); // the closure counted its round 0
+        c->launches = l0;
+        if (e != cudaSuccess) {
+            G.exec = nullptr;
+            for (cudaStream_t &x : c->sc) {
+                if (x)
+                    cudaStreamDestroy(x);
+                x = nullptr;
+            }
+            cudaGetLastError();
+            return fail(C3D_ERR_CUDA, std::string("c3d_stage: stage graph: ") +
+                                          cudaGetErrorString(e));
+        }
+        G.key = key;
+    }
+    G.used = ++c->sgTick;
+    C3D_CUDA(cudaGraphLaunch(G.exec, c->stream));
+    c->launches += G.launches;
+    c->psiReady = false;
+    *used = true;
+    return C3D_OK;
+}
+
 c3d_status c3d_stage(c3d_ctx *c, int stage, double dt)
 {
     if (!c || stage < 0 || stage > 1)
         return fail(C3D_ERR_INVALID, "c3d_stage: bad argument");
     c3d_status s;
+    bool used = false;
+    if ((s = stage_graph(c, stage, dt, &used)) != C3D_OK)
+        return s;
+    if (used)
+        return C3D_OK;
     if (stage == 0) {
         C3D_CUDA(launch_rk(c->g, c->u, c->uOld, 0, c->numSMs, c->stream));
         c->launches += 1;
@@ -1430,6 +1696,7 @@ c3d_status c3d_closure_stats_get(c3d_ctx *c, c3d_closure_stats *st)
     st->hessFp64 = (long long)h[STAT_H_FP64];
     st->escalated = (long long)h[STAT_ESCALATED];
     st->certified = (long long)h[STAT_CERTIFIED];
+    st->hostSyncs = c->hostSyncs;
     return C3D_OK;
 }
 

@@ -814,12 +814,9 @@ __device__ void escalate_fp64(S &sl, const Outputs &O, int lane)
 
 // gext (mixed precision): the FP64 moments <m_i e^{alpha.m}> and fqext = <e^{alpha.m}> of
 // the pass, from which g and f are formed instead of from row 0 of the reduced-precision H.
-// fqOnly: f from fqext (the quadrature sum) with g from row 0 of H (the mixed closure's FP64
-// visits).
 template <class S>
 __device__ void after_hessian(S &sl, const ClosureParams &P, const Outputs &O, int lane,
-                              double m0, const double *gext = nullptr, double fqext = 0.0,
-                              bool fqOnly = false)
+                              double m0, const double *gext = nullptr, double fqext = 0.0)
 {
     const int nm = P.nm;
     C3D_NCLK_DECL
@@ -836,7 +833,7 @@ __device__ void after_hessian(S &sl, const ClosureParams &P, const Outputs &O, i
     }
     double f = 0.0;
     if (lane == 0) {
-        f = (gext || fqOnly) ? fqext : sl.L[0] / (m0 * m0);
+        f = gext ? fqext : sl.L[0] / (m0 * m0);
         for (int i = 0; i < nm; ++i)
             f = __dsub_rn(f, __dmul_rn(sl.alpha[i], sl.u[i]));
     }

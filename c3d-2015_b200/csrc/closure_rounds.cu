@@ -17,6 +17,7 @@
 // needs many iterations only ever occupies the short lists of later rounds.
 #include "closure_core.cuh"
 
+#include <mutex>
 #include <vector>
 #include "rounds_launch.h"
 #include "umma.cuh"
@@ -255,16 +256,14 @@ __global__ void __launch_bounds__(RW * 32, 2)
                 z1 = __dadd_rn(z1, __dmul_rn(a.y, m));
             }
             const double wq = ch[nm2 * QCP + lane];
-            // the quadrature sum of f: for trials, and in the mixed closure for FP64 Hessian
-            // visits too (their base objective, summed like the trials')
             if (need[0] != NEED_NONE) {
                 c0 = __dmul_rn(wq, exp(z0));
-                if (need[0] == NEED_TRIAL || P.mixed)
+                if (need[0] == NEED_TRIAL)
                     fpart0 = __dadd_rn(fpart0, c0);
             }
             if (need[1] != NEED_NONE) {
                 c1 = __dmul_rn(wq, exp(z1));
-                if (need[1] == NEED_TRIAL || P.mixed)
+                if (need[1] == NEED_TRIAL)
                     fpart1 = __dadd_rn(fpart1, c1);
             }
         }
@@ -314,9 +313,9 @@ __global__ void __launch_bounds__(RW * 32, 2)
     }
     const double fq0 = warp_sum(fpart0), fq1 = warp_sum(fpart1);
     if (lane == 0) {
-        if (need[0] == NEED_TRIAL || (P.mixed && need[0] == NEED_H))
+        if (need[0] == NEED_TRIAL)
             state[cell[0]].s.fquad = fq0;
-        if (need[1] == NEED_TRIAL || (P.mixed && need[1] == NEED_H))
+        if (need[1] == NEED_TRIAL)
             state[cell[1]].s.fquad = fq1;
     }
 }
@@ -964,9 +963,6 @@ __global__ void __launch_bounds__(RWN * 32)
                 const double *e = buf + (size_t)pos * BSTR + NM2P;
                 after_hessian(sl, P, O, lane, m0, e, e[NMP]);
             }
-        } else if (GAUNT && P.mixed) {
-            // FP64 visit of the mixed closure: f from the quadrature sum, as for its trials
-            after_hessian(sl, P, O, lane, m0, nullptr, sl.s.fquad, true);
         } else {
             after_hessian(sl, P, O, lane, m0);
         }
@@ -1070,13 +1066,15 @@ struct TierHandles {
     cudaGraphConditionalHandle h[NLISTS];
 };
 
-// Picks each used list's launch size (SWITCH branch; NTIER = none) from its counter; bit l of
-// mask marks list l as used.
-__global__ void rounds_tier_kernel(const Lists in, TierHandles th, unsigned int mask, long long cap,
-                                   unsigned long long *launches)
+// Picks each used list's launch size (SWITCH branch; NTIER = none) from its counter (bit l of
+// mask marks list l as used) and clears the counters of the lists the round fills.
+__global__ void rounds_tier_kernel(const Lists in, Lists out, TierHandles th, unsigned int mask,
+                                   long long cap, unsigned long long *launches)
 {
     if (threadIdx.x != 0)
         return;
+    for (int l = 0; l < NLISTS; ++l)
+        *out.count[l] = 0;
     unsigned long long l2 = 1;
     for (int l = 0; l < NLISTS; ++l) {
         if (!((mask >> l) & 1u))
@@ -1092,7 +1090,7 @@ __global__ void rounds_tier_kernel(const Lists in, TierHandles th, unsigned int 
         l2 += t < NTIER ? 2 : 0;
     }
     if (launches)
-        atomicAdd(launches, l2 + 1); // + the carry kernel
+        atomicAdd(launches, l2);
 }
 
 // Entries past cap stay for the next round: appended to that round's list.
@@ -1139,7 +1137,7 @@ __global__ void rounds_cond_kernel(const Lists in, unsigned int mask, unsigned i
 }
 
 // Appends a conditional node after the current dependencies of the graph being captured on st.
-static cudaError_t capture_conditional(cudaStream_t st, cudaGraphConditionalHandle h,
+cudaError_t capture_conditional(cudaStream_t st, cudaGraphConditionalHandle h,
                                        cudaGraphConditionalNodeType type, unsigned int size,
                                        cudaGraph_t **bodies)
 {
@@ -1166,16 +1164,32 @@ static cudaError_t capture_conditional(cudaStream_t st, cudaGraphConditionalHand
     return e;
 }
 
-// The instantiated closure graph of one configuration (rebuilt when any launch parameter
-// changes), with the streams its capture uses.
+// Graph capture and instantiation run one thread at a time in the process (contexts driven
+// from several host threads, as the serving loop does, build their graphs in turn; launches of
+// built graphs do not wait).
+std::mutex &graph_build_mutex()
+{
+    static std::mutex m;
+    return m;
+}
+
+// The instantiated closure graphs of the last few configurations (a configuration is every
+// launch parameter; switching, e.g., between precisions reuses its graph), with the streams
+// their capture uses.
 struct RoundsGraph {
-    std::vector<unsigned char> key;
-    cudaGraphExec_t exec = nullptr;
+    static constexpr int SLOTS = 6;
+    struct Slot {
+        std::vector<unsigned char> key;
+        cudaGraphExec_t exec = nullptr;
+        unsigned long long used = 0;
+    } slot[SLOTS];
+    unsigned long long tick = 0;
     cudaStream_t cs[3] = {nullptr, nullptr, nullptr};
     ~RoundsGraph()
     {
-        if (exec)
-            cudaGraphExecDestroy(exec);
+        for (Slot &s : slot)
+            if (s.exec)
+                cudaGraphExecDestroy(s.exec);
         for (cudaStream_t s : cs)
             if (s)
                 cudaStreamDestroy(s);
@@ -1282,9 +1296,10 @@ template <int NT, int NT2, bool GAUNT> static cudaError_t rounds_t(const RoundsL
         A.count[l] = R.counts + l;
         B.count[l] = R.counts + NLISTS + l;
     }
-    // the lists a round can fill: FP64 Hessian passes, the mixed closure's BF16 and 3xTF32
-    // ones, and probe passes (first visits; set up with the probe kernels' launch attributes)
-    const unsigned int usedLists = 1u | (mixed ? 6u : 0u) | (probe ? 8u : 0u);
+    // the lists the graph's rounds can fill: FP64 Hessian passes and, when the mixed closure
+    // routes any visit to reduced precision, its BF16 and 3xTF32 ones (probe passes happen in
+    // round 0 only: no later visit is a first visit)
+    const unsigned int usedLists = 1u | (mixed && P.mixIterMax > 0 ? 6u : 0u);
 
     // pass + Newton kernels of list l: entries la[0 .. nb) (with nDev, at most *nDev of them),
     // the cells still in need appended to out
@@ -1376,98 +1391,114 @@ template <int NT, int NT2, bool GAUNT> static cudaError_t rounds_t(const RoundsL
         return cudaGetLastError();
     };
 
+    // Appends the closure to the graph being captured on cs[0] (top: that capture's top-level
+    // graph, which owns the conditional handles); cs[1], cs[2] capture the loop and switch
+    // bodies.
+    auto capture_into = [&](cudaGraph_t top, cudaStream_t const *cs) -> cudaError_t {
+        const long long cap = R.batch;
+        cudaGraphConditionalHandle hLoop;
+        TierHandles th[2];
+        cudaError_t ec = cudaGraphConditionalHandleCreate(&hLoop, top, 1, cudaGraphCondAssignDefault);
+        // one handle per SWITCH node the graph has (a handle without its node makes the
+        // graph invalid)
+        for (int hr = 0; hr < 2 && ec == cudaSuccess; ++hr)
+            for (int l = 0; l < NLISTS && ec == cudaSuccess; ++l)
+                if ((usedLists >> l) & 1u)
+                    ec = cudaGraphConditionalHandleCreate(&th[hr].h[l], top, NTIER,
+                                                          cudaGraphCondAssignDefault);
+        if (ec == cudaSuccess)
+            ec = cudaMemsetAsync(R.counts + 2 * NLISTS, 0, sizeof(unsigned int), cs[0]);
+        const long long launches0 = *R.launches;
+        if (ec == cudaSuccess)
+            ec = round0(cs[0]);
+        *R.launches = launches0;
+        cudaGraph_t *loopBody = nullptr;
+        if (ec == cudaSuccess)
+            ec = capture_conditional(cs[0], hLoop, cudaGraphCondTypeWhile, 1, &loopBody);
+        if (ec == cudaSuccess)
+            ec = cudaStreamBeginCaptureToGraph(cs[1], loopBody[0], nullptr, nullptr, 0,
+                                               cudaStreamCaptureModeRelaxed);
+        if (ec != cudaSuccess)
+            return ec;
+        for (int hr = 0; hr < 2 && ec == cudaSuccess; ++hr) {
+            const Lists &X = hr == 0 ? A : B, &Y = hr == 0 ? B : A;
+            rounds_tier_kernel<<<1, 32, 0, cs[1]>>>(X, Y, th[hr], usedLists, cap, R.launchDev);
+            ec = cudaGetLastError();
+            for (int l = 0; l < NLISTS && ec == cudaSuccess; ++l) {
+                if (!((usedLists >> l) & 1u))
+                    continue;
+                cudaGraph_t *tiers = nullptr;
+                ec = capture_conditional(cs[1], th[hr].h[l], cudaGraphCondTypeSwitch, NTIER, &tiers);
+                for (int t = 0; t < NTIER && ec == cudaSuccess; ++t) {
+                    ec = cudaStreamBeginCaptureToGraph(cs[2], tiers[t], nullptr, nullptr, 0,
+                                                       cudaStreamCaptureModeRelaxed);
+                    if (ec == cudaSuccess) {
+                        cudaError_t el = launch_list(l, X.list[l], (int)tier_entries(t, cap),
+                                                     X.count[l], Y, cs[2]);
+                        cudaGraph_t body = nullptr;
+                        ec = cudaStreamEndCapture(cs[2], &body);
+                        if (ec == cudaSuccess)
+                            ec = el;
+                    }
+                }
+            }
+            if (ec == cudaSuccess && cap < R.ncells) { // no list can outgrow cap otherwise
+                rounds_carry_kernel<<<1, 1024, 0, cs[1]>>>(X, Y, usedLists, cap);
+                ec = cudaGetLastError();
+            }
+        }
+        if (ec == cudaSuccess) {
+            rounds_cond_kernel<<<1, 32, 0, cs[1]>>>(A, usedLists, R.counts + 2 * NLISTS,
+                                                    R.maxRounds, R.errorFlag, hLoop, R.launchDev);
+            ec = cudaGetLastError();
+        }
+        cudaGraph_t body = nullptr;
+        cudaError_t eb = cudaStreamEndCapture(cs[1], &body);
+        return ec == cudaSuccess ? eb : ec;
+    };
+
+    const long long round0Launches = probe ? 2 * ((R.ncells + R.batch - 1) / R.batch) : 1;
+    if (R.captureTop) {
+        // inside the capture of a whole RK stage
+        e = capture_into(R.captureTop, R.captureStreams);
+        if (e == cudaSuccess)
+            *R.launches += round0Launches + 1;
+        return e;
+    }
     if (R.graphs) {
-        RoundsGraph *G = reinterpret_cast<RoundsGraph *>(R.graphs);
+        RoundsGraph *RG = reinterpret_cast<RoundsGraph *>(R.graphs);
         std::vector<unsigned char> key = rounds_key(R, GAUNT);
-        const long long round0Launches = probe ? 2 * ((R.ncells + R.batch - 1) / R.batch) : 1;
-        if (!G->exec || G->key != key) {
+        RoundsGraph::Slot *G = nullptr;
+        for (RoundsGraph::Slot &s : RG->slot)
+            if (s.exec && s.key == key)
+                G = &s;
+        if (!G) {
+            std::lock_guard<std::mutex> lk(graph_build_mutex());
+            // the least recently used slot; a graph in it may still run on the stream and is
+            // destroyed once the stream is idle
+            G = &RG->slot[0];
+            for (RoundsGraph::Slot &s : RG->slot)
+                if (s.used < G->used)
+                    G = &s;
             if (G->exec) {
+                if ((e = cudaStreamSynchronize(st)) != cudaSuccess)
+                    return e;
                 cudaGraphExecDestroy(G->exec);
                 G->exec = nullptr;
             }
             for (int i = 0; i < 3; ++i)
-                if (!G->cs[i] && (e = cudaStreamCreateWithFlags(&G->cs[i], cudaStreamNonBlocking)) !=
-                                     cudaSuccess)
+                if (!RG->cs[i] && (e = cudaStreamCreateWithFlags(&RG->cs[i], cudaStreamNonBlocking)) !=
+                                      cudaSuccess)
                     return e;
-            const long long cap = R.batch;
             cudaGraph_t top = nullptr;
             if ((e = cudaGraphCreate(&top, 0)) != cudaSuccess)
                 return e;
-            cudaGraphConditionalHandle hLoop;
-            TierHandles th[2];
-            e = cudaGraphConditionalHandleCreate(&hLoop, top, 1, cudaGraphCondAssignDefault);
-            // one handle per SWITCH node the graph has (a handle without its node makes the
-            // graph invalid)
-            for (int hr = 0; hr < 2 && e == cudaSuccess; ++hr)
-                for (int l = 0; l < NLISTS && e == cudaSuccess; ++l)
-                    if ((usedLists >> l) & 1u)
-                        e = cudaGraphConditionalHandleCreate(&th[hr].h[l], top, NTIER,
-                                                             cudaGraphCondAssignDefault);
-            if (e == cudaSuccess)
-                e = cudaStreamBeginCaptureToGraph(G->cs[0], top, nullptr, nullptr, 0,
-                                                  cudaStreamCaptureModeRelaxed);
+            e = cudaStreamBeginCaptureToGraph(RG->cs[0], top, nullptr, nullptr, 0,
+                                              cudaStreamCaptureModeRelaxed);
             if (e == cudaSuccess) {
-                const long long launches0 = *R.launches;
-                cudaError_t ec = cudaMemsetAsync(R.counts + 2 * NLISTS, 0, sizeof(unsigned int),
-                                                 G->cs[0]);
-                if (ec == cudaSuccess)
-                    ec = round0(G->cs[0]);
-                *R.launches = launches0;
-                cudaGraph_t *loopBody = nullptr;
-                if (ec == cudaSuccess)
-                    ec = capture_conditional(G->cs[0], hLoop, cudaGraphCondTypeWhile, 1, &loopBody);
-                if (ec == cudaSuccess)
-                    ec = cudaStreamBeginCaptureToGraph(G->cs[1], loopBody[0], nullptr, nullptr, 0,
-                                                       cudaStreamCaptureModeRelaxed);
-                if (ec == cudaSuccess) {
-                    for (int hr = 0; hr < 2 && ec == cudaSuccess; ++hr) {
-                        const Lists &X = hr == 0 ? A : B, &Y = hr == 0 ? B : A;
-                        ec = cudaMemsetAsync(Y.count[0], 0, NLISTS * sizeof(unsigned int),
-                                             G->cs[1]);
-                        if (ec == cudaSuccess) {
-                            rounds_tier_kernel<<<1, 32, 0, G->cs[1]>>>(X, th[hr], usedLists, cap,
-                                                                      R.launchDev);
-                            ec = cudaGetLastError();
-                        }
-                        for (int l = 0; l < NLISTS && ec == cudaSuccess; ++l) {
-                            if (!((usedLists >> l) & 1u))
-                                continue;
-                            cudaGraph_t *tiers = nullptr;
-                            ec = capture_conditional(G->cs[1], th[hr].h[l], cudaGraphCondTypeSwitch,
-                                                     NTIER, &tiers);
-                            for (int t = 0; t < NTIER && ec == cudaSuccess; ++t) {
-                                ec = cudaStreamBeginCaptureToGraph(G->cs[2], tiers[t], nullptr,
-                                                                   nullptr, 0,
-                                                                   cudaStreamCaptureModeRelaxed);
-                                if (ec == cudaSuccess) {
-                                    cudaError_t el = launch_list(
-                                        l, X.list[l], (int)tier_entries(t, cap), X.count[l], Y,
-                                        G->cs[2]);
-                                    cudaGraph_t body = nullptr;
-                                    ec = cudaStreamEndCapture(G->cs[2], &body);
-                                    if (ec == cudaSuccess)
-                                        ec = el;
-                                }
-                            }
-                        }
-                        if (ec == cudaSuccess) {
-                            rounds_carry_kernel<<<1, 1024, 0, G->cs[1]>>>(X, Y, usedLists, cap);
-                            ec = cudaGetLastError();
-                        }
-                    }
-                    if (ec == cudaSuccess) {
-                        rounds_cond_kernel<<<1, 32, 0, G->cs[1]>>>(
-                            A, usedLists, R.counts + 2 * NLISTS, R.maxRounds, R.errorFlag, hLoop,
-                            R.launchDev);
-                        ec = cudaGetLastError();
-                    }
-                    cudaGraph_t body = nullptr;
-                    cudaError_t eb = cudaStreamEndCapture(G->cs[1], &body);
-                    if (ec == cudaSuccess)
-                        ec = eb;
-                }
+                const cudaError_t ec = capture_into(top, RG->cs);
                 cudaGraph_t topOut = nullptr;
-                e = cudaStreamEndCapture(G->cs[0], &topOut);
+                e = cudaStreamEndCapture(RG->cs[0], &topOut);
                 if (e == cudaSuccess)
                     e = ec;
             }
@@ -1477,7 +1508,7 @@ template <int NT, int NT2, bool GAUNT> static cudaError_t rounds_t(const RoundsL
             if (e != cudaSuccess) {
                 // a failed capture may leave its streams unusable: start over with new ones
                 G->exec = nullptr;
-                for (cudaStream_t &cs : G->cs) {
+                for (cudaStream_t &cs : RG->cs) {
                     if (cs)
                         cudaStreamDestroy(cs);
                     cs = nullptr;
@@ -1487,6 +1518,7 @@ template <int NT, int NT2, bool GAUNT> static cudaError_t rounds_t(const RoundsL
             }
             G->key = key;
         }
+        G->used = ++RG->tick;
         *R.launches += round0Launches + 1;
         return cudaGraphLaunch(G->exec, st);
     }
@@ -1503,6 +1535,8 @@ template <int NT, int NT2, bool GAUNT> static cudaError_t rounds_t(const RoundsL
             e = cudaStreamSynchronize(st);
         if (e != cudaSuccess)
             return e;
+        if (R.hostSyncs)
+            ++*R.hostSyncs;
         long long cnt[NLISTS], total = 0;
         for (int l = 0; l < NLISTS; ++l)
             total += (cnt[l] = R.hostCount[l]);

@@ -4,6 +4,7 @@
 #include "c3d_common.cuh"
 
 #include <cstddef>
+#include <mutex>
 
 namespace c3d {
 
@@ -38,6 +39,7 @@ struct RoundsLaunch {
     int *errorFlag;
     cudaStream_t stream;
     long long *launches;
+    long long *hostSyncs; // host-driven rounds: one wait per round
     long long maxRounds;
     // ansatz hand-off to the kinetic flux (null psi: none): psi[q psiNall + c] of every cell
     // the probe solves, and the list (with its device count) of cells whose psi is rewritten
@@ -50,6 +52,11 @@ struct RoundsLaunch {
     // counter of the kernels its loop launches
     void *graphs;
     unsigned long long *launchDev;
+    // capture into an RK stage's graph (null: launch): the closure is appended to the graph
+    // being captured on captureStreams[0], whose top-level graph is captureTop;
+    // captureStreams[1], [2] capture the loop and switch bodies
+    cudaGraph_t captureTop;
+    cudaStream_t *captureStreams;
 };
 
 cudaError_t launch_closure_rounds(const RoundsLaunch &R, bool gaunt);
@@ -58,6 +65,12 @@ size_t rounds_buf_doubles(int nm, int nm2, bool gaunt, bool mixed);
 size_t mixed_a_chunk_bytes(int nm2, int fmt);
 bool rounds_gaunt_supported(int nm);
 void *rounds_graph_new();
+std::mutex &graph_build_mutex(); // held while a graph is captured and instantiated
+// Appends a conditional node (WHILE, IF or SWITCH with size bodies) after the current
+// dependencies of the graph being captured on st; *bodies receives its body graphs.
+cudaError_t capture_conditional(cudaStream_t st, cudaGraphConditionalHandle h,
+                                cudaGraphConditionalNodeType type, unsigned int size,
+                                cudaGraph_t **bodies);
 void rounds_graph_free(void *g);
 
 } // namespace c3d

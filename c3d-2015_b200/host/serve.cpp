@@ -100,6 +100,11 @@ void c3d_server::run(Request &r)
     c3d_host::Solver s;
     int steps = 0;
     c3d_status st = s.init(r.cfg, nullptr);
+    // launch by launch: capturing CUDA graphs on worker threads while other workers create,
+    // free and synchronise their contexts crashed the process in testing (cause not found),
+    // so the serving loop's problems do not use the stage and closure graphs
+    if (st == C3D_OK && s.ctx())
+        st = c3d_set_graphs(s.ctx(), 0);
     if (st == C3D_OK)
         st = s.run(&steps);
     if (st == C3D_OK || st == C3D_ERR_CLOSURE) {

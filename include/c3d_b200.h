@@ -126,6 +126,8 @@ typedef struct {
     long long hessFp64;        /*   ... with FP64 moments */
     long long escalated;       /*   reduced-precision visits redone in FP64 */
     long long certified;       /* first visits ended by the convergence certificate */
+    long long hostSyncs;       /* host waits inside the stages since creation (the face-ghost
+                                  mirror check and host-driven rounds; 0 with graphs) */
 } c3d_closure_stats;
 
 /* Creates a context on the current CUDA device with the tables M[nq*nm],
