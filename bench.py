@@ -356,72 +356,198 @@ def standalone_vectors(c3d, N, n):
     return q, u, a_iso
 
 
+HIST_EDGES = [1, 2, 4, 8, 16, 32, 64, 128]  # iteration-count bins [1], [2,3], [4,7], ...
+STANDALONE_REF_SAMPLE_S = 2.0               # CPU seconds of the reference per order
+
+
+def _hist(iters):
+    h = np.histogram(iters, bins=HIST_EDGES + [1 << 30])[0]
+    return [int(x) for x in h]
+
+
+def _ref_standalone_worker(conn, nm, nm2, nq, u, a, w, M, M2, tol, ladder, target_s):
+    """Spawned process (one per order: opt() sizes its thread-private scratch once): the
+    reference's unbatched opt() (src/opt/opt.cpp:139-355) over the vectors with OpenMP, on a
+    prefix sized for about target_s seconds."""
+    L = ctypes.CDLL(os.path.join(REPO, "oracle", "_ref", "libc3dref.so"))
+    lad = np.array([float(x) for x in ladder.split(",")])
+    L.c3dref_set_ladder(len(lad), lad.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+    L.c3dref_opt_init(nm, nm2)
+    dp, ip = ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)
+    L.c3dref_opt_many.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_long, dp,
+                                  dp, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                  ctypes.c_double, dp, dp, dp, ip, ip, dp]
+
+    def run(n):
+        uu, aa = np.ascontiguousarray(u[:n]).copy(), np.ascontiguousarray(a[:n]).copy()
+        it = np.zeros(n, np.int32)
+        t0 = time.perf_counter()
+        L.c3dref_opt_many(nm, nm2, nq, n, uu.ctypes.data_as(dp), aa.ctypes.data_as(dp), 100,
+                          tol, 1.1, 1e10, w.ctypes.data_as(dp), M.ctypes.data_as(dp),
+                          M2.ctypes.data_as(dp), it.ctypes.data_as(ip), None, None)
+        return time.perf_counter() - t0, aa, it
+    threads = L.c3dref_num_threads()
+    n0 = min(len(u), 8 * threads)
+    t, _, _ = run(n0)
+    n = int(min(len(u), max(n0, n0 / max(t, 1e-6) * target_s)))
+    t, aa, it = run(n)
+    conn.send(dict(n=n, seconds=t, threads=threads, alpha=aa, iters=it))
+    conn.close()
+
+
+def ref_standalone(q, u, a_iso):
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    r, w = ctx.Pipe(duplex=False)
+    M2 = c3d_quadrature_m2(q)
+    p = ctx.Process(target=_ref_standalone_worker,
+                    args=(w, q["nm"], q["nm2"], q["nq"], u, a_iso, q["w"], q["M"], M2,
+                          STANDALONE_TOL, STANDALONE_LADDER, STANDALONE_REF_SAMPLE_S))
+    p.start()
+    w.close()
+    res = r.recv()
+    p.join()
+    return res
+
+
+def c3d_quadrature_m2(q):
+    import c3d
+    return c3d.quadrature(q["N"], q["Q"], with_m2=True)["M2"]
+
+
 def standalone_closure(torch, c3d, stream, graphs=True):
-    """FP64 vs mixed closure of the standalone workload (one context per order, Gaunt form).
-    Unbatched rules
-    (|g| <= |u| MN_TOL, gamma <= 1.1), MN_TOL 1e-8. Device-resident vectors, CUDA events
-    around each c3d_closure_vectors call after an untimed solve of the same vectors. For
-    N <= 2 the mixed closure keeps FP64 Hessians (c3d_set_precision)."""
+    """FP64 vs mixed closure of the standalone workload (one context per order, Gaunt form,
+    unbatched rules: |g| <= |u| MN_TOL, gamma <= 1.1, MN_TOL 1e-8). Device-resident vectors;
+    CUDA events around each solve after an untimed solve of the same vectors. Headline: all
+    seven orders in ONE launch (c3d_group_closure_vectors: one CUDA graph whose branches are
+    the orders' closures); per order, its own closure call (iteration histograms, failures,
+    mixed vs FP64) and the reference's opt() on a bounded sample of its vectors (rate on the
+    host cores, multipliers and iteration counts against the GPU's). For N <= 2 the mixed
+    closure keeps FP64 Hessians (c3d_set_precision)."""
     L = c3d.lib()
     per_n, tot = [], {0: [0, 0.0], 1: [0, 0.0]}
-    diffs = []
-    for N in range(1, 8):
-        q, u, a_iso = standalone_vectors(c3d, N, STANDALONE_PER_N)
+    diffs, ref_rows = [], []
+    solvers, vecs = [], []
+
+    def bufs(u, a):
         n = len(u)
-        with tempfile.TemporaryDirectory() as tmp:
-            deck = os.path.join(tmp, "input.deck")
-            kv = dict(SOLVER="mn", TFINAL="1", OUTDT="1000", OUTPUT_DATA="false",
-                      OUTPUT_OPT_STATS="false", OUTPUT_TIMINGS="false", NX=2, NY=2, NZ=2,
-                      MPIX=1, MPIY=1, MPIZ=1, AX=-1, AY=-1, AZ=-1, BX=1, BY=1, BZ=1,
-                      MOMENT_ORDER=N, QUAD_ORDER=2 * (N + 3), CFL_FACTOR=0.5, CROSS_SECTION=1.0,
-                      INIT_FLOOR=1e-4, GAUSS_SIGMA=0.1, INIT_COND="gaussian_psi", THETA=2.0,
-                      OMP_THREADS=1, PN_USE_KINETIC_FLUX=0, MN_TOL=STANDALONE_TOL,
-                      MN_TOL_GAMMA=1.1, MN_COND_H_MAX=1e10, MN_MAX_ITER=100, MN_BATCHED="false",
-                      MN_USE_GAUNT_COEF="true", MN_USE_GAUNT_SPARSE="true", CUDA_KINETIC="true",
-                      CUDA_BATCHED="true", CUDA_BATCH_SIZE=50, REG_LADDER=STANDALONE_LADDER)
-            with open(deck, "w") as f:
-                f.write("".join(f"{k} {v}\n" for k, v in kv.items()))
-            solver = c3d.Solver(deck, stream=ctypes.c_void_p(stream.cuda_stream))
-        h = solver.ctx_handle
-        c3d.check(L.c3d_set_graphs(h, 1 if graphs else 0), "graphs")
-        row = dict(N=N, nm=q["nm"], nq=q["nq"], vectors=n)
-        alphas = {}
-        for mode in (0, 1):
-            c3d.check(L.c3d_set_precision(h, mode, 0.0, 0.0, 0, 0.0), "precision")
-            for warm in (True, False):
-                # the untimed pass is the full solve too: every kernel the timed one launches
-                # (rare-path rounds included) is loaded before the events
-                m = n
-                du = torch.tensor(u[:m], device="cuda")
-                da = torch.tensor(a_iso[:m], device="cuda")
-                it = torch.zeros(m, dtype=torch.int32, device="cuda")
-                stt = torch.zeros(m, dtype=torch.int32, device="cuda")
-                torch.cuda.synchronize()
-                e0 = torch.cuda.Event(enable_timing=True)
-                e1 = torch.cuda.Event(enable_timing=True)
-                e0.record(stream)
-                c3d.check(L.c3d_closure_vectors(h, m, ctypes.c_void_p(du.data_ptr()),
-                                                ctypes.c_void_p(da.data_ptr()),
-                                                ctypes.c_void_p(it.data_ptr()), None, None,
-                                                ctypes.c_void_p(stt.data_ptr())), "closure")
-                e1.record(stream)
-                torch.cuda.synchronize()
-            ms = e0.elapsed_time(e1)
-            key = "fp64" if mode == 0 else "mixed"
-            row[key] = dict(solves_per_s=n / (ms * 1e-3), ms=ms,
-                            iters_per_solve=float(it.double().mean()),
-                            failed=int((stt != 0).sum()))
-            tot[mode][0] += n
-            tot[mode][1] += ms
-            alphas[mode] = da.cpu().numpy()
-        d = np.linalg.norm(alphas[1] - alphas[0], axis=1) / np.linalg.norm(alphas[0], axis=1)
-        diffs.append(d)
-        f, x = row["fp64"], row["mixed"]
-        per_n.append([N, round(f["solves_per_s"]), round(x["solves_per_s"]),
-                      round(x["solves_per_s"] / f["solves_per_s"], 3),
-                      round(f["iters_per_solve"], 3), round(x["iters_per_solve"], 3),
-                      f["failed"], x["failed"], float("%.3g" % np.median(d))])
-        solver.close()
+        return (torch.tensor(u, device="cuda"), torch.tensor(a, device="cuda"),
+                torch.zeros(n, dtype=torch.int32, device="cuda"),
+                torch.zeros(n, dtype=torch.int32, device="cuda"))
+
+    try:
+        for N in range(1, 8):
+            q, u, a_iso = standalone_vectors(c3d, N, STANDALONE_PER_N)
+            n = len(u)
+            with tempfile.TemporaryDirectory() as tmp:
+                deck = os.path.join(tmp, "input.deck")
+                kv = dict(SOLVER="mn", TFINAL="1", OUTDT="1000", OUTPUT_DATA="false",
+                          OUTPUT_OPT_STATS="false", OUTPUT_TIMINGS="false", NX=2, NY=2, NZ=2,
+                          MPIX=1, MPIY=1, MPIZ=1, AX=-1, AY=-1, AZ=-1, BX=1, BY=1, BZ=1,
+                          MOMENT_ORDER=N, QUAD_ORDER=2 * (N + 3), CFL_FACTOR=0.5,
+                          CROSS_SECTION=1.0, INIT_FLOOR=1e-4, GAUSS_SIGMA=0.1,
+                          INIT_COND="gaussian_psi", THETA=2.0, OMP_THREADS=1,
+                          PN_USE_KINETIC_FLUX=0, MN_TOL=STANDALONE_TOL, MN_TOL_GAMMA=1.1,
+                          MN_COND_H_MAX=1e10, MN_MAX_ITER=100, MN_BATCHED="false",
+                          MN_USE_GAUNT_COEF="true", MN_USE_GAUNT_SPARSE="true",
+                          CUDA_KINETIC="true", CUDA_BATCHED="true", CUDA_BATCH_SIZE=50,
+                          REG_LADDER=STANDALONE_LADDER)
+                with open(deck, "w") as f:
+                    f.write("".join(f"{k} {v}\n" for k, v in kv.items()))
+                solver = c3d.Solver(deck, stream=ctypes.c_void_p(stream.cuda_stream))
+            solvers.append(solver)
+            vecs.append((u, a_iso))
+            h = solver.ctx_handle
+            c3d.check(L.c3d_set_graphs(h, 1 if graphs else 0), "graphs")
+            row = dict(N=N, nm=q["nm"], nq=q["nq"], vectors=n)
+            alphas, iters = {}, {}
+            for mode in (0, 1):
+                c3d.check(L.c3d_set_precision(h, mode, 0.0, 0.0, 0, 0.0), "precision")
+                for warm in (True, False):
+                    # the untimed pass is the full solve too: every kernel the timed one
+                    # launches (rare-path rounds included) is loaded before the events
+                    du, da, it, stt = bufs(u, a_iso)
+                    torch.cuda.synchronize()
+                    e0 = torch.cuda.Event(enable_timing=True)
+                    e1 = torch.cuda.Event(enable_timing=True)
+                    e0.record(stream)
+                    c3d.check(L.c3d_closure_vectors(h, n, ctypes.c_void_p(du.data_ptr()),
+                                                    ctypes.c_void_p(da.data_ptr()),
+                                                    ctypes.c_void_p(it.data_ptr()), None, None,
+                                                    ctypes.c_void_p(stt.data_ptr())), "closure")
+                    e1.record(stream)
+                    torch.cuda.synchronize()
+                ms = e0.elapsed_time(e1)
+                key = "fp64" if mode == 0 else "mixed"
+                row[key] = dict(solves_per_s=n / (ms * 1e-3), ms=ms,
+                                iters_per_solve=float(it.double().mean()),
+                                failed=int((stt != 0).sum()))
+                tot[mode][0] += n
+                tot[mode][1] += ms
+                alphas[mode] = da.cpu().numpy()
+                iters[mode] = it.cpu().numpy()
+                if mode == 0:
+                    ok0 = stt.cpu().numpy() == 0
+            d = np.linalg.norm(alphas[1] - alphas[0], axis=1) / np.linalg.norm(alphas[0], axis=1)
+            diffs.append(d)
+            f, x = row["fp64"], row["mixed"]
+            per_n.append([N, round(f["solves_per_s"]), round(x["solves_per_s"]),
+                          round(x["solves_per_s"] / f["solves_per_s"], 3),
+                          round(f["iters_per_solve"], 3), round(x["iters_per_solve"], 3),
+                          f["failed"], x["failed"], float("%.3g" % np.median(d)),
+                          _hist(iters[0]), _hist(iters[1])])
+            # the reference's opt() on a prefix of the same vectors, without those the FP64
+            # closure reports as exhausting the ladder (there the reference aborts,
+            # src/opt/opt.cpp:261-266)
+            try:
+                rr = ref_standalone(q, u[ok0], a_iso[ok0])
+                m = rr["n"]
+                ra = rr["alpha"]
+                ok = np.isfinite(ra).all(axis=1)
+
+                def err(ag):
+                    g = ag[ok0][:m][ok]
+                    e = np.linalg.norm(g - ra[ok], axis=1) / np.linalg.norm(ra[ok], axis=1)
+                    return [float("%.3g" % np.median(e)), float("%.3g" % np.percentile(e, 99))]
+                ref_rows.append([N, m, round(m / rr["seconds"]), rr["threads"],
+                                 float("%.4g" % np.mean(rr["iters"] == iters[0][ok0][:m])),
+                                 err(alphas[0]), err(alphas[1])])
+            except Exception as ex:  # reported, not fatal
+                ref_rows.append([N, f"failed: {ex}"])
+        group = None
+        if graphs:
+            # all seven orders in one launch: one CUDA graph, the orders' closures as its
+            # parallel branches
+            G = c3d.Group([s.ctx_handle for s in solvers])
+            counts = [len(u) for u, _ in vecs]
+            group = dict(launches=1, vectors=int(sum(counts)))
+            for mode in (0, 1):
+                for s in solvers:
+                    c3d.check(L.c3d_set_precision(s.ctx_handle, mode, 0.0, 0.0, 0, 0.0), "prec")
+                for warm in (True, False):
+                    gb = [bufs(u, a) for u, a in vecs]
+                    torch.cuda.synchronize()
+                    e0 = torch.cuda.Event(enable_timing=True)
+                    e1 = torch.cuda.Event(enable_timing=True)
+                    e0.record(stream)
+                    G.closure_vectors(counts, [b[0].data_ptr() for b in gb],
+                                      [b[1].data_ptr() for b in gb],
+                                      iters=[b[2].data_ptr() for b in gb],
+                                      status=[b[3].data_ptr() for b in gb])
+                    e1.record(stream)
+                    torch.cuda.synchronize()
+                for s in solvers:
+                    s.sync()
+                ms = e0.elapsed_time(e1)
+                key = "fp64" if mode == 0 else "mixed"
+                group[key + "_solves_per_s"] = group["vectors"] / (ms * 1e-3)
+                group[key + "_ms"] = ms
+                group[key + "_failed"] = int(sum(int((b[3] != 0).sum()) for b in gb))
+            group["mixed_over_fp64"] = group["mixed_solves_per_s"] / group["fp64_solves_per_s"]
+            G.close()
+    finally:
+        for s in solvers:
+            s.close()
     dall = np.concatenate(diffs)
     f64 = tot[0][0] / (tot[0][1] * 1e-3)
     mix = tot[1][0] / (tot[1][1] * 1e-3)
@@ -430,13 +556,28 @@ def standalone_closure(torch, c3d, stream, graphs=True):
                  f"({STANDALONE_PER_N} per order), tensor quadrature 2(N+3) x 4(N+3), "
                  "seeded multipliers, solved from the isotropic start (unbatched rules, MN_TOL "
                  "1e-8)",
-        fp64_solves_per_s=f64, mixed_solves_per_s=mix, mixed_over_fp64=mix / f64,
+        one_launch=group,
+        per_order_calls=dict(fp64_solves_per_s=f64, mixed_solves_per_s=mix,
+                             mixed_over_fp64=mix / f64, launches=7),
         alpha_rel_diff_median=float(np.median(dall)),
         alpha_rel_diff_p99=float(np.percentile(dall, 99)),
         per_order_columns=["N", "fp64 solves/s", "mixed solves/s", "mixed/fp64",
                            "iters fp64", "iters mixed", "failed fp64", "failed mixed",
-                           "alpha rel diff median"],
-        per_order=per_n)
+                           "alpha rel diff median", "iteration histogram fp64",
+                           "iteration histogram mixed"],
+        histogram_bins=f"iterations in [{HIST_EDGES[0]}, {HIST_EDGES[1]}), ... "
+                       f"[{HIST_EDGES[-1]}, inf)",
+        per_order=per_n,
+        reference_columns=["N", "sample vectors", "reference solves/s", "threads",
+                           "iteration counts equal to the GPU FP64 (fraction)",
+                           "alpha rel err vs reference, GPU FP64 [median, p99]",
+                           "alpha rel err vs reference, GPU mixed [median, p99]"],
+        reference=ref_rows,
+        reference_note="the reference's unbatched opt() (oracle/_ref, OpenMP over vectors, "
+                       "direct Hessian) on a prefix of each order's vectors sized for ~"
+                       f"{STANDALONE_REF_SAMPLE_S:g} s, one process per order; vectors the FP64 "
+                       "closure reports as exhausting the ladder are left out (the reference "
+                       "aborts on them)")
 
 
 # ------------------------------------------------------------------ B200 arm
@@ -622,36 +763,35 @@ def b200_arm(args):
             flops = closure_flops(nm, nq, sst.totalIters, sst.trials, args.hessian, sst.certified)
         per_launch_s = ms[0] * 1e-3 / max(1, closure_launches)
         achieved = flops / max(1, closure_launches) / per_launch_s / 1e12
-        roofline = dict(bound="tensor",
-                        pipe=("fp64 (DMMA m8n8k4 + DFMA); the mixed closure's BF16 / 3xTF32 "
-                              "moments run on tcgen05 beside it (lowp_tflops)" if precision == 1
-                              else "fp64 (DMMA m8n8k4 + DFMA)"),
-                        achieved=achieved,
-                        peak=peak, unit="TFLOP/s", frac=achieved / peak if peak else None,
-                        traffic=(profile_traffic("closure_rounds_m6_64")
-                                 if args.engine == "rounds" and args.hessian == "gaunt" else None),
-                        traffic_source="profiles/closure_rounds_m6_64.txt: one closure's DRAM "
-                                       "bytes at 64^3 (ncu) scaled by solved cells to 128^3",
-                        peak_source="in-run cuBLAS DGEMM 8192^3 via torch (FP64 is not in "
-                                    "MEASURED_PEAKS.json)",
-                        kernel=(("closure work-list rounds: rounds_pass_mixed_kernel<7,22,2> "
-                                 "(first-visit probe) + rounds_pass_gaunt_kernel<7,22> + "
-                                 "rounds_newton_kernel" if args.hessian == "gaunt" else
-                                 "closure work-list rounds: rounds_pass_direct_kernel<7> + "
-                                 "rounds_newton_kernel") if args.engine == "rounds" else
-                                ("closure_gaunt_kernel<7,22,8>" if args.hessian == "gaunt"
-                                 else "closure_fp64_kernel<7,8>")),
-                        unit_of_launch="one c3d_closure call (all its kernels)",
-                        flops_per_launch=flops / max(1, closure_launches),
-                        closure_ms_per_launch=ms[0] / max(1, closure_launches),
-                        flux_ms_per_launch=ms[1] / max(1, int(cnt[1])),
-                        closure_share_of_step=ms[0] / split["max_ms"])
+        closure_roofline = dict(
+            bound="tensor",
+            pipe=("fp64 (DMMA m8n8k4 + DFMA); the mixed closure's BF16 / 3xTF32 moments run on "
+                  "tcgen05 beside it (lowp_tflops)" if precision == 1
+                  else "fp64 (DMMA m8n8k4 + DFMA)"),
+            achieved=achieved, peak=peak, unit="TFLOP/s", frac=achieved / peak if peak else None,
+            traffic=(profile_traffic("closure_rounds_m6_64")
+                     if args.engine == "rounds" and args.hessian == "gaunt" else None),
+            traffic_source="profiles/closure_rounds_m6_64.txt: one closure's DRAM bytes at 64^3 "
+                           "(ncu) scaled by solved cells to 128^3",
+            peak_source="in-run cuBLAS DGEMM 8192^3 via torch (FP64 is not in "
+                        "MEASURED_PEAKS.json)",
+            kernel=(("closure work-list rounds: rounds_pass_mixed_kernel<7,22,2> (first-visit "
+                     "probe) + rounds_pass_gaunt_kernel<7,22> + rounds_newton_kernel"
+                     if args.hessian == "gaunt" else
+                     "closure work-list rounds: rounds_pass_direct_kernel<7> + "
+                     "rounds_newton_kernel") if args.engine == "rounds" else
+                    ("closure_gaunt_kernel<7,22,8>" if args.hessian == "gaunt"
+                     else "closure_fp64_kernel<7,8>")),
+            unit_of_launch="one c3d_closure call (all its kernels)",
+            flops_per_launch=flops / max(1, closure_launches),
+            ms_per_launch=ms[0] / max(1, closure_launches),
+            share_of_step=ms[0] / split["max_ms"])
         if low is not None:
-            roofline["lowp_tflops"] = low / max(1, closure_launches) / per_launch_s / 1e12
-            roofline["kernel"] = ("closure work-list rounds: rounds_pass_mixed_kernel<7,22,2> "
-                                  "(first-visit probe), <7,22,0|1> (tcgen05 Hessian moments), "
-                                  "rounds_pass_gaunt_kernel<7,22> (trials, FP64 Hessians) + "
-                                  "rounds_newton_kernel")
+            closure_roofline["lowp_tflops"] = low / max(1, closure_launches) / per_launch_s / 1e12
+            closure_roofline["kernel"] = (
+                "closure work-list rounds: rounds_pass_mixed_kernel<7,22,2> (first-visit probe), "
+                "<7,22,0|1> (tcgen05 Hessian moments), rounds_pass_gaunt_kernel<7,22> (trials, "
+                "FP64 Hessians) + rounds_newton_kernel")
         compare = None
         if other is not None:
             fp, mx = (other, head) if precision == 1 else (head, other)
@@ -680,21 +820,44 @@ def b200_arm(args):
                               f"{args.steps} timed steps from the same start state, mixed vs "
                               "the FP64 drop-in (all cells incl. ghosts); the FP64 drop-in "
                               "matches the C oracle to 1e-12 (tests)")
-        # the kinetic flux, second in the step: HBM view of the materialised-psi variant and
-        # its tensor-pipe work (exponents and projection)
-        nall_c = solver.nall
+        # the dominant kernel: the kinetic flux's stencil + projection (kinetic_staged_kernel),
+        # one launch per flux call when the closure handed its ansatz over (psi of all
+        # directions within the 32 GiB budget). Algorithmic work per (cell, direction):
+        # 2 nm FLOPs of projection + 60 of the three axes' limited upwind differences; bytes:
+        # psi of the interior cells and the two face-ghost layers read once, the flux written.
+        n_ = CONFIGS[cfg]["n"]
+        face_ghosts = 12 * n_ * n_  # two layers on each of the six faces
+        handoff = solver.nall * nq * 8 <= (32 << 30)
         flux_ms = ms[1] / max(1, int(cnt[1]))
-        flux_bytes = 8.0 * (nall_c * nm + cells * nm + nall_c * nq + cells * nq)
-        flux_flops = 2.0 * nm * nq * (nall_c + cells)
-        flux_line = dict(ms_per_call=flux_ms, variant="materialised psi (FP64)",
-                         hbm_bytes_per_call=flux_bytes,
-                         achieved_gbs=flux_bytes / (flux_ms * 1e-3) / 1e9,
-                         hbm_peak_gbs=HBM_PEAK_GBS,
-                         hbm_frac=flux_bytes / (flux_ms * 1e-3) / 1e9 / HBM_PEAK_GBS,
-                         contraction_tflops=flux_flops / (flux_ms * 1e-3) / 1e12,
-                         note="FP64-pipe and issue bound: exponents and projection on DMMA "
-                              "plus the limiter's FP64 arithmetic on shared-memory staged psi "
-                              "(profiles/kinetic_flux_m6_64.txt)")
+        stencil_flops = float((2 * nm + 60) * nq) * cells
+        stencil_bytes = 8.0 * ((cells + face_ghosts) * nq + cells * nm)
+        achieved_k = stencil_flops / (flux_ms * 1e-3) / 1e12
+        traffic_k = profile_traffic("kinetic_staged_m6_64")
+        if traffic_k is not None:
+            traffic_k *= cells / 64 ** 3  # ncu capture at 64^3, scaled by (cell, direction) pairs
+        roofline = dict(
+            bound="tensor", pipe="fp64 (DMMA m8n8k4 projection + DFMA/ALU limiter)",
+            kernel="kinetic_staged_kernel<7> (kinetic flux: MUSCL stencil + projection)",
+            achieved=achieved_k, peak=peak, unit="TFLOP/s",
+            frac=achieved_k / peak if peak else None,
+            traffic=traffic_k,
+            traffic_source="profiles/kinetic_staged_m6_64.txt: dram__bytes_read.sum + "
+                           "dram__bytes_write.sum of one launch at 64^3 (ncu), scaled by "
+                           "(cell, direction) pairs to this grid",
+            peak_source="in-run cuBLAS DGEMM 8192^3 via torch (FP64 is not in "
+                        "MEASURED_PEAKS.json)",
+            flops_per_launch=stencil_flops,
+            flops_per_cell_direction=2 * nm + 60,
+            ms_per_launch=flux_ms, stencil_only=handoff,
+            share_of_step=ms[1] / split["max_ms"],
+            hbm=dict(algorithmic_bytes_per_launch=stencil_bytes,
+                     achieved_gbs=stencil_bytes / (flux_ms * 1e-3) / 1e9,
+                     peak_gbs=HBM_PEAK_GBS,
+                     frac=stencil_bytes / (flux_ms * 1e-3) / 1e9 / HBM_PEAK_GBS,
+                     peak_source="MEASURED_PEAKS.json hbm_gbs (of measured)"),
+            note="FP64-pipe and issue bound (ncu: FP64 pipe, ALU and shared-memory wavefronts "
+                 "busy, DRAM idle most of the launch); the closure is second "
+                 "(closure_roofline)")
         # CPU baseline: the reference closure on a bounded sample of this workload's cells
         cpu = None
         try:
@@ -736,7 +899,8 @@ def b200_arm(args):
                         cells_per_step=2 * cells, l2="inputs larger than L2 (u, alpha 0.9 GB each)",
                         flux_autotune=tuned,
                         parallelism=f"replicas x{world}"),
-            roofline=roofline, flux=flux_line, cpu_baseline=cpu, precision_compare=compare,
+            roofline=roofline, closure_roofline=closure_roofline, cpu_baseline=cpu,
+            precision_compare=compare,
             standalone_closure=standalone,
             e2e=dict(value=e2e_value, unit=UNIT, h2d_bytes_per_step=2 * nv * 8,
                      d2h_bytes_per_step=2 * nv * 8, steps=e_steps),

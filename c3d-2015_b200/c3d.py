@@ -47,7 +47,8 @@ HEADER_SYMBOLS = [
     "c3d_closure_records_fp", "c3d_line_stats_enable", "c3d_line_stats_get", "c3d_stage",
     "c3d_set_x_halo_external", "c3d_copy_x_planes", "c3d_set_precision",
     "c3d_set_certificate", "c3d_autotune", "c3d_closure_vectors_noalloc_check",
-    "c3d_set_limits", "c3d_set_ansatz_handoff", "c3d_set_graphs",
+    "c3d_set_limits", "c3d_set_ansatz_handoff", "c3d_set_graphs", "c3d_group_create",
+    "c3d_group_closure_vectors", "c3d_group_destroy",
 ]
 
 
@@ -125,6 +126,10 @@ def lib():
         L.c3d_set_limits.argtypes = [vp, ctypes.c_longlong, ctypes.c_longlong, ctypes.c_longlong]
         L.c3d_set_ansatz_handoff.argtypes = [vp, ctypes.c_int]
         L.c3d_set_graphs.argtypes = [vp, ctypes.c_int]
+        L.c3d_group_create.argtypes = [ctypes.c_int, ctypes.POINTER(vp), ctypes.POINTER(vp)]
+        L.c3d_group_closure_vectors.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)] + \
+            [ctypes.POINTER(vp)] * 6
+        L.c3d_group_destroy.argtypes = [vp]
         L.c3d_timing_enable.argtypes = [vp, ctypes.c_int]
         L.c3d_timing_get.argtypes = [vp, _dp, ctypes.POINTER(ctypes.c_longlong)]
         L.c3d_launch_count.argtypes = [vp]
@@ -371,6 +376,33 @@ class Context:
                                st_ptr=None):
         check(lib().c3d_closure_vectors(self.h, n, u_ptr, a_ptr, it_ptr, ig_ptr, rg_ptr, st_ptr),
               "c3d_closure_vectors")
+
+
+class Group:
+    """Standalone closures of several contexts (context handles, e.g. one per moment order on
+    one stream) as one CUDA graph launch (c3d_group_closure_vectors)."""
+
+    def __init__(self, handles):
+        self.k = len(handles)
+        arr = (ctypes.c_void_p * self.k)(*handles)
+        h = ctypes.c_void_p()
+        check(lib().c3d_group_create(self.k, arr, ctypes.byref(h)), "c3d_group_create")
+        self.h = h
+
+    def closure_vectors(self, n, u, a, iters=None, iter_gamma=None, reg=None, status=None):
+        """n: vector counts; u, a, ...: device pointers (ints) per context (None: no record)."""
+        P = ctypes.c_void_p * self.k
+
+        def arr(v):
+            return None if v is None else P(*v)
+        check(lib().c3d_group_closure_vectors(self.h, (ctypes.c_longlong * self.k)(*n), arr(u),
+                                              arr(a), arr(iters), arr(iter_gamma), arr(reg),
+                                              arr(status)), "c3d_group_closure_vectors")
+
+    def close(self):
+        if self.h:
+            lib().c3d_group_destroy(self.h)
+            self.h = None
 
 
 class Solver:

@@ -1155,6 +1155,187 @@ c3d_status c3d_closure_vectors(c3d_ctx *c, long long n, double *u, double *alpha
     return run_closure(c, n, u, alpha, iters, iterGamma, regIndex, status);
 }
 
+// Several contexts' standalone closures as parallel branches of one CUDA graph. cs: three
+// capture streams per context (its closure, the round loop's body, the switch bodies) and an
+// origin stream that forks to and joins the contexts' branches; the graph launches on the
+// contexts' common stream.
+struct c3d_group {
+    std::vector<c3d_ctx *> ctx;
+    std::vector<cudaStream_t> cs;
+    cudaStream_t stream = nullptr;
+    std::vector<unsigned char> key;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<long long> launches; // per context: launches of one replay counted on the host
+};
+
+static void group_streams_free(c3d_group *g)
+{
+    for (cudaStream_t &s : g->cs) {
+        if (s)
+            cudaStreamDestroy(s);
+        s = nullptr;
+    }
+}
+
+static cudaError_t group_streams_make(c3d_group *g)
+{
+    for (cudaStream_t &s : g->cs)
+        if (!s) {
+            cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+            if (e != cudaSuccess)
+                return e;
+        }
+    return cudaSuccess;
+}
+
+c3d_status c3d_group_create(int count, c3d_ctx *const *ctx, c3d_group **out)
+{
+    if (!out || !ctx || count < 1)
+        return fail(C3D_ERR_INVALID, "c3d_group_create: bad argument");
+    *out = nullptr;
+    for (int k = 0; k < count; ++k) {
+        if (!ctx[k] || ctx[k]->solver != 1)
+            return fail(C3D_ERR_INVALID, "c3d_group_create: contexts must be M_N contexts");
+        if (ctx[k]->stream != ctx[0]->stream)
+            return fail(C3D_ERR_INVALID, "c3d_group_create: contexts must share one stream");
+        for (int j = 0; j < k; ++j)
+            if (ctx[j] == ctx[k])
+                return fail(C3D_ERR_INVALID, "c3d_group_create: a context appears twice");
+    }
+    c3d_group *g = new c3d_group();
+    g->ctx.assign(ctx, ctx + count);
+    g->stream = ctx[0]->stream;
+    g->cs.assign(3 * (size_t)count + 1, nullptr);
+    g->launches.assign(count, 0);
+    cudaError_t e = group_streams_make(g);
+    if (e != cudaSuccess) {
+        group_streams_free(g);
+        delete g;
+        return fail(C3D_ERR_CUDA, std::string("c3d_group_create: ") + cudaGetErrorString(e));
+    }
+    *out = g;
+    return C3D_OK;
+}
+
+void c3d_group_destroy(c3d_group *g)
+{
+    if (!g)
+        return;
+    cudaStreamSynchronize(g->stream); // a replay may still run
+    if (g->exec)
+        cudaGraphExecDestroy(g->exec);
+    group_streams_free(g);
+    delete g;
+}
+
+c3d_status c3d_group_closure_vectors(c3d_group *g, const long long *n, double *const *u,
+                                     double *const *alpha, int *const *iters,
+                                     int *const *iterGamma, int *const *regIndex,
+                                     int *const *status)
+{
+    if (!g || !n || !u || !alpha)
+        return fail(C3D_ERR_INVALID, "c3d_group_closure_vectors: bad argument");
+    const int K = (int)g->ctx.size();
+    auto rec = [](int *const *a, int k) -> int * { return a ? a[k] : nullptr; };
+    for (int k = 0; k < K; ++k) {
+        const c3d_ctx *c = g->ctx[k];
+        if (n[k] < 0 || (n[k] > 0 && (!u[k] || !alpha[k])))
+            return fail(C3D_ERR_INVALID, "c3d_group_closure_vectors: bad vectors");
+        if (c->engine != 0 || !c->graphs || c->timing)
+            return fail(C3D_ERR_INVALID, "c3d_group_closure_vectors: the contexts need the "
+                                         "work-list engine, graphs on and timing off");
+    }
+    // set-up of every closure (buffers are allocated here, never while capturing) and the
+    // graph's key
+    std::vector<RoundsLaunch> R(K);
+    std::vector<unsigned char> key;
+    for (int k = 0; k < K; ++k) {
+        c3d_ctx *c = g->ctx[k];
+        key.push_back((unsigned char)(n[k] > 0));
+        if (n[k] == 0)
+            continue;
+        c3d_status s = rounds_setup(c, n[k], u[k], alpha[k], rec(iters, k), rec(iterGamma, k),
+                                    rec(regIndex, k), rec(status, k), nullptr, false,
+                                    g->cs[3 * k], R[k]);
+        if (s != C3D_OK)
+            return s;
+        const std::vector<unsigned char> kk = rounds_graph_key(R[k], c->gaunt);
+        key.insert(key.end(), kk.begin(), kk.end());
+    }
+    if (!g->exec || key != g->key) {
+        std::lock_guard<std::mutex> lk(graph_build_mutex());
+        if (g->exec) {
+            C3D_CUDA(cudaStreamSynchronize(g->stream));
+            cudaGraphExecDestroy(g->exec);
+            g->exec = nullptr;
+        }
+        C3D_CUDA(group_streams_make(g));
+        cudaStream_t o = g->cs[3 * K];
+        std::vector<cudaEvent_t> ev(K + 1, nullptr);
+        cudaError_t e = cudaSuccess;
+        for (cudaEvent_t &x : ev)
+            if (e == cudaSuccess)
+                e = cudaEventCreateWithFlags(&x, cudaEventDisableTiming);
+        cudaGraph_t top = nullptr;
+        if (e == cudaSuccess)
+            e = cudaGraphCreate(&top, 0);
+        if (e == cudaSuccess) {
+            e = cudaStreamBeginCaptureToGraph(o, top, nullptr, nullptr, 0,
+                                              cudaStreamCaptureModeRelaxed);
+            cudaError_t ec = e == cudaSuccess ? cudaEventRecord(ev[K], o) : e;
+            for (int k = 0; k < K && ec == cudaSuccess; ++k) {
+                c3d_ctx *c = g->ctx[k];
+                g->launches[k] = 0;
+                if (n[k] == 0)
+                    continue;
+                cudaStream_t *cs = &g->cs[3 * k];
+                ec = cudaStreamWaitEvent(cs[0], ev[K], 0);
+                if (ec != cudaSuccess)
+                    break;
+                R[k].stream = cs[0];
+                R[k].captureTop = top;
+                R[k].captureStreams = cs;
+                const long long l0 = c->launches;
+                ec = launch_closure_rounds(R[k], c->gaunt);
+                g->launches[k] = c->launches - l0;
+                c->launches = l0;
+                if (ec == cudaSuccess)
+                    ec = cudaEventRecord(ev[k], cs[0]);
+                if (ec == cudaSuccess)
+                    ec = cudaStreamWaitEvent(o, ev[k], 0);
+            }
+            if (e == cudaSuccess) {
+                cudaGraph_t out = nullptr;
+                e = cudaStreamEndCapture(o, &out);
+                if (e == cudaSuccess)
+                    e = ec;
+            }
+        }
+        if (e == cudaSuccess)
+            e = cudaGraphInstantiate(&g->exec, top, 0);
+        if (top)
+            cudaGraphDestroy(top);
+        for (cudaEvent_t x : ev)
+            if (x)
+                cudaEventDestroy(x);
+        if (e != cudaSuccess) {
+            g->exec = nullptr;
+            g->key.clear();
+            group_streams_free(g); // streams left in a broken capture are replaced
+            cudaGetLastError();
+            return fail(C3D_ERR_CUDA, std::string("c3d_group_closure_vectors: group graph: ") +
+                                          cudaGetErrorString(e));
+        }
+        g->key = key;
+    }
+    C3D_CUDA(cudaGraphLaunch(g->exec, g->stream));
+    for (int k = 0; k < K; ++k) {
+        g->ctx[k]->launches += g->launches[k];
+        g->ctx[k]->psiReady = false;
+    }
+    return C3D_OK;
+}
+
 c3d_status c3d_flux_kinetic(c3d_ctx *c, int alphaIsU)
 {
     if (!c)

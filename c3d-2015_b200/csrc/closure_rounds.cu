@@ -1202,7 +1202,7 @@ template <class T> static void key_add(std::vector<unsigned char> &k, const T &v
     k.insert(k.end(), b, b + sizeof(T));
 }
 
-static std::vector<unsigned char> rounds_key(const RoundsLaunch &R, bool gaunt)
+std::vector<unsigned char> rounds_graph_key(const RoundsLaunch &R, bool gaunt)
 {
     std::vector<unsigned char> k;
     key_add(k, *R.P);
@@ -1467,7 +1467,7 @@ template <int NT, int NT2, bool GAUNT> static cudaError_t rounds_t(const RoundsL
     }
     if (R.graphs) {
         RoundsGraph *RG = reinterpret_cast<RoundsGraph *>(R.graphs);
-        std::vector<unsigned char> key = rounds_key(R, GAUNT);
+        std::vector<unsigned char> key = rounds_graph_key(R, GAUNT);
         RoundsGraph::Slot *G = nullptr;
         for (RoundsGraph::Slot &s : RG->slot)
             if (s.exec && s.key == key)

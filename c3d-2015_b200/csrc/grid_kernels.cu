@@ -127,15 +127,21 @@ __global__ void ghost_mirror_check_kernel(GridDims g, const double *__restrict__
 // psi[q nall + ghost] = psi[q nall + image] for every face ghost and direction: the closure
 // copied the face ghosts' multipliers from their periodic images, so their ansatz values are
 // the images' too (the probe pass wrote the solved cells' values).
+// A thread per face ghost (its image found once) walks the directions; consecutive threads
+// hold consecutive ghosts, so per direction a warp's copies are contiguous runs (x and y faces)
+// or pairs (z faces).
 __global__ void psi_face_copy_kernel(GridDims g, int nq, double *__restrict__ psi)
 {
-    const long long nf = ghost_faces(g), nall = g.nall(), total = nf * nq;
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
-         e += (long long)gridDim.x * blockDim.x) {
-        const long long f = e % nf, q = e / nf;
+    const long long nf = ghost_faces(g), nall = g.nall();
+    for (long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x; f < nf;
+         f += (long long)gridDim.x * blockDim.x) {
         long long dst, src;
         ghost_pair(g, f, dst, src);
-        psi[q * nall + dst] = psi[q * nall + src];
+        const double *s = psi + src;
+        double *d = psi + dst;
+#pragma unroll 4
+        for (int q = 0; q < nq; ++q)
+            d[(long long)q * nall] = s[(long long)q * nall];
     }
 }
 
@@ -513,15 +519,19 @@ __device__ __forceinline__ double axis_flux_m3(double om, double w, double th, d
 // reads (offsets -2, -1, +1 for a positive cosine, -1, +1, +2 otherwise; L values each), and
 // the sub-stage's two projection k-steps and its directions' cosines and weights; warp d
 // copies direction d (warp 0 also the projection data), each warp arriving on the stage's
-// mbarrier with its bytes. Each thread forms the limited differences of two (cell,
-// direction) pairs from shared memory (branch-free: the staged slots put the stencil values
-// of either sign of the cosine at fixed places, and the limiter is the three-operand minmod),
-// then the CTA projects the sub-stage's S tile onto the moments with DMMAs (k-steps 2v,
-// 2v + 1 of the 32-direction fragment tile, in order), so the flux has the same values as
-// kinetic_dmma_kernel's.
+// mbarrier with its bytes. Each thread forms the limited differences of the two (cell,
+// direction) pairs whose values it holds in the DMMA A fragments of the sub-stage's two
+// k-steps (cell 8 warp + lane / 4, direction 4 k + lane % 4), from shared memory and
+// branch-free (the staged slots put the stencil values of either sign of the cosine at fixed
+// places; the limiter is the three-operand minmod), then projects them onto the moments with
+// DMMAs straight from its registers (k-steps 2v, 2v + 1 of the 32-direction fragment tile, in
+// order), so the flux has the same values as kinetic_dmma_kernel's. One barrier per sub-stage,
+// before its buffers are refilled.
 constexpr int KDS = 8;                      // directions per sub-stage
 constexpr int KRUN = 64;                    // longest cell run per CTA
-constexpr int KPER = (KRUN + 4) + 6 * KRUN; // doubles staged per direction
+// doubles staged per direction: the runs, padded so that the four directions a warp reads
+// at once (one DMMA k-step) fall on two disjoint halves of the shared-memory banks
+constexpr int KPER = (KRUN + 4) + 6 * KRUN + 4;
 template <int NT> struct KinStage {
     static constexpr int FRAG = 2 * NT * 32;                    // two projection k-steps
     static constexpr int DOUBLES = KDS * KPER + FRAG + 4 * KDS; // + xi, eta, mu, w of KDS dirs
@@ -535,11 +545,9 @@ __global__ void __launch_bounds__(256, 3)
 {
     constexpr int TILE = 8 * NT * 32 + 128; // one 32-direction tile of mfP
     constexpr int SD = KinStage<NT>::DOUBLES, FRAG = KinStage<NT>::FRAG;
-    constexpr int CS = 68;
     static_assert((SD * 8) % 16 == 0 && (KPER * 8) % 16 == 0, "stage alignment");
     static_assert(KDS * 32 == 256, "one warp per direction of a sub-stage");
     extern __shared__ __align__(128) double kinSmem[];
-    double *sS = kinSmem + 2 * SD; // KDS x CS
     __shared__ uint64_t pbar[2];
     __shared__ long long sRun[9];
     const int nm = g.nm;
@@ -650,9 +658,12 @@ __global__ void __launch_bounds__(256, 3)
         // sub-stage are then not used)
         const bool ok = fbar_wait(&pbar[u & 1], (u >> 1) & 1);
         const double *dirs = st + KDS * KPER + FRAG; // xi[KDS], eta[KDS], mu[KDS], w[KDS]
+        double afr[2]; // the thread's own A fragments of the sub-stage's two k-steps
 #pragma unroll
         for (int r = 0; r < 2; ++r) {
-            const int pr = tid + 256 * r, cl = pr & 63, d = pr >> 6;
+            // cell 8 warp + lane / 4, direction 4 r + lane % 4: the element of the DMMA A
+            // fragment (k-step r) the thread holds
+            const int cl = cw, d = 4 * r + (lane & 3);
             const int ql = KDS * u + d;
             double sv = 0.0;
             if (cl < L && ql < nqc) {
@@ -675,22 +686,21 @@ __global__ void __launch_bounds__(256, 3)
                                                zb[3]);
                 sv = fx * rdx + fy * rdy + fz * rdz;
             }
-            sS[d * CS + cl] = sv;
+            afr[r] = sv;
         }
+        // projection straight from the registers; one barrier per sub-stage (before its stage
+        // is refilled), where a timed-out wait is agreed on
+        const double *B = st + KDS * KPER;
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+#pragma unroll
+            for (int jj = 0; jj < NT; ++jj)
+                dmma_g(acc[jj][0], acc[jj][1], afr[h], B[(h * NT + jj) * 32 + lane]);
         if (__syncthreads_or(!ok)) {
             if (tid == 0)
                 atomicExch(errorFlag, 1);
             return;
         }
-        const double *B = st + KDS * KPER;
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const double a = sS[(4 * h + (lane & 3)) * CS + 8 * warp + (lane >> 2)];
-#pragma unroll
-            for (int jj = 0; jj < NT; ++jj)
-                dmma_g(acc[jj][0], acc[jj][1], a, B[(h * NT + jj) * 32 + lane]);
-        }
-        __syncthreads();
         if (u + 2 < nu)
             issue(u + 2);
     }
@@ -835,7 +845,7 @@ cudaError_t launch_psi_handoff(const GridDims &g, int nq, const double *M, const
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess || !faceCopy)
         return e;
-    psi_face_copy_kernel<<<grid_for(ghost_faces(g) * nq, 256, numSMs), 256, 0, st>>>(g, nq, psi);
+    psi_face_copy_kernel<<<grid_for(ghost_faces(g), 256, numSMs), 256, 0, st>>>(g, nq, psi);
     return cudaGetLastError();
 }
 
@@ -1038,7 +1048,7 @@ static cudaError_t kinetic_t(const GridDims &g, const double *alpha, const doubl
         // run length chosen by the autotuner, 0 for min(64, nz))
         const int L = runLen > 0 ? runLen : (g.nz < KRUN ? g.nz : KRUN);
         if (L % 2 == 0 && L <= KRUN && g.nz % L == 0) {
-            const size_t smem = (size_t)(2 * KinStage<NT>::DOUBLES + KDS * 68) * 8;
+            const size_t smem = (size_t)(2 * KinStage<NT>::DOUBLES) * 8;
             auto kern = kinetic_staged_kernel<NT>;
             cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                  (int)smem);

@@ -5,6 +5,7 @@
 
 #include <cstddef>
 #include <mutex>
+#include <vector>
 
 namespace c3d {
 
@@ -72,5 +73,7 @@ cudaError_t capture_conditional(cudaStream_t st, cudaGraphConditionalHandle h,
                                 cudaGraphConditionalNodeType type, unsigned int size,
                                 cudaGraph_t **bodies);
 void rounds_graph_free(void *g);
+// What a captured closure depends on (options, sizes, buffers): equal keys, same graph.
+std::vector<unsigned char> rounds_graph_key(const RoundsLaunch &R, bool gaunt);
 
 } // namespace c3d

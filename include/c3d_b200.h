@@ -299,6 +299,26 @@ c3d_status c3d_set_ghost_mirroring(c3d_ctx *ctx, int on);
 c3d_status c3d_closure_vectors(c3d_ctx *ctx, long long n, double *u, double *alpha, int *iters,
                                int *iterGamma, int *regIndex, int *status);
 
+/* Closure group: the standalone closures of several contexts (e.g. one per moment order, each
+ * with its own tables and options) as ONE launch -- a CUDA graph whose parallel branches are
+ * the contexts' closures, each with its work-list rounds in a device-side loop, so that the
+ * orders' rounds share the GPU and no closure waits for the host. The contexts must be M_N
+ * contexts on one stream (the one they were created with; the group launches there), with the
+ * work-list engine and graphs on (the defaults) and timing off; a context appears once. The
+ * graph is rebuilt when a context's options, a size or a buffer changes. Per context k:
+ * n[k] vectors at u[k], alpha[k] (device, solved in place), records iters/iterGamma/regIndex/
+ * status[k] as in c3d_closure_vectors (each array of pointers, or an entry of one, may be
+ * NULL). Results are those of calling c3d_closure_vectors per context, bit for bit. Errors
+ * (failed cells, round limit) are reported per context by c3d_sync. No counterpart in the
+ * reference, whose closure works one batch of one order at a time. */
+typedef struct c3d_group c3d_group;
+c3d_status c3d_group_create(int count, c3d_ctx *const *ctx, c3d_group **out);
+c3d_status c3d_group_closure_vectors(c3d_group *group, const long long *n, double *const *u,
+                                     double *const *alpha, int *const *iters,
+                                     int *const *iterGamma, int *const *regIndex,
+                                     int *const *status);
+void c3d_group_destroy(c3d_group *group);
+
 /* Tables of src/init.cpp:509-548 (host arrays), so callers without GSL can
  * build M, w, xi, eta, mu identical to the host's. M2 may be NULL. */
 void c3d_build_quadrature(int momentOrder, int quadOrder, double *w, double *xi, double *eta,

@@ -1,0 +1,162 @@
+"""Closure groups (c3d_group_closure_vectors): the standalone closures of the seven moment
+orders N = 1..7, one context each on one stream, as one CUDA graph launch give bit for bit the
+results of the per-context closures (multipliers, moments, iteration counts, ladder indices,
+statuses), in FP64 and in the mixed closure; a changed vector count rebuilds the graph; the
+group's argument checks.
+
+Workload: the standalone closure vectors (alpha_k ~ N(0, s^2), s log-uniform in [0.1, 5],
+unit density, u = <m e^{alpha.m}>, solved from the isotropic multipliers) with the unbatched
+rules of opt() (src/opt/opt.cpp:139-355), Gaunt sparse Hessians, MN_TOL 1e-8."""
+import ctypes
+
+import numpy as np
+import pytest
+
+import c3d
+
+pytestmark = pytest.mark.gpu
+
+LADDER = "0,1e-3,1e-2,1e-1,5e-1"
+
+
+def _vectors(N, n):
+    q = c3d.quadrature(N, 2 * (N + 3))
+    nm, nq = q["nm"], q["nq"]
+    M = q["M"].reshape(nq, nm)
+    rng = np.random.default_rng([2015, N])
+    s = np.exp(rng.uniform(np.log(0.1), np.log(5.0), n))
+    a = rng.standard_normal((n, nm)) * s[:, None]
+    a[:, 0] = 0.0
+    u = (np.exp(a @ M.T) * q["w"]) @ M
+    a[:, 0] = -2.0 * np.sqrt(np.pi) * np.log(u[:, 0])
+    u = (np.exp(a @ M.T) * q["w"]) @ M
+    a_iso = np.zeros_like(a)
+    a_iso[:, 0] = 2.0 * np.sqrt(np.pi) * np.log(u[:, 0] / (2.0 * np.sqrt(np.pi)))
+    return u, a_iso
+
+
+def _solver(tmp_path, N, stream):
+    kv = dict(SOLVER="mn", TFINAL="1", OUTDT="1000", OUTPUT_DATA="false",
+              OUTPUT_OPT_STATS="false", OUTPUT_TIMINGS="false", NX=2, NY=2, NZ=2, MPIX=1, MPIY=1,
+              MPIZ=1, AX=-1, AY=-1, AZ=-1, BX=1, BY=1, BZ=1, MOMENT_ORDER=N,
+              QUAD_ORDER=2 * (N + 3), CFL_FACTOR=0.5, CROSS_SECTION=1.0, INIT_FLOOR=1e-4,
+              GAUSS_SIGMA=0.1, INIT_COND="gaussian_psi", THETA=2.0, OMP_THREADS=1,
+              PN_USE_KINETIC_FLUX=0, MN_TOL=1e-8, MN_TOL_GAMMA=1.1, MN_COND_H_MAX=1e10,
+              MN_MAX_ITER=100, MN_BATCHED="false", MN_USE_GAUNT_COEF="true",
+              MN_USE_GAUNT_SPARSE="true", REG_LADDER=LADDER)
+    p = tmp_path / f"n{N}.deck"
+    p.write_text("".join(f"{k} {v}\n" for k, v in kv.items()))
+    return c3d.Solver(str(p), stream=ctypes.c_void_p(stream.cuda_stream))
+
+
+def _bufs(torch, u, a):
+    n = len(u)
+    return dict(u=torch.tensor(u, device="cuda"), a=torch.tensor(a, device="cuda"),
+                it=torch.zeros(n, dtype=torch.int32, device="cuda"),
+                rg=torch.zeros(n, dtype=torch.int32, device="cuda"),
+                st=torch.zeros(n, dtype=torch.int32, device="cuda"))
+
+
+def _closure(s, n, b, reg=True):
+    c3d.check(c3d.lib().c3d_closure_vectors(s.ctx_handle, n, b["u"].data_ptr(), b["a"].data_ptr(),
+                                            b["it"].data_ptr(), None,
+                                            b["rg"].data_ptr() if reg else None,
+                                            b["st"].data_ptr()), "closure")
+
+
+def _host(b):
+    return {k: v.cpu().numpy() for k, v in b.items()}
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_group_matches_per_context_closures(tmp_path, mode):
+    import torch
+    L = c3d.lib()
+    stream = torch.cuda.Stream()
+    orders = list(range(1, 8))
+    solvers = [_solver(tmp_path, N, stream) for N in orders]
+    for s in solvers:
+        c3d.check(L.c3d_set_precision(s.ctx_handle, mode, 0.0, 0.0, 0, 0.0), "precision")
+    counts = [1500, 900, 1200, 700, 800, 600, 500]
+    data = [_vectors(N, n) for N, n in zip(orders, counts)]
+    with torch.cuda.stream(stream):
+        ref = []
+        for s, (u, a) in zip(solvers, data):
+            b = _bufs(torch, u, a)
+            _closure(s, len(u), b)
+            ref.append(b)
+        stream.synchronize()
+        ref = [_host(b) for b in ref]
+        group = c3d.Group([s.ctx_handle for s in solvers])
+        for rep in range(2):  # the second call replays the instantiated graph
+            bs = [_bufs(torch, u, a) for u, a in data]
+            group.closure_vectors(counts, [b["u"].data_ptr() for b in bs],
+                                  [b["a"].data_ptr() for b in bs],
+                                  iters=[b["it"].data_ptr() for b in bs],
+                                  reg=[b["rg"].data_ptr() for b in bs],
+                                  status=[b["st"].data_ptr() for b in bs])
+            stream.synchronize()
+            for N, b, r in zip(orders, bs, ref):
+                h = _host(b)
+                for k in ("u", "a", "it", "rg", "st"):
+                    assert np.array_equal(h[k], r[k]), (mode, rep, N, k)
+            for s in solvers:
+                s.sync()
+        group.close()
+    assert (ref[6]["it"] > 3).sum() > 100  # Newton-heavy: many rounds per order
+    for s in solvers:
+        s.close()
+
+
+def test_group_rebuilds_on_new_counts_and_skips_empty(tmp_path):
+    import torch
+    L = c3d.lib()
+    stream = torch.cuda.Stream()
+    solvers = [_solver(tmp_path, N, stream) for N in (3, 6)]
+    group = c3d.Group([s.ctx_handle for s in solvers])
+    with torch.cuda.stream(stream):
+        for counts in ([400, 300], [0, 500], [350, 0]):
+            data = [_vectors(N, max(n, 1)) for N, n in zip((3, 6), counts)]
+            bs = [_bufs(torch, u[:n], a[:n]) if n else None for (u, a), n in zip(data, counts)]
+            refs = []
+            for s, (u, a), n in zip(solvers, data, counts):
+                if not n:
+                    refs.append(None)
+                    continue
+                b = _bufs(torch, u[:n], a[:n])
+                _closure(s, n, b, reg=False)
+                refs.append(b)
+            group.closure_vectors(counts, [b["u"].data_ptr() if b else None for b in bs],
+                                  [b["a"].data_ptr() if b else None for b in bs],
+                                  iters=[b["it"].data_ptr() if b else None for b in bs],
+                                  status=[b["st"].data_ptr() if b else None for b in bs])
+            stream.synchronize()
+            for b, r in zip(bs, refs):
+                if b is None:
+                    continue
+                assert np.array_equal(b["a"].cpu().numpy(), r["a"].cpu().numpy())
+                assert np.array_equal(b["it"].cpu().numpy(), r["it"].cpu().numpy())
+    group.close()
+    assert L.c3d_launch_count(solvers[1].ctx_handle) > 0
+    for s in solvers:
+        s.close()
+
+
+def test_group_argument_checks(tmp_path):
+    import torch
+    s1, s2 = torch.cuda.Stream(), torch.cuda.Stream()
+    a = _solver(tmp_path, 2, s1)
+    b = _solver(tmp_path, 3, s2)
+    with pytest.raises(c3d.C3DError, match="one stream"):
+        c3d.Group([a.ctx_handle, b.ctx_handle])
+    with pytest.raises(c3d.C3DError, match="twice"):
+        c3d.Group([a.ctx_handle, a.ctx_handle])
+    g = c3d.Group([a.ctx_handle])
+    c3d.check(c3d.lib().c3d_set_graphs(a.ctx_handle, 0), "graphs")
+    u, al = _vectors(2, 10)
+    bb = _bufs(torch, u, al)
+    with pytest.raises(c3d.C3DError, match="graphs on"):
+        g.closure_vectors([10], [bb["u"].data_ptr()], [bb["a"].data_ptr()])
+    g.close()
+    a.close()
+    b.close()
