@@ -48,7 +48,7 @@ HEADER_SYMBOLS = [
     "c3d_set_x_halo_external", "c3d_copy_x_planes", "c3d_set_precision",
     "c3d_set_certificate", "c3d_autotune", "c3d_closure_vectors_noalloc_check",
     "c3d_set_limits", "c3d_set_ansatz_handoff", "c3d_set_graphs", "c3d_group_create",
-    "c3d_group_closure_vectors", "c3d_group_destroy",
+    "c3d_group_closure_vectors", "c3d_group_step", "c3d_group_destroy",
 ]
 
 
@@ -129,6 +129,7 @@ def lib():
         L.c3d_group_create.argtypes = [ctypes.c_int, ctypes.POINTER(vp), ctypes.POINTER(vp)]
         L.c3d_group_closure_vectors.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)] + \
             [ctypes.POINTER(vp)] * 6
+        L.c3d_group_step.argtypes = [vp, _dp]
         L.c3d_group_destroy.argtypes = [vp]
         L.c3d_timing_enable.argtypes = [vp, ctypes.c_int]
         L.c3d_timing_get.argtypes = [vp, _dp, ctypes.POINTER(ctypes.c_longlong)]
@@ -398,6 +399,11 @@ class Group:
         check(lib().c3d_group_closure_vectors(self.h, (ctypes.c_longlong * self.k)(*n), arr(u),
                                               arr(a), arr(iters), arr(iter_gamma), arr(reg),
                                               arr(status)), "c3d_group_closure_vectors")
+
+    def step(self, dt):
+        """One RK step of every context (dt: one value per context) in one graph launch."""
+        d = np.ascontiguousarray(dt, dtype=np.float64)
+        check(lib().c3d_group_step(self.h, d.ctypes.data_as(_dp)), "c3d_group_step")
 
     def close(self):
         if self.h:

@@ -1166,6 +1166,10 @@ struct c3d_group {
     std::vector<unsigned char> key;
     cudaGraphExec_t exec = nullptr;
     std::vector<long long> launches; // per context: launches of one replay counted on the host
+    // c3d_group_step's graph: every context's RK step as one branch
+    std::vector<unsigned char> stepKey;
+    cudaGraphExec_t stepExec = nullptr;
+    std::vector<long long> stepLaunches;
 };
 
 static void group_streams_free(c3d_group *g)
@@ -1207,6 +1211,7 @@ c3d_status c3d_group_create(int count, c3d_ctx *const *ctx, c3d_group **out)
     g->stream = ctx[0]->stream;
     g->cs.assign(3 * (size_t)count + 1, nullptr);
     g->launches.assign(count, 0);
+    g->stepLaunches.assign(count, 0);
     cudaError_t e = group_streams_make(g);
     if (e != cudaSuccess) {
         group_streams_free(g);
@@ -1224,6 +1229,8 @@ void c3d_group_destroy(c3d_group *g)
     cudaStreamSynchronize(g->stream); // a replay may still run
     if (g->exec)
         cudaGraphExecDestroy(g->exec);
+    if (g->stepExec)
+        cudaGraphExecDestroy(g->stepExec);
     group_streams_free(g);
     delete g;
 }
@@ -1470,21 +1477,20 @@ __global__ void mirror_if_kernel(const int *flag, cudaGraphConditionalHandle h)
         cudaGraphSetConditional(h, *flag == 0 ? 1u : 0u);
 }
 
-// One M_N RK stage of update() as a CUDA graph: [RK save,] ghost fill, the closure (with
-// face-ghost mirroring: the mirror check picks, through an IF node, the mirrored closure with
-// its ghost copies or the closure of every cell), the ansatz hand-off, the kinetic flux and
-// the Euler stage[, RK average]. Nothing in it waits for the host. *used is false when the
-// context's options need the stage run launch by launch (timing events, the x-line log,
-// re-projection, the persistent engine, P_N).
-static c3d_status stage_graph(c3d_ctx *c, int stage, double dt, bool *used)
+// Whether a context's RK stages can run as CUDA graphs: the work-list engine with graphs on,
+// and none of the options that need the stage launch by launch (timing events, the x-line
+// log, re-projection) or the P_N solver.
+static bool stage_graphs_usable(const c3d_ctx *c)
 {
-    *used = false;
-    if (!c->graphs || c->engine != 0 || c->timing || c->lineCap != 0 || c->reproject ||
-        c->solver != 1)
-        return C3D_OK;
-    const bool mirrorPath = c->mirror && !c->xHaloExternal;
-    // buffers first (nothing is allocated while capturing)
-    if (mirrorPath) {
+    return c->graphs && c->engine == 0 && !c->timing && c->lineCap == 0 && !c->reproject &&
+           c->solver == 1;
+}
+
+// Buffers of a stage capture, allocated before it (nothing is allocated while capturing);
+// *handoff: whether the closure hands its ansatz to the flux.
+static c3d_status stage_prepare(c3d_ctx *c, bool *handoff)
+{
+    if (c->mirror && !c->xHaloExternal) {
         c3d_status sm = ensure_cellmap(c);
         if (sm != C3D_OK)
             return sm;
@@ -1497,10 +1503,9 @@ static c3d_status stage_graph(c3d_ctx *c, int stage, double dt, bool *used)
     if (!c->launchDev) {
         C3D_CUDA(cudaMalloc(&c->launchDev, sizeof(unsigned long long)));
         C3D_CUDA(cudaMemset(c->launchDev, 0, sizeof(unsigned long long)));
-        Rall.launchDev = c->launchDev;
     }
-    const bool handoff = Rall.psi != nullptr;
-    if (!handoff) {
+    *handoff = Rall.psi != nullptr;
+    if (!*handoff) {
         const size_t need = (size_t)c->qChunk * c->g.nall() * 8;
         if (!c->psi || c->psiAlloc < need) {
             if (c->psi)
@@ -1511,26 +1516,149 @@ static c3d_status stage_graph(c3d_ctx *c, int stage, double dt, bool *used)
             c->psiAlloc = need;
         }
     }
+    for (cudaStream_t &x : c->sc)
+        if (!x)
+            C3D_CUDA(cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking));
+    return C3D_OK;
+}
+
+// What a captured stage depends on: equal keys, same graph.
+static std::vector<unsigned char> stage_key(const c3d_ctx *c, int stage, double dt, bool handoff)
+{
     std::vector<unsigned char> key;
-    auto skey = [](std::vector<unsigned char> &k, const auto &v) {
+    auto skey = [&key](const auto &v) {
         const unsigned char *b = reinterpret_cast<const unsigned char *>(&v);
-        k.insert(k.end(), b, b + sizeof(v));
+        key.insert(key.end(), b, b + sizeof(v));
     };
-    skey(key, stage);
-    skey(key, dt);
-    skey(key, c->cp);
-    skey(key, mirrorPath);
-    skey(key, c->gaunt);
-    skey(key, handoff);
-    skey(key, c->qChunk);
-    skey(key, c->runLen);
-    skey(key, c->maxRounds);
-    skey(key, c->rBatchUse);
+    const bool mirrorPath = c->mirror && !c->xHaloExternal;
+    skey(stage);
+    skey(dt);
+    skey(c->cp);
+    skey(mirrorPath);
+    skey(c->gaunt);
+    skey(handoff);
+    skey(c->qChunk);
+    skey(c->runLen);
+    skey(c->maxRounds);
+    skey(c->rBatchUse);
     const void *ptrs[] = {c->psi, c->rState, c->rBuf, c->rListA, c->rCounts, c->cellMap,
                           c->gChunksC, c->chunks, c->gStream, c->mixF64, c->mixA[0],
-                          c->mixA[1], c->g0, c->psiRefresh, c->launchDev};
+                          c->mixA[1], c->g0, c->psiRefresh, c->launchDev, c->u, c->alpha};
     for (const void *p : ptrs)
-        skey(key, p);
+        skey(p);
+    return key;
+}
+
+// Appends one M_N RK stage of update() to the graph being captured on cs[0] (its top-level
+// graph: top): [RK save,] ghost fill, the closure (with face-ghost mirroring: the mirror check
+// picks, through an IF node, the mirrored closure with its ghost copies or the closure of
+// every cell), the ansatz hand-off, the kinetic flux and the Euler stage[, RK average].
+// Nothing in it waits for the host. cs[1] captures the IF bodies, cs[1..3] (mirrored) or
+// cs[0..2] the closure's round loop and switch bodies. *launches: the kernels of one replay
+// the host counts (the closure's device-side loop counts its own).
+static cudaError_t stage_capture(c3d_ctx *c, int stage, double dt, bool handoff, cudaGraph_t top,
+                                 cudaStream_t *cs, long long *launches)
+{
+    const bool mirrorPath = c->mirror && !c->xHaloExternal;
+    const long long l0 = c->launches;
+    long long n = 0;
+    cudaStream_t s0 = cs[0];
+    cudaError_t ec = cudaSuccess;
+    if (stage == 0)
+        ec = launch_rk(c->g, c->u, c->uOld, 0, c->numSMs, s0);
+    if (ec == cudaSuccess)
+        ec = launch_ghost_fill(c->g, c->u, c->numSMs, s0, c->xHaloExternal);
+    n += (stage == 0) + 1;
+    // the closure on stream cs[k] (its bodies on the next two) and what follows it
+    auto closure = [&](bool mirrored, int k) -> cudaError_t {
+        RoundsLaunch R;
+        c3d_status rs = mirrored
+                            ? rounds_setup(c, c->cellMapCount, c->u, c->alpha, c->iters,
+                                           c->iterGamma, c->regIdx, c->status, c->cellMap, true,
+                                           cs[k], R)
+                            : rounds_setup(c, c->g.nall(), c->u, c->alpha, c->iters,
+                                           c->iterGamma, c->regIdx, c->status, nullptr, true,
+                                           cs[k], R);
+        if (rs != C3D_OK)
+            return cudaErrorInvalidValue;
+        R.captureTop = top;
+        R.captureStreams = &cs[k];
+        cudaError_t er = launch_closure_rounds(R, c->gaunt);
+        cudaStream_t sk = cs[k];
+        if (er == cudaSuccess && mirrored) {
+            er = launch_ghost_fill(c->g, c->alpha, c->numSMs, sk);
+            if (er == cudaSuccess)
+                er = launch_ghost_fill(c->g, c->u, c->numSMs, sk);
+            for (int *a : {c->iters, c->iterGamma, c->regIdx, c->status})
+                if (er == cudaSuccess)
+                    er = launch_ghost_fill_int(c->g, a, c->numSMs, sk);
+            for (double *a : {c->cellGamma, c->cellErr})
+                if (er == cudaSuccess)
+                    er = launch_ghost_fill_1(c->g, a, c->numSMs, sk);
+            if (er == cudaSuccess)
+                er = launch_ghost_stats(c->g, c->iters, c->iterGamma, c->regIdx, c->status,
+                                        c->stats, c->numSMs, sk);
+        }
+        if (er == cudaSuccess && R.psi)
+            er = launch_psi_handoff(c->g, c->nq, c->M, c->alpha, mirrored, c->psiRefresh,
+                                    c->psiRefreshCount, c->psi, c->numSMs, sk);
+        return er;
+    };
+    if (ec == cudaSuccess && mirrorPath) {
+        ec = cudaMemsetAsync(c->mirrorFlag, 0, sizeof(int), s0);
+        if (ec == cudaSuccess)
+            ec = launch_ghost_mirror_check(c->g, c->alpha, c->mirrorFlag, c->numSMs, s0);
+        cudaGraphConditionalHandle hIf;
+        if (ec == cudaSuccess)
+            ec = cudaGraphConditionalHandleCreate(&hIf, top, 0, cudaGraphCondAssignDefault);
+        if (ec == cudaSuccess) {
+            mirror_if_kernel<<<1, 32, 0, s0>>>(c->mirrorFlag, hIf);
+            ec = cudaGetLastError();
+        }
+        cudaGraph_t *bodies = nullptr;
+        if (ec == cudaSuccess)
+            ec = capture_conditional(s0, hIf, cudaGraphCondTypeIf, 2, &bodies);
+        for (int b = 0; b < 2 && ec == cudaSuccess; ++b) {
+            ec = cudaStreamBeginCaptureToGraph(cs[1], bodies[b], nullptr, nullptr, 0,
+                                               cudaStreamCaptureModeRelaxed);
+            if (ec == cudaSuccess) {
+                cudaError_t eb = closure(b == 0, 1);
+                cudaGraph_t out = nullptr;
+                ec = cudaStreamEndCapture(cs[1], &out);
+                if (ec == cudaSuccess)
+                    ec = eb;
+            }
+        }
+        n += 3 + 9;
+    } else if (ec == cudaSuccess) {
+        ec = closure(false, 0);
+    }
+    if (ec == cudaSuccess)
+        ec = launch_kinetic_flux(c->g, c->alpha, c->mfA, c->mfP, c->xi, c->eta, c->nq, c->qChunk,
+                                 c->runLen, c->dx, c->dy, c->dz, c->theta, 0, c->psi, handoff,
+                                 c->flux, c->errorFlag, s0);
+    if (ec == cudaSuccess)
+        ec = launch_euler(c->g, c->u, c->flux, c->sigT, c->sigS, dt, c->numSMs, s0);
+    if (ec == cudaSuccess && stage == 1)
+        ec = launch_rk(c->g, c->u, c->uOld, 1, c->numSMs, s0);
+    n += (handoff ? 1 + 2 : 2 * ceil_div(c->nq, c->qChunk)) + 1 + (stage == 1);
+    *launches = n + (c->launches - l0); // the closure counted its round 0
+    c->launches = l0;
+    return ec;
+}
+
+// One M_N RK stage as a CUDA graph of its own, cached per configuration (stage_capture).
+// *used is false when the context's options need the stage run launch by launch.
+static c3d_status stage_graph(c3d_ctx *c, int stage, double dt, bool *used)
+{
+    *used = false;
+    if (!stage_graphs_usable(c))
+        return C3D_OK;
+    bool handoff = false;
+    c3d_status s = stage_prepare(c, &handoff);
+    if (s != C3D_OK)
+        return s;
+    const std::vector<unsigned char> key = stage_key(c, stage, dt, handoff);
     c3d_ctx::StageGraph *Gp = nullptr;
     for (auto &g : c->sg)
         if (g.exec && g.key == key)
@@ -1550,106 +1678,22 @@ static c3d_status stage_graph(c3d_ctx *c, int stage, double dt, bool *used)
             cudaGraphExecDestroy(G.exec);
             G.exec = nullptr;
         }
-        for (cudaStream_t &x : c->sc)
-            if (!x)
-                C3D_CUDA(cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking));
         cudaGraph_t top = nullptr;
         C3D_CUDA(cudaGraphCreate(&top, 0));
         long long launches = 0;
-        const long long l0 = c->launches;
         cudaError_t e = cudaStreamBeginCaptureToGraph(c->sc[0], top, nullptr, nullptr, 0,
                                                       cudaStreamCaptureModeRelaxed);
-        cudaError_t ec = cudaSuccess;
         if (e == cudaSuccess) {
-            cudaStream_t s0 = c->sc[0];
-            if (stage == 0)
-                ec = launch_rk(c->g, c->u, c->uOld, 0, c->numSMs, s0);
-            if (ec == cudaSuccess)
-                ec = launch_ghost_fill(c->g, c->u, c->numSMs, s0, c->xHaloExternal);
-            launches += (stage == 0) + 1;
-            // the closure on stream sc[k] (its bodies on the next two) and what follows it
-            auto closure = [&](bool mirrored, int k) -> cudaError_t {
-                RoundsLaunch R;
-                c3d_status rs = mirrored
-                                    ? rounds_setup(c, c->cellMapCount, c->u, c->alpha, c->iters,
-                                                   c->iterGamma, c->regIdx, c->status, c->cellMap,
-                                                   true, c->sc[k], R)
-                                    : rounds_setup(c, c->g.nall(), c->u, c->alpha, c->iters,
-                                                   c->iterGamma, c->regIdx, c->status, nullptr,
-                                                   true, c->sc[k], R);
-                if (rs != C3D_OK)
-                    return cudaErrorInvalidValue;
-                R.captureTop = top;
-                R.captureStreams = &c->sc[k];
-                cudaError_t er = launch_closure_rounds(R, c->gaunt);
-                cudaStream_t sk = c->sc[k];
-                if (er == cudaSuccess && mirrored) {
-                    er = launch_ghost_fill(c->g, c->alpha, c->numSMs, sk);
-                    if (er == cudaSuccess)
-                        er = launch_ghost_fill(c->g, c->u, c->numSMs, sk);
-                    for (int *a : {c->iters, c->iterGamma, c->regIdx, c->status})
-                        if (er == cudaSuccess)
-                            er = launch_ghost_fill_int(c->g, a, c->numSMs, sk);
-                    for (double *a : {c->cellGamma, c->cellErr})
-                        if (er == cudaSuccess)
-                            er = launch_ghost_fill_1(c->g, a, c->numSMs, sk);
-                    if (er == cudaSuccess)
-                        er = launch_ghost_stats(c->g, c->iters, c->iterGamma, c->regIdx, c->status,
-                                                c->stats, c->numSMs, sk);
-                }
-                if (er == cudaSuccess && R.psi)
-                    er = launch_psi_handoff(c->g, c->nq, c->M, c->alpha, mirrored, c->psiRefresh,
-                                            c->psiRefreshCount, c->psi, c->numSMs, sk);
-                return er;
-            };
-            if (ec == cudaSuccess && mirrorPath) {
-                ec = cudaMemsetAsync(c->mirrorFlag, 0, sizeof(int), s0);
-                if (ec == cudaSuccess)
-                    ec = launch_ghost_mirror_check(c->g, c->alpha, c->mirrorFlag, c->numSMs, s0);
-                cudaGraphConditionalHandle hIf;
-                if (ec == cudaSuccess)
-                    ec = cudaGraphConditionalHandleCreate(&hIf, top, 0, cudaGraphCondAssignDefault);
-                if (ec == cudaSuccess) {
-                    mirror_if_kernel<<<1, 32, 0, s0>>>(c->mirrorFlag, hIf);
-                    ec = cudaGetLastError();
-                }
-                cudaGraph_t *bodies = nullptr;
-                if (ec == cudaSuccess)
-                    ec = capture_conditional(s0, hIf, cudaGraphCondTypeIf, 2, &bodies);
-                for (int b = 0; b < 2 && ec == cudaSuccess; ++b) {
-                    ec = cudaStreamBeginCaptureToGraph(c->sc[1], bodies[b], nullptr, nullptr, 0,
-                                                       cudaStreamCaptureModeRelaxed);
-                    if (ec == cudaSuccess) {
-                        cudaError_t eb = closure(b == 0, 1);
-                        cudaGraph_t out = nullptr;
-                        ec = cudaStreamEndCapture(c->sc[1], &out);
-                        if (ec == cudaSuccess)
-                            ec = eb;
-                    }
-                }
-                launches += 3 + 9;
-            } else if (ec == cudaSuccess) {
-                ec = closure(false, 0);
-            }
-            if (ec == cudaSuccess)
-                ec = launch_kinetic_flux(c->g, c->alpha, c->mfA, c->mfP, c->xi, c->eta, c->nq,
-                                         c->qChunk, c->runLen, c->dx, c->dy, c->dz, c->theta, 0,
-                                         c->psi, handoff, c->flux, c->errorFlag, s0);
-            if (ec == cudaSuccess)
-                ec = launch_euler(c->g, c->u, c->flux, c->sigT, c->sigS, dt, c->numSMs, s0);
-            if (ec == cudaSuccess && stage == 1)
-                ec = launch_rk(c->g, c->u, c->uOld, 1, c->numSMs, s0);
-            launches += (handoff ? 1 + 2 : 2 * ceil_div(c->nq, c->qChunk)) + 1 + (stage == 1);
+            const cudaError_t ec = stage_capture(c, stage, dt, handoff, top, c->sc, &launches);
             cudaGraph_t out = nullptr;
-            e = cudaStreamEndCapture(s0, &out);
+            e = cudaStreamEndCapture(c->sc[0], &out);
             if (e == cudaSuccess)
                 e = ec;
         }
         if (e == cudaSuccess)
             e = cudaGraphInstantiate(&G.exec, top, 0);
         cudaGraphDestroy(top);
-        G.launches = launches + (c->launches - l0); // the closure counted its round 0
-        c->launches = l0;
+        G.launches = launches;
         if (e != cudaSuccess) {
             G.exec = nullptr;
             for (cudaStream_t &x : c->sc) {
@@ -1668,6 +1712,105 @@ static c3d_status stage_graph(c3d_ctx *c, int stage, double dt, bool *used)
     c->launches += G.launches;
     c->psiReady = false;
     *used = true;
+    return C3D_OK;
+}
+
+c3d_status c3d_group_step(c3d_group *g, const double *dt)
+{
+    if (!g || !dt)
+        return fail(C3D_ERR_INVALID, "c3d_group_step: bad argument");
+    const int K = (int)g->ctx.size();
+    for (int k = 0; k < K; ++k) {
+        if (!stage_graphs_usable(g->ctx[k]))
+            return fail(C3D_ERR_INVALID, "c3d_group_step: the contexts need the work-list "
+                                         "engine, graphs on, timing, line log and re-projection "
+                                         "off");
+        if (!(dt[k] > 0.0))
+            return fail(C3D_ERR_INVALID, "c3d_group_step: dt must be positive");
+    }
+    std::vector<unsigned char> key;
+    std::vector<char> handoff(K, 0);
+    for (int k = 0; k < K; ++k) {
+        bool h = false;
+        c3d_status s = stage_prepare(g->ctx[k], &h);
+        if (s != C3D_OK)
+            return s;
+        handoff[k] = h;
+        for (int stage = 0; stage < 2; ++stage) {
+            const std::vector<unsigned char> kk = stage_key(g->ctx[k], stage, dt[k], h);
+            key.insert(key.end(), kk.begin(), kk.end());
+        }
+    }
+    if (!g->stepExec || key != g->stepKey) {
+        std::lock_guard<std::mutex> lk(graph_build_mutex());
+        if (g->stepExec) {
+            C3D_CUDA(cudaStreamSynchronize(g->stream));
+            cudaGraphExecDestroy(g->stepExec);
+            g->stepExec = nullptr;
+        }
+        C3D_CUDA(group_streams_make(g));
+        cudaStream_t o = g->cs[3 * K];
+        std::vector<cudaEvent_t> ev(K + 1, nullptr);
+        cudaError_t e = cudaSuccess;
+        for (cudaEvent_t &x : ev)
+            if (e == cudaSuccess)
+                e = cudaEventCreateWithFlags(&x, cudaEventDisableTiming);
+        cudaGraph_t top = nullptr;
+        if (e == cudaSuccess)
+            e = cudaGraphCreate(&top, 0);
+        if (e == cudaSuccess) {
+            e = cudaStreamBeginCaptureToGraph(o, top, nullptr, nullptr, 0,
+                                              cudaStreamCaptureModeRelaxed);
+            cudaError_t ec = e == cudaSuccess ? cudaEventRecord(ev[K], o) : e;
+            for (int k = 0; k < K && ec == cudaSuccess; ++k) {
+                c3d_ctx *c = g->ctx[k];
+                g->stepLaunches[k] = 0;
+                ec = cudaStreamWaitEvent(c->sc[0], ev[K], 0);
+                for (int stage = 0; stage < 2 && ec == cudaSuccess; ++stage) {
+                    long long n = 0;
+                    ec = stage_capture(c, stage, dt[k], handoff[k] != 0, top, c->sc, &n);
+                    g->stepLaunches[k] += n;
+                }
+                if (ec == cudaSuccess)
+                    ec = cudaEventRecord(ev[k], c->sc[0]);
+                if (ec == cudaSuccess)
+                    ec = cudaStreamWaitEvent(o, ev[k], 0);
+            }
+            if (e == cudaSuccess) {
+                cudaGraph_t out = nullptr;
+                e = cudaStreamEndCapture(o, &out);
+                if (e == cudaSuccess)
+                    e = ec;
+            }
+        }
+        if (e == cudaSuccess)
+            e = cudaGraphInstantiate(&g->stepExec, top, 0);
+        if (top)
+            cudaGraphDestroy(top);
+        for (cudaEvent_t x : ev)
+            if (x)
+                cudaEventDestroy(x);
+        if (e != cudaSuccess) {
+            g->stepExec = nullptr;
+            g->stepKey.clear();
+            group_streams_free(g);
+            for (c3d_ctx *c : g->ctx)
+                for (cudaStream_t &x : c->sc) {
+                    if (x)
+                        cudaStreamDestroy(x);
+                    x = nullptr;
+                }
+            cudaGetLastError();
+            return fail(C3D_ERR_CUDA, std::string("c3d_group_step: group graph: ") +
+                                          cudaGetErrorString(e));
+        }
+        g->stepKey = key;
+    }
+    C3D_CUDA(cudaGraphLaunch(g->stepExec, g->stream));
+    for (int k = 0; k < K; ++k) {
+        g->ctx[k]->launches += g->stepLaunches[k];
+        g->ctx[k]->psiReady = false;
+    }
     return C3D_OK;
 }
 

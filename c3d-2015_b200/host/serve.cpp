@@ -1,6 +1,6 @@
 // Serving loop (include/c3d_serve.h): admission of independent problems against a
-// device-memory budget, a pool of host threads each driving one problem's context to
-// completion, per-request completion latency.
+// device-memory budget, one scheduling thread that steps every admitted problem in one CUDA
+// graph launch per pass, per-request completion latency.
 #include "../../include/c3d_serve.h"
 #include "deck.h"
 #include "solver.h"
@@ -73,45 +73,84 @@ struct Request {
     std::vector<double> u; // final interior moments
 };
 
+// An admitted problem: its solver (context on the server's stream), the dt of each step of its
+// time loop and the steps taken so far.
+struct Active {
+    Request *r = nullptr;
+    std::unique_ptr<c3d_host::Solver> s;
+    std::vector<double> plan;
+    size_t next = 0;
+};
+
 } // namespace
 
 struct c3d_server {
     int device = 0;
+    int slots = 1;        // problems active at once at most
     long long budget = 0; // 0: unlimited
     long long inUse = 0, peakBytes = 0;
-    int active = 0, peakActive = 0;
+    int peakActive = 0;
     long long nextId = 1;
     bool stopping = false;
+    cudaStream_t stream = nullptr; // every problem's context
     std::mutex m;
     std::condition_variable cv;
     std::deque<Request *> pending;
     std::map<long long, std::unique_ptr<Request>> all;
-    std::vector<std::thread> workers;
+    std::thread scheduler;
 
-    void work();
-    void run(Request &r);
+    void schedule();
+    void admit(std::vector<std::unique_ptr<Active>> &active);
+    void finish(Active &a, c3d_status st);
 };
 
-// One problem on its own context: init (tables, initial state, device upload), the time
-// loop, the final state back to the host.
-void c3d_server::run(Request &r)
+// Admission: requests in arrival order while a slot is free and the budget holds their
+// estimated footprint; each gets its solver (tables, initial state, device context on the
+// server's stream) and its step plan.
+void c3d_server::admit(std::vector<std::unique_ptr<Active>> &active)
 {
-    cudaSetDevice(device);
-    c3d_host::Solver s;
-    int steps = 0;
-    c3d_status st = s.init(r.cfg, nullptr);
-    // launch by launch: capturing CUDA graphs on worker threads while other workers create,
-    // free and synchronise their contexts crashed the process in testing (cause not found),
-    // so the serving loop's problems do not use the stage and closure graphs
-    if (st == C3D_OK && s.ctx())
-        st = c3d_set_graphs(s.ctx(), 0);
-    if (st == C3D_OK)
-        st = s.run(&steps);
-    if (st == C3D_OK || st == C3D_ERR_CLOSURE) {
-        c3d_status p = s.pull();
+    for (;;) {
+        Request *r = nullptr;
+        {
+            std::lock_guard<std::mutex> lk(m);
+            if (pending.empty() || (int)active.size() >= slots)
+                return;
+            const long long need = pending.front()->bytes;
+            if (!(budget == 0 || inUse == 0 || inUse + need <= budget))
+                return;
+            r = pending.front();
+            pending.pop_front();
+            inUse += r->bytes;
+            peakBytes = inUse > peakBytes ? inUse : peakBytes;
+            const int na = (int)active.size() + 1;
+            peakActive = na > peakActive ? na : peakActive;
+        }
+        std::unique_ptr<Active> a(new Active());
+        a->r = r;
+        a->s.reset(new c3d_host::Solver());
+        c3d_status st = a->s->init(r->cfg, stream);
+        if (st == C3D_OK)
+            st = a->s->plan(a->plan);
+        if (st != C3D_OK || a->plan.empty()) {
+            finish(*a, st);
+            continue;
+        }
+        active.push_back(std::move(a));
+    }
+}
+
+// A problem's end: its status (the closure's failures included), final interior moments,
+// completion time; its device memory is released and its budget share returned.
+void c3d_server::finish(Active &a, c3d_status st)
+{
+    Request &r = *a.r;
+    if (st == C3D_OK && a.s->ctx())
+        st = c3d_sync(a.s->ctx());
+    if ((st == C3D_OK || st == C3D_ERR_CLOSURE) && a.s->ctx()) {
+        c3d_status p = a.s->pull();
         if (p == C3D_OK) {
             const c3d_host::Config &c = r.cfg;
-            const int nm = s.nm();
+            const int nm = a.s->nm();
             const long long nyg = c.ny + 4, nzg = c.nz + 4;
             r.u.resize((size_t)c.nx * c.ny * c.nz * nm);
             size_t o = 0;
@@ -120,47 +159,87 @@ void c3d_server::run(Request &r)
                     for (int k = 2; k < c.nz + 2; ++k) {
                         const long long cell = k + nzg * (j + nyg * (long long)i);
                         for (int mm = 0; mm < nm; ++mm)
-                            r.u[o++] = s.u[(size_t)cell * nm + mm];
+                            r.u[o++] = a.s->u[(size_t)cell * nm + mm];
                     }
         } else {
             st = p;
         }
     }
-    r.status = st;
-    r.steps = steps;
+    a.s.reset(); // frees the context
+    {
+        std::lock_guard<std::mutex> lk(m);
+        r.status = st;
+        r.steps = (int)a.next;
+        r.done = Clock::now();
+        r.finished = true;
+        inUse -= r.bytes;
+    }
+    cv.notify_all();
 }
 
-void c3d_server::work()
+// The scheduling loop (one host thread): every pass admits what fits, then advances every
+// active problem by one step -- the M_N problems all in ONE launch, a CUDA graph whose branches
+// are their RK steps (c3d_group_step; rebuilt when the set of problems or a dt changes), the
+// others (P_N, or options that need launch-by-launch stages) by c3d_step on the same stream --
+// and, while the GPU runs the pass, admits the next requests. Problems that took their last
+// step, or failed, are finished after the pass.
+void c3d_server::schedule()
 {
+    cudaSetDevice(device);
+    std::vector<std::unique_ptr<Active>> active;
+    c3d_group *group = nullptr;
+    std::vector<c3d_ctx *> members;
     for (;;) {
-        Request *r = nullptr;
-        {
+        admit(active);
+        if (active.empty()) {
             std::unique_lock<std::mutex> lk(m);
-            cv.wait(lk, [&] {
-                if (pending.empty())
-                    return stopping;
-                const long long need = pending.front()->bytes;
-                return budget == 0 || inUse == 0 || inUse + need <= budget;
-            });
-            if (pending.empty())
-                return;
-            r = pending.front();
-            pending.pop_front();
-            inUse += r->bytes;
-            ++active;
-            peakBytes = inUse > peakBytes ? inUse : peakBytes;
-            peakActive = active > peakActive ? active : peakActive;
+            cv.wait(lk, [&] { return stopping || !pending.empty(); });
+            if (stopping && pending.empty())
+                break;
+            continue;
         }
-        run(*r);
-        {
-            std::lock_guard<std::mutex> lk(m);
-            r->done = Clock::now();
-            r->finished = true;
-            inUse -= r->bytes;
-            --active;
+        std::vector<c3d_ctx *> grouped;
+        std::vector<double> dts;
+        for (auto &a : active)
+            if (a->s->graphable()) {
+                grouped.push_back(a->s->ctx());
+                dts.push_back(a->plan[a->next]);
+            }
+        c3d_status gs = C3D_OK;
+        if (grouped != members) {
+            if (group)
+                c3d_group_destroy(group);
+            group = nullptr;
+            members = grouped;
+            if (!members.empty())
+                gs = c3d_group_create((int)members.size(), members.data(), &group);
         }
-        cv.notify_all();
+        if (gs == C3D_OK && group)
+            gs = c3d_group_step(group, dts.data());
+        std::vector<c3d_status> st(active.size(), C3D_OK);
+        for (size_t k = 0; k < active.size(); ++k) {
+            Active &a = *active[k];
+            st[k] = a.s->graphable() ? gs : a.s->update(a.plan[a.next]);
+        }
+        admit(active); // overlaps the pass on the GPU; new problems join the next pass
+        cudaStreamSynchronize(stream);
+        // the problems of this pass are active[0 .. st.size()), in order; admitted ones follow
+        for (size_t k = 0, j = 0; k < active.size(); ++j) {
+            Active &a = *active[k];
+            const bool stepped = j < st.size();
+            const c3d_status sk = stepped ? st[j] : C3D_OK;
+            if (stepped && sk == C3D_OK)
+                ++a.next;
+            if (sk != C3D_OK || a.next >= a.plan.size()) {
+                finish(a, sk);
+                active.erase(active.begin() + (long)k);
+                continue;
+            }
+            ++k;
+        }
     }
+    if (group)
+        c3d_group_destroy(group);
 }
 
 extern "C" {
@@ -172,9 +251,11 @@ c3d_status c3d_server_create(int workers, size_t hbmBudgetBytes, c3d_server **ou
     std::unique_ptr<c3d_server> s(new c3d_server());
     if (cudaGetDevice(&s->device) != cudaSuccess)
         return C3D_ERR_NO_DEVICE;
+    if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return C3D_ERR_CUDA;
     s->budget = (long long)hbmBudgetBytes;
-    for (int w = 0; w < workers; ++w)
-        s->workers.emplace_back([p = s.get()] { p->work(); });
+    s->slots = workers;
+    s->scheduler = std::thread([p = s.get()] { p->schedule(); });
     *out = s.release();
     return C3D_OK;
 }
@@ -263,8 +344,8 @@ void c3d_server_destroy(c3d_server *s)
         s->stopping = true;
     }
     s->cv.notify_all();
-    for (auto &t : s->workers)
-        t.join();
+    s->scheduler.join();
+    cudaStreamDestroy(s->stream);
     delete s;
 }
 

@@ -431,43 +431,70 @@ c3d_status Solver::restore(const std::string &path, double *time)
     return ctx_ ? push() : C3D_OK;
 }
 
+// The time loop of src/main.cpp:57-76 (or NSTEPS steps of dt_max): step(dt) for each update,
+// out(t) at each output time; stops at the first status that is not C3D_OK. A positive OUTDT
+// is required with TFINAL (the reference's loop never ends otherwise).
+c3d_status Solver::walk(const std::function<c3d_status(double)> &step,
+                        const std::function<c3d_status(double)> &out) const
+{
+    c3d_status s;
+    if (cfg_.nsteps >= 0) {
+        for (int n = 0; n < cfg_.nsteps; ++n)
+            if ((s = step(maxDt_)) != C3D_OK)
+                return s;
+        return out(cfg_.nsteps * maxDt_);
+    }
+    if (!(cfg_.outDt > 0.0))
+        return C3D_ERR_INVALID;
+    double t = 0.0, dt;
+    const double tFinal = cfg_.tFinal;
+    for (double tOut = std::min(t + cfg_.outDt, tFinal); tOut <= tFinal;
+         tOut = std::min(tOut + cfg_.outDt, tFinal)) {
+        dt = maxDt_;
+        while (t < tOut - 1e-14 * tOut) {
+            t += dt;
+            if (t > tOut) {
+                dt = tOut - (t - dt);
+                t = tOut;
+            }
+            if ((s = step(dt)) != C3D_OK)
+                return s;
+        }
+        if ((s = out(t)) != C3D_OK)
+            return s;
+        if (tOut > tFinal - 1e-14 * tFinal)
+            break;
+    }
+    return C3D_OK;
+}
+
+c3d_status Solver::plan(std::vector<double> &dts) const
+{
+    dts.clear();
+    return walk(
+        [&](double dt) {
+            dts.push_back(dt);
+            return C3D_OK;
+        },
+        [](double) { return C3D_OK; });
+}
+
 c3d_status Solver::run(int *stepsTaken)
 {
     int steps = 0;
     c3d_status s = C3D_OK;
     if (cfg_.outputData && (s = outputData(0.0, "output")) != C3D_OK)
         return s;
-    if (cfg_.nsteps >= 0) {
-        for (int n = 0; n < cfg_.nsteps; ++n) {
-            if ((s = update(maxDt_)) != C3D_OK)
-                return s;
-            ++steps;
-        }
-        if (cfg_.outputData && (s = outputData(cfg_.nsteps * maxDt_, "output")) != C3D_OK)
-            return s;
-    } else {
-        // src/main.cpp:57-76
-        double t = 0.0, dt;
-        const double tFinal = cfg_.tFinal;
-        for (double tOut = std::min(t + cfg_.outDt, tFinal); tOut <= tFinal;
-             tOut = std::min(tOut + cfg_.outDt, tFinal)) {
-            dt = maxDt_;
-            while (t < tOut - 1e-14 * tOut) {
-                t += dt;
-                if (t > tOut) {
-                    dt = tOut - (t - dt);
-                    t = tOut;
-                }
-                if ((s = update(dt)) != C3D_OK)
-                    return s;
+    s = walk(
+        [&](double dt) {
+            c3d_status e = update(dt);
+            if (e == C3D_OK)
                 ++steps;
-            }
-            if (cfg_.outputData && (s = outputData(t, "output")) != C3D_OK)
-                return s;
-            if (tOut > tFinal - 1e-14 * tFinal)
-                break;
-        }
-    }
+            return e;
+        },
+        [&](double t) { return cfg_.outputData ? outputData(t, "output") : C3D_OK; });
+    if (s != C3D_OK)
+        return s;
     if (stepsTaken)
         *stepsTaken = steps;
     if ((s = c3d_sync(ctx_)) != C3D_OK)

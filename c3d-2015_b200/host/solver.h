@@ -25,6 +25,7 @@
 #include "../../include/c3d_b200.h"
 #include "deck.h"
 
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -73,6 +74,8 @@ public:
     c3d_status update(double dt);
     // The time loop of src/main.cpp:57-76 (or NSTEPS steps); returns the steps taken.
     c3d_status run(int *stepsTaken);
+    // The dt of each update run() makes, in order (C3D_ERR_INVALID for TFINAL with OUTDT <= 0).
+    c3d_status plan(std::vector<double> &dts) const;
     // Copies device state to the host arrays (u, alpha).
     c3d_status pull();
     // Copies the host arrays to the device (u, alpha, sigma_t, sigma_s).
@@ -92,6 +95,13 @@ public:
     const Config &config() const { return cfg_; }
     c3d_ctx *ctx() { return ctx_; }
     int nm() const { return nm_; }
+    // Whether its steps can run as CUDA graphs (c3d_group_step): M_N without re-projection,
+    // per-update timers or x-line statistics.
+    bool graphable() const
+    {
+        return cfg_.solver == "mn" && !cfg_.mnReproject && !cfg_.outputTimings &&
+               !cfg_.outputOptStats;
+    }
     int nq() const { return nq_; }
     long long ncellsAll() const { return (long long)(cfg_.nx + 4) * (cfg_.ny + 4) * (cfg_.nz + 4); }
     double dx() const { return dx_; }
@@ -106,6 +116,8 @@ public:
     std::vector<int> betaRow, betaCol;
 
 private:
+    c3d_status walk(const std::function<c3d_status(double)> &step,
+                    const std::function<c3d_status(double)> &out) const;
     Config cfg_;
     c3d_ctx *ctx_ = nullptr;
     c3d_params params_{};

@@ -1,12 +1,15 @@
 /*
  * Serving loop of libc3d_b200.so (no counterpart in the reference, which runs one problem per
  * process): independent transport problems, each given as input.deck text, are admitted
- * against a device-memory budget, run concurrently (one device context and stream per problem,
- * stepped by a pool of host threads, so their kernels overlap on the GPU) and keep their state
- * on the device from submission to completion. A request that arrives while others run waits
- * in arrival order until the active problems' estimated footprints leave room for its own, so
- * problems are admitted as earlier ones finish. Each problem's result is what c3d_solver_run
- * gives for it alone, bit for bit: contexts share nothing but the GPU.
+ * against a device-memory budget and keep their state on the device from submission to
+ * completion. One scheduling thread advances every admitted problem by one time step per pass,
+ * the M_N problems together in ONE launch: a CUDA graph whose parallel branches are their RK
+ * steps (c3d_group_step), rebuilt when the set of problems changes. While the GPU runs a pass
+ * the thread admits the requests that arrived (in arrival order, while the active problems'
+ * estimated footprints leave room), which join the next pass; problems that took their last
+ * step leave after it. Each problem's result is what c3d_solver_run gives for it alone, bit for
+ * bit: problems share launches but no data. Output keys of the decks are ignored (results come
+ * back through c3d_server_wait).
  */
 #ifndef C3D_SERVE_H
 #define C3D_SERVE_H
@@ -19,8 +22,9 @@ extern "C" {
 
 typedef struct c3d_server c3d_server;
 
-/* workers: problems run at once at most; hbmBudgetBytes: device memory the admitted problems'
- * estimated footprints may add up to (0: no limit). Uses the current CUDA device. */
+/* workers: problems active at once at most (slots of the shared pass); hbmBudgetBytes: device
+ * memory the admitted problems' estimated footprints may add up to (0: no limit). Uses the
+ * current CUDA device. */
 c3d_status c3d_server_create(int workers, size_t hbmBudgetBytes, c3d_server **out);
 
 /* Queues a problem (input.deck text, the reference's keys; NSTEPS or TFINAL bound its run);
