@@ -537,7 +537,10 @@ def standalone_closure(torch, c3d, stream, graphs=True):
                     e1.record(stream)
                     torch.cuda.synchronize()
                 for s in solvers:
-                    s.sync()
+                    # failed vectors (status 2: ladder exhausted) are counted, not raised
+                    st_ = L.c3d_sync(s.ctx_handle)
+                    if st_ not in (c3d.C3D_OK, 4):
+                        c3d.check(st_, "group closure")
                 ms = e0.elapsed_time(e1)
                 key = "fp64" if mode == 0 else "mixed"
                 group[key + "_solves_per_s"] = group["vectors"] / (ms * 1e-3)
@@ -578,6 +581,90 @@ def standalone_closure(torch, c3d, stream, graphs=True):
                        f"{STANDALONE_REF_SAMPLE_S:g} s, one process per order; vectors the FP64 "
                        "closure reports as exhausting the ladder are left out (the reference "
                        "aborts on them)")
+
+
+# ------------------------------------------------------------------ serving workload
+SERVE_STREAM = 256        # problems of the seeded stream
+SERVE_PROBLEMS = 16       # of which the bench runs the first ... per arm (bounded run time)
+SERVE_GAP_S = 0.05        # mean of the exponential inter-arrival gaps
+SERVE_BUDGET = 150 << 30  # device-memory budget of the admitted problems
+SERVE_SLOTS = 64          # problems active at once at most
+
+
+def serving_stream(n_problems, mixed):
+    """The serving workload's seeded problem stream: cubic grid with edge uniform in 16..96,
+    N in {1, 3, 5}, sigma_s uniform in [0.5, 20], a Gaussian pulse of width uniform in
+    [0.02, 0.2] over a 1e-8 floor, final time uniform in [0.1, 0.5]; Poisson arrivals with a
+    mean gap of 50 ms. Quadrature 2(N+3) mu x 4(N+3) phi, Gaunt sparse Hessian, MN_TOL 1e-6,
+    batched rules, the benchmark ladder. Returns [(arrival_s, deck_text, edge, N)]."""
+    rng = np.random.default_rng(2015_5)
+    out, t = [], 0.0
+    for k in range(SERVE_STREAM):
+        n = int(rng.integers(16, 97))
+        N = int(rng.choice([1, 3, 5]))
+        sig_s = float(rng.uniform(0.5, 20.0))
+        width = float(rng.uniform(0.02, 0.2))
+        tf = float(rng.uniform(0.1, 0.5))
+        t += float(rng.exponential(SERVE_GAP_S))
+        if k >= n_problems:
+            continue
+        kv = dict(SOLVER="mn", TFINAL=repr(tf), OUTDT=repr(tf), OUTPUT_DATA="false",
+                  OUTPUT_OPT_STATS="false", OUTPUT_TIMINGS="false", NX=n, NY=n, NZ=n,
+                  MPIX=1, MPIY=1, MPIZ=1, AX=-1, AY=-1, AZ=-1, BX=1, BY=1, BZ=1,
+                  MOMENT_ORDER=N, QUAD_ORDER=2 * (N + 3), CFL_FACTOR=0.5, CROSS_SECTION=sig_s,
+                  INIT_FLOOR=1e-8, GAUSS_SIGMA=width, INIT_COND="gaussian_psi", THETA=2.0,
+                  OMP_THREADS=1, PN_USE_KINETIC_FLUX=0, MN_TOL=MN_TOL, MN_TOL_GAMMA=1.1,
+                  MN_COND_H_MAX=1e10, MN_MAX_ITER=100, MN_BATCHED="true",
+                  MN_USE_GAUNT_COEF="true", MN_USE_GAUNT_SPARSE="true", CUDA_KINETIC="true",
+                  CUDA_BATCHED="true", CUDA_BATCH_SIZE=50, REG_LADDER=LADDER,
+                  MN_MIXED_PRECISION="true" if mixed else "false")
+        out.append((t, "".join(f"{k_} {v}\n" for k_, v in kv.items()), n, N))
+    return out
+
+
+def serving_workload(c3d, n_problems):
+    """The serving workload on the B200 serving loop (include/c3d_serve.h), mixed and FP64 arms
+    on the same seeded stream: requests submitted at their arrival times by a host thread,
+    completion latency per request (submission to result) and aggregate cell-solves/s (interior
+    cells x 2 stages x steps of every problem, over the time from the first submission to the
+    last completion)."""
+    res = {}
+    for mixed in (True, False):
+        stream = serving_stream(n_problems, mixed)
+        srv = c3d.Server(workers=SERVE_SLOTS, hbm_budget=SERVE_BUDGET)
+        ids = [None] * len(stream)
+        t0 = time.perf_counter()
+
+        def feed():
+            for k, (ta, deck, _, _) in enumerate(stream):
+                d = ta - (time.perf_counter() - t0)
+                if d > 0:
+                    time.sleep(d)
+                ids[k] = srv.submit(deck)
+        th = threading.Thread(target=feed)
+        th.start()
+        th.join()
+        lat, solves, failed = [], 0, 0
+        for (ta, deck, n, N), rid in zip(stream, ids):
+            st, u, latency, steps = srv.wait(rid)
+            lat.append(latency)
+            solves += n ** 3 * 2 * steps
+            failed += int(st != 0)
+        wall = time.perf_counter() - t0
+        peak_bytes, peak_active = srv.stats()
+        srv.close()
+        res["mixed" if mixed else "fp64"] = dict(
+            cell_solves_per_s=solves / wall, wall_s=wall, cell_solves=solves,
+            latency_p50_s=float(np.percentile(lat, 50)),
+            latency_p99_s=float(np.percentile(lat, 99)), failed_problems=failed,
+            peak_active=peak_active, peak_budget_gb=peak_bytes / 1e9)
+    res["mixed_over_fp64"] = res["mixed"]["cell_solves_per_s"] / res["fp64"]["cell_solves_per_s"]
+    res["workload"] = (f"first {n_problems} of the {SERVE_STREAM}-problem seeded stream: edge "
+                       "uniform 16..96, N in {1,3,5}, sigma_s U[0.5,20], pulse width U[0.02,0.2] "
+                       "floor 1e-8, final time U[0.1,0.5], Poisson arrivals (mean gap 50 ms), "
+                       f"{SERVE_BUDGET >> 30} GiB budget, up to {SERVE_SLOTS} problems per pass "
+                       "(one CUDA graph launch steps them all)")
+    return res
 
 
 # ------------------------------------------------------------------ B200 arm
@@ -641,11 +728,13 @@ def b200_arm(args):
                                   ctypes.c_void_p(a_.data_ptr()), None, None, 0), "set_state")
 
     # flux autotuner (direction chunk, z run per CTA), on the initial state
-    tq, tr, tms = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
-    c3d.check(L.c3d_autotune(ctxh, ctypes.byref(tq), ctypes.byref(tr), ctypes.byref(tms)),
-              "autotune")
-    tuned = dict(q_chunk=tq.value, z_run=tr.value or min(64, CONFIGS[cfg]["n"]),
-                 flux_ms=tms.value)
+    tuned = None
+    if args.autotune:
+        tq, tr, tms = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+        c3d.check(L.c3d_autotune(ctxh, ctypes.byref(tq), ctypes.byref(tr), ctypes.byref(tms)),
+                  "autotune")
+        tuned = dict(q_chunk=tq.value, z_run=tr.value or min(64, CONFIGS[cfg]["n"]),
+                     flux_ms=tms.value)
 
     # warm-up (FP64), then the start state S of both timed arms
     set_precision(0)
@@ -876,6 +965,12 @@ def b200_arm(args):
             cpu = dict(value=None, unit=UNIT, cores=os.cpu_count(), kind="reference",
                        sample=f"failed: {ex}")
         hist = {str(i): int(st.iterHist[i]) for i in range(64) if st.iterHist[i]}
+        serving = None
+        if args.serving and world == 1:
+            try:
+                serving = serving_workload(c3d, args.serve_problems)
+            except Exception as ex:  # reported, not fatal
+                serving = dict(error=str(ex))
         standalone = None
         if args.standalone and world == 1:
             try:
@@ -901,7 +996,7 @@ def b200_arm(args):
                         parallelism=f"replicas x{world}"),
             roofline=roofline, closure_roofline=closure_roofline, cpu_baseline=cpu,
             precision_compare=compare,
-            standalone_closure=standalone,
+            standalone_closure=standalone, serving=serving,
             e2e=dict(value=e2e_value, unit=UNIT, h2d_bytes_per_step=2 * nv * 8,
                      d2h_bytes_per_step=2 * nv * 8, steps=e_steps),
             gpu_launches=int(launches), clocks=clk,
@@ -952,6 +1047,13 @@ def main():
     ap.add_argument("--no-compare", dest="compare", action="store_false",
                     help="skip the other precision's arm")
     ap.set_defaults(compare=True)
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false",
+                    help="skip the flux autotuner (keeps its defaults; for launch lists)")
+    ap.add_argument("--no-serving", dest="serving", action="store_false",
+                    help="skip the serving workload (a bounded sample of the 256-problem "
+                         "stream, mixed vs FP64)")
+    ap.add_argument("--serve-problems", type=int, default=SERVE_PROBLEMS,
+                    help="problems of the seeded serving stream to run per arm")
     ap.add_argument("--no-standalone", dest="standalone", action="store_false",
                     help="skip the standalone-closure comparison (2^20 vectors, N = 1..7)")
     ap.set_defaults(standalone=True)

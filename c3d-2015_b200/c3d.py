@@ -511,7 +511,7 @@ class Solver:
 
 class Server:
     """Serving loop (include/c3d_serve.h): problems given as deck text, admitted against a
-    device-memory budget and run concurrently, one context and host thread each."""
+    device-memory budget and stepped together, one CUDA graph launch per pass."""
 
     def __init__(self, workers=4, hbm_budget=0):
         h = ctypes.c_void_p()

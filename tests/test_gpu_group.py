@@ -43,7 +43,8 @@ def _solver(tmp_path, N, stream):
               GAUSS_SIGMA=0.1, INIT_COND="gaussian_psi", THETA=2.0, OMP_THREADS=1,
               PN_USE_KINETIC_FLUX=0, MN_TOL=1e-8, MN_TOL_GAMMA=1.1, MN_COND_H_MAX=1e10,
               MN_MAX_ITER=100, MN_BATCHED="false", MN_USE_GAUNT_COEF="true",
-              MN_USE_GAUNT_SPARSE="true", REG_LADDER=LADDER)
+              MN_USE_GAUNT_SPARSE="true", CUDA_KINETIC="true", CUDA_BATCHED="true",
+              CUDA_BATCH_SIZE=50, REG_LADDER=LADDER)
     p = tmp_path / f"n{N}.deck"
     p.write_text("".join(f"{k} {v}\n" for k, v in kv.items()))
     return c3d.Solver(str(p), stream=ctypes.c_void_p(stream.cuda_stream))
@@ -100,8 +101,8 @@ def test_group_matches_per_context_closures(tmp_path, mode):
                 h = _host(b)
                 for k in ("u", "a", "it", "rg", "st"):
                     assert np.array_equal(h[k], r[k]), (mode, rep, N, k)
-            for s in solvers:
-                s.sync()
+            for s in solvers:  # vectors that exhaust the ladder are reported, not raised here
+                assert L.c3d_sync(s.ctx_handle) in (c3d.C3D_OK, 4)
         group.close()
     assert (ref[6]["it"] > 3).sum() > 100  # Newton-heavy: many rounds per order
     for s in solvers:
