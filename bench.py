@@ -212,13 +212,13 @@ def fp64_peak_tflops():
     return best
 
 
-def profile_traffic(kernel):
+def profile_traffic(kernel, key="dram_bytes_per_launch_full_workload:"):
     """DRAM bytes per launch from the committed ncu summary, if present."""
     p = os.path.join(REPO, "profiles", f"{kernel}.txt")
     if not os.path.exists(p):
         return None
     for line in open(p):
-        if line.startswith("dram_bytes_per_launch_full_workload:"):
+        if line.startswith(key):
             try:
                 return float(line.split(":", 1)[1].split()[0])
             except ValueError:
@@ -921,7 +921,7 @@ def b200_arm(args):
         stencil_flops = float((2 * nm + 60) * nq) * cells
         stencil_bytes = 8.0 * ((cells + face_ghosts) * nq + cells * nm)
         achieved_k = stencil_flops / (flux_ms * 1e-3) / 1e12
-        traffic_k = profile_traffic("kinetic_staged_m6_64")
+        traffic_k = profile_traffic("kinetic_staged_m6_64", "dram_bytes_per_launch:")
         if traffic_k is not None:
             traffic_k *= cells / 64 ** 3  # ncu capture at 64^3, scaled by (cell, direction) pairs
         roofline = dict(

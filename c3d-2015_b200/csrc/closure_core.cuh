@@ -1056,6 +1056,11 @@ __device__ void after_probe(S &sl, const ClosureParams &P, const Outputs &O, int
     if (lane == 0) {
         sl.s.passes += 1;
         sl.s.need = NEED_H;
+        // mixed precision: a gradient already within the polish range would make the
+        // reduced-precision Hessian visit of this iteration escalate (after_hessian); the cell
+        // goes to the FP64 visit directly, with the same permanent FP64 routing
+        if (P.mixed && P.mixPolish > 0.0 && err > sl.s.rtol && err <= P.mixPolish * sl.s.rtol)
+            sl.s.fp64 = 1;
     }
     __syncwarp();
 }

@@ -126,22 +126,50 @@ __global__ void ghost_mirror_check_kernel(GridDims g, const double *__restrict__
 
 // psi[q nall + ghost] = psi[q nall + image] for every face ghost and direction: the closure
 // copied the face ghosts' multipliers from their periodic images, so their ansatz values are
-// the images' too (the probe pass wrote the solved cells' values).
-// A thread per face ghost (its image found once) walks the directions; consecutive threads
-// hold consecutive ghosts, so per direction a warp's copies are contiguous runs (x and y faces)
-// or pairs (z faces).
-__global__ void psi_face_copy_kernel(GridDims g, int nq, double *__restrict__ psi)
+// the images' too (the probe pass wrote the solved cells' values). Grid x: one thread per x-
+// or y-face ghost (consecutive threads hold consecutive cells of a z line, so a warp's copies
+// per direction are contiguous runs) or per z-face pair (the two ghost layers k = 0, 1 or
+// nz+2, nz+3 of one (i, j) line, contiguous, copied as one 16-byte access when nz is even);
+// grid y: blocks of qPer directions.
+__global__ void psi_face_copy_kernel(GridDims g, int nq, int qPer, double *__restrict__ psi)
 {
-    const long long nf = ghost_faces(g), nall = g.nall();
-    for (long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x; f < nf;
-         f += (long long)gridDim.x * blockDim.x) {
-        long long dst, src;
-        ghost_pair(g, f, dst, src);
-        const double *s = psi + src;
-        double *d = psi + dst;
+    const long long fxy = 4LL * g.ny * g.nz + 4LL * g.nx * g.nz;
+    const long long nxy = (long long)g.nx * g.ny, nall = g.nall();
+    const long long total = fxy + 2 * nxy;
+    const int q0 = blockIdx.y * qPer, q1 = min(nq, q0 + qPer);
+    const bool vec = (g.nz & 1) == 0; // then every z-face pair and nall are even
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        if (t < fxy) {
+            long long dst, src;
+            ghost_pair(g, t, dst, src);
+            const double *sp = psi + src;
+            double *dp = psi + dst;
 #pragma unroll 4
-        for (int q = 0; q < nq; ++q)
-            d[(long long)q * nall] = s[(long long)q * nall];
+            for (int q = q0; q < q1; ++q)
+                dp[(long long)q * nall] = sp[(long long)q * nall];
+        } else {
+            const long long r = t - fxy;
+            const int side = (int)(r / nxy);
+            const long long r2 = r % nxy;
+            const int i = 2 + (int)(r2 / g.ny), j = 2 + (int)(r2 % g.ny);
+            const long long dst = g.cell(i, j, side == 0 ? 0 : g.nz + 2);
+            const long long src = g.cell(i, j, side == 0 ? g.nz : 2);
+            if (vec) {
+                const double2 *sp = reinterpret_cast<const double2 *>(psi + src);
+                double2 *dp = reinterpret_cast<double2 *>(psi + dst);
+                const long long step = nall / 2;
+#pragma unroll 4
+                for (int q = q0; q < q1; ++q)
+                    dp[(long long)q * step] = sp[(long long)q * step];
+            } else {
+#pragma unroll 4
+                for (int q = q0; q < q1; ++q) {
+                    psi[(long long)q * nall + dst] = psi[(long long)q * nall + src];
+                    psi[(long long)q * nall + dst + 1] = psi[(long long)q * nall + src + 1];
+                }
+            }
+        }
     }
 }
 
@@ -846,7 +874,10 @@ cudaError_t launch_psi_handoff(const GridDims &g, int nq, const double *M, const
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess || !faceCopy)
         return e;
-    psi_face_copy_kernel<<<grid_for(ghost_faces(g), 256, numSMs), 256, 0, st>>>(g, nq, psi);
+    constexpr int QPER = 64;
+    const long long threads = 4LL * g.ny * g.nz + 4LL * g.nx * g.nz + 2LL * g.nx * g.ny;
+    const dim3 grid((unsigned)((threads + 255) / 256), (unsigned)ceil_div(nq, QPER));
+    psi_face_copy_kernel<<<grid, 256, 0, st>>>(g, nq, QPER, psi);
     return cudaGetLastError();
 }
 

@@ -35,8 +35,9 @@ def _c2_deck():
     return m.c2_deck("gaussian_psi")
 
 
-def _deck(tmp_path, n, mixed, name):
-    kw = dict(NX=n, NY=n, NZ=n, MOMENT_ORDER=6, QUAD_ORDER=28, CFL_FACTOR=0.5, CROSS_SECTION=1.0,
+def _deck(tmp_path, n, mixed, name, dims=None):
+    nx, ny, nz = dims or (n, n, n)
+    kw = dict(NX=nx, NY=ny, NZ=nz, MOMENT_ORDER=6, QUAD_ORDER=28, CFL_FACTOR=0.5, CROSS_SECTION=1.0,
               INIT_FLOOR=1e-10, GAUSS_SIGMA=0.02, INIT_COND="gaussian_psi", THETA=2.0,
               MN_TOL=1e-6, MN_BATCHED="true", MN_USE_GAUNT_COEF="true",
               MN_USE_GAUNT_SPARSE="true", REG_LADDER=",".join(str(x) for x in LADDER),
@@ -48,14 +49,17 @@ def _deck(tmp_path, n, mixed, name):
     return str(p)
 
 
+@pytest.mark.parametrize("dims", [None, (20, 18, 23)])
 @pytest.mark.parametrize("mixed", [False, True])
 @pytest.mark.parametrize("mirror", [True, False])
-def test_handoff_matches_formed_ansatz(tmp_path, mixed, mirror):
+def test_handoff_matches_formed_ansatz(tmp_path, mixed, mirror, dims):
+    """dims: 24^3 (even nz: the face-ghost copy's paired z-face path and the staged stencil),
+    or 20 x 18 x 23 (odd nz: the scalar z-face copies and the global-load stencil)."""
     L = c3d.lib()
     n = 24
     out = {}
     for handoff in (True, False):
-        s = c3d.Solver(_deck(tmp_path, n, mixed, f"h{int(handoff)}.deck"))
+        s = c3d.Solver(_deck(tmp_path, n, mixed, f"h{int(handoff)}.deck", dims))
         ctx = s.ctx_handle
         c3d.check(L.c3d_set_ghost_mirroring(ctx, int(mirror)), "mirroring")
         c3d.check(L.c3d_set_ansatz_handoff(ctx, 0), "handoff")
