@@ -585,7 +585,7 @@ def standalone_closure(torch, c3d, stream, graphs=True):
 
 # ------------------------------------------------------------------ serving workload
 SERVE_STREAM = 256        # problems of the seeded stream
-SERVE_PROBLEMS = 16       # of which the bench runs the first ... per arm (bounded run time)
+SERVE_PROBLEMS = 8        # of which the bench runs the first ... per arm (bounded run time)
 SERVE_GAP_S = 0.05        # mean of the exponential inter-arrival gaps
 SERVE_BUDGET = 150 << 30  # device-memory budget of the admitted problems
 SERVE_SLOTS = 64          # problems active at once at most
@@ -652,12 +652,14 @@ def serving_workload(c3d, n_problems):
             failed += int(st != 0)
         wall = time.perf_counter() - t0
         peak_bytes, peak_active = srv.stats()
+        sched = srv.timing()
         srv.close()
         res["mixed" if mixed else "fp64"] = dict(
             cell_solves_per_s=solves / wall, wall_s=wall, cell_solves=solves,
             latency_p50_s=float(np.percentile(lat, 50)),
             latency_p99_s=float(np.percentile(lat, 99)), failed_problems=failed,
-            peak_active=peak_active, peak_budget_gb=peak_bytes / 1e9)
+            peak_active=peak_active, peak_budget_gb=peak_bytes / 1e9,
+            scheduler={k: (round(v, 3) if isinstance(v, float) else v) for k, v in sched.items()})
     res["mixed_over_fp64"] = res["mixed"]["cell_solves_per_s"] / res["fp64"]["cell_solves_per_s"]
     res["workload"] = (f"first {n_problems} of the {SERVE_STREAM}-problem seeded stream: edge "
                        "uniform 16..96, N in {1,3,5}, sigma_s U[0.5,20], pulse width U[0.02,0.2] "

@@ -32,7 +32,7 @@ SOLVER_SYMBOLS = [
 # the symbols include/c3d_serve.h declares
 SERVE_SYMBOLS = [
     "c3d_server_create", "c3d_server_submit", "c3d_server_wait", "c3d_server_stats",
-    "c3d_server_estimate", "c3d_server_destroy",
+    "c3d_server_estimate", "c3d_server_timing", "c3d_server_destroy",
 ]
 
 # the symbols include/c3d_b200.h declares
@@ -162,6 +162,7 @@ def lib():
                                       _ip]
         L.c3d_server_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong), _ip]
         L.c3d_server_estimate.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_longlong)]
+        L.c3d_server_timing.argtypes = [vp, _dp, ctypes.POINTER(ctypes.c_longlong)]
         L.c3d_server_destroy.argtypes = [vp]
         L.c3d_solver_output_timings.argtypes = [vp, ctypes.c_char_p]
         L.c3d_solver_output_opt_stats.argtypes = [vp, ctypes.c_char_p]
@@ -540,6 +541,15 @@ class Server:
         pa = ctypes.c_int(0)
         check(lib().c3d_server_stats(self.h, ctypes.byref(pb), ctypes.byref(pa)), "stats")
         return pb.value, pa.value
+
+    def timing(self):
+        """Scheduler accounting: seconds admitting, launching, waiting for passes, finishing;
+        passes and group builds."""
+        t = np.zeros(4)
+        n = (ctypes.c_longlong * 2)()
+        check(lib().c3d_server_timing(self.h, t.ctypes.data_as(_dp), n), "timing")
+        return dict(admit_s=t[0], launch_s=t[1], wait_s=t[2], finish_s=t[3], passes=n[0],
+                    group_builds=n[1])
 
     @staticmethod
     def estimate(deck_text):

@@ -1762,10 +1762,12 @@ c3d_status c3d_group_step(c3d_group *g, const double *dt)
             e = cudaStreamBeginCaptureToGraph(o, top, nullptr, nullptr, 0,
                                               cudaStreamCaptureModeRelaxed);
             cudaError_t ec = e == cudaSuccess ? cudaEventRecord(ev[K], o) : e;
+            // the contexts' steps one after another: each step fills the GPU with its own
+            // kernels, and measured as parallel branches they ran slower than in sequence
             for (int k = 0; k < K && ec == cudaSuccess; ++k) {
                 c3d_ctx *c = g->ctx[k];
                 g->stepLaunches[k] = 0;
-                ec = cudaStreamWaitEvent(c->sc[0], ev[K], 0);
+                ec = cudaStreamWaitEvent(c->sc[0], k == 0 ? ev[K] : ev[k - 1], 0);
                 for (int stage = 0; stage < 2 && ec == cudaSuccess; ++stage) {
                     long long n = 0;
                     ec = stage_capture(c, stage, dt[k], handoff[k] != 0, top, c->sc, &n);
@@ -1773,9 +1775,9 @@ c3d_status c3d_group_step(c3d_group *g, const double *dt)
                 }
                 if (ec == cudaSuccess)
                     ec = cudaEventRecord(ev[k], c->sc[0]);
-                if (ec == cudaSuccess)
-                    ec = cudaStreamWaitEvent(o, ev[k], 0);
             }
+            if (ec == cudaSuccess)
+                ec = cudaStreamWaitEvent(o, ev[K - 1], 0);
             if (e == cudaSuccess) {
                 cudaGraph_t out = nullptr;
                 e = cudaStreamEndCapture(o, &out);

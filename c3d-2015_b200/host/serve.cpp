@@ -93,6 +93,11 @@ struct c3d_server {
     long long nextId = 1;
     bool stopping = false;
     cudaStream_t stream = nullptr; // every problem's context
+    // scheduler accounting (c3d_server_timing): host seconds in admission (problem set-up),
+    // in group creation and step launches (graph builds included), waiting for passes, and
+    // finishing problems; passes run and group (re)builds
+    double tAdmit = 0, tLaunch = 0, tWait = 0, tFinish = 0;
+    long long passes = 0, builds = 0;
     std::mutex m;
     std::condition_variable cv;
     std::deque<Request *> pending;
@@ -189,8 +194,18 @@ void c3d_server::schedule()
     std::vector<std::unique_ptr<Active>> active;
     c3d_group *group = nullptr;
     std::vector<c3d_ctx *> members;
+    auto now = [] { return Clock::now(); };
+    auto secs = [](Clock::time_point a, Clock::time_point b) {
+        return std::chrono::duration<double>(b - a).count();
+    };
+    auto acc = [&](double &x, double v) {
+        std::lock_guard<std::mutex> lk(m);
+        x += v;
+    };
     for (;;) {
+        Clock::time_point t0 = now();
         admit(active);
+        acc(tAdmit, secs(t0, now()));
         if (active.empty()) {
             std::unique_lock<std::mutex> lk(m);
             cv.wait(lk, [&] { return stopping || !pending.empty(); });
@@ -206,13 +221,17 @@ void c3d_server::schedule()
                 dts.push_back(a->plan[a->next]);
             }
         c3d_status gs = C3D_OK;
+        t0 = now();
         if (grouped != members) {
             if (group)
                 c3d_group_destroy(group);
             group = nullptr;
             members = grouped;
-            if (!members.empty())
+            if (!members.empty()) {
                 gs = c3d_group_create((int)members.size(), members.data(), &group);
+                std::lock_guard<std::mutex> lk(m);
+                ++builds;
+            }
         }
         if (gs == C3D_OK && group)
             gs = c3d_group_step(group, dts.data());
@@ -221,8 +240,18 @@ void c3d_server::schedule()
             Active &a = *active[k];
             st[k] = a.s->graphable() ? gs : a.s->update(a.plan[a.next]);
         }
+        Clock::time_point t1 = now();
+        {
+            std::lock_guard<std::mutex> lk(m);
+            ++passes;
+            tLaunch += secs(t0, t1);
+        }
         admit(active); // overlaps the pass on the GPU; new problems join the next pass
+        Clock::time_point t2 = now();
+        acc(tAdmit, secs(t1, t2));
         cudaStreamSynchronize(stream);
+        Clock::time_point t3 = now();
+        acc(tWait, secs(t2, t3));
         // the problems of this pass are active[0 .. st.size()), in order; admitted ones follow
         for (size_t k = 0, j = 0; k < active.size(); ++j) {
             Active &a = *active[k];
@@ -237,6 +266,7 @@ void c3d_server::schedule()
             }
             ++k;
         }
+        acc(tFinish, secs(t3, now()));
     }
     if (group)
         c3d_group_destroy(group);
@@ -332,6 +362,24 @@ c3d_status c3d_server_stats(c3d_server *s, long long *peakBytes, int *peakActive
         *peakBytes = s->peakBytes;
     if (peakActive)
         *peakActive = s->peakActive;
+    return C3D_OK;
+}
+
+c3d_status c3d_server_timing(c3d_server *s, double *seconds, long long *counts)
+{
+    if (!s)
+        return C3D_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(s->m);
+    if (seconds) {
+        seconds[0] = s->tAdmit;
+        seconds[1] = s->tLaunch;
+        seconds[2] = s->tWait;
+        seconds[3] = s->tFinish;
+    }
+    if (counts) {
+        counts[0] = s->passes;
+        counts[1] = s->builds;
+    }
     return C3D_OK;
 }
 

@@ -318,9 +318,9 @@ c3d_status c3d_group_closure_vectors(c3d_group *group, const long long *n, doubl
                                      int *const *iterGamma, int *const *regIndex,
                                      int *const *status);
 /* One SSP-RK2 step of every context of the group (dt[k] for context k; each as c3d_step) as
- * ONE CUDA graph launch whose parallel branches are the contexts' steps: the independent
- * problems' stages share the GPU in one launch. Results are those of c3d_step per context, bit
- * for bit. Each context needs the work-list engine and graphs on, and timing, the x-line log
+ * ONE CUDA graph launch that runs the contexts' steps one after another (each step's kernels
+ * fill the GPU; as parallel branches the same steps ran slower). Results are those of c3d_step
+ * per context, bit for bit. Each context needs the work-list engine and graphs on, and timing, the x-line log
  * and re-projection off. The graph is rebuilt when a dt, an option or a buffer changes. */
 c3d_status c3d_group_step(c3d_group *group, const double *dt);
 void c3d_group_destroy(c3d_group *group);

@@ -41,6 +41,13 @@ c3d_status c3d_server_wait(c3d_server *s, long long id, int *dims, double *u, lo
 /* Peak estimated device bytes and peak number of problems active at once so far. */
 c3d_status c3d_server_stats(c3d_server *s, long long *peakBytes, int *peakActive);
 
+/* Where the scheduling thread's time went so far: seconds[0] admitting problems (host set-up
+ * of tables, initial state and device context), [1] creating groups and launching passes
+ * (graph captures included), [2] waiting for passes to finish on the GPU, [3] finishing problems
+ * (results to the host, contexts freed); counts[0] passes, [1] group builds. Either pointer may
+ * be NULL. */
+c3d_status c3d_server_timing(c3d_server *s, double *seconds, long long *counts);
+
 /* Estimated device footprint of a deck's problem in bytes (the admission test's figure). */
 c3d_status c3d_server_estimate(const char *deckText, long long *bytes);
 

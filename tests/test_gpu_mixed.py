@@ -131,12 +131,14 @@ def test_mixed_precision_routing(m6_cells, levels):
     """Thresholds route the Hessians: with no condition bound every Hessian after the
     first (3xTF32, no record yet; many first iterations end on the convergence certificate
     without one) is BF16 unless a factorisation fails; with zero bounds they are FP64.
-    Either way every cell meets the FP64 residual."""
+    Either way every cell meets the FP64 residual. The polish is off here (polish 1), which
+    would otherwise send first visits whose probe gradient lies within 1e3 of the tolerance
+    to FP64 Hessians (covered by the other tests, which use the default)."""
     S = m6_cells
     if levels == "bf16":
-        m = _solve(S, 1, 1e300, 1e300)
+        m = _solve(S, 1, 1e300, 1e300, polish=1.0)
     else:
-        m = _solve(S, 1, 1e-300, 1e-300)
+        m = _solve(S, 1, 1e-300, 1e-300, polish=1.0)
     st = m["stats"]
     assert (m["st"] == 0).all()
     assert _residual(S["T"], m["u"], m["a"]).max() <= TOL * 1.001
