@@ -1018,6 +1018,21 @@ def b200_arm(args):
             failed_cells_timed=int(st.failed), syncs_with_failed_cells=failed[0],
             closure_phase_clocks=dict(refill=st.clkRefill, passes=st.clkPass,
                                       newton_logic=st.clkSerial, n_passes=st.passes))
+        # compact figures of the other two workloads, near the end of the line
+        summary = {}
+        ol = (standalone or {}).get("one_launch")
+        if ol:
+            summary["standalone_one_launch"] = dict(
+                fp64_solves_per_s=round(ol["fp64_solves_per_s"]),
+                mixed_solves_per_s=round(ol["mixed_solves_per_s"]),
+                mixed_over_fp64=round(ol["mixed_over_fp64"], 3))
+        if serving and "mixed" in serving:
+            summary["serving"] = {a: dict(cell_solves_per_s=round(serving[a]["cell_solves_per_s"]),
+                                          p50_s=round(serving[a]["latency_p50_s"], 3),
+                                          p99_s=round(serving[a]["latency_p99_s"], 3))
+                                  for a in ("mixed", "fp64")}
+        if summary:
+            line["workloads"] = summary
         if compare is not None:
             # last key, so that it stays in a tail of the output: the mixed arm's error
             line["accuracy"] = dict(vs="fp64 drop-in arm", moments_rel_l2=compare["moments_rel_l2"],

@@ -11,7 +11,8 @@ through the C ABI twice in a row on different vectors, and checks each call agai
 context-based c3d_closure_vectors on the same inputs: identical Newton iteration counts
 and statuses, multipliers and moments within 1e-10 relative (the tolerance of the
 closure parity tests). It also checks that a call leaves the device's free memory and
-torch's reserved pool unchanged, runs the largest sizes the static array accepts
+torch's reserved pool unchanged, compares a call with the C oracle on its own (iteration
+counts except rounding ties, multipliers 1e-10), runs the largest sizes the static array accepts
 (nm = 64, nq = 2048, which fill it to its last byte), and reads a call's outcome with
 c3d_closure_vectors_noalloc_check. This file is named to be collected last.
 """
@@ -136,6 +137,32 @@ def test_noalloc_matches_existing_entry_point_twice():
     for call, seed in enumerate((11, 12)):  # two calls in a row, different vectors
         ite = _compare(q, 3000, seed, dM, dw)
         assert ite.max() > 1, call  # the vectors need real Newton work
+
+
+def test_noalloc_matches_oracle(oracle):
+    """The entry point against the C oracle (the reference's batched closure restated) on 400
+    M_4 vectors, on its own: identical Newton iteration counts and statuses except rounding
+    ties (the oracle's margins), multipliers within 1e-10 relative on the other vectors."""
+    import torch
+    from oracle_lib import make_opts, tie_cells
+    q = c3d.quadrature(4, 20)
+    T = oracle.tables(4, 20)
+    assert np.array_equal(T["M"], q["M"])
+    dM = torch.tensor(q["M"], device="cuda")
+    dw = torch.tensor(q["w"], device="cuda")
+    u, a0 = _vectors(q, 400, 13)
+    un, an, itn, stn = _noalloc(q, u, a0, dM, dw)
+    uo, ao = u.copy(), a0.copy()
+    ro = oracle.closure(make_opts(q["nm"], q["nq"], batched=True, tol=1e-8, ladder=LADDER), T,
+                        uo, ao)
+    ties = tie_cells(ro)
+    assert np.array_equal(stn, ro["status"])
+    mism = itn != ro["totalIter"]
+    assert not (mism & ~ties).any(), int((mism & ~ties).sum())
+    ok = ~ties & (ro["status"] == 0)
+    rel = np.linalg.norm(an[ok] - ao[ok], axis=1) / np.linalg.norm(ao[ok], axis=1)
+    assert ok.sum() > 300 and rel.max() <= 1e-10, (int(ok.sum()), rel.max())
+    assert itn.max() > 1
 
 
 def test_noalloc_largest_sizes():
