@@ -48,7 +48,7 @@ HEADER_SYMBOLS = [
     "c3d_set_x_halo_external", "c3d_copy_x_planes", "c3d_set_precision",
     "c3d_set_certificate", "c3d_autotune", "c3d_closure_vectors_noalloc_check",
     "c3d_set_limits", "c3d_set_ansatz_handoff", "c3d_set_graphs", "c3d_group_create",
-    "c3d_group_closure_vectors", "c3d_group_step", "c3d_group_destroy",
+    "c3d_group_closure_vectors", "c3d_group_step", "c3d_group_destroy", "c3d_stage_part",
 ]
 
 
@@ -171,6 +171,7 @@ def lib():
         L.c3d_line_stats_enable.argtypes = [vp, ctypes.c_int]
         L.c3d_line_stats_get.argtypes = [vp, _dp, _ip]
         L.c3d_stage.argtypes = [vp, ctypes.c_int, ctypes.c_double]
+        L.c3d_stage_part.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int]
         L.c3d_set_x_halo_external.argtypes = [vp, ctypes.c_int]
         L.c3d_copy_x_planes.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp,
                                         ctypes.c_int, ctypes.c_int]
@@ -280,6 +281,10 @@ class Context:
 
     def stage(self, stage, dt):
         check(lib().c3d_stage(self.h, stage, dt), "c3d_stage")
+
+    def stage_part(self, stage, dt, part):
+        """c3d_stage_part: part 0 needs no x halo, part 1 runs once the x ghosts are filled."""
+        check(lib().c3d_stage_part(self.h, stage, dt, part), "c3d_stage_part")
 
     def set_x_halo_external(self, on=True):
         check(lib().c3d_set_x_halo_external(self.h, int(bool(on))), "c3d_set_x_halo_external")

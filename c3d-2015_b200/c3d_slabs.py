@@ -52,25 +52,34 @@ class XHaloExchange:
         c.copy_x_planes(0, 0, 2, self.recv_lo.data_ptr(), False, self.device)
         c.copy_x_planes(0, self.nx + 2, 2, self.recv_hi.data_ptr(), False, self.device)
 
-    def exchange(self):
-        """One halo exchange with the neighbouring ranks (torch.distributed must be set up
-        for world > 1). Sends and receives are issued in the same order on every rank, so
-        that with two ranks (left == right) they pair up correctly whatever the backend."""
-        self.pack()
+    def start(self):
+        """Starts the exchange of the packed planes with the neighbouring ranks
+        (torch.distributed must be set up for world > 1) and returns its requests. Sends and
+        receives are issued in the same order on every rank, so that with two ranks
+        (left == right) they pair up correctly whatever the backend."""
         if self.world == 1:
             self.recv_lo.copy_(self.send_hi)
             self.recv_hi.copy_(self.send_lo)
-        else:
-            import torch.distributed as dist
-            ops = [dist.P2POp(dist.isend, self.send_hi, self.right, tag=self.TO_LOW),
-                   dist.P2POp(dist.irecv, self.recv_lo, self.left, tag=self.TO_LOW),
-                   dist.P2POp(dist.isend, self.send_lo, self.left, tag=self.TO_HIGH),
-                   dist.P2POp(dist.irecv, self.recv_hi, self.right, tag=self.TO_HIGH)]
-            for r in dist.batch_isend_irecv(ops):
-                r.wait()
-            if self.device:
-                torch.cuda.current_stream().synchronize()
+            return []
+        import torch.distributed as dist
+        ops = [dist.P2POp(dist.isend, self.send_hi, self.right, tag=self.TO_LOW),
+               dist.P2POp(dist.irecv, self.recv_lo, self.left, tag=self.TO_LOW),
+               dist.P2POp(dist.isend, self.send_lo, self.left, tag=self.TO_HIGH),
+               dist.P2POp(dist.irecv, self.recv_hi, self.right, tag=self.TO_HIGH)]
+        return dist.batch_isend_irecv(ops)
+
+    def finish(self, reqs):
+        """Waits for the exchange started by start() and fills the x ghost planes."""
+        for r in reqs:
+            r.wait()
+        if self.device and reqs:
+            torch.cuda.current_stream().synchronize()
         self.unpack()
+
+    def exchange(self):
+        """One halo exchange with the neighbouring ranks, blocking: pack, start, finish."""
+        self.pack()
+        self.finish(self.start())
 
 
 def exchange_local(halos):
@@ -88,16 +97,43 @@ def exchange_local(halos):
         h.unpack()
 
 
-def step_slab(ctx, halo, dt):
-    """update(dt) of one rank's slab: a halo exchange before each RK stage."""
+def step_slab(ctx, halo, dt, overlap=True):
+    """update(dt) of one rank's slab: a halo exchange before each RK stage. With overlap (M_N
+    slab contexts) the exchange runs while the stage's first part (c3d_stage_part: the closure
+    of the cells that need no halo) runs on the GPU: pack, start the exchange, part 0, finish
+    the exchange (x ghosts filled), part 1. Results are the same either way."""
     for stage in (0, 1):
-        halo.exchange()
-        ctx.stage(stage, dt)
+        if overlap:
+            halo.pack()
+            reqs = halo.start()
+            ctx.stage_part(stage, dt, 0)
+            halo.finish(reqs)
+            ctx.stage_part(stage, dt, 1)
+        else:
+            halo.exchange()
+            ctx.stage(stage, dt)
 
 
-def step_slabs_local(ctxs, halos, dt):
-    """update(dt) of all slabs held by one process."""
+def step_slabs_local(ctxs, halos, dt, overlap=False):
+    """update(dt) of all slabs held by one process (overlap: the split stage of step_slab,
+    the planes packed before every slab's part 0)."""
     for stage in (0, 1):
-        exchange_local(halos)
+        if not overlap:
+            exchange_local(halos)
+            for c in ctxs:
+                c.stage(stage, dt)
+            continue
+        for h in halos:
+            h.pack()
         for c in ctxs:
-            c.stage(stage, dt)
+            c.stage_part(stage, dt, 0)
+        w = len(halos)
+        for r, h in enumerate(halos):
+            h.recv_lo.copy_(halos[(r - 1) % w].send_hi)
+            h.recv_hi.copy_(halos[(r + 1) % w].send_lo)
+        if halos and halos[0].device:
+            torch.cuda.current_stream().synchronize()
+        for h in halos:
+            h.unpack()
+        for c in ctxs:
+            c.stage_part(stage, dt, 1)

@@ -195,6 +195,10 @@ struct c3d_ctx {
     // face-ghost mirroring: when every face ghost's multipliers equal its periodic image's
     // (bitwise), the closure solves only the other cells (cellMap) and copies the face ghosts
     int *cellMap = nullptr;
+    // x-slab split of the closure (c3d_stage_part): cells of the x-planes 2 .. nx+1, and of the
+    // four x-ghost planes
+    int *xSplit[2] = {nullptr, nullptr};
+    long long xSplitCount[2] = {0, 0};
     long long cellMapCount = 0;
     int *mirrorFlag = nullptr;     // device
     int *mirrorHost = nullptr;     // pinned
@@ -257,7 +261,7 @@ static void free_ctx(c3d_ctx *c)
                     c->rCounts, c->rBuf, c->mfA, c->mfP, c->cellMap, c->mirrorFlag,
                     c->gChunksC, c->cellGamma, c->cellErr, c->lineLog, c->mixF64,
                     c->mixA[0], c->mixA[1], c->cellCond, c->g0, c->psiRefresh,
-                    c->psiRefreshCount};
+                    c->psiRefreshCount, c->xSplit[0], c->xSplit[1]};
     for (void *p : ptrs)
         if (p)
             cudaFree(p);
@@ -1844,6 +1848,87 @@ c3d_status c3d_stage(c3d_ctx *c, int stage, double dt)
         if ((s = c3d_flux_kinetic(c, 1)) != C3D_OK)
             return s;
     }
+    if ((s = c3d_euler(c, dt)) != C3D_OK)
+        return s;
+    if (stage == 1) {
+        C3D_CUDA(launch_rk(c->g, c->u, c->uOld, 1, c->numSMs, c->stream));
+        c->launches += 1;
+    }
+    return C3D_OK;
+}
+
+// The cells of the x-slab split: x is the slowest index of the I3D layout, so each x-plane is
+// a contiguous block of (ny+4)(nz+4) cells.
+static c3d_status ensure_xsplit(c3d_ctx *c)
+{
+    if (c->xSplit[0])
+        return C3D_OK;
+    const long long P = (long long)c->g.nyg() * c->g.nzg();
+    std::vector<int> part[2];
+    part[0].reserve((size_t)(c->g.nx * P));
+    part[1].reserve((size_t)(4 * P));
+    for (int i = 0; i < c->g.nxg(); ++i) {
+        const int w = (i < 2 || i >= c->g.nx + 2) ? 1 : 0;
+        for (long long p = 0; p < P; ++p)
+            part[w].push_back((int)(i * P + p));
+    }
+    for (int w = 0; w < 2; ++w) {
+        if (cudaMalloc(&c->xSplit[w], part[w].size() * sizeof(int)) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(C3D_ERR_OOM, "c3d_stage_part: device allocation failed");
+        }
+        C3D_CUDA(cudaMemcpy(c->xSplit[w], part[w].data(), part[w].size() * sizeof(int),
+                            cudaMemcpyHostToDevice));
+        c->xSplitCount[w] = (long long)part[w].size();
+    }
+    return C3D_OK;
+}
+
+c3d_status c3d_stage_part(c3d_ctx *c, int stage, double dt, int part)
+{
+    if (!c || stage < 0 || stage > 1 || part < 0 || part > 1)
+        return fail(C3D_ERR_INVALID, "c3d_stage_part: bad argument");
+    if (c->solver != 1 || !c->xHaloExternal || c->engine != 0)
+        return fail(C3D_ERR_INVALID, "c3d_stage_part: the split stage is for M_N slab contexts "
+                                     "(c3d_set_x_halo_external) on the work-list engine");
+    c3d_status s = ensure_xsplit(c);
+    if (s != C3D_OK)
+        return s;
+    if (part == 0) {
+        if (stage == 0) {
+            C3D_CUDA(launch_rk(c->g, c->u, c->uOld, 0, c->numSMs, c->stream));
+            c->launches += 1;
+        }
+        if ((s = c3d_ghost_fill(c)) != C3D_OK) // the y and z faces
+            return s;
+    }
+    cudaEvent_t t0 = nullptr;
+    timing_begin(c, &t0);
+    s = run_closure(c, c->xSplitCount[part], c->u, c->alpha, c->iters, c->iterGamma, c->regIdx,
+                    c->status, c->xSplit[part], true);
+    if (s != C3D_OK)
+        return s;
+    if ((s = finish_handoff(c, false)) != C3D_OK)
+        return s;
+    if (part == 1) {
+        if (c->lineLog && c->lineCount < c->lineCap) {
+            C3D_CUDA(launch_line_log(c->g, c->cp, c->iters, c->iterGamma, c->regIdx,
+                                     c->cellGamma, c->cellErr,
+                                     c->lineLog + (size_t)c->lineCount * c->g.nx * 5, c->stream));
+            c->lineCount++;
+            c->launches += 1;
+        }
+        if (c->reproject) {
+            C3D_CUDA(launch_reproject(c->g, c->u, c->alpha, c->mfA, c->mfP, c->nq, c->errorFlag,
+                                      c->stream));
+            c->launches += 1;
+        }
+    }
+    timing_end(c, 0, t0);
+    if (part == 0)
+        return C3D_OK;
+    if ((s = c3d_flux_kinetic(c, 0)) != C3D_OK)
+        return s;
     if ((s = c3d_euler(c, dt)) != C3D_OK)
         return s;
     if (stage == 1) {

@@ -171,6 +171,17 @@ c3d_status c3d_stage(c3d_ctx *ctx, int stage, double dt);
  * face-ghost mirroring is off for such a context. */
 c3d_status c3d_set_x_halo_external(c3d_ctx *ctx, int on);
 
+/* One RK stage of a slab context (c3d_set_x_halo_external on; M_N, work-list engine) in two
+ * parts, so that the halo exchange overlaps the closure: part 0 = [stage 0: save u,] the y and
+ * z ghost fill and the closure of the cells of the x-planes 2 .. nx+1, which need no halo;
+ * part 1 = the closure of the four x-ghost planes, then the flux and Euler stage [stage 1: RK
+ * average]. The caller copies u's first and last two interior x-planes out before part 0 (they
+ * hold the stage's pre-closure moments, as the reference's exchange before the closure,
+ * src/update.cpp:216-221), exchanges them while part 0 runs, and fills the x ghost planes
+ * before part 1. Part 0 then part 1 equals c3d_stage bit for bit (cells are solved
+ * independently). Launch by launch (no stage graph). */
+c3d_status c3d_stage_part(c3d_ctx *ctx, int stage, double dt, int part);
+
 /* Copies the x-planes i0 .. i0+count-1 (ghost indices 0 .. nx+3; each plane (ny+4)(nz+4) nm
  * doubles, contiguous) of u (field 0) or alpha (field 1) to (toBuf = 1) or from (toBuf = 0)
  * buf: a device buffer (where = 1, ordered on the context's stream) or a host buffer

@@ -33,6 +33,25 @@ class _HostSlab:
         pass
 
 
+class _HostStageSlab(_HostSlab):
+    """_HostSlab with the split stage of c3d_stage_part: part 0 changes the interior planes
+    (as a closure may regularise moments), part 1 records whether the x ghosts hold the
+    neighbours' planes from before their part 0 -- want[stage]."""
+
+    def __init__(self, u, n, want):
+        super().__init__(u)
+        self.n, self.want, self.ok = n, want, []
+
+    def stage_part(self, stage, dt, part):
+        n = self.n
+        if part == 0:
+            self.u[2:n + 2] *= 2.0
+        else:
+            ghosts = np.concatenate([self.u[0:2], self.u[n + 2:n + 4]])
+            ref = np.concatenate([self.want[stage][0:2], self.want[stage][n + 2:n + 4]])
+            self.ok.append(bool(np.array_equal(ghosts, ref)))
+
+
 def _global_periodic(u, nx):
     g = u.copy()
     g[0:2] = u[nx:nx + 2]
@@ -56,7 +75,16 @@ def _worker(rank, world, port, nx, q):
         h = c3d_slabs.XHaloExchange(slab, n, (ny + 4) * (nz + 4) * nm, rank, world, device=False)
         h.exchange()
         want = _global_periodic(u, nx)[x0:x0 + n + 4]
-        q.put((rank, bool(np.array_equal(slab.u, want))))
+        ok = bool(np.array_equal(slab.u, want))
+        # the overlapped step: planes packed before part 0, exchanged while it runs, the
+        # ghosts filled before part 1 (stage s sees the planes of 2^s u)
+        wants = [_global_periodic(f * u, nx)[x0:x0 + n + 4] for f in (1.0, 2.0)]
+        st = _HostStageSlab(u[x0:x0 + n + 4].copy(), n, wants)
+        st.u[0:2] = np.nan
+        st.u[n + 2:n + 4] = np.nan
+        hs = c3d_slabs.XHaloExchange(st, n, (ny + 4) * (nz + 4) * nm, rank, world, device=False)
+        c3d_slabs.step_slab(st, hs, 0.1, overlap=True)
+        q.put((rank, ok and st.ok == [True, True]))
     finally:
         dist.destroy_process_group()
 
@@ -83,8 +111,10 @@ def test_slab_bounds():
 
 
 @pytest.mark.gpu
-def test_two_slabs_on_one_gpu_equal_single_domain(oracle):
-    """Two x-slabs of an 8^3 M_2 grid, stepped with the halo exchange: interiors bit for bit
+@pytest.mark.parametrize("overlap", [False, True])
+def test_two_slabs_on_one_gpu_equal_single_domain(oracle, overlap):
+    """Two x-slabs of an 8^3 M_2 grid, stepped with the halo exchange (overlap: the split
+    stage, c3d_stage_part, with the planes exchanged between its parts): interiors bit for bit
     equal to the single-domain run after two steps."""
     from test_gpu_kernels import _setup
     import c3d
@@ -111,7 +141,7 @@ def test_two_slabs_on_one_gpu_equal_single_domain(oracle):
         bounds.append((x0, nl))
     for _ in range(2):
         g.step(S["dt"])
-        c3d_slabs.step_slabs_local(ctxs, halos, S["dt"])
+        c3d_slabs.step_slabs_local(ctxs, halos, S["dt"], overlap=overlap)
     g.sync()
     ug, _ = g.get_state()
     ug = ug.reshape(n + 4, n + 4, n + 4, nm)
