@@ -161,7 +161,8 @@ def test_noalloc_matches_oracle(oracle):
     assert not (mism & ~ties).any(), int((mism & ~ties).sum())
     ok = ~ties & (ro["status"] == 0)
     rel = np.linalg.norm(an[ok] - ao[ok], axis=1) / np.linalg.norm(ao[ok], axis=1)
-    assert ok.sum() > 300 and rel.max() <= 1e-10, (int(ok.sum()), rel.max())
+    assert ok.sum() > 150, (int(ok.sum()), int(ties.sum()))  # ~1/3 are ties at MN_TOL 1e-8
+    assert rel.max() <= 1e-10, rel.max()
     assert itn.max() > 1
 
 
