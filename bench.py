@@ -415,6 +415,56 @@ def c3d_quadrature_m2(q):
     return c3d.quadrature(q["N"], q["Q"], with_m2=True)["M2"]
 
 
+def standalone_one_order(args):
+    """One order of the standalone workload, closed once (for launch lists: with --no-graphs
+    every kernel launches from the host)."""
+    import torch
+    import c3d
+    L = c3d.lib()
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    N, n = args.standalone_order, args.standalone_vectors
+    q, u, a_iso = standalone_vectors(c3d, N, n)
+    with tempfile.TemporaryDirectory() as tmp:
+        deck = os.path.join(tmp, "input.deck")
+        with open(deck, "w") as f:
+            f.write(standalone_deck(N))
+        solver = c3d.Solver(deck, stream=ctypes.c_void_p(stream.cuda_stream))
+    h = solver.ctx_handle
+    c3d.check(L.c3d_set_graphs(h, 1 if args.graphs else 0), "graphs")
+    c3d.check(L.c3d_set_precision(h, 1 if args.precision == "mixed" else 0, 0.0, 0.0, 0, 0.0),
+              "precision")
+    du = torch.tensor(u, device="cuda")
+    da = torch.tensor(a_iso, device="cuda")
+    it = torch.zeros(n, dtype=torch.int32, device="cuda")
+    stt = torch.zeros(n, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    c3d.check(L.c3d_closure_vectors(h, n, ctypes.c_void_p(du.data_ptr()),
+                                    ctypes.c_void_p(da.data_ptr()), ctypes.c_void_p(it.data_ptr()),
+                                    None, None, ctypes.c_void_p(stt.data_ptr())), "closure")
+    L.c3d_sync(h)
+    torch.cuda.synchronize()
+    print(json.dumps(dict(order=N, vectors=n, precision=args.precision,
+                          seconds=time.perf_counter() - t0,
+                          iters_per_solve=float(it.double().mean()),
+                          failed=int((stt != 0).sum()))), flush=True)
+    solver.close()
+
+
+def standalone_deck(N):
+    kv = dict(SOLVER="mn", TFINAL="1", OUTDT="1000", OUTPUT_DATA="false",
+              OUTPUT_OPT_STATS="false", OUTPUT_TIMINGS="false", NX=2, NY=2, NZ=2,
+              MPIX=1, MPIY=1, MPIZ=1, AX=-1, AY=-1, AZ=-1, BX=1, BY=1, BZ=1,
+              MOMENT_ORDER=N, QUAD_ORDER=2 * (N + 3), CFL_FACTOR=0.5, CROSS_SECTION=1.0,
+              INIT_FLOOR=1e-4, GAUSS_SIGMA=0.1, INIT_COND="gaussian_psi", THETA=2.0,
+              OMP_THREADS=1, PN_USE_KINETIC_FLUX=0, MN_TOL=STANDALONE_TOL, MN_TOL_GAMMA=1.1,
+              MN_COND_H_MAX=1e10, MN_MAX_ITER=100, MN_BATCHED="false",
+              MN_USE_GAUNT_COEF="true", MN_USE_GAUNT_SPARSE="true", CUDA_KINETIC="true",
+              CUDA_BATCHED="true", CUDA_BATCH_SIZE=50, REG_LADDER=STANDALONE_LADDER)
+    return "".join(f"{k} {v}\n" for k, v in kv.items())
+
+
 def standalone_closure(torch, c3d, stream, graphs=True):
     """FP64 vs mixed closure of the standalone workload (one context per order, Gaunt form,
     unbatched rules: |g| <= |u| MN_TOL, gamma <= 1.1, MN_TOL 1e-8). Device-resident vectors;
@@ -441,19 +491,8 @@ def standalone_closure(torch, c3d, stream, graphs=True):
             n = len(u)
             with tempfile.TemporaryDirectory() as tmp:
                 deck = os.path.join(tmp, "input.deck")
-                kv = dict(SOLVER="mn", TFINAL="1", OUTDT="1000", OUTPUT_DATA="false",
-                          OUTPUT_OPT_STATS="false", OUTPUT_TIMINGS="false", NX=2, NY=2, NZ=2,
-                          MPIX=1, MPIY=1, MPIZ=1, AX=-1, AY=-1, AZ=-1, BX=1, BY=1, BZ=1,
-                          MOMENT_ORDER=N, QUAD_ORDER=2 * (N + 3), CFL_FACTOR=0.5,
-                          CROSS_SECTION=1.0, INIT_FLOOR=1e-4, GAUSS_SIGMA=0.1,
-                          INIT_COND="gaussian_psi", THETA=2.0, OMP_THREADS=1,
-                          PN_USE_KINETIC_FLUX=0, MN_TOL=STANDALONE_TOL, MN_TOL_GAMMA=1.1,
-                          MN_COND_H_MAX=1e10, MN_MAX_ITER=100, MN_BATCHED="false",
-                          MN_USE_GAUNT_COEF="true", MN_USE_GAUNT_SPARSE="true",
-                          CUDA_KINETIC="true", CUDA_BATCHED="true", CUDA_BATCH_SIZE=50,
-                          REG_LADDER=STANDALONE_LADDER)
                 with open(deck, "w") as f:
-                    f.write("".join(f"{k} {v}\n" for k, v in kv.items()))
+                    f.write(standalone_deck(N))
                 solver = c3d.Solver(deck, stream=ctypes.c_void_p(stream.cuda_stream))
             solvers.append(solver)
             vecs.append((u, a_iso))
@@ -1074,7 +1113,14 @@ def main():
     ap.add_argument("--no-standalone", dest="standalone", action="store_false",
                     help="skip the standalone-closure comparison (2^20 vectors, N = 1..7)")
     ap.set_defaults(standalone=True)
+    ap.add_argument("--standalone-order", type=int, default=0,
+                    help="profiling aid: only one order's standalone closure (the first "
+                         "--standalone-vectors vectors), in the --precision arm, then exit")
+    ap.add_argument("--standalone-vectors", type=int, default=40000)
     args = ap.parse_args()
+    if args.standalone_order:
+        standalone_one_order(args)
+        return
     if args.engine != "rounds" or args.hessian != "gaunt":
         # the mixed closure is built on the work-list engine's Gaunt form
         args.precision = "fp64"
