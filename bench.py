@@ -1032,7 +1032,8 @@ def b200_arm(args):
                                  "deck's default)" if args.hessian == "gaunt" else "direct"),
                         engine=args.engine,
                         mn_tol=MN_TOL, mn_batched=True, ladder=LADDER,
-                        cells_per_step=2 * cells, l2="inputs larger than L2 (u, alpha 0.9 GB each)",
+                        cells_per_step=2 * cells,
+                        l2=f"inputs larger than L2 (u, alpha {nv * 8 / 1e9:.2f} GB each)",
                         flux_autotune=tuned,
                         parallelism=f"replicas x{world}"),
             roofline=roofline, closure_roofline=closure_roofline, cpu_baseline=cpu,
@@ -1043,9 +1044,12 @@ def b200_arm(args):
             gpu_launches=int(launches), clocks=clk,
             stage_graphs=dict(launches_per_step=launches / args.steps,
                               host_syncs_per_step=head["syncs"] / args.steps,
-                              note="each RK stage is one CUDA graph launch (closure rounds in a "
-                                   "device-side conditional loop); launches counted by the "
-                                   "library, device-side loop kernels included"),
+                              note=("each RK stage is one CUDA graph launch (closure rounds in a "
+                                    "device-side conditional loop)" if args.graphs else
+                                    "--no-graphs: kernels launched one by one, closure rounds "
+                                    "driven by the host") +
+                                   "; launches counted by the library, device-side loop "
+                                   "kernels included"),
             closure_only=dict(value=cells / (ms[0] / max(1, closure_launches) * 1e-3), unit=UNIT,
                               ms_per_closure=ms[0] / max(1, closure_launches),
                               note="interior cell-solves per second of the closure alone (the "
