@@ -52,8 +52,8 @@ cudaError_t launch_rk(const GridDims &g, double *u, double *uOld, int mode, int 
                       cudaStream_t st);
 cudaError_t launch_kinetic_flux(const GridDims &g, const double *alpha, const double *mfA,
                                 const double *mfP, const double *xi, const double *eta, int nq,
-                                int qChunk, int runLen, double dx, double dy, double dz,
-                                double theta, int isPn, double *psi, bool psiReady, double *flux,
+                                int qChunk, int runLen, double theta, int isPn, double *psi,
+                                bool psiReady, double *flux,
                                 int *errorFlag, cudaStream_t st);
 cudaError_t launch_psi_handoff(const GridDims &g, int nq, const double *M, const double *alpha,
                                bool faceCopy, const int *refresh, const unsigned int *refreshCount,
@@ -72,7 +72,8 @@ cudaError_t launch_ghost_stats(const GridDims &g, const int *iters, const int *i
 cudaError_t launch_ghost_mirror_check(const GridDims &g, const double *a, int *flag, int numSMs,
                                       cudaStream_t st);
 void flux_frags(int nm, int nq, const double *M, const double *w, const double *xi,
-                const double *eta, const double *mu, double *mfA, double *mfP);
+                const double *eta, const double *mu, double rdx, double rdy, double rdz,
+                double *mfA, double *mfP);
 cudaError_t launch_moment_flux(const GridDims &g, const double *u, const double *ops, double dx,
                                double dy, double dz, double *flux, cudaStream_t st);
 } // namespace c3d
@@ -372,7 +373,8 @@ c3d_status c3d_create(const c3d_params *p, const double *M, const double *w, con
     std::vector<double> ch = build_chunks(nm, nq, M, w);
     ok = ok && alloc((void **)&c->chunks, ch.size() * 8);
     std::vector<double> mfA(flux_frag_doubles(nm, nq, 0)), mfP(flux_frag_doubles(nm, nq, 1));
-    flux_frags(nm, nq, M, w, xi, eta, mu, mfA.data(), mfP.data());
+    flux_frags(nm, nq, M, w, xi, eta, mu, 1.0 / p->dx, 1.0 / p->dy, 1.0 / p->dz, mfA.data(),
+               mfP.data());
     ok = ok && alloc((void **)&c->mfA, mfA.size() * 8) && alloc((void **)&c->mfP, mfP.size() * 8);
     if (ok && pnOps)
         ok = alloc((void **)&c->pnops, (size_t)6 * nm * nm * 8);
@@ -1368,7 +1370,7 @@ c3d_status c3d_flux_kinetic(c3d_ctx *c, int alphaIsU)
     cudaEvent_t t0 = nullptr;
     timing_begin(c, &t0);
     C3D_CUDA(launch_kinetic_flux(c->g, a, c->mfA, c->mfP, c->xi, c->eta, c->nq, c->qChunk,
-                                 c->runLen, c->dx, c->dy, c->dz, c->theta, isPn, c->psi, ready,
+                                 c->runLen, c->theta, isPn, c->psi, ready,
                                  c->flux, c->errorFlag, c->stream));
     timing_end(c, 1, t0);
     int nch = ceil_div(c->nq, c->qChunk);
@@ -1639,7 +1641,7 @@ static cudaError_t stage_capture(c3d_ctx *c, int stage, double dt, bool handoff,
     }
     if (ec == cudaSuccess)
         ec = launch_kinetic_flux(c->g, c->alpha, c->mfA, c->mfP, c->xi, c->eta, c->nq, c->qChunk,
-                                 c->runLen, c->dx, c->dy, c->dz, c->theta, 0, c->psi, handoff,
+                                 c->runLen, c->theta, 0, c->psi, handoff,
                                  c->flux, c->errorFlag, s0);
     if (ec == cudaSuccess)
         ec = launch_euler(c->g, c->u, c->flux, c->sigT, c->sigS, dt, c->numSMs, s0);
@@ -2355,6 +2357,7 @@ void solveH_cuda(int nm, int nm2, int nq, int batchSize, double *alphas, double 
 static struct {
     c3d_ctx *ctx = nullptr;
     int nx = 0, ny = 0, nz = 0, nm = 0, nq = 0, isPn = -1;
+    double dx = 0.0, dy = 0.0, dz = 0.0;
 } g_f;
 
 void solveFluxKinetic_cuda(int nx, int ny, int nz, int nm, int nq, double dx, double dy, double dz,
@@ -2366,8 +2369,9 @@ void solveFluxKinetic_cuda(int nx, int ny, int nz, int nm, int nq, double dx, do
         fprintf(stderr, "[c3d_b200] solveFluxKinetic_cuda: grid (with ghosts) too small\n");
         return;
     }
+    // the flux fragments carry cosine x weight / spacing: a new spacing needs a new context
     if (!g_f.ctx || g_f.nx != nx || g_f.ny != ny || g_f.nz != nz || g_f.nm != nm || g_f.nq != nq ||
-        g_f.isPn != isPn) {
+        g_f.isPn != isPn || g_f.dx != dx || g_f.dy != dy || g_f.dz != dz) {
         if (g_f.ctx)
             c3d_destroy(g_f.ctx);
         g_f.ctx = nullptr;
@@ -2395,11 +2399,9 @@ void solveFluxKinetic_cuda(int nx, int ny, int nz, int nm, int nq, double dx, do
             return;
         }
         g_f.nx = nx; g_f.ny = ny; g_f.nz = nz; g_f.nm = nm; g_f.nq = nq; g_f.isPn = isPn;
+        g_f.dx = dx; g_f.dy = dy; g_f.dz = dz;
     }
     c3d_ctx *c = g_f.ctx;
-    c->dx = dx;
-    c->dy = dy;
-    c->dz = dz;
     size_t vb = c->g.nall() * nm * 8;
     cudaMemcpyAsync(c->alpha, alpha, vb, cudaMemcpyHostToDevice, c->stream);
     cudaMemsetAsync(c->flux, 0, vb, c->stream);

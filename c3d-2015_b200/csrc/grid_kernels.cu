@@ -256,7 +256,9 @@ __global__ void rk_kernel(GridDims g, double *__restrict__ u, double *__restrict
 // doubles and a CTA stages a tile with one bulk copy:
 //   ansatz     [j 0..3][k-step 0..2NT-1][lane]  M[32t + 8j + lane/4][4k + lane%4]   (B of Z = A M^T)
 //   projection [k-step 0..7][j 0..NT-1][lane]   M[32t + 4k + lane%4][8j + lane/4]   (B of F += S M)
-//              followed by xi, eta, mu, w of the tile's 32 directions.
+//              followed by c_x = (xi w)/dx, c_y = (eta w)/dy, c_z = (mu w)/dz and w of the
+//              tile's 32 directions (a direction's limited differences along each axis are
+//              weighted by c, whose sign is the cosine's).
 // Directions past nq and moments past nm are zero.
 
 constexpr int FLUX_STAGES = 2;
@@ -391,26 +393,29 @@ __device__ __forceinline__ double minmod_sel(double x, double y)
     return (x * y > 0.0) ? (fabs(x) < fabs(y) ? x : y) : 0.0;
 }
 
-// Limited upwind difference along one axis for either sign of the direction cosine om,
-// src/flux_kinetic.cpp:130-189, times om w. With h = +1/2 (om > 0: values k1..k4 at offsets
-// -2..1) or h = -1/2 (om <= 0: offsets -1..2),
-//   f = ((k3 + h s(k2,k3,k4)) - k2) - h s(k1,k2,k3),  s(l,c,r) = slopefit (src/flux_kinetic.cpp:56-61);
-// h s is exact, so the fused forms below round as the reference's expression.
-__device__ __forceinline__ double axis_flux_bf(double om, double w, double th, const double *pc,
+// Limited upwind difference along one axis for either sign of the direction weight c (the
+// cosine's sign), src/flux_kinetic.cpp:130-189. With h = +1/2 (c > 0: values k1..k4 at offsets
+// -2..1) or h = -1/2 (c <= 0: offsets -1..2),
+//   f = ((k3 + h s(k2,k3,k4)) - k2) - h s(k1,k2,k3),  s(l,c,r) = slopefit (src/flux_kinetic.cpp:56-61)
+//     = minmod(th (r - c), minmod((r - l) / 2, th (c - l))).
+// Here s' = 2 s = minmod(2th (r - c), minmod(r - l, 2th (c - l))) and h s = (h/2) s': scaling by
+// powers of two commutes with rounding and with the minmod's comparisons, so f rounds as the
+// reference's expression with two multiplications fewer per axis (th2 = 2 th).
+__device__ __forceinline__ double axis_flux_bf(double c, double th2, const double *pc,
                                                long long st)
 {
-    const bool pos = om > 0;
+    const bool pos = c > 0;
     const double *b = pos ? pc - 2 * st : pc - st;
     const double k1 = b[0], k2 = b[st], k3 = b[2 * st], k4 = b[3 * st];
-    const double h = pos ? 0.5 : -0.5;
-    const double t32 = th * (k3 - k2);
-    const double s1 = minmod_sel(th * (k4 - k3), minmod_sel(0.5 * (k4 - k2), t32));
-    const double s2 = minmod_sel(t32, minmod_sel(0.5 * (k3 - k1), th * (k2 - k1)));
-    const double f = fma(-h, s2, fma(h, s1, k3) - k2);
-    return f * om * w;
+    const double q = pos ? 0.25 : -0.25; // h / 2
+    const double t32 = th2 * (k3 - k2);
+    const double s1 = minmod_sel(th2 * (k4 - k3), minmod_sel(k4 - k2, t32));
+    const double s2 = minmod_sel(t32, minmod_sel(k3 - k1, th2 * (k2 - k1)));
+    return fma(-q, s2, fma(q, s1, k3) - k2);
 }
 
-// flux(c) (+)= sum_q m_q (Fx/dx + Fy/dy + Fz/dz) for 64 interior cells per CTA (consecutive
+// flux(c) (+)= sum_q m_q (c_x fx + c_y fy + c_z fz) (c = cosine x weight / spacing of the
+// direction, fx.. the limited differences) for 64 interior cells per CTA (consecutive
 // in the interior numbering). Per direction tile: the limited upwind differences S[q][cell]
 // of the CTA (each thread 8 (cell, direction) pairs, loads issued two pairs at a time) go to
 // shared memory, then F += S^T M on the FP64 tensor pipe (warp w: cells 8w..8w+7, all moment
@@ -418,11 +423,12 @@ __device__ __forceinline__ double axis_flux_bf(double om, double w, double th, c
 template <int NT>
 __global__ void __launch_bounds__(256)
     kinetic_dmma_kernel(GridDims g, const double *__restrict__ psi, const double *__restrict__ mfP,
-                        int q0, int nqc, double rdx, double rdy, double rdz, double theta,
-                        int accumulate, double *__restrict__ flux, int *errorFlag)
+                        int q0, int nqc, double theta, int accumulate, double *__restrict__ flux,
+                        int *errorFlag)
 {
     constexpr int TILE = 8 * NT * 32 + 128;
     constexpr int CS = 68; // S tile row stride (cells)
+    const double th2 = 2.0 * theta;
     extern __shared__ __align__(128) double kinSmem[]; // sB[FLUX_STAGES][TILE], sS[32 * CS]
     double(*sB)[TILE] = reinterpret_cast<double(*)[TILE]>(kinSmem);
     double *sS = kinSmem + FLUX_STAGES * TILE;
@@ -466,7 +472,7 @@ __global__ void __launch_bounds__(256)
                 atomicExch(errorFlag, 1);
             return;
         }
-        const double *dirs = sB[s] + 8 * NT * 32; // xi, eta, mu, w per direction
+        const double *dirs = sB[s] + 8 * NT * 32; // c_x, c_y, c_z, w per direction
 #pragma unroll 2
         for (int i = 0; i < 8; ++i) {
             const int qq = (tid >> 6) + 4 * i;
@@ -474,11 +480,11 @@ __global__ void __launch_bounds__(256)
             double sv = 0.0;
             if (c >= 0 && ql < nqc) {
                 const double *pc = psi + (long long)ql * nall + c;
-                const double wq = dirs[qq + 96];
-                const double fx = axis_flux_bf(dirs[qq], wq, theta, pc, sx);
-                const double fy = axis_flux_bf(dirs[qq + 32], wq, theta, pc, sy);
-                const double fz = axis_flux_bf(dirs[qq + 64], wq, theta, pc, sz);
-                sv = fx * rdx + fy * rdy + fz * rdz;
+                const double cx = dirs[qq], cy = dirs[qq + 32], cz = dirs[qq + 64];
+                const double fx = axis_flux_bf(cx, th2, pc, sx);
+                const double fy = axis_flux_bf(cy, th2, pc, sy);
+                const double fz = axis_flux_bf(cz, th2, pc, sz);
+                sv = fx * cx + fy * cy + fz * cz;
             }
             sS[qq * CS + cl] = sv;
         }
@@ -523,19 +529,18 @@ __device__ __forceinline__ double minmod3(double p, double q, double s)
     return same ? m : 0.0;
 }
 
-// The limited upwind difference along one axis of src/flux_kinetic.cpp:130-189 times om w,
-// from the four stencil values k1..k4 (offsets -2..1 with h = 1/2 for om > 0, -1..2 with
-// h = -1/2 otherwise): f = ((k3 + h s(k2,k3,k4)) - k2) - h s(k1,k2,k3), s = slopefit
-// (src/flux_kinetic.cpp:56-61); h s is exact, so the fused forms round as the reference's
-// expression.
-__device__ __forceinline__ double axis_flux_m3(double om, double w, double th, double h, double k1,
-                                               double k2, double k3, double k4)
+// The limited upwind difference along one axis of src/flux_kinetic.cpp:130-189 from the four
+// stencil values k1..k4 (offsets -2..1 with h = 1/2 for a positive cosine, -1..2 with h = -1/2
+// otherwise): f = ((k3 + h s(k2,k3,k4)) - k2) - h s(k1,k2,k3), s = slopefit
+// (src/flux_kinetic.cpp:56-61), evaluated as in axis_flux_bf: s' = 2 s from 2 th (th2) and
+// unscaled centred differences, q = h / 2, so f rounds as the reference's expression.
+__device__ __forceinline__ double axis_flux_m3(double q, double th2, double k1, double k2,
+                                               double k3, double k4)
 {
-    const double t32 = th * (k3 - k2);
-    const double s1 = minmod3(th * (k4 - k3), 0.5 * (k4 - k2), t32);
-    const double s2 = minmod3(t32, 0.5 * (k3 - k1), th * (k2 - k1));
-    const double f = fma(-h, s2, fma(h, s1, k3) - k2);
-    return f * om * w;
+    const double t32 = th2 * (k3 - k2);
+    const double s1 = minmod3(th2 * (k4 - k3), k4 - k2, t32);
+    const double s2 = minmod3(t32, k3 - k1, th2 * (k2 - k1));
+    return fma(-q, s2, fma(q, s1, k3) - k2);
 }
 
 // The kinetic flux of kinetic_dmma_kernel with psi staged in shared memory. A CTA owns one
@@ -563,14 +568,14 @@ constexpr int KRUN = 64;                    // longest cell run per CTA
 constexpr int KPER = (KRUN + 4) + 6 * KRUN;
 template <int NT> struct KinStage {
     static constexpr int FRAG = 2 * NT * 32;                    // two projection k-steps
-    static constexpr int DOUBLES = KDS * KPER + FRAG + 4 * KDS; // + xi, eta, mu, w of KDS dirs
+    static constexpr int DOUBLES = KDS * KPER + FRAG + 4 * KDS; // + c_x, c_y, c_z, w of KDS dirs
 };
 template <int NT>
 __global__ void __launch_bounds__(256, 3)
     kinetic_staged_kernel(GridDims g, const double *__restrict__ psi, const double *__restrict__ mfP,
                           const double *__restrict__ xiAll, const double *__restrict__ etaAll,
-                          int q0, int nqc, int L, double rdx, double rdy, double rdz, double theta,
-                          int accumulate, double *__restrict__ flux, int *errorFlag)
+                          int q0, int nqc, int L, double theta, int accumulate,
+                          double *__restrict__ flux, int *errorFlag)
 {
     constexpr int TILE = 8 * NT * 32 + 128; // one 32-direction tile of mfP
     constexpr int SD = KinStage<NT>::DOUBLES, FRAG = KinStage<NT>::FRAG;
@@ -579,6 +584,7 @@ __global__ void __launch_bounds__(256, 3)
     extern __shared__ __align__(128) double kinSmem[];
     __shared__ uint64_t pbar[2];
     __shared__ long long sRun[9];
+    const double th2 = 2.0 * theta;
     const int nm = g.nm;
     const long long nall = g.nall();
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -651,7 +657,7 @@ __global__ void __launch_bounds__(256, 3)
                 dst = st + KDS * KPER;
                 nb = FRAG * 8;
             } else {
-                src = tile + 8 * NT * 32 + 32 * (lane - 8) + KDS * v; // xi, eta, mu, w
+                src = tile + 8 * NT * 32 + 32 * (lane - 8) + KDS * v; // c_x, c_y, c_z, w
                 dst = st + KDS * KPER + FRAG + KDS * (lane - 8);
                 nb = KDS * 8;
             }
@@ -686,7 +692,7 @@ __global__ void __launch_bounds__(256, 3)
         // a timed-out wait is agreed on at the barrier after the stencil (the data of that
         // sub-stage are then not used)
         const bool ok = fbar_wait(&pbar[u & 1], (u >> 1) & 1);
-        const double *dirs = st + KDS * KPER + FRAG; // xi[KDS], eta[KDS], mu[KDS], w[KDS]
+        const double *dirs = st + KDS * KPER + FRAG; // c_x[KDS], c_y[KDS], c_z[KDS], w[KDS]
         double afr[2]; // the thread's own A fragments of the sub-stage's two k-steps
 #pragma unroll
         for (int r = 0; r < 2; ++r) {
@@ -698,22 +704,21 @@ __global__ void __launch_bounds__(256, 3)
             if (cl < L && ql < nqc) {
                 const double *P = st + d * KPER;
                 const double *xr = P + (L + 4), *yr = xr + 3 * L;
-                const double wq = dirs[3 * KDS + d];
                 const double c0 = P[cl + 2];
+                // the direction's weights c = cosine x w / spacing per axis
                 const double ox = dirs[d], oy = dirs[KDS + d], oz = dirs[2 * KDS + d];
                 // branch-free: the staged x and y slots hold offsets (-2, -1, +1) for a positive
                 // cosine and (-1, +1, +2) otherwise, so k1 and k4 always come from slots 0 and 2
                 // and the cell's own value is k3 or k2; the z run holds offsets -2 .. +2
                 const bool px = ox > 0, py = oy > 0, pz = oz > 0;
                 const double ax = xr[L + cl], ay = yr[L + cl];
-                const double fx = axis_flux_m3(ox, wq, theta, px ? 0.5 : -0.5, xr[cl], px ? ax : c0,
+                const double fx = axis_flux_m3(px ? 0.25 : -0.25, th2, xr[cl], px ? ax : c0,
                                                px ? c0 : ax, xr[2 * L + cl]);
-                const double fy = axis_flux_m3(oy, wq, theta, py ? 0.5 : -0.5, yr[cl], py ? ay : c0,
+                const double fy = axis_flux_m3(py ? 0.25 : -0.25, th2, yr[cl], py ? ay : c0,
                                                py ? c0 : ay, yr[2 * L + cl]);
                 const double *zb = P + cl + (pz ? 0 : 1);
-                const double fz = axis_flux_m3(oz, wq, theta, pz ? 0.5 : -0.5, zb[0], zb[1], zb[2],
-                                               zb[3]);
-                sv = fx * rdx + fy * rdy + fz * rdz;
+                const double fz = axis_flux_m3(pz ? 0.25 : -0.25, th2, zb[0], zb[1], zb[2], zb[3]);
+                sv = fx * ox + fy * oy + fz * oz;
             }
             afr[r] = sv;
         }
@@ -1036,7 +1041,8 @@ size_t flux_frag_doubles(int nm, int nq, int which)
 }
 
 void flux_frags(int nm, int nq, const double *M, const double *w, const double *xi,
-                const double *eta, const double *mu, double *mfA, double *mfP)
+                const double *eta, const double *mu, double rdx, double rdy, double rdz,
+                double *mfA, double *mfP)
 {
     const int NT = (nm + 7) / 8, KS = 2 * NT, nt = (nq + 31) / 32;
     auto m = [&](int q, int k) { return (q < nq && k < nm) ? M[(size_t)q * nm + k] : 0.0; };
@@ -1054,9 +1060,9 @@ void flux_frags(int nm, int nq, const double *M, const double *w, const double *
         double *D = P + 8 * NT * 32;
         for (int qq = 0; qq < 32; ++qq) {
             int q = 32 * t + qq;
-            D[qq] = q < nq ? xi[q] : 0.0;
-            D[32 + qq] = q < nq ? eta[q] : 0.0;
-            D[64 + qq] = q < nq ? mu[q] : 0.0;
+            D[qq] = q < nq ? (xi[q] * w[q]) * rdx : 0.0;
+            D[32 + qq] = q < nq ? (eta[q] * w[q]) * rdy : 0.0;
+            D[64 + qq] = q < nq ? (mu[q] * w[q]) * rdz : 0.0;
             D[96 + qq] = q < nq ? w[q] : 0.0;
         }
     }
@@ -1065,9 +1071,8 @@ void flux_frags(int nm, int nq, const double *M, const double *w, const double *
 template <int NT>
 static cudaError_t kinetic_t(const GridDims &g, const double *alpha, const double *mfA,
                              const double *mfP, const double *xi, const double *eta, int nq,
-                             int qChunk, int runLen, double dx, double dy, double dz,
-                             double theta, int isPn, double *psi, bool psiReady, double *flux,
-                             int *errorFlag, cudaStream_t st)
+                             int qChunk, int runLen, double theta, int isPn, double *psi,
+                             bool psiReady, double *flux, int *errorFlag, cudaStream_t st)
 {
     if (psiReady)
         qChunk = nq; // psi of every direction is in place: the stencil alone, in one pass
@@ -1087,8 +1092,7 @@ static cudaError_t kinetic_t(const GridDims &g, const double *alpha, const doubl
             if (e != cudaSuccess)
                 return e;
             kern<<<(unsigned)((long long)g.nx * g.ny * (g.nz / L)), 256, smem, st>>>(
-                    g, psi, mfP, xi, eta, q0, nqc, L, 1.0 / dx, 1.0 / dy, 1.0 / dz, theta,
-                    q0 > 0 ? 1 : 0, flux, errorFlag);
+                    g, psi, mfP, xi, eta, q0, nqc, L, theta, q0 > 0 ? 1 : 0, flux, errorFlag);
             e = cudaGetLastError();
             if (e != cudaSuccess)
                 return e;
@@ -1104,8 +1108,7 @@ static cudaError_t kinetic_t(const GridDims &g, const double *alpha, const doubl
                 return e;
         }
         kinetic_dmma_kernel<NT><<<(unsigned)((g.ninterior() + 63) / 64), 256, kinSmem, st>>>(
-            g, psi, mfP, q0, nqc, 1.0 / dx, 1.0 / dy, 1.0 / dz, theta, q0 > 0 ? 1 : 0, flux,
-            errorFlag);
+            g, psi, mfP, q0, nqc, theta, q0 > 0 ? 1 : 0, flux, errorFlag);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess)
             return e;
@@ -1118,16 +1121,15 @@ static cudaError_t kinetic_t(const GridDims &g, const double *alpha, const doubl
 // closure), so only the stencil and projection run.
 cudaError_t launch_kinetic_flux(const GridDims &g, const double *alpha, const double *mfA,
                                 const double *mfP, const double *xi, const double *eta, int nq,
-                                int qChunk, int runLen, double dx, double dy, double dz,
-                                double theta, int isPn, double *psi, bool psiReady, double *flux,
-                                int *errorFlag, cudaStream_t st)
+                                int qChunk, int runLen, double theta, int isPn, double *psi,
+                                bool psiReady, double *flux, int *errorFlag, cudaStream_t st)
 {
     if (qChunk < nq && (qChunk & 31))
         return cudaErrorInvalidValue;
 #define C3D_NT_CASE(NT)                                                                            \
     case NT:                                                                                       \
-        return kinetic_t<NT>(g, alpha, mfA, mfP, xi, eta, nq, qChunk, runLen, dx, dy, dz, theta, \
-                             isPn, psi, psiReady, flux, errorFlag, st);
+        return kinetic_t<NT>(g, alpha, mfA, mfP, xi, eta, nq, qChunk, runLen, theta, isPn, psi,  \
+                             psiReady, flux, errorFlag, st);
     switch ((g.nm + 7) / 8) {
         C3D_NT_CASE(1)
         C3D_NT_CASE(2)
