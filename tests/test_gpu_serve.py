@@ -49,8 +49,13 @@ def test_results_alone_and_in_the_mix(tmp_path):
         assert np.array_equal(u, ua)
         lat.append(latency)
     _, peak = srv.stats()
+    sched = srv.timing()
     srv.close()
-    assert peak >= 2  # the problems overlapped on the device
+    assert peak >= 2  # the problems were active together, stepped in shared passes
+    # every problem stepped through the scheduler's passes, and the group was rebuilt as
+    # problems came and went
+    assert sched["passes"] >= max(n for _, n in alone) and sched["group_builds"] >= 2
+    assert sched["wait_s"] > 0 and min(sched.values()) >= 0, sched
     print("latency p50 %.3f s  p99 %.3f s" % (np.percentile(lat, 50), np.percentile(lat, 99)))
 
 

@@ -128,6 +128,8 @@ def test_two_slabs_on_one_gpu_equal_single_domain(oracle, overlap):
     sig = S["sig"].reshape(n + 4, n + 4, n + 4)
     g = c3d.Context(nx=n, ny=n, nz=n, **kw)
     g.set_state(u=S["u"], alpha=S["alpha"], sig_t=S["sig"], sig_s=S["sig"])
+    with pytest.raises(c3d.C3DError, match="slab"):
+        g.stage_part(0, S["dt"], 0)  # the split stage belongs to slab contexts
     ctxs, halos, bounds = [], [], []
     for r in range(2):
         x0, nl = c3d_slabs.slab_bounds(n, 2, r)
