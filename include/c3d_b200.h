@@ -320,8 +320,9 @@ c3d_status c3d_closure_vectors(c3d_ctx *ctx, long long n, double *u, double *alp
  * n[k] vectors at u[k], alpha[k] (device, solved in place), records iters/iterGamma/regIndex/
  * status[k] as in c3d_closure_vectors (each array of pointers, or an entry of one, may be
  * NULL). Results are those of calling c3d_closure_vectors per context, bit for bit. Errors
- * (failed cells, round limit) are reported per context by c3d_sync. No counterpart in the
- * reference, whose closure works one batch of one order at a time. */
+ * (failed cells, round limit) are reported per context by c3d_sync. The group refers to its
+ * contexts: destroy it before any of them. No counterpart in the reference, whose closure
+ * works one batch of one order at a time. */
 typedef struct c3d_group c3d_group;
 c3d_status c3d_group_create(int count, c3d_ctx *const *ctx, c3d_group **out);
 c3d_status c3d_group_closure_vectors(c3d_group *group, const long long *n, double *const *u,
