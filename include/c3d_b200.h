@@ -12,8 +12,9 @@
  * 2. The device-resident step API that the C++ host (c3d-2015_b200/host) uses
  *    to run update() (src/update.cpp:185-275) on one GPU: state stays in HBM
  *    across stages and steps, the MPI halo exchange (src/comm.cpp) is an
- *    on-device periodic ghost fill, and the closure is a persistent
- *    work-queue kernel. Every function returns a c3d_status; none aborts.
+ *    on-device periodic ghost fill, and the closure runs as work-list rounds in a
+ *    device-side graph loop (or as persistent work-queue kernels). Every function
+ *    returns a c3d_status; none aborts.
  *
  * Arrays use the reference's layouts: per-cell moment vectors with the moment
  * index fastest (IU, src/global.h:16), cells over the grid including two ghost
