@@ -53,8 +53,9 @@ cudaError_t launch_rk(const GridDims &g, double *u, double *uOld, int mode, int 
 cudaError_t launch_kinetic_flux(const GridDims &g, const double *alpha, const double *mfA,
                                 const double *mfP, const double *xi, const double *eta, int nq,
                                 int qChunk, int runLen, double theta, int isPn, double *psi,
-                                bool psiReady, double *flux,
-                                int *errorFlag, cudaStream_t st);
+                                bool psiReady, double *flux, int *errorFlag,
+                                const int *wrapFlag, cudaStream_t st);
+bool kinetic_staged_used(const GridDims &g, int runLen);
 cudaError_t launch_psi_handoff(const GridDims &g, int nq, const double *M, const double *alpha,
                                bool faceCopy, const int *refresh, const unsigned int *refreshCount,
                                double *psi, int numSMs, cudaStream_t st);
@@ -1370,8 +1371,8 @@ c3d_status c3d_flux_kinetic(c3d_ctx *c, int alphaIsU)
     cudaEvent_t t0 = nullptr;
     timing_begin(c, &t0);
     C3D_CUDA(launch_kinetic_flux(c->g, a, c->mfA, c->mfP, c->xi, c->eta, c->nq, c->qChunk,
-                                 c->runLen, c->theta, isPn, c->psi, ready,
-                                 c->flux, c->errorFlag, c->stream));
+                                 c->runLen, c->theta, isPn, c->psi, ready, c->flux,
+                                 c->errorFlag, nullptr, c->stream));
     timing_end(c, 1, t0);
     int nch = ceil_div(c->nq, c->qChunk);
     c->launches += ready ? 1 : 2 * nch;
@@ -1566,6 +1567,10 @@ static cudaError_t stage_capture(c3d_ctx *c, int stage, double dt, bool handoff,
                                  cudaStream_t *cs, long long *launches)
 {
     const bool mirrorPath = c->mirror && !c->xHaloExternal;
+    // mirrored closure with the hand-off and the staged stencil: the face ghosts' psi is not
+    // copied; the stencil reads their periodic images (the mirror flag tells it, on the device,
+    // which closure body ran)
+    const bool wrap = mirrorPath && handoff && kinetic_staged_used(c->g, c->runLen);
     const long long l0 = c->launches;
     long long n = 0;
     cudaStream_t s0 = cs[0];
@@ -1606,7 +1611,7 @@ static cudaError_t stage_capture(c3d_ctx *c, int stage, double dt, bool handoff,
                                         c->stats, c->numSMs, sk);
         }
         if (er == cudaSuccess && R.psi)
-            er = launch_psi_handoff(c->g, c->nq, c->M, c->alpha, mirrored, c->psiRefresh,
+            er = launch_psi_handoff(c->g, c->nq, c->M, c->alpha, mirrored && !wrap, c->psiRefresh,
                                     c->psiRefreshCount, c->psi, c->numSMs, sk);
         return er;
     };
@@ -1641,13 +1646,13 @@ static cudaError_t stage_capture(c3d_ctx *c, int stage, double dt, bool handoff,
     }
     if (ec == cudaSuccess)
         ec = launch_kinetic_flux(c->g, c->alpha, c->mfA, c->mfP, c->xi, c->eta, c->nq, c->qChunk,
-                                 c->runLen, c->theta, 0, c->psi, handoff,
-                                 c->flux, c->errorFlag, s0);
+                                 c->runLen, c->theta, 0, c->psi, handoff, c->flux, c->errorFlag,
+                                 wrap ? c->mirrorFlag : nullptr, s0);
     if (ec == cudaSuccess)
         ec = launch_euler(c->g, c->u, c->flux, c->sigT, c->sigS, dt, c->numSMs, s0);
     if (ec == cudaSuccess && stage == 1)
         ec = launch_rk(c->g, c->u, c->uOld, 1, c->numSMs, s0);
-    n += (handoff ? 1 + 2 : 2 * ceil_div(c->nq, c->qChunk)) + 1 + (stage == 1);
+    n += (handoff ? 1 + (wrap ? 1 : 2) : 2 * ceil_div(c->nq, c->qChunk)) + 1 + (stage == 1);
     *launches = n + (c->launches - l0); // the closure counted its round 0
     c->launches = l0;
     return ec;

@@ -575,7 +575,7 @@ __global__ void __launch_bounds__(256, 3)
     kinetic_staged_kernel(GridDims g, const double *__restrict__ psi, const double *__restrict__ mfP,
                           const double *__restrict__ xiAll, const double *__restrict__ etaAll,
                           int q0, int nqc, int L, double theta, int accumulate,
-                          double *__restrict__ flux, int *errorFlag)
+                          double *__restrict__ flux, int *errorFlag, const int *wrapFlag)
 {
     constexpr int TILE = 8 * NT * 32 + 128; // one 32-direction tile of mfP
     constexpr int SD = KinStage<NT>::DOUBLES, FRAG = KinStage<NT>::FRAG;
@@ -610,9 +610,17 @@ __global__ void __launch_bounds__(256, 3)
     const int t0 = q0 >> 5, nu = (nqc + KDS - 1) / KDS;
     // start cell of run r: 0 the cell run with its z halo, 1-4 x offsets -2, -1, +1, +2,
     // 5-8 y offsets -2, -1, +1, +2
+    // wrap (the closure copied the face ghosts from their periodic images and their psi was
+    // not copied): stencil values of face ghosts are read at the images instead -- the x and
+    // y neighbour lines of the periodic grid, and the z halo pairs of runs at either end
+    const bool wrap = wrapFlag && *wrapFlag == 0;
+    const bool lowB = wrap && k0 == 2, highB = wrap && k0 + L == g.nz + 2;
     if (tid < 9) {
         const int r = tid, o = (r - 1) & 3, d = o < 2 ? o - 2 : o - 1;
-        sRun[r] = r == 0 ? g.cell(i, j, k0 - 2) : r <= 4 ? g.cell(i + d, j, k0) : g.cell(i, j + d, k0);
+        auto per = [&](int a, int n) { return !wrap ? a : a < 2 ? a + n : a >= n + 2 ? a - n : a; };
+        sRun[r] = r == 0    ? g.cell(i, j, k0 - 2)
+                  : r <= 4 ? g.cell(per(i + d, g.nx), j, k0)
+                           : g.cell(i, per(j + d, g.ny), k0);
     }
     const uint32_t perDir = (uint32_t)((L + 4) + 6 * L) * 8;
     // a direction's stage: the cell run, then x slots 0-2, then y slots 0-2 (offsets -2, -1,
@@ -648,6 +656,19 @@ __global__ void __launch_bounds__(256, 3)
             src = psi + (long long)ql * nall + sRun[r];
             dst = st + d * KPER + off;
             nb = (uint32_t)(r == 0 ? L + 4 : L) * 8;
+            if (r == 0 && (lowB || highB)) {
+                // the run without the halo pairs that lanes 12 and 13 bring from the images
+                src += lowB ? 2 : 0;
+                dst += lowB ? 2 : 0;
+                nb -= (uint32_t)(2 * lowB + 2 * highB) * 8;
+            }
+        } else if (d < nd && ((lane == 12 && lowB) || (lane == 13 && highB))) {
+            // z halo pair of a run at the low end (ghosts k = 0, 1 = images nz, nz + 1) or the
+            // high end (k = nz + 2, nz + 3 = images 2, 3); 16-byte aligned: nz and L are even
+            const int ql = KDS * u + d;
+            src = psi + (long long)ql * nall + g.cell(i, j, lane == 12 ? g.nz : 2);
+            dst = st + d * KPER + (lane == 12 ? 0 : L + 2);
+            nb = 16;
         } else if (d == 0 && lane >= 7 && lane <= 11) {
             const int ql = KDS * u;
             const double *tile = mfP + (size_t)(t0 + (ql >> 5)) * TILE;
@@ -1072,7 +1093,8 @@ template <int NT>
 static cudaError_t kinetic_t(const GridDims &g, const double *alpha, const double *mfA,
                              const double *mfP, const double *xi, const double *eta, int nq,
                              int qChunk, int runLen, double theta, int isPn, double *psi,
-                             bool psiReady, double *flux, int *errorFlag, cudaStream_t st)
+                             bool psiReady, double *flux, int *errorFlag, const int *wrapFlag,
+                             cudaStream_t st)
 {
     if (psiReady)
         qChunk = nq; // psi of every direction is in place: the stencil alone, in one pass
@@ -1092,12 +1114,15 @@ static cudaError_t kinetic_t(const GridDims &g, const double *alpha, const doubl
             if (e != cudaSuccess)
                 return e;
             kern<<<(unsigned)((long long)g.nx * g.ny * (g.nz / L)), 256, smem, st>>>(
-                    g, psi, mfP, xi, eta, q0, nqc, L, theta, q0 > 0 ? 1 : 0, flux, errorFlag);
+                    g, psi, mfP, xi, eta, q0, nqc, L, theta, q0 > 0 ? 1 : 0, flux, errorFlag,
+                    wrapFlag);
             e = cudaGetLastError();
             if (e != cudaSuccess)
                 return e;
             continue;
         }
+        if (wrapFlag) // the global-load form reads the face ghosts themselves
+            return cudaErrorInvalidValue;
         const size_t kinSmem = (size_t)(FLUX_STAGES * (8 * NT * 32 + 128) + 32 * 68) * 8;
         // opt in above the 48 KB default for the dynamic part plus the ~1.3 KB static part
         if (kinSmem > 46 * 1024) {
@@ -1119,17 +1144,26 @@ static cudaError_t kinetic_t(const GridDims &g, const double *alpha, const doubl
 // qChunk: a multiple of 32 unless it covers all of nq.
 // psiReady: psi[q nall + c] already holds the ansatz of every direction (handed off by the
 // closure), so only the stencil and projection run.
+// wrapFlag (staged stencil only, else null): a device flag; when it reads 0 the face ghosts'
+// psi is not in place and their stencil values are read at their periodic images.
+bool kinetic_staged_used(const GridDims &g, int runLen)
+{
+    const int L = runLen > 0 ? runLen : (g.nz < KRUN ? g.nz : KRUN);
+    return L % 2 == 0 && L <= KRUN && g.nz % L == 0;
+}
+
 cudaError_t launch_kinetic_flux(const GridDims &g, const double *alpha, const double *mfA,
                                 const double *mfP, const double *xi, const double *eta, int nq,
                                 int qChunk, int runLen, double theta, int isPn, double *psi,
-                                bool psiReady, double *flux, int *errorFlag, cudaStream_t st)
+                                bool psiReady, double *flux, int *errorFlag, const int *wrapFlag,
+                                cudaStream_t st)
 {
     if (qChunk < nq && (qChunk & 31))
         return cudaErrorInvalidValue;
 #define C3D_NT_CASE(NT)                                                                            \
     case NT:                                                                                       \
         return kinetic_t<NT>(g, alpha, mfA, mfP, xi, eta, nq, qChunk, runLen, theta, isPn, psi,  \
-                             psiReady, flux, errorFlag, st);
+                             psiReady, flux, errorFlag, wrapFlag, st);
     switch ((g.nm + 7) / 8) {
         C3D_NT_CASE(1)
         C3D_NT_CASE(2)
