@@ -58,7 +58,7 @@ cudaError_t launch_kinetic_flux(const GridDims &g, const double *alpha, const do
 bool kinetic_staged_used(const GridDims &g, int runLen);
 cudaError_t launch_psi_handoff(const GridDims &g, int nq, const double *M, const double *alpha,
                                bool faceCopy, const int *refresh, const unsigned int *refreshCount,
-                               double *psi, int numSMs, cudaStream_t st);
+                               double *psi, int *psiValid, int numSMs, cudaStream_t st);
 size_t flux_frag_doubles(int nm, int nq, int which);
 cudaError_t launch_reproject(const GridDims &g, double *u, double *alpha, const double *mfA,
                              const double *mfP, int nq, int *errorFlag, cudaStream_t st);
@@ -148,6 +148,9 @@ struct c3d_ctx {
     bool handoff = true;                // c3d_set_ansatz_handoff
     int *psiRefresh = nullptr;          // cells whose psi is rewritten after the closure
     unsigned int *psiRefreshCount = nullptr;
+    // device flag: psi holds the ansatz of every cell but the face ghosts for the current
+    // multipliers (set by a closure's hand-off, cleared by whatever may break that)
+    int *psiValid = nullptr;
     long long launches = 0;
     long long hostSyncs = 0; // host waits inside the stages (c3d_closure_stats.hostSyncs)
     // device buffers
@@ -263,7 +266,7 @@ static void free_ctx(c3d_ctx *c)
                     c->rCounts, c->rBuf, c->mfA, c->mfP, c->cellMap, c->mirrorFlag,
                     c->gChunksC, c->cellGamma, c->cellErr, c->lineLog, c->mixF64,
                     c->mixA[0], c->mixA[1], c->cellCond, c->g0, c->psiRefresh,
-                    c->psiRefreshCount, c->xSplit[0], c->xSplit[1]};
+                    c->psiRefreshCount, c->xSplit[0], c->xSplit[1], c->psiValid};
     for (void *p : ptrs)
         if (p)
             cudaFree(p);
@@ -285,6 +288,13 @@ static void free_ctx(c3d_ctx *c)
     if (c->ownStream && c->stream)
         cudaStreamDestroy(c->stream);
     delete c;
+}
+
+// psi no longer matches the multipliers (or may not): the next hand-off closure writes all of it.
+static void psi_invalidate(c3d_ctx *c)
+{
+    if (c->psiValid)
+        cudaMemsetAsync(c->psiValid, 0, sizeof(int), c->stream);
 }
 
 extern "C" {
@@ -435,10 +445,12 @@ void c3d_destroy(c3d_ctx *ctx)
 c3d_status c3d_set_state(c3d_ctx *c, const double *u, const double *alpha, const double *sigT,
                          const double *sigS, int where)
 {
-    if (c && alpha)
-        c->psiReady = false;
     if (!c)
         return fail(C3D_ERR_INVALID, "c3d_set_state: null context");
+    if (alpha) {
+        c->psiReady = false;
+        psi_invalidate(c);
+    }
     const long long nall = c->g.nall();
     const size_t vb = nall * c->g.nm * 8, sb = nall * 8;
     cudaMemcpyKind k = where ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
@@ -613,6 +625,12 @@ static c3d_status rounds_setup(c3d_ctx *c, long long n, double *u, double *alpha
             // budget
             const size_t need = (size_t)c->nq * c->g.nall() * 8;
             if (need <= c->psiBytes) {
+                if (!c->psiRefresh) {
+                    C3D_CUDA(cudaMalloc(&c->psiRefresh, (size_t)c->g.nall() * sizeof(int)));
+                    C3D_CUDA(cudaMalloc(&c->psiRefreshCount, sizeof(unsigned int)));
+                    C3D_CUDA(cudaMalloc(&c->psiValid, sizeof(int)));
+                    C3D_CUDA(cudaMemset(c->psiValid, 0, sizeof(int)));
+                }
                 if (!c->psi || c->psiAlloc < need) {
                     if (c->psi)
                         cudaFree(c->psi);
@@ -620,16 +638,17 @@ static c3d_status rounds_setup(c3d_ctx *c, long long n, double *u, double *alpha
                     c->psiAlloc = 0;
                     C3D_CUDA(cudaMalloc(&c->psi, need));
                     c->psiAlloc = need;
-                }
-                if (!c->psiRefresh) {
-                    C3D_CUDA(cudaMalloc(&c->psiRefresh, (size_t)c->g.nall() * sizeof(int)));
-                    C3D_CUDA(cudaMalloc(&c->psiRefreshCount, sizeof(unsigned int)));
+                    C3D_CUDA(cudaMemset(c->psiValid, 0, sizeof(int)));
                 }
                 C3D_CUDA(cudaMemsetAsync(c->psiRefreshCount, 0, sizeof(unsigned int), st));
                 R.psi = c->psi;
                 R.psiNall = c->g.nall();
                 R.refresh = c->psiRefresh;
                 R.refreshCount = c->psiRefreshCount;
+                R.psiValid = c->psiValid;
+                R.gnx = c->g.nx;
+                R.gny = c->g.ny;
+                R.gnz = c->g.nz;
             }
         }
         R.stream = st;
@@ -650,6 +669,8 @@ static c3d_status run_closure(c3d_ctx *c, long long n, double *u, double *alpha,
         if (s != C3D_OK)
             return s;
         c->psiReady = false;
+        if (gridRecords && !R.psi)
+            psi_invalidate(c);
         cudaError_t e = launch_closure_rounds(R, c->gaunt);
         if (e == cudaErrorLaunchTimeout)
             return fail(C3D_ERR_TIMEOUT, "closure: round limit exceeded");
@@ -659,6 +680,8 @@ static c3d_status run_closure(c3d_ctx *c, long long n, double *u, double *alpha,
         return C3D_OK;
     }
     c->cp.probe = 0; // the persistent kernels always form H
+    if (gridRecords)
+        psi_invalidate(c);
     ClosureLaunch L{};
     L.P = &c->cp;
     L.chunks = c->chunks;
@@ -713,6 +736,7 @@ c3d_status c3d_closure(c3d_ctx *c)
         C3D_CUDA(launch_reproject(c->g, c->u, c->alpha, c->mfA, c->mfP, c->nq, c->errorFlag,
                                   c->stream));
         c->launches += 1;
+        psi_invalidate(c); // alpha_0 moved
     }
     timing_end(c, 0, t0);
     return C3D_OK;
@@ -727,7 +751,7 @@ static c3d_status finish_handoff(c3d_ctx *c, bool faceCopy)
         return C3D_OK;
     c->psiHandoffPending = false;
     C3D_CUDA(launch_psi_handoff(c->g, c->nq, c->M, c->alpha, faceCopy, c->psiRefresh,
-                                c->psiRefreshCount, c->psi, c->numSMs, c->stream));
+                                c->psiRefreshCount, c->psi, c->psiValid, c->numSMs, c->stream));
     c->launches += faceCopy ? 2 : 1;
     c->psiReady = true;
     return C3D_OK;
@@ -938,6 +962,7 @@ c3d_status c3d_set_gaunt(c3d_ctx *c, int nm2, const double *M2, const int *rowPt
 {
     if (!c)
         return fail(C3D_ERR_INVALID, "c3d_set_gaunt: null context");
+    psi_invalidate(c); // the closure may no longer hand its ansatz over
     if (!M2 || !rowPtr || !colInd || !val) {
         // back to the direct form (FP64: the mixed closure needs the Gaunt form)
         c->gaunt = false;
@@ -1082,6 +1107,7 @@ c3d_status c3d_set_precision(c3d_ctx *c, int mode, double condBf16, double condM
 {
     if (!c || mode < 0 || mode > 1)
         return fail(C3D_ERR_INVALID, "c3d_set_precision: mode must be 0 (FP64) or 1 (mixed)");
+    psi_invalidate(c); // the closure may no longer hand its ansatz over
     if (mode == 1 && (!c->gaunt || c->engine != 0))
         return fail(C3D_ERR_INVALID,
                     "c3d_set_precision: the mixed closure needs the Gaunt form and engine 0");
@@ -1101,6 +1127,7 @@ c3d_status c3d_set_certificate(c3d_ctx *c, int on)
 {
     if (!c)
         return fail(C3D_ERR_INVALID, "c3d_set_certificate: null context");
+    psi_invalidate(c); // the closure may no longer hand its ansatz over
     c->certificate = on != 0;
     return C3D_OK;
 }
@@ -1109,6 +1136,7 @@ c3d_status c3d_set_engine(c3d_ctx *c, int engine)
 {
     if (!c || engine < 0 || engine > 1)
         return fail(C3D_ERR_INVALID, "c3d_set_engine: engine must be 0 (work list) or 1 (persistent)");
+    psi_invalidate(c); // the closure may no longer hand its ansatz over
     c->engine = engine;
     if (engine != 0)
         c->cp.mixed = 0; // the persistent kernels are FP64 only
@@ -1127,6 +1155,7 @@ c3d_status c3d_set_ansatz_handoff(c3d_ctx *c, int on)
 {
     if (!c)
         return fail(C3D_ERR_INVALID, "c3d_set_ansatz_handoff: null context");
+    psi_invalidate(c); // the closure may no longer hand its ansatz over
     c->handoff = on != 0;
     if (!c->handoff)
         c->psiReady = false;
@@ -1368,6 +1397,8 @@ c3d_status c3d_flux_kinetic(c3d_ctx *c, int alphaIsU)
     const bool ready = c->psiReady && !alphaIsU && isPn == 0 &&
                        c->psiAlloc >= (size_t)c->nq * c->g.nall() * 8;
     c->psiReady = false;
+    if (!ready)
+        psi_invalidate(c); // the ansatz kernel writes psi
     cudaEvent_t t0 = nullptr;
     timing_begin(c, &t0);
     C3D_CUDA(launch_kinetic_flux(c->g, a, c->mfA, c->mfP, c->xi, c->eta, c->nq, c->qChunk,
@@ -1612,7 +1643,7 @@ static cudaError_t stage_capture(c3d_ctx *c, int stage, double dt, bool handoff,
         }
         if (er == cudaSuccess && R.psi)
             er = launch_psi_handoff(c->g, c->nq, c->M, c->alpha, mirrored && !wrap, c->psiRefresh,
-                                    c->psiRefreshCount, c->psi, c->numSMs, sk);
+                                    c->psiRefreshCount, c->psi, c->psiValid, c->numSMs, sk);
         return er;
     };
     if (ec == cudaSuccess && mirrorPath) {
@@ -1644,6 +1675,8 @@ static cudaError_t stage_capture(c3d_ctx *c, int stage, double dt, bool handoff,
     } else if (ec == cudaSuccess) {
         ec = closure(false, 0);
     }
+    if (ec == cudaSuccess && !handoff && c->psiValid) // the ansatz kernel writes psi
+        ec = cudaMemsetAsync(c->psiValid, 0, sizeof(int), s0);
     if (ec == cudaSuccess)
         ec = launch_kinetic_flux(c->g, c->alpha, c->mfA, c->mfP, c->xi, c->eta, c->nq, c->qChunk,
                                  c->runLen, c->theta, 0, c->psi, handoff, c->flux, c->errorFlag,
@@ -1929,6 +1962,7 @@ c3d_status c3d_stage_part(c3d_ctx *c, int stage, double dt, int part)
             C3D_CUDA(launch_reproject(c->g, c->u, c->alpha, c->mfA, c->mfP, c->nq, c->errorFlag,
                                       c->stream));
             c->launches += 1;
+            psi_invalidate(c); // alpha_0 moved
         }
     }
     timing_end(c, 0, t0);
@@ -1968,8 +2002,10 @@ c3d_status c3d_copy_x_planes(c3d_ctx *c, int field, int i0, int count, void *buf
         return fail(C3D_ERR_INVALID, "c3d_copy_x_planes: bad argument");
     const size_t plane = (size_t)c->g.nyg() * c->g.nzg() * c->g.nm;
     double *a = (field == 0 ? c->u : c->alpha) + (size_t)i0 * plane;
-    if (field == 1 && !toBuf)
+    if (field == 1 && !toBuf) {
         c->psiReady = false;
+        psi_invalidate(c);
+    }
     const size_t bytes = (size_t)count * plane * sizeof(double);
     cudaMemcpyKind k = where ? cudaMemcpyDeviceToDevice
                              : (toBuf ? cudaMemcpyDeviceToHost : cudaMemcpyHostToDevice);
@@ -2038,6 +2074,7 @@ c3d_status c3d_line_stats_enable(c3d_ctx *c, int maxClosures)
 {
     if (!c || maxClosures < 0)
         return fail(C3D_ERR_INVALID, "c3d_line_stats_enable: bad argument");
+    psi_invalidate(c); // the closure may no longer hand its ansatz over
     if (c->lineLog) {
         cudaFree(c->lineLog);
         c->lineLog = nullptr;

@@ -501,6 +501,11 @@ struct FirstRound {
     long long nall;
     int *refresh;
     unsigned int *refreshCount;
+    // nonzero: psi already holds the ansatz of every cell but the face ghosts for the closure's
+    // starting multipliers (the previous closure's final ones), so the probe writes only the
+    // face ghosts' (gnx, gny, gnz: the interior sizes that tell them)
+    const int *psiValid;
+    int gnx, gny, gnz;
 };
 constexpr int PSTR = 17; // row stride (cells) of the probe's psi tile
 template <int NT, int NT2, int KIND, bool ZD>
@@ -545,6 +550,7 @@ __global__ void __launch_bounds__(RW * 32, KIND == 1 ? 1 : KIND == 2 ? 3 : 2)
     // psi = u_0 e^{alpha_scaled . m_q} (the scaling shifts alpha_0 by log(u_0) 2 sqrt(pi), and
     // m_0 = 1 / (2 sqrt(pi)))
     const bool emit = KIND == 2 && !list && first.psi != nullptr;
+    const bool valid = emit && first.psiValid && *first.psiValid != 0;
     long long cell[2];
     double scale[2], u0e[2] = {0.0, 0.0};
 #pragma unroll
@@ -559,8 +565,18 @@ __global__ void __launch_bounds__(RW * 32, KIND == 1 ? 1 : KIND == 2 ? 3 : 2)
             ascale = log(u0e[e]) * 2.0 * sqrt(M_PI);
         }
         if constexpr (KIND == 2)
-            if (lane == 0)
-                psiCell[2 * warp + e] = emit ? gc : -1;
+            if (lane == 0) {
+                bool need = emit;
+                if (valid && gc >= 0) {
+                    // only a face ghost's psi may be missing (its image's was read instead)
+                    const int gz = first.gnz + 4, gy = first.gny + 4;
+                    const int k = (int)(gc % gz), j = (int)((gc / gz) % gy), i = (int)(gc / gz / gy);
+                    const int in = (i >= 2 && i < first.gnx + 2) + (j >= 2 && j < first.gny + 2) +
+                                   (k >= 2 && k < first.gnz + 2);
+                    need = in == 2;
+                }
+                psiCell[2 * warp + e] = need ? gc : -1;
+            }
         for (int i = lane; i < nm; i += 32) {
             double a = 0.0;
             if (cell[e] >= 0) {
@@ -1365,8 +1381,9 @@ template <int NT, int NT2, bool GAUNT> static cudaError_t rounds_t(const RoundsL
             if constexpr (GAUNT) {
                 for (long long off = 0; off < R.ncells; off += R.batch) {
                     const int nb = (int)((R.ncells - off) < R.batch ? (R.ncells - off) : R.batch);
-                    const FirstRound fr{off,    R.cellMap, R.u,       R.alpha,
-                                        R.psi,  R.psiNall, R.refresh, R.refreshCount};
+                    const FirstRound fr{off,       R.cellMap,      R.u,      R.alpha,
+                                        R.psi,     R.psiNall,      R.refresh, R.refreshCount,
+                                        R.psiValid, R.gnx,         R.gny,    R.gnz};
                     const unsigned grid = (unsigned)((nb + MXC - 1) / MXC);
                     if (mixed)
                         rounds_pass_mixed_kernel<NT, NT2, 2, true><<<grid, RW * 32, mixSmem[2], s>>>(

@@ -892,12 +892,16 @@ cudaError_t launch_ghost_mirror_check(const GridDims &g, const double *a, int *f
 
 // The refresh comes first: a face ghost copies its image's final psi, and the image may be
 // one of the refreshed cells.
+// psiValid (may be null): set once psi holds every non-face-ghost cell's ansatz for the final
+// multipliers, so that the next closure's probe pass need not write it again.
 cudaError_t launch_psi_handoff(const GridDims &g, int nq, const double *M, const double *alpha,
                                bool faceCopy, const int *refresh, const unsigned int *refreshCount,
-                               double *psi, int numSMs, cudaStream_t st)
+                               double *psi, int *psiValid, int numSMs, cudaStream_t st)
 {
     psi_refresh_kernel<<<2 * numSMs, 256, 0, st>>>(g, nq, M, alpha, refresh, refreshCount, psi);
     cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess && psiValid)
+        e = cudaMemsetAsync(psiValid, 1, sizeof(int), st);
     if (e != cudaSuccess || !faceCopy)
         return e;
     constexpr int QPER = 64;

@@ -49,6 +49,10 @@ struct RoundsLaunch {
     long long psiNall;
     int *refresh;
     unsigned int *refreshCount;
+    // device flag: psi holds every non-face-ghost cell's ansatz for the starting multipliers
+    // (the probe then writes only face ghosts); gnx..gnz the grid's interior sizes
+    const int *psiValid;
+    int gnx, gny, gnz;
     // graph-resident round loop (rounds_graph_new; null: host-driven rounds) and the device
     // counter of the kernels its loop launches
     void *graphs;
