@@ -508,6 +508,22 @@ struct FirstRound {
     int gnx, gny, gnz;
 };
 constexpr int PSTR = 17; // row stride (cells) of the probe's psi tile
+constexpr int PRS = 3;   // stages of the mixed probe's psi read ring (chunks k .. k + 2)
+
+// 8-byte asynchronous global -> shared copy (zero fill when !valid; src is not read then)
+__device__ __forceinline__ void cp_async8(double *dst, const double *src, bool valid)
+{
+    const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src),
+                 "r"(valid ? 8 : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait()
+{
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
 template <int NT, int NT2, int KIND, bool ZD>
 __global__ void __launch_bounds__(RW * 32, KIND == 1 ? 1 : KIND == 2 ? 3 : 2)
     rounds_pass_mixed_kernel(ClosureParams P, const double *__restrict__ f64c,
@@ -537,13 +553,16 @@ __global__ void __launch_bounds__(RW * 32, KIND == 1 ? 1 : KIND == 2 ? 3 : 2)
     double2 *alph = reinterpret_cast<double2 *>(cbuf + QC * CST2);          // RW x nm
     double *zbuf = reinterpret_cast<double *>(alph + RW * nm);              // ZD: QC x ZS
     double *psiT = zbuf + (ZD ? QC * ZS : 0);                               // probe: QC x PSTR
-    long long *psiCell = reinterpret_cast<long long *>(psiT + (KIND == 2 ? QC * PSTR : 0));
+    double *psiR = psiT + (KIND == 2 ? QC * PSTR : 0); // mixed probe: PRS x QC x PSTR
+    long long *psiCell =
+        reinterpret_cast<long long *>(psiR + (KIND == 2 && ZD ? PRS * QC * PSTR : 0));
     uint64_t *full = reinterpret_cast<uint64_t *>(psiCell + (KIND == 2 ? MXC : 0));
     uint64_t *mmab = full + GSTAGES;
     uint64_t *fin = mmab + GSTAGES;
     __shared__ uint32_t s_tmem;
     __shared__ int s_abort;
     __shared__ int s_shift[MXC];
+    __shared__ long long s_gc[MXC];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int base = blockIdx.x * MXC;
     // first round of a grid closure: hand the ansatz of every direction to the kinetic flux,
@@ -553,6 +572,7 @@ __global__ void __launch_bounds__(RW * 32, KIND == 1 ? 1 : KIND == 2 ? 3 : 2)
     const bool valid = emit && first.psiValid && *first.psiValid != 0;
     long long cell[2];
     double scale[2], u0e[2] = {0.0, 0.0};
+    int needMine = 0; // lane 0: one of the warp's cells has its psi written by this pass
 #pragma unroll
     for (int e = 0; e < 2; ++e) {
         const int pos = base + 2 * warp + e;
@@ -576,6 +596,8 @@ __global__ void __launch_bounds__(RW * 32, KIND == 1 ? 1 : KIND == 2 ? 3 : 2)
                     need = in == 2;
                 }
                 psiCell[2 * warp + e] = need ? gc : -1;
+                s_gc[2 * warp + e] = gc;
+                needMine |= need && gc >= 0;
             }
         for (int i = lane; i < nm; i += 32) {
             double a = 0.0;
@@ -618,9 +640,36 @@ __global__ void __launch_bounds__(RW * 32, KIND == 1 ? 1 : KIND == 2 ? 3 : 2)
         if (warp == 0)
             tmem_alloc(&s_tmem, 32);
     tc_fence_before();
-    __syncthreads();
+    const int anyNeed = __syncthreads_or(needMine);
     tc_fence_after();
     const uint32_t tmem = TC ? s_tmem : 0u;
+    // mixed probe with psi valid and no cell of the CTA needing its psi written: psi already
+    // holds u_0 e^{alpha_scaled . m_q} of every cell, so the pass reads e^{alpha_scaled . m_q}
+    // back (psi / u_0) instead of forming the exponent tile and the exponentials; the reads
+    // run two chunks ahead through a ring of asynchronous copies
+    const bool rd = ZD && valid && !anyNeed;
+    auto psi_fetch = [&](int kc) {
+        double *dst = psiR + (kc % PRS) * QC * PSTR;
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            const int row = 4 * warp + 2 * i + (lane >> 4), j = lane & 15;
+            const int q = kc * QC + row;
+            const long long gc = s_gc[j];
+            const bool ok = kc < nchunks && gc >= 0 && q < P.nq;
+            cp_async8(dst + row * PSTR + j, ok ? first.psi + (long long)q * first.nall + gc : first.psi,
+                      ok);
+        }
+        cp_async_commit();
+    };
+    if constexpr (KIND == 2 && ZD) {
+        if (rd) {
+            // u0e holds 1 / u_0 from here on: the read path writes no psi
+            u0e[0] = 1.0 / u0e[0];
+            u0e[1] = 1.0 / u0e[1];
+            psi_fetch(0);
+            psi_fetch(1);
+        }
+    }
     const double2 *aw = alph + warp * nm;
     double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
     double fpart0 = 0.0, fpart1 = 0.0, cmax0 = 0.0, cmax1 = 0.0;
@@ -629,12 +678,22 @@ __global__ void __launch_bounds__(RW * 32, KIND == 1 ? 1 : KIND == 2 ? 3 : 2)
         const uint32_t s = k % GSTAGES, parity = (k / GSTAGES) & 1u;
         if (!mbar_wait(&full[s], parity))
             s_abort = 1;
+        if constexpr (KIND == 2 && ZD)
+            if (rd)
+                cp_async_wait<1>(); // this thread's copies of chunk k have landed
         if (__syncthreads_or(s_abort))
             break;
         const unsigned char *stb = smem_raw + s * stg;
         const double *ch = reinterpret_cast<const double *>(stb);
-        double z0 = 0.0, z1 = 0.0;
-        if constexpr (ZD) {
+        double z0 = 0.0, z1 = 0.0, ez0 = 0.0, ez1 = 0.0;
+        if (KIND == 2 && ZD && rd) {
+            // stage (k + 2) % PRS was last read in chunk k - 1, before the barrier above
+            psi_fetch(k + 2);
+            const double *pr = psiR + (k % PRS) * QC * PSTR + lane * PSTR + 2 * warp;
+            const bool qv = k * QC + lane < P.nq; // padded directions: exponent 0
+            ez0 = cell[0] >= 0 && qv ? pr[0] * u0e[0] : 1.0;
+            ez1 = cell[1] >= 0 && qv ? pr[1] * u0e[1] : 1.0;
+        } else if constexpr (ZD) {
             // A[dir r][k] = M2[k][8 dt + r], B[k][cell n] = alpha_n[k] (zero for k >= nm)
             const int dt = warp & 3, ct = warp >> 2, r = lane >> 2, kq = lane & 3;
             const int nb = 8 * ct + r;
@@ -665,9 +724,12 @@ __global__ void __launch_bounds__(RW * 32, KIND == 1 ? 1 : KIND == 2 ? 3 : 2)
             }
         }
         const double wq = ch[nm * QCP + lane];
-        const double ez0 = exp(z0), ez1 = exp(z1);
+        if (!(KIND == 2 && ZD && rd)) {
+            ez0 = exp(z0);
+            ez1 = exp(z1);
+        }
         if constexpr (KIND == 2) {
-            if (emit) {
+            if (emit && !rd) {
                 psiT[lane * PSTR + 2 * warp] = u0e[0] * ez0;
                 psiT[lane * PSTR + 2 * warp + 1] = u0e[1] * ez1;
             }
@@ -728,7 +790,7 @@ __global__ void __launch_bounds__(RW * 32, KIND == 1 ? 1 : KIND == 2 ? 3 : 2)
         }
         if constexpr (KIND == 2) {
             // the chunk's psi rows: warp w stores directions 4w .. 4w + 3, 16 cells each
-            if (emit) {
+            if (emit && !rd) {
 #pragma unroll
                 for (int i = 0; i < 2; ++i) {
                     const int row = 4 * warp + 2 * i + (lane >> 4), j = lane & 15;
@@ -766,6 +828,9 @@ __global__ void __launch_bounds__(RW * 32, KIND == 1 ? 1 : KIND == 2 ? 3 : 2)
             }
         }
     }
+    if constexpr (KIND == 2 && ZD)
+        if (rd)
+            cp_async_wait<0>(); // no copy outstanding past the loop (an abort leaves it early)
     // every MMA complete before the accumulators are read and the columns freed
     if (TC && tid == 0) {
         umma_commit(fin);
@@ -1058,7 +1123,8 @@ template <int NT, int KIND, bool ZD> static size_t mixed_pass_smem(const Closure
     const size_t stg = f64Pad + (KIND < 2 ? mixed_a_chunk_bytes(nm2, KIND) : 0);
     return GSTAGES * stg + GSTAGES * (size_t)K::NP * MXC * QC * K::ES + (size_t)QC * CST2 * 8 +
            (size_t)RW * P.nm * 16 + (ZD ? (size_t)QC * ZS * 8 : 0) +
-           (KIND == 2 ? (size_t)QC * PSTR * 8 + MXC * 8 : 0) + (2 * GSTAGES + 1) * 8;
+           (KIND == 2 ? (size_t)QC * PSTR * 8 + MXC * 8 : 0) +
+           (KIND == 2 && ZD ? (size_t)PRS * QC * PSTR * 8 : 0) + (2 * GSTAGES + 1) * 8;
 }
 
 // ---------------------------------------------------------------- graph-resident round loop
