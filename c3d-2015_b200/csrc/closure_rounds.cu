@@ -141,6 +141,7 @@ template <int NT> using TSlot = Slot<NT, true>;
 template <int NT> struct alignas(16) ProbeSlot {
     static constexpr int NMP = Cfg<NT>::NMP;
     double u[NMP], alpha[NMP], alpha0[NMP], uOrig[NMP], g[NMP], d[NMP], alphaOld[NMP];
+    double pm[NMP + 8]; // the cell's probe entry, loaded before the cell's state
     SlotScalars s;
 };
 template <int NT, int MODE>
@@ -958,6 +959,15 @@ __global__ void __launch_bounds__(RWN * 32)
     const long long cell = active ? (list ? list[pos] : first.off + pos) : -1;
     const bool needH = MODE != 2 && active && state[cell].s.need == NEED_H;
     SlotT &sl = slots[warp];
+    // probe visits: the probe entry's loads go out before the cell's state is read, so the
+    // two global round trips overlap
+    constexpr int PMR = (BSTR + 31) / 32;
+    double pmr[PMR];
+    if constexpr (MODE == 2)
+        if (active)
+#pragma unroll
+            for (int r = 0; r < PMR; ++r)
+                pmr[r] = lane + 32 * r < BSTR ? buf[(size_t)pos * BSTR + lane + 32 * r] : 0.0;
     C3D_NCLK_DECL
     long long gcell = -1; // probe visits: the grid cell, for the ansatz hand-off's refresh list
     if (MODE == 2 && active && first.refresh)
@@ -1026,8 +1036,14 @@ __global__ void __launch_bounds__(RWN * 32)
     if (active) {
     C3D_NCLK(O.stats, 0, lane);
     if constexpr (MODE == 2) {
-        if (sl.s.need == NEED_PROBE)
-            after_probe(sl, P, O, lane, m0, buf + (size_t)pos * BSTR, g0, g0n);
+        if (sl.s.need == NEED_PROBE) {
+#pragma unroll
+            for (int r = 0; r < PMR; ++r)
+                if (lane + 32 * r < BSTR)
+                    sl.pm[lane + 32 * r] = pmr[r];
+            __syncwarp();
+            after_probe(sl, P, O, lane, m0, sl.pm, g0, g0n);
+        }
     } else if (sl.s.need == NEED_H) {
         if (lane == 0) {
             sl.s.hprec = MIX ? level : 0;
