@@ -31,6 +31,19 @@ def pytest_collection_modifyitems(config, items):
             it.add_marker(skip)
 
 
+def pytest_terminal_summary(terminalreporter):
+    """Tie exemptions of the closure parity checks that ran: cells checked, cells exempted
+    as rounding ties, and how many of those differ from the oracle in iteration count."""
+    mod = sys.modules.get("oracle_lib")
+    log = getattr(mod, "TIE_LOG", None)
+    if not log:
+        return
+    terminalreporter.section("rounding-tie exemptions")
+    for label, n, ties, differ in log:
+        terminalreporter.write_line(f"{label}: {ties} tie cells of {n}, {differ} of them with "
+                                    f"another iteration count")
+
+
 @pytest.fixture(scope="session")
 def oracle():
     from oracle_lib import Oracle

@@ -81,6 +81,18 @@ TIE_COND_REL = 0.5
 TIE_GAMMA_REL = 1e-2
 
 
+TIE_LOG = []
+
+
+def log_ties(label, ties, mism):
+    """Records, per parity check, how many cells were exempted as rounding ties and how many
+    of those actually took another iteration count than the oracle, so that a regression
+    hiding inside the exemption shows in the run's summary (tests/conftest.py prints it)."""
+    test = os.environ.get("PYTEST_CURRENT_TEST", "").split("::")[-1].split(" ")[0]
+    label = f"{test} {label}" if test and not label.startswith(test.split("[")[0]) else label
+    TIE_LOG.append((label, int(len(ties)), int(ties.sum()), int((mism & ties).sum())))
+
+
 def tie_cells(records):
     """Boolean mask of cells whose solve met a rounding-tie decision, or ran into the
     iteration cap (MN_MAX_ITER Newton steps without converging: the iterates of such a solve

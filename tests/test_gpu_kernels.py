@@ -12,7 +12,7 @@ import numpy as np
 import pytest
 
 import c3d
-from oracle_lib import make_opts, tie_cells
+from oracle_lib import log_ties, make_opts, tie_cells
 
 pytestmark = pytest.mark.gpu
 
@@ -104,6 +104,7 @@ def test_closure_matches_oracle(oracle, batched):
     assert (rec["status"] == 0).all()
     ties = tie_cells(out)
     mism = rec["iters"] != out["totalIter"]
+    log_ties(f"test_closure_matches_oracle[batched={batched}]", ties, mism)
     assert not (mism & ~ties).any(), np.nonzero(mism & ~ties)[0][:10]
     ok = ~ties & (rec["regIndex"] == out["regIndex"])
     ag = ag.reshape(-1, nm)
@@ -157,6 +158,7 @@ def test_step_stages_match_oracle(oracle):
             rec = ctx.records()
             ties = tie_cells(out)
             mism = rec["iters"] != out["totalIter"]
+            log_ties("test_step_stages_match_oracle", ties, mism)
             assert not (mism & ~ties).any()
             if (rec["regIndex"] != out["regIndex"]).any():
                 ctx.set_state(u=u, alpha=a)  # continue from the oracle's state
@@ -334,6 +336,7 @@ def test_gaunt_closure_matches_oracle(oracle, mode, N, Q):
     assert (rec["status"] == 0).all()
     ties = tie_cells(out)
     mism = rec["iters"] != out["totalIter"]
+    log_ties(f"test_gaunt_closure_matches_oracle[mode={mode},N={N},Q={Q}]", ties, mism)
     assert not (mism & ~ties).any(), np.nonzero(mism & ~ties)[0][:10]
     ok = ~ties & (rec["regIndex"] == out["regIndex"])
     ag = ag.reshape(-1, nm)
@@ -371,6 +374,7 @@ def test_engines_match_oracle(oracle, engine, gaunt):
     assert (rec["status"] == 0).all()
     ties = tie_cells(out)
     mism = rec["iters"] != out["totalIter"]
+    log_ties(f"test_engines_match_oracle[engine={engine},gaunt={gaunt}]", ties, mism)
     assert not (mism & ~ties).any(), np.nonzero(mism & ~ties)[0][:10]
     ok = ~ties & (rec["regIndex"] == out["regIndex"])
     ag = ag.reshape(-1, nm)

@@ -14,7 +14,7 @@ import numpy as np
 import pytest
 
 import c3d
-from oracle_lib import deck_text, make_opts, tie_cells
+from oracle_lib import deck_text, log_ties, make_opts, tie_cells
 from test_gpu_kernels import _gaunt_csr
 
 pytestmark = pytest.mark.gpu
@@ -71,6 +71,7 @@ def test_m6_cells_match_oracle(oracle, tmp_path):
         ctx.close()
         assert (stg == 0).all(), engine
         mism = itg != ro["totalIter"]
+        log_ties(f"test_m6_cells_match_oracle[engine={engine}]", ties, mism)
         assert not (mism & ~ties).any(), (engine, int((mism & ~ties).sum()))
         ok = ~mism & (ro["status"] == 0)
         rel = np.linalg.norm(ag[ok] - ao[ok], axis=1) / np.linalg.norm(ao[ok], axis=1)
@@ -123,6 +124,7 @@ def test_m6_grid_stages_match_oracle(oracle, tmp_path):
             ties_total += int(ties.sum())
             multi += int((out["totalIter"] > 1).sum())
             mism = (rec["iters"] != out["totalIter"]) | (rec["regIndex"] != out["regIndex"])
+            log_ties(f"test_m6_grid_stages_match_oracle[step={step},stage={stage}]", ties, mism)
             bad = np.nonzero(mism & ~ties)[0][:6]
             assert len(bad) == 0, (step, stage, [
                 (int(c), int(rec["iters"][c]), int(out["totalIter"][c]), int(rec["regIndex"][c]),

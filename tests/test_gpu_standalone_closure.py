@@ -12,7 +12,7 @@ import numpy as np
 import pytest
 
 import c3d
-from oracle_lib import make_opts, tie_cells
+from oracle_lib import log_ties, make_opts, tie_cells
 
 pytestmark = pytest.mark.gpu
 
@@ -63,6 +63,7 @@ def test_standalone_closure_matches_oracle(oracle, N):
     ties = tie_cells(ro)
     assert np.array_equal(stg, ro["status"])
     mism = itg != ro["totalIter"]
+    log_ties(f"test_standalone_closure_matches_oracle[N={N}]", ties, mism)
     assert not (mism & ~ties).any(), (N, int((mism & ~ties).sum()))
     ok = ~ties & (rgg == ro["regIndex"]) & (ro["status"] == 0)
     rel = np.linalg.norm(ag[ok] - ao[ok], axis=1) / np.linalg.norm(ao[ok], axis=1)

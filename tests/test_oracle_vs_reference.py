@@ -16,7 +16,7 @@ import numpy as np
 import pytest
 
 import c3d
-from oracle_lib import (REF_SO, deck_text, make_opts, run_reference, tie_cells)
+from oracle_lib import (REF_SO, deck_text, log_ties, make_opts, run_reference, tie_cells)
 
 pytestmark = pytest.mark.skipif(not os.path.exists(REF_SO), reason="reference build absent")
 
@@ -145,6 +145,7 @@ def test_closure_steps_vs_reference(oracle, batched, ladder, gaunt):
         it_ref, _, reg_ref = ref["iters"][s]
         ties = tie_cells(rec)
         mism = rec["totalIter"] != it_ref
+        log_ties(f"oracle vs reference, step {s}", ties, mism)
         assert not (mism & ~ties).any(), np.nonzero(mism & ~ties)[0][:10]
         total_mism += int(mism.sum())
         if (rec["regIndex"] == reg_ref).all():
@@ -190,6 +191,7 @@ def test_standalone_closure_vs_reference(oracle):
     out = oracle.closure(make_opts(nm, nq, batched=False), T, uo, ao)
     ties = tie_cells(out)
     mism = out["totalIter"] != it_ref
+    log_ties("oracle vs reference opt(), unbatched", ties, mism)
     assert not (mism & ~ties).any()
     ok = ~ties & (out["regIndex"] == 0)
     assert np.abs(ao[ok] - a_ref[ok]).max() <= 1e-10 * max(1.0, np.abs(a_ref).max())

@@ -144,7 +144,7 @@ def test_noalloc_matches_oracle(oracle):
     M_4 vectors, on its own: identical Newton iteration counts and statuses except rounding
     ties (the oracle's margins), multipliers within 1e-10 relative on the other vectors."""
     import torch
-    from oracle_lib import make_opts, tie_cells
+    from oracle_lib import log_ties, make_opts, tie_cells
     q = c3d.quadrature(4, 20)
     T = oracle.tables(4, 20)
     assert np.array_equal(T["M"], q["M"])
@@ -158,6 +158,7 @@ def test_noalloc_matches_oracle(oracle):
     ties = tie_cells(ro)
     assert np.array_equal(stn, ro["status"])
     mism = itn != ro["totalIter"]
+    log_ties("test_noalloc_matches_oracle", ties, mism)
     assert not (mism & ~ties).any(), int((mism & ~ties).sum())
     ok = ~ties & (ro["status"] == 0)
     rel = np.linalg.norm(an[ok] - ao[ok], axis=1) / np.linalg.norm(ao[ok], axis=1)
