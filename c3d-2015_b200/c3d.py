@@ -49,6 +49,7 @@ HEADER_SYMBOLS = [
     "c3d_set_certificate", "c3d_autotune", "c3d_closure_vectors_noalloc_check",
     "c3d_set_limits", "c3d_set_ansatz_handoff", "c3d_set_graphs", "c3d_group_create",
     "c3d_group_closure_vectors", "c3d_group_step", "c3d_group_destroy", "c3d_stage_part",
+    "c3d_gaunt_build",
 ]
 
 
@@ -116,6 +117,9 @@ def lib():
                                        ctypes.POINTER(vp)]
         L.c3d_build_quadrature.argtypes = [ctypes.c_int, ctypes.c_int] + [_dp] * 6
         L.c3d_set_gaunt.argtypes = [vp, ctypes.c_int, _dp, _ip, _ip, _dp]
+        L.c3d_gaunt_build.argtypes = [ctypes.c_int] * 3 + [_dp, ctypes.c_double, _dp, _ip,
+                                      ctypes.c_longlong, _ip, _dp,
+                                      ctypes.POINTER(ctypes.c_longlong)]
         L.c3d_set_engine.argtypes = [vp, ctypes.c_int]
         L.c3d_set_precision.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                         ctypes.c_int, ctypes.c_double]
@@ -187,6 +191,26 @@ def check(status, what=""):
 
 def _p(a):
     return None if a is None else a.ctypes.data
+
+
+def gaunt_build(nm, nm2, nq, M2, threshold=1e-13):
+    """The Gaunt tables built on the device (c3d_gaunt_build): the dense table
+    beta[nm*nm, nm2] and the CSR of its entries above the threshold (rowPtr, colInd, val),
+    in the form c3d_set_gaunt takes."""
+    M2 = np.ascontiguousarray(M2, dtype=np.float64)
+    if M2.size != nq * nm2:
+        raise C3DError("gaunt_build: M2 must hold nq * nm2 values")
+    beta = np.zeros(nm * nm * nm2)
+    row = np.zeros(nm * nm + 1, np.int32)
+    cap = nm * nm * nm2
+    col, val = np.zeros(cap, np.int32), np.zeros(cap)
+    nnz = ctypes.c_longlong(0)
+    check(lib().c3d_gaunt_build(nm, nm2, nq, M2.ctypes.data_as(_dp), threshold,
+                                beta.ctypes.data_as(_dp), row.ctypes.data_as(_ip), cap,
+                                col.ctypes.data_as(_ip), val.ctypes.data_as(_dp),
+                                ctypes.byref(nnz)), "gaunt_build")
+    n = nnz.value
+    return beta.reshape(nm * nm, nm2), row, col[:n].copy(), val[:n].copy()
 
 
 def quadrature(N, Q, with_m2=False):

@@ -210,6 +210,20 @@ c3d_status c3d_closure_stats_reset(c3d_ctx *ctx);
 c3d_status c3d_set_gaunt(c3d_ctx *ctx, int nm2, const double *M2, const int *rowPtr,
                          const int *colInd, const double *val);
 
+/* The Gaunt tables built on the device (replaces the host loop of src/init.cpp:288-336).
+ * beta_ij is the least-squares solution of M2 beta_ij = m_i .* m_j over the nq quadrature
+ * points (one Householder QR of M2, then one solve per pair, pair = i*nm + j); the sparse
+ * table keeps |beta| > threshold (1e-13 for MN_USE_GAUNT_SPARSE) in (pair, k) order, as
+ * c3d_set_gaunt takes it. M2[nq*nm2] (q-major, the host layout of src/global.h IM2) and all
+ * outputs are host arrays: beta[nm*nm*nm2] (dense, may be NULL), rowPtr[nm*nm+1] with
+ * colInd/val of room for capacity entries (all three NULL: count only); *nnz receives the
+ * entry count (C3D_ERR_INVALID when it exceeds capacity). Needs nm <= nm2 <= nq and
+ * (nq + nm2) * 8 <= 200 KiB. Allocates device memory for the call and synchronises. The
+ * sums run in another order than the host build's, so the values agree to rounding. */
+c3d_status c3d_gaunt_build(int nm, int nm2, int nq, const double *M2, double threshold,
+                           double *beta, int *rowPtr, long long capacity, int *colInd,
+                           double *val, long long *nnz);
+
 /* Closure engine: 0 (default) runs rounds over a device work list -- a pass kernel for
  * the quadrature sums of every listed cell, then a Newton kernel with one warp per cell,
  * re-listing cells that need another pass (the reference's Optimization::opt stacks,
