@@ -630,6 +630,27 @@ SERVE_BUDGET = 150 << 30  # device-memory budget of the admitted problems
 SERVE_SLOTS = 64          # problems active at once at most
 
 
+def gaunt_table_times(c3d, N, Q):
+    """Seconds to build the Gaunt tables of order N over the Q-point quadrature: on the host
+    (c3d_gaunt_dense, the least-squares loop of the reference's init) and on the device
+    (c3d_gaunt_build, second call), with the largest difference between the two."""
+    q = c3d.quadrature(N, Q, with_m2=True)
+    nm, nm2, nq = q["nm"], q["nm2"], q["nq"]
+    L = c3d.lib()
+    L.c3d_gaunt_dense.argtypes = [ctypes.c_int] * 3 + [ctypes.POINTER(ctypes.c_double)] * 2
+    beta = np.zeros(nm * nm * nm2)
+    t0 = time.perf_counter()
+    L.c3d_gaunt_dense(nm, nm2, nq, q["M2"].ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                      beta.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+    host = time.perf_counter() - t0
+    c3d.gaunt_build(nm, nm2, nq, q["M2"])
+    t0 = time.perf_counter()
+    dev = c3d.gaunt_build(nm, nm2, nq, q["M2"])[0]
+    device = time.perf_counter() - t0
+    return dict(N=N, Q=Q, host_s=round(host, 4), device_s=round(device, 4),
+                max_abs_diff=float(np.abs(dev.ravel() - beta).max()))
+
+
 def serving_stream(n_problems, mixed):
     """The serving workload's seeded problem stream: cubic grid with edge uniform in 16..96,
     N in {1, 3, 5}, sigma_s uniform in [0.5, 20], a Gaussian pulse of width uniform in
@@ -1074,6 +1095,8 @@ def b200_arm(args):
                                           p50_s=round(serving[a]["latency_p50_s"], 3),
                                           p99_s=round(serving[a]["latency_p99_s"], 3))
                                   for a in ("mixed", "fp64")}
+        wl = CONFIGS[cfg]
+        summary["gaunt_tables"] = gaunt_table_times(c3d, wl["N"], wl["Q"])
         if summary:
             line["workloads"] = summary
         if compare is not None:

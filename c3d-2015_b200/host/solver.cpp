@@ -84,6 +84,7 @@ std::string parse_config(const InputDeck &d, Config &c)
             return "REG_LADDER must list 1 to 16 values";
     }
     d.get("MN_REPROJECT", c.mnReproject);
+    d.get("MN_GAUNT_ON_DEVICE", c.mnGauntOnDevice);
     d.get("MN_MIXED_PRECISION", c.mnMixed);
     d.get("MN_MIXED_COND_BF16", c.mnMixedCondBf16);
     d.get("MN_MIXED_COND_MAX", c.mnMixedCondMax);
@@ -242,7 +243,7 @@ void Solver::prepare(const Config &cfg)
     }
 }
 
-void Solver::prepare_gaunt()
+c3d_status Solver::prepare_gaunt()
 {
     // Gaunt coefficients by least squares over the quadrature (src/init.cpp:287-336)
     const int N = cfg_.momentOrder, nm = nm_, nq = nq_;
@@ -251,9 +252,25 @@ void Solver::prepare_gaunt()
     M2.assign((size_t)nq * nm2, 0.0);
     c3d_build_quadrature(N, cfg_.quadOrder, w2.data(), xi2.data(), eta2.data(), mu2.data(),
                          M1.data(), M2.data());
+    double thr = cfg_.mnUseGauntSparse ? 1e-13 : 0.0;
+    if (cfg_.mnGauntOnDevice) {
+        // the same least-squares tables built on the device (values agree to rounding)
+        const long long cap = (long long)nm * nm * nm2;
+        betaRow.assign((size_t)nm * nm + 1, 0);
+        betaCol.assign((size_t)cap, 0);
+        betaVal.assign((size_t)cap, 0.0);
+        long long nnz = 0;
+        c3d_status s = c3d_gaunt_build(nm, nm2, nq, M2.data(), thr, nullptr, betaRow.data(), cap,
+                                       betaCol.data(), betaVal.data(), &nnz);
+        if (s != C3D_OK)
+            return s;
+        betaCol.resize(nnz > 0 ? (size_t)nnz : 1);
+        betaVal.resize(nnz > 0 ? (size_t)nnz : 1);
+        nm2_ = nm2;
+        return C3D_OK;
+    }
     std::vector<double> beta((size_t)nm * nm * nm2);
     c3d_gaunt_dense(nm, nm2, nq, M2.data(), beta.data());
-    double thr = cfg_.mnUseGauntSparse ? 1e-13 : 0.0;
     int nnz = c3d_gaunt_csr_threshold(nm, nm2, beta.data(), thr, nullptr, nullptr, nullptr);
     betaRow.assign((size_t)nm * nm + 1, 0);
     betaCol.assign(nnz > 0 ? nnz : 1, 0);
@@ -261,6 +278,7 @@ void Solver::prepare_gaunt()
     c3d_gaunt_csr_threshold(nm, nm2, beta.data(), thr, betaVal.data(), betaCol.data(),
                             betaRow.data());
     nm2_ = nm2;
+    return C3D_OK;
 }
 
 c3d_status Solver::init(const Config &cfg, void *stream)
@@ -275,7 +293,8 @@ c3d_status Solver::init(const Config &cfg, void *stream)
             fprintf(stderr, "[c3d_b200] MN_USE_GAUNT_COEF: Gaunt form provided for N <= 7; the "
                             "closure forms H by direct quadrature (same H up to rounding)\n");
         } else {
-            prepare_gaunt();
+            if ((s = prepare_gaunt()) != C3D_OK)
+                return s;
             s = c3d_set_gaunt(ctx_, nm2_, M2.data(), betaRow.data(), betaCol.data(),
                               betaVal.data());
             if (s != C3D_OK)

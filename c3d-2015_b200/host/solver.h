@@ -47,6 +47,7 @@ struct Config {
     int mnMaxIter = 0;
     bool mnBatched = true, mnUseGaunt = false, mnUseGauntSparse = false;
     bool mnReproject = false; // optional MN_REPROJECT (readme.txt robustness note)
+    bool mnGauntOnDevice = false; // optional MN_GAUNT_ON_DEVICE: beta from c3d_gaunt_build
     bool mnMixed = false;     // optional MN_MIXED_PRECISION
     double mnMixedCondBf16 = 0.0, mnMixedCondMax = 0.0;
     int mnMixedIterMax = 0;
@@ -122,7 +123,7 @@ private:
     c3d_ctx *ctx_ = nullptr;
     c3d_params params_{};
     int nm_ = 0, nq_ = 0, nm2_ = 0;
-    void prepare_gaunt();
+    c3d_status prepare_gaunt();
     double dx_ = 0, dy_ = 0, dz_ = 0, maxDt_ = 0;
     int numUpdates_ = 0;
     std::vector<double> updateTimes_; // 8 seconds per update (OUTPUT_TIMINGS)

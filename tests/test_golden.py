@@ -107,15 +107,18 @@ def test_gpu_c1_golden(tmp_path):
 
 
 @pytest.mark.gpu
-def test_gpu_c2_golden(tmp_path):
+@pytest.mark.parametrize("gaunt_on_device", [False, True])
+def test_gpu_c2_golden(tmp_path, gaunt_on_device):
     """The M_4 64^3 deck with the sigma checkerboard (Gaunt sparse Hessian, MN_TOL 1e-6)
     against the reference's own CPU path: per-cell Newton iteration counts and ladder indices
     of all six closures of three steps identical (ghost cells included); after steps 1 and 3
     the interior moments of the 4096 sample cells and the moment sums over every x-, y- and
-    z-plane within 1e-12 relative L2."""
+    z-plane within 1e-12 relative L2. Also with the Gaunt tables built on the device
+    (MN_GAUNT_ON_DEVICE true), whose values differ from the host build's at rounding level."""
     mg = _golden_module()
     G = np.load(os.path.join(GOLD, "c2_m4_64.npz"))
-    s = c3d.Solver(_deck(tmp_path, mg.c2_deck("gaussian_psi")))
+    deck = mg.c2_deck("gaussian_psi") + ("MN_GAUNT_ON_DEVICE true\n" if gaunt_on_device else "")
+    s = c3d.Solver(_deck(tmp_path, deck))
     L = c3d.lib()
     dt = s.max_dt
     assert dt == float(G["dt"])
